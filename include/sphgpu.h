@@ -1,0 +1,172 @@
+/*
+ * sphgpu.h -- C ABI of the B200 SPH/CRKSPH hydro derivative path.
+ *
+ * This is the drop-in boundary for Spheral's fluid-hydro hot path.  A thin
+ * C++ adapter (GpuSPHHydroBase<Dim<3>>, shown in INTEGRATION.md) implements
+ * the Physics<Dim<3>> virtuals of the reference by calling these entry
+ * points, so the reference's integrators and drivers keep working unchanged.
+ *
+ * Conventions (all entry points):
+ *   - every call returns SPHGPU_OK (0) or a negative SPHGPU_ERR_* code; no
+ *     C++ exception crosses the ABI.  sphgpu_last_error() returns a
+ *     thread-local description of the last failure.
+ *   - host arrays use the reference's Field storage order: one AoS record
+ *     per node, internal nodes only.  Vector = (x,y,z); SymTensor =
+ *     (xx,xy,xz,yy,yz,zz) (GeomSymmetricTensor<3> element order,
+ *     src/Geometry/GeomSymmetricTensorBase.hh); Tensor = row major
+ *     (xx,xy,xz,yx,yy,yz,zx,zy,zz) (src/Geometry/GeomTensorBase.hh).
+ *   - the handle owns all device memory; the caller owns the handle.
+ *   - calls are synchronous with respect to the host unless stated.
+ */
+#ifndef SPHGPU_H
+#define SPHGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (replace Spheral::dbc::VERIFYError, src/Utilities/DBC.hh:20-40) */
+#define SPHGPU_OK                 0
+#define SPHGPU_ERR_ARG           -1  /* bad argument / unknown field key        */
+#define SPHGPU_ERR_CUDA          -2  /* CUDA runtime failure                    */
+#define SPHGPU_ERR_CAPACITY      -3  /* neighbor/ghost capacity exceeded        */
+#define SPHGPU_ERR_STATE         -4  /* call out of order (e.g. no neighbors)   */
+#define SPHGPU_ERR_UNSUPPORTED   -5  /* option outside the implemented subset   */
+#define SPHGPU_ERR_NUMERIC       -6  /* non-finite / non-positive state         */
+#define SPHGPU_ERR_NOMEM         -7  /* device allocation failed                */
+#define SPHGPU_ERR_ADMISSION     -8  /* serving: request exceeds memory budget  */
+
+/* ---- enumerations mirroring the reference's Python factory options ---- */
+#define SPHGPU_HYDRO_SPH          0  /* SPHHydroBase   (src/SPH/SPHHydroBase.hh:40)      */
+#define SPHGPU_HYDRO_CRKSPH       1  /* CRKSPHHydroBase (src/CRKSPH/CRKSPHHydroBase.hh:59) */
+
+#define SPHGPU_KERNEL_BSPLINE     0  /* BSplineKernel<Dim<3>>    (src/Kernel/BSplineKernelInline.hh) */
+#define SPHGPU_KERNEL_WENDLANDC4  1  /* WendlandC4Kernel<Dim<3>> (src/Kernel/WendlandC4KernelInline.hh) */
+
+#define SPHGPU_DENSITY_RIGOROUS_SUM 0 /* MassDensityType::RigorousSumDensity */
+#define SPHGPU_DENSITY_INTEGRATE    1 /* MassDensityType::IntegrateDensity   */
+
+#define SPHGPU_H_IDEAL            0  /* HEvolutionType::IdealH      */
+#define SPHGPU_H_INTEGRATE        1  /* HEvolutionType::IntegrateH  */
+
+#define SPHGPU_PRECISION_FP64     0  /* plain all-FP64 pair arithmetic                     */
+#define SPHGPU_PRECISION_MIXED    1  /* FP32 pair arithmetic, Kahan FP32 sums, FP64 state  */
+
+#define SPHGPU_CRK_SUMVOLUME      0  /* CRKVolumeType::CRKSumVolume       */
+#define SPHGPU_CRK_MASSOVERDENSITY 1 /* CRKVolumeType::CRKMassOverDensity */
+
+/* Problem configuration: every physics switch of SPHHydroBase's constructor
+ * (src/SPH/SPHHydroBase.cc:82-141), MonaghanGingoldViscosity
+ * (src/ArtificialViscosity/MonaghanGingoldViscosity.cc:43-50), GammaLawGas,
+ * the FluidNodeList limits (src/NodeList/FluidNodeLists.py:11-35), the periodic
+ * box (PeriodicBoundary pairs, src/Boundary/PeriodicBoundary.cc:67-73) and the
+ * integrator time-step controls (src/Integrator/Integrator.cc:166-212). */
+typedef struct sphgpu_config {
+  int32_t hydro;                 /* SPHGPU_HYDRO_*                       */
+  int32_t kernel;                /* SPHGPU_KERNEL_*                      */
+  int32_t num_points;            /* TableKernel numPoints (drivers: 1000) */
+  int32_t precision;             /* SPHGPU_PRECISION_*                   */
+  double  nPerh;                 /* nodes per smoothing scale            */
+  double  Cl, Cq, epsilon2;      /* Q coefficients, eps^2 (C++ default 1e-2) */
+  int32_t linearInExpansion;
+  int32_t quadraticInExpansion;
+  double  cfl;
+  double  epsTensile, nTensile;
+  double  hmin, hmax, hminratio;
+  double  rhoMin, rhoMax;
+  double  gamma;                 /* GammaLawGas gamma (mu irrelevant for P, cs) */
+  int32_t compatibleEnergyEvolution;
+  int32_t gradhCorrection;
+  int32_t XSPH;
+  int32_t correctVelocityGradient;
+  int32_t densityUpdate;         /* SPHGPU_DENSITY_*                     */
+  int32_t HUpdate;               /* SPHGPU_H_*                           */
+  int32_t useVelocityMagnitudeForDt;
+  int32_t crkVolumeType;         /* SPHGPU_CRK_* (CRKSPH only)            */
+  double  xmin[3], xmax[3];      /* periodic box planes                  */
+  int32_t periodic[3];           /* 1 = PeriodicBoundary along that axis */
+  int32_t max_neighbors;         /* per-node neighbor capacity (0 = 1024) */
+  double  dtMin, dtMax, dtGrowth, lastDt;  /* Integrator controls       */
+} sphgpu_config;
+
+typedef struct sphgpu_problem sphgpu_problem;
+
+/* Thread-local text of the last error (never NULL). */
+const char* sphgpu_last_error(void);
+
+/* Replaces the SPHHydroBase / CRKSPHHydroBase constructors plus
+ * initializeProblemStartup (src/SPH/SPHHydroBase.cc:82-230): builds the
+ * TableKernel, W(0) and nPerh tables and reserves device storage for
+ * n_internal nodes of one FluidNodeList on the current CUDA device. */
+int sphgpu_create(const sphgpu_config* cfg, int64_t n_internal, sphgpu_problem** out);
+void sphgpu_destroy(sphgpu_problem* p);
+
+/* Host -> device copy of the evolved state of the internal nodes, AoS as in
+ * the reference Fields ("position", "velocity", "mass", "mass density",
+ * "specific thermal energy", "H"); pressure and sound speed are recomputed
+ * from the EOS (SPHHydroBase::initializeProblemStartup, :194-197). */
+int sphgpu_set_state(sphgpu_problem* p, const double* position, const double* velocity,
+                     const double* mass, const double* massDensity,
+                     const double* specificThermalEnergy, const double* H);
+/* Same, from device pointers already resident on this GPU (no host copy). */
+int sphgpu_set_state_device(sphgpu_problem* p, const double* position, const double* velocity,
+                            const double* mass, const double* massDensity,
+                            const double* specificThermalEnergy, const double* H);
+int sphgpu_get_state(sphgpu_problem* p, double* position, double* velocity, double* mass,
+                     double* massDensity, double* specificThermalEnergy, double* H);
+
+/* State / StateDerivatives lookup by the reference's field key
+ * (src/Hydro/HydroFieldNames.cc), e.g. "delta velocity hydro",
+ * "delta specific thermal energy", "delta mass density", "new H",
+ * "velocity gradient", "pressure", "sound speed".  `count` is the number of
+ * doubles in `out` and must equal n_internal * components. */
+int sphgpu_get_field(sphgpu_problem* p, const char* key, double* out, int64_t count);
+int sphgpu_field_components(const char* key, int32_t* components);
+
+/* Integrator::setGhostNodes (src/Integrator/Integrator.cc:445-597) without
+ * ghost culling: periodic ghost images in boundary order x, y, z, then
+ * ConnectivityMap::computeConnectivity (src/Neighbor/ConnectivityMap.cc:521-890). */
+int sphgpu_build_neighbors(sphgpu_problem* p);
+int sphgpu_connectivity_size(sphgpu_problem* p, int64_t* num_ghosts, int64_t* num_entries);
+/* CSR of the ConnectivityMap: offsets[n_internal+1], neighbors[num_entries]
+ * sorted ascending per node (ghost j >= n_internal), and for each ghost the
+ * internal node it images (ghost_root[num_ghosts]).  Any pointer may be NULL. */
+int sphgpu_get_connectivity(sphgpu_problem* p, int64_t* offsets, int32_t* neighbors,
+                            int32_t* ghost_root);
+
+/* Physics::initialize (SPHHydroBase::initialize, src/SPH/SPHHydroBase.cc:430-466;
+ * CRKSPHHydroBase::initialize, src/CRKSPH/CRKSPHHydroBase.cc:583-641). */
+int sphgpu_initialize(sphgpu_problem* p, double time, double dt);
+/* Physics::evaluateDerivatives (src/SPH/SPHHydroBase.cc:471-928;
+ * src/CRKSPH/CRKSPHHydroBase.cc:646-1102).  Derivatives are zeroed first
+ * (StateDerivatives::Zero, src/DataBase/StateDerivatives.cc:155). */
+int sphgpu_evaluate_derivatives(sphgpu_problem* p, double time, double dt);
+/* Physics::finalizeDerivatives (src/SPH/SPHHydroBase.cc:933-957). */
+int sphgpu_finalize_derivatives(sphgpu_problem* p, double time, double dt);
+/* Physics::finalize (src/SPH/SPHHydroBase.cc:962-1105; CRK :1192-1332). */
+int sphgpu_finalize(sphgpu_problem* p, double time, double dt);
+/* GenericHydro::dt (src/Physics/GenericHydro.cc:114-331): cfl * min dt. */
+int sphgpu_dt(sphgpu_problem* p, double* dt_out);
+/* CheapSynchronousRK2::step (src/Integrator/CheapSynchronousRK2.cc:81-143),
+ * nsteps times; *time advances, *last_dt receives the last step size. */
+int sphgpu_step_rk2(sphgpu_problem* p, double* time, int64_t nsteps, double* last_dt);
+/* SpheralConservation (src/SimulationControl/SpheralConservation.py:27-63):
+ * out = {mass, px, py, pz, kinetic E, thermal E, total E, 0}, FP64 on device. */
+int sphgpu_conservation(sphgpu_problem* p, double out[8]);
+
+/* Pair interactions (the reference's ncalc summed over nodes,
+ * src/SPH/SPHHydroBase.cc:674) of the current connectivity. */
+int sphgpu_num_pairs(sphgpu_problem* p, int64_t* pairs);
+/* Synchronise the problem's stream; returns the first device error. */
+int sphgpu_synchronize(sphgpu_problem* p);
+/* CUDA stream the problem launches on (cudaStream_t as void*). */
+int sphgpu_get_stream(sphgpu_problem* p, void** stream);
+int sphgpu_set_stream(sphgpu_problem* p, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPHGPU_H */

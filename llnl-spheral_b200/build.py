@@ -1,0 +1,81 @@
+"""Build libsphgpu.so (CUDA sm_100a kernels + C-ABI) in-tree with nvcc.
+
+FP64 parity translation units are compiled with -fmad=false so that no FMA is
+contracted: their per-pair arithmetic matches the x86-64 FP64 reference bit
+for bit.  The mixed-precision unit keeps FMA contraction on.
+
+    python llnl-spheral_b200/build.py [--force] [--verbose]
+"""
+import argparse
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(BUILD, "libsphgpu.so")
+NVCC = os.environ.get("NVCC", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+          "-I" + os.path.join(HERE, "..", "include")]
+# (source, extra flags)
+UNITS = [
+    ("api.cu", ["-fmad=false"]),
+    ("nbrs.cu", ["-fmad=false"]),
+    ("sph.cu", ["-fmad=false"]),
+    ("sph_mixed.cu", []),
+    ("table.cc", []),
+]
+HEADERS = ["devmath.cuh", "problem.cuh", "scan.cuh", "mixed.cuh"]
+
+
+def _mtime(p):
+    return os.path.getmtime(p) if os.path.exists(p) else 0.0
+
+
+def needs_build():
+    if not os.path.exists(LIB):
+        return True
+    t = _mtime(LIB)
+    deps = [os.path.join(CSRC, u) for u, _ in UNITS] + [os.path.join(CSRC, h) for h in HEADERS]
+    deps.append(os.path.join(HERE, "..", "include", "sphgpu.h"))
+    deps.append(os.path.abspath(__file__))
+    return any(_mtime(d) > t for d in deps)
+
+
+def build(force=False, verbose=False, ptxas_info=False):
+    if not force and not needs_build():
+        return LIB
+    os.makedirs(BUILD, exist_ok=True)
+    objs = []
+    for src, extra in UNITS:
+        path = os.path.join(CSRC, src)
+        if not os.path.exists(path):
+            continue
+        obj = os.path.join(BUILD, src + ".o")
+        cmd = [NVCC] + ARCH + COMMON + extra + ["-c", path, "-o", obj]
+        if ptxas_info and src.endswith(".cu"):
+            cmd += ["-Xptxas", "-v"]
+        if src.endswith(".cc"):
+            cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off",
+                   "-fno-fast-math", "-c", path, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
+        objs.append(obj)
+    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--ptxas-info", action="store_true")
+    a = ap.parse_args()
+    print(build(force=a.force, verbose=a.verbose, ptxas_info=a.ptxas_info))
+    sys.exit(0)

@@ -1,0 +1,618 @@
+// SPH hydro kernels, plain FP64 form (compiled with -fmad=false).
+//
+// Replaces the reference's serial loops:
+//   pack_records         Integrator::applyGhostBoundaries (src/Integrator/Integrator.cc:602-660)
+//   sph_eval_fp64        SPHHydroBase::evaluateDerivatives (src/SPH/SPHHydroBase.cc:471-928)
+//   gradh                computeSPHOmegaGradhCorrection (src/SPH/computeSPHOmegaGradhCorrection.cc:28-137)
+//   sum_density          computeSPHSumMassDensity (src/SPH/computeSPHSumMassDensity.cc:27-111)
+//   compatible_energy    SpecificThermalEnergyPolicy::update (src/Hydro/SpecificThermalEnergyPolicy.cc:66-189)
+//   update               State::update with the SPH policies (src/DataBase/State.cc:166-287,
+//                        IncrementFieldList.cc:107-151, IncrementBoundedState.cc:120-136,
+//                        ReplaceBoundedState.cc:121-150, PressurePolicy/SoundSpeedPolicy)
+//   hydro_dt             GenericHydro::dt (src/Physics/GenericHydro.cc:114-331)
+//   enforce_boundaries   PeriodicBoundary violation mapping (src/Boundary/PeriodicBoundary.cc:145-203)
+//
+// Pair loops gather: one thread owns node i and walks its ascending CSR row.
+// The reference visits each unordered pair once, from the lower index (the
+// "owner"), and scatters to both nodes.  Here every pair term is formed in
+// owner orientation (r_ij = r_owner - r_other, owner-side Q, owner-side
+// tensile factor) and only node i's side is accumulated.  Node i's sums then
+// receive the same terms in the same order as in the reference: first the
+// pairs owned by lower indices (ascending), then its own (ascending, ghosts
+// last), with self terms inserted where the reference adds them.
+#include <cfloat>
+
+#include "problem.cuh"
+
+namespace sphgpu {
+
+namespace {
+
+constexpr double kFltMin = 1.17549435082228750797e-38;   // FLT_MIN
+constexpr double kFltMax = 3.40282346638528859812e+38;   // FLT_MAX
+constexpr double kDblEps = 2.220446049250313e-16;
+
+inline int nblk(int64_t work, int threads) {
+  int64_t b = (work + threads - 1)/threads;
+  return (int)(b < 1 ? 1 : b);
+}
+
+__device__ __forceinline__ double ldg(const double* p) { return __ldg(p); }
+
+struct Rec {
+  V3 r, v;
+  double m, rho, cs, Hdet;
+  Sym H;
+  double Prho, mrho, P, somega;
+};
+
+__device__ __forceinline__ Rec loadRec(const double* rec, int64_t k) {
+  const double2* q = reinterpret_cast<const double2*>(rec + k*RECW);
+  const double2 a0 = __ldg(q + 0), a1 = __ldg(q + 1), a2 = __ldg(q + 2), a3 = __ldg(q + 3), a4 = __ldg(q + 4);
+  const double2 a5 = __ldg(q + 5), a6 = __ldg(q + 6), a7 = __ldg(q + 7), a8 = __ldg(q + 8), a9 = __ldg(q + 9);
+  Rec R;
+  R.r = V3{a0.x, a0.y, a1.x};
+  R.v = V3{a1.y, a2.x, a2.y};
+  R.m = a3.x; R.rho = a3.y; R.cs = a4.x; R.Hdet = a4.y;
+  R.H = Sym{a5.x, a5.y, a6.x, a6.y, a7.x, a7.y};
+  R.Prho = a8.x; R.mrho = a8.y; R.P = a9.x; R.somega = a9.y;
+  return R;
+}
+
+__device__ __forceinline__ V3 selv(bool c, const V3& a, const V3& b) {
+  return V3{c ? a.x : b.x, c ? a.y : b.y, c ? a.z : b.z};
+}
+__device__ __forceinline__ Sym sels(bool c, const Sym& a, const Sym& b) {
+  return Sym{c ? a.xx : b.xx, c ? a.xy : b.xy, c ? a.xz : b.xz, c ? a.yy : b.yy, c ? a.yz : b.yz, c ? a.zz : b.zz};
+}
+
+// ---------------------------------------------------------------- records
+__global__ void pack_records_kernel(const double* S, int64_t n, const int32_t* groot, const uint32_t* gcode,
+                                    int64_t ntot, BoxBCs bcs, double* rec) {
+  for (int64_t k = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; k < ntot; k += (int64_t)gridDim.x*blockDim.x) {
+    const int64_t r = k < n ? k : groot[k - n];
+    V3 x{S[S_X*n + r], S[S_Y*n + r], S[S_Z*n + r]};
+    if (k >= n) x = ghostPosition(bcs, x, gcode[k - n]);
+    const Sym H{S[(S_H + 0)*n + r], S[(S_H + 1)*n + r], S[(S_H + 2)*n + r],
+                S[(S_H + 3)*n + r], S[(S_H + 4)*n + r], S[(S_H + 5)*n + r]};
+    const double m = S[S_M*n + r], rho = S[S_RHO*n + r], P = S[S_P*n + r];
+    const double somega = safeInv(S[S_OMEGA*n + r], 1.0e-30);
+    double2* q = reinterpret_cast<double2*>(rec + k*RECW);
+    q[0] = make_double2(x.x, x.y);
+    q[1] = make_double2(x.z, S[S_VX*n + r]);
+    q[2] = make_double2(S[S_VY*n + r], S[S_VZ*n + r]);
+    q[3] = make_double2(m, rho);
+    q[4] = make_double2(S[S_CS*n + r], sdet(H));
+    q[5] = make_double2(H.xx, H.xy);
+    q[6] = make_double2(H.xz, H.yy);
+    q[7] = make_double2(H.yz, H.zz);
+    q[8] = make_double2(somega*P/(rho*rho), m/rho);
+    q[9] = make_double2(P, somega);
+  }
+}
+
+// ---------------------------------------------------------------- derivatives
+// One directed pair (i, j) of SPHHydroBase::evaluateDerivatives, formed in
+// owner orientation, accumulated into node i.
+template<bool XSPH, bool TENSILE, bool COMPAT>
+__global__ void __launch_bounds__(128) sph_eval_fp64_kernel(Params P, const double* rec, int64_t n,
+                                                            const int64_t* offsets, const int32_t* nbr,
+                                                            double* D, double* pacc, int64_t ecap) {
+  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Rec I = loadRec(rec, i);
+  double rhoSum = 0.0, norm = 0.0, wns = 0.0, maxvp = 0.0, effvp = 0.0, viscW = 0.0, DepsDt = 0.0;
+  double XSPHw = 0.0;
+  V3 DvDt{0.0, 0.0, 0.0}, XSPHdv{0.0, 0.0, 0.0};
+  Sym m2{0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  T9 DvDx{0, 0, 0, 0, 0, 0, 0, 0, 0}, M{0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const double Cl = P.Cl*(0.5*(1.0 + 1.0)*1.0);   // Cl *= 0.5*(fCli + fClj)*fshear, multipliers 1
+  const double Cq = P.Cq*(0.5*(1.0 + 1.0)*1.0);
+  const int64_t k0 = offsets[i], k1 = offsets[i + 1];
+  for (int64_t k = k0; k < k1; ++k) {
+    const int32_t j = __ldg(nbr + k);
+    const Rec J = loadRec(rec, j);
+    const bool own = j > (int32_t)i;       // calculatePairInteraction: i is the owner
+    // owner side A, other side B
+    const V3 rA = selv(own, I.r, J.r), rB = selv(own, J.r, I.r);
+    const V3 vA = selv(own, I.v, J.v), vB = selv(own, J.v, I.v);
+    const Sym HA = sels(own, I.H, J.H), HB = sels(own, J.H, I.H);
+    const double HdetA = own ? I.Hdet : J.Hdet, HdetB = own ? J.Hdet : I.Hdet;
+    const double mA = own ? I.m : J.m, mB = own ? J.m : I.m;
+    const double rhoA = own ? I.rho : J.rho, rhoB = own ? J.rho : I.rho;
+    const double csA = own ? I.cs : J.cs, csB = own ? J.cs : I.cs;
+    const double mrhoA = own ? I.mrho : J.mrho, mrhoB = own ? J.mrho : I.mrho;
+
+    const V3 rij = vsub(rA, rB);
+    const V3 etaA = sdot(HA, rij);
+    const V3 etaB = sdot(HB, rij);
+    const double etaMagA = mag(etaA);
+    const double etaMagB = mag(etaB);
+    const V3 HetaA = sdot(HA, unitVector(etaA));
+    const V3 HetaB = sdot(HB, unitVector(etaB));
+    double WA, gWA, WB, gWB;
+    tableKernelAndGrad(P.W, etaMagA, HdetA, WA, gWA);
+    tableKernelAndGrad(P.W, etaMagB, HdetB, WB, gWB);
+    const V3 gradWA = vmul(HetaA, gWA);
+    const V3 gradWB = vmul(HetaB, gWB);
+    // node i's side of the symmetric quantities
+    const double Wi = own ? WA : WB;
+    const double gWi = own ? gWA : gWB;
+    const V3 gradWi = selv(own, gradWA, gradWB);
+
+    // moments for the ideal H
+    const double rij2 = mag2(rij);
+    const double thptS = safeInvVar(rij2*rij2*rij2);
+    wns += 1.0*fabs(gWi);
+    {
+      const double g2 = 1.0*mag2(gradWi);
+      const Sym thpt = smul(selfdyad(rij), thptS);
+      m2 = sadd(m2, smul(thpt, g2));
+    }
+    // sum density / normalization (single NodeList)
+    rhoSum += (own ? mB : mA)*Wi;
+    norm += (own ? mrhoA : mrhoB)*Wi;
+
+    // Monaghan-Gingold Pi_ij
+    const V3 vij = vsub(vA, vB);
+    const double muA = dot(vij, etaA)/(mag2(etaA) + P.eps2);
+    const double muB = dot(vij, etaB)/(mag2(etaB) + P.eps2);
+    const double mA0 = dmin(0.0, muA), mB0 = dmin(0.0, muB);
+    const double eA = -Cl*csA*(P.linearInExp ? muA : mA0) + Cq*(P.quadInExp ? -sgn(muA)*muA*muA : mA0*mA0);
+    const double eB = -Cl*csB*(P.linearInExp ? muB : mB0) + Cq*(P.quadInExp ? -sgn(muB)*muB*muB : mB0*mB0);
+    const double qA = eA/rhoA, qB = eB/rhoB;   // (e/rho) * Tensor::one
+    // 0.5*(Pi * gradWQ), with WQ = W (same table): the off-diagonal zeros of
+    // Pi only add signed zeros.
+    const V3 QaccA = vmul(vmul(gradWA, qA), 0.5);
+    const V3 QaccB = vmul(vmul(gradWB, qB), 0.5);
+    const double workQA = dot(vij, QaccA);
+    const double workQB = dot(vij, QaccB);
+    const double QA = rhoA*rhoA*fabs(qA);
+    const double QB = rhoB*rhoB*fabs(qB);
+    const double Qi = own ? QA : QB;
+    maxvp = dmax(maxvp, Qi);
+    effvp += (own ? mrhoB : mrhoA)*Qi*Wi;
+    viscW += (own ? mB : mA)*(own ? workQA : workQB);
+
+    // pressure terms (tensile correction uses the owner's W)
+    double PrhoA, PrhoB;
+    if (TENSILE) {
+      const double PA = own ? I.P : J.P, PB = own ? J.P : I.P;
+      const double sOA = own ? I.somega : J.somega, sOB = own ? J.somega : I.somega;
+      const double x = WA/(HdetA*P.WnPerh);
+      const double fij = P.epsTensile*(x*x*x*x);
+      const double RA = fij*(PA < 0.0 ? -PA : 0.0);
+      const double RB = fij*(PB < 0.0 ? -PB : 0.0);
+      PrhoA = sOA*(PA + RA)/(rhoA*rhoA);
+      PrhoB = sOB*(PB + RB)/(rhoB*rhoB);
+    } else {
+      PrhoA = own ? I.Prho : J.Prho;
+      PrhoB = own ? J.Prho : I.Prho;
+    }
+    const V3 deltaDvDt = vadd(vadd(vadd(vmul(gradWA, PrhoA), vmul(gradWB, PrhoB)), QaccA), QaccB);
+    DvDt = vadd(DvDt, vmul(deltaDvDt, own ? -mB : mA));
+    const double Prhoi = own ? PrhoA : PrhoB;
+    const double workQi = own ? workQA : workQB;
+    DepsDt += (own ? mB : mA)*(Prhoi*dot(vij, gradWi) + workQi);
+    if (COMPAT) {
+      pacc[k] = deltaDvDt.x;
+      pacc[ecap + k] = deltaDvDt.y;
+      pacc[2*ecap + k] = deltaDvDt.z;
+    }
+    const double mo = own ? mB : mA;      // the other node's mass
+    tsubfrom(DvDx, tmul(dyad(vij, gradWi), mo));
+    if (XSPH) {
+      const double w = 0.5*(mrhoA*WA + mrhoB*WB);
+      XSPHw += w;
+      const V3 dv = vmul(vij, w);
+      XSPHdv = own ? vsub(XSPHdv, dv) : vadd(XSPHdv, dv);
+    }
+    tsubfrom(M, tmul(dyad(rij, gradWi), mo));
+  }
+
+  // ---- per-node finish (src/SPH/SPHHydroBase.cc:834-902)
+  const double mi = I.m, rhoi = I.rho, Hdeti = I.Hdet;
+  const int numNeighbors = (int)(k1 - k0);
+  rhoSum += mi*P.W0*Hdeti;
+  norm += mi/rhoi*P.W0*Hdeti;
+  T9 Mi = M, DvDxi = DvDx;
+  if (P.correctVelGrad && fabs(tdet(Mi)) > 1.0e-10 && numNeighbors > 8) {
+    Mi = tinverse(Mi);
+    DvDxi = tdot(DvDxi, Mi);
+  } else {
+    DvDxi = tdiv(DvDxi, rhoi);
+  }
+  const double DrhoDt = -rhoi*ttrace(DvDxi);
+  wns = dmax(0.0, wns/Hdeti);
+  wns = sgn(wns)*pow(fabs(wns), 0.3333333333333333);          // Dim<3>::rootnu
+  m2 = sdiv(m2, Hdeti*Hdeti);
+  V3 DxDt = I.v;
+  if (XSPH) {
+    XSPHw += Hdeti*mi/rhoi*P.W0;
+    DxDt = vadd(I.v, vdiv(XSPHdv, dmax(1.0e-30, XSPHw)));
+  }
+  const Sym DHDt = smul(sdiv(sneg(I.H), 3.0), ttrace(DvDxi));
+  // SPHSmoothingScale::idealSmoothingScale (src/NodeList/SPHSmoothingScale.cc:118-199)
+  double nPerhCur;
+  if (fuzzyEqual(wns, 0.0)) {
+    nPerhCur = 0.5*P.nPerh;
+  } else {
+    // TableKernel::equivalentNodesPerSmoothingScale with bisectSearch
+    const int nt = P.W.n;
+    const bool ascnd = ldg(P.wsum + nt - 1) >= ldg(P.wsum);
+    int jl = -1, ju = nt;
+    while (ju - jl > 1) {
+      const int jm = (ju + jl)/2;
+      if ((wns >= ldg(P.wsum + jm)) == ascnd) jl = jm; else ju = jm;
+    }
+    const int lb = jl, ub = lb + 1;
+    if (lb == -1) nPerhCur = ldg(P.nperh);
+    else if (ub == nt) nPerhCur = ldg(P.nperh + nt - 1);
+    else {
+      const double nl = ldg(P.nperh + lb), nu = ldg(P.nperh + ub);
+      const double wl = ldg(P.wsum + lb), wu = ldg(P.wsum + ub);
+      nPerhCur = dmin(nu, dmax(nl, nl + (wns - wl)/(wu - wl)*(nu - nl)));
+    }
+  }
+  const double s = dmin(4.0, dmax(0.25, P.nPerh/(nPerhCur + 1.0e-30)));
+  const double a = s < 1.0 ? 0.4*(1.0 + s*s) : 0.4*(1.0 + 1.0/(s*s*s));
+  const double hi0 = 1.0/I.H.xx;
+  const double hi1 = dmin(P.hmax, dmax(P.hmin, hi0*(1.0 - a + a*s)));
+  const double hinv = 1.0/hi1;
+
+  // ---- stores (SoA, coalesced across the warp)
+  double* d = D + i;
+  d[(D_DXDT + 0)*n] = DxDt.x; d[(D_DXDT + 1)*n] = DxDt.y; d[(D_DXDT + 2)*n] = DxDt.z;
+  d[(D_DVDT + 0)*n] = DvDt.x; d[(D_DVDT + 1)*n] = DvDt.y; d[(D_DVDT + 2)*n] = DvDt.z;
+  d[D_DRHODT*n] = DrhoDt;
+  d[D_DEPSDT*n] = DepsDt;
+  d[(D_DHDT + 0)*n] = DHDt.xx; d[(D_DHDT + 1)*n] = DHDt.xy; d[(D_DHDT + 2)*n] = DHDt.xz;
+  d[(D_DHDT + 3)*n] = DHDt.yy; d[(D_DHDT + 4)*n] = DHDt.yz; d[(D_DHDT + 5)*n] = DHDt.zz;
+  d[(D_HIDEAL + 0)*n] = 1.0*hinv; d[(D_HIDEAL + 1)*n] = 0.0*hinv; d[(D_HIDEAL + 2)*n] = 0.0*hinv;
+  d[(D_HIDEAL + 3)*n] = 1.0*hinv; d[(D_HIDEAL + 4)*n] = 0.0*hinv; d[(D_HIDEAL + 5)*n] = 1.0*hinv;
+  const double* dv = &DvDxi.xx;
+  const double* mm = &Mi.xx;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    d[(D_DVDX + c)*n] = dv[c];
+    d[(D_LDVDX + c)*n] = dv[c];     // localDvDx: same material everywhere
+    d[(D_M + c)*n] = mm[c];
+    d[(D_LM + c)*n] = mm[c];
+  }
+  d[D_RHOSUM*n] = rhoSum;
+  d[D_NORM*n] = norm;
+  d[D_WNS*n] = wns;
+  d[(D_M2 + 0)*n] = m2.xx; d[(D_M2 + 1)*n] = m2.xy; d[(D_M2 + 2)*n] = m2.xz;
+  d[(D_M2 + 3)*n] = m2.yy; d[(D_M2 + 4)*n] = m2.yz; d[(D_M2 + 5)*n] = m2.zz;
+  d[D_XSPHW*n] = XSPHw;
+  d[(D_XSPHDV + 0)*n] = XSPHdv.x; d[(D_XSPHDV + 1)*n] = XSPHdv.y; d[(D_XSPHDV + 2)*n] = XSPHdv.z;
+  d[D_MAXVP*n] = maxvp;
+  d[D_EFFVP*n] = effvp;
+  d[D_VISCW*n] = viscW;
+}
+
+// ---------------------------------------------------------------- grad-h
+__global__ void gradh_kernel(Params P, const double* rec, int64_t n, const int64_t* offsets, const int32_t* nbr,
+                             double* S) {
+  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t k0 = offsets[i], k1 = offsets[i + 1];
+  if (k1 == k0) { S[S_OMEGA*n + i] = 1.0; return; }
+  const Rec I = loadRec(rec, i);
+  const double W0 = tableKernel(P.W, 0.0, I.Hdet);
+  double omega = 0.0, gradsum = 0.0;
+  bool selfDone = false;
+  for (int64_t k = k0; k < k1; ++k) {
+    const int32_t j = __ldg(nbr + k);
+    if (!selfDone && j > (int32_t)i) { omega += W0; selfDone = true; }
+    const V3 rj{ldg(rec + (int64_t)j*RECW + R_X), ldg(rec + (int64_t)j*RECW + R_Y), ldg(rec + (int64_t)j*RECW + R_Z)};
+    const V3 rij = vsub(I.r, rj);
+    const double eta = mag(sdot(I.H, rij));
+    double W, gW;
+    tableKernelAndGrad(P.W, eta, I.Hdet, W, gW);
+    omega += W;
+    gradsum += eta*gW;
+  }
+  if (!selfDone) omega += W0;
+  S[S_OMEGA*n + i] = -gradsum/(3*omega);
+}
+
+// ---------------------------------------------------------------- sum density
+__global__ void sum_density_kernel(Params P, const double* rec, int64_t n, const int64_t* offsets,
+                                   const int32_t* nbr, double* S) {
+  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const V3 ri{ldg(rec + i*RECW + R_X), ldg(rec + i*RECW + R_Y), ldg(rec + i*RECW + R_Z)};
+  const double mi = ldg(rec + i*RECW + R_M), Hdeti = ldg(rec + i*RECW + R_HDET);
+  const double W0 = tableKernel(P.W, 0.0, Hdeti);
+  double rho = 0.0;
+  bool selfDone = false;
+  const int64_t k0 = offsets[i], k1 = offsets[i + 1];
+  for (int64_t k = k0; k < k1; ++k) {
+    const int32_t j = __ldg(nbr + k);
+    if (!selfDone && j > (int32_t)i) { rho += mi*W0; selfDone = true; }
+    const Rec J = loadRec(rec, j);
+    const V3 rij = vsub(ri, J.r);
+    const double eta = mag(sdot(J.H, rij));
+    rho += J.m*tableKernel(P.W, eta, J.Hdet);
+  }
+  if (!selfDone) rho += mi*W0;
+  S[S_RHO*n + i] = rho;
+}
+
+// ---------------------------------------------------------------- compatible energy
+__global__ void compatible_energy_kernel(int64_t n, const int64_t* offsets, const int32_t* nbr,
+                                         const int32_t* groot, const double* pacc, int64_t ecap,
+                                         const double* D, double* S, const double* d_dt, double scale) {
+  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double multiplier = scale*(*d_dt);
+  const double hdt = 0.5*multiplier;
+  const double weighti = fabs(D[D_DEPSDT*n + i]) + kDblEps;
+  const double mi = S[S_M*n + i];
+  const V3 vi{S[S_VX*n + i], S[S_VY*n + i], S[S_VZ*n + i]};
+  const V3 ai{D[(D_DVDT + 0)*n + i], D[(D_DVDT + 1)*n + i], D[(D_DVDT + 2)*n + i]};
+  const V3 vi12 = vadd(vi, vmul(ai, hdt));
+  double DepsDti = 0.0;
+  const int64_t k0 = offsets[i], k1 = offsets[i + 1];
+  for (int64_t k = k0; k < k1; ++k) {
+    const int32_t j = __ldg(nbr + k);
+    const int64_t r = j < n ? (int64_t)j : (int64_t)__ldg(groot + (j - n));
+    const double weightj = fabs(ldg(D + D_DEPSDT*n + r)) + kDblEps;
+    const double mj = ldg(S + S_M*n + r);
+    const V3 vj{ldg(S + S_VX*n + r), ldg(S + S_VY*n + r), ldg(S + S_VZ*n + r)};
+    const V3 aj{ldg(D + (D_DVDT + 0)*n + r), ldg(D + (D_DVDT + 1)*n + r), ldg(D + (D_DVDT + 2)*n + r)};
+    const V3 vj12 = vadd(vj, vmul(aj, hdt));
+    const V3 dd{ldg(pacc + k), ldg(pacc + ecap + k), ldg(pacc + 2*ecap + k)};
+    if (j > (int32_t)i) {
+      const V3 pai = vmul(dd, -mj);
+      const double duij = dot(vsub(vj12, vi12), pai);
+      const double wi = weighti/(weighti + weightj);
+      DepsDti += wi*duij;
+    } else {
+      const V3 paj = vmul(dd, -mi);                 // owner j's pair acceleration
+      const double duji = dot(vsub(vi12, vj12), paj);
+      const double wj = weightj/(weightj + weighti);
+      DepsDti += (1.0 - wj)*duji*mj/mi;
+    }
+  }
+  S[S_EPS*n + i] += DepsDti*multiplier;
+}
+
+// ---------------------------------------------------------------- policies
+__device__ __forceinline__ bool hInsideBounds(const Sym& H, double hmin, double hmax) {
+  const V3 ev = eigenValues(H);
+  return vmin(ev) > 1.0/hmax && vmax(ev) < 1.0/hmin;
+}
+
+__global__ void update_kernel(Params P, int64_t n, double* S, const double* D, const double* d_dt, double scale,
+                              int timeAdvanceOnly, int epsDone, int* err) {
+  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double mult = scale*(*d_dt);
+  // H: IncrementBoundedState (half step / IntegrateH) or ReplaceBoundedState (IdealH)
+  Sym H{S[(S_H + 0)*n + i], S[(S_H + 1)*n + i], S[(S_H + 2)*n + i],
+        S[(S_H + 3)*n + i], S[(S_H + 4)*n + i], S[(S_H + 5)*n + i]};
+  Sym Hn;
+  if (timeAdvanceOnly || P.HUpdate == SPHGPU_H_INTEGRATE) {
+    const Sym dH{D[(D_DHDT + 0)*n + i], D[(D_DHDT + 1)*n + i], D[(D_DHDT + 2)*n + i],
+                 D[(D_DHDT + 3)*n + i], D[(D_DHDT + 4)*n + i], D[(D_DHDT + 5)*n + i]};
+    Hn = sadd(H, smul(dH, mult));
+  } else {
+    Hn = Sym{D[(D_HIDEAL + 0)*n + i], D[(D_HIDEAL + 1)*n + i], D[(D_HIDEAL + 2)*n + i],
+             D[(D_HIDEAL + 3)*n + i], D[(D_HIDEAL + 4)*n + i], D[(D_HIDEAL + 5)*n + i]};
+  }
+  if (!hInsideBounds(Hn, P.hmin, P.hmax)) atomicOr(err, DERR_H_CLAMP);
+  S[(S_H + 0)*n + i] = Hn.xx; S[(S_H + 1)*n + i] = Hn.xy; S[(S_H + 2)*n + i] = Hn.xz;
+  S[(S_H + 3)*n + i] = Hn.yy; S[(S_H + 4)*n + i] = Hn.yz; S[(S_H + 5)*n + i] = Hn.zz;
+  // mass density: IncrementBoundedState
+  const double rho = dmin(P.rhoMax, dmax(P.rhoMin, S[S_RHO*n + i] + mult*(D[D_DRHODT*n + i])));
+  S[S_RHO*n + i] = rho;
+  // position: IncrementFieldList
+  for (int c = 0; c < 3; ++c) S[(S_X + c)*n + i] = S[(S_X + c)*n + i] + D[(D_DXDT + c)*n + i]*mult;
+  // specific thermal energy: IncrementFieldList (or the compatible policy, already applied)
+  double eps = S[S_EPS*n + i];
+  if (!epsDone) {
+    eps = eps + mult*(D[D_DEPSDT*n + i]);
+    S[S_EPS*n + i] = eps;
+  }
+  // pressure, sound speed (GammaLawGas, no active pressure limits)
+  const double g1 = P.gamma - 1.0;
+  S[S_P*n + i] = g1*rho*eps;
+  S[S_CS*n + i] = sqrt(dmax(0.0, P.gamma*g1*eps));
+  // velocity: IncrementFieldList (after the energy it depends on)
+  for (int c = 0; c < 3; ++c) S[(S_VX + c)*n + i] = S[(S_VX + c)*n + i] + D[(D_DVDT + c)*n + i]*mult;
+}
+
+__global__ void eos_kernel(double gamma, int64_t n, double* S) {
+  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double g1 = gamma - 1.0;
+  const double rho = S[S_RHO*n + i], eps = S[S_EPS*n + i];
+  S[S_P*n + i] = g1*rho*eps;
+  S[S_CS*n + i] = sqrt(dmax(0.0, gamma*g1*eps));
+}
+
+__global__ void enforce_boundaries_kernel(int64_t n, double* S, BoxBCs bcs) {
+  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  V3 r{S[S_X*n + i], S[S_Y*n + i], S[S_Z*n + i]};
+  for (int pb = 0; pb < 6; pb += 2) {
+    if (!bcs.periodic[pb >> 1]) continue;
+    for (int sub = 0; sub < 2; ++sub) {
+      const PlanarBC& bc = bcs.bc[pb + sub];
+      if (planeCompare(bc.enter, r) == 1) r = mapPositionThroughPlanes(r, bc.enter, bc.exit);
+    }
+    const PlaneD& plane1 = bcs.bc[pb].enter;
+    const PlaneD& plane2 = bcs.bc[pb].exit;
+    if (planeCompare(plane1, r) == 1 || planeCompare(plane2, r) == 1) {
+      const double L = minimumDistance(plane1, plane2.point);
+      const V3 p0 = vadd(r, vmul(plane1.normal, dot(vsub(plane1.point, r), plane1.normal)));
+      const double f = dmax(-1.0, dmin(1.0, fmod(signedDistance(plane1, r)/L, 1.0)));
+      r = vadd(p0, vmul(plane1.normal, f*L));
+    }
+  }
+  S[S_X*n + i] = r.x; S[S_Y*n + i] = r.y; S[S_Z*n + i] = r.z;
+}
+
+// ---------------------------------------------------------------- dt
+__global__ void hydro_dt_kernel(Params P, int64_t n, const double* S, const double* D, const int64_t* offsets,
+                                const int32_t* nbr, const int32_t* groot, unsigned long long* out) {
+  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+  double minDt = kFltMax;
+  if (i < n) {
+    const Sym H{S[(S_H + 0)*n + i], S[(S_H + 1)*n + i], S[(S_H + 2)*n + i],
+                S[(S_H + 3)*n + i], S[(S_H + 4)*n + i], S[(S_H + 5)*n + i]};
+    const double nodeScale = 1.0/vmax(eigenValues(H))/P.nPerh;
+    const double cs = S[S_CS*n + i], rho = S[S_RHO*n + i];
+    const double csDt = nodeScale/(cs + kFltMin);
+    if (csDt < minDt) minDt = csDt;
+    const double csq = sqrt(D[D_MAXVP*n + i]/rho);
+    const double csqDt = nodeScale/(csq + kFltMin);
+    if (csqDt < minDt) minDt = csqDt;
+    const double divv = D[(D_DVDX + 0)*n + i] + D[(D_DVDX + 4)*n + i] + D[(D_DVDX + 8)*n + i];
+    const double divvDt = 1.0/(fabs(divv) + kFltMin);
+    if (divvDt < minDt) minDt = divvDt;
+    const V3 vi{S[S_VX*n + i], S[S_VY*n + i], S[S_VZ*n + i]};
+    for (int64_t k = offsets[i]; k < offsets[i + 1]; ++k) {
+      const int32_t j = __ldg(nbr + k);
+      const int64_t r = j < n ? (int64_t)j : (int64_t)__ldg(groot + (j - n));
+      const V3 vj{ldg(S + S_VX*n + r), ldg(S + S_VY*n + r), ldg(S + S_VZ*n + r)};
+      const double vij = mag(vsub(vi, vj));
+      const double dtVelDiff = nodeScale*safeInvVar(vij, 1e-30);
+      if (dtVelDiff < minDt) minDt = dtVelDiff;
+    }
+    const V3 a{D[(D_DVDT + 0)*n + i], D[(D_DVDT + 1)*n + i], D[(D_DVDT + 2)*n + i]};
+    const double dtAcc = sqrt(nodeScale/(mag(a) + kFltMin));
+    if (dtAcc < minDt) minDt = dtAcc;
+    if (P.useVelMagDt) {
+      const double velDt = nodeScale/(mag(vi) + 1.0e-10);
+      if (velDt < minDt) minDt = velDt;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) minDt = dmin(minDt, __shfl_xor_sync(0xffffffffu, minDt, o));
+  if ((threadIdx.x & 31) == 0) atomicMin(out, (unsigned long long)__double_as_longlong(minDt));
+}
+
+// Integrator::selectDt on the device: dt stays resident for the step kernels.
+__global__ void select_dt_kernel(const unsigned long long* minDtBits, double cfl, double dtMin, double dtMax,
+                                 double dtGrowth, double* d_dt, double* d_lastDt, double* d_vote) {
+  const double vote = cfl*__longlong_as_double((long long)*minDtBits);
+  double dt = dtMax;
+  if (vote > 0.0 && vote < dt) dt = vote;
+  dt = dmin(dt, dtGrowth*(*d_lastDt));
+  dt = dmin(dtMax, dmax(dtMin, dt));
+  *d_dt = dt;
+  *d_vote = vote;
+}
+
+// ---------------------------------------------------------------- conservation
+__global__ void conservation_partials_kernel(int64_t n, const double* S, double* partials) {
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x*blockDim.x) {
+    const double m = S[S_M*n + i];
+    const V3 v{S[S_VX*n + i], S[S_VY*n + i], S[S_VZ*n + i]};
+    acc[0] += m;
+    acc[1] += m*v.x; acc[2] += m*v.y; acc[3] += m*v.z;
+    acc[4] += 0.5*m*mag2(v);
+    acc[5] += m*S[S_EPS*n + i];
+  }
+  __shared__ double sh[6][256];
+  for (int c = 0; c < 6; ++c) sh[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int s = blockDim.x/2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) for (int c = 0; c < 6; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) for (int c = 0; c < 6; ++c) partials[blockIdx.x*6 + c] = sh[c][0];
+}
+
+__global__ void conservation_final_kernel(const double* partials, int nb, double* out) {
+  if (threadIdx.x != 0) return;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int b = 0; b < nb; ++b) for (int c = 0; c < 6; ++c) acc[c] += partials[b*6 + c];
+  for (int c = 0; c < 6; ++c) out[c] = acc[c];
+  out[6] = acc[4] + acc[5];
+  out[7] = 0.0;
+}
+
+}  // namespace
+
+// ================================================================ launchers
+void pack_records(Problem& p) {
+  const int64_t ntot = p.n + p.G;
+  int blocks = nblk(ntot, 256);
+  if (blocks > 148*64) blocks = 148*64;
+  pack_records_kernel<<<blocks, 256, 0, p.stream>>>(p.S, p.n, p.groot, p.gcode, ntot, p.prm.bcs, p.rec);
+}
+
+void launch_gradh(Problem& p) {
+  gradh_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr, p.S);
+}
+
+void launch_eval_sph_fp64(Problem& p) {
+  const bool xsph = p.prm.XSPH != 0, tens = p.prm.epsTensile != 0.0, comp = p.prm.compatible != 0;
+  const int threads = 128;
+  const int blocks = nblk(p.n, threads);
+#define SPH_LAUNCH(X, T, C) \
+  sph_eval_fp64_kernel<X, T, C><<<blocks, threads, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr, p.D, p.pacc, p.ecap)
+  if (xsph) {
+    if (tens) { if (comp) SPH_LAUNCH(true, true, true); else SPH_LAUNCH(true, true, false); }
+    else      { if (comp) SPH_LAUNCH(true, false, true); else SPH_LAUNCH(true, false, false); }
+  } else {
+    if (tens) { if (comp) SPH_LAUNCH(false, true, true); else SPH_LAUNCH(false, true, false); }
+    else      { if (comp) SPH_LAUNCH(false, false, true); else SPH_LAUNCH(false, false, false); }
+  }
+#undef SPH_LAUNCH
+}
+
+void launch_sum_density(Problem& p) {
+  sum_density_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr, p.S);
+}
+
+void launch_compatible_energy(Problem& p, const double* d_dt, double scale) {
+  compatible_energy_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.n, p.offsets, p.nbr, p.groot, p.pacc, p.ecap,
+                                                                 p.D, p.S, d_dt, scale);
+}
+
+void launch_update(Problem& p, const double* d_dt, double scale, bool timeAdvanceOnly) {
+  const int epsDone = (!timeAdvanceOnly && p.prm.compatible) ? 1 : 0;
+  update_kernel<<<nblk(p.n, 256), 256, 0, p.stream>>>(p.prm, p.n, p.S, p.D, d_dt, scale,
+                                                      timeAdvanceOnly ? 1 : 0, epsDone, p.d_err);
+}
+
+void launch_eos(Problem& p) {
+  eos_kernel<<<nblk(p.n, 256), 256, 0, p.stream>>>(p.prm.gamma, p.n, p.S);
+}
+
+void launch_enforce_boundaries(Problem& p) {
+  enforce_boundaries_kernel<<<nblk(p.n, 256), 256, 0, p.stream>>>(p.n, p.S, p.prm.bcs);
+}
+
+// d_out[0] = min dt bits (as double after the kernel), scratch in d_scal.
+void launch_dt(Problem& p, double* d_out) {
+  unsigned long long* bits = reinterpret_cast<unsigned long long*>(d_out);
+  const double init = kFltMax;
+  cudaMemcpyAsync(bits, &init, sizeof(double), cudaMemcpyHostToDevice, p.stream);
+  hydro_dt_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.n, p.S, p.D, p.offsets, p.nbr, p.groot, bits);
+}
+
+void launch_select_dt(Problem& p, double* d_dt, double* d_lastDt) {
+  double* minDt = p.d_scal + 10;
+  launch_dt(p, minDt);
+  select_dt_kernel<<<1, 1, 0, p.stream>>>(reinterpret_cast<unsigned long long*>(minDt), p.prm.cfl,
+                                          p.cfg.dtMin, p.cfg.dtMax, p.cfg.dtGrowth, d_dt, d_lastDt,
+                                          p.d_scal + 11);
+}
+
+void launch_conservation(Problem& p, double* d_out8) {
+  const int nb = 148*4;
+  conservation_partials_kernel<<<nb, 256, 0, p.stream>>>(p.n, p.S, p.d_red);
+  conservation_final_kernel<<<1, 32, 0, p.stream>>>(p.d_red, nb, d_out8);
+}
+
+void launch_zero_derivs(Problem& p) {
+  cudaMemsetAsync(p.D, 0, sizeof(double)*NDERIV*(size_t)p.n, p.stream);
+}
+
+}  // namespace sphgpu

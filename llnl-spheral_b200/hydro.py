@@ -1,0 +1,152 @@
+"""Host-side mirror of the reference's hydro package interface over the C-ABI.
+
+``SPHHydro`` keeps the names and argument meaning of Spheral's SPH factory
+(src/SPH/SPHHydros.py:12-59) and of the Physics<Dim> methods the integrator
+calls (src/Physics/Physics.hh:51-159): ``initialize``, ``evaluateDerivatives``,
+``finalizeDerivatives``, ``finalize``, ``dt``; fields are read by the
+reference's State/StateDerivatives keys (src/Hydro/HydroFieldNames.cc).
+``CheapSynchronousRK2Integrator.step`` advances one
+CheapSynchronousRK2::step (src/Integrator/CheapSynchronousRK2.cc:81-143).
+
+Every call goes through libsphgpu.so; errors raise RuntimeError with the
+library's message (the reference throws VERIFYError).  There is no CPU path.
+"""
+import ctypes
+
+import numpy as np
+
+from . import abi
+
+FIELD_COMPONENTS = {
+    "position": 3, "velocity": 3, "mass": 1, "mass density": 1, "specific thermal energy": 1, "H": 6,
+    "pressure": 1, "sound speed": 1, "grad h corrections": 1, "new mass density": 1, "normalization": 1,
+    "delta position": 3, "delta mass density": 1, "delta velocity hydro": 3,
+    "delta specific thermal energy": 1, "velocity gradient": 9, "internal velocity gradient": 9,
+    "M SPH gradient correction": 9, "local M SPH gradient correction": 9, "delta H": 6, "new H": 6,
+    "max viscous pressure": 1, "effective viscous pressure": 1, "viscous work rate": 1,
+    "XSPH weight sum": 1, "XSPH delta vi": 3, "weighted neighbor sum": 1, "mass second moment": 6,
+}
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+class SPHHydro:
+    """One FluidNodeList evolved by the B200 SPH hydro path.
+
+    ``cfg`` is an ``abi.SphConfig`` (see ``abi.make_config``); ``nodes`` a
+    ``generators.NodeSet`` (or anything with pos, vel, mass, rho, eps, H AoS
+    arrays).
+    """
+
+    def __init__(self, cfg, nodes=None, n=None):
+        self.lib = abi.load_library()
+        self.cfg = cfg.copy()
+        self.n = int(nodes.n if nodes is not None else n)
+        h = ctypes.c_void_p()
+        abi.check(self.lib.sphgpu_create(ctypes.byref(self.cfg), self.n, ctypes.byref(h)), self.lib)
+        self.h = h
+        self.time = 0.0
+        if nodes is not None:
+            self.set_state(nodes)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.sphgpu_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- state
+    def set_state(self, nodes):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
+                (nodes.pos, nodes.vel, nodes.mass, nodes.rho, nodes.eps, nodes.H)]
+        abi.check(self.lib.sphgpu_set_state(self.h, *[_p(a) for a in arrs]), self.lib)
+
+    def set_state_device(self, ptrs):
+        """ptrs: six device pointers (int) in the order of set_state."""
+        abi.check(self.lib.sphgpu_set_state_device(self.h, *[ctypes.c_void_p(int(q)) for q in ptrs]), self.lib)
+
+    def field(self, key):
+        c = FIELD_COMPONENTS[key]
+        out = np.empty(self.n * c)
+        abi.check(self.lib.sphgpu_get_field(self.h, key.encode(), _p(out), out.size), self.lib)
+        return out.reshape(self.n, c) if c > 1 else out
+
+    # ---- Integrator::setGhostNodes + ConnectivityMap
+    def build_neighbors(self):
+        abi.check(self.lib.sphgpu_build_neighbors(self.h), self.lib)
+
+    setGhostNodes = build_neighbors
+
+    def connectivity(self):
+        g = ctypes.c_int64()
+        e = ctypes.c_int64()
+        abi.check(self.lib.sphgpu_connectivity_size(self.h, ctypes.byref(g), ctypes.byref(e)), self.lib)
+        off = np.empty(self.n + 1, dtype=np.int64)
+        nb = np.empty(max(e.value, 1), dtype=np.int32)
+        root = np.empty(max(g.value, 1), dtype=np.int32)
+        abi.check(self.lib.sphgpu_get_connectivity(self.h, _p(off), _p(nb), _p(root)), self.lib)
+        return off, nb[:e.value], root[:g.value]
+
+    def num_pairs(self):
+        v = ctypes.c_int64()
+        abi.check(self.lib.sphgpu_num_pairs(self.h, ctypes.byref(v)), self.lib)
+        return v.value
+
+    # ---- Physics<Dim> methods
+    def initialize(self, time=0.0, dt=0.0):
+        abi.check(self.lib.sphgpu_initialize(self.h, time, dt), self.lib)
+
+    def evaluateDerivatives(self, time=0.0, dt=0.0):
+        abi.check(self.lib.sphgpu_evaluate_derivatives(self.h, time, dt), self.lib)
+
+    def finalizeDerivatives(self, time=0.0, dt=0.0):
+        abi.check(self.lib.sphgpu_finalize_derivatives(self.h, time, dt), self.lib)
+
+    def finalize(self, time=0.0, dt=0.0):
+        abi.check(self.lib.sphgpu_finalize(self.h, time, dt), self.lib)
+
+    def dt(self):
+        v = ctypes.c_double()
+        abi.check(self.lib.sphgpu_dt(self.h, ctypes.byref(v)), self.lib)
+        return v.value
+
+    # ---- integrator
+    def step(self, nsteps=1):
+        t = ctypes.c_double(self.time)
+        dt = ctypes.c_double()
+        abi.check(self.lib.sphgpu_step_rk2(self.h, ctypes.byref(t), int(nsteps), ctypes.byref(dt)), self.lib)
+        self.time = t.value
+        return t.value, dt.value
+
+    def conservation(self):
+        out = np.empty(8)
+        abi.check(self.lib.sphgpu_conservation(self.h, _p(out)), self.lib)
+        return out
+
+    def synchronize(self):
+        abi.check(self.lib.sphgpu_synchronize(self.h), self.lib)
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        abi.check(self.lib.sphgpu_get_stream(self.h, ctypes.byref(s)), self.lib)
+        return s.value
+
+
+class CheapSynchronousRK2Integrator:
+    """Drives SPHHydro.step like the reference integrator (one package)."""
+
+    def __init__(self, hydro, dtMin=None, dtMax=None):
+        self.hydro = hydro
+
+    def step(self, maxTime=None):
+        return self.hydro.step(1)
+
+    def advance(self, nsteps):
+        return self.hydro.step(nsteps)
