@@ -276,9 +276,9 @@ int build_ghosts(Problem& p) {
     const PlanarBC bc = p.prm.bcs.bc[b];
     if (cudaMemsetAsync(hbits, 0, sizeof(unsigned long long), st) != cudaSuccess) return cuda_status(cudaGetLastError(), "memset");
     ghost_hmax_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, p.groot, ntot, bc,
-                                                           p.prm.kernelExtent, hbits);
+                                                           p.prm.kernelExtent, hbits); ++p.launches;
     ghost_flag_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, ntot, bc, p.prm.kernelExtent,
-                                                           hbits, p.counts);
+                                                           hbits, p.counts); ++p.launches;
     int64_t total = 0;
     int rc = exclusive_scan_i32(p, p.counts, ntot, p.offsets, &total);
     if (rc) return rc;
@@ -286,7 +286,7 @@ int build_ghosts(Problem& p) {
     rc = ensure_capacity_ghosts(p, (ntot - p.n) + total);
     if (rc) return rc;
     ghost_scatter_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, p.groot, p.gcode, ntot,
-                                                              p.counts, p.offsets, bc, b, p.d_err);
+                                                              p.counts, p.offsets, bc, b, p.d_err); ++p.launches;
     ntot += total;
   }
   p.G = ntot - p.n;
@@ -303,7 +303,7 @@ int build_cells_and_csr(Problem& p) {
   for (int a = 0; a < 3; ++a) { init[a] = ~0ULL; init[3 + a] = 0ULL; }
   init[6] = 0ULL;
   cudaMemcpyAsync(bb, init, sizeof(init), cudaMemcpyHostToDevice, st);
-  node_bounds_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, p.groot, ntot, bb);
+  node_bounds_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, p.groot, ntot, bb); ++p.launches;
   unsigned long long res[7];
   cudaMemcpyAsync(res, bb, sizeof(res), cudaMemcpyDeviceToHost, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_status(cudaGetLastError(), "bounds");
@@ -347,13 +347,13 @@ int build_cells_and_csr(Problem& p) {
   p.gcell = g.cell;
   // ---- counting sort of all nodes by cell
   cudaMemsetAsync(p.cellFill, 0, sizeof(int32_t)*ncells, st);
-  cell_index_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, ntot, g, p.cidx, p.cellFill);
+  cell_index_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, ntot, g, p.cidx, p.cellFill); ++p.launches;
   int64_t tot = 0;
   int rc = exclusive_scan_i32(p, p.cellFill, ncells, cellStart, &tot);
   if (rc) return rc;
   cudaMemsetAsync(p.cellFill, 0, sizeof(int32_t)*ncells, st);
   cell_scatter_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, p.groot, ntot, p.cidx,
-                                                           cellStart, p.cellFill, p.sortedIdx, p.cand, p.candcap);
+                                                           cellStart, p.cellFill, p.sortedIdx, p.cand, p.candcap); ++p.launches;
   // ---- neighbor counts, offsets, fill
   const double k2 = p.prm.kernelExtent*p.prm.kernelExtent;
   const int threads = 256;
@@ -361,13 +361,14 @@ int build_cells_and_csr(Problem& p) {
   const int64_t blocks = (warps*32 + threads - 1)/threads;
   nbr_walk_kernel<false><<<(unsigned)blocks, threads, 0, st>>>(p.S, p.n, g, cellStart, p.sortedIdx, p.cand,
                                                                  p.candcap, k2, p.counts, nullptr, nullptr,
-                                                                 p.maxNbr, p.d_err, nullptr);
+                                                                 p.maxNbr, p.d_err, nullptr); ++p.launches;
   int64_t E = 0;
   rc = exclusive_scan_i32(p, p.counts, p.n, p.offsets, &E);
   if (rc) return rc;
   int herr = 0;
   cudaMemcpyAsync(&herr, p.d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_status(cudaGetLastError(), "nbr count");
+  if (herr & (DERR_NBR_CAPACITY | DERR_GHOST_CHAIN)) cudaMemsetAsync(p.d_err, 0, sizeof(int), st);
   if (herr & DERR_NBR_CAPACITY) {
     set_error("a node has more neighbors than max_neighbors");
     return SPHGPU_ERR_CAPACITY;
@@ -388,7 +389,7 @@ int build_cells_and_csr(Problem& p) {
   }
   nbr_walk_kernel<true><<<(unsigned)blocks, threads, smem, st>>>(p.S, p.n, g, cellStart, p.sortedIdx, p.cand,
                                                                    p.candcap, k2, p.counts, p.offsets, p.nbr,
-                                                                   p.maxNbr, p.d_err, pc);
+                                                                   p.maxNbr, p.d_err, pc); ++p.launches;
   unsigned long long pairs = 0;
   cudaMemcpyAsync(&pairs, pc, sizeof(pairs), cudaMemcpyDeviceToHost, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_status(cudaGetLastError(), "nbr fill");

@@ -138,6 +138,7 @@ struct Problem {
   double* pinned = nullptr;     // pinned host staging for get/set
   int64_t pinnedcap = 0;
 
+  int64_t launches = 0;         // kernels launched by this problem (diagnostics)
   bool haveNbrs = false;
   bool haveDerivs = false;
   double time = 0.0;

@@ -543,11 +543,11 @@ void pack_records(Problem& p) {
   const int64_t ntot = p.n + p.G;
   int blocks = nblk(ntot, 256);
   if (blocks > 148*64) blocks = 148*64;
-  pack_records_kernel<<<blocks, 256, 0, p.stream>>>(p.S, p.n, p.groot, p.gcode, ntot, p.prm.bcs, p.rec);
+  pack_records_kernel<<<blocks, 256, 0, p.stream>>>(p.S, p.n, p.groot, p.gcode, ntot, p.prm.bcs, p.rec); ++p.launches;
 }
 
 void launch_gradh(Problem& p) {
-  gradh_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr, p.S);
+  gradh_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr, p.S); ++p.launches;
 }
 
 void launch_eval_sph_fp64(Problem& p) {
@@ -563,30 +563,31 @@ void launch_eval_sph_fp64(Problem& p) {
     if (tens) { if (comp) SPH_LAUNCH(false, true, true); else SPH_LAUNCH(false, true, false); }
     else      { if (comp) SPH_LAUNCH(false, false, true); else SPH_LAUNCH(false, false, false); }
   }
+  ++p.launches;
 #undef SPH_LAUNCH
 }
 
 void launch_sum_density(Problem& p) {
-  sum_density_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr, p.S);
+  sum_density_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr, p.S); ++p.launches;
 }
 
 void launch_compatible_energy(Problem& p, const double* d_dt, double scale) {
   compatible_energy_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.n, p.offsets, p.nbr, p.groot, p.pacc, p.ecap,
-                                                                 p.D, p.S, d_dt, scale);
+                                                                 p.D, p.S, d_dt, scale); ++p.launches;
 }
 
 void launch_update(Problem& p, const double* d_dt, double scale, bool timeAdvanceOnly) {
   const int epsDone = (!timeAdvanceOnly && p.prm.compatible) ? 1 : 0;
   update_kernel<<<nblk(p.n, 256), 256, 0, p.stream>>>(p.prm, p.n, p.S, p.D, d_dt, scale,
-                                                      timeAdvanceOnly ? 1 : 0, epsDone, p.d_err);
+                                                      timeAdvanceOnly ? 1 : 0, epsDone, p.d_err); ++p.launches;
 }
 
 void launch_eos(Problem& p) {
-  eos_kernel<<<nblk(p.n, 256), 256, 0, p.stream>>>(p.prm.gamma, p.n, p.S);
+  eos_kernel<<<nblk(p.n, 256), 256, 0, p.stream>>>(p.prm.gamma, p.n, p.S); ++p.launches;
 }
 
 void launch_enforce_boundaries(Problem& p) {
-  enforce_boundaries_kernel<<<nblk(p.n, 256), 256, 0, p.stream>>>(p.n, p.S, p.prm.bcs);
+  enforce_boundaries_kernel<<<nblk(p.n, 256), 256, 0, p.stream>>>(p.n, p.S, p.prm.bcs); ++p.launches;
 }
 
 // d_out[0] = min dt bits (as double after the kernel), scratch in d_scal.
@@ -594,7 +595,7 @@ void launch_dt(Problem& p, double* d_out) {
   unsigned long long* bits = reinterpret_cast<unsigned long long*>(d_out);
   const double init = kFltMax;
   cudaMemcpyAsync(bits, &init, sizeof(double), cudaMemcpyHostToDevice, p.stream);
-  hydro_dt_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.n, p.S, p.D, p.offsets, p.nbr, p.groot, bits);
+  hydro_dt_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.n, p.S, p.D, p.offsets, p.nbr, p.groot, bits); ++p.launches;
 }
 
 void launch_select_dt(Problem& p, double* d_dt, double* d_lastDt) {
@@ -602,13 +603,13 @@ void launch_select_dt(Problem& p, double* d_dt, double* d_lastDt) {
   launch_dt(p, minDt);
   select_dt_kernel<<<1, 1, 0, p.stream>>>(reinterpret_cast<unsigned long long*>(minDt), p.prm.cfl,
                                           p.cfg.dtMin, p.cfg.dtMax, p.cfg.dtGrowth, d_dt, d_lastDt,
-                                          p.d_scal + 11);
+                                          p.d_scal + 11); ++p.launches;
 }
 
 void launch_conservation(Problem& p, double* d_out8) {
   const int nb = 148*4;
-  conservation_partials_kernel<<<nb, 256, 0, p.stream>>>(p.n, p.S, p.d_red);
-  conservation_final_kernel<<<1, 32, 0, p.stream>>>(p.d_red, nb, d_out8);
+  conservation_partials_kernel<<<nb, 256, 0, p.stream>>>(p.n, p.S, p.d_red); ++p.launches;
+  conservation_final_kernel<<<1, 32, 0, p.stream>>>(p.d_red, nb, d_out8); ++p.launches;
 }
 
 void launch_zero_derivs(Problem& p) {

@@ -304,7 +304,7 @@ int prepare_mixed(Problem& p) {
       set_error("mixed table allocation failed");
       return SPHGPU_ERR_NOMEM;
     }
-    table_to_float_kernel<<<8, 256, 0, p.stream>>>(p.prm.W.coef, p.prm.W.n, p.coefF);
+    table_to_float_kernel<<<8, 256, 0, p.stream>>>(p.prm.W.coef, p.prm.W.n, p.coefF); ++p.launches;
   }
   const int64_t need = p.candcap;
   if (need > p.mreccap) {
@@ -323,7 +323,7 @@ void launch_eval_sph_mixed(Problem& p) {
   const int64_t ntot = p.n + p.G;
   int blocks = nblk(ntot, 256);
   if (blocks > 148*64) blocks = 148*64;
-  pack_mixed_kernel<<<blocks, 256, 0, p.stream>>>(p.S, p.n, p.groot, p.gcode, ntot, p.prm.bcs, p.mrec);
+  pack_mixed_kernel<<<blocks, 256, 0, p.stream>>>(p.S, p.n, p.groot, p.gcode, ntot, p.prm.bcs, p.mrec); ++p.launches;
   const bool xsph = p.prm.XSPH != 0, tens = p.prm.epsTensile != 0.0, comp = p.prm.compatible != 0;
   const int threads = 128;
   const int nb = nblk(p.n, threads);
@@ -337,6 +337,7 @@ void launch_eval_sph_mixed(Problem& p) {
     if (tens) { if (comp) MIX_LAUNCH(false, true, true); else MIX_LAUNCH(false, true, false); }
     else      { if (comp) MIX_LAUNCH(false, false, true); else MIX_LAUNCH(false, false, false); }
   }
+  ++p.launches;
 #undef MIX_LAUNCH
 }
 

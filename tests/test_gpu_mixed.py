@@ -1,0 +1,68 @@
+"""Mixed-precision form (FP32 pair arithmetic, Kahan FP32 sums, FP64 state)
+against the plain FP64 GPU path and the oracle.
+
+Tolerances (from the hot-path specification): every derivative field within
+1e-5 max relative error, normwise (||mixed - fp64||_inf / ||fp64||_inf);
+relative total-energy drift <= 1e-6 over 200 RK2 steps.
+"""
+import numpy as np
+import pytest
+
+from conftest import normwise
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ["delta velocity hydro", "delta specific thermal energy", "delta mass density", "velocity gradient",
+          "new mass density", "new H", "M SPH gradient correction", "max viscous pressure"]
+
+
+def _evolved_sod(pkg, steps=5):
+    gen, abi = pkg.generators, pkg.abi
+    box = ((0.0, 0.0, 0.0), (1.0, 0.125, 0.125))
+    ns = gen.sod(nx=64, ny=8, nz=8, box=box)
+    cfg = gen.sod_config(abi, ns_box=box)
+    g = pkg.SPHHydro(cfg, ns)
+    g.build_neighbors()
+    g.evaluateDerivatives()
+    g.step(steps)
+    pos, vel, rho, eps, H = (g.field(k) for k in ("position", "velocity", "mass density",
+                                                  "specific thermal energy", "H"))
+    return gen.NodeSet(pos, vel, ns.mass, rho, eps, H, ns.dx), cfg
+
+
+@pytest.mark.parametrize("which", ["sod_evolved", "kh"])
+def test_mixed_derivative_errors(gpu_lib, pkg, oracle_mod, which):
+    gen, abi = pkg.generators, pkg.abi
+    if which == "sod_evolved":
+        ns, cfg = _evolved_sod(pkg)
+    else:
+        ns = gen.kelvin_helmholtz(nx=32, ny=32, nz=16, box=((0, 0, 0), (1.0, 1.0, 0.5)))
+        cfg = gen.kh_config(abi, xmax=(1.0, 1.0, 0.5))
+    cm = cfg.copy()
+    cm.precision = abi.PRECISION_MIXED
+    f = pkg.SPHHydro(cfg, ns)
+    m = pkg.SPHHydro(cm, ns)
+    o = oracle_mod.OracleProblem(cfg, ns)
+    for p in (f, m):
+        p.build_neighbors()
+        p.evaluateDerivatives()
+    o.build_neighbors()
+    o.evaluate_derivatives()
+    for k in FIELDS:
+        ref = o.field(k)
+        assert normwise(f.field(k), ref) <= 1e-12, k
+        assert normwise(m.field(k), ref) <= 1e-5, k
+
+
+def test_mixed_energy_drift_200_steps(gpu_lib, pkg):
+    gen, abi = pkg.generators, pkg.abi
+    box = ((0.0, 0.0, 0.0), (1.0, 0.125, 0.125))
+    ns = gen.sod(nx=64, ny=8, nz=8, box=box)
+    cfg = gen.sod_config(abi, ns_box=box, precision=abi.PRECISION_MIXED)
+    m = pkg.SPHHydro(cfg, ns)
+    m.build_neighbors()
+    m.evaluateDerivatives()
+    e0 = m.conservation()[6]
+    m.step(200)
+    e1 = m.conservation()[6]
+    assert abs(e1 - e0) / abs(e0) <= 1e-6

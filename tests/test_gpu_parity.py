@@ -1,0 +1,187 @@
+"""GPU (CUDA sm_100a, through the C-ABI) against the CPU oracle.
+
+Tolerances:
+  - ghost sets and ConnectivityMap CSR: bit-exact (integer work);
+  - plain FP64 derivatives: within 1e-12 normwise (||gpu - oracle||_inf /
+    ||oracle||_inf), the tolerance of the hot-path specification.  The thread-
+    per-node gather reproduces the reference's accumulation order, so all
+    fields except the cube root of the ideal-H zeroth moment (CUDA pow vs
+    glibc pow, <= 2 ulp) are in fact bit-exact, which is asserted too;
+  - states after RK2 steps: 1e-12 normwise.
+"""
+import numpy as np
+import pytest
+
+from conftest import normwise
+
+pytestmark = pytest.mark.gpu
+
+DERIV_KEYS = ["delta velocity hydro", "delta specific thermal energy", "delta mass density", "delta position",
+              "new mass density", "normalization", "velocity gradient", "internal velocity gradient",
+              "M SPH gradient correction", "local M SPH gradient correction", "delta H", "new H",
+              "weighted neighbor sum", "mass second moment", "max viscous pressure",
+              "effective viscous pressure", "viscous work rate", "XSPH weight sum", "XSPH delta vi"]
+POW_KEYS = {"weighted neighbor sum", "new H"}
+STATE_KEYS = ["position", "velocity", "mass density", "specific thermal energy", "H", "pressure", "sound speed"]
+
+
+def _sod(gen, abi, nx=32, ny=8, nz=8, **cfgkw):
+    box = ((0.0, 0.0, 0.0), (1.0, ny / nx, nz / nx))
+    ns = gen.sod(nx=nx, ny=ny, nz=nz, box=box)
+    return ns, gen.sod_config(abi, ns_box=box, **cfgkw)
+
+
+def _kh(gen, abi, nx=24, ny=24, nz=12, **cfgkw):
+    ns = gen.kelvin_helmholtz(nx=nx, ny=ny, nz=nz, box=((0, 0, 0), (1.0, 1.0, nz / nx)))
+    return ns, gen.kh_config(abi, xmax=(1.0, 1.0, nz / nx), **cfgkw)
+
+
+CASES = {
+    "sod": lambda g, a: _sod(g, a),
+    "kh": lambda g, a: _kh(g, a),
+    "sod_gradh_xsph": lambda g, a: _sod(g, a, gradhCorrection=1, XSPH=1),
+    "sod_tensile_integrateH": lambda g, a: _sod(g, a, epsTensile=0.3, HUpdate=a.H_INTEGRATE),
+    "kh_noncompatible_integrate_density": lambda g, a: _kh(g, a, compatibleEnergyEvolution=0,
+                                                          densityUpdate=a.DENSITY_INTEGRATE),
+    "sod_expansion_viscosity": lambda g, a: _sod(g, a, linearInExpansion=1, quadraticInExpansion=1, Cq=1.5),
+    "sod_x_periodic_only": lambda g, a: _sod(g, a, periodic=(1, 0, 0)),
+}
+
+
+def _pair(pkg, oracle_mod, case):
+    gen, abi = pkg.generators, pkg.abi
+    ns, cfg = CASES[case](gen, abi)
+    return pkg.SPHHydro(cfg, ns), oracle_mod.OracleProblem(cfg, ns), ns
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_connectivity_bitexact(gpu_lib, pkg, oracle_mod, case):
+    g, o, ns = _pair(pkg, oracle_mod, case)
+    g.build_neighbors()
+    o.build_neighbors()
+    go, gn, gr = g.connectivity()
+    oo, on, orr = o.connectivity()
+    assert np.array_equal(gr, orr)
+    assert np.array_equal(go, oo)
+    assert np.array_equal(gn, on)
+    assert g.num_pairs() == o.num_pairs()
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_evaluate_derivatives_parity(gpu_lib, pkg, oracle_mod, case):
+    g, o, ns = _pair(pkg, oracle_mod, case)
+    g.build_neighbors()
+    o.build_neighbors()
+    g.initialize()
+    o.initialize()
+    g.evaluateDerivatives()
+    o.evaluate_derivatives()
+    for k in DERIV_KEYS:
+        a, b = g.field(k), o.field(k)
+        assert normwise(a, b) <= 1e-12, k
+        if k not in POW_KEYS:
+            assert np.array_equal(a, b), k
+    assert g.dt() == o.dt()
+
+
+@pytest.mark.parametrize("case", ["sod", "kh", "sod_gradh_xsph", "sod_tensile_integrateH",
+                                  "kh_noncompatible_integrate_density"])
+def test_rk2_steps_parity(gpu_lib, pkg, oracle_mod, case):
+    g, o, ns = _pair(pkg, oracle_mod, case)
+    g.build_neighbors()
+    o.build_neighbors()
+    g.evaluateDerivatives()
+    o.evaluate_derivatives()
+    for _ in range(8):
+        tg, dtg = g.step(1)
+        to, dto = o.step(1)
+        assert abs(dtg - dto) <= 1e-12 * dto
+    for k in STATE_KEYS:
+        assert normwise(g.field(k), o.field(k)) <= 1e-12, k
+    for k in ("delta velocity hydro", "delta specific thermal energy", "delta mass density"):
+        assert normwise(g.field(k), o.field(k)) <= 1e-12, k
+
+
+def test_energy_conservation_compatible(gpu_lib, pkg):
+    gen, abi = pkg.generators, pkg.abi
+    ns, cfg = _sod(gen, abi, nx=64, ny=8, nz=8)
+    g = pkg.SPHHydro(cfg, ns)
+    g.build_neighbors()
+    g.evaluateDerivatives()
+    c0 = g.conservation()
+    g.step(20)
+    c1 = g.conservation()
+    assert abs(c1[6] - c0[6]) <= 1e-12 * abs(c0[6])
+    assert np.all(np.abs(c1[1:4]) <= 1e-12 * c0[0])
+
+
+@pytest.mark.parametrize("shrink", [5.0, 1.6])
+def test_sparse_and_empty_neighbor_lists(gpu_lib, pkg, oracle_mod, shrink):
+    """shrink 5: kappa*h < node spacing, so every list is empty (E = 0) and the
+    zero-neighbor branches run (M not inverted, Wsum = 0 ideal H, omega = 1);
+    shrink 1.6: ragged lists of a few neighbors each."""
+    gen, abi = pkg.generators, pkg.abi
+    ns, cfg = _sod(gen, abi, nx=16, ny=4, nz=4, gradhCorrection=1)
+    ns.H[:, [0, 3, 5]] *= shrink
+    g = pkg.SPHHydro(cfg, ns)
+    o = oracle_mod.OracleProblem(cfg, ns)
+    g.build_neighbors()
+    o.build_neighbors()
+    go, gn, _ = g.connectivity()
+    oo, on, _ = o.connectivity()
+    assert np.array_equal(go, oo) and np.array_equal(gn, on)
+    if shrink == 5.0:
+        assert len(gn) == 0
+    g.initialize()
+    o.initialize()
+    g.evaluateDerivatives()
+    o.evaluate_derivatives()
+    for k in DERIV_KEYS + ["grad h corrections"]:
+        assert normwise(g.field(k), o.field(k)) <= 1e-12, k
+
+
+def test_error_paths_return_status(gpu_lib, pkg):
+    gen, abi = pkg.generators, pkg.abi
+    ns, cfg = _sod(gen, abi, nx=16, ny=4, nz=4)
+    g = pkg.SPHHydro(cfg, n=ns.n)
+    with pytest.raises(RuntimeError, match="connectivity not built"):
+        g.evaluateDerivatives()
+    bad = gen.NodeSet(ns.pos, ns.vel, -ns.mass, ns.rho, ns.eps, ns.H, ns.dx)
+    with pytest.raises(RuntimeError, match="non-positive"):
+        g.set_state(bad)
+    # more neighbors than the per-node capacity is reported, not truncated
+    cfg2 = cfg.copy()
+    cfg2.max_neighbors = 64
+    g2 = pkg.SPHHydro(cfg2, ns)
+    with pytest.raises(RuntimeError, match="neighbor"):
+        g2.build_neighbors()
+    # the same problem still works after the error
+    g.set_state(ns)
+    g.build_neighbors()
+    g.evaluateDerivatives()
+
+
+def test_large_neighbor_counts(gpu_lib, pkg, oracle_mod):
+    """nPerh = 3 gives ~900 neighbors per node with the B-spline (capacity 1024)."""
+    gen, abi = pkg.generators, pkg.abi
+    ns, cfg = _sod(gen, abi, nx=24, ny=8, nz=8, nPerh=3.0)
+    ns.H[:, [0, 3, 5]] = 1.0 / (3.0 * ns.dx[0])
+    g = pkg.SPHHydro(cfg, ns)
+    o = oracle_mod.OracleProblem(cfg, ns)
+    g.build_neighbors()
+    o.build_neighbors()
+    go, gn, _ = g.connectivity()
+    oo, on, _ = o.connectivity()
+    assert np.array_equal(gn, on) and np.array_equal(go, oo)
+    assert np.diff(go).max() > 700
+    g.evaluateDerivatives()
+    o.evaluate_derivatives()
+    assert np.array_equal(g.field("delta velocity hydro"), o.field("delta velocity hydro"))
+
+
+def test_empty_problem_rejected(gpu_lib, pkg):
+    abi = pkg.abi
+    import ctypes
+    h = ctypes.c_void_p()
+    cfg = abi.make_config()
+    assert gpu_lib.sphgpu_create(ctypes.byref(cfg), 0, ctypes.byref(h)) == abi.ERR_ARG

@@ -1,0 +1,173 @@
+"""The reference's own known-answer tests, restated against the CPU oracle.
+
+  src/Kernel/tests/testTableKernel.py          table vs analytic W / grad W
+                                               (fuzzyEqual 1e-3 / 1e-2),
+                                               monotone nPerh / Wsum tables
+  src/Neighbor/tests/testNestedGridNeighbor.py neighbor sets against a brute
+                                               force search (checkNeighbors,
+                                               src/SimulationControl/SpheralTestUtilities.py:69-91)
+  src/Neighbor/ConnectivityMap.cc:315-516      ConnectivityMap::valid() invariants
+  src/SPH/tests/testLinearVelocityGradient.py  corrected velocity gradient of a
+                                               linear field within 5e-5
+  src/Hydro/SpecificThermalEnergyPolicy.cc:144 pair forces antisymmetric
+                                               (momentum and, with compatible
+                                               energy, total energy conserved)
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+from conftest import normwise
+
+
+def fuzzyEqual(lhs, rhs, fuzz):
+    return abs(lhs - rhs) / max(1.0, abs(lhs) + abs(rhs)) < fuzz
+
+
+@pytest.mark.parametrize("ktype", [0, 1])
+def test_table_vs_analytic(oracle_mod, ktype):
+    T = oracle_mod.OracleTable(ktype, 1000)
+    L = oracle_mod.lib()
+    extent = 2.0 if ktype == 0 else 1.0
+    eta = np.linspace(0.0, extent, 2001)[:-1]
+    W, gW = T.eval(eta)
+    for e, w, g in zip(eta, W, gW):
+        assert fuzzyEqual(w, L.orc_base_kernel(ktype, 0, e), 1.0e-3)
+        assert fuzzyEqual(g, L.orc_base_kernel(ktype, 1, e), 1.0e-2)
+
+
+@pytest.mark.parametrize("ktype", [0, 1])
+def test_nperh_tables_monotone_and_roundtrip(oracle_mod, ktype):
+    T = oracle_mod.OracleTable(ktype, 1000)
+    co = T.coeffs()
+    nperh, wsum = co[9], co[10]
+    assert np.all(np.diff(nperh) > 0.0)
+    assert np.all(np.diff(wsum) >= 0.0)
+    # For nPerh < 1/kernelExtent only the (zeroed) origin is summed, so the
+    # reference's Wsum table starts with a run of zeros; past it the table is
+    # strictly increasing and the nPerh lookup inverts it.
+    start = int(np.nonzero(wsum > 0.0)[0][0])
+    assert np.all(wsum[:start] == 0.0)
+    assert np.all(np.diff(wsum[start:]) > 0.0)
+    back = T.nperh(wsum[start:])
+    assert all(fuzzyEqual(a, b, 1.0e-10) for a, b in zip(back, nperh[start:]))
+
+
+def _small_sod(gen, nx=16, ny=4, nz=4, seed=7, jitter=0.01):
+    box = ((0.0, 0.0, 0.0), (1.0, ny / nx, nz / nx))
+    return gen.sod(nx=nx, ny=ny, nz=nz, box=box, seed=seed, jitter=jitter), box
+
+
+def _brute_force_neighbors(nodes_pos, nodes_H, ghost_pos, ghost_root, kappa):
+    n = nodes_pos.shape[0]
+    allpos = np.vstack([nodes_pos, ghost_pos])
+    allH = np.vstack([nodes_H, nodes_H[ghost_root]]) if len(ghost_root) else nodes_H
+    k2 = kappa * kappa
+    rows = []
+    for i in range(n):
+        r = nodes_pos[i] - allpos
+        Hi = nodes_H[i]
+
+        def eta2(H, r):
+            ex = H[..., 0] * r[:, 0] + H[..., 1] * r[:, 1] + H[..., 2] * r[:, 2]
+            ey = H[..., 1] * r[:, 0] + H[..., 3] * r[:, 1] + H[..., 4] * r[:, 2]
+            ez = H[..., 2] * r[:, 0] + H[..., 4] * r[:, 1] + H[..., 5] * r[:, 2]
+            return ex * ex + ey * ey + ez * ez
+        m = (eta2(Hi, r) <= k2) | (eta2(allH, r) <= k2)
+        m[i] = False
+        rows.append(np.nonzero(m)[0])
+    return rows
+
+
+def test_connectivity_matches_brute_force(pkg, oracle_mod):
+    gen, abi = pkg.generators, pkg.abi
+    ns, box = _small_sod(gen, nx=16, ny=4, nz=4, jitter=0.2)
+    # anisotropic, varied H exercises the eta_i OR eta_j predicate
+    rng = np.random.default_rng(3)
+    ns.H[:, 0] *= rng.uniform(0.8, 1.25, ns.n)
+    ns.H[:, 3] *= rng.uniform(0.8, 1.25, ns.n)
+    ns.H[:, 5] *= rng.uniform(0.8, 1.25, ns.n)
+    ns.H[:, 1] = 0.05 * ns.H[:, 0] * rng.uniform(-1, 1, ns.n)
+    cfg = gen.sod_config(abi, ns_box=box)
+    o = oracle_mod.OracleProblem(cfg, ns)
+    o.build_neighbors()
+    off, nb, root = o.connectivity()
+    rows = _brute_force_neighbors(ns.pos, ns.H, o.ghost_positions(), root, 2.0)
+    for i in range(ns.n):
+        assert np.array_equal(nb[off[i]:off[i + 1]], rows[i]), i
+
+
+def test_connectivity_valid(pkg, oracle_mod):
+    gen, abi = pkg.generators, pkg.abi
+    ns, box = _small_sod(gen)
+    o = oracle_mod.OracleProblem(gen.sod_config(abi, ns_box=box), ns)
+    o.build_neighbors()
+    off, nb, root = o.connectivity()
+    n = ns.n
+    sets = []
+    for i in range(n):
+        row = nb[off[i]:off[i + 1]]
+        assert np.all(np.diff(row) > 0), "sorted and unique"
+        assert i not in row, "no self interaction"
+        assert np.all(row < n + len(root))
+        sets.append(set(row.tolist()))
+    for i in range(n):
+        for j in sets[i]:
+            if j < n:
+                assert i in sets[j], "internal pairs are symmetric"
+    assert np.all((root >= 0) & (root < n))
+
+
+def test_linear_velocity_gradient(pkg, oracle_mod):
+    """testLinearVelocityGradient: v = (1 + x, 0, 0) on a +-20% jittered
+    lattice; the M-corrected gradient is exact to 5e-5 away from the periodic
+    wrap of the linear field."""
+    gen, abi = pkg.generators, pkg.abi
+    nx = 20
+    box = ((0.0, 0.0, 0.0), (1.0, 0.5, 0.5))
+    ns = gen.sod(nx=nx, ny=10, nz=10, box=box, rho1=1.0, rho2=1.0, P1=1.0, P2=1.0, jitter=0.2, seed=14892042)
+    ns.vel[:, 0] = 1.0 + ns.pos[:, 0]
+    cfg = gen.sod_config(abi, ns_box=box, nPerh=2.01)
+    o = oracle_mod.OracleProblem(cfg, ns)
+    o.build_neighbors()
+    o.evaluate_derivatives()
+    DvDx = o.field("velocity gradient").reshape(-1, 3, 3)
+    h = 2.01 / nx
+    interior = (ns.pos[:, 0] > 2.2 * h + 0.0) & (ns.pos[:, 0] < 1.0 - 2.2 * h)
+    exact = np.zeros((3, 3))
+    exact[0, 0] = 1.0
+    err = np.abs(DvDx[interior] - exact[None]).max()
+    assert interior.sum() > 100
+    assert err < 5.0e-5
+
+
+def test_pair_forces_conserve_momentum_and_energy(pkg, oracle_mod):
+    gen, abi = pkg.generators, pkg.abi
+    ns, box = _small_sod(gen, nx=24, ny=4, nz=4)
+    ns.vel[:, 0] = 0.1 * np.sin(2 * np.pi * ns.pos[:, 0])
+    o = oracle_mod.OracleProblem(gen.sod_config(abi, ns_box=box), ns)
+    o.build_neighbors()
+    o.evaluate_derivatives()
+    a = o.field("delta velocity hydro")
+    m = ns.mass
+    ptot = (m[:, None] * a).sum(axis=0)
+    scale = (m[:, None] * np.abs(a)).sum(axis=0)
+    assert np.all(np.abs(ptot) <= 1e-12 * scale.max())
+    c0 = o.conservation()
+    for _ in range(5):
+        o.step(1)
+    c1 = o.conservation()
+    assert abs(c1[6] - c0[6]) <= 1e-12 * abs(c0[6])
+
+
+def test_oracle_step_runs_kelvin_helmholtz(pkg, oracle_mod):
+    gen, abi = pkg.generators, pkg.abi
+    ns = gen.kelvin_helmholtz(nx=16, ny=16, nz=8, box=((0, 0, 0), (1.0, 1.0, 0.5)))
+    cfg = gen.kh_config(abi, xmax=(1.0, 1.0, 0.5))
+    o = oracle_mod.OracleProblem(cfg, ns)
+    o.build_neighbors()
+    off, nb, root = o.connectivity()
+    assert 5.0 <= len(nb) / ns.n <= 7.5        # Wendland C4, kappa = 1, nPerh 1.35: ~6 neighbors
+    t, dt = o.step(2)
+    assert t > 0.0 and dt > 0.0
