@@ -159,6 +159,17 @@ int sphgpu_conservation(sphgpu_problem* p, double out[8]);
 /* Pair interactions (the reference's ncalc summed over nodes,
  * src/SPH/SPHHydroBase.cc:674) of the current connectivity. */
 int sphgpu_num_pairs(sphgpu_problem* p, int64_t* pairs);
+/* Number of CUDA kernels this problem has launched so far (diagnostics; the
+ * reference's per-node "work" timing field, src/SPH/SPHHydroBase.cc:598,905-925,
+ * has no device counterpart). */
+int sphgpu_kernel_launches(sphgpu_problem* p, int64_t* launches);
+/* Kernel schedules (no counterpart in the reference, whose loops are serial).
+ * stage "neighbor walk": 0 = automatic (thread per node while the 27-cell
+ * candidate set is small, warp per node otherwise), 1 = thread per node,
+ * 2 = warp per node.  Every schedule yields the same ConnectivityMap.
+ * sphgpu_get_schedule reports the schedule the last call actually used. */
+int sphgpu_set_schedule(sphgpu_problem* p, const char* stage, int32_t schedule);
+int sphgpu_get_schedule(sphgpu_problem* p, const char* stage, int32_t* schedule);
 /* Synchronise the problem's stream; returns the first device error. */
 int sphgpu_synchronize(sphgpu_problem* p);
 /* CUDA stream the problem launches on (cudaStream_t as void*). */

@@ -25,6 +25,7 @@ UNITS = [
     ("nbrs.cu", ["-fmad=false"]),
     ("sph.cu", ["-fmad=false"]),
     ("sph_mixed.cu", []),
+    ("crk.cu", ["-fmad=false"]),
     ("table.cc", []),
 ]
 HEADERS = ["devmath.cuh", "problem.cuh", "scan.cuh", "mixed.cuh"]

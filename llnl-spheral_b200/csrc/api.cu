@@ -109,7 +109,7 @@ inline int grid1(int64_t work, int threads = 256) {
 
 struct FieldSpec {
   const char* key;
-  int array;      // 0 = state S, 1 = derivatives D
+  int array;      // 0 = state S, 1 = derivatives D, 2 = CRKSPH fields K
   int field;
   int comps;
 };
@@ -143,6 +143,18 @@ const FieldSpec kFields[] = {
     {"max viscous pressure", 1, D_MAXVP, 1},
     {"effective viscous pressure", 1, D_EFFVP, 1},
     {"viscous work rate", 1, D_VISCW, 1},
+    {"node volume", 0, S_VOL, 1},
+    {"A CRKSPH correction", 2, K_A, 1},
+    {"B CRKSPH correction", 2, K_B, 3},
+    {"grad A CRKSPH correction", 2, K_GRADA, 3},
+    {"grad B CRKSPH correction", 2, K_GRADB, 9},
+    {"m0 CRKSPH moment", 2, K_M0, 1},
+    {"m1 CRKSPH moment", 2, K_M1, 3},
+    {"m2 CRKSPH moment", 2, K_M2, 6},
+    {"grad m0 CRKSPH moment", 2, K_GRADM0, 3},
+    {"grad m1 CRKSPH moment", 2, K_GRADM1, 9},
+    {"grad m2 CRKSPH moment", 2, K_GRADM2, 27},
+    {"mass density gradient", 2, K_GRADRHO, 3},
 };
 
 const FieldSpec* findField(const char* key) {
@@ -168,7 +180,13 @@ int check_device_error(Problem& p, const char* where) {
 }
 
 int validate_config(const sphgpu_config& c) {
-  if (c.hydro != SPHGPU_HYDRO_SPH) { set_error("only SPHGPU_HYDRO_SPH is implemented"); return SPHGPU_ERR_UNSUPPORTED; }
+  if (c.hydro != SPHGPU_HYDRO_SPH && c.hydro != SPHGPU_HYDRO_CRKSPH) { set_error("unknown hydro"); return SPHGPU_ERR_ARG; }
+  if (c.hydro == SPHGPU_HYDRO_CRKSPH && c.precision != SPHGPU_PRECISION_FP64) {
+    set_error("CRKSPH runs in the plain FP64 form only"); return SPHGPU_ERR_UNSUPPORTED;
+  }
+  if (c.crkVolumeType != SPHGPU_CRK_SUMVOLUME && c.crkVolumeType != SPHGPU_CRK_MASSOVERDENSITY) {
+    set_error("unknown crkVolumeType"); return SPHGPU_ERR_ARG;
+  }
   if (c.kernel != SPHGPU_KERNEL_BSPLINE && c.kernel != SPHGPU_KERNEL_WENDLANDC4) { set_error("unknown kernel"); return SPHGPU_ERR_ARG; }
   if (c.num_points < 4) { set_error("num_points must be >= 4"); return SPHGPU_ERR_ARG; }
   if (c.precision != SPHGPU_PRECISION_FP64 && c.precision != SPHGPU_PRECISION_MIXED) { set_error("unknown precision"); return SPHGPU_ERR_ARG; }
@@ -186,7 +204,7 @@ void free_problem(Problem* p) {
   if (p == nullptr) return;
   void* ptrs[] = {p->S, p->S0, p->D, p->rec, p->groot, p->gcode, p->gpos, p->cand, p->cidx, p->sortedIdx,
                   p->cellStart, p->cellFill, p->counts, p->offsets, p->nbr, p->pacc, p->tableCoef, p->nperhTab,
-                  p->wsumTab, p->blockSums, p->d_err, p->d_scal, p->d_red, p->staging, p->coefF, p->mrec};
+                  p->wsumTab, p->blockSums, p->d_err, p->d_scal, p->d_red, p->staging, p->coefF, p->mrec, p->K, p->crec};
   for (void* q : ptrs) if (q) cudaFree(q);
   if (p->pinned) cudaFreeHost(p->pinned);
   if (p->ownStream && p->stream) cudaStreamDestroy(p->stream);
@@ -202,7 +220,7 @@ int upload_aos(Problem& p, const double* host, int comps, int field, bool device
     SPH_CHECK(cudaMemcpyAsync(p.staging, host, sizeof(double)*(size_t)cnt, cudaMemcpyHostToDevice, p.stream));
     src = p.staging;
   }
-  aos_to_soa_kernel<<<grid1(cnt), 256, 0, p.stream>>>(src, comps, p.n, p.S + (int64_t)field*p.n);
+  aos_to_soa_kernel<<<grid1(cnt), 256, 0, p.stream>>>(src, comps, p.n, p.S + (int64_t)field*p.n); ++p.launches;
   SPH_CHECK(cudaGetLastError());
   if (!device) SPH_CHECK(cudaStreamSynchronize(p.stream));
   return SPHGPU_OK;
@@ -211,7 +229,7 @@ int upload_aos(Problem& p, const double* host, int comps, int field, bool device
 int download_aos(Problem& p, const double* base, int comps, int field, double* host) {
   if (host == nullptr) return SPHGPU_OK;
   const int64_t cnt = p.n*comps;
-  soa_to_aos_kernel<<<grid1(cnt), 256, 0, p.stream>>>(base + (int64_t)field*p.n, comps, p.n, p.staging);
+  soa_to_aos_kernel<<<grid1(cnt), 256, 0, p.stream>>>(base + (int64_t)field*p.n, comps, p.n, p.staging); ++p.launches;
   SPH_CHECK(cudaGetLastError());
   SPH_CHECK(cudaMemcpyAsync(host, p.staging, sizeof(double)*(size_t)cnt, cudaMemcpyDeviceToHost, p.stream));
   SPH_CHECK(cudaStreamSynchronize(p.stream));
@@ -227,13 +245,20 @@ int set_state_impl(Problem& p, const double* pos, const double* vel, const doubl
   SPH_TRY(upload_aos(p, eps, 1, S_EPS, device));
   SPH_TRY(upload_aos(p, H, 6, S_H, device));
   // initializeProblemStartup: omega = 1, P and cs from the EOS.
-  fill_kernel<<<grid1(p.n), 256, 0, p.stream>>>(p.S + (int64_t)S_OMEGA*p.n, p.n, 1.0);
+  fill_kernel<<<grid1(p.n), 256, 0, p.stream>>>(p.S + (int64_t)S_OMEGA*p.n, p.n, 1.0); ++p.launches;
   launch_eos(p);
-  check_state_kernel<<<grid1(p.n), 256, 0, p.stream>>>(p.S, p.n, p.d_err);
+  check_state_kernel<<<grid1(p.n), 256, 0, p.stream>>>(p.S, p.n, p.d_err); ++p.launches;
   SPH_CHECK(cudaGetLastError());
   SPH_TRY(check_device_error(p, "set_state"));
   p.haveNbrs = false;
+  p.crkVolumeReady = false;
   return SPHGPU_OK;
+}
+
+// CRKSPH volume: CRKSumVolume or mass/density (records must be packed).
+void crk_volume(Problem& p) {
+  if (p.cfg.crkVolumeType == SPHGPU_CRK_SUMVOLUME) launch_crk_sum_volume(p);
+  else launch_crk_volume_from_density(p);
 }
 
 int build_neighbors_impl(Problem& p) {
@@ -241,7 +266,38 @@ int build_neighbors_impl(Problem& p) {
   SPH_TRY(build_cells_and_csr(p));
   SPH_TRY(check_device_error(p, "build_neighbors"));
   p.haveNbrs = true;
+  if (p.prm.hydro == SPHGPU_HYDRO_CRKSPH) {
+    SPH_TRY(crk_prepare(p));
+    if (!p.crkVolumeReady) {
+      // CRKSPHHydroBase::initializeProblemStartup (src/CRKSPH/CRKSPHHydroBase.cc:279-300)
+      pack_records(p);
+      crk_volume(p);
+      p.crkVolumeReady = true;
+    }
+  }
   return SPHGPU_OK;
+}
+
+// Physics::initialize: grad-h (SPH) or the CRKSPH moments and corrections.
+int initialize_impl(Problem& p) {
+  if (p.prm.hydro == SPHGPU_HYDRO_CRKSPH) {
+    SPH_TRY(crk_prepare(p));
+    launch_crk_initialize(p);
+  } else if (p.prm.gradh) {
+    launch_gradh(p);
+    pack_records(p);
+  }
+  return cuda_status(cudaGetLastError(), "initialize");
+}
+
+// Physics::finalize: CRK volumes then the summed density, or the SPH sum.
+void finalize_impl(Problem& p) {
+  if (p.prm.hydro == SPHGPU_HYDRO_CRKSPH) {
+    crk_volume(p);
+    if (p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM) launch_crk_sum_density(p);
+  } else if (p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM) {
+    launch_sum_density(p);
+  }
 }
 
 int require_nbrs(Problem& p) {
@@ -250,7 +306,10 @@ int require_nbrs(Problem& p) {
 }
 
 int launch_eval(Problem& p) {
-  if (p.cfg.precision == SPHGPU_PRECISION_MIXED) {
+  if (p.prm.hydro == SPHGPU_HYDRO_CRKSPH) {
+    SPH_TRY(crk_prepare(p));
+    launch_crk_eval(p);
+  } else if (p.cfg.precision == SPHGPU_PRECISION_MIXED) {
     SPH_TRY(prepare_mixed(p));
     launch_eval_sph_mixed(p);
   } else {
@@ -274,10 +333,7 @@ int step_impl(Problem& p) {
   launch_update(p, d_dt, 0.5, true);
   pack_records(p);
   // initializeDerivatives + derivs.Zero + evaluateDerivatives at the mid point
-  if (p.prm.gradh) {
-    launch_gradh(p);
-    pack_records(p);
-  }
+  SPH_TRY(initialize_impl(p));
   SPH_TRY(launch_eval(p));
   // full step from state0 with the mid-point derivatives
   SPH_CHECK(cudaMemcpyAsync(p.S, p.S0, sizeof(double)*NSTATE*(size_t)p.n, cudaMemcpyDeviceToDevice, p.stream));
@@ -285,7 +341,7 @@ int step_impl(Problem& p) {
   launch_update(p, d_dt, 1.0, false);
   // applyGhostBoundaries; postStepFinalize (sum density); enforceBoundaries
   pack_records(p);
-  if (p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM) launch_sum_density(p);
+  finalize_impl(p);
   launch_enforce_boundaries(p);
   SPH_CHECK(cudaMemcpyAsync(d_lastDt, d_dt, sizeof(double), cudaMemcpyDeviceToDevice, p.stream));
   SPH_CHECK(cudaGetLastError());
@@ -312,9 +368,9 @@ int exclusive_scan_i32(Problem& p, const int32_t* in, int64_t n, int64_t* out, i
   const int64_t tiles = (n + SCAN_TILE - 1)/SCAN_TILE;
   SPH_TRY(ensure_block_sums(p, tiles + 1));
   int64_t* dtotal = p.blockSums + tiles;
-  if (tiles > 0) scan_tile_sums_kernel<<<(unsigned)tiles, SCAN_THREADS, 0, p.stream>>>(in, n, p.blockSums);
-  scan_sums_kernel<<<1, SCAN_THREADS, 0, p.stream>>>(p.blockSums, tiles, dtotal);
-  scan_apply_kernel<<<(unsigned)(tiles > 0 ? tiles : 1), SCAN_THREADS, 0, p.stream>>>(in, n, p.blockSums, out, dtotal);
+  if (tiles > 0) scan_tile_sums_kernel<<<(unsigned)tiles, SCAN_THREADS, 0, p.stream>>>(in, n, p.blockSums); p.launches += (tiles > 0);
+  scan_sums_kernel<<<1, SCAN_THREADS, 0, p.stream>>>(p.blockSums, tiles, dtotal); ++p.launches;
+  scan_apply_kernel<<<(unsigned)(tiles > 0 ? tiles : 1), SCAN_THREADS, 0, p.stream>>>(in, n, p.blockSums, out, dtotal); ++p.launches;
   SPH_CHECK(cudaGetLastError());
   SPH_CHECK(cudaMemcpyAsync(total, dtotal, sizeof(int64_t), cudaMemcpyDeviceToHost, p.stream));
   SPH_CHECK(cudaStreamSynchronize(p.stream));
@@ -347,7 +403,7 @@ int ensure_capacity_ghosts(Problem& p, int64_t need) {
   SPH_TRY(grow_preserve(p.cidx, 0, nc, p.stream));
   SPH_TRY(grow_preserve(p.sortedIdx, 0, nc, p.stream));
   cudaFree(p.cand);
-  SPH_TRY(dalloc(p.cand, 9*nc));
+  SPH_TRY(dalloc(p.cand, 10*nc));
   cudaFree(p.rec);
   SPH_TRY(dalloc(p.rec, RECW*nc));
   p.candcap = nc;
@@ -425,6 +481,7 @@ int sphgpu_create(const sphgpu_config* cfg, int64_t n_internal, sphgpu_problem**
     P.linearInExp = cfg->linearInExpansion; P.quadInExp = cfg->quadraticInExpansion;
     P.useVelMagDt = cfg->useVelocityMagnitudeForDt; P.HUpdate = cfg->HUpdate; P.densityUpdate = cfg->densityUpdate;
     P.gradh = cfg->gradhCorrection;
+    P.hydro = cfg->hydro;
     // periodic planes: PeriodicBoundary(plane1 = (xmin, +e_a), plane2 = (xmax, -e_a))
     for (int a = 0; a < 3; ++a) {
       P.bcs.periodic[a] = cfg->periodic[a] ? 1 : 0;
@@ -439,7 +496,8 @@ int sphgpu_create(const sphgpu_config* cfg, int64_t n_internal, sphgpu_problem**
     if ((rc = dalloc(p->S, NSTATE*n)) != SPHGPU_OK) break;
     if ((rc = dalloc(p->S0, NSTATE*n)) != SPHGPU_OK) break;
     if ((rc = dalloc(p->D, NDERIV*n)) != SPHGPU_OK) break;
-    if ((rc = dalloc(p->staging, 9*n)) != SPHGPU_OK) break;
+    // widest field: Tensor (9) for SPH, the third-rank grad m2 (27) for CRKSPH
+    if ((rc = dalloc(p->staging, (cfg->hydro == SPHGPU_HYDRO_CRKSPH ? 27 : 9)*n)) != SPHGPU_OK) break;
     if ((rc = dalloc(p->d_err, 4)) != SPHGPU_OK) break;
     if ((rc = dalloc(p->d_scal, 32)) != SPHGPU_OK) break;
     p->redcap = 148*4*8;
@@ -502,7 +560,8 @@ int sphgpu_get_field(sphgpu_problem* p, const char* key, double* out, int64_t co
   const FieldSpec* f = findField(key);
   if (f == nullptr) { set_error(std::string("unknown field key: ") + (key ? key : "(null)")); return SPHGPU_ERR_ARG; }
   if (count != p->n*f->comps) { set_error("sphgpu_get_field: count mismatch"); return SPHGPU_ERR_ARG; }
-  return download_aos(*p, f->array == 0 ? p->S : p->D, f->comps, f->field, out);
+  if (f->array == 2 && p->K == nullptr) { set_error("CRKSPH fields exist for CRKSPH problems only"); return SPHGPU_ERR_STATE; }
+  return download_aos(*p, f->array == 0 ? p->S : (f->array == 1 ? p->D : p->K), f->comps, f->field, out);
 }
 
 int sphgpu_build_neighbors(sphgpu_problem* p) {
@@ -534,11 +593,8 @@ int sphgpu_initialize(sphgpu_problem* p, double time, double dt) {
   if (p == nullptr) return SPHGPU_ERR_ARG;
   (void)time; (void)dt;
   SPH_TRY(require_nbrs(*p));
-  if (p->prm.gradh) {
-    pack_records(*p);
-    launch_gradh(*p);
-  }
-  return cuda_status(cudaGetLastError(), "initialize");
+  pack_records(*p);
+  return initialize_impl(*p);
 }
 
 int sphgpu_evaluate_derivatives(sphgpu_problem* p, double time, double dt) {
@@ -562,7 +618,7 @@ int sphgpu_finalize(sphgpu_problem* p, double time, double dt) {
   (void)time; (void)dt;
   SPH_TRY(require_nbrs(*p));
   pack_records(*p);
-  if (p->prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM) launch_sum_density(*p);
+  finalize_impl(*p);
   return cuda_status(cudaGetLastError(), "finalize");
 }
 
@@ -602,6 +658,36 @@ int sphgpu_num_pairs(sphgpu_problem* p, int64_t* pairs) {
   SPH_TRY(require_nbrs(*p));
   *pairs = p->pairs;
   return SPHGPU_OK;
+}
+
+int sphgpu_kernel_launches(sphgpu_problem* p, int64_t* launches) {
+  if (p == nullptr || launches == nullptr) return SPHGPU_ERR_ARG;
+  *launches = p->launches;
+  return SPHGPU_OK;
+}
+
+int sphgpu_set_schedule(sphgpu_problem* p, const char* stage, int32_t schedule) {
+  if (p == nullptr || stage == nullptr) return SPHGPU_ERR_ARG;
+  if (std::strcmp(stage, "neighbor walk") == 0) {
+    if (schedule < NBR_SCHEDULE_AUTO || schedule > NBR_SCHEDULE_WARP) {
+      set_error("neighbor walk schedule must be 0 (auto), 1 (thread per node) or 2 (warp per node)");
+      return SPHGPU_ERR_ARG;
+    }
+    p->nbrSchedule = schedule;
+    return SPHGPU_OK;
+  }
+  set_error(std::string("unknown schedule stage: ") + stage);
+  return SPHGPU_ERR_ARG;
+}
+
+int sphgpu_get_schedule(sphgpu_problem* p, const char* stage, int32_t* schedule) {
+  if (p == nullptr || stage == nullptr || schedule == nullptr) return SPHGPU_ERR_ARG;
+  if (std::strcmp(stage, "neighbor walk") == 0) {
+    *schedule = p->lastNbrSchedule;
+    return SPHGPU_OK;
+  }
+  set_error(std::string("unknown schedule stage: ") + stage);
+  return SPHGPU_ERR_ARG;
 }
 
 int sphgpu_synchronize(sphgpu_problem* p) {

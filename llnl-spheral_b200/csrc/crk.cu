@@ -1,0 +1,484 @@
+// CRKSPH hydro kernels (linear order), plain FP64 form (compiled with -fmad=false).
+//
+// Replaces:
+//   crk_moments_corrections  computeCRKSPHMoments (src/CRKSPH/computeCRKSPHMoments.cc:40-287,
+//                            NodeCoupling = 1) fused with computeLinearCRKSPHCorrections
+//                            (src/CRKSPH/computeCRKSPHCorrections.cc:210-283)
+//   crk_eval                 CRKSPHHydroBase::evaluateDerivatives
+//                            (src/CRKSPH/CRKSPHHydroBase.cc:646-1102) with
+//                            CRKSPHKernelAndGradient (src/CRKSPH/CRKSPHUtilitiesInline.hh:58-129)
+//   crk_sum_volume           computeCRKSPHSumVolume (src/CRKSPH/computeCRKSPHSumVolume.cc:43-127)
+//   crk_sum_density          computeCRKSPHSumMassDensity (src/CRKSPH/computeCRKSPHSumMassDensity.cc:28-139)
+//
+// All pair loops gather over node i's ascending CSR row.  Every CRKSPH pair
+// term is even or odd under i <-> j with exact FP negation, so it is formed
+// from node i's side; the only order-sensitive products (0.5*w_i*w_j) are
+// taken in the reference's owner order.  Self terms enter where the
+// reference adds them, so node sums see the reference's summation order.
+#include "problem.cuh"
+
+namespace sphgpu {
+
+namespace {
+
+inline int nblk(int64_t work, int threads) {
+  int64_t b = (work + threads - 1)/threads;
+  return (int)(b < 1 ? 1 : b);
+}
+
+__device__ __forceinline__ double ldg(const double* p) { return __ldg(p); }
+__device__ __forceinline__ double& el(V3& v, int i) { return (&v.x)[i]; }
+__device__ __forceinline__ double el(const V3& v, int i) { return (&v.x)[i]; }
+__device__ __forceinline__ double& el(T9& t, int i, int j) { return (&t.xx)[3*i + j]; }
+__device__ __forceinline__ double el(const T9& t, int i, int j) { return (&t.xx)[3*i + j]; }
+__device__ __forceinline__ int symIndex(int i, int j) {
+  // xx xy xz / xy yy yz / xz yz zz
+  return i == 0 ? j : (i == 1 ? (j == 0 ? 1 : j + 2) : (j == 0 ? 2 : (j == 1 ? 4 : 5)));
+}
+__device__ __forceinline__ double sel(const Sym& s, int i, int j) { return (&s.xx)[symIndex(i, j)]; }
+
+struct CRec {
+  V3 r, v;
+  double m, rho, cs, P, Hdet, vol;
+  Sym H;
+  double A;
+  V3 B, gA;
+  T9 gB;
+};
+
+__device__ __forceinline__ CRec loadCRec(const double* crec, int64_t k) {
+  const double2* q = reinterpret_cast<const double2*>(crec + k*CRECW);
+  double2 a[17];
+#pragma unroll
+  for (int t = 0; t < 17; ++t) a[t] = __ldg(q + t);
+  const double* d = reinterpret_cast<const double*>(a);
+  CRec R;
+  R.r = V3{d[C_X], d[C_Y], d[C_Z]};
+  R.v = V3{d[C_VX], d[C_VY], d[C_VZ]};
+  R.m = d[C_M]; R.rho = d[C_RHO]; R.cs = d[C_CS]; R.P = d[C_P]; R.Hdet = d[C_HDET]; R.vol = d[C_VOL];
+  R.H = Sym{d[C_H], d[C_H + 1], d[C_H + 2], d[C_H + 3], d[C_H + 4], d[C_H + 5]};
+  R.A = d[C_A];
+  R.B = V3{d[C_B], d[C_B + 1], d[C_B + 2]};
+  R.gA = V3{d[C_GRADA], d[C_GRADA + 1], d[C_GRADA + 2]};
+  R.gB = T9{d[C_GRADB], d[C_GRADB + 1], d[C_GRADB + 2], d[C_GRADB + 3], d[C_GRADB + 4], d[C_GRADB + 5],
+            d[C_GRADB + 6], d[C_GRADB + 7], d[C_GRADB + 8]};
+  return R;
+}
+
+__global__ void pack_crk_records_kernel(const double* S, const double* K, int64_t n, const int32_t* groot,
+                                        const uint32_t* gcode, int64_t ntot, BoxBCs bcs, double* crec) {
+  for (int64_t k = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; k < ntot; k += (int64_t)gridDim.x*blockDim.x) {
+    const int64_t r = k < n ? k : groot[k - n];
+    V3 x{S[S_X*n + r], S[S_Y*n + r], S[S_Z*n + r]};
+    if (k >= n) x = ghostPosition(bcs, x, gcode[k - n]);
+    const Sym H{S[(S_H + 0)*n + r], S[(S_H + 1)*n + r], S[(S_H + 2)*n + r],
+                S[(S_H + 3)*n + r], S[(S_H + 4)*n + r], S[(S_H + 5)*n + r]};
+    double v[CRECW];
+    v[C_X] = x.x; v[C_Y] = x.y; v[C_Z] = x.z;
+    v[C_VX] = S[S_VX*n + r]; v[C_VY] = S[S_VY*n + r]; v[C_VZ] = S[S_VZ*n + r];
+    v[C_M] = S[S_M*n + r]; v[C_RHO] = S[S_RHO*n + r]; v[C_CS] = S[S_CS*n + r]; v[C_P] = S[S_P*n + r];
+    v[C_HDET] = sdet(H); v[C_VOL] = S[S_VOL*n + r];
+    v[C_H] = H.xx; v[C_H + 1] = H.xy; v[C_H + 2] = H.xz; v[C_H + 3] = H.yy; v[C_H + 4] = H.yz; v[C_H + 5] = H.zz;
+    v[C_A] = K[K_A*n + r];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      v[C_B + c] = K[(K_B + c)*n + r];
+      v[C_GRADA + c] = K[(K_GRADA + c)*n + r];
+    }
+#pragma unroll
+    for (int c = 0; c < 9; ++c) v[C_GRADB + c] = K[(K_GRADB + c)*n + r];
+    double2* q = reinterpret_cast<double2*>(crec + k*CRECW);
+#pragma unroll
+    for (int t = 0; t < CRECW/2; ++t) q[t] = make_double2(v[2*t], v[2*t + 1]);
+  }
+}
+
+// Record fields shared with the SPH record (positions, H, Hdet).
+__device__ __forceinline__ V3 recPos(const double* rec, int64_t j) {
+  return V3{ldg(rec + j*RECW + R_X), ldg(rec + j*RECW + R_Y), ldg(rec + j*RECW + R_Z)};
+}
+__device__ __forceinline__ Sym recH(const double* rec, int64_t j) {
+  const double* h = rec + j*RECW + R_H;
+  return Sym{ldg(h), ldg(h + 1), ldg(h + 2), ldg(h + 3), ldg(h + 4), ldg(h + 5)};
+}
+
+// ---------------------------------------------------------------- volumes
+__global__ void crk_sum_volume_kernel(Params P, const double* rec, int64_t n, const int64_t* offsets,
+                                      const int32_t* nbr, double* S) {
+  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const V3 ri = recPos(rec, i);
+  const Sym Hi = recH(rec, i);
+  const double Hdeti = ldg(rec + i*RECW + R_HDET);
+  const double half = 0.5*P.W.extent;
+  const double etaVolMax = half*half*half*(4.0/3.0*3.14159265358979323846);
+  double vol = 0.0;
+  for (int64_t k = offsets[i]; k < offsets[i + 1]; ++k) {
+    const int32_t j = __ldg(nbr + k);
+    const V3 rij = vsub(ri, recPos(rec, j));
+    vol += tableKernel(P.W, mag(sdot(Hi, rij)), Hdeti);
+  }
+  vol += tableKernel(P.W, 0.0, Hdeti);
+  S[S_VOL*n + i] = dmin(etaVolMax/Hdeti, 1.0/vol);
+}
+
+__global__ void crk_volume_from_density_kernel(int64_t n, double* S) {
+  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  S[S_VOL*n + i] = S[S_M*n + i]/S[S_RHO*n + i];
+}
+
+__global__ void crk_sum_density_kernel(Params P, const double* rec, int64_t n, const int64_t* offsets,
+                                       const int32_t* nbr, const int32_t* groot, double* S) {
+  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double mi = S[S_M*n + i], Vi = S[S_VOL*n + i];
+  const double Hdeti = ldg(rec + i*RECW + R_HDET);
+  const V3 ri = recPos(rec, i);
+  double wsum = 0.0, rho = 0.0, vol1 = 0.0;
+  for (int64_t k = offsets[i]; k < offsets[i + 1]; ++k) {
+    const int32_t j = __ldg(nbr + k);
+    const int64_t r = j < n ? (int64_t)j : (int64_t)__ldg(groot + (j - n));
+    const double mj = ldg(S + S_M*n + r), Vj = ldg(S + S_VOL*n + r);
+    const V3 rij = vsub(ri, recPos(rec, j));
+    const double Wj = tableKernel(P.W, mag(sdot(recH(rec, j), rij)), ldg(rec + (int64_t)j*RECW + R_HDET));
+    wsum += Vj*Wj;
+    rho += mj*Vj*Wj;
+    vol1 += Vj*Vj*Wj;
+  }
+  const double W0 = tableKernel(P.W, 0.0, Hdeti);
+  wsum += Vi*W0;
+  vol1 = (vol1 + Vi*Vi*W0)/wsum;
+  S[S_RHO*n + i] = dmax(dmax(P.rhoMin, 0.1*mi*Hdeti), dmin(P.rhoMax, (rho + mi*Vi*W0)/(wsum*vol1)));
+}
+
+// ---------------------------------------------------------------- moments + corrections
+__global__ void __launch_bounds__(128) crk_moments_corrections_kernel(Params P, const double* rec, int64_t n,
+                                                                      const int64_t* offsets, const int32_t* nbr,
+                                                                      const int32_t* groot, const double* S,
+                                                                      double* K) {
+  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const V3 ri = recPos(rec, i);
+  const Sym Hi = recH(rec, i);
+  const double Hdeti = ldg(rec + i*RECW + R_HDET);
+  const double wi = S[S_VOL*n + i];
+  double m0 = 0.0;
+  V3 m1{0, 0, 0}, gm0{0, 0, 0};
+  double m2[6] = {0, 0, 0, 0, 0, 0};
+  T9 gm1{0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double gm2[27];
+#pragma unroll
+  for (int c = 0; c < 27; ++c) gm2[c] = 0.0;
+  const double wwself = wi*tableKernel(P.W, 0.0, Hdeti);
+  bool selfDone = false;
+  const int64_t k0 = offsets[i], k1 = offsets[i + 1];
+  for (int64_t k = k0; k <= k1; ++k) {
+    const int32_t j = k < k1 ? __ldg(nbr + k) : INT32_MAX;
+    if (!selfDone && j > (int32_t)i) {
+      m0 += wwself;
+      gm1.xx += 1.0*wwself; gm1.xy += 0.0*wwself; gm1.xz += 0.0*wwself;
+      gm1.yx += 0.0*wwself; gm1.yy += 1.0*wwself; gm1.yz += 0.0*wwself;
+      gm1.zx += 0.0*wwself; gm1.zy += 0.0*wwself; gm1.zz += 1.0*wwself;
+      selfDone = true;
+    }
+    if (k == k1) break;
+    const int64_t r = j < n ? (int64_t)j : (int64_t)__ldg(groot + (j - n));
+    const double wj = ldg(S + S_VOL*n + r);
+    const V3 rij = vsub(ri, recPos(rec, j));
+    const Sym Hj = recH(rec, j);
+    const double Hdetj = ldg(rec + (int64_t)j*RECW + R_HDET);
+    const V3 etai = sdot(Hi, rij);
+    const V3 etaj = sdot(Hj, rij);
+    double Wa, gWa, Wb, gWb;
+    tableKernelAndGrad(P.W, mag(etai), Hdeti, Wa, gWa);
+    tableKernelAndGrad(P.W, mag(etaj), Hdetj, Wb, gWb);
+    const double Wij = 0.5*(Wa + Wb);
+    const V3 gradWj = vmul(vadd(vmul(sdot(Hj, unitVector(etaj)), gWb), vmul(sdot(Hi, unitVector(etai)), gWa)), 0.5);
+    const double wwj = wj*Wij;
+    m0 += wwj;
+#pragma unroll
+    for (int ii = 0; ii < 3; ++ii) el(gm0, ii) += wj*el(gradWj, ii);
+#pragma unroll
+    for (int ii = 0; ii < 3; ++ii) {
+      el(m1, ii) += wwj*el(rij, ii);
+#pragma unroll
+      for (int jj = 0; jj < 3; ++jj) el(gm1, ii, jj) += wj*el(rij, ii)*el(gradWj, jj);
+      el(gm1, ii, ii) += wj*Wij;
+    }
+#pragma unroll
+    for (int ii = 0; ii < 3; ++ii) {
+#pragma unroll
+      for (int jj = ii; jj < 3; ++jj) m2[symIndex(ii, jj)] += wwj*(el(rij, ii)*el(rij, jj));
+#pragma unroll
+      for (int jj = 0; jj < 3; ++jj) {
+        const double thpt = el(rij, ii)*el(rij, jj);
+#pragma unroll
+        for (int kk = 0; kk < 3; ++kk) gm2[9*ii + 3*jj + kk] += wj*thpt*el(gradWj, kk);
+        gm2[9*ii + 3*jj + jj] += wwj*el(rij, ii);
+        gm2[9*jj + 3*ii + jj] += wwj*el(rij, ii);
+      }
+    }
+  }
+  // computeLinearCRKSPHCorrections
+  const Sym m2s{m2[0], m2[1], m2[2], m2[3], m2[4], m2[5]};
+  const double hdet2 = 1.0/(Hdeti*Hdeti);
+  const double m2det = sdet(m2s);
+  Sym m2inv{0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  if (fabs(m2det) > 1.0e-5*hdet2) {
+    const Sym c{m2s.yy*m2s.zz - m2s.yz*m2s.yz, m2s.yz*m2s.xz - m2s.xy*m2s.zz, m2s.xy*m2s.yz - m2s.yy*m2s.xz,
+                m2s.xx*m2s.zz - m2s.xz*m2s.xz, m2s.xy*m2s.xz - m2s.xx*m2s.yz, m2s.xx*m2s.yy - m2s.xy*m2s.xy};
+    m2inv = sdiv(c, m2det);
+  }
+  const V3 m2invm1 = sdot(m2inv, m1);
+  const double Ainv = m0 - dot(m2invm1, m1);
+  const double A = 1.0/Ainv;
+  const V3 B{-m2invm1.x, -m2invm1.y, -m2invm1.z};
+  V3 gA = vmul(gm0, -A*A);
+  T9 gB{0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int ii = 0; ii < 3; ++ii) {
+    for (int jj = 0; jj < 3; ++jj) {
+      for (int kk = 0; kk < 3; ++kk) {
+        el(gA, ii) += A*A*sel(m2inv, jj, kk)*el(m1, kk)*el(gm1, jj, ii);
+        el(gA, ii) += A*A*sel(m2inv, jj, kk)*el(gm1, kk, ii)*el(m1, jj);
+        el(gB, ii, jj) -= sel(m2inv, ii, kk)*el(gm1, kk, jj);
+        for (int ll = 0; ll < 3; ++ll) {
+          for (int mm = 0; mm < 3; ++mm) {
+            el(gA, ii) -= A*A*sel(m2inv, jj, kk)*gm2[9*kk + 3*ll + ii]*sel(m2inv, ll, mm)*el(m1, mm)*el(m1, jj);
+            el(gB, ii, jj) += sel(m2inv, ii, kk)*gm2[9*kk + 3*ll + jj]*sel(m2inv, ll, mm)*el(m1, mm);
+          }
+        }
+      }
+    }
+  }
+  double* o = K + i;
+  o[K_A*n] = A;
+  for (int c = 0; c < 3; ++c) {
+    o[(K_B + c)*n] = el(B, c);
+    o[(K_GRADA + c)*n] = el(gA, c);
+    o[(K_M1 + c)*n] = el(m1, c);
+    o[(K_GRADM0 + c)*n] = el(gm0, c);
+  }
+  for (int c = 0; c < 9; ++c) {
+    o[(K_GRADB + c)*n] = (&gB.xx)[c];
+    o[(K_GRADM1 + c)*n] = (&gm1.xx)[c];
+  }
+  o[K_M0*n] = m0;
+  for (int c = 0; c < 6; ++c) o[(K_M2 + c)*n] = m2[c];
+  for (int c = 0; c < 27; ++c) o[(K_GRADM2 + c)*n] = gm2[c];
+}
+
+// CRKSPHKernelAndGradient, LinearOrder (correction limits at +-max never bind).
+__device__ __forceinline__ void crkKernel(const TableDev& T, const V3& rij, const V3& etai, const Sym& Hi,
+                                          double Hdeti, const V3& etaj, const Sym& Hj, double Hdetj, double Ai,
+                                          const V3& Bi, const V3& gradAi, const T9& gradBi, double& WCRK,
+                                          double& gradWSPH, V3& gradWCRK) {
+  double Wa, gWa, Wb, gWb;
+  tableKernelAndGrad(T, mag(etai), Hdeti, Wa, gWa);
+  tableKernelAndGrad(T, mag(etaj), Hdetj, Wb, gWb);
+  const double Wij = 0.5*(Wa + Wb);
+  const V3 gradWij = vmul(vadd(vmul(sdot(Hi, unitVector(etai)), gWa), vmul(sdot(Hj, unitVector(etaj)), gWb)), 0.5);
+  gradWSPH = 0.5*(gWa + gWb);
+  const double correction0 = Ai*(1.0 + dot(Bi, rij));
+  const double correction = dmax(-1.7976931348623157e308, dmin(1.7976931348623157e308, correction0));
+  WCRK = correction*Wij;
+  gradWCRK = vmul(gradWij, correction);
+  if (correction0 > -1.7976931348623157e308 && correction0 < 1.7976931348623157e308) {
+    gradWCRK = vadd(gradWCRK, vadd(vmul(vmul(Bi, Ai), Wij), vmul(vmul(gradAi, 1.0 + dot(Bi, rij)), Wij)));
+#pragma unroll
+    for (int ii = 0; ii < 3; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < 3; ++jj) el(gradWCRK, ii) += Ai*Wij*el(gradBi, jj, ii)*el(rij, jj);
+  }
+}
+
+template<bool XSPH, bool COMPAT>
+__global__ void __launch_bounds__(128) crk_eval_kernel(Params P, const double* crec, int64_t n,
+                                                       const int64_t* offsets, const int32_t* nbr, double* D,
+                                                       double* K, double* pacc, int64_t ecap) {
+  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const CRec I = loadCRec(crec, i);
+  const double Cl = P.Cl*(0.5*(1.0 + 1.0)*1.0);
+  const double Cq = P.Cq*(0.5*(1.0 + 1.0)*1.0);
+  double wns = 0.0, maxvp = 0.0, effvp = 0.0, viscW = 0.0, DepsDt = 0.0;
+  V3 DvDt{0, 0, 0}, gradRho{0, 0, 0}, XSPHdv{0, 0, 0};
+  Sym m2{0, 0, 0, 0, 0, 0};
+  T9 DvDx{0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const int64_t k0 = offsets[i], k1 = offsets[i + 1];
+  for (int64_t k = k0; k < k1; ++k) {
+    const int32_t j = __ldg(nbr + k);
+    const CRec J = loadCRec(crec, j);
+    const bool own = j > (int32_t)i;
+    const V3 rij = vsub(I.r, J.r);
+    const V3 etai = sdot(I.H, rij);
+    const V3 etaj = sdot(J.H, rij);
+    const V3 vij = vsub(I.v, J.v);
+    double Wj, gWj, Wi, gWi;
+    V3 gradWj, gradWi;
+    crkKernel(P.W, rij, etai, I.H, I.Hdet, etaj, J.H, J.Hdet, I.A, I.B, I.gA, I.gB, Wj, gWj, gradWj);
+    crkKernel(P.W, V3{-rij.x, -rij.y, -rij.z}, V3{-etaj.x, -etaj.y, -etaj.z}, J.H, J.Hdet,
+              V3{-etai.x, -etai.y, -etai.z}, I.H, I.Hdet, J.A, J.B, J.gA, J.gB, Wi, gWi, gradWi);
+    const V3 deltagrad = vsub(gradWj, gradWi);
+    // SPH moments for the ideal H
+    {
+      double W0a, gW0a;
+      tableKernelAndGrad(P.W, mag(etai), I.Hdet, W0a, gW0a);
+      const V3 gradWSPHi = vmul(sdot(I.H, unitVector(etai)), gW0a);
+      const double rij2 = mag2(rij);
+      const Sym thpt = smul(selfdyad(rij), safeInvVar(rij2*rij2*rij2));
+      wns += 1.0*fabs(gWi);
+      m2 = sadd(m2, smul(thpt, 1.0*mag2(gradWSPHi)));
+    }
+    // Monaghan-Gingold Pi (orientation-invariant mu)
+    const double mui = dot(vij, etai)/(mag2(etai) + P.eps2);
+    const double muj = dot(vij, etaj)/(mag2(etaj) + P.eps2);
+    const double mi0 = dmin(0.0, mui), mj0 = dmin(0.0, muj);
+    const double ei = -Cl*I.cs*(P.linearInExp ? mui : mi0) + Cq*(P.quadInExp ? -sgn(mui)*mui*mui : mi0*mi0);
+    const double ej = -Cl*J.cs*(P.linearInExp ? muj : mj0) + Cq*(P.quadInExp ? -sgn(muj)*muj*muj : mj0*mj0);
+    const double qi = ei/I.rho, qj = ej/J.rho;
+    // (rho_i^2 Pi_i + rho_j^2 Pi_j).dot(deltagrad): owner term first
+    const double qsi = qi*(I.rho*I.rho), qsj = qj*(J.rho*J.rho);
+    const double qsum = own ? qsi + qsj : qsj + qsi;
+    const V3 Qacc = vmul(deltagrad, qsum);
+    const double workQi = J.rho*J.rho*dot(vmul(vij, qj), deltagrad);
+    const double Qi = I.rho*I.rho*fabs(qi);
+    maxvp = dmax(maxvp, 4.0*Qi);
+    effvp += J.vol*Qi*Wj;
+    const double f = own ? 0.5*I.vol*J.vol : 0.5*J.vol*I.vol;    // 0.5*weight_owner*weight_other
+    viscW += f/I.m*workQi;
+    tsubfrom(DvDx, tmul(dyad(vij, gradWj), J.vol));
+    gradRho = vadd(gradRho, vmul(gradWj, J.vol*(J.rho - I.rho)));
+    const double Psum = own ? I.P + J.P : J.P + I.P;
+    const V3 force = vmul(vadd(vmul(deltagrad, Psum), Qacc), f);
+    DvDt = vsub(DvDt, vdiv(force, I.m));
+    if (COMPAT) {
+      // owner's pair acceleration (-force_owner/m_owner)
+      const V3 pa = own ? vdiv(V3{-force.x, -force.y, -force.z}, I.m) : vdiv(force, J.m);
+      pacc[k] = pa.x;
+      pacc[ecap + k] = pa.y;
+      pacc[2*ecap + k] = pa.z;
+    }
+    DepsDt += f*(J.P*dot(vij, deltagrad) + workQi)/I.m;
+    if (XSPH) XSPHdv = vsub(XSPHdv, vmul(vij, J.vol*Wj));
+  }
+  // ---- per-node finish (src/CRKSPH/CRKSPHHydroBase.cc:1036-1081)
+  const double DrhoDt = -I.rho*ttrace(DvDx);
+  wns = dmax(0.0, wns/I.Hdet);
+  wns = sgn(wns)*pow(fabs(wns), 0.3333333333333333);
+  m2 = sdiv(m2, I.Hdet*I.Hdet);
+  const V3 DxDt = XSPH ? vadd(I.v, XSPHdv) : I.v;
+  const Sym DHDt = smul(sdiv(sneg(I.H), 3.0), ttrace(DvDx));
+  double nPerhCur;
+  if (fuzzyEqual(wns, 0.0)) {
+    nPerhCur = 0.5*P.nPerh;
+  } else {
+    const int nt = P.W.n;
+    const bool ascnd = ldg(P.wsum + nt - 1) >= ldg(P.wsum);
+    int jl = -1, ju = nt;
+    while (ju - jl > 1) {
+      const int jm = (ju + jl)/2;
+      if ((wns >= ldg(P.wsum + jm)) == ascnd) jl = jm; else ju = jm;
+    }
+    if (jl == -1) nPerhCur = ldg(P.nperh);
+    else if (jl + 1 == nt) nPerhCur = ldg(P.nperh + nt - 1);
+    else {
+      const double nl = ldg(P.nperh + jl), nu = ldg(P.nperh + jl + 1);
+      const double wl = ldg(P.wsum + jl), wu = ldg(P.wsum + jl + 1);
+      nPerhCur = dmin(nu, dmax(nl, nl + (wns - wl)/(wu - wl)*(nu - nl)));
+    }
+  }
+  const double s = dmin(4.0, dmax(0.25, P.nPerh/(nPerhCur + 1.0e-30)));
+  const double a = s < 1.0 ? 0.4*(1.0 + s*s) : 0.4*(1.0 + 1.0/(s*s*s));
+  const double hi1 = dmin(P.hmax, dmax(P.hmin, (1.0/I.H.xx)*(1.0 - a + a*s)));
+  const double hinv = 1.0/hi1;
+
+  double* d = D + i;
+  d[(D_DXDT + 0)*n] = DxDt.x; d[(D_DXDT + 1)*n] = DxDt.y; d[(D_DXDT + 2)*n] = DxDt.z;
+  d[(D_DVDT + 0)*n] = DvDt.x; d[(D_DVDT + 1)*n] = DvDt.y; d[(D_DVDT + 2)*n] = DvDt.z;
+  d[D_DRHODT*n] = DrhoDt;
+  d[D_DEPSDT*n] = DepsDt;
+  d[(D_DHDT + 0)*n] = DHDt.xx; d[(D_DHDT + 1)*n] = DHDt.xy; d[(D_DHDT + 2)*n] = DHDt.xz;
+  d[(D_DHDT + 3)*n] = DHDt.yy; d[(D_DHDT + 4)*n] = DHDt.yz; d[(D_DHDT + 5)*n] = DHDt.zz;
+  d[(D_HIDEAL + 0)*n] = 1.0*hinv; d[(D_HIDEAL + 1)*n] = 0.0*hinv; d[(D_HIDEAL + 2)*n] = 0.0*hinv;
+  d[(D_HIDEAL + 3)*n] = 1.0*hinv; d[(D_HIDEAL + 4)*n] = 0.0*hinv; d[(D_HIDEAL + 5)*n] = 1.0*hinv;
+  const double* dv = &DvDx.xx;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    d[(D_DVDX + c)*n] = dv[c];
+    d[(D_LDVDX + c)*n] = dv[c];
+  }
+  d[D_WNS*n] = wns;
+  d[(D_M2 + 0)*n] = m2.xx; d[(D_M2 + 1)*n] = m2.xy; d[(D_M2 + 2)*n] = m2.xz;
+  d[(D_M2 + 3)*n] = m2.yy; d[(D_M2 + 4)*n] = m2.yz; d[(D_M2 + 5)*n] = m2.zz;
+  d[(D_XSPHDV + 0)*n] = XSPHdv.x; d[(D_XSPHDV + 1)*n] = XSPHdv.y; d[(D_XSPHDV + 2)*n] = XSPHdv.z;
+  d[D_MAXVP*n] = maxvp;
+  d[D_EFFVP*n] = effvp;
+  d[D_VISCW*n] = viscW;
+  K[(K_GRADRHO + 0)*n + i] = gradRho.x;
+  K[(K_GRADRHO + 1)*n + i] = gradRho.y;
+  K[(K_GRADRHO + 2)*n + i] = gradRho.z;
+}
+
+}  // namespace
+
+int crk_prepare(Problem& p) {
+  if (p.K == nullptr) {
+    if (cudaMalloc(&p.K, sizeof(double)*NCRK*(size_t)p.n) != cudaSuccess) {
+      set_error("CRKSPH field allocation failed");
+      return SPHGPU_ERR_NOMEM;
+    }
+    cudaMemsetAsync(p.K, 0, sizeof(double)*NCRK*(size_t)p.n, p.stream);
+  }
+  if (p.candcap > p.creccap) {
+    cudaFree(p.crec);
+    p.crec = nullptr;
+    if (cudaMalloc(&p.crec, sizeof(double)*CRECW*(size_t)p.candcap) != cudaSuccess) {
+      set_error("CRKSPH record allocation failed");
+      return SPHGPU_ERR_NOMEM;
+    }
+    p.creccap = p.candcap;
+  }
+  return SPHGPU_OK;
+}
+
+void launch_crk_sum_volume(Problem& p) {
+  crk_sum_volume_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr, p.S);
+  ++p.launches;
+}
+
+void launch_crk_volume_from_density(Problem& p) {
+  crk_volume_from_density_kernel<<<nblk(p.n, 256), 256, 0, p.stream>>>(p.n, p.S);
+  ++p.launches;
+}
+
+void launch_crk_sum_density(Problem& p) {
+  crk_sum_density_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr, p.groot, p.S);
+  ++p.launches;
+}
+
+void launch_crk_initialize(Problem& p) {
+  crk_moments_corrections_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr,
+                                                                       p.groot, p.S, p.K);
+  ++p.launches;
+}
+
+void launch_crk_eval(Problem& p) {
+  const int64_t ntot = p.n + p.G;
+  int blocks = nblk(ntot, 256);
+  if (blocks > 148*64) blocks = 148*64;
+  pack_crk_records_kernel<<<blocks, 256, 0, p.stream>>>(p.S, p.K, p.n, p.groot, p.gcode, ntot, p.prm.bcs, p.crec);
+  ++p.launches;
+  const int nb = nblk(p.n, 128);
+  const bool xsph = p.prm.XSPH != 0, comp = p.prm.compatible != 0;
+  if (xsph) {
+    if (comp) crk_eval_kernel<true, true><<<nb, 128, 0, p.stream>>>(p.prm, p.crec, p.n, p.offsets, p.nbr, p.D, p.K, p.pacc, p.ecap);
+    else crk_eval_kernel<true, false><<<nb, 128, 0, p.stream>>>(p.prm, p.crec, p.n, p.offsets, p.nbr, p.D, p.K, p.pacc, p.ecap);
+  } else {
+    if (comp) crk_eval_kernel<false, true><<<nb, 128, 0, p.stream>>>(p.prm, p.crec, p.n, p.offsets, p.nbr, p.D, p.K, p.pacc, p.ecap);
+    else crk_eval_kernel<false, false><<<nb, 128, 0, p.stream>>>(p.prm, p.crec, p.n, p.offsets, p.nbr, p.D, p.K, p.pacc, p.ecap);
+  }
+  ++p.launches;
+}
+
+}  // namespace sphgpu

@@ -13,10 +13,12 @@
 // Kernels and their bounds (see the roofline notes in the design document):
 //   ghost_hmax / ghost_flag / ghost_scatter  O(N+G) streaming, HBM bound
 //   node_bounds / cell_index / cell_scatter  O(N+G) streaming + atomics
-//   nbr_walk<COUNT|FILL>                     warp per node over the 27
-//                                            neighbouring cells; candidates
-//                                            read coalesced from the
-//                                            cell-sorted SoA copy (L2 resident)
+//   nbr_thread<COUNT|FILL>                   thread per node (cell-sorted
+//                                            order) over the 27 neighbouring
+//                                            cells; 80-byte candidate records
+//                                            shared by a warp through L1
+//   nbr_walk<COUNT|FILL>                     warp per node, for large
+//                                            candidate sets
 #include <cstdio>
 #include <climits>
 
@@ -29,10 +31,6 @@ namespace {
 __device__ __forceinline__ unsigned long long orderedBits(double v) {
   const unsigned long long b = (unsigned long long)__double_as_longlong(v);
   return (b & 0x8000000000000000ULL) ? ~b : (b | 0x8000000000000000ULL);
-}
-__device__ __forceinline__ double fromOrderedBits(unsigned long long b) {
-  const unsigned long long r = (b & 0x8000000000000000ULL) ? (b & 0x7fffffffffffffffULL) : ~b;
-  return __longlong_as_double((long long)r);
 }
 
 __device__ __forceinline__ V3 nodePos(const double* S, int64_t n, const double* gpos, int64_t gcap, int64_t k) {
@@ -148,31 +146,142 @@ __global__ void cell_index_kernel(const double* S, int64_t n, const double* gpos
   }
 }
 
+// Candidate record of the cell-sorted node list: position, H and the node
+// index, 80 bytes, read as five 16-byte loads.
+struct __align__(16) NbrCand {
+  double x, y, z;
+  double hxx, hxy, hxz, hyy, hyz, hzz;
+  int32_t idx, pad;
+};
+static_assert(sizeof(NbrCand) == 80, "candidate record is five 16-byte words");
+
+__device__ __forceinline__ NbrCand loadCand(const NbrCand* c) {
+  const double2* q = reinterpret_cast<const double2*>(c);
+  const double2 a = __ldg(q), b = __ldg(q + 1), d = __ldg(q + 2), e = __ldg(q + 3), f = __ldg(q + 4);
+  NbrCand r;
+  r.x = a.x; r.y = a.y; r.z = b.x; r.hxx = b.y; r.hxy = d.x; r.hxz = d.y; r.hyy = e.x; r.hyz = e.y; r.hzz = f.x;
+  r.idx = __double_as_longlong(f.y) & 0xffffffff;
+  r.pad = 0;
+  return r;
+}
+
 __global__ void cell_scatter_kernel(const double* S, int64_t n, const double* gpos, int64_t gcap,
                                     const int32_t* groot, int64_t ntot, const int32_t* cidx,
                                     const int64_t* cellStart, int32_t* cellFill, int32_t* sortedIdx,
-                                    double* cand, int64_t candcap) {
+                                    NbrCand* cand) {
   for (int64_t k = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; k < ntot; k += (int64_t)gridDim.x*blockDim.x) {
     const int c = cidx[k];
     const int64_t slot = cellStart[c] + atomicAdd(cellFill + c, 1);
     sortedIdx[slot] = (int32_t)k;
     const V3 r = nodePos(S, n, gpos, gcap, k);
     const Sym H = nodeH(S, n, groot, k);
-    cand[0*candcap + slot] = r.x; cand[1*candcap + slot] = r.y; cand[2*candcap + slot] = r.z;
-    cand[3*candcap + slot] = H.xx; cand[4*candcap + slot] = H.xy; cand[5*candcap + slot] = H.xz;
-    cand[6*candcap + slot] = H.yy; cand[7*candcap + slot] = H.yz; cand[8*candcap + slot] = H.zz;
+    double2* q = reinterpret_cast<double2*>(cand + slot);
+    q[0] = make_double2(r.x, r.y);
+    q[1] = make_double2(r.z, H.xx);
+    q[2] = make_double2(H.xy, H.xz);
+    q[3] = make_double2(H.yy, H.yz);
+    q[4] = make_double2(H.zz, __longlong_as_double((long long)(uint32_t)k));
+  }
+}
+
+// Thread per internal node, nodes taken in cell-sorted order so that the
+// threads of a warp share their candidate rows (L1 broadcast).  The 27
+// neighbouring cells are walked as 9 x-rows (three cells each, contiguous in
+// the sorted order) and the exact ConnectivityMap predicate is applied.
+// COUNT pass: per-node counts and their maximum.  FILL pass: the neighbor
+// indices are insertion-sorted into a per-thread shared-memory list of
+// capacity `cap` (element c of thread t at lst[c*blockDim + t], conflict
+// free) and stored ascending at offsets[i].
+template<bool FILL>
+__global__ void __launch_bounds__(256) nbr_thread_kernel(int64_t n, int64_t ntot, Grid g, const int64_t* cellStart,
+                                                         const NbrCand* cand, double kernelExtent2, int32_t* counts,
+                                                         const int64_t* offsets, int32_t* nbr, int cap,
+                                                         int* maxCount, int* err,
+                                                         unsigned long long* pairCount) {
+  extern __shared__ int32_t lst[];
+  const int tid = threadIdx.x;
+  const int bd = blockDim.x;
+  const int64_t s = blockIdx.x*(int64_t)bd + tid;
+  NbrCand me;
+  bool active = s < ntot;
+  if (active) {
+    me = loadCand(cand + s);
+    active = me.idx < n;
+  }
+  int count = 0, above = 0;
+  if (active) {
+    const int32_t i = me.idx;
+    const V3 ri{me.x, me.y, me.z};
+    const Sym Hi{me.hxx, me.hxy, me.hxz, me.hyy, me.hyz, me.hzz};
+    const int cx = cellCoord(ri.x, g.lo[0], g.cell, g.dim[0]);
+    const int cy = cellCoord(ri.y, g.lo[1], g.cell, g.dim[1]);
+    const int cz = cellCoord(ri.z, g.lo[2], g.cell, g.dim[2]);
+    const int x0 = cx > 0 ? cx - 1 : 0;
+    const int x1 = cx + 1 < g.dim[0] ? cx + 1 : g.dim[0] - 1;
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int z = cz + dz;
+      if (z < 0 || z >= g.dim[2]) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int y = cy + dy;
+        if (y < 0 || y >= g.dim[1]) continue;
+        const int cbase = (z*g.dim[1] + y)*g.dim[0];
+        const int64_t start = cellStart[cbase + x0];
+        const int64_t end = cellStart[cbase + x1 + 1];
+        for (int64_t k = start; k < end; ++k) {
+          const NbrCand c = loadCand(cand + k);
+          const V3 rij = vsub(ri, V3{c.x, c.y, c.z});
+          const double eta2i = mag2(sdot(Hi, rij));
+          const double eta2j = mag2(sdot(Sym{c.hxx, c.hxy, c.hxz, c.hyy, c.hyz, c.hzz}, rij));
+          if ((eta2i <= kernelExtent2 || eta2j <= kernelExtent2) && c.idx != i) {
+            if (FILL) {
+              if (count < cap) {
+                int p = count;
+                while (p > 0) {
+                  const int32_t prev = lst[(p - 1)*bd + tid];
+                  if (prev < c.idx) break;
+                  lst[p*bd + tid] = prev;
+                  --p;
+                }
+                lst[p*bd + tid] = c.idx;
+              }
+              above += (c.idx > i);
+            }
+            ++count;
+          }
+        }
+      }
+    }
+    if (!FILL) {
+      counts[i] = count;
+    } else if (count <= cap) {
+      const int64_t o = offsets[i];
+      for (int c = 0; c < count; ++c) nbr[o + c] = lst[c*bd + tid];
+    } else {
+      atomicOr(err, DERR_NBR_CAPACITY);
+    }
+  }
+  if (!FILL) {
+    int m = count;
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((tid & 31) == 0 && m > 0) atomicMax(maxCount, m);
+  } else {
+    unsigned long long a = (unsigned long long)above;
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if ((tid & 31) == 0 && a) atomicAdd(pairCount, a);
   }
 }
 
 // Warp per internal node: walk the 27 neighbouring cells, apply the exact
 // ConnectivityMap predicate, count (FILL=false) or collect, sort ascending
-// and store (FILL=true) the neighbor indices.
+// and store (FILL=true) the neighbor indices.  Used when the candidate sets
+// are large (many nodes per cell), where a warp per node keeps the SMs full.
 template<bool FILL>
 __global__ void __launch_bounds__(256) nbr_walk_kernel(const double* S, int64_t n, Grid g,
-                                                       const int64_t* cellStart, const int32_t* sortedIdx,
-                                                       const double* cand, int64_t candcap, double kernelExtent2,
+                                                       const int64_t* cellStart, const NbrCand* cand,
+                                                       double kernelExtent2,
                                                        int32_t* counts, const int64_t* offsets, int32_t* nbr,
-                                                       int maxNbr, int* err, unsigned long long* pairCount) {
+                                                       int maxNbr, int* err, int* maxCount,
+                                                       unsigned long long* pairCount) {
   extern __shared__ int32_t sbuf_all[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -203,10 +312,10 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const double* S, int64_t 
         bool pass = false;
         int32_t j = -1;
         if (k < end) {
-          j = sortedIdx[k];
-          const V3 rj{cand[k], cand[candcap + k], cand[2*candcap + k]};
-          const Sym Hj{cand[3*candcap + k], cand[4*candcap + k], cand[5*candcap + k],
-                       cand[6*candcap + k], cand[7*candcap + k], cand[8*candcap + k]};
+          const NbrCand c = loadCand(cand + k);
+          j = c.idx;
+          const V3 rj{c.x, c.y, c.z};
+          const Sym Hj{c.hxx, c.hxy, c.hxz, c.hyy, c.hyz, c.hzz};
           const V3 rij = vsub(ri, rj);
           const double eta2i = mag2(sdot(Hi, rij));
           const double eta2j = mag2(sdot(Hj, rij));
@@ -225,6 +334,7 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const double* S, int64_t 
     if (lane == 0) {
       counts[i] = count;
       if (count > maxNbr) atomicOr(err, DERR_NBR_CAPACITY);
+      atomicMax(maxCount, count);
     }
     return;
   }
@@ -352,24 +462,41 @@ int build_cells_and_csr(Problem& p) {
   int rc = exclusive_scan_i32(p, p.cellFill, ncells, cellStart, &tot);
   if (rc) return rc;
   cudaMemsetAsync(p.cellFill, 0, sizeof(int32_t)*ncells, st);
+  NbrCand* cand = reinterpret_cast<NbrCand*>(p.cand);
   cell_scatter_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, p.groot, ntot, p.cidx,
-                                                           cellStart, p.cellFill, p.sortedIdx, p.cand, p.candcap); ++p.launches;
+                                                           cellStart, p.cellFill, p.sortedIdx, cand); ++p.launches;
   // ---- neighbor counts, offsets, fill
   const double k2 = p.prm.kernelExtent*p.prm.kernelExtent;
-  const int threads = 256;
-  const int64_t warps = p.n;
-  const int64_t blocks = (warps*32 + threads - 1)/threads;
-  nbr_walk_kernel<false><<<(unsigned)blocks, threads, 0, st>>>(p.S, p.n, g, cellStart, p.sortedIdx, p.cand,
-                                                                 p.candcap, k2, p.counts, nullptr, nullptr,
-                                                                 p.maxNbr, p.d_err, nullptr); ++p.launches;
+  // Schedule: a thread per node while the 27-cell candidate set is small, a
+  // warp per node once it is large enough to keep 32 lanes busy.
+  const double candPerNode = 27.0*(double)ntot/(double)ncells;
+  const bool warpSchedule = p.nbrSchedule == NBR_SCHEDULE_WARP ||
+                            (p.nbrSchedule == NBR_SCHEDULE_AUTO && candPerNode > 384.0);
+  p.lastNbrSchedule = warpSchedule ? NBR_SCHEDULE_WARP : NBR_SCHEDULE_THREAD;
+  int* dMaxCount = reinterpret_cast<int*>(p.d_scal + 10);
+  cudaMemsetAsync(dMaxCount, 0, sizeof(int), st);
+  const int wthreads = 256;
+  const int64_t wblocks = (p.n*32 + wthreads - 1)/wthreads;
+  const int tthreads = 256;
+  const int64_t tblocks = (ntot + tthreads - 1)/tthreads;
+  if (warpSchedule) {
+    nbr_walk_kernel<false><<<(unsigned)wblocks, wthreads, 0, st>>>(p.S, p.n, g, cellStart, cand, k2, p.counts,
+                                                                     nullptr, nullptr, p.maxNbr, p.d_err,
+                                                                     dMaxCount, nullptr); ++p.launches;
+  } else {
+    nbr_thread_kernel<false><<<(unsigned)tblocks, tthreads, 0, st>>>(p.n, ntot, g, cellStart, cand, k2, p.counts,
+                                                                       nullptr, nullptr, 0, dMaxCount, p.d_err,
+                                                                       nullptr); ++p.launches;
+  }
   int64_t E = 0;
   rc = exclusive_scan_i32(p, p.counts, p.n, p.offsets, &E);
   if (rc) return rc;
-  int herr = 0;
+  int herr = 0, maxCount = 0;
   cudaMemcpyAsync(&herr, p.d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&maxCount, dMaxCount, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_status(cudaGetLastError(), "nbr count");
   if (herr & (DERR_NBR_CAPACITY | DERR_GHOST_CHAIN)) cudaMemsetAsync(p.d_err, 0, sizeof(int), st);
-  if (herr & DERR_NBR_CAPACITY) {
+  if ((herr & DERR_NBR_CAPACITY) || maxCount > p.maxNbr) {
     set_error("a node has more neighbors than max_neighbors");
     return SPHGPU_ERR_CAPACITY;
   }
@@ -377,19 +504,41 @@ int build_cells_and_csr(Problem& p) {
     set_error("a ghost image was imaged twice through one periodic axis");
     return SPHGPU_ERR_UNSUPPORTED;
   }
+  p.maxCount = maxCount;
   rc = ensure_capacity_entries(p, E);
   if (rc) return rc;
   unsigned long long* pc = reinterpret_cast<unsigned long long*>(p.d_scal + 8);
   cudaMemsetAsync(pc, 0, sizeof(unsigned long long), st);
-  const size_t smem = sizeof(int32_t)*(threads/32)*(size_t)p.maxNbr;
-  if (smem > 48*1024) {
-    const cudaError_t e = cudaFuncSetAttribute(nbr_walk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)smem);
-    if (e != cudaSuccess) return cuda_status(e, "nbr smem attribute");
+  // per-thread list capacity: shrink the block until the lists fit
+  int fthreads = tthreads;
+  const int tcap = maxCount > 0 ? maxCount : 1;
+  while (fthreads > 32 && sizeof(int32_t)*(size_t)fthreads*tcap > 96*1024) fthreads >>= 1;
+  const bool threadFill = !warpSchedule && sizeof(int32_t)*(size_t)fthreads*tcap <= 200*1024;
+  if (threadFill) {
+    const size_t smem = sizeof(int32_t)*(size_t)fthreads*tcap;
+    if (smem > 48*1024) {
+      const cudaError_t e = cudaFuncSetAttribute(nbr_thread_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+      if (e != cudaSuccess) return cuda_status(e, "nbr smem attribute");
+    }
+    const int64_t fblocks = (ntot + fthreads - 1)/fthreads;
+    nbr_thread_kernel<true><<<(unsigned)fblocks, fthreads, smem, st>>>(p.n, ntot, g, cellStart, cand, k2, p.counts,
+                                                                         p.offsets, p.nbr, tcap, nullptr, p.d_err,
+                                                                         pc); ++p.launches;
+  } else {
+    // bitonic sort pads each warp's list to a power of two >= 32
+    int wcap = 32;
+    while (wcap < maxCount) wcap <<= 1;
+    const size_t smem = sizeof(int32_t)*(wthreads/32)*(size_t)wcap;
+    if (smem > 48*1024) {
+      const cudaError_t e = cudaFuncSetAttribute(nbr_walk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+      if (e != cudaSuccess) return cuda_status(e, "nbr smem attribute");
+    }
+    nbr_walk_kernel<true><<<(unsigned)wblocks, wthreads, smem, st>>>(p.S, p.n, g, cellStart, cand, k2, p.counts,
+                                                                       p.offsets, p.nbr, wcap, p.d_err, nullptr,
+                                                                       pc); ++p.launches;
   }
-  nbr_walk_kernel<true><<<(unsigned)blocks, threads, smem, st>>>(p.S, p.n, g, cellStart, p.sortedIdx, p.cand,
-                                                                   p.candcap, k2, p.counts, p.offsets, p.nbr,
-                                                                   p.maxNbr, p.d_err, pc); ++p.launches;
   unsigned long long pairs = 0;
   cudaMemcpyAsync(&pairs, pc, sizeof(pairs), cudaMemcpyDeviceToHost, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_status(cudaGetLastError(), "nbr fill");

@@ -28,7 +28,35 @@ namespace sphgpu {
 enum StateField {
   S_X = 0, S_Y, S_Z, S_VX, S_VY, S_VZ, S_M, S_RHO, S_EPS, S_P, S_CS, S_OMEGA,
   S_H = 12,            // 6 components xx,xy,xz,yy,yz,zz
-  NSTATE = 18
+  S_VOL = 18,          // CRKSPH "node volume"
+  NSTATE = 19
+};
+
+// CRKSPH corrections and moments of the internal nodes, SoA [NCRK][n].
+enum CrkField {
+  K_A = 0,             // 1  "A CRKSPH correction"
+  K_B = 1,             // 3  "B CRKSPH correction"
+  K_GRADA = 4,         // 3  "grad A CRKSPH correction"
+  K_GRADB = 7,         // 9  "grad B CRKSPH correction" (row major)
+  K_M0 = 16,           // 1  "m0 CRKSPH moment"
+  K_M1 = 17,           // 3  "m1 CRKSPH moment"
+  K_M2 = 20,           // 6  "m2 CRKSPH moment"
+  K_GRADM0 = 26,       // 3  "grad m0 CRKSPH moment"
+  K_GRADM1 = 29,       // 9  "grad m1 CRKSPH moment"
+  K_GRADM2 = 38,       // 27 "grad m2 CRKSPH moment" (i*9 + j*3 + k)
+  K_GRADRHO = 65,      // 3  "mass density gradient"
+  NCRK = 68
+};
+
+// CRKSPH pair record: the SPH record fields plus volume and corrections.
+enum CrkRecField {
+  C_X = 0, C_Y, C_Z, C_VX, C_VY, C_VZ, C_M, C_RHO, C_CS, C_P, C_HDET, C_VOL,
+  C_H = 12,            // 6
+  C_A = 18,
+  C_B = 19,            // 3
+  C_GRADA = 22,        // 3
+  C_GRADB = 25,        // 9
+  CRECW = 34           // 272 bytes
 };
 
 enum DerivField {
@@ -77,6 +105,7 @@ struct Params {
   double kernelExtent;
   int compatible, XSPH, correctVelGrad, linearInExp, quadInExp, useVelMagDt;
   int HUpdate, densityUpdate, gradh;
+  int hydro;               // SPHGPU_HYDRO_*
   BoxBCs bcs;
 };
 
@@ -91,10 +120,17 @@ struct Problem {
   int64_t E = 0, ecap = 0;  // CSR entries
   int64_t pairs = 0;        // unordered pairs (ncalc)
   int maxNbr = 1024;
+  int maxCount = 0;         // largest neighbor count of the current connectivity
+  int nbrSchedule = 0;      // NBR_SCHEDULE_* requested for the neighbor walk
+  int lastNbrSchedule = 0;  // schedule the last build used
 
   double* S = nullptr;
   double* S0 = nullptr;
   double* D = nullptr;
+  double* K = nullptr;          // [NCRK][n] CRKSPH fields (CRKSPH problems only)
+  double* crec = nullptr;       // [n+G][CRECW] CRKSPH pair records
+  int64_t creccap = 0;
+  bool crkVolumeReady = false;
   double* rec = nullptr;
   int64_t reccap = 0;
 
@@ -103,7 +139,7 @@ struct Problem {
   double* gpos = nullptr;   // [3][gcap] ghost positions during creation
 
   // cell list
-  double* cand = nullptr;       // [9][candcap] sorted x,y,z,H6
+  double* cand = nullptr;       // [candcap] 80-byte records x,y,z,H6,index (cell order)
   int32_t* cidx = nullptr;      // [candcap] cell index of each node (unsorted)
   int32_t* sortedIdx = nullptr; // [candcap]
   int64_t candcap = 0;
@@ -154,6 +190,13 @@ enum DevError {
   DERR_NONPOSITIVE = 8,
 };
 
+// Neighbor-walk schedules (values of sphgpu_set_schedule's "neighbor walk").
+enum NbrSchedule {
+  NBR_SCHEDULE_AUTO = 0,     // thread per node for small candidate sets, else warp
+  NBR_SCHEDULE_THREAD = 1,   // thread per node, cell-sorted order
+  NBR_SCHEDULE_WARP = 2,     // warp per node
+};
+
 // ---- launchers (ghosts/neighbors: nbrs.cu; physics: sph.cu) ----
 int build_ghosts(Problem& p);
 int build_cells_and_csr(Problem& p);
@@ -170,6 +213,13 @@ void launch_dt(Problem& p, double* d_out);
 void launch_select_dt(Problem& p, double* d_dt, double* d_lastDt);
 void launch_conservation(Problem& p, double* d_out8);
 void launch_zero_derivs(Problem& p);
+// CRKSPH (crk.cu)
+int crk_prepare(Problem& p);
+void launch_crk_sum_volume(Problem& p);
+void launch_crk_volume_from_density(Problem& p);
+void launch_crk_sum_density(Problem& p);
+void launch_crk_initialize(Problem& p);
+void launch_crk_eval(Problem& p);
 
 // device buffer helpers (api.cu)
 int ensure_capacity_ghosts(Problem& p, int64_t gcap);

@@ -195,9 +195,11 @@ __global__ void __launch_bounds__(128) sph_eval_fp64_kernel(Params P, const doub
     const double workQi = own ? workQA : workQB;
     DepsDt += (own ? mB : mA)*(Prhoi*dot(vij, gradWi) + workQi);
     if (COMPAT) {
-      pacc[k] = deltaDvDt.x;
-      pacc[ecap + k] = deltaDvDt.y;
-      pacc[2*ecap + k] = deltaDvDt.z;
+      // the owner's pair acceleration, -m_other*deltaDvDt
+      const V3 pa = vmul(deltaDvDt, -mB);
+      pacc[k] = pa.x;
+      pacc[ecap + k] = pa.y;
+      pacc[2*ecap + k] = pa.z;
     }
     const double mo = own ? mB : mA;      // the other node's mass
     tsubfrom(DvDx, tmul(dyad(vij, gradWi), mo));
@@ -363,15 +365,13 @@ __global__ void compatible_energy_kernel(int64_t n, const int64_t* offsets, cons
     const V3 vj{ldg(S + S_VX*n + r), ldg(S + S_VY*n + r), ldg(S + S_VZ*n + r)};
     const V3 aj{ldg(D + (D_DVDT + 0)*n + r), ldg(D + (D_DVDT + 1)*n + r), ldg(D + (D_DVDT + 2)*n + r)};
     const V3 vj12 = vadd(vj, vmul(aj, hdt));
-    const V3 dd{ldg(pacc + k), ldg(pacc + ecap + k), ldg(pacc + 2*ecap + k)};
+    const V3 pa{ldg(pacc + k), ldg(pacc + ecap + k), ldg(pacc + 2*ecap + k)};   // owner's pair acceleration
     if (j > (int32_t)i) {
-      const V3 pai = vmul(dd, -mj);
-      const double duij = dot(vsub(vj12, vi12), pai);
+      const double duij = dot(vsub(vj12, vi12), pa);
       const double wi = weighti/(weighti + weightj);
       DepsDti += wi*duij;
     } else {
-      const V3 paj = vmul(dd, -mi);                 // owner j's pair acceleration
-      const double duji = dot(vsub(vi12, vj12), paj);
+      const double duji = dot(vsub(vi12, vj12), pa);
       const double wj = weightj/(weightj + weighti);
       DepsDti += (1.0 - wj)*duji*mj/mi;
     }
@@ -410,6 +410,14 @@ __global__ void update_kernel(Params P, int64_t n, double* S, const double* D, c
   S[S_RHO*n + i] = rho;
   // position: IncrementFieldList
   for (int c = 0; c < 3; ++c) S[(S_X + c)*n + i] = S[(S_X + c)*n + i] + D[(D_DXDT + c)*n + i]*mult;
+  // CRKSPH node volume: ContinuityVolumePolicy (after mass density and H)
+  if (P.hydro == SPHGPU_HYDRO_CRKSPH) {
+    const double m = S[S_M*n + i];
+    const double volMin = 0.5*m*safeInvVar(rho);
+    const double volMax = 4.0*3.14159265358979323846/(3.0*sdet(Hn));
+    const double dVdt = -m*safeInvVar(rho*rho)*D[D_DRHODT*n + i];
+    S[S_VOL*n + i] = dmax(volMin, dmin(volMax, S[S_VOL*n + i] + mult*dVdt));
+  }
   // specific thermal energy: IncrementFieldList (or the compatible policy, already applied)
   double eps = S[S_EPS*n + i];
   if (!epsDone) {

@@ -191,10 +191,12 @@ __global__ void __launch_bounds__(128) sph_eval_mixed_kernel(Params P, const flo
     DvDt[0].add(-J.m*dd.x); DvDt[1].add(-J.m*dd.y); DvDt[2].add(-J.m*dd.z);
     DepsDt.add(J.m*(Prhoi*(vij.x*gradWi.x + vij.y*gradWi.y + vij.z*gradWi.z) + workQi));
     if (COMPAT) {
-      const double sgnO = j > (int32_t)i ? 1.0 : -1.0;   // owner orientation
-      pacc[k] = sgnO*(double)dd.x;
-      pacc[ecap + k] = sgnO*(double)dd.y;
-      pacc[2*ecap + k] = sgnO*(double)dd.z;
+      // the owner's pair acceleration: -m_other*deltaDvDt in owner orientation
+      const bool own = j > (int32_t)i;
+      const double s = own ? -(double)J.m : (double)I.m;
+      pacc[k] = s*(double)dd.x;
+      pacc[ecap + k] = s*(double)dd.y;
+      pacc[2*ecap + k] = s*(double)dd.z;
     }
     const float mj = J.m;
     const F3 mg{mj*gradWi.x, mj*gradWi.y, mj*gradWi.z};

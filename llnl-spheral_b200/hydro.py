@@ -25,6 +25,10 @@ FIELD_COMPONENTS = {
     "M SPH gradient correction": 9, "local M SPH gradient correction": 9, "delta H": 6, "new H": 6,
     "max viscous pressure": 1, "effective viscous pressure": 1, "viscous work rate": 1,
     "XSPH weight sum": 1, "XSPH delta vi": 3, "weighted neighbor sum": 1, "mass second moment": 6,
+    "node volume": 1, "A CRKSPH correction": 1, "B CRKSPH correction": 3, "grad A CRKSPH correction": 3,
+    "grad B CRKSPH correction": 9, "m0 CRKSPH moment": 1, "m1 CRKSPH moment": 3, "m2 CRKSPH moment": 6,
+    "grad m0 CRKSPH moment": 3, "grad m1 CRKSPH moment": 9, "grad m2 CRKSPH moment": 27,
+    "mass density gradient": 3,
 }
 
 
@@ -129,6 +133,19 @@ class SPHHydro:
         out = np.empty(8)
         abi.check(self.lib.sphgpu_conservation(self.h, _p(out)), self.lib)
         return out
+
+    def kernel_launches(self):
+        v = ctypes.c_int64()
+        abi.check(self.lib.sphgpu_kernel_launches(self.h, ctypes.byref(v)), self.lib)
+        return v.value
+
+    def set_schedule(self, stage, schedule):
+        abi.check(self.lib.sphgpu_set_schedule(self.h, stage.encode(), int(schedule)), self.lib)
+
+    def schedule(self, stage):
+        v = ctypes.c_int32()
+        abi.check(self.lib.sphgpu_get_schedule(self.h, stage.encode(), ctypes.byref(v)), self.lib)
+        return v.value
 
     def synchronize(self):
         abi.check(self.lib.sphgpu_synchronize(self.h), self.lib)

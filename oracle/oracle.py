@@ -70,6 +70,10 @@ FIELD_COMPONENTS = {
     "M SPH gradient correction": 9, "local M SPH gradient correction": 9, "delta H": 6, "new H": 6,
     "max viscous pressure": 1, "effective viscous pressure": 1, "viscous work rate": 1,
     "XSPH weight sum": 1, "XSPH delta vi": 3, "weighted neighbor sum": 1, "mass second moment": 6,
+    "node volume": 1, "A CRKSPH correction": 1, "B CRKSPH correction": 3, "grad A CRKSPH correction": 3,
+    "grad B CRKSPH correction": 9, "m0 CRKSPH moment": 1, "m1 CRKSPH moment": 3, "m2 CRKSPH moment": 6,
+    "grad m0 CRKSPH moment": 3, "grad m1 CRKSPH moment": 9, "grad m2 CRKSPH moment": 27,
+    "mass density gradient": 3,
 }
 
 

@@ -38,6 +38,7 @@
 #include <cstdint>
 #include <cstring>
 #include <algorithm>
+#include <array>
 #include <string>
 #include <vector>
 
@@ -74,8 +75,15 @@ struct Problem {
   std::vector<T9> DvDx, localDvDx, M, localM;
   std::vector<Sym> DHDt, Hideal, m2;
   std::vector<std::vector<V3>> pairAcc;
+  // CRKSPH (linear order): volume, corrections and their moments (all nodes).
+  std::vector<double> vol, A, m0;
+  std::vector<V3> B, gradA, m1, gradm0, gradRho;
+  std::vector<T9> gradB, gradm1;
+  std::vector<Sym> cm2;                      // CRK second moment (m2 above is the ideal-H one)
+  std::vector<std::array<double, 27>> gradm2;
   double time = 0.0, lastDt = 1e-5;
   int cycle = 0;
+  bool crkVolumeReady = false;
   std::string err;
 };
 
@@ -675,6 +683,376 @@ bool stepRK2(Problem& p, double& dtOut) {
   return true;
 }
 
+// ====================================================================== CRKSPH
+//   moments      computeCRKSPHMoments src/CRKSPH/computeCRKSPHMoments.cc:40-287 (LinearOrder,
+//                NodeCoupling = 1)
+//   corrections  computeLinearCRKSPHCorrections src/CRKSPH/computeCRKSPHCorrections.cc:210-283
+//   kernel       CRKSPHKernelAndGradient src/CRKSPH/CRKSPHUtilitiesInline.hh:58-129
+//   derivatives  CRKSPHHydroBase::evaluateDerivatives src/CRKSPH/CRKSPHHydroBase.cc:646-1102
+//   volume       computeCRKSPHSumVolume src/CRKSPH/computeCRKSPHSumVolume.cc:43-127,
+//                ContinuityVolumePolicy::update src/CRKSPH/ContinuityVolumePolicy.cc:67-95
+//   density      computeCRKSPHSumMassDensity src/CRKSPH/computeCRKSPHSumMassDensity.cc:28-139
+
+inline double& el(V3& v, int i) { return (&v.x)[i]; }
+inline double el(const V3& v, int i) { return (&v.x)[i]; }
+inline double& el(T9& t, int i, int j) { return (&t.xx)[3*i + j]; }
+inline double el(const T9& t, int i, int j) { return (&t.xx)[3*i + j]; }
+inline double& sel(Sym& s, int i, int j) {
+  static const int map[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+  return (&s.xx)[map[i][j]];
+}
+inline double sel(const Sym& s, int i, int j) {
+  static const int map[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+  return (&s.xx)[map[i][j]];
+}
+
+template<typename T>
+void ghostCopy(Problem& p, std::vector<T>& f) {
+  for (size_t b = 0; b < p.bcs.size(); ++b)
+    for (size_t k = 0; k < p.control[b].size(); ++k) f[p.ghosts[b][k]] = f[p.control[b][k]];
+}
+
+void crkResize(Problem& p) {
+  const int n = numNodes(p);
+  p.vol.resize(n, 0.0); p.A.resize(n, 0.0); p.B.resize(n, V3{0, 0, 0});
+  p.gradA.resize(n, V3{0, 0, 0}); p.gradB.resize(n, tzero());
+}
+
+void crkSumVolume(Problem& p) {
+  const int n = numNodes(p);
+  const double etaVolMax = (0.5*p.W.extent)*(0.5*p.W.extent)*(0.5*p.W.extent)*(4.0/3.0*M_PI);
+  p.vol.assign(n, 0.0);
+  for (int i = 0; i < p.nInt; ++i) {
+    const V3& ri = p.pos[i];
+    const Sym& Hi = p.H[i];
+    const double Hdeti = sdet(Hi);
+    for (int j : p.conn[i]) {
+      if (!calcPair(i, j)) continue;
+      const Sym& Hj = p.H[j];
+      const double Hdetj = sdet(Hj);
+      const V3 rij = vsub(ri, p.pos[j]);
+      const double etai = mag(sdot(Hi, rij));
+      const double etaj = mag(sdot(Hj, rij));
+      p.vol[i] += p.W.kernelValue(etai, Hdeti);
+      p.vol[j] += p.W.kernelValue(etaj, Hdetj);
+    }
+    p.vol[i] += p.W.kernelValue(0.0, Hdeti);
+    p.vol[i] = std::min(etaVolMax/Hdeti, 1.0/p.vol[i]);
+  }
+  ghostCopy(p, p.vol);
+}
+
+void crkSumDensity(Problem& p) {
+  const int n = numNodes(p);
+  std::vector<double> wsum(n, 0.0), vol1(n, 0.0);
+  for (int i = 0; i < n; ++i) p.rho[i] = 0.0;
+  for (int i = 0; i < p.nInt; ++i) {
+    const V3& ri = p.pos[i];
+    const double mi = p.m[i], Vi = p.vol[i];
+    const Sym& Hi = p.H[i];
+    const double Hdeti = sdet(Hi);
+    for (int j : p.conn[i]) {
+      if (!calcPair(i, j)) continue;
+      const double mj = p.m[j], Vj = p.vol[j];
+      const Sym& Hj = p.H[j];
+      const double Hdetj = sdet(Hj);
+      const V3 rij = vsub(ri, p.pos[j]);
+      const double Wi = p.W.kernelValue(mag(sdot(Hi, rij)), Hdeti);
+      const double Wj = p.W.kernelValue(mag(sdot(Hj, rij)), Hdetj);
+      wsum[i] += Vj*Wj;
+      wsum[j] += Vi*Wi;
+      p.rho[i] += mj*Vj*Wj;
+      p.rho[j] += mi*Vi*Wi;
+      vol1[i] += Vj*Vj*Wj;
+      vol1[j] += Vi*Vi*Wi;
+    }
+    const double W0 = p.W.kernelValue(0.0, Hdeti);
+    wsum[i] += Vi*W0;
+    vol1[i] = (vol1[i] + Vi*Vi*W0)/wsum[i];
+    p.rho[i] = std::max(std::max(p.cfg.rhoMin, 0.1*mi*sdet(p.H[i])),
+                        std::min(p.cfg.rhoMax, (p.rho[i] + mi*Vi*W0)/(wsum[i]*vol1[i])));
+  }
+}
+
+void crkMoments(Problem& p) {
+  const int n = numNodes(p);
+  p.m0.assign(n, 0.0); p.m1.assign(n, V3{0, 0, 0}); p.cm2.assign(n, Sym{0, 0, 0, 0, 0, 0});
+  p.gradm0.assign(n, V3{0, 0, 0}); p.gradm1.assign(n, tzero());
+  std::array<double, 27> z{};
+  p.gradm2.assign(n, z);
+  const double fij = 1.0;
+  for (int i = 0; i < p.nInt; ++i) {
+    const double weighti = p.vol[i];
+    const V3& ri = p.pos[i];
+    const Sym& Hi = p.H[i];
+    const double Hdeti = sdet(Hi);
+    const double wwself = weighti*p.W.kernelValue(0.0, Hdeti);
+    p.m0[i] += wwself;
+    taddto(p.gradm1[i], tdiag(wwself));
+    for (int j : p.conn[i]) {
+      if (!calcPair(i, j)) continue;
+      const double weightj = p.vol[j];
+      const Sym& Hj = p.H[j];
+      const double Hdetj = sdet(Hj);
+      const double wi = weighti, wj = weightj;
+      const V3 rij = vsub(ri, p.pos[j]);
+      const V3 etai = sdot(Hi, rij);
+      const V3 etaj = sdot(Hj, rij);
+      const auto WWi = p.W.kernelAndGradValue(mag(etai), Hdeti);
+      const auto WWj = p.W.kernelAndGradValue(mag(etaj), Hdetj);
+      const double Wi = 0.5*(WWi.first + WWj.first);
+      const double Wj = Wi;
+      const V3 gradWj = vmul(vadd(vmul(sdot(Hj, unitVector(etaj)), WWj.second),
+                                  vmul(sdot(Hi, unitVector(etai)), WWi.second)), 0.5);
+      const V3 gradWi = vneg(gradWj);
+      const double wwi = wi*Wi, wwj = wj*Wj;
+      p.m0[i] += fij*wwj;
+      p.m0[j] += fij*wwi;
+      for (int ii = 0; ii < 3; ++ii) {
+        el(p.gradm0[i], ii) += fij*wj*el(gradWj, ii);
+        el(p.gradm0[j], ii) += fij*wi*el(gradWi, ii);
+      }
+      for (int ii = 0; ii < 3; ++ii) {
+        el(p.m1[i], ii) += fij*wwj*el(rij, ii);
+        el(p.m1[j], ii) -= fij*wwi*el(rij, ii);
+        for (int jj = 0; jj < 3; ++jj) {
+          el(p.gradm1[i], ii, jj) += fij*wj*el(rij, ii)*el(gradWj, jj);
+          el(p.gradm1[j], ii, jj) -= fij*wi*el(rij, ii)*el(gradWi, jj);
+        }
+        el(p.gradm1[i], ii, ii) += fij*wj*Wj;
+        el(p.gradm1[j], ii, ii) += fij*wi*Wi;
+      }
+      for (int ii = 0; ii < 3; ++ii) {
+        for (int jj = ii; jj < 3; ++jj) {
+          const double thpt = el(rij, ii)*el(rij, jj);
+          sel(p.cm2[i], ii, jj) += fij*wwj*thpt;
+          sel(p.cm2[j], ii, jj) += fij*wwi*thpt;
+        }
+        for (int jj = 0; jj < 3; ++jj) {
+          const double thpt = el(rij, ii)*el(rij, jj);
+          for (int kk = 0; kk < 3; ++kk) {
+            p.gradm2[i][9*ii + 3*jj + kk] += fij*wj*thpt*el(gradWj, kk);
+            p.gradm2[j][9*ii + 3*jj + kk] += fij*wi*thpt*el(gradWi, kk);
+          }
+          p.gradm2[i][9*ii + 3*jj + jj] += fij*wwj*el(rij, ii);
+          p.gradm2[i][9*jj + 3*ii + jj] += fij*wwj*el(rij, ii);
+          p.gradm2[j][9*ii + 3*jj + jj] -= fij*wwi*el(rij, ii);
+          p.gradm2[j][9*jj + 3*ii + jj] -= fij*wwi*el(rij, ii);
+        }
+      }
+    }
+  }
+}
+
+void crkCorrections(Problem& p) {
+  crkResize(p);
+  for (int i = 0; i < p.nInt; ++i) {
+    const V3& m1i = p.m1[i];
+    const Sym& m2i = p.cm2[i];
+    const double Hd = sdet(p.H[i]);
+    const double hdet2 = 1.0/(Hd*Hd);
+    const double m2det = sdet(m2i);
+    const Sym m2inv = std::abs(m2det) > 1.0e-5*hdet2 ? sinverse(m2i) : Sym{0, 0, 0, 0, 0, 0};
+    const V3 m2invm1 = sdot(m2inv, m1i);
+    const double Ainv = p.m0[i] - dot(m2invm1, m1i);
+    double& A = p.A[i];
+    A = 1.0/Ainv;
+    p.B[i] = vneg(m2invm1);
+    V3& gA = p.gradA[i];
+    gA = vmul(p.gradm0[i], -A*A);
+    T9& gB = p.gradB[i];
+    gB = tzero();
+    const T9& gm1 = p.gradm1[i];
+    const std::array<double, 27>& gm2 = p.gradm2[i];
+    for (int ii = 0; ii < 3; ++ii) {
+      for (int jj = 0; jj < 3; ++jj) {
+        for (int kk = 0; kk < 3; ++kk) {
+          el(gA, ii) += A*A*sel(m2inv, jj, kk)*el(m1i, kk)*el(gm1, jj, ii);
+          el(gA, ii) += A*A*sel(m2inv, jj, kk)*el(gm1, kk, ii)*el(m1i, jj);
+          el(gB, ii, jj) -= sel(m2inv, ii, kk)*el(gm1, kk, jj);
+          for (int ll = 0; ll < 3; ++ll) {
+            for (int mm = 0; mm < 3; ++mm) {
+              el(gA, ii) -= A*A*sel(m2inv, jj, kk)*gm2[9*kk + 3*ll + ii]*sel(m2inv, ll, mm)*el(m1i, mm)*el(m1i, jj);
+              el(gB, ii, jj) += sel(m2inv, ii, kk)*gm2[9*kk + 3*ll + jj]*sel(m2inv, ll, mm)*el(m1i, mm);
+            }
+          }
+        }
+      }
+    }
+  }
+  ghostCopy(p, p.A); ghostCopy(p, p.B); ghostCopy(p, p.gradA); ghostCopy(p, p.gradB);
+}
+
+// CRKSPHKernelAndGradient, LinearOrder, no correction limits in effect.
+void crkKernel(const TableKernel& W, const V3& rij, const V3& etai, const Sym& Hi, double Hdeti,
+               const V3& etaj, const Sym& Hj, double Hdetj, double Ai, const V3& Bi, const V3& gradAi,
+               const T9& gradBi, double& WCRK, double& gradWSPH, V3& gradWCRK) {
+  const double correctionMin = -DBL_MAX, correctionMax = DBL_MAX;
+  const auto WWi = W.kernelAndGradValue(mag(etai), Hdeti);
+  const auto WWj = W.kernelAndGradValue(mag(etaj), Hdetj);
+  const double Wij = 0.5*(WWi.first + WWj.first);
+  const V3 gradWij = vmul(vadd(vmul(sdot(Hi, unitVector(etai)), WWi.second),
+                               vmul(sdot(Hj, unitVector(etaj)), WWj.second)), 0.5);
+  gradWSPH = 0.5*(WWi.second + WWj.second);
+  const double correction0 = Ai*(1.0 + dot(Bi, rij));
+  const double correction = std::max(correctionMin, std::min(correctionMax, correction0));
+  WCRK = correction*Wij;
+  gradWCRK = vmul(gradWij, correction);
+  if (correction0 > correctionMin && correction0 < correctionMax) {
+    gradWCRK = vadd(gradWCRK, vadd(vmul(vmul(Bi, Ai), Wij), vmul(vmul(gradAi, 1.0 + dot(Bi, rij)), Wij)));
+    for (int ii = 0; ii < 3; ++ii)
+      for (int jj = 0; jj < 3; ++jj)
+        el(gradWCRK, ii) += Ai*Wij*el(gradBi, jj, ii)*el(rij, jj);
+  }
+}
+
+void crkEvaluateDerivatives(Problem& p) {
+  zeroDerivs(p);
+  const int n = numNodes(p);
+  p.gradRho.assign(n, V3{0, 0, 0});
+  const TableKernel& W = p.W;
+  const double nPerh = p.cfg.nPerh;
+  const bool compatible = p.cfg.compatibleEnergyEvolution != 0;
+  const bool XSPH = p.cfg.XSPH != 0;
+  for (int i = 0; i < p.nInt; ++i) {
+    const V3& ri = p.pos[i]; const double mi = p.m[i]; const V3& vi = p.vel[i];
+    const double rhoi = p.rho[i]; const double Pi = p.P[i]; const Sym& Hi = p.H[i]; const double ci = p.cs[i];
+    const double Ai = p.A[i]; const V3& Bi = p.B[i]; const V3& gradAi = p.gradA[i]; const T9& gradBi = p.gradB[i];
+    const double Hdeti = sdet(Hi);
+    const double weighti = p.vol[i];
+    for (int j : p.conn[i]) {
+      if (!calcPair(i, j)) continue;
+      const V3& rj = p.pos[j]; const double mj = p.m[j]; const V3& vj = p.vel[j];
+      const double rhoj = p.rho[j]; const double Pj = p.P[j]; const Sym& Hj = p.H[j]; const double cj = p.cs[j];
+      const double Aj = p.A[j]; const V3& Bj = p.B[j]; const V3& gradAj = p.gradA[j]; const T9& gradBj = p.gradB[j];
+      const double Hdetj = sdet(Hj);
+      const double weightj = p.vol[j];
+      const V3 rij = vsub(ri, rj);
+      const V3 etai = sdot(Hi, rij);
+      const V3 etaj = sdot(Hj, rij);
+      const V3 vij = vsub(vi, vj);
+      double Wj, gWj, Wi, gWi;
+      V3 gradWj, gradWi;
+      crkKernel(W, rij, etai, Hi, Hdeti, etaj, Hj, Hdetj, Ai, Bi, gradAi, gradBi, Wj, gWj, gradWj);
+      crkKernel(W, vneg(rij), vneg(etaj), Hj, Hdetj, vneg(etai), Hi, Hdeti, Aj, Bj, gradAj, gradBj, Wi, gWi, gradWi);
+      const V3 deltagrad = vsub(gradWj, gradWi);
+      const V3 gradWSPHi = vmul(sdot(Hi, unitVector(etai)), W.gradValue(mag(etai), Hdeti));
+      const V3 gradWSPHj = vmul(sdot(Hj, unitVector(etaj)), W.gradValue(mag(etaj), Hdetj));
+      {
+        const double fweightij = 1.0;
+        const double rij2 = mag2(rij);
+        const Sym thpt = smul(selfdyad(rij), safeInvVar(rij2*rij2*rij2));
+        p.wns[i] += fweightij*std::abs(gWi);
+        p.wns[j] += 1.0/fweightij*std::abs(gWj);
+        p.m2[i] = sadd(p.m2[i], smul(thpt, fweightij*mag2(gradWSPHi)));
+        p.m2[j] = sadd(p.m2[j], smul(thpt, 1.0/fweightij*mag2(gradWSPHj)));
+      }
+      T9 QPi, QPj;
+      Piij(p, etai, vi, rhoi, ci, etaj, vj, rhoj, cj, QPi, QPj);
+      T9 Qsum = tmul(QPi, rhoi*rhoi);
+      taddto(Qsum, tmul(QPj, rhoj*rhoj));
+      const V3 Qaccij = tvdot(Qsum, deltagrad);
+      const double workQi = rhoj*rhoj*dot(tvdot(QPj, vij), deltagrad);
+      const double workQj = rhoi*rhoi*dot(tvdot(QPi, vij), deltagrad);
+      const double Qi = rhoi*rhoi*(maxAbsElement(V3{QPi.xx, QPi.yy, QPi.zz}));
+      const double Qj = rhoj*rhoj*(maxAbsElement(V3{QPj.xx, QPj.yy, QPj.zz}));
+      p.maxvp[i] = std::max(p.maxvp[i], 4.0*Qi);
+      p.maxvp[j] = std::max(p.maxvp[j], 4.0*Qj);
+      p.effvp[i] += weightj*Qi*Wj;
+      p.effvp[j] += weighti*Qj*Wi;
+      p.viscW[i] += 0.5*weighti*weightj/mi*workQi;
+      p.viscW[j] += 0.5*weighti*weightj/mj*workQj;
+      const T9 deltaDvDxi = tmul(dyad(vij, gradWj), -weightj);
+      const T9 deltaDvDxj = tmul(dyad(vij, gradWi), weighti);
+      taddto(p.DvDx[i], deltaDvDxi);
+      taddto(p.DvDx[j], deltaDvDxj);
+      taddto(p.localDvDx[i], deltaDvDxi);
+      taddto(p.localDvDx[j], deltaDvDxj);
+      p.gradRho[i] = vadd(p.gradRho[i], vmul(gradWj, weightj*(rhoj - rhoi)));
+      p.gradRho[j] = vadd(p.gradRho[j], vmul(gradWi, weighti*(rhoi - rhoj)));
+      const V3 forceij = vmul(vadd(vmul(deltagrad, Pi + Pj), Qaccij), 0.5*weighti*weightj);
+      const V3 forceji = vmul(vadd(vmul(deltagrad, Pi + Pj), Qaccij), 0.5*weighti*weightj);
+      p.DvDt[i] = vsub(p.DvDt[i], vdiv(forceij, mi));
+      p.DvDt[j] = vadd(p.DvDt[j], vdiv(forceji, mj));
+      if (compatible) {
+        p.pairAcc[i].push_back(vdiv(vneg(forceij), mi));
+        p.pairAcc[j].push_back(vdiv(forceji, mj));
+      }
+      p.DepsDt[i] += 0.5*weighti*weightj*(Pj*dot(vij, deltagrad) + workQi)/mi;
+      p.DepsDt[j] += 0.5*weighti*weightj*(Pi*dot(vij, deltagrad) + workQj)/mj;
+      if (XSPH) {
+        p.XSPHdv[i] = vsub(p.XSPHdv[i], vmul(vij, weightj*Wj));
+        p.XSPHdv[j] = vadd(p.XSPHdv[j], vmul(vij, weighti*Wi));
+      }
+    }
+    p.DrhoDt[i] = -rhoi*ttrace(p.DvDx[i]);
+    p.wns[i] = CubeRootHalley2(std::max(0.0, p.wns[i]/Hdeti));
+    p.m2[i] = sdiv(p.m2[i], Hdeti*Hdeti);
+    p.DxDt[i] = XSPH ? vadd(vi, p.XSPHdv[i]) : vi;
+    p.DHDt[i] = smul(sdiv(sneg(Hi), 3), ttrace(p.DvDx[i]));
+    const double zerothMoment = p.wns[i];
+    double cur;
+    if (fuzzyEqual(zerothMoment, 0.0)) cur = 0.5*nPerh;
+    else cur = W.equivalentNodesPerSmoothingScale(zerothMoment);
+    const double s = std::min(4.0, std::max(0.25, nPerh/(cur + 1.0e-30)));
+    double a;
+    if (s < 1.0) a = 0.4*(1.0 + s*s);
+    else a = 0.4*(1.0 + 1.0/(s*s*s));
+    const double hi0 = 1.0/Hi.xx;
+    const double hi1 = std::min(p.cfg.hmax, std::max(p.cfg.hmin, hi0*(1.0 - a + a*s)));
+    const double inv = 1.0/hi1;
+    p.Hideal[i] = Sym{1.0*inv, 0.0*inv, 0.0*inv, 1.0*inv, 0.0*inv, 1.0*inv};
+  }
+}
+
+// ContinuityVolumePolicy (fires after the mass density and H updates).
+void crkVolumeUpdate(Problem& p, double multiplier) {
+  for (int i = 0; i < p.nInt; ++i) {
+    const double volMin = 0.5*p.m[i]*safeInvVar(p.rho[i]);
+    const double volMax = 4.0*M_PI/(3.0*sdet(p.H[i]));
+    const double dVdt = -p.m[i]*safeInvVar(p.rho[i]*p.rho[i])*p.DrhoDt[i];
+    p.vol[i] = std::max(volMin, std::min(volMax, p.vol[i] + multiplier*dVdt));
+  }
+}
+
+void crkInitialize(Problem& p) {
+  crkMoments(p);
+  crkCorrections(p);
+}
+
+bool crkStepRK2(Problem& p, double& dtOut) {
+  const double t = p.time;
+  preStepInitialize(p);
+  crkResize(p);
+  ghostCopy(p, p.vol);
+  const double dt = selectDt(p);
+  const double hdt = 0.5*dt;
+  const std::vector<V3> pos0 = p.pos, vel0 = p.vel;
+  const std::vector<double> rho0 = p.rho, eps0 = p.eps, P0 = p.P, cs0 = p.cs, vol0 = p.vol;
+  const std::vector<Sym> H0 = p.H;
+  if (!stateUpdate(p, hdt, true)) return false;
+  crkVolumeUpdate(p, hdt);
+  p.time = t + hdt;
+  applyGhostBoundaries(p);
+  ghostCopy(p, p.vol);
+  crkInitialize(p);
+  crkEvaluateDerivatives(p);
+  finalizeDerivatives(p);
+  p.pos = pos0; p.vel = vel0; p.rho = rho0; p.eps = eps0; p.P = P0; p.cs = cs0; p.H = H0; p.vol = vol0;
+  if (!stateUpdate(p, dt, false)) return false;
+  crkVolumeUpdate(p, dt);
+  p.time = t + dt;
+  applyGhostBoundaries(p);
+  ghostCopy(p, p.vol);
+  crkSumVolume(p);
+  if (p.cfg.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM) crkSumDensity(p);
+  enforceBoundaries(p);
+  p.cycle += 1;
+  p.lastDt = dt;
+  dtOut = dt;
+  return true;
+}
+
 }  // namespace
 
 // ============================================================== C API
@@ -709,6 +1087,17 @@ void orc_destroy(void* h) { delete static_cast<Problem*>(h); }
 int orc_build_neighbors(void* h) {
   Problem& p = *static_cast<Problem*>(h);
   preStepInitialize(p);
+  if (p.cfg.hydro == SPHGPU_HYDRO_CRKSPH) {
+    // CRKSPHHydroBase::initializeProblemStartup volumes (first call) and the
+    // ghost copy of the evolved volume afterwards.
+    crkResize(p);
+    if (!p.crkVolumeReady) {
+      if (p.cfg.crkVolumeType == SPHGPU_CRK_SUMVOLUME) crkSumVolume(p);
+      else for (int i = 0; i < numNodes(p); ++i) p.vol[i] = p.m[i]/p.rho[i];
+      p.crkVolumeReady = true;
+    }
+    ghostCopy(p, p.vol);
+  }
   return 0;
 }
 
@@ -752,20 +1141,39 @@ int orc_get_ghost_positions(void* h, double* out) {
   return 0;
 }
 
-int orc_initialize(void* h) { initializeDerivatives(*static_cast<Problem*>(h)); return 0; }
+int orc_initialize(void* h) {
+  Problem& p = *static_cast<Problem*>(h);
+  if (p.cfg.hydro == SPHGPU_HYDRO_CRKSPH) crkInitialize(p);
+  else initializeDerivatives(p);
+  return 0;
+}
 int orc_evaluate_derivatives(void* h) {
   Problem& p = *static_cast<Problem*>(h);
-  evaluateDerivatives(p);
+  if (p.cfg.hydro == SPHGPU_HYDRO_CRKSPH) crkEvaluateDerivatives(p);
+  else evaluateDerivatives(p);
   finalizeDerivatives(p);
   return 0;
 }
-int orc_finalize(void* h) { finalizeStep(*static_cast<Problem*>(h)); return 0; }
+int orc_finalize(void* h) {
+  Problem& p = *static_cast<Problem*>(h);
+  if (p.cfg.hydro == SPHGPU_HYDRO_CRKSPH) {
+    if (p.cfg.crkVolumeType == SPHGPU_CRK_SUMVOLUME) crkSumVolume(p);
+    else for (int i = 0; i < numNodes(p); ++i) p.vol[i] = p.m[i]/p.rho[i];
+    if (p.cfg.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM) crkSumDensity(p);
+  } else {
+    finalizeStep(p);
+  }
+  return 0;
+}
 double orc_dt(void* h) { return hydroDt(*static_cast<Problem*>(h)); }
 
 int orc_step_rk2(void* h, int nsteps, double* time, double* lastDt) {
   Problem& p = *static_cast<Problem*>(h);
   double dt = 0.0;
-  for (int s = 0; s < nsteps; ++s) if (!stepRK2(p, dt)) return -6;
+  for (int s = 0; s < nsteps; ++s) {
+    const bool ok = p.cfg.hydro == SPHGPU_HYDRO_CRKSPH ? crkStepRK2(p, dt) : stepRK2(p, dt);
+    if (!ok) return -6;
+  }
   if (time) *time = p.time;
   if (lastDt) *lastDt = dt;
   return 0;
@@ -814,8 +1222,46 @@ int orc_get_field(void* h, const char* key, double* out) {
   if (k == "XSPH delta vi") return V(p.XSPHdv);
   if (k == "weighted neighbor sum") return S(p.wns);
   if (k == "mass second moment") return Y(p.m2);
+  if (k == "node volume") return S(p.vol);
+  if (k == "A CRKSPH correction") return S(p.A);
+  if (k == "B CRKSPH correction") return V(p.B);
+  if (k == "grad A CRKSPH correction") return V(p.gradA);
+  if (k == "grad B CRKSPH correction") return T(p.gradB);
+  if (k == "m0 CRKSPH moment") return S(p.m0);
+  if (k == "m1 CRKSPH moment") return V(p.m1);
+  if (k == "m2 CRKSPH moment") return Y(p.cm2);
+  if (k == "grad m0 CRKSPH moment") return V(p.gradm0);
+  if (k == "grad m1 CRKSPH moment") return T(p.gradm1);
+  if (k == "mass density gradient") return V(p.gradRho);
+  if (k == "grad m2 CRKSPH moment") {
+    for (int i = 0; i < n; ++i) for (int c = 0; c < 27; ++c) out[27*i + c] = p.gradm2[i][c];
+    return 0;
+  }
   g_err = "unknown field key " + k;
   return -1;
+}
+
+// CRK reproducing conditions at each internal node i (after orc_initialize):
+// out[4i] = sum_j V_j W^R_ij (self included, should be 1),
+// out[4i+1..3] = sum_j V_j W^R_ij (r_j - r_i) (should vanish), with
+// W^R_ij = A_i (1 + B_i . r_ij) W_ij and W_ij the symmetrized kernel.
+int orc_crk_reproduction(void* h, double* out) {
+  Problem& p = *static_cast<Problem*>(h);
+  for (int i = 0; i < p.nInt; ++i) {
+    const double Hdeti = sdet(p.H[i]);
+    double s0 = p.vol[i]*p.A[i]*p.W.kernelValue(0.0, Hdeti);
+    V3 s1{0, 0, 0};
+    for (int j : p.conn[i]) {
+      const V3 rij = vsub(p.pos[i], p.pos[j]);
+      const double Wij = 0.5*(p.W.kernelValue(mag(sdot(p.H[i], rij)), Hdeti) +
+                              p.W.kernelValue(mag(sdot(p.H[j], rij)), sdet(p.H[j])));
+      const double WR = p.A[i]*(1.0 + dot(p.B[i], rij))*Wij;
+      s0 += p.vol[j]*WR;
+      s1 = vadd(s1, vmul(vneg(rij), p.vol[j]*WR));
+    }
+    out[4*i] = s0; out[4*i + 1] = s1.x; out[4*i + 2] = s1.y; out[4*i + 3] = s1.z;
+  }
+  return 0;
 }
 
 // Pair-wise accelerations per node, flattened in the reference's push order

@@ -67,6 +67,22 @@ def test_connectivity_bitexact(gpu_lib, pkg, oracle_mod, case):
     assert g.num_pairs() == o.num_pairs()
 
 
+@pytest.mark.parametrize("case", ["sod", "kh", "sod_x_periodic_only"])
+@pytest.mark.parametrize("schedule", [1, 2])
+def test_connectivity_every_schedule(gpu_lib, pkg, oracle_mod, case, schedule):
+    """Thread-per-node and warp-per-node neighbor walks give the same CSR."""
+    g, o, ns = _pair(pkg, oracle_mod, case)
+    g.set_schedule("neighbor walk", schedule)
+    g.build_neighbors()
+    assert g.schedule("neighbor walk") == schedule
+    o.build_neighbors()
+    go, gn, gr = g.connectivity()
+    oo, on, orr = o.connectivity()
+    assert np.array_equal(go, oo)
+    assert np.array_equal(gn, on)
+    assert g.num_pairs() == o.num_pairs()
+
+
 @pytest.mark.parametrize("case", list(CASES))
 def test_evaluate_derivatives_parity(gpu_lib, pkg, oracle_mod, case):
     g, o, ns = _pair(pkg, oracle_mod, case)
