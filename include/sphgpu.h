@@ -155,6 +155,20 @@ int sphgpu_step_rk2(sphgpu_problem* p, double* time, int64_t nsteps, double* las
 /* SpheralConservation (src/SimulationControl/SpheralConservation.py:27-63):
  * out = {mass, px, py, pz, kinetic E, thermal E, total E, 0}, FP64 on device. */
 int sphgpu_conservation(sphgpu_problem* p, double out[8]);
+/* The same sums over caller-owned DEVICE arrays (reference Field layout:
+ * mass[n], velocity[3n] AoS, specificThermalEnergy[n]) with no problem
+ * handle and no allocation: no counterpart in the reference.  For callers
+ * that must not allocate device memory when they ask for the sums (state in
+ * their own buffers under a fixed HBM budget).  Scratch is a fixed device
+ * array inside the library, so n <= 16,777,216 (larger n returns
+ * SPHGPU_ERR_CAPACITY).  The first call on each device looks up the scratch
+ * address (set-up); make it before any stream capture.  Work is issued on
+ * `stream` (cudaStream_t as void*, NULL = default stream); the call returns
+ * after the results are in `out` (host memory).  Calls that overlap in time
+ * on one device share the scratch and race. */
+int sphgpu_conservation_noalloc(const double* mass, const double* velocity,
+                                const double* specificThermalEnergy, int64_t n, void* stream,
+                                double out[8]);
 
 /* Pair interactions (the reference's ncalc summed over nodes,
  * src/SPH/SPHHydroBase.cc:674) of the current connectivity. */

@@ -148,6 +148,7 @@ def load_library(path=None):
     lib.sphgpu_conservation.argtypes = [P, P]
     lib.sphgpu_num_pairs.argtypes = [P, ctypes.POINTER(I64)]
     lib.sphgpu_kernel_launches.argtypes = [P, ctypes.POINTER(I64)]
+    lib.sphgpu_conservation_noalloc.argtypes = [P, P, P, I64, P, P]
     lib.sphgpu_set_schedule.argtypes = [P, ctypes.c_char_p, ctypes.c_int32]
     lib.sphgpu_get_schedule.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32)]
     lib.sphgpu_synchronize.argtypes = [P]

@@ -26,6 +26,7 @@ UNITS = [
     ("sph.cu", ["-fmad=false"]),
     ("sph_mixed.cu", []),
     ("crk.cu", ["-fmad=false"]),
+    ("noalloc.cu", []),
     ("table.cc", []),
 ]
 HEADERS = ["devmath.cuh", "problem.cuh", "scan.cuh", "mixed.cuh"]
