@@ -51,6 +51,14 @@ def parse():
     ap.add_argument("--nx", type=int, default=128, help="lattice size per axis (default: the full workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=200,
+                    help="RK2 steps of the mixed-vs-FP64 error and energy-drift line (0: skip)")
+    ap.add_argument("--no-configs", dest="configs", action="store_false",
+                    help="skip the Sod (plain FP64) and CRKSPH Kelvin-Helmholtz lines")
+    ap.add_argument("--batch", type=int, default=256, help="problems in the batched-ensemble line (0: skip)")
+    ap.add_argument("--serving", type=float, default=2.0,
+                    help="seconds of Poisson arrivals in the serving line (0: skip; 60 = the full trace)")
+    ap.add_argument("--serving-steps", type=int, default=20, help="RK2 steps per served request (full: 200)")
     return ap.parse_args()
 
 
@@ -262,6 +270,211 @@ def measure_e2e(pkg, ns, cfg, steps, warmup):
             "ms_per_step": 1e3 * el / steps}
 
 
+ACCURACY_FIELDS = ["delta velocity hydro", "delta specific thermal energy", "delta mass density",
+                   "velocity gradient", "new mass density", "new H", "M SPH gradient correction",
+                   "max viscous pressure", "weighted neighbor sum"]
+
+
+def measure_accuracy(pkg, ns, cfg, steps):
+    """Mixed form against plain FP64 on the same node set: max and RMS
+    relative error of every derivative field (normwise: ||d||/||fp64||) at
+    the start, and the relative total-energy drift of each form over
+    `steps` RK2 steps."""
+    abi = pkg.abi
+    cf, cm = cfg.copy(), cfg.copy()
+    cf.precision = abi.PRECISION_FP64
+    cm.precision = abi.PRECISION_MIXED
+    hf, hm = pkg.SPHHydro(cf, ns), pkg.SPHHydro(cm, ns)
+    for h in (hf, hm):
+        h.build_neighbors()
+        h.evaluateDerivatives()
+    errs = {}
+    for k in ACCURACY_FIELDS:
+        a, b = hm.field(k), hf.field(k)
+        d = np.abs(a - b)
+        errs[k] = {"max_rel": float(d.max() / max(np.abs(b).max(), 1e-300)),
+                   "rms_rel": float(np.sqrt(np.mean(d * d)) / max(np.sqrt(np.mean(b * b)), 1e-300))}
+    drift = {}
+    for name, h in (("plain_fp64", hf), ("mixed", hm)):
+        e0 = h.conservation()[6]
+        h.step(steps)
+        drift[name] = float(abs(h.conservation()[6] - e0) / abs(e0))
+    hf.close()
+    hm.close()
+    return {"field_error_vs_fp64": errs,
+            "max_field_error": max(v["max_rel"] for v in errs.values()),
+            "energy_drift": drift, "drift_steps": steps}
+
+
+def measure_rate(pkg, ns, cfg, steps, warmup, eval_reps=5):
+    """Step rate (pair-interactions/s, ms per step) and the derivative
+    evaluation time of one problem."""
+    import torch
+    h = pkg.SPHHydro(cfg, ns)
+    h.build_neighbors()
+    h.initialize()
+    h.evaluateDerivatives()
+    stream = torch.cuda.ExternalStream(h.stream())
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    h.synchronize()
+    a.record(stream)
+    for _ in range(eval_reps):
+        h.evaluateDerivatives()
+    b.record(stream)
+    h.synchronize()
+    eval_ms = a.elapsed_time(b) / eval_reps
+    eval_pairs = h.num_pairs()
+    for _ in range(warmup):
+        h.step(1)
+    h.synchronize()
+    a.record(stream)
+    pairs = 0
+    for _ in range(steps):
+        h.step(1)
+        pairs += h.num_pairs()
+    b.record(stream)
+    h.synchronize()
+    ms = a.elapsed_time(b)
+    h.close()
+    return {"value": pairs / (ms / 1e3), "unit": METRIC, "ms_per_step": ms / steps,
+            "eval_ms": eval_ms, "eval_pair_interactions_per_s": eval_pairs / (eval_ms / 1e3)}
+
+
+def measure_config_sod(pkg, steps, warmup):
+    """Sod tube, plain FP64: 256x32x32 = 262,144 nodes, cubic B-spline
+    nPerh 1.51 (~122 neighbors), fixed dt 1e-4."""
+    gen, abi = pkg.generators, pkg.abi
+    box = ((0.0, 0.0, 0.0), (1.0, 0.125, 0.125))
+    ns = gen.sod(nx=256, ny=32, nz=32, box=box)
+    out = {}
+    for name, prec in (("plain_fp64", abi.PRECISION_FP64), ("mixed", abi.PRECISION_MIXED)):
+        out[name] = measure_rate(pkg, ns, gen.sod_config(abi, ns_box=box, precision=prec), steps, warmup)
+    out["config"] = {"workload": "Sod tube 256x32x32 = 262,144 nodes in [0,1]x[0,0.125]^2 (periodic), "
+                                 "cubic B-spline TableKernel(1000) nPerh 1.51, MG Cl=Cq=1, compatible energy, "
+                                 "fixed dt 1e-4"}
+    return out
+
+
+def measure_config_crk(pkg, steps, warmup, drift_steps):
+    """CRKSPH Kelvin-Helmholtz 128x128x64 = 1,048,576 nodes (Wendland C4,
+    nPerh 1.35, linear corrections, CRKSumVolume): plain FP64 against the
+    mixed form, step rate and energy drift over `drift_steps` steps."""
+    gen, abi = pkg.generators, pkg.abi
+    ns = gen.kelvin_helmholtz(nx=128, ny=128, nz=64, box=((0, 0, 0), (1.0, 1.0, 1.0)))
+    out = {}
+    for name, prec in (("plain_fp64", abi.PRECISION_FP64), ("mixed", abi.PRECISION_MIXED)):
+        cfg = gen.kh_config(abi, hydro=abi.HYDRO_CRKSPH, precision=prec)
+        out[name] = measure_rate(pkg, ns, cfg, steps, warmup)
+        if drift_steps > 0:
+            h = pkg.SPHHydro(cfg, ns)
+            h.build_neighbors()
+            h.initialize()
+            h.evaluateDerivatives()
+            e0 = h.conservation()[6]
+            h.step(drift_steps)
+            out[name]["energy_drift"] = float(abs(h.conservation()[6] - e0) / abs(e0))
+            out[name]["drift_steps"] = drift_steps
+            h.close()
+    out["mixed_over_plain"] = out["mixed"]["value"] / out["plain_fp64"]["value"]
+    out["config"] = {"workload": "CRKSPH Kelvin-Helmholtz 128x128x64 = 1,048,576 nodes in the unit cube "
+                                 "(dz = 2 dx), Wendland C4 nPerh 1.35, linear corrections, CRKSumVolume, "
+                                 "Courant dt"}
+    return out
+
+
+def batch_specs(pkg, count, seed=20261203, nmin=4096, nmax=262144):
+    """The batched-ensemble workload: `count` Sod-type tubes, n log-uniform in
+    [nmin, nmax] as an 8k x k x k lattice, gamma ~ U[1.3, 1.67], left/right
+    density ratio ~ U[2, 8], cubic B-spline nPerh 1.51, mixed form."""
+    gen, abi = pkg.generators, pkg.abi
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = float(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))
+        kk = int(min(32, max(8, round((n / 8.0) ** (1.0 / 3.0)))))
+        gamma = float(rng.uniform(1.3, 1.67))
+        ratio = float(rng.uniform(2.0, 8.0))
+        box = ((0.0, 0.0, 0.0), (1.0, 0.125, 0.125))
+        ns = gen.sod(nx=8 * kk, ny=kk, nz=kk, box=box, gamma=gamma, rho1=1.0, rho2=1.0 / ratio, P1=1.0,
+                     P2=0.1795, seed=seed + 1 + k)
+        cfg = gen.sod_config(abi, ns_box=box, gamma=gamma, precision=abi.PRECISION_MIXED)
+        out.append((ns, cfg))
+    return out
+
+
+def measure_batch(pkg, count, steps, warmup):
+    """Batched ensemble: every stage one launch over all members (autotuned),
+    against the same problems stepped one at a time (one launch per problem
+    per stage)."""
+    import torch
+    specs = batch_specs(pkg, count)
+    probs = [pkg.SPHHydro(cfg, ns) for ns, cfg in specs]
+    nodes = sum(ns.n for ns, _ in specs)
+    batch = pkg.SPHBatch(probs)
+    batch.build_neighbors()
+    batch.evaluateDerivatives()
+    tune = batch.autotune()
+    for _ in range(warmup):
+        batch.step(1)
+    torch.cuda.synchronize()
+    l0 = batch.kernel_launches()
+    t0 = time.perf_counter()
+    pairs = 0
+    for _ in range(steps):
+        batch.step(1)
+        pairs += batch.num_pairs()
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    launches = batch.kernel_launches() - l0
+    for _ in range(warmup):
+        for p in probs:
+            p.step(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lpairs = 0
+    for _ in range(steps):
+        for p in probs:
+            p.step(1)
+            lpairs += p.num_pairs()
+    torch.cuda.synchronize()
+    t_loop = time.perf_counter() - t0
+    batch.close()
+    for p in probs:
+        p.close()
+    return {"value": pairs / t_batch, "unit": METRIC, "ms_per_step": 1e3 * t_batch / steps,
+            "one_launch_per_problem": {"value": lpairs / t_loop, "unit": METRIC,
+                                       "ms_per_step": 1e3 * t_loop / steps},
+            "batched_over_loop": (pairs / t_batch) / (lpairs / t_loop),
+            "kernel_launches_per_step": launches / steps,
+            "autotuned": {"neighbor walk": ["auto", "thread per node", "warp per node"][tune["neighbor walk"]],
+                          "pair loop threads": tune["pair loop"]},
+            "config": {"workload": "%d Sod-type tubes, n log-uniform in [4096, 262144] (8k x k x k), "
+                                   "gamma ~ U[1.3, 1.67], density ratio ~ U[2, 8], cubic B-spline nPerh 1.51, "
+                                   "mixed form, fixed dt 1e-4" % count,
+                       "nodes": nodes, "steps": steps, "warmup": warmup}}
+
+
+def measure_serving(pkg, duration, nsteps, rate=20.0, budget=150e9):
+    """Continuous-batching request loop on a seeded Poisson trace, mixed form
+    and plain FP64 on the same trace."""
+    s = pkg.serving
+    trace = s.poisson_trace(rate=rate, duration=duration, nsteps=nsteps)
+    out = {}
+    for name, prec in (("mixed", pkg.abi.PRECISION_MIXED), ("plain_fp64", pkg.abi.PRECISION_FP64)):
+        ttc, makespan, stats = s.serve(trace, prec, budget_bytes=budget)
+        t = np.array(ttc)
+        out[name] = {"ttc_p50_s": float(np.percentile(t, 50)), "ttc_p99_s": float(np.percentile(t, 99)),
+                     "pair_interactions_per_s": stats["pair_interactions"] / makespan, "makespan_s": makespan,
+                     "completed": int(stats["completed"]), "peak_device_gb": stats["peak_bytes"] / 1e9,
+                     "batched_steps": int(stats["ticks"])}
+    out["config"] = {"trace": "Poisson arrivals at %.0f/s for %.1f s (%d requests, seeded), 50/50 "
+                              "Kelvin-Helmholtz / Sod-type, n log-uniform in [8192, 1048576], %d RK2 steps each, "
+                              "admission by device footprint under %.0f GB" % (rate, duration, len(trace), nsteps,
+                                                                              budget / 1e9)}
+    return out
+
+
 def cpu_baseline(pkg, ns, cfg):
     """The oracle (a serial FP64 restatement of the reference path) on the
     same workload: one RK2 step after the start-up evaluation, 1 core."""
@@ -414,6 +627,24 @@ def run_ours(args):
             result["cpu_baseline"] = cpu_baseline(pkg, ns, cfg)
     hm.close()
     hp.close()
+    if args.accuracy_steps > 0:
+        acc = measure_accuracy(pkg, ns, cfg, args.accuracy_steps)
+        if rank == 0:
+            result["accuracy"] = acc
+    if args.configs:
+        rsod = measure_config_sod(pkg, max(3, args.steps // 2), 2)
+        rcrk = measure_config_crk(pkg, max(3, args.steps // 2), 2, args.accuracy_steps)
+        if rank == 0:
+            result["sod_fp64"] = rsod
+            result["crk_kh"] = rcrk
+    if args.batch > 0:
+        rb = measure_batch(pkg, args.batch, max(2, args.steps // 3), 1)
+        if rank == 0:
+            result["batch"] = rb
+    if args.serving > 0:
+        rs = measure_serving(pkg, args.serving, args.serving_steps)
+        if rank == 0:
+            result["serving"] = rs
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

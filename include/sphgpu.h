@@ -152,6 +152,8 @@ int sphgpu_dt(sphgpu_problem* p, double* dt_out);
 /* CheapSynchronousRK2::step (src/Integrator/CheapSynchronousRK2.cc:81-143),
  * nsteps times; *time advances, *last_dt receives the last step size. */
 int sphgpu_step_rk2(sphgpu_problem* p, double* time, int64_t nsteps, double* last_dt);
+/* Integrator::currentTime and lastDt (src/Integrator/Integrator.hh) of the problem. */
+int sphgpu_time(sphgpu_problem* p, double* time, double* last_dt);
 /* SpheralConservation (src/SimulationControl/SpheralConservation.py:27-63):
  * out = {mass, px, py, pz, kinetic E, thermal E, total E, 0}, FP64 on device. */
 int sphgpu_conservation(sphgpu_problem* p, double out[8]);
@@ -181,9 +183,90 @@ int sphgpu_kernel_launches(sphgpu_problem* p, int64_t* launches);
  * stage "neighbor walk": 0 = automatic (thread per node while the 27-cell
  * candidate set is small, warp per node otherwise), 1 = thread per node,
  * 2 = warp per node.  Every schedule yields the same ConnectivityMap.
- * sphgpu_get_schedule reports the schedule the last call actually used. */
+ * stage "pair loop": threads per block of the derivative kernels, 64 or 128.
+ * stage "neighbor filter": 1 (default) = an FP32 pre-test decides the pairs
+ * clearly inside or outside the kernel support and the exact FP64 test the
+ * rest (used only while every H has condition number <= 100, where the FP32
+ * error is far inside the band, so the ConnectivityMap is unchanged); 0 = the
+ * FP64 test for every candidate.  stage "step graph": 1 = the part of each
+ * RK2 step after the ghost/connectivity rebuild (records, dt, updates,
+ * derivatives, compatible energy, sum density, boundaries) is captured once
+ * as a CUDA graph and replayed every step (re-captured when a buffer moves);
+ * 0 = eager launches.  sphgpu_get_schedule reports what the last call used. */
 int sphgpu_set_schedule(sphgpu_problem* p, const char* stage, int32_t schedule);
 int sphgpu_get_schedule(sphgpu_problem* p, const char* stage, int32_t* schedule);
+/* Autotuner: times every schedule of the neighbor walk and the pair loop on
+ * the problem's own data (CUDA events, median of three) and keeps the
+ * fastest.  Results do not depend on the schedule; the call leaves the
+ * connectivity rebuilt and the derivatives evaluated at the current state (as
+ * sphgpu_build_neighbors, sphgpu_initialize and sphgpu_evaluate_derivatives
+ * do).  report (may be NULL) = {neighbor schedule, ms thread, ms warp,
+ * pair-loop threads, ms 64, ms 128, 0, 0}. */
+int sphgpu_autotune(sphgpu_problem* p, double report[8]);
+/* ---- batches (no counterpart in the reference, which advances one problem
+ * at a time).  A batch advances many independent problems together: each
+ * stage of a call is ONE kernel launch over all members, whose blocks are
+ * dealt to the members through a per-member block-offset table.  Members keep
+ * their own device state and may differ in size, kernel, gamma, hydro form
+ * and precision; a member's results are bit-identical to running it alone.
+ * Members must live on the current device.  A batch works on its own stream
+ * and first waits for work pending on its members' streams. */
+typedef struct sphgpu_batch sphgpu_batch;
+int sphgpu_batch_create(sphgpu_problem* const* members, int32_t count, sphgpu_batch** out);
+void sphgpu_batch_destroy(sphgpu_batch* b);
+int sphgpu_batch_size(sphgpu_batch* b, int32_t* count);
+/* sphgpu_build_neighbors for every member. */
+int sphgpu_batch_build_neighbors(sphgpu_batch* b);
+/* sphgpu_initialize + sphgpu_evaluate_derivatives for every member. */
+int sphgpu_batch_evaluate_derivatives(sphgpu_batch* b);
+/* nsteps CheapSynchronousRK2 steps of every member, each with its own dt;
+ * every member's time and last dt advance as with sphgpu_step_rk2. */
+int sphgpu_batch_step_rk2(sphgpu_batch* b, int64_t nsteps);
+/* Pair interactions of the members' current connectivity, summed. */
+int sphgpu_batch_pairs(sphgpu_batch* b, int64_t* pairs);
+int sphgpu_batch_kernel_launches(sphgpu_batch* b, int64_t* launches);
+/* Schedule for all members that have not set their own (see sphgpu_set_schedule). */
+int sphgpu_batch_set_schedule(sphgpu_batch* b, const char* stage, int32_t schedule);
+/* sphgpu_autotune over the whole batch (one schedule per stage for all members). */
+int sphgpu_batch_autotune(sphgpu_batch* b, double report[8]);
+int sphgpu_batch_get_stream(sphgpu_batch* b, void** stream);
+
+/* ---- serving (no counterpart in the reference).  A continuous-batching
+ * request loop: simulations are submitted as they arrive, admitted first come
+ * first served while their device-memory footprint fits under the budget
+ * (and at most max_members run at once), advanced together by one batched
+ * RK2 step per tick with their state resident on the device, and retired
+ * when they reach their step count.  A request larger than the whole budget
+ * fails with SPHGPU_ERR_ADMISSION (reported through sphgpu_server_status). */
+typedef struct sphgpu_server sphgpu_server;
+#define SPHGPU_REQ_QUEUED  0
+#define SPHGPU_REQ_RUNNING 1
+#define SPHGPU_REQ_DONE    2
+#define SPHGPU_REQ_FAILED  3
+/* Device bytes the server charges for a request before it runs (host only;
+ * positions and H as for sphgpu_set_state). */
+int sphgpu_estimate_footprint(const sphgpu_config* cfg, int64_t n, const double* position, const double* H,
+                              int64_t* bytes);
+int sphgpu_server_create(double hbm_budget_bytes, int32_t max_members, sphgpu_server** out);
+void sphgpu_server_destroy(sphgpu_server* s);
+/* Queue a simulation: configuration, initial state (host AoS arrays as for
+ * sphgpu_set_state, copied at submission) and its number of RK2 steps. */
+int sphgpu_server_submit(sphgpu_server* s, const sphgpu_config* cfg, int64_t n, const double* position,
+                         const double* velocity, const double* mass, const double* massDensity,
+                         const double* specificThermalEnergy, const double* H, int64_t nsteps, int64_t* id);
+/* Admit what fits, advance every running simulation by one RK2 step, retire
+ * the finished ones.  Returns the running and queued counts afterwards. */
+int sphgpu_server_tick(sphgpu_server* s, int32_t* running, int32_t* queued);
+/* Requests finished (done or failed) since the last call, up to `capacity`. */
+int sphgpu_server_finished(sphgpu_server* s, int64_t* ids, int32_t capacity, int32_t* count);
+int sphgpu_server_status(sphgpu_server* s, int64_t id, int32_t* state, int64_t* steps_done, int64_t* pairs);
+/* Final state of a finished request (any pointer may be NULL); releases it. */
+int sphgpu_server_fetch(sphgpu_server* s, int64_t id, double* position, double* velocity, double* mass,
+                        double* massDensity, double* specificThermalEnergy, double* H, double* time);
+/* {bytes in use, peak bytes in use, budget, pair interactions, ticks,
+ *  completed requests, simulation steps, kernel launches} */
+int sphgpu_server_stats(sphgpu_server* s, double out[8]);
+
 /* Synchronise the problem's stream; returns the first device error. */
 int sphgpu_synchronize(sphgpu_problem* p);
 /* CUDA stream the problem launches on (cudaStream_t as void*). */

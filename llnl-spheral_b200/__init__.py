@@ -12,4 +12,5 @@ name carries a hyphen).
 from . import abi  # noqa: F401
 from . import generators  # noqa: F401
 from . import hydro  # noqa: F401
-from .hydro import SPHHydro, CheapSynchronousRK2Integrator  # noqa: F401
+from .hydro import SPHHydro, SPHBatch, CheapSynchronousRK2Integrator  # noqa: F401
+from . import serving  # noqa: F401

@@ -148,6 +148,31 @@ def load_library(path=None):
     lib.sphgpu_conservation.argtypes = [P, P]
     lib.sphgpu_num_pairs.argtypes = [P, ctypes.POINTER(I64)]
     lib.sphgpu_kernel_launches.argtypes = [P, ctypes.POINTER(I64)]
+    lib.sphgpu_time.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    lib.sphgpu_batch_create.argtypes = [P, ctypes.c_int32, ctypes.POINTER(P)]
+    lib.sphgpu_batch_destroy.argtypes = [P]
+    lib.sphgpu_batch_destroy.restype = None
+    lib.sphgpu_batch_size.argtypes = [P, ctypes.POINTER(ctypes.c_int32)]
+    lib.sphgpu_batch_build_neighbors.argtypes = [P]
+    lib.sphgpu_batch_evaluate_derivatives.argtypes = [P]
+    lib.sphgpu_batch_step_rk2.argtypes = [P, I64]
+    lib.sphgpu_batch_pairs.argtypes = [P, ctypes.POINTER(I64)]
+    lib.sphgpu_batch_kernel_launches.argtypes = [P, ctypes.POINTER(I64)]
+    lib.sphgpu_batch_set_schedule.argtypes = [P, ctypes.c_char_p, ctypes.c_int32]
+    lib.sphgpu_batch_get_stream.argtypes = [P, ctypes.POINTER(P)]
+    lib.sphgpu_autotune.argtypes = [P, P]
+    lib.sphgpu_batch_autotune.argtypes = [P, P]
+    lib.sphgpu_estimate_footprint.argtypes = [P, I64, P, P, ctypes.POINTER(I64)]
+    lib.sphgpu_server_create.argtypes =[ctypes.c_double, ctypes.c_int32, ctypes.POINTER(P)]
+    lib.sphgpu_server_destroy.argtypes = [P]
+    lib.sphgpu_server_destroy.restype = None
+    lib.sphgpu_server_submit.argtypes = [P, P, I64] + [P] * 6 + [I64, ctypes.POINTER(I64)]
+    lib.sphgpu_server_tick.argtypes = [P, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
+    lib.sphgpu_server_finished.argtypes = [P, P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+    lib.sphgpu_server_status.argtypes = [P, I64, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(I64),
+                                         ctypes.POINTER(I64)]
+    lib.sphgpu_server_fetch.argtypes = [P, I64] + [P] * 6 + [ctypes.POINTER(ctypes.c_double)]
+    lib.sphgpu_server_stats.argtypes = [P, P]
     lib.sphgpu_conservation_noalloc.argtypes = [P, P, P, I64, P, P]
     lib.sphgpu_set_schedule.argtypes = [P, ctypes.c_char_p, ctypes.c_int32]
     lib.sphgpu_get_schedule.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32)]

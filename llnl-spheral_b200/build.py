@@ -22,14 +22,17 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 # (source, extra flags)
 UNITS = [
     ("api.cu", ["-fmad=false"]),
+    ("batch.cu", []),
     ("nbrs.cu", ["-fmad=false"]),
     ("sph.cu", ["-fmad=false"]),
     ("sph_mixed.cu", []),
     ("crk.cu", ["-fmad=false"]),
+    ("crk_mixed.cu", []),
     ("noalloc.cu", []),
+    ("server.cu", []),
     ("table.cc", []),
 ]
-HEADERS = ["devmath.cuh", "problem.cuh", "scan.cuh", "mixed.cuh"]
+HEADERS = ["devmath.cuh", "problem.cuh", "mixed.cuh"]
 
 
 def _mtime(p):

@@ -1,9 +1,13 @@
 // C-ABI of the B200 SPH hydro path and the host-side orchestration of one
-// CheapSynchronousRK2 step (src/Integrator/CheapSynchronousRK2.cc:81-143).
+// CheapSynchronousRK2 step (src/Integrator/CheapSynchronousRK2.cc:81-143),
+// for one problem or for a batch of independent problems.
 //
-// All device work of a problem is issued on the problem's stream.  Each call
-// returns SPHGPU_OK or a negative status (no exceptions cross the ABI); the
-// text of the last failure is kept per host thread.
+// A problem's own calls run as a batch of one member on the problem's
+// stream; a batch runs every stage as one launch over all its members on
+// the batch's stream.  Each call returns SPHGPU_OK or a negative status (no
+// exceptions cross the ABI); the text of the last failure is kept per host
+// thread.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <cmath>
@@ -12,7 +16,6 @@
 #include <vector>
 
 #include "problem.cuh"
-#include "scan.cuh"
 #include "mixed.cuh"
 
 namespace sphgpu {
@@ -29,17 +32,6 @@ int cuda_status(cudaError_t e, const char* where) {
   return e == cudaErrorMemoryAllocation ? SPHGPU_ERR_NOMEM : SPHGPU_ERR_CUDA;
 }
 
-#define SPH_CHECK(call)                                                 \
-  do {                                                                  \
-    const cudaError_t e__ = (call);                                     \
-    if (e__ != cudaSuccess) return cuda_status(e__, #call);             \
-  } while (0)
-
-#define SPH_TRY(expr)                                                   \
-  do {                                                                  \
-    const int rc__ = (expr);                                            \
-    if (rc__ != SPHGPU_OK) return rc__;                                 \
-  } while (0)
 
 namespace {
 
@@ -163,27 +155,8 @@ const FieldSpec* findField(const char* key) {
   return nullptr;
 }
 
-int check_device_error(Problem& p, const char* where) {
-  int herr = 0;
-  SPH_CHECK(cudaMemcpyAsync(&herr, p.d_err, sizeof(int), cudaMemcpyDeviceToHost, p.stream));
-  SPH_CHECK(cudaStreamSynchronize(p.stream));
-  if (herr == 0) return SPHGPU_OK;
-  cudaMemsetAsync(p.d_err, 0, sizeof(int), p.stream);
-  std::string msg = std::string(where) + ":";
-  int rc = SPHGPU_ERR_NUMERIC;
-  if (herr & DERR_NBR_CAPACITY) { msg += " neighbor capacity exceeded;"; rc = SPHGPU_ERR_CAPACITY; }
-  if (herr & DERR_GHOST_CHAIN) { msg += " ghost imaged twice on one axis;"; rc = SPHGPU_ERR_UNSUPPORTED; }
-  if (herr & DERR_H_CLAMP) { msg += " H eigenvalue clamp (hmin/hmax) would be active;"; rc = SPHGPU_ERR_UNSUPPORTED; }
-  if (herr & DERR_NONPOSITIVE) { msg += " non-positive mass/density/det(H) or non-finite state;"; rc = SPHGPU_ERR_NUMERIC; }
-  set_error(msg);
-  return rc;
-}
-
 int validate_config(const sphgpu_config& c) {
   if (c.hydro != SPHGPU_HYDRO_SPH && c.hydro != SPHGPU_HYDRO_CRKSPH) { set_error("unknown hydro"); return SPHGPU_ERR_ARG; }
-  if (c.hydro == SPHGPU_HYDRO_CRKSPH && c.precision != SPHGPU_PRECISION_FP64) {
-    set_error("CRKSPH runs in the plain FP64 form only"); return SPHGPU_ERR_UNSUPPORTED;
-  }
   if (c.crkVolumeType != SPHGPU_CRK_SUMVOLUME && c.crkVolumeType != SPHGPU_CRK_MASSOVERDENSITY) {
     set_error("unknown crkVolumeType"); return SPHGPU_ERR_ARG;
   }
@@ -204,11 +177,19 @@ void free_problem(Problem* p) {
   if (p == nullptr) return;
   void* ptrs[] = {p->S, p->S0, p->D, p->rec, p->groot, p->gcode, p->gpos, p->cand, p->cidx, p->sortedIdx,
                   p->cellStart, p->cellFill, p->counts, p->offsets, p->nbr, p->pacc, p->tableCoef, p->nperhTab,
-                  p->wsumTab, p->blockSums, p->d_err, p->d_scal, p->d_red, p->staging, p->coefF, p->mrec, p->K, p->crec};
+                  p->wsumTab, p->blockSums, p->d_err, p->d_scal, p->d_red, p->staging, p->coefF, p->mrec, p->K, p->crec, p->hmaxi};
   for (void* q : ptrs) if (q) cudaFree(q);
   if (p->pinned) cudaFreeHost(p->pinned);
+  if (p->solo) { batch_free(*p->solo); delete p->solo; p->solo = nullptr; }
   if (p->ownStream && p->stream) cudaStreamDestroy(p->stream);
   delete p;
+}
+
+// The problem as a batch of one.  Its descriptor is re-uploaded on every
+// call: another batch holding the same problem may have moved its buffers.
+Batch& solo(Problem* p) {
+  p->solo->memDirty = true;
+  return *p->solo;
 }
 
 // AoS host array -> SoA fields of S (via the device staging buffer).
@@ -236,6 +217,50 @@ int download_aos(Problem& p, const double* base, int comps, int field, double* h
   return SPHGPU_OK;
 }
 
+// Every member's device error word; reports and clears the words that are set.
+int batch_check_errors(Batch& b, const char* where) {
+  const int slot = -1;
+  std::vector<double> errs;
+  SPH_TRY(batch_gather(b, &slot, 1, errs));
+  int rc = SPHGPU_OK;
+  std::string msg;
+  for (size_t m = 0; m < b.mem.size(); ++m) {
+    const int herr = (int)errs[m];
+    if (herr == 0) continue;
+    cudaMemsetAsync(b.mem[m]->d_err, 0, sizeof(int), b.stream);
+    msg = std::string(where) + ":";
+    if (b.mem.size() > 1) msg += " member " + std::to_string(m) + ":";
+    int r = SPHGPU_ERR_NUMERIC;
+    if (herr & DERR_NBR_CAPACITY) { msg += " neighbor capacity exceeded;"; r = SPHGPU_ERR_CAPACITY; }
+    if (herr & DERR_GHOST_CHAIN) { msg += " ghost imaged twice on one axis;"; r = SPHGPU_ERR_UNSUPPORTED; }
+    if (herr & DERR_H_CLAMP) { msg += " H eigenvalue clamp (hmin/hmax) would be active;"; r = SPHGPU_ERR_UNSUPPORTED; }
+    if (herr & DERR_NONPOSITIVE) { msg += " non-positive mass/density/det(H) or non-finite state;"; r = SPHGPU_ERR_NUMERIC; }
+    if (rc == SPHGPU_OK) rc = r;
+  }
+  if (rc != SPHGPU_OK) {
+    cudaStreamSynchronize(b.stream);
+    set_error(msg);
+  }
+  return rc;
+}
+
+__global__ void __launch_bounds__(256) copy_state_kernel(const Member* mem, BlockMap bm, int toStart) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int64_t k = mb.block*blockDim.x + threadIdx.x;
+  if (k >= NSTATE*M.n) return;
+  if (toStart) M.S0[k] = M.S[k];
+  else M.S[k] = M.S0[k];
+}
+
+int copy_state(Batch& b, bool toStart) {
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(batch_map_items(b, [](const Problem& p) { return (int64_t)NSTATE*p.n; }, 256, &bm, &grid));
+  if (grid) { copy_state_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm, toStart ? 1 : 0); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "state copy");
+}
+
 int set_state_impl(Problem& p, const double* pos, const double* vel, const double* mass, const double* rho,
                    const double* eps, const double* H, bool device) {
   SPH_TRY(upload_aos(p, pos, 3, S_X, device));
@@ -246,135 +271,363 @@ int set_state_impl(Problem& p, const double* pos, const double* vel, const doubl
   SPH_TRY(upload_aos(p, H, 6, S_H, device));
   // initializeProblemStartup: omega = 1, P and cs from the EOS.
   fill_kernel<<<grid1(p.n), 256, 0, p.stream>>>(p.S + (int64_t)S_OMEGA*p.n, p.n, 1.0); ++p.launches;
-  launch_eos(p);
+  SPH_TRY(launch_eos(solo(&p)));
   check_state_kernel<<<grid1(p.n), 256, 0, p.stream>>>(p.S, p.n, p.d_err); ++p.launches;
   SPH_CHECK(cudaGetLastError());
-  SPH_TRY(check_device_error(p, "set_state"));
+  SPH_TRY(batch_check_errors(solo(&p), "set_state"));
   p.haveNbrs = false;
   p.crkVolumeReady = false;
   return SPHGPU_OK;
 }
 
-// CRKSPH volume: CRKSumVolume or mass/density (records must be packed).
-void crk_volume(Problem& p) {
-  if (p.cfg.crkVolumeType == SPHGPU_CRK_SUMVOLUME) launch_crk_sum_volume(p);
-  else launch_crk_volume_from_density(p);
+bool anyMember(const Batch& b, bool (*pred)(const Problem&)) {
+  for (const Problem* p : b.mem) if (pred(*p)) return true;
+  return false;
+}
+bool isCrkP(const Problem& p) { return p.prm.hydro == SPHGPU_HYDRO_CRKSPH; }
+bool needsStartupVolume(const Problem& p) { return isCrkP(p) && !p.crkVolumeReady; }
+bool isMixedSph(const Problem& p) { return !isCrkP(p) && p.cfg.precision == SPHGPU_PRECISION_MIXED; }
+bool isMixedCrk(const Problem& p) { return isCrkP(p) && p.cfg.precision == SPHGPU_PRECISION_MIXED; }
+bool hasGradh(const Problem& p) { return !isCrkP(p) && p.prm.gradh; }
+
+// CRKSPH volume (CRKSumVolume or mass/density) of the CRKSPH members;
+// `startupOnly` restricts it to members that have none yet.
+int crk_volume(Batch& b, bool startupOnly) {
+  SPH_TRY(launch_crk_sum_volume(b, startupOnly));
+  SPH_TRY(launch_crk_volume_from_density(b, startupOnly));
+  return SPHGPU_OK;
 }
 
-int build_neighbors_impl(Problem& p) {
-  SPH_TRY(build_ghosts(p));
-  SPH_TRY(build_cells_and_csr(p));
-  SPH_TRY(check_device_error(p, "build_neighbors"));
-  p.haveNbrs = true;
-  if (p.prm.hydro == SPHGPU_HYDRO_CRKSPH) {
-    SPH_TRY(crk_prepare(p));
-    if (!p.crkVolumeReady) {
-      // CRKSPHHydroBase::initializeProblemStartup (src/CRKSPH/CRKSPHHydroBase.cc:279-300)
-      pack_records(p);
-      crk_volume(p);
-      p.crkVolumeReady = true;
+// Ghosts and connectivity of every member (Integrator::setGhostNodes +
+// ConnectivityMap::computeConnectivity), then the CRKSPH start-up volume
+// (CRKSPHHydroBase::initializeProblemStartup, src/CRKSPH/CRKSPHHydroBase.cc:279-300).
+int build_neighbors_impl(Batch& b) {
+  SPH_TRY(build_connectivity(b));
+  for (Problem* p : b.mem) p->haveNbrs = true;
+  if (anyMember(b, isCrkP)) {
+    SPH_TRY(crk_prepare(b));
+    if (anyMember(b, needsStartupVolume)) {
+      SPH_TRY(pack_records(b));
+      SPH_TRY(crk_volume(b, true));
+      for (Problem* p : b.mem) if (isCrkP(*p)) p->crkVolumeReady = true;
     }
   }
   return SPHGPU_OK;
 }
 
 // Physics::initialize: grad-h (SPH) or the CRKSPH moments and corrections.
-int initialize_impl(Problem& p) {
-  if (p.prm.hydro == SPHGPU_HYDRO_CRKSPH) {
-    SPH_TRY(crk_prepare(p));
-    launch_crk_initialize(p);
-  } else if (p.prm.gradh) {
-    launch_gradh(p);
-    pack_records(p);
+int initialize_impl(Batch& b) {
+  if (anyMember(b, isCrkP)) {
+    SPH_TRY(crk_prepare(b));
+    SPH_TRY(launch_crk_initialize(b));
+  }
+  if (anyMember(b, hasGradh)) {
+    SPH_TRY(launch_gradh(b));
+    SPH_TRY(pack_records(b, PACK_FOR_EVAL));
   }
   return cuda_status(cudaGetLastError(), "initialize");
 }
 
 // Physics::finalize: CRK volumes then the summed density, or the SPH sum.
-void finalize_impl(Problem& p) {
-  if (p.prm.hydro == SPHGPU_HYDRO_CRKSPH) {
-    crk_volume(p);
-    if (p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM) launch_crk_sum_density(p);
-  } else if (p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM) {
-    launch_sum_density(p);
+int finalize_impl(Batch& b) {
+  if (anyMember(b, isCrkP)) {
+    SPH_TRY(crk_volume(b, false));
+    SPH_TRY(launch_crk_sum_density(b));
   }
-}
-
-int require_nbrs(Problem& p) {
-  if (!p.haveNbrs) { set_error("connectivity not built (call sphgpu_build_neighbors)"); return SPHGPU_ERR_STATE; }
+  SPH_TRY(launch_sum_density(b));
   return SPHGPU_OK;
 }
 
-int launch_eval(Problem& p) {
-  if (p.prm.hydro == SPHGPU_HYDRO_CRKSPH) {
-    SPH_TRY(crk_prepare(p));
-    launch_crk_eval(p);
-  } else if (p.cfg.precision == SPHGPU_PRECISION_MIXED) {
-    SPH_TRY(prepare_mixed(p));
-    launch_eval_sph_mixed(p);
-  } else {
-    launch_eval_sph_fp64(p);
+int require_nbrs(Batch& b) {
+  for (Problem* p : b.mem)
+    if (!p->haveNbrs) { set_error("connectivity not built (call sphgpu_build_neighbors)"); return SPHGPU_ERR_STATE; }
+  return SPHGPU_OK;
+}
+
+int launch_eval(Batch& b) {
+  if (anyMember(b, isCrkP)) {
+    SPH_TRY(crk_prepare(b));
+    SPH_TRY(launch_crk_eval(b));
+    if (anyMember(b, isMixedCrk)) {
+      SPH_TRY(prepare_mixed(b));
+      SPH_TRY(launch_crk_eval_mixed(b));
+    }
   }
+  if (anyMember(b, isMixedSph)) {
+    SPH_TRY(prepare_mixed(b));
+    SPH_TRY(launch_eval_sph_mixed(b));
+  }
+  SPH_TRY(launch_eval_sph_fp64(b));
   return cuda_status(cudaGetLastError(), "evaluate");
 }
 
-// CheapSynchronousRK2::step.
-int step_impl(Problem& p) {
-  double* d_dt = p.d_scal + 12;
-  double* d_lastDt = p.d_scal + 13;
-  // preStepInitialize: ghosts + connectivity every cycle, then ghost state.
-  SPH_TRY(build_neighbors_impl(p));
-  pack_records(p);
-  // selectDt with the previous derivatives, state at the step start.
-  launch_select_dt(p, d_dt, d_lastDt);
-  // state0 copy
-  SPH_CHECK(cudaMemcpyAsync(p.S0, p.S, sizeof(double)*NSTATE*(size_t)p.n, cudaMemcpyDeviceToDevice, p.stream));
+// CheapSynchronousRK2::step for every member, each with its own dt.
+// The part of the step after the connectivity: no host synchronisation and
+// no allocation, so it can be captured as a CUDA graph.
+int step_after_connectivity(Batch& b) {
+  // selectDt with the previous derivatives, state at the step start
+  // (reads the state and derivatives directly: no records needed yet).
+  SPH_TRY(launch_select_dt(b));
+  SPH_TRY(copy_state(b, true));                  // state0
   // trial advance to the mid point (updateAsIncrement for every policy)
-  launch_update(p, d_dt, 0.5, true);
-  pack_records(p);
+  SPH_TRY(launch_update(b, 0.5, true));
+  SPH_TRY(pack_records(b, PACK_FOR_EVAL));
   // initializeDerivatives + derivs.Zero + evaluateDerivatives at the mid point
-  SPH_TRY(initialize_impl(p));
-  SPH_TRY(launch_eval(p));
+  SPH_TRY(initialize_impl(b));
+  SPH_TRY(launch_eval(b));
   // full step from state0 with the mid-point derivatives
-  SPH_CHECK(cudaMemcpyAsync(p.S, p.S0, sizeof(double)*NSTATE*(size_t)p.n, cudaMemcpyDeviceToDevice, p.stream));
-  if (p.prm.compatible) launch_compatible_energy(p, d_dt, 1.0);
-  launch_update(p, d_dt, 1.0, false);
+  SPH_TRY(copy_state(b, false));
+  SPH_TRY(launch_compatible_energy(b, 1.0));
+  SPH_TRY(launch_update(b, 1.0, false));
   // applyGhostBoundaries; postStepFinalize (sum density); enforceBoundaries
-  pack_records(p);
-  finalize_impl(p);
-  launch_enforce_boundaries(p);
-  SPH_CHECK(cudaMemcpyAsync(d_lastDt, d_dt, sizeof(double), cudaMemcpyDeviceToDevice, p.stream));
-  SPH_CHECK(cudaGetLastError());
-  double dt = 0.0;
-  SPH_CHECK(cudaMemcpyAsync(&dt, d_dt, sizeof(double), cudaMemcpyDeviceToHost, p.stream));
-  SPH_TRY(check_device_error(p, "step_rk2"));
-  p.time += dt;
-  p.lastDt = dt;
-  p.cycle += 1;
-  p.haveDerivs = true;
+  SPH_TRY(pack_records(b, PACK_FOR_FINALIZE));
+  SPH_TRY(finalize_impl(b));
+  SPH_TRY(launch_enforce_boundaries(b));
+  SPH_TRY(launch_finish_step(b));
   return SPHGPU_OK;
+}
+
+// A key of everything the captured graph depends on: buffer addresses and
+// capacities, sizes fixed per problem, the schedules.
+uint64_t graph_key(const Batch& b) {
+  uint64_t h = 1469598103934665603ULL;
+  auto mix = [&](uint64_t v) { h ^= v; h *= 1099511628211ULL; };
+  mix(b.mem.size());
+  mix((uint64_t)b.evalThreads);
+  for (const Problem* p : b.mem) {
+    const void* ptrs[] = {p->S, p->S0, p->D, p->K, p->rec, p->crec, p->mrec, p->groot, p->gcode, p->counts,
+                          p->offsets, p->nbr, p->pacc, p->d_scal, p->d_red, p->d_err, p->coefF, p};
+    for (const void* q : ptrs) mix((uint64_t)(uintptr_t)q);
+    mix((uint64_t)p->n); mix((uint64_t)p->gcap); mix((uint64_t)p->ecap); mix((uint64_t)p->candcap);
+  }
+  return h;
+}
+
+int enable_graph(Batch& b) {
+  if (b.sideStream == nullptr) SPH_CHECK(cudaStreamCreateWithFlags(&b.sideStream, cudaStreamNonBlocking));
+  if (b.memGraphEvent == nullptr) SPH_CHECK(cudaEventCreateWithFlags(&b.memGraphEvent, cudaEventDisableTiming));
+  if (b.d_mapArena == nullptr) {
+    b.mapArenaCap = 1 << 18;
+    SPH_CHECK(cudaMalloc(&b.d_mapArena, sizeof(int32_t)*b.mapArenaCap));
+  }
+  return SPHGPU_OK;
+}
+
+// Descriptors of this step into the slot the captured graph reads.
+int upload_graph_descriptors(Batch& b) {
+  const int nm = (int)b.mem.size();
+  if (nm > b.memGraphCap) {
+    cudaStreamSynchronize(b.stream);
+    cudaFree(b.d_memGraph); cudaFreeHost(b.h_memGraph);
+    b.d_memGraph = nullptr; b.h_memGraph = nullptr;
+    b.memGraphCap = nm + 16;
+    if (cudaMalloc(&b.d_memGraph, sizeof(Member)*b.memGraphCap) != cudaSuccess ||
+        cudaMallocHost(&b.h_memGraph, sizeof(Member)*b.memGraphCap) != cudaSuccess) {
+      b.memGraphCap = 0;
+      set_error("graph descriptor allocation failed");
+      return SPHGPU_ERR_NOMEM;
+    }
+  }
+  SPH_CHECK(cudaEventSynchronize(b.memGraphEvent));
+  for (int m = 0; m < nm; ++m) b.h_memGraph[m] = describe_member(*b.mem[m]);
+  SPH_CHECK(cudaMemcpyAsync(b.d_memGraph, b.h_memGraph, sizeof(Member)*nm, cudaMemcpyHostToDevice, b.stream));
+  SPH_CHECK(cudaEventRecord(b.memGraphEvent, b.stream));
+  b.d_mem = b.d_memGraph;
+  b.memDirty = false;
+  return SPHGPU_OK;
+}
+
+int capture_step(Batch& b) {
+  if (b.graphExec) { cudaGraphExecDestroy(b.graphExec); b.graphExec = nullptr; }
+  b.mapArenaPos = 0;
+  const int64_t l0 = b.launches;
+  std::vector<int64_t> m0;
+  for (Problem* p : b.mem) m0.push_back(p->launches);
+  SPH_CHECK(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeRelaxed));
+  b.capturing = true;
+  b.capacityGrids = true;
+  const int rc = step_after_connectivity(b);
+  b.capturing = false;
+  b.capacityGrids = false;
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(b.stream, &graph);
+  // launches are counted when the graph is replayed
+  b.graphLaunches = b.launches - l0;
+  b.launches = l0;
+  for (size_t m = 0; m < b.mem.size(); ++m) b.mem[m]->launches = m0[m];
+  if (rc != SPHGPU_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
+  if (e != cudaSuccess) return cuda_status(e, "graph capture");
+  const cudaError_t ei = cudaGraphInstantiate(&b.graphExec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ei != cudaSuccess) { b.graphExec = nullptr; return cuda_status(ei, "graph instantiate"); }
+  b.graphKey = graph_key(b);
+  return SPHGPU_OK;
+}
+
+int step_impl(Batch& b) {
+  // preStepInitialize: ghosts + connectivity every cycle, then ghost state.
+  SPH_TRY(build_neighbors_impl(b));
+  if (b.useGraph) {
+    // everything the replay touches must exist before the capture
+    if (anyMember(b, isCrkP)) SPH_TRY(crk_prepare(b));
+    if (anyMember(b, isMixedSph) || anyMember(b, isMixedCrk)) SPH_TRY(prepare_mixed(b));
+    SPH_TRY(enable_graph(b));
+    SPH_TRY(upload_graph_descriptors(b));
+    if (b.graphExec == nullptr || graph_key(b) != b.graphKey) SPH_TRY(capture_step(b));
+    SPH_CHECK(cudaGraphLaunch(b.graphExec, b.stream));
+    b.launches += b.graphLaunches;
+    for (Problem* p : b.mem) p->launches += b.graphLaunches;
+    b.memDirty = true;     // the next eager call uploads to the rotating slots again
+  } else {
+    SPH_TRY(step_after_connectivity(b));
+  }
+  const int slots[2] = {SC_DT, -1};
+  std::vector<double> res;
+  SPH_TRY(batch_gather(b, slots, 2, res));
+  for (size_t m = 0; m < b.mem.size(); ++m) {
+    if ((int)res[2*m + 1] != 0) return batch_check_errors(b, "step_rk2");
+  }
+  for (size_t m = 0; m < b.mem.size(); ++m) {
+    Problem& p = *b.mem[m];
+    p.time += res[2*m];
+    p.lastDt = res[2*m];
+    p.cycle += 1;
+    p.haveDerivs = true;
+  }
+  return SPHGPU_OK;
+}
+
+int set_schedule_impl(Batch& b, int* nbrSchedule, const char* stage, int32_t schedule) {
+  if (std::strcmp(stage, "neighbor walk") == 0) {
+    if (schedule < NBR_SCHEDULE_AUTO || schedule > NBR_SCHEDULE_WARP) {
+      set_error("neighbor walk schedule must be 0 (auto), 1 (thread per node) or 2 (warp per node)");
+      return SPHGPU_ERR_ARG;
+    }
+    *nbrSchedule = schedule;
+    return SPHGPU_OK;
+  }
+  if (std::strcmp(stage, "pair loop") == 0) {
+    if (schedule != 64 && schedule != 128) {
+      set_error("pair loop schedule is the threads per block: 64 or 128");
+      return SPHGPU_ERR_ARG;
+    }
+    b.evalThreads = schedule;
+    return SPHGPU_OK;
+  }
+  if (std::strcmp(stage, "neighbor filter") == 0) {
+    if (schedule != 0 && schedule != 1) {
+      set_error("neighbor filter is 0 (exact FP64 test only) or 1 (FP32 pre-test)");
+      return SPHGPU_ERR_ARG;
+    }
+    for (Problem* p : b.mem) p->nbrFilter = schedule != 0;
+    return SPHGPU_OK;
+  }
+  if (std::strcmp(stage, "step graph") == 0) {
+    if (schedule != 0 && schedule != 1) {
+      set_error("step graph is 0 (eager launches) or 1 (CUDA-graph replay)");
+      return SPHGPU_ERR_ARG;
+    }
+    b.useGraph = schedule != 0;
+    return SPHGPU_OK;
+  }
+  set_error(std::string("unknown schedule stage: ") + stage);
+  return SPHGPU_ERR_ARG;
+}
+
+// Autotuner: every candidate schedule of a stage is run on the batch's own
+// data and timed with CUDA events on the batch stream (one warm run, then the
+// median of three); the fastest is kept.  All schedules give bit-identical
+// results, so tuning changes speed only.  report = {neighbor schedule,
+// ms thread, ms warp, pair-loop threads, ms 64, ms 128, 0, 0}.
+int autotune_impl(Batch& b, double* report) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  SPH_CHECK(cudaEventCreate(&e0));
+  SPH_CHECK(cudaEventCreate(&e1));
+  auto timeit = [&](auto fn, double* ms) -> int {
+    SPH_TRY(fn());
+    double t[3];
+    for (int r = 0; r < 3; ++r) {
+      SPH_CHECK(cudaEventRecord(e0, b.stream));
+      SPH_TRY(fn());
+      SPH_CHECK(cudaEventRecord(e1, b.stream));
+      SPH_CHECK(cudaEventSynchronize(e1));
+      float f = 0.0f;
+      SPH_CHECK(cudaEventElapsedTime(&f, e0, e1));
+      t[r] = f;
+    }
+    std::sort(t, t + 3);
+    *ms = t[1];
+    return SPHGPU_OK;
+  };
+  double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int rc = SPHGPU_OK;
+  do {
+    // neighbor walk: thread per node vs warp per node
+    const int schedules[2] = {NBR_SCHEDULE_THREAD, NBR_SCHEDULE_WARP};
+    double best = 1e300;
+    int bestS = NBR_SCHEDULE_AUTO;
+    for (int k = 0; k < 2 && rc == SPHGPU_OK; ++k) {
+      b.nbrSchedule = schedules[k];
+      double ms = 0.0;
+      rc = timeit([&]() { return build_neighbors_impl(b); }, &ms);
+      out[1 + k] = ms;
+      if (ms < best) { best = ms; bestS = schedules[k]; }
+    }
+    if (rc != SPHGPU_OK) break;
+    b.nbrSchedule = bestS;
+    out[0] = bestS;
+    if ((rc = build_neighbors_impl(b)) != SPHGPU_OK) break;
+    if ((rc = pack_records(b)) != SPHGPU_OK) break;
+    if ((rc = initialize_impl(b)) != SPHGPU_OK) break;
+    // pair loop: threads per block
+    const int widths[2] = {64, 128};
+    best = 1e300;
+    int bestW = 128;
+    for (int k = 0; k < 2 && rc == SPHGPU_OK; ++k) {
+      b.evalThreads = widths[k];
+      double ms = 0.0;
+      rc = timeit([&]() { return launch_eval(b); }, &ms);
+      out[4 + k] = ms;
+      if (ms < best) { best = ms; bestW = widths[k]; }
+    }
+    b.evalThreads = bestW;
+    out[3] = bestW;
+  } while (false);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc == SPHGPU_OK && report) for (int k = 0; k < 8; ++k) report[k] = out[k];
+  return rc;
 }
 
 }  // namespace
 
+int batch_step_rk2(Batch& b) {
+  b.memDirty = true;
+  for (Problem* p : b.mem) SPH_CHECK(cudaStreamSynchronize(p->stream));
+  return step_impl(b);
+}
+
+// Device bytes a problem holds, from its buffer capacities.
+int64_t problem_bytes(const Problem& p) {
+  const int64_t n = p.n;
+  const int stagingComps = p.cfg.hydro == SPHGPU_HYDRO_CRKSPH ? 27 : 9;
+  int64_t b = 8*(2*(int64_t)NSTATE*n + (int64_t)NDERIV*n + stagingComps*n + n + NSCAL + 148*4*8) + 16;
+  b += 8*(6 + 2)*(int64_t)p.prm.W.n;                                  // tables
+  b += p.gcap*(4 + 4 + 24);                                           // groot, gcode, gpos
+  b += p.candcap*(4 + 4 + 4 + 112 + 8*RECW) + 8*(p.candcap + 1);       // counts, cidx, sortedIdx, cand, rec, offsets
+  b += p.ecap*(4 + (p.pacc ? 24 : 0));                                // nbr, pacc
+  b += p.cellcap*(8 + 4) + 8 + 8*p.blockSumsCap;
+  b += 8*(int64_t)MRECW*p.mreccap + (p.coefF ? 4*6*(int64_t)p.prm.W.n : 0);
+  b += 8*(int64_t)CRECW*p.creccap + (p.K ? 8*(int64_t)NCRK*n : 0);
+  return b;
+}
+
 int ensure_block_sums(Problem& p, int64_t nblocks) {
   if (nblocks <= p.blockSumsCap) return SPHGPU_OK;
   cudaFree(p.blockSums);
+  p.blockSums = nullptr;
   p.blockSumsCap = nblocks + 64;
   return dalloc(p.blockSums, p.blockSumsCap);
-}
-
-int exclusive_scan_i32(Problem& p, const int32_t* in, int64_t n, int64_t* out, int64_t* total) {
-  const int64_t tiles = (n + SCAN_TILE - 1)/SCAN_TILE;
-  SPH_TRY(ensure_block_sums(p, tiles + 1));
-  int64_t* dtotal = p.blockSums + tiles;
-  if (tiles > 0) scan_tile_sums_kernel<<<(unsigned)tiles, SCAN_THREADS, 0, p.stream>>>(in, n, p.blockSums); p.launches += (tiles > 0);
-  scan_sums_kernel<<<1, SCAN_THREADS, 0, p.stream>>>(p.blockSums, tiles, dtotal); ++p.launches;
-  scan_apply_kernel<<<(unsigned)(tiles > 0 ? tiles : 1), SCAN_THREADS, 0, p.stream>>>(in, n, p.blockSums, out, dtotal); ++p.launches;
-  SPH_CHECK(cudaGetLastError());
-  SPH_CHECK(cudaMemcpyAsync(total, dtotal, sizeof(int64_t), cudaMemcpyDeviceToHost, p.stream));
-  SPH_CHECK(cudaStreamSynchronize(p.stream));
-  return SPHGPU_OK;
 }
 
 // Ghost arrays and every (n + ghosts)-sized buffer; contents are preserved
@@ -403,7 +656,7 @@ int ensure_capacity_ghosts(Problem& p, int64_t need) {
   SPH_TRY(grow_preserve(p.cidx, 0, nc, p.stream));
   SPH_TRY(grow_preserve(p.sortedIdx, 0, nc, p.stream));
   cudaFree(p.cand);
-  SPH_TRY(dalloc(p.cand, 10*nc));
+  SPH_TRY(dalloc(p.cand, 14*nc));          // 64-byte records + 48-byte FP64 H
   cudaFree(p.rec);
   SPH_TRY(dalloc(p.rec, RECW*nc));
   p.candcap = nc;
@@ -431,7 +684,6 @@ using namespace sphgpu;
 
 extern "C" {
 
-struct sphgpu_problem : public Problem {};
 
 const char* sphgpu_last_error(void) { return g_last_error.c_str(); }
 
@@ -482,6 +734,7 @@ int sphgpu_create(const sphgpu_config* cfg, int64_t n_internal, sphgpu_problem**
     P.useVelMagDt = cfg->useVelocityMagnitudeForDt; P.HUpdate = cfg->HUpdate; P.densityUpdate = cfg->densityUpdate;
     P.gradh = cfg->gradhCorrection;
     P.hydro = cfg->hydro;
+    P.dtMin = cfg->dtMin; P.dtMax = cfg->dtMax; P.dtGrowth = cfg->dtGrowth;
     // periodic planes: PeriodicBoundary(plane1 = (xmin, +e_a), plane2 = (xmax, -e_a))
     for (int a = 0; a < 3; ++a) {
       P.bcs.periodic[a] = cfg->periodic[a] ? 1 : 0;
@@ -499,15 +752,21 @@ int sphgpu_create(const sphgpu_config* cfg, int64_t n_internal, sphgpu_problem**
     // widest field: Tensor (9) for SPH, the third-rank grad m2 (27) for CRKSPH
     if ((rc = dalloc(p->staging, (cfg->hydro == SPHGPU_HYDRO_CRKSPH ? 27 : 9)*n)) != SPHGPU_OK) break;
     if ((rc = dalloc(p->d_err, 4)) != SPHGPU_OK) break;
-    if ((rc = dalloc(p->d_scal, 32)) != SPHGPU_OK) break;
+    if ((rc = dalloc(p->hmaxi, n)) != SPHGPU_OK) break;
+    if ((rc = dalloc(p->d_scal, NSCAL)) != SPHGPU_OK) break;
     p->redcap = 148*4*8;
     if ((rc = dalloc(p->d_red, p->redcap)) != SPHGPU_OK) break;
     cudaMemset(p->d_err, 0, 4*sizeof(int));
     cudaMemset(p->D, 0, sizeof(double)*NDERIV*(size_t)n);
     cudaMemset(p->S, 0, sizeof(double)*NSTATE*(size_t)n);
     p->lastDt = cfg->lastDt;
-    cudaMemcpy(p->d_scal + 13, &p->lastDt, sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemset(p->d_scal, 0, sizeof(double)*NSCAL);
+    cudaMemcpy(p->d_scal + SC_LASTDT, &p->lastDt, sizeof(double), cudaMemcpyHostToDevice);
     if ((rc = ensure_capacity_ghosts(*p, n/2 + 4096)) != SPHGPU_OK) break;
+    p->solo = new (std::nothrow) Batch();
+    if (p->solo == nullptr) { set_error("host allocation failed"); rc = SPHGPU_ERR_NOMEM; break; }
+    if ((rc = batch_init(solo(p), p->stream)) != SPHGPU_OK) break;
+    p->solo->mem.push_back(p);
     if ((rc = cuda_status(cudaDeviceSynchronize(), "create")) != SPHGPU_OK) break;
   } while (false);
   if (rc != SPHGPU_OK) {
@@ -566,14 +825,14 @@ int sphgpu_get_field(sphgpu_problem* p, const char* key, double* out, int64_t co
 
 int sphgpu_build_neighbors(sphgpu_problem* p) {
   if (p == nullptr) return SPHGPU_ERR_ARG;
-  SPH_TRY(build_neighbors_impl(*p));
-  pack_records(*p);
-  return cuda_status(cudaGetLastError(), "pack_records");
+  SPH_TRY(build_neighbors_impl(solo(p)));
+  SPH_TRY(pack_records(solo(p)));
+  return batch_check_errors(solo(p), "build_neighbors");
 }
 
 int sphgpu_connectivity_size(sphgpu_problem* p, int64_t* num_ghosts, int64_t* num_entries) {
   if (p == nullptr) return SPHGPU_ERR_ARG;
-  SPH_TRY(require_nbrs(*p));
+  SPH_TRY(require_nbrs(solo(p)));
   if (num_ghosts) *num_ghosts = p->G;
   if (num_entries) *num_entries = p->E;
   return SPHGPU_OK;
@@ -581,7 +840,7 @@ int sphgpu_connectivity_size(sphgpu_problem* p, int64_t* num_ghosts, int64_t* nu
 
 int sphgpu_get_connectivity(sphgpu_problem* p, int64_t* offsets, int32_t* neighbors, int32_t* ghost_root) {
   if (p == nullptr) return SPHGPU_ERR_ARG;
-  SPH_TRY(require_nbrs(*p));
+  SPH_TRY(require_nbrs(solo(p)));
   if (offsets) SPH_CHECK(cudaMemcpyAsync(offsets, p->offsets, sizeof(int64_t)*(size_t)(p->n + 1), cudaMemcpyDeviceToHost, p->stream));
   if (neighbors && p->E) SPH_CHECK(cudaMemcpyAsync(neighbors, p->nbr, sizeof(int32_t)*(size_t)p->E, cudaMemcpyDeviceToHost, p->stream));
   if (ghost_root && p->G) SPH_CHECK(cudaMemcpyAsync(ghost_root, p->groot, sizeof(int32_t)*(size_t)p->G, cudaMemcpyDeviceToHost, p->stream));
@@ -592,17 +851,17 @@ int sphgpu_get_connectivity(sphgpu_problem* p, int64_t* offsets, int32_t* neighb
 int sphgpu_initialize(sphgpu_problem* p, double time, double dt) {
   if (p == nullptr) return SPHGPU_ERR_ARG;
   (void)time; (void)dt;
-  SPH_TRY(require_nbrs(*p));
-  pack_records(*p);
-  return initialize_impl(*p);
+  SPH_TRY(require_nbrs(solo(p)));
+  SPH_TRY(pack_records(solo(p)));
+  return initialize_impl(solo(p));
 }
 
 int sphgpu_evaluate_derivatives(sphgpu_problem* p, double time, double dt) {
   if (p == nullptr) return SPHGPU_ERR_ARG;
   (void)time; (void)dt;
-  SPH_TRY(require_nbrs(*p));
-  pack_records(*p);
-  SPH_TRY(launch_eval(*p));
+  SPH_TRY(require_nbrs(solo(p)));
+  SPH_TRY(pack_records(solo(p)));
+  SPH_TRY(launch_eval(solo(p)));
   p->haveDerivs = true;
   return SPHGPU_OK;
 }
@@ -616,29 +875,33 @@ int sphgpu_finalize_derivatives(sphgpu_problem* p, double time, double dt) {
 int sphgpu_finalize(sphgpu_problem* p, double time, double dt) {
   if (p == nullptr) return SPHGPU_ERR_ARG;
   (void)time; (void)dt;
-  SPH_TRY(require_nbrs(*p));
-  pack_records(*p);
-  finalize_impl(*p);
-  return cuda_status(cudaGetLastError(), "finalize");
+  SPH_TRY(require_nbrs(solo(p)));
+  SPH_TRY(pack_records(solo(p)));
+  return finalize_impl(solo(p));
 }
 
 int sphgpu_dt(sphgpu_problem* p, double* dt_out) {
   if (p == nullptr || dt_out == nullptr) return SPHGPU_ERR_ARG;
-  SPH_TRY(require_nbrs(*p));
-  double* bits = p->d_scal + 14;
-  launch_dt(*p, bits);
-  SPH_CHECK(cudaGetLastError());
-  double minDt = 0.0;
-  SPH_CHECK(cudaMemcpyAsync(&minDt, bits, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
-  SPH_CHECK(cudaStreamSynchronize(p->stream));
-  *dt_out = p->cfg.cfl*minDt;
+  SPH_TRY(require_nbrs(solo(p)));
+  SPH_TRY(launch_dt(solo(p), SC_DTOUT));
+  const int slot = SC_DTOUT;
+  std::vector<double> v;
+  SPH_TRY(batch_gather(solo(p), &slot, 1, v));
+  *dt_out = p->cfg.cfl*v[0];
   return SPHGPU_OK;
 }
 
 int sphgpu_step_rk2(sphgpu_problem* p, double* time, int64_t nsteps, double* last_dt) {
   if (p == nullptr || nsteps < 0) return SPHGPU_ERR_ARG;
   if (time) p->time = *time;
-  for (int64_t s = 0; s < nsteps; ++s) SPH_TRY(step_impl(*p));
+  for (int64_t s = 0; s < nsteps; ++s) SPH_TRY(step_impl(solo(p)));
+  if (time) *time = p->time;
+  if (last_dt) *last_dt = p->lastDt;
+  return SPHGPU_OK;
+}
+
+int sphgpu_time(sphgpu_problem* p, double* time, double* last_dt) {
+  if (p == nullptr) return SPHGPU_ERR_ARG;
   if (time) *time = p->time;
   if (last_dt) *last_dt = p->lastDt;
   return SPHGPU_OK;
@@ -646,16 +909,18 @@ int sphgpu_step_rk2(sphgpu_problem* p, double* time, int64_t nsteps, double* las
 
 int sphgpu_conservation(sphgpu_problem* p, double out[8]) {
   if (p == nullptr || out == nullptr) return SPHGPU_ERR_ARG;
-  launch_conservation(*p, p->d_scal + 16);
-  SPH_CHECK(cudaGetLastError());
-  SPH_CHECK(cudaMemcpyAsync(out, p->d_scal + 16, sizeof(double)*8, cudaMemcpyDeviceToHost, p->stream));
-  SPH_CHECK(cudaStreamSynchronize(p->stream));
+  SPH_TRY(launch_conservation(solo(p)));
+  const int slots[8] = {SC_CONS, SC_CONS + 1, SC_CONS + 2, SC_CONS + 3, SC_CONS + 4, SC_CONS + 5, SC_CONS + 6,
+                        SC_CONS + 7};
+  std::vector<double> v;
+  SPH_TRY(batch_gather(solo(p), slots, 8, v));
+  for (int c = 0; c < 8; ++c) out[c] = v[c];
   return SPHGPU_OK;
 }
 
 int sphgpu_num_pairs(sphgpu_problem* p, int64_t* pairs) {
   if (p == nullptr || pairs == nullptr) return SPHGPU_ERR_ARG;
-  SPH_TRY(require_nbrs(*p));
+  SPH_TRY(require_nbrs(solo(p)));
   *pairs = p->pairs;
   return SPHGPU_OK;
 }
@@ -668,16 +933,7 @@ int sphgpu_kernel_launches(sphgpu_problem* p, int64_t* launches) {
 
 int sphgpu_set_schedule(sphgpu_problem* p, const char* stage, int32_t schedule) {
   if (p == nullptr || stage == nullptr) return SPHGPU_ERR_ARG;
-  if (std::strcmp(stage, "neighbor walk") == 0) {
-    if (schedule < NBR_SCHEDULE_AUTO || schedule > NBR_SCHEDULE_WARP) {
-      set_error("neighbor walk schedule must be 0 (auto), 1 (thread per node) or 2 (warp per node)");
-      return SPHGPU_ERR_ARG;
-    }
-    p->nbrSchedule = schedule;
-    return SPHGPU_OK;
-  }
-  set_error(std::string("unknown schedule stage: ") + stage);
-  return SPHGPU_ERR_ARG;
+  return set_schedule_impl(*p->solo, &p->nbrSchedule, stage, schedule);
 }
 
 int sphgpu_get_schedule(sphgpu_problem* p, const char* stage, int32_t* schedule) {
@@ -686,14 +942,27 @@ int sphgpu_get_schedule(sphgpu_problem* p, const char* stage, int32_t* schedule)
     *schedule = p->lastNbrSchedule;
     return SPHGPU_OK;
   }
+  if (std::strcmp(stage, "pair loop") == 0) {
+    *schedule = p->solo->evalThreads;
+    return SPHGPU_OK;
+  }
+  if (std::strcmp(stage, "step graph") == 0) {
+    *schedule = p->solo->useGraph ? 1 : 0;
+    return SPHGPU_OK;
+  }
   set_error(std::string("unknown schedule stage: ") + stage);
   return SPHGPU_ERR_ARG;
+}
+
+int sphgpu_autotune(sphgpu_problem* p, double report[8]) {
+  if (p == nullptr) return SPHGPU_ERR_ARG;
+  return autotune_impl(solo(p), report);
 }
 
 int sphgpu_synchronize(sphgpu_problem* p) {
   if (p == nullptr) return SPHGPU_ERR_ARG;
   SPH_CHECK(cudaStreamSynchronize(p->stream));
-  return check_device_error(*p, "synchronize");
+  return batch_check_errors(solo(p), "synchronize");
 }
 
 int sphgpu_get_stream(sphgpu_problem* p, void** stream) {
@@ -708,6 +977,123 @@ int sphgpu_set_stream(sphgpu_problem* p, void* stream) {
   if (p->ownStream) cudaStreamDestroy(p->stream);
   p->stream = (cudaStream_t)stream;
   p->ownStream = false;
+  p->solo->stream = p->stream;
+  return SPHGPU_OK;
+}
+
+// ---------------------------------------------------------------- batches
+
+namespace {
+
+// A member may have pending work on its own stream: order the batch after it.
+int batch_begin(Batch& b) {
+  // members' buffers may have moved under their own calls since the last upload
+  b.memDirty = true;
+  for (Problem* p : b.mem) SPH_CHECK(cudaStreamSynchronize(p->stream));
+  return SPHGPU_OK;
+}
+
+}  // namespace
+
+int sphgpu_batch_create(sphgpu_problem* const* members, int32_t count, sphgpu_batch** out) {
+  if (members == nullptr || out == nullptr || count <= 0) { set_error("sphgpu_batch_create: bad arguments"); return SPHGPU_ERR_ARG; }
+  *out = nullptr;
+  int dev = 0;
+  SPH_CHECK(cudaGetDevice(&dev));
+  for (int32_t m = 0; m < count; ++m) {
+    if (members[m] == nullptr) { set_error("sphgpu_batch_create: null member"); return SPHGPU_ERR_ARG; }
+    if (members[m]->device != dev) { set_error("sphgpu_batch_create: members must live on the current device"); return SPHGPU_ERR_ARG; }
+    for (int32_t k = 0; k < m; ++k)
+      if (members[k] == members[m]) { set_error("sphgpu_batch_create: a problem appears twice"); return SPHGPU_ERR_ARG; }
+  }
+  sphgpu_batch* b = new (std::nothrow) sphgpu_batch();
+  if (b == nullptr) { set_error("host allocation failed"); return SPHGPU_ERR_NOMEM; }
+  cudaStream_t st = nullptr;
+  int rc = cuda_status(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "batch stream");
+  if (rc == SPHGPU_OK) {
+    b->ownStream = true;
+    rc = batch_init(*b, st);
+    b->ownStream = true;
+  }
+  if (rc != SPHGPU_OK) {
+    if (st && !b->stream) cudaStreamDestroy(st);
+    batch_free(*b);
+    delete b;
+    return rc;
+  }
+  for (int32_t m = 0; m < count; ++m) b->mem.push_back(members[m]);
+  b->memDirty = true;
+  *out = b;
+  return SPHGPU_OK;
+}
+
+void sphgpu_batch_destroy(sphgpu_batch* b) {
+  if (b == nullptr) return;
+  batch_free(*b);
+  delete b;
+}
+
+int sphgpu_batch_size(sphgpu_batch* b, int32_t* count) {
+  if (b == nullptr || count == nullptr) return SPHGPU_ERR_ARG;
+  *count = (int32_t)b->mem.size();
+  return SPHGPU_OK;
+}
+
+int sphgpu_batch_build_neighbors(sphgpu_batch* b) {
+  if (b == nullptr) return SPHGPU_ERR_ARG;
+  SPH_TRY(batch_begin(*b));
+  SPH_TRY(build_neighbors_impl(*b));
+  SPH_TRY(pack_records(*b));
+  return batch_check_errors(*b, "batch build_neighbors");
+}
+
+int sphgpu_batch_evaluate_derivatives(sphgpu_batch* b) {
+  if (b == nullptr) return SPHGPU_ERR_ARG;
+  SPH_TRY(batch_begin(*b));
+  SPH_TRY(require_nbrs(*b));
+  SPH_TRY(pack_records(*b));
+  SPH_TRY(initialize_impl(*b));
+  SPH_TRY(launch_eval(*b));
+  for (Problem* p : b->mem) p->haveDerivs = true;
+  return batch_check_errors(*b, "batch evaluate_derivatives");
+}
+
+int sphgpu_batch_step_rk2(sphgpu_batch* b, int64_t nsteps) {
+  if (b == nullptr || nsteps < 0) return SPHGPU_ERR_ARG;
+  SPH_TRY(batch_begin(*b));
+  for (int64_t s = 0; s < nsteps; ++s) SPH_TRY(step_impl(*b));
+  return SPHGPU_OK;
+}
+
+int sphgpu_batch_pairs(sphgpu_batch* b, int64_t* pairs) {
+  if (b == nullptr || pairs == nullptr) return SPHGPU_ERR_ARG;
+  SPH_TRY(require_nbrs(*b));
+  int64_t t = 0;
+  for (Problem* p : b->mem) t += p->pairs;
+  *pairs = t;
+  return SPHGPU_OK;
+}
+
+int sphgpu_batch_kernel_launches(sphgpu_batch* b, int64_t* launches) {
+  if (b == nullptr || launches == nullptr) return SPHGPU_ERR_ARG;
+  *launches = b->launches;
+  return SPHGPU_OK;
+}
+
+int sphgpu_batch_set_schedule(sphgpu_batch* b, const char* stage, int32_t schedule) {
+  if (b == nullptr || stage == nullptr) return SPHGPU_ERR_ARG;
+  return set_schedule_impl(*b, &b->nbrSchedule, stage, schedule);
+}
+
+int sphgpu_batch_autotune(sphgpu_batch* b, double report[8]) {
+  if (b == nullptr) return SPHGPU_ERR_ARG;
+  SPH_TRY(batch_begin(*b));
+  return autotune_impl(*b, report);
+}
+
+int sphgpu_batch_get_stream(sphgpu_batch* b, void** stream) {
+  if (b == nullptr || stream == nullptr) return SPHGPU_ERR_ARG;
+  *stream = (void*)b->stream;
   return SPHGPU_OK;
 }
 

@@ -21,11 +21,6 @@ namespace sphgpu {
 
 namespace {
 
-inline int nblk(int64_t work, int threads) {
-  int64_t b = (work + threads - 1)/threads;
-  return (int)(b < 1 ? 1 : b);
-}
-
 __device__ __forceinline__ double ldg(const double* p) { return __ldg(p); }
 __device__ __forceinline__ double& el(V3& v, int i) { return (&v.x)[i]; }
 __device__ __forceinline__ double el(const V3& v, int i) { return (&v.x)[i]; }
@@ -65,9 +60,19 @@ __device__ __forceinline__ CRec loadCRec(const double* crec, int64_t k) {
   return R;
 }
 
-__global__ void pack_crk_records_kernel(const double* S, const double* K, int64_t n, const int32_t* groot,
-                                        const uint32_t* gcode, int64_t ntot, BoxBCs bcs, double* crec) {
-  for (int64_t k = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; k < ntot; k += (int64_t)gridDim.x*blockDim.x) {
+__global__ void __launch_bounds__(256) pack_crk_records_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const double* S = MB.S;
+  const double* K = MB.K;
+  const BoxBCs& bcs = MB.prm.bcs;
+  const int32_t* groot = MB.groot;
+  const uint32_t* gcode = MB.gcode;
+  double* crec = MB.crec;
+  {
+    const int64_t k = mb.block*blockDim.x + threadIdx.x;
+    if (k >= n + scalI(MB.scal, SC_G)) return;
     const int64_t r = k < n ? k : groot[k - n];
     V3 x{S[S_X*n + r], S[S_Y*n + r], S[S_Z*n + r]};
     if (k >= n) x = ghostPosition(bcs, x, gcode[k - n]);
@@ -103,10 +108,17 @@ __device__ __forceinline__ Sym recH(const double* rec, int64_t j) {
 }
 
 // ---------------------------------------------------------------- volumes
-__global__ void crk_sum_volume_kernel(Params P, const double* rec, int64_t n, const int64_t* offsets,
-                                      const int32_t* nbr, double* S) {
-  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) crk_sum_volume_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const Params& P = MB.prm;
+  const double* rec = MB.rec;
+  const int64_t* offsets = MB.offsets;
+  const int32_t* nbr = MB.nbr;
+  double* S = MB.S;
   const V3 ri = recPos(rec, i);
   const Sym Hi = recH(rec, i);
   const double Hdeti = ldg(rec + i*RECW + R_HDET);
@@ -122,16 +134,28 @@ __global__ void crk_sum_volume_kernel(Params P, const double* rec, int64_t n, co
   S[S_VOL*n + i] = dmin(etaVolMax/Hdeti, 1.0/vol);
 }
 
-__global__ void crk_volume_from_density_kernel(int64_t n, double* S) {
-  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) crk_volume_from_density_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
+  double* S = MB.S;
   S[S_VOL*n + i] = S[S_M*n + i]/S[S_RHO*n + i];
 }
 
-__global__ void crk_sum_density_kernel(Params P, const double* rec, int64_t n, const int64_t* offsets,
-                                       const int32_t* nbr, const int32_t* groot, double* S) {
-  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) crk_sum_density_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const Params& P = MB.prm;
+  const double* rec = MB.rec;
+  const int64_t* offsets = MB.offsets;
+  const int32_t* nbr = MB.nbr;
+  const int32_t* groot = MB.groot;
+  double* S = MB.S;
   const double mi = S[S_M*n + i], Vi = S[S_VOL*n + i];
   const double Hdeti = ldg(rec + i*RECW + R_HDET);
   const V3 ri = recPos(rec, i);
@@ -153,12 +177,19 @@ __global__ void crk_sum_density_kernel(Params P, const double* rec, int64_t n, c
 }
 
 // ---------------------------------------------------------------- moments + corrections
-__global__ void __launch_bounds__(128) crk_moments_corrections_kernel(Params P, const double* rec, int64_t n,
-                                                                      const int64_t* offsets, const int32_t* nbr,
-                                                                      const int32_t* groot, const double* S,
-                                                                      double* K) {
-  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) crk_moments_corrections_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const Params& P = MB.prm;
+  const double* rec = MB.rec;
+  const int64_t* offsets = MB.offsets;
+  const int32_t* nbr = MB.nbr;
+  const int32_t* groot = MB.groot;
+  const double* S = MB.S;
+  double* K = MB.K;
   const V3 ri = recPos(rec, i);
   const Sym Hi = recH(rec, i);
   const double Hdeti = ldg(rec + i*RECW + R_HDET);
@@ -292,12 +323,21 @@ __device__ __forceinline__ void crkKernel(const TableDev& T, const V3& rij, cons
   }
 }
 
-template<bool XSPH, bool COMPAT>
-__global__ void __launch_bounds__(128) crk_eval_kernel(Params P, const double* crec, int64_t n,
-                                                       const int64_t* offsets, const int32_t* nbr, double* D,
-                                                       double* K, double* pacc, int64_t ecap) {
-  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+template<bool XSPH, bool COMPAT, bool SOLO>
+__global__ void __launch_bounds__(128) crk_eval_kernel(const Member* mem, BlockMap bm, const Member single) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = SOLO ? single : mem[mb.m];   // one member: read from the kernel parameters
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const Params& P = MB.prm;
+  const double* crec = MB.crec;
+  const int64_t* offsets = MB.offsets;
+  const int32_t* nbr = MB.nbr;
+  double* D = MB.D;
+  double* K = MB.K;
+  double* pacc = MB.pacc;
+  const int64_t ecap = MB.ecap;
   const CRec I = loadCRec(crec, i);
   const double Cl = P.Cl*(0.5*(1.0 + 1.0)*1.0);
   const double Cq = P.Cq*(0.5*(1.0 + 1.0)*1.0);
@@ -422,63 +462,112 @@ __global__ void __launch_bounds__(128) crk_eval_kernel(Params P, const double* c
 
 }  // namespace
 
-int crk_prepare(Problem& p) {
-  if (p.K == nullptr) {
-    if (cudaMalloc(&p.K, sizeof(double)*NCRK*(size_t)p.n) != cudaSuccess) {
-      set_error("CRKSPH field allocation failed");
-      return SPHGPU_ERR_NOMEM;
+int crk_prepare(Batch& b) {
+  for (Problem* pp : b.mem) {
+    Problem& p = *pp;
+    if (p.prm.hydro != SPHGPU_HYDRO_CRKSPH) continue;
+    if (p.K == nullptr) {
+      if (cudaMalloc(&p.K, sizeof(double)*NCRK*(size_t)p.n) != cudaSuccess) {
+        set_error("CRKSPH field allocation failed");
+        return SPHGPU_ERR_NOMEM;
+      }
+      cudaMemsetAsync(p.K, 0, sizeof(double)*NCRK*(size_t)p.n, b.stream);
+      b.memDirty = true;
     }
-    cudaMemsetAsync(p.K, 0, sizeof(double)*NCRK*(size_t)p.n, p.stream);
-  }
-  if (p.candcap > p.creccap) {
-    cudaFree(p.crec);
-    p.crec = nullptr;
-    if (cudaMalloc(&p.crec, sizeof(double)*CRECW*(size_t)p.candcap) != cudaSuccess) {
-      set_error("CRKSPH record allocation failed");
-      return SPHGPU_ERR_NOMEM;
+    if (p.candcap > p.creccap) {
+      cudaStreamSynchronize(b.stream);
+      cudaFree(p.crec);
+      p.crec = nullptr;
+      if (cudaMalloc(&p.crec, sizeof(double)*CRECW*(size_t)p.candcap) != cudaSuccess) {
+        p.creccap = 0;
+        set_error("CRKSPH record allocation failed");
+        return SPHGPU_ERR_NOMEM;
+      }
+      p.creccap = p.candcap;
+      b.memDirty = true;
     }
-    p.creccap = p.candcap;
   }
+  if (b.memDirty) SPH_TRY(batch_upload(b));
   return SPHGPU_OK;
 }
 
-void launch_crk_sum_volume(Problem& p) {
-  crk_sum_volume_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr, p.S);
-  ++p.launches;
+namespace {
+
+bool isCrk(const Problem& p) { return p.prm.hydro == SPHGPU_HYDRO_CRKSPH; }
+bool isCrkFp64(const Problem& p) { return isCrk(p) && p.cfg.precision == SPHGPU_PRECISION_FP64; }
+
+int crk_nodes(Batch& b, int threads, BlockMap* bm, unsigned* grid, bool (*pred)(const Problem&)) {
+  return batch_map_items(b, [&](const Problem& p) { return pred(p) ? p.n : (int64_t)0; }, threads, bm, grid);
 }
 
-void launch_crk_volume_from_density(Problem& p) {
-  crk_volume_from_density_kernel<<<nblk(p.n, 256), 256, 0, p.stream>>>(p.n, p.S);
-  ++p.launches;
+bool crkSumVolume(const Problem& p) { return isCrk(p) && p.cfg.crkVolumeType == SPHGPU_CRK_SUMVOLUME; }
+bool crkMassOverDensity(const Problem& p) { return isCrk(p) && p.cfg.crkVolumeType != SPHGPU_CRK_SUMVOLUME; }
+bool crkSumDensity(const Problem& p) { return isCrk(p) && p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM; }
+
+}  // namespace
+
+int launch_crk_sum_volume(Batch& b, bool startupOnly) {
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) {
+    return crkSumVolume(p) && !(startupOnly && p.crkVolumeReady) ? p.n : (int64_t)0; }, 128, &bm, &grid));
+  if (grid) { crk_sum_volume_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "CRK sum volume");
 }
 
-void launch_crk_sum_density(Problem& p) {
-  crk_sum_density_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr, p.groot, p.S);
-  ++p.launches;
+int launch_crk_volume_from_density(Batch& b, bool startupOnly) {
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) {
+    return crkMassOverDensity(p) && !(startupOnly && p.crkVolumeReady) ? p.n : (int64_t)0; }, 256, &bm, &grid));
+  if (grid) { crk_volume_from_density_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "CRK volume");
 }
 
-void launch_crk_initialize(Problem& p) {
-  crk_moments_corrections_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr,
-                                                                       p.groot, p.S, p.K);
-  ++p.launches;
+int launch_crk_sum_density(Batch& b) {
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(crk_nodes(b, 128, &bm, &grid, crkSumDensity));
+  if (grid) { crk_sum_density_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "CRK sum density");
 }
 
-void launch_crk_eval(Problem& p) {
-  const int64_t ntot = p.n + p.G;
-  int blocks = nblk(ntot, 256);
-  if (blocks > 148*64) blocks = 148*64;
-  pack_crk_records_kernel<<<blocks, 256, 0, p.stream>>>(p.S, p.K, p.n, p.groot, p.gcode, ntot, p.prm.bcs, p.crec);
-  ++p.launches;
-  const int nb = nblk(p.n, 128);
-  const bool xsph = p.prm.XSPH != 0, comp = p.prm.compatible != 0;
-  if (xsph) {
-    if (comp) crk_eval_kernel<true, true><<<nb, 128, 0, p.stream>>>(p.prm, p.crec, p.n, p.offsets, p.nbr, p.D, p.K, p.pacc, p.ecap);
-    else crk_eval_kernel<true, false><<<nb, 128, 0, p.stream>>>(p.prm, p.crec, p.n, p.offsets, p.nbr, p.D, p.K, p.pacc, p.ecap);
-  } else {
-    if (comp) crk_eval_kernel<false, true><<<nb, 128, 0, p.stream>>>(p.prm, p.crec, p.n, p.offsets, p.nbr, p.D, p.K, p.pacc, p.ecap);
-    else crk_eval_kernel<false, false><<<nb, 128, 0, p.stream>>>(p.prm, p.crec, p.n, p.offsets, p.nbr, p.D, p.K, p.pacc, p.ecap);
+int launch_crk_initialize(Batch& b) {
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(crk_nodes(b, 128, &bm, &grid, isCrk));
+  if (grid) { crk_moments_corrections_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "CRK moments");
+}
+
+int launch_crk_eval(Batch& b) {
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return isCrkFp64(p) ? (b.capacityGrids ? p.candcap : p.n + p.G) : (int64_t)0; }, 256, &bm, &grid));
+  if (grid) { pack_crk_records_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  auto key = [](const Problem& p) { return (p.prm.XSPH ? 2 : 0) | (p.prm.compatible ? 1 : 0); };
+  const bool solo = b.mem.size() == 1;
+  const Member one = solo ? describe_member(*b.mem[0]) : Member{};
+  bool present[4] = {false, false, false, false};
+  for (Problem* p : b.mem) if (isCrkFp64(*p)) present[key(*p)] = true;
+  for (int v = 0; v < 4; ++v) {
+    if (!present[v]) continue;
+    SPH_TRY(batch_map_items(b, [&](const Problem& p) { return isCrkFp64(p) && key(p) == v ? p.n : (int64_t)0; }, b.evalThreads,
+                            &bm, &grid));
+    if (!grid) continue;
+#define CRK_LAUNCH(X, C)                                                                               \
+    if (solo) crk_eval_kernel<X, C, true><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one);     \
+    else crk_eval_kernel<X, C, false><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one)
+    switch (v) {
+      case 0: CRK_LAUNCH(false, false); break;
+      case 1: CRK_LAUNCH(false, true); break;
+      case 2: CRK_LAUNCH(true, false); break;
+      default: CRK_LAUNCH(true, true); break;
+    }
+#undef CRK_LAUNCH
+    batch_count_launch(b);
   }
-  ++p.launches;
+  return cuda_status(cudaGetLastError(), "CRK evaluate");
 }
 
 }  // namespace sphgpu

@@ -1,4 +1,5 @@
-// Periodic ghost images, cell list and ConnectivityMap CSR on the device.
+// Periodic ghost images, cell list and ConnectivityMap CSR on the device,
+// for every member of a batch in one launch per stage.
 //
 // Replaces, for one FluidNodeList in a periodic box:
 //   PlanarBoundary::setGhostNodes     src/Boundary/PlanarBoundary.cc:114-181
@@ -10,16 +11,24 @@
 // |H_i r_ij|^2 <= kappa^2 || |H_j r_ij|^2 <= kappa^2 are evaluated in the
 // reference's FP64 operation order, so neighbor sets are bit-identical.
 //
+// The build is sized on the device: the ghost counts, the cell grid, the
+// entry count and the longest list are produced by kernels into each member's
+// scalar slots and read there by the next kernels; launches are sized for the
+// buffer capacities.  The host plans the capacities from the previous build,
+// launches every stage, and reads the sizes back once at the end; a capacity
+// overflow sets an error bit and the build is redone with larger buffers.
+//
 // Kernels and their bounds (see the roofline notes in the design document):
 //   ghost_hmax / ghost_flag / ghost_scatter  O(N+G) streaming, HBM bound
 //   node_bounds / cell_index / cell_scatter  O(N+G) streaming + atomics
 //   nbr_thread<COUNT|FILL>                   thread per node (cell-sorted
 //                                            order) over the 27 neighbouring
-//                                            cells; 80-byte candidate records
+//                                            cells; 64-byte candidate records
 //                                            shared by a warp through L1
 //   nbr_walk<COUNT|FILL>                     warp per node, for large
 //                                            candidate sets
 #include <cstdio>
+#include <cstring>
 #include <climits>
 
 #include "problem.cuh"
@@ -28,83 +37,176 @@ namespace sphgpu {
 
 namespace {
 
+constexpr int kGhostThreads = 256;
+constexpr float kFilterTol = 1.0e-3f;
+
 __device__ __forceinline__ unsigned long long orderedBits(double v) {
   const unsigned long long b = (unsigned long long)__double_as_longlong(v);
   return (b & 0x8000000000000000ULL) ? ~b : (b | 0x8000000000000000ULL);
 }
-
-__device__ __forceinline__ V3 nodePos(const double* S, int64_t n, const double* gpos, int64_t gcap, int64_t k) {
-  if (k < n) return V3{S[S_X*n + k], S[S_Y*n + k], S[S_Z*n + k]};
-  const int64_t g = k - n;
-  return V3{gpos[g], gpos[gcap + g], gpos[2*gcap + g]};
+__device__ __forceinline__ double fromOrderedBits(unsigned long long b) {
+  const unsigned long long r = (b & 0x8000000000000000ULL) ? (b & 0x7fffffffffffffffULL) : ~b;
+  return __longlong_as_double((long long)r);
 }
-__device__ __forceinline__ Sym nodeH(const double* S, int64_t n, const int32_t* groot, int64_t k) {
-  const int64_t r = k < n ? k : groot[k - n];
+
+__device__ __forceinline__ V3 nodePos(const Member& M, int64_t k) {
+  const int64_t n = M.n;
+  if (k < n) return V3{M.S[S_X*n + k], M.S[S_Y*n + k], M.S[S_Z*n + k]};
+  const int64_t g = k - n;
+  return V3{M.gpos[g], M.gpos[M.gcap + g], M.gpos[2*M.gcap + g]};
+}
+__device__ __forceinline__ Sym nodeH(const Member& M, int64_t k) {
+  const int64_t n = M.n;
+  const int64_t r = k < n ? k : M.groot[k - n];
+  const double* S = M.S;
   return Sym{S[(S_H + 0)*n + r], S[(S_H + 1)*n + r], S[(S_H + 2)*n + r],
              S[(S_H + 3)*n + r], S[(S_H + 4)*n + r], S[(S_H + 5)*n + r]};
 }
 
+// internal + ghost nodes of the current build
+__device__ __forceinline__ int64_t allNodes(const Member& M) { return M.n + scalI(M.scal, SC_G); }
+
+__device__ __forceinline__ Grid loadGrid(const Member& M) {
+  const double* s = M.scal + SC_GRID;
+  Grid g;
+  g.lo[0] = s[0]; g.lo[1] = s[1]; g.lo[2] = s[2];
+  g.cell = s[3];
+  g.dim[0] = (int)scalI(M.scal, SC_GRID + 4);
+  g.dim[1] = (int)scalI(M.scal, SC_GRID + 5);
+  g.dim[2] = (int)scalI(M.scal, SC_GRID + 6);
+  g.filterTol = (float)s[7];
+  return g;
+}
+
+// ---------------------------------------------------------------- ghosts
+// Start of a build: no ghosts yet.
+__global__ void build_init_kernel(const Member* mem, int nmem) {
+  const int m = blockIdx.x*blockDim.x + threadIdx.x;
+  if (m >= nmem) return;
+  double* s = mem[m].scal;
+  setScalI(s, SC_NTOT, mem[m].n);
+  setScalI(s, SC_G, 0);
+  s[SC_HMAX] = 0.0;
+  s[SC_MAXCOND] = 0.0;
+}
+
+// 1/min(eig(H)) of every internal node, once per build (ghosts share their
+// root's H, so every boundary pass and the cell size read it from here), and
+// the largest condition number of H (bounds the FP32 pre-test error).
+__global__ void __launch_bounds__(kGhostThreads) node_hmax_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
+  double cond = 0.0;
+  if (i < M.n) {
+    const V3 ev = eigenValues(nodeH(M, i));
+    M.hmaxi[i] = 1.0/vmin(ev);
+    cond = vmax(ev)/vmin(ev);
+    if (!(cond < 1.0e300)) cond = 1.0e300;     // degenerate H: no FP32 pre-test
+  }
+  for (int o = 16; o > 0; o >>= 1) cond = dmax(cond, __shfl_xor_sync(0xffffffffu, cond, o));
+  if ((threadIdx.x & 31) == 0 && cond > 0.0)
+    atomicMax(reinterpret_cast<unsigned long long*>(M.scal + SC_MAXCOND),
+              (unsigned long long)__double_as_longlong(cond));
+}
+
+__device__ __forceinline__ double nodeHmax(const Member& M, int64_t k) {
+  return M.hmaxi[k < M.n ? k : M.groot[k - M.n]];
+}
+
 // hmax of PlanarBoundary::setGhostNodes: max 1/min(eig(H)) over nodes within
 // kernelExtent*hmaxi of either plane.
-__global__ void ghost_hmax_kernel(const double* S, int64_t n, const double* gpos, int64_t gcap,
-                                  const int32_t* groot, int64_t ntot, PlanarBC bc, double kernelExtent,
-                                  unsigned long long* out) {
+__global__ void __launch_bounds__(kGhostThreads) ghost_hmax_kernel(const Member* mem, BlockMap bm, int b) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int64_t k = mb.block*blockDim.x + threadIdx.x;
   double best = 0.0;
-  for (int64_t k = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; k < ntot; k += (int64_t)gridDim.x*blockDim.x) {
-    const V3 r = nodePos(S, n, gpos, gcap, k);
-    const Sym H = nodeH(S, n, groot, k);
-    const double hmaxi = 1.0/vmin(eigenValues(H));
-    if (hmaxi > best && dmin(minimumDistance(bc.exit, r), minimumDistance(bc.enter, r)) < kernelExtent*hmaxi)
-      best = hmaxi;
+  if (k < scalI(M.scal, SC_NTOT) && M.prm.bcs.periodic[b >> 1]) {
+    const PlanarBC& bc = M.prm.bcs.bc[b];
+    const V3 r = nodePos(M, k);
+    const double hmaxi = nodeHmax(M, k);
+    if (dmin(minimumDistance(bc.exit, r), minimumDistance(bc.enter, r)) < M.prm.kernelExtent*hmaxi) best = hmaxi;
   }
   for (int o = 16; o > 0; o >>= 1) best = dmax(best, __shfl_xor_sync(0xffffffffu, best, o));
-  if ((threadIdx.x & 31) == 0 && best > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(best));
+  if ((threadIdx.x & 31) == 0 && best > 0.0)
+    atomicMax(reinterpret_cast<unsigned long long*>(M.scal + SC_HMAX), (unsigned long long)__double_as_longlong(best));
 }
 
-__global__ void ghost_flag_kernel(const double* S, int64_t n, const double* gpos, int64_t gcap, int64_t ntot,
-                                  PlanarBC bc, double kernelExtent, const unsigned long long* hmaxBits,
-                                  int32_t* flags) {
-  const double hmax = __longlong_as_double((long long)*hmaxBits);
-  for (int64_t k = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; k < ntot; k += (int64_t)gridDim.x*blockDim.x) {
-    int f = 0;
-    if (hmax > 0.0) {
-      const V3 r = nodePos(S, n, gpos, gcap, k);
-      const double disti = signedDistance(bc.exit, r)/hmax;
-      f = (disti >= 0.0 && disti <= kernelExtent) ? 1 : 0;
-    }
-    flags[k] = f;
+__global__ void __launch_bounds__(kGhostThreads) ghost_flag_kernel(const Member* mem, BlockMap bm, int b) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int64_t k = mb.block*blockDim.x + threadIdx.x;
+  if (k >= scalI(M.scal, SC_NTOT)) return;
+  int f = 0;
+  const double hmax = M.scal[SC_HMAX];
+  if (M.prm.bcs.periodic[b >> 1] && hmax > 0.0) {
+    const V3 r = nodePos(M, k);
+    const double disti = signedDistance(M.prm.bcs.bc[b].exit, r)/hmax;
+    f = (disti >= 0.0 && disti <= M.prm.kernelExtent) ? 1 : 0;
   }
+  M.counts[k] = f;
 }
 
-__global__ void ghost_scatter_kernel(const double* S, int64_t n, double* gpos, int64_t gcap,
-                                     int32_t* groot, uint32_t* gcode, int64_t ntot,
-                                     const int32_t* flags, const int64_t* slots, PlanarBC bc, int b,
-                                     int* err) {
-  for (int64_t k = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; k < ntot; k += (int64_t)gridDim.x*blockDim.x) {
-    if (!flags[k]) continue;
-    const int64_t g = (ntot - n) + slots[k];     // ghost index of the new image
-    const V3 r = nodePos(S, n, gpos, gcap, k);
-    const V3 gp = mapPositionThroughPlanes(r, bc.exit, bc.enter);
-    const int32_t root = k < n ? (int32_t)k : groot[k - n];
-    uint32_t code = k < n ? 0u : gcode[k - n];
-    const int axis = b >> 1;
-    if ((code >> (2*axis)) & 3u) atomicOr(err, DERR_GHOST_CHAIN);
-    code |= (uint32_t)((b & 1) + 1) << (2*axis);
-    groot[g] = root;
-    gcode[g] = code;
-    gpos[g] = gp.x; gpos[gcap + g] = gp.y; gpos[2*gcap + g] = gp.z;
+__global__ void __launch_bounds__(kGhostThreads) ghost_scatter_kernel(const Member* mem, BlockMap bm, int b) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int64_t k = mb.block*blockDim.x + threadIdx.x;
+  const int64_t ntot = scalI(M.scal, SC_NTOT);
+  if (k >= ntot || !M.counts[k]) return;
+  const int64_t n = M.n;
+  const int64_t g = (ntot - n) + M.offsets[k];     // ghost index of the new image
+  if (g >= M.gcap) {
+    atomicOr(M.err, DERR_GHOST_CAPACITY);
+    return;
   }
+  const PlanarBC& bc = M.prm.bcs.bc[b];
+  const V3 gp = mapPositionThroughPlanes(nodePos(M, k), bc.exit, bc.enter);
+  const int32_t root = k < n ? (int32_t)k : M.groot[k - n];
+  uint32_t code = k < n ? 0u : M.gcode[k - n];
+  const int axis = b >> 1;
+  if ((code >> (2*axis)) & 3u) atomicOr(M.err, DERR_GHOST_CHAIN);
+  code |= (uint32_t)((b & 1) + 1) << (2*axis);
+  M.groot[g] = root;
+  M.gcode[g] = code;
+  M.gpos[g] = gp.x; M.gpos[M.gcap + g] = gp.y; M.gpos[2*M.gcap + g] = gp.z;
 }
 
-// Global bounding box of all nodes and max of 1/min(eig(H)) (cell size).
-__global__ void node_bounds_kernel(const double* S, int64_t n, const double* gpos, int64_t gcap,
-                                   const int32_t* groot, int64_t ntot, unsigned long long* out) {
+// After a boundary pass: the new images join the node set (at most up to the
+// ghost capacity; beyond it the build is redone), hmax restarts.
+__global__ void ghost_advance_kernel(const Member* mem, int nmem) {
+  const int m = blockIdx.x*blockDim.x + threadIdx.x;
+  if (m >= nmem) return;
+  const Member& M = mem[m];
+  int64_t g = scalI(M.scal, SC_NTOT) - M.n + scalI(M.scal, SC_TOTAL);
+  if (g > M.gcap) {
+    atomicOr(M.err, DERR_GHOST_CAPACITY);
+    g = M.gcap;
+  }
+  setScalI(M.scal, SC_NTOT, M.n + g);
+  setScalI(M.scal, SC_G, g);
+  M.scal[SC_HMAX] = 0.0;
+}
+
+// ---------------------------------------------------------------- cells
+__global__ void bounds_init_kernel(const Member* mem, int nmem) {
+  const int m = blockIdx.x*blockDim.x + threadIdx.x;
+  if (m >= nmem) return;
+  unsigned long long* bb = reinterpret_cast<unsigned long long*>(mem[m].scal + SC_BOUNDS);
+  for (int a = 0; a < 3; ++a) { bb[a] = ~0ULL; bb[3 + a] = 0ULL; }
+  bb[6] = 0ULL;
+}
+
+// Bounding box of all nodes and max of 1/min(eig(H)) (cell size).
+__global__ void __launch_bounds__(kGhostThreads) node_bounds_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int64_t k = mb.block*blockDim.x + threadIdx.x;
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300}, h = 0.0;
-  for (int64_t k = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; k < ntot; k += (int64_t)gridDim.x*blockDim.x) {
-    const V3 r = nodePos(S, n, gpos, gcap, k);
-    lo[0] = fmin(lo[0], r.x); lo[1] = fmin(lo[1], r.y); lo[2] = fmin(lo[2], r.z);
-    hi[0] = fmax(hi[0], r.x); hi[1] = fmax(hi[1], r.y); hi[2] = fmax(hi[2], r.z);
-    if (k < n) h = fmax(h, 1.0/vmin(eigenValues(nodeH(S, n, groot, k))));
+  if (k < allNodes(M)) {
+    const V3 r = nodePos(M, k);
+    lo[0] = r.x; lo[1] = r.y; lo[2] = r.z;
+    hi[0] = r.x; hi[1] = r.y; hi[2] = r.z;
+    if (k < M.n) h = M.hmaxi[k];
   }
   for (int o = 16; o > 0; o >>= 1) {
     for (int a = 0; a < 3; ++a) {
@@ -113,7 +215,19 @@ __global__ void node_bounds_kernel(const double* S, int64_t n, const double* gpo
     }
     h = fmax(h, __shfl_xor_sync(0xffffffffu, h, o));
   }
+  __shared__ double sh[kGhostThreads/32][7];
+  const int w = threadIdx.x >> 5;
   if ((threadIdx.x & 31) == 0) {
+    for (int a = 0; a < 3; ++a) { sh[w][a] = lo[a]; sh[w][3 + a] = hi[a]; }
+    sh[w][6] = h;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int ww = 1; ww < (int)(blockDim.x >> 5); ++ww) {
+      for (int a = 0; a < 3; ++a) { lo[a] = fmin(lo[a], sh[ww][a]); hi[a] = fmax(hi[a], sh[ww][3 + a]); }
+      h = fmax(h, sh[ww][6]);
+    }
+    unsigned long long* out = reinterpret_cast<unsigned long long*>(M.scal + SC_BOUNDS);
     for (int a = 0; a < 3; ++a) {
       atomicMin(out + a, orderedBits(lo[a]));
       atomicMax(out + 3 + a, orderedBits(hi[a]));
@@ -122,66 +236,163 @@ __global__ void node_bounds_kernel(const double* S, int64_t n, const double* gpo
   }
 }
 
-struct Grid {
-  double lo[3];
-  double cell;
-  int dim[3];
-};
+// Uniform grid of cells of edge >= kappa*max(1/lambda_min(H)) (the margin
+// covers the libm difference of the eigenvalue solve for anisotropic H),
+// enlarged until the cells fit the cell buffers (larger cells only widen the
+// candidate set).  Also resets the walk's counters and sets the FP32
+// pre-test tolerance: only when every H has condition number <= 100.
+__global__ void grid_kernel(const Member* mem, int nmem) {
+  const int m = blockIdx.x*blockDim.x + threadIdx.x;
+  if (m >= nmem) return;
+  const Member& M = mem[m];
+  const unsigned long long* bb = reinterpret_cast<const unsigned long long*>(M.scal + SC_BOUNDS);
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) { lo[a] = fromOrderedBits(bb[a]); hi[a] = fromOrderedBits(bb[3 + a]); }
+  const double hmaxAll = fromOrderedBits(bb[6]);
+  double cell = M.prm.kernelExtent*hmaxAll*1.001;
+  if (!(cell > 0.0) || !(cell < 1.0e300)) {
+    atomicOr(M.err, DERR_NONPOSITIVE);
+    cell = 1.0;
+  }
+  const int64_t maxCells = M.cellcap < ((int64_t)1 << 26) ? M.cellcap : ((int64_t)1 << 26);
+  int64_t dim[3] = {1, 1, 1}, ncells = 1;
+  for (int attempt = 0; attempt < 200; ++attempt) {
+    ncells = 1;
+    for (int a = 0; a < 3; ++a) {
+      const double d = (hi[a] - lo[a])/cell;
+      const int64_t mm = d < 1.0e6 ? (int64_t)d + 1 : (int64_t)1 << 20;
+      dim[a] = mm < (1 << 20) ? mm : (1 << 20);
+      ncells *= dim[a];
+    }
+    if (ncells <= maxCells) break;
+    cell *= 1.26;
+  }
+  double* s = M.scal + SC_GRID;
+  s[0] = lo[0]; s[1] = lo[1]; s[2] = lo[2];
+  s[3] = cell;
+  for (int a = 0; a < 3; ++a) setScalI(M.scal, SC_GRID + 4 + a, dim[a]);
+  const double cond = M.scal[SC_MAXCOND];
+  s[7] = (M.grid.filterTol > 0.0f && cond > 0.0 && cond <= 100.0) ? (double)M.grid.filterTol : 0.0;
+  setScalI(M.scal, SC_NCELLS, ncells);
+  setScalI(M.scal, SC_MAXCOUNT, 0);
+  setScalI(M.scal, SC_PAIRS, 0);
+}
 
 __device__ __forceinline__ int cellCoord(double x, double lo, double cell, int dim) {
   int c = int((x - lo)/cell);
   return c < 0 ? 0 : (c >= dim ? dim - 1 : c);
 }
 
-__global__ void cell_index_kernel(const double* S, int64_t n, const double* gpos, int64_t gcap, int64_t ntot,
-                                  Grid g, int32_t* cidx, int32_t* cellCount) {
-  for (int64_t k = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; k < ntot; k += (int64_t)gridDim.x*blockDim.x) {
-    const V3 r = nodePos(S, n, gpos, gcap, k);
-    const int cx = cellCoord(r.x, g.lo[0], g.cell, g.dim[0]);
-    const int cy = cellCoord(r.y, g.lo[1], g.cell, g.dim[1]);
-    const int cz = cellCoord(r.z, g.lo[2], g.cell, g.dim[2]);
-    const int c = (cz*g.dim[1] + cy)*g.dim[0] + cx;
-    cidx[k] = c;
-    atomicAdd(cellCount + c, 1);
-  }
+__global__ void __launch_bounds__(kGhostThreads) cell_zero_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int64_t c = mb.block*blockDim.x + threadIdx.x;
+  if (c < scalI(M.scal, SC_NCELLS)) M.cellFill[c] = 0;
 }
 
-// Candidate record of the cell-sorted node list: position, H and the node
-// index, 80 bytes, read as five 16-byte loads.
+__global__ void __launch_bounds__(kGhostThreads) cell_index_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int64_t k = mb.block*blockDim.x + threadIdx.x;
+  if (k >= allNodes(M)) return;
+  const Grid g = loadGrid(M);
+  const V3 r = nodePos(M, k);
+  const int cx = cellCoord(r.x, g.lo[0], g.cell, g.dim[0]);
+  const int cy = cellCoord(r.y, g.lo[1], g.cell, g.dim[1]);
+  const int cz = cellCoord(r.z, g.lo[2], g.cell, g.dim[2]);
+  const int c = (cz*g.dim[1] + cy)*g.dim[0] + cx;
+  M.cidx[k] = c;
+  atomicAdd(M.cellFill + c, 1);
+}
+
+// Candidate record of the cell-sorted node list, 64 bytes read as four
+// 16-byte loads: FP64 position, node index, FP32 copy of H.  The FP64 H of
+// the same slot sits in a second array (48 bytes) and is read only when the
+// FP32 pre-test cannot decide.
 struct __align__(16) NbrCand {
   double x, y, z;
-  double hxx, hxy, hxz, hyy, hyz, hzz;
-  int32_t idx, pad;
+  int32_t idx;
+  float h[6];
+  float pad;
 };
-static_assert(sizeof(NbrCand) == 80, "candidate record is five 16-byte words");
+static_assert(sizeof(NbrCand) == 64, "candidate record is four 16-byte words");
 
 __device__ __forceinline__ NbrCand loadCand(const NbrCand* c) {
   const double2* q = reinterpret_cast<const double2*>(c);
-  const double2 a = __ldg(q), b = __ldg(q + 1), d = __ldg(q + 2), e = __ldg(q + 3), f = __ldg(q + 4);
+  const double2 a = __ldg(q);
+  const double2 b = __ldg(q + 1);
+  const float4 f = __ldg(reinterpret_cast<const float4*>(q + 2));
+  const float4 g = __ldg(reinterpret_cast<const float4*>(q + 3));
   NbrCand r;
-  r.x = a.x; r.y = a.y; r.z = b.x; r.hxx = b.y; r.hxy = d.x; r.hxz = d.y; r.hyy = e.x; r.hyz = e.y; r.hzz = f.x;
-  r.idx = __double_as_longlong(f.y) & 0xffffffff;
-  r.pad = 0;
+  r.x = a.x; r.y = a.y; r.z = b.x;
+  const uint64_t w = (uint64_t)__double_as_longlong(b.y);
+  r.idx = (int32_t)(uint32_t)(w & 0xffffffffu);
+  r.h[0] = __uint_as_float((uint32_t)(w >> 32));
+  r.h[1] = f.x; r.h[2] = f.y; r.h[3] = f.z; r.h[4] = f.w; r.h[5] = g.x;
+  r.pad = 0.0f;
   return r;
 }
 
-__global__ void cell_scatter_kernel(const double* S, int64_t n, const double* gpos, int64_t gcap,
-                                    const int32_t* groot, int64_t ntot, const int32_t* cidx,
-                                    const int64_t* cellStart, int32_t* cellFill, int32_t* sortedIdx,
-                                    NbrCand* cand) {
-  for (int64_t k = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; k < ntot; k += (int64_t)gridDim.x*blockDim.x) {
-    const int c = cidx[k];
-    const int64_t slot = cellStart[c] + atomicAdd(cellFill + c, 1);
-    sortedIdx[slot] = (int32_t)k;
-    const V3 r = nodePos(S, n, gpos, gcap, k);
-    const Sym H = nodeH(S, n, groot, k);
-    double2* q = reinterpret_cast<double2*>(cand + slot);
-    q[0] = make_double2(r.x, r.y);
-    q[1] = make_double2(r.z, H.xx);
-    q[2] = make_double2(H.xy, H.xz);
-    q[3] = make_double2(H.yy, H.yz);
-    q[4] = make_double2(H.zz, __longlong_as_double((long long)(uint32_t)k));
+__device__ __forceinline__ const double* candHArray(const Member& M) {
+  return static_cast<const double*>(M.cand) + 8*M.candcap;
+}
+
+__device__ __forceinline__ Sym loadCandH(const double* candH, int64_t k) {
+  const double2* q = reinterpret_cast<const double2*>(candH + 6*k);
+  const double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+  return Sym{a.x, a.y, b.x, b.y, c.x, c.y};
+}
+
+__device__ __forceinline__ float symEta2F(const float* h, float x, float y, float z) {
+  const float ex = __fmaf_rn(h[0], x, __fmaf_rn(h[1], y, h[2]*z));
+  const float ey = __fmaf_rn(h[1], x, __fmaf_rn(h[3], y, h[4]*z));
+  const float ez = __fmaf_rn(h[2], x, __fmaf_rn(h[4], y, h[5]*z));
+  return __fmaf_rn(ex, ex, __fmaf_rn(ey, ey, ez*ez));
+}
+
+// ConnectivityMap predicate |H_i r_ij|^2 <= kappa^2 || |H_j r_ij|^2 <= kappa^2.
+// A FP32 pre-test on r_ij = r_i - r_j (formed in FP64, rounded once) decides
+// every pair whose eta^2 lies outside the band kappa^2 (1 -+ tol); inside the
+// band the test is the exact FP64 one in the reference's operation order.
+// The FP32 error of eta^2 is below 1e-6 cond(H) relative, and tol is only set
+// (1e-3) when every H has cond(H) <= 100, so the result equals the exact test.
+__device__ __forceinline__ bool neighborTest(const V3& ri, const Sym& Hi, const float* hif, const NbrCand& c,
+                                             const double* candH, int64_t k, double k2, float tol) {
+  const double dx = ri.x - c.x, dy = ri.y - c.y, dz = ri.z - c.z;
+  if (tol > 0.0f) {
+    const float fx = (float)dx, fy = (float)dy, fz = (float)dz;
+    const float e2i = symEta2F(hif, fx, fy, fz);
+    const float e2j = symEta2F(c.h, fx, fy, fz);
+    const float k2f = (float)k2;
+    const float lo = k2f*(1.0f - tol), hi = k2f*(1.0f + tol);
+    if (e2i <= lo || e2j <= lo) return true;
+    if (e2i > hi && e2j > hi) return false;
   }
+  const V3 rij{dx, dy, dz};
+  return mag2(sdot(Hi, rij)) <= k2 || mag2(sdot(loadCandH(candH, k), rij)) <= k2;
+}
+
+__global__ void __launch_bounds__(kGhostThreads) cell_scatter_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int64_t k = mb.block*blockDim.x + threadIdx.x;
+  if (k >= allNodes(M)) return;
+  const int c = M.cidx[k];
+  const int64_t slot = M.cellStart[c] + atomicAdd(M.cellFill + c, 1);
+  M.sortedIdx[slot] = (int32_t)k;
+  const V3 r = nodePos(M, k);
+  const Sym H = nodeH(M, k);
+  double2* q = reinterpret_cast<double2*>(static_cast<NbrCand*>(M.cand) + slot);
+  const uint64_t w = (uint64_t)(uint32_t)k | ((uint64_t)__float_as_uint((float)H.xx) << 32);
+  q[0] = make_double2(r.x, r.y);
+  q[1] = make_double2(r.z, __longlong_as_double((long long)w));
+  float4* f = reinterpret_cast<float4*>(q + 2);
+  f[0] = make_float4((float)H.xy, (float)H.xz, (float)H.yy, (float)H.yz);
+  f[1] = make_float4((float)H.zz, 0.0f, 0.0f, 0.0f);
+  double2* h = reinterpret_cast<double2*>(const_cast<double*>(candHArray(M)) + 6*slot);
+  h[0] = make_double2(H.xx, H.xy);
+  h[1] = make_double2(H.xz, H.yy);
+  h[2] = make_double2(H.yz, H.zz);
 }
 
 // Thread per internal node, nodes taken in cell-sorted order so that the
@@ -193,26 +404,30 @@ __global__ void cell_scatter_kernel(const double* S, int64_t n, const double* gp
 // capacity `cap` (element c of thread t at lst[c*blockDim + t], conflict
 // free) and stored ascending at offsets[i].
 template<bool FILL>
-__global__ void __launch_bounds__(256) nbr_thread_kernel(int64_t n, int64_t ntot, Grid g, const int64_t* cellStart,
-                                                         const NbrCand* cand, double kernelExtent2, int32_t* counts,
-                                                         const int64_t* offsets, int32_t* nbr, int cap,
-                                                         int* maxCount, int* err,
-                                                         unsigned long long* pairCount) {
+__global__ void __launch_bounds__(256) nbr_thread_kernel(const Member* mem, BlockMap bm, int cap, int maxNbr) {
   extern __shared__ int32_t lst[];
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
   const int tid = threadIdx.x;
   const int bd = blockDim.x;
-  const int64_t s = blockIdx.x*(int64_t)bd + tid;
+  const int64_t s = mb.block*bd + tid;
+  const int64_t n = M.n;
+  const NbrCand* cand = static_cast<const NbrCand*>(M.cand);
   NbrCand me;
-  bool active = s < ntot;
+  bool active = s < allNodes(M);
   if (active) {
     me = loadCand(cand + s);
     active = me.idx < n;
   }
   int count = 0, above = 0;
   if (active) {
+    const Grid g = loadGrid(M);
+    const double kernelExtent2 = M.prm.kernelExtent*M.prm.kernelExtent;
+    const int64_t* cellStart = M.cellStart;
+    const double* candH = candHArray(M);
     const int32_t i = me.idx;
     const V3 ri{me.x, me.y, me.z};
-    const Sym Hi{me.hxx, me.hxy, me.hxz, me.hyy, me.hyz, me.hzz};
+    const Sym Hi = loadCandH(candH, s);
     const int cx = cellCoord(ri.x, g.lo[0], g.cell, g.dim[0]);
     const int cy = cellCoord(ri.y, g.lo[1], g.cell, g.dim[1]);
     const int cz = cellCoord(ri.z, g.lo[2], g.cell, g.dim[2]);
@@ -229,10 +444,7 @@ __global__ void __launch_bounds__(256) nbr_thread_kernel(int64_t n, int64_t ntot
         const int64_t end = cellStart[cbase + x1 + 1];
         for (int64_t k = start; k < end; ++k) {
           const NbrCand c = loadCand(cand + k);
-          const V3 rij = vsub(ri, V3{c.x, c.y, c.z});
-          const double eta2i = mag2(sdot(Hi, rij));
-          const double eta2j = mag2(sdot(Sym{c.hxx, c.hxy, c.hxz, c.hyy, c.hyz, c.hzz}, rij));
-          if ((eta2i <= kernelExtent2 || eta2j <= kernelExtent2) && c.idx != i) {
+          if (c.idx != i && neighborTest(ri, Hi, me.h, c, candH, k, kernelExtent2, g.filterTol)) {
             if (FILL) {
               if (count < cap) {
                 int p = count;
@@ -252,22 +464,23 @@ __global__ void __launch_bounds__(256) nbr_thread_kernel(int64_t n, int64_t ntot
       }
     }
     if (!FILL) {
-      counts[i] = count;
-    } else if (count <= cap) {
-      const int64_t o = offsets[i];
-      for (int c = 0; c < count; ++c) nbr[o + c] = lst[c*bd + tid];
+      M.counts[i] = count;
+      if (count > maxNbr) atomicOr(M.err, DERR_NBR_CAPACITY);
     } else {
-      atomicOr(err, DERR_NBR_CAPACITY);
+      const int64_t o = M.offsets[i];
+      if (count > cap) atomicOr(M.err, DERR_LIST_CAPACITY);
+      else if (o + count > M.ecap) atomicOr(M.err, DERR_ENTRY_CAPACITY);
+      else for (int c = 0; c < count; ++c) M.nbr[o + c] = lst[c*bd + tid];
     }
   }
   if (!FILL) {
     int m = count;
     for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((tid & 31) == 0 && m > 0) atomicMax(maxCount, m);
+    if ((tid & 31) == 0 && m > 0) atomicMax(reinterpret_cast<int*>(M.scal + SC_MAXCOUNT), m);
   } else {
     unsigned long long a = (unsigned long long)above;
     for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if ((tid & 31) == 0 && a) atomicAdd(pairCount, a);
+    if ((tid & 31) == 0 && a) atomicAdd(reinterpret_cast<unsigned long long*>(M.scal + SC_PAIRS), a);
   }
 }
 
@@ -275,22 +488,27 @@ __global__ void __launch_bounds__(256) nbr_thread_kernel(int64_t n, int64_t ntot
 // ConnectivityMap predicate, count (FILL=false) or collect, sort ascending
 // and store (FILL=true) the neighbor indices.  Used when the candidate sets
 // are large (many nodes per cell), where a warp per node keeps the SMs full.
+// `cap` is the per-warp list capacity (a power of two >= 32).
 template<bool FILL>
-__global__ void __launch_bounds__(256) nbr_walk_kernel(const double* S, int64_t n, Grid g,
-                                                       const int64_t* cellStart, const NbrCand* cand,
-                                                       double kernelExtent2,
-                                                       int32_t* counts, const int64_t* offsets, int32_t* nbr,
-                                                       int maxNbr, int* err, int* maxCount,
-                                                       unsigned long long* pairCount) {
+__global__ void __launch_bounds__(256) nbr_walk_kernel(const Member* mem, BlockMap bm, int cap, int maxNbr) {
   extern __shared__ int32_t sbuf_all[];
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  int32_t* sbuf = sbuf_all + (FILL ? wib*maxNbr : 0);
-  const int64_t i = (blockIdx.x*(int64_t)blockDim.x + threadIdx.x) >> 5;
+  int32_t* sbuf = sbuf_all + (FILL ? wib*cap : 0);
+  const int64_t n = M.n;
+  const int64_t i = (mb.block*(int64_t)blockDim.x + threadIdx.x) >> 5;
   if (i >= n) return;
+  const double* S = M.S;
+  const Grid g = loadGrid(M);
+  const NbrCand* cand = static_cast<const NbrCand*>(M.cand);
+  const double kernelExtent2 = M.prm.kernelExtent*M.prm.kernelExtent;
   const V3 ri{S[S_X*n + i], S[S_Y*n + i], S[S_Z*n + i]};
   const Sym Hi{S[(S_H + 0)*n + i], S[(S_H + 1)*n + i], S[(S_H + 2)*n + i],
                S[(S_H + 3)*n + i], S[(S_H + 4)*n + i], S[(S_H + 5)*n + i]};
+  const float hif[6] = {(float)Hi.xx, (float)Hi.xy, (float)Hi.xz, (float)Hi.yy, (float)Hi.yz, (float)Hi.zz};
+  const double* candH = candHArray(M);
   const int cx = cellCoord(ri.x, g.lo[0], g.cell, g.dim[0]);
   const int cy = cellCoord(ri.y, g.lo[1], g.cell, g.dim[1]);
   const int cz = cellCoord(ri.z, g.lo[2], g.cell, g.dim[2]);
@@ -305,8 +523,8 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const double* S, int64_t 
       const int x0 = cx > 0 ? cx - 1 : 0;
       const int x1 = cx + 1 < g.dim[0] ? cx + 1 : g.dim[0] - 1;
       const int cbase = (z*g.dim[1] + y)*g.dim[0];
-      const int64_t start = cellStart[cbase + x0];
-      const int64_t end = cellStart[cbase + x1 + 1];
+      const int64_t start = M.cellStart[cbase + x0];
+      const int64_t end = M.cellStart[cbase + x1 + 1];
       for (int64_t base = start; base < end; base += 32) {
         const int64_t k = base + lane;
         bool pass = false;
@@ -314,17 +532,12 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const double* S, int64_t 
         if (k < end) {
           const NbrCand c = loadCand(cand + k);
           j = c.idx;
-          const V3 rj{c.x, c.y, c.z};
-          const Sym Hj{c.hxx, c.hxy, c.hxz, c.hyy, c.hyz, c.hzz};
-          const V3 rij = vsub(ri, rj);
-          const double eta2i = mag2(sdot(Hi, rij));
-          const double eta2j = mag2(sdot(Hj, rij));
-          pass = (eta2i <= kernelExtent2 || eta2j <= kernelExtent2) && (j != (int32_t)i);
+          pass = j != (int32_t)i && neighborTest(ri, Hi, hif, c, candH, k, kernelExtent2, g.filterTol);
         }
         const unsigned ballot = __ballot_sync(0xffffffffu, pass);
         if (FILL && pass) {
           const int pos = count + __popc(ballot & ((1u << lane) - 1u));
-          if (pos < maxNbr) sbuf[pos] = j;
+          if (pos < cap) sbuf[pos] = j;
         }
         count += __popc(ballot);
       }
@@ -332,13 +545,17 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const double* S, int64_t 
   }
   if (!FILL) {
     if (lane == 0) {
-      counts[i] = count;
-      if (count > maxNbr) atomicOr(err, DERR_NBR_CAPACITY);
-      atomicMax(maxCount, count);
+      M.counts[i] = count;
+      if (count > maxNbr) atomicOr(M.err, DERR_NBR_CAPACITY);
+      atomicMax(reinterpret_cast<int*>(M.scal + SC_MAXCOUNT), count);
     }
     return;
   }
-  if (count > maxNbr) return;
+  const int64_t o = M.offsets[i];
+  if (count > cap || o + count > M.ecap) {
+    if (lane == 0) atomicOr(M.err, count > cap ? DERR_LIST_CAPACITY : DERR_ENTRY_CAPACITY);
+    return;
+  }
   // bitonic sort of sbuf[0:count] (padded to a power of two)
   int size = 32;
   while (size < count) size <<= 1;
@@ -357,194 +574,208 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const double* S, int64_t 
       __syncwarp();
     }
   }
-  const int64_t o = offsets[i];
   int above = 0;
   for (int t = lane; t < count; t += 32) {
     const int32_t j = sbuf[t];
-    nbr[o + t] = j;
+    M.nbr[o + t] = j;
     above += (j > (int32_t)i);
   }
   for (int s = 16; s > 0; s >>= 1) above += __shfl_xor_sync(0xffffffffu, above, s);
-  if (lane == 0) atomicAdd(pairCount, (unsigned long long)above);
+  if (lane == 0 && above)
+    atomicAdd(reinterpret_cast<unsigned long long*>(M.scal + SC_PAIRS), (unsigned long long)above);
 }
 
-inline int nblocks(int64_t work, int threads, int cap = 148*32) {
-  int64_t b = (work + threads - 1)/threads;
-  if (b < 1) b = 1;
-  return (int)(b < cap ? b : cap);
+int64_t asI64(double stored) {
+  int64_t v;
+  std::memcpy(&v, &stored, sizeof(v));
+  return v;
 }
 
-}  // namespace
-
-int build_ghosts(Problem& p) {
-  cudaStream_t st = p.stream;
-  p.G = 0;
-  int64_t ntot = p.n;
-  unsigned long long* hbits = reinterpret_cast<unsigned long long*>(p.d_scal);
-  for (int b = 0; b < 6; ++b) {
-    if (!p.prm.bcs.periodic[b >> 1]) continue;
-    const PlanarBC bc = p.prm.bcs.bc[b];
-    if (cudaMemsetAsync(hbits, 0, sizeof(unsigned long long), st) != cudaSuccess) return cuda_status(cudaGetLastError(), "memset");
-    ghost_hmax_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, p.groot, ntot, bc,
-                                                           p.prm.kernelExtent, hbits); ++p.launches;
-    ghost_flag_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, ntot, bc, p.prm.kernelExtent,
-                                                           hbits, p.counts); ++p.launches;
-    int64_t total = 0;
-    int rc = exclusive_scan_i32(p, p.counts, ntot, p.offsets, &total);
-    if (rc) return rc;
-    if (total == 0) continue;
-    rc = ensure_capacity_ghosts(p, (ntot - p.n) + total);
-    if (rc) return rc;
-    ghost_scatter_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, p.groot, p.gcode, ntot,
-                                                              p.counts, p.offsets, bc, b, p.d_err); ++p.launches;
-    ntot += total;
-  }
-  p.G = ntot - p.n;
-  return cuda_status(cudaGetLastError(), "build_ghosts");
+int asI32(double stored) {
+  int v;
+  std::memcpy(&v, &stored, sizeof(v));
+  return v;
 }
 
-int build_cells_and_csr(Problem& p) {
-  cudaStream_t st = p.stream;
-  const int64_t ntot = p.n + p.G;
-  if (ntot > INT_MAX) { set_error("too many nodes for 32-bit neighbor indices"); return SPHGPU_ERR_CAPACITY; }
-  // ---- grid
-  unsigned long long* bb = reinterpret_cast<unsigned long long*>(p.d_scal);
-  unsigned long long init[7];
-  for (int a = 0; a < 3; ++a) { init[a] = ~0ULL; init[3 + a] = 0ULL; }
-  init[6] = 0ULL;
-  cudaMemcpyAsync(bb, init, sizeof(init), cudaMemcpyHostToDevice, st);
-  node_bounds_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, p.groot, ntot, bb); ++p.launches;
-  unsigned long long res[7];
-  cudaMemcpyAsync(res, bb, sizeof(res), cudaMemcpyDeviceToHost, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_status(cudaGetLastError(), "bounds");
-  auto fromBits = [](unsigned long long b) {
-    const unsigned long long r = (b & 0x8000000000000000ULL) ? (b & 0x7fffffffffffffffULL) : ~b;
-    double d; memcpy(&d, &r, sizeof(d)); return d;
-  };
-  Grid g;
-  double hi[3];
-  for (int a = 0; a < 3; ++a) { g.lo[a] = fromBits(res[a]); hi[a] = fromBits(res[3 + a]); }
-  const double hmaxAll = fromBits(res[6]);
-  // cell size >= interaction radius kappa*max(1/lambda_min); the margin
-  // covers the libm difference of the eigenvalue solve for anisotropic H.
-  g.cell = p.prm.kernelExtent*hmaxAll*1.001;
-  if (!(g.cell > 0.0)) { set_error("non-positive smoothing scale"); return SPHGPU_ERR_NUMERIC; }
-  // Larger cells only widen the candidate set; cap the cell count so that
-  // 32-bit cell indices cannot overflow.
-  int64_t ncells = 1;
-  for (int attempt = 0; attempt < 64; ++attempt) {
-    ncells = 1;
-    for (int a = 0; a < 3; ++a) {
-      const double d = (hi[a] - g.lo[a])/g.cell;
-      const int64_t m = (int64_t)d + 1;
-      g.dim[a] = (int)(m < (1 << 20) ? m : (1 << 20));
-      ncells *= g.dim[a];
+int64_t grow(int64_t v) { return v + v/4 + 1024; }
+
+// Capacities for the next build, from the previous one (or first estimates).
+int plan_capacities(Batch& b) {
+  for (Problem* pp : b.mem) {
+    Problem& p = *pp;
+    const int64_t oldg = p.gcap, oldc = p.candcap, olde = p.ecap, oldcells = p.cellcap;
+    if (p.G > 0) SPH_TRY(ensure_capacity_ghosts(p, grow(p.G)));
+    const int64_t cellsNeed = p.ncells > 0 ? grow(p.ncells) : p.candcap/2 + 64;
+    if (cellsNeed + 1 > p.cellcap) {
+      cudaStreamSynchronize(b.stream);
+      cudaFree(p.cellStart); cudaFree(p.cellFill);
+      p.cellStart = nullptr; p.cellFill = nullptr;
+      p.cellcap = cellsNeed + 1;
+      if (cudaMalloc(&p.cellStart, sizeof(int64_t)*(p.cellcap + 1)) != cudaSuccess ||
+          cudaMalloc(&p.cellFill, sizeof(int32_t)*p.cellcap) != cudaSuccess) {
+        p.cellcap = 0;
+        set_error("cell list allocation failed");
+        return SPHGPU_ERR_NOMEM;
+      }
     }
-    if (ncells <= ((int64_t)1 << 26)) break;
-    g.cell *= 1.26;
+    // the first build guesses 32 entries per node; an overflow redoes it
+    SPH_TRY(ensure_capacity_entries(p, p.E > 0 ? p.E + p.E/8 : 32*p.n));
+    if (p.fillCap < 8) p.fillCap = p.maxCount > 0 ? p.maxCount + p.maxCount/4 + 8 : 64;
+    const int64_t tiles = ((p.candcap > p.cellcap ? p.candcap : p.cellcap) + 1023)/1024 + 2;
+    if (tiles > p.blockSumsCap) SPH_TRY(ensure_block_sums(p, tiles));
+    if (p.gcap != oldg || p.candcap != oldc || p.ecap != olde || p.cellcap != oldcells) b.memDirty = true;
+    // schedule: a warp per node once the 27-cell candidate set of the last
+    // build kept 32 lanes busy
+    const double candPerNode = p.ncells > 0 ? 27.0*(double)(p.n + p.G)/(double)p.ncells : 0.0;
+    const int req = p.nbrSchedule != NBR_SCHEDULE_AUTO ? p.nbrSchedule : b.nbrSchedule;
+    p.fillSchedule = (req == NBR_SCHEDULE_WARP || (req == NBR_SCHEDULE_AUTO && candPerNode > 384.0))
+                         ? NBR_SCHEDULE_WARP : NBR_SCHEDULE_THREAD;
+    p.grid.filterTol = p.nbrFilter ? kFilterTol : 0.0f;
   }
-  if (ncells > ((int64_t)1 << 26)) { set_error("cell grid too large"); return SPHGPU_ERR_CAPACITY; }
-  if (ncells + 1 > p.cellcap) {
-    cudaFree(p.cellStart); cudaFree(p.cellFill);
-    p.cellcap = ncells + 1;
-    if (cudaMalloc(&p.cellStart, sizeof(int64_t)*(p.cellcap + 1)) != cudaSuccess ||
-        cudaMalloc(&p.cellFill, sizeof(int32_t)*p.cellcap) != cudaSuccess) {
-      set_error("cell list allocation failed"); return SPHGPU_ERR_NOMEM;
-    }
+  b.memDirty = true;
+  return SPHGPU_OK;
+}
+
+int launch_build(Batch& b) {
+  cudaStream_t st = b.stream;
+  const int nm = (int)b.mem.size();
+  SPH_TRY(batch_upload(b));
+  BlockMap bm;
+  unsigned grid = 0;
+  // ---- ghosts: six planar boundaries in order, sizes kept on the device
+  build_init_kernel<<<(nm + 127)/128, 128, 0, st>>>(b.d_mem, nm); batch_count_launch(b);
+  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.n; }, kGhostThreads, &bm, &grid));
+  if (grid) { node_hmax_kernel<<<grid, kGhostThreads, 0, st>>>(b.d_mem, bm); batch_count_launch(b); }
+  BlockMap cap;
+  unsigned capGrid = 0;
+  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.candcap; }, kGhostThreads, &cap, &capGrid));
+  for (int bnd = 0; bnd < 6; ++bnd) {
+    bool any = false;
+    for (Problem* p : b.mem) any = any || p->prm.bcs.periodic[bnd >> 1];
+    if (!any) continue;
+    ghost_hmax_kernel<<<capGrid, kGhostThreads, 0, st>>>(b.d_mem, cap, bnd); batch_count_launch(b);
+    ghost_flag_kernel<<<capGrid, kGhostThreads, 0, st>>>(b.d_mem, cap, bnd); batch_count_launch(b);
+    SPH_TRY(batch_scan(b, SCAN_FLAGS));
+    ghost_scatter_kernel<<<capGrid, kGhostThreads, 0, st>>>(b.d_mem, cap, bnd); batch_count_launch(b);
+    ghost_advance_kernel<<<(nm + 127)/128, 128, 0, st>>>(b.d_mem, nm); batch_count_launch(b);
   }
-  int64_t* cellStart = reinterpret_cast<int64_t*>(p.cellStart);
-  for (int a = 0; a < 3; ++a) { p.gdim[a] = g.dim[a]; p.glo[a] = g.lo[a]; }
-  p.gcell = g.cell;
-  // ---- counting sort of all nodes by cell
-  cudaMemsetAsync(p.cellFill, 0, sizeof(int32_t)*ncells, st);
-  cell_index_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, ntot, g, p.cidx, p.cellFill); ++p.launches;
-  int64_t tot = 0;
-  int rc = exclusive_scan_i32(p, p.cellFill, ncells, cellStart, &tot);
-  if (rc) return rc;
-  cudaMemsetAsync(p.cellFill, 0, sizeof(int32_t)*ncells, st);
-  NbrCand* cand = reinterpret_cast<NbrCand*>(p.cand);
-  cell_scatter_kernel<<<nblocks(ntot, 256), 256, 0, st>>>(p.S, p.n, p.gpos, p.gcap, p.groot, ntot, p.cidx,
-                                                           cellStart, p.cellFill, p.sortedIdx, cand); ++p.launches;
-  // ---- neighbor counts, offsets, fill
-  const double k2 = p.prm.kernelExtent*p.prm.kernelExtent;
-  // Schedule: a thread per node while the 27-cell candidate set is small, a
-  // warp per node once it is large enough to keep 32 lanes busy.
-  const double candPerNode = 27.0*(double)ntot/(double)ncells;
-  const bool warpSchedule = p.nbrSchedule == NBR_SCHEDULE_WARP ||
-                            (p.nbrSchedule == NBR_SCHEDULE_AUTO && candPerNode > 384.0);
-  p.lastNbrSchedule = warpSchedule ? NBR_SCHEDULE_WARP : NBR_SCHEDULE_THREAD;
-  int* dMaxCount = reinterpret_cast<int*>(p.d_scal + 10);
-  cudaMemsetAsync(dMaxCount, 0, sizeof(int), st);
-  const int wthreads = 256;
-  const int64_t wblocks = (p.n*32 + wthreads - 1)/wthreads;
-  const int tthreads = 256;
-  const int64_t tblocks = (ntot + tthreads - 1)/tthreads;
-  if (warpSchedule) {
-    nbr_walk_kernel<false><<<(unsigned)wblocks, wthreads, 0, st>>>(p.S, p.n, g, cellStart, cand, k2, p.counts,
-                                                                     nullptr, nullptr, p.maxNbr, p.d_err,
-                                                                     dMaxCount, nullptr); ++p.launches;
-  } else {
-    nbr_thread_kernel<false><<<(unsigned)tblocks, tthreads, 0, st>>>(p.n, ntot, g, cellStart, cand, k2, p.counts,
-                                                                       nullptr, nullptr, 0, dMaxCount, p.d_err,
-                                                                       nullptr); ++p.launches;
+  // ---- cell grid and counting sort of all nodes by cell
+  bounds_init_kernel<<<(nm + 127)/128, 128, 0, st>>>(b.d_mem, nm); batch_count_launch(b);
+  node_bounds_kernel<<<capGrid, kGhostThreads, 0, st>>>(b.d_mem, cap); batch_count_launch(b);
+  grid_kernel<<<(nm + 127)/128, 128, 0, st>>>(b.d_mem, nm); batch_count_launch(b);
+  BlockMap cm;
+  unsigned cgrid = 0;
+  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.cellcap; }, kGhostThreads, &cm, &cgrid));
+  cell_zero_kernel<<<cgrid, kGhostThreads, 0, st>>>(b.d_mem, cm); batch_count_launch(b);
+  cell_index_kernel<<<capGrid, kGhostThreads, 0, st>>>(b.d_mem, cap); batch_count_launch(b);
+  SPH_TRY(batch_scan(b, SCAN_CELLS));
+  cell_zero_kernel<<<cgrid, kGhostThreads, 0, st>>>(b.d_mem, cm); batch_count_launch(b);
+  cell_scatter_kernel<<<capGrid, kGhostThreads, 0, st>>>(b.d_mem, cap); batch_count_launch(b);
+  // ---- neighbor counts, offsets, lists
+  int maxNbr = 0, tcap = 1, wmax = 0;
+  for (Problem* p : b.mem) {
+    maxNbr = p->maxNbr > maxNbr ? p->maxNbr : maxNbr;
+    if (p->fillSchedule == NBR_SCHEDULE_WARP) wmax = p->fillCap > wmax ? p->fillCap : wmax;
+    else tcap = p->fillCap > tcap ? p->fillCap : tcap;
   }
-  int64_t E = 0;
-  rc = exclusive_scan_i32(p, p.counts, p.n, p.offsets, &E);
-  if (rc) return rc;
-  int herr = 0, maxCount = 0;
-  cudaMemcpyAsync(&herr, p.d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(&maxCount, dMaxCount, sizeof(int), cudaMemcpyDeviceToHost, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_status(cudaGetLastError(), "nbr count");
-  if (herr & (DERR_NBR_CAPACITY | DERR_GHOST_CHAIN)) cudaMemsetAsync(p.d_err, 0, sizeof(int), st);
-  if ((herr & DERR_NBR_CAPACITY) || maxCount > p.maxNbr) {
-    set_error("a node has more neighbors than max_neighbors");
-    return SPHGPU_ERR_CAPACITY;
-  }
-  if (herr & DERR_GHOST_CHAIN) {
-    set_error("a ghost image was imaged twice through one periodic axis");
-    return SPHGPU_ERR_UNSUPPORTED;
-  }
-  p.maxCount = maxCount;
-  rc = ensure_capacity_entries(p, E);
-  if (rc) return rc;
-  unsigned long long* pc = reinterpret_cast<unsigned long long*>(p.d_scal + 8);
-  cudaMemsetAsync(pc, 0, sizeof(unsigned long long), st);
-  // per-thread list capacity: shrink the block until the lists fit
+  const int wthreads = 256, tthreads = 256;
   int fthreads = tthreads;
-  const int tcap = maxCount > 0 ? maxCount : 1;
   while (fthreads > 32 && sizeof(int32_t)*(size_t)fthreads*tcap > 96*1024) fthreads >>= 1;
-  const bool threadFill = !warpSchedule && sizeof(int32_t)*(size_t)fthreads*tcap <= 200*1024;
-  if (threadFill) {
+  if (sizeof(int32_t)*(size_t)fthreads*tcap > 200*1024) {
+    // lists too long for a thread each: these members take the warp schedule
+    for (Problem* p : b.mem) {
+      if (p->fillSchedule != NBR_SCHEDULE_WARP) {
+        p->fillSchedule = NBR_SCHEDULE_WARP;
+        wmax = p->fillCap > wmax ? p->fillCap : wmax;
+      }
+    }
+  }
+  BlockMap tmap, wmap, fmap;
+  unsigned tgrid = 0, wgrid = 0, fgrid = 0;
+  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.fillSchedule == NBR_SCHEDULE_WARP ? (int64_t)0 : p.candcap; },
+                          tthreads, &tmap, &tgrid));
+  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.fillSchedule == NBR_SCHEDULE_WARP ? 32*p.n : (int64_t)0; },
+                          wthreads, &wmap, &wgrid));
+  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.fillSchedule == NBR_SCHEDULE_WARP ? (int64_t)0 : p.candcap; },
+                          fthreads, &fmap, &fgrid));
+  for (Problem* p : b.mem) p->lastNbrSchedule = p->fillSchedule;
+  b.lastNbrSchedule = nm ? b.mem[0]->lastNbrSchedule : 0;
+  if (tgrid) { nbr_thread_kernel<false><<<tgrid, tthreads, 0, st>>>(b.d_mem, tmap, 0, maxNbr); batch_count_launch(b); }
+  if (wgrid) { nbr_walk_kernel<false><<<wgrid, wthreads, 0, st>>>(b.d_mem, wmap, 0, maxNbr); batch_count_launch(b); }
+  SPH_TRY(batch_scan(b, SCAN_COUNTS));
+  if (fgrid) {
     const size_t smem = sizeof(int32_t)*(size_t)fthreads*tcap;
     if (smem > 48*1024) {
       const cudaError_t e = cudaFuncSetAttribute(nbr_thread_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)smem);
       if (e != cudaSuccess) return cuda_status(e, "nbr smem attribute");
     }
-    const int64_t fblocks = (ntot + fthreads - 1)/fthreads;
-    nbr_thread_kernel<true><<<(unsigned)fblocks, fthreads, smem, st>>>(p.n, ntot, g, cellStart, cand, k2, p.counts,
-                                                                         p.offsets, p.nbr, tcap, nullptr, p.d_err,
-                                                                         pc); ++p.launches;
-  } else {
+    nbr_thread_kernel<true><<<fgrid, fthreads, smem, st>>>(b.d_mem, fmap, tcap, maxNbr); batch_count_launch(b);
+  }
+  if (wgrid) {
     // bitonic sort pads each warp's list to a power of two >= 32
     int wcap = 32;
-    while (wcap < maxCount) wcap <<= 1;
+    while (wcap < wmax) wcap <<= 1;
     const size_t smem = sizeof(int32_t)*(wthreads/32)*(size_t)wcap;
     if (smem > 48*1024) {
       const cudaError_t e = cudaFuncSetAttribute(nbr_walk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)smem);
       if (e != cudaSuccess) return cuda_status(e, "nbr smem attribute");
     }
-    nbr_walk_kernel<true><<<(unsigned)wblocks, wthreads, smem, st>>>(p.S, p.n, g, cellStart, cand, k2, p.counts,
-                                                                       p.offsets, p.nbr, wcap, p.d_err, nullptr,
-                                                                       pc); ++p.launches;
+    nbr_walk_kernel<true><<<wgrid, wthreads, smem, st>>>(b.d_mem, wmap, wcap, maxNbr); batch_count_launch(b);
   }
-  unsigned long long pairs = 0;
-  cudaMemcpyAsync(&pairs, pc, sizeof(pairs), cudaMemcpyDeviceToHost, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_status(cudaGetLastError(), "nbr fill");
-  p.E = E;
-  p.pairs = (int64_t)pairs;
-  return SPHGPU_OK;
+  return cuda_status(cudaGetLastError(), "neighbor build");
+}
+
+}  // namespace
+
+// Ghosts and ConnectivityMap of every member: all stages launched with the
+// sizes kept on the device, then one read-back of the sizes; a capacity
+// overflow grows the buffers and repeats the build.
+int build_connectivity(Batch& b) {
+  const int nm = (int)b.mem.size();
+  for (Problem* p : b.mem) {
+    if (p->n + p->gcap > INT_MAX) { set_error("too many nodes for 32-bit neighbor indices"); return SPHGPU_ERR_CAPACITY; }
+  }
+  for (int attempt = 0; attempt < 6; ++attempt) {
+    SPH_TRY(plan_capacities(b));
+    SPH_TRY(launch_build(b));
+    const int slots[6] = {SC_G, SC_TOTAL, SC_MAXCOUNT, SC_PAIRS, SC_NCELLS, -1};
+    std::vector<double> r;
+    SPH_TRY(batch_gather(b, slots, 6, r));
+    bool redo = false;
+    for (int m = 0; m < nm; ++m) {
+      Problem& p = *b.mem[m];
+      const int herr = (int)r[m*6 + 5];
+      p.G = asI64(r[m*6]);
+      p.ntot = p.n + p.G;
+      p.E = asI64(r[m*6 + 1]);
+      p.maxCount = asI32(r[m*6 + 2]);
+      p.pairs = asI64(r[m*6 + 3]);
+      p.ncells = asI64(r[m*6 + 4]);
+      if (herr) cudaMemsetAsync(p.d_err, 0, sizeof(int), b.stream);
+      if ((herr & DERR_NBR_CAPACITY) || p.maxCount > p.maxNbr) {
+        set_error("a node has more neighbors than max_neighbors");
+        return SPHGPU_ERR_CAPACITY;
+      }
+      if (herr & DERR_GHOST_CHAIN) {
+        set_error("a ghost image was imaged twice through one periodic axis");
+        return SPHGPU_ERR_UNSUPPORTED;
+      }
+      if (herr & DERR_NONPOSITIVE) {
+        set_error("non-positive or non-finite smoothing scale");
+        return SPHGPU_ERR_NUMERIC;
+      }
+      if (herr & DERR_GHOST_CAPACITY) { p.G = 2*p.gcap; redo = true; }        // ghost count unknown: double
+      if (herr & DERR_ENTRY_CAPACITY) redo = true;                           // p.E is the true entry count
+      if (herr & DERR_LIST_CAPACITY) { p.fillCap = p.maxCount + p.maxCount/4 + 8; redo = true; }
+      else if (p.fillCap > 2*p.maxCount + 64) p.fillCap = 0;                 // re-plan a tighter list
+    }
+    if (!redo) return SPHGPU_OK;
+    SPH_CHECK(cudaStreamSynchronize(b.stream));
+  }
+  set_error("neighbor build: capacities did not converge");
+  return SPHGPU_ERR_CAPACITY;
 }
 
 }  // namespace sphgpu

@@ -93,7 +93,7 @@ enum RecField {
   RECW = 20
 };
 
-// Read-only physics parameters, passed by value to kernels.
+// Read-only physics parameters of one problem (in its Member descriptor).
 struct Params {
   TableDev W;
   const double* nperh;     // TableKernel nPerh table
@@ -106,8 +106,19 @@ struct Params {
   int compatible, XSPH, correctVelGrad, linearInExp, quadInExp, useVelMagDt;
   int HUpdate, densityUpdate, gradh;
   int hydro;               // SPHGPU_HYDRO_*
+  double dtMin, dtMax, dtGrowth;   // Integrator time-step controls
   BoxBCs bcs;
 };
+
+// Uniform cell grid of one member's neighbor search.
+struct Grid {
+  double lo[3];
+  double cell;
+  int dim[3];
+  float filterTol;     // relative band of the FP32 neighbor pre-test (0: exact test only)
+};
+
+struct Batch;
 
 struct Problem {
   sphgpu_config cfg{};
@@ -123,6 +134,9 @@ struct Problem {
   int maxCount = 0;         // largest neighbor count of the current connectivity
   int nbrSchedule = 0;      // NBR_SCHEDULE_* requested for the neighbor walk
   int lastNbrSchedule = 0;  // schedule the last build used
+  bool nbrFilter = true;    // FP32 pre-test in the neighbor walk (exact either way)
+  int fillCap = 0;          // neighbor-list capacity planned for the fill pass
+  int fillSchedule = 0;     // schedule planned for this build (NBR_SCHEDULE_THREAD/WARP)
 
   double* S = nullptr;
   double* S0 = nullptr;
@@ -139,16 +153,17 @@ struct Problem {
   double* gpos = nullptr;   // [3][gcap] ghost positions during creation
 
   // cell list
-  double* cand = nullptr;       // [candcap] 80-byte records x,y,z,H6,index (cell order)
+  double* cand = nullptr;       // cell order: [candcap] 64-byte records (FP64 x,y,z, index,
+                                // FP32 H) then [candcap] 48-byte FP64 H
   int32_t* cidx = nullptr;      // [candcap] cell index of each node (unsorted)
   int32_t* sortedIdx = nullptr; // [candcap]
   int64_t candcap = 0;
-  int32_t* cellStart = nullptr; // [ncells+1]
+  int64_t* cellStart = nullptr; // [ncells+1]
   int32_t* cellFill = nullptr;  // [ncells]
   int64_t cellcap = 0;
-  int gdim[3] = {1, 1, 1};
-  double glo[3] = {0, 0, 0};
-  double gcell = 1.0;
+  int64_t ncells = 0;
+  int64_t ntot = 0;             // n + ghosts created so far (ghost passes)
+  Grid grid{};
 
   int32_t* counts = nullptr;    // [n]
   int64_t* offsets = nullptr;   // [n+1]
@@ -167,14 +182,16 @@ struct Problem {
   int64_t* blockSums = nullptr; // scan scratch
   int64_t blockSumsCap = 0;
   int* d_err = nullptr;         // device error word
-  double* d_scal = nullptr;     // small reduction results (16 doubles)
+  double* d_scal = nullptr;     // NSCAL scalar slots (ScalSlot)
   double* d_red = nullptr;      // reduction partials
   int64_t redcap = 0;
   double* staging = nullptr;    // host<->device AoS staging, 9*n doubles
+  double* hmaxi = nullptr;      // [n] 1/min(eig(H)) of each internal node, per build
   double* pinned = nullptr;     // pinned host staging for get/set
   int64_t pinnedcap = 0;
 
-  int64_t launches = 0;         // kernels launched by this problem (diagnostics)
+  Batch* solo = nullptr;        // this problem as a batch of one
+  int64_t launches = 0;         // kernels launched for this problem (diagnostics)
   bool haveNbrs = false;
   bool haveDerivs = false;
   double time = 0.0;
@@ -188,6 +205,9 @@ enum DevError {
   DERR_GHOST_CHAIN = 2,
   DERR_H_CLAMP = 4,
   DERR_NONPOSITIVE = 8,
+  DERR_GHOST_CAPACITY = 16,   // more ghosts than the ghost buffers hold (build is redone)
+  DERR_ENTRY_CAPACITY = 32,   // more CSR entries than the entry buffers hold (build is redone)
+  DERR_LIST_CAPACITY = 64,    // a neighbor list longer than the fill pass's list (build is redone)
 };
 
 // Neighbor-walk schedules (values of sphgpu_set_schedule's "neighbor walk").
@@ -197,38 +217,201 @@ enum NbrSchedule {
   NBR_SCHEDULE_WARP = 2,     // warp per node
 };
 
-// ---- launchers (ghosts/neighbors: nbrs.cu; physics: sph.cu) ----
-int build_ghosts(Problem& p);
-int build_cells_and_csr(Problem& p);
-void pack_records(Problem& p);
-void launch_gradh(Problem& p);
-void launch_eval_sph_fp64(Problem& p);
-void launch_eval_sph_mixed(Problem& p);
-void launch_sum_density(Problem& p);
-void launch_update(Problem& p, const double* d_dt, double scale, bool timeAdvanceOnly);
-void launch_compatible_energy(Problem& p, const double* d_dt, double scale);
-void launch_enforce_boundaries(Problem& p);
-void launch_eos(Problem& p);
-void launch_dt(Problem& p, double* d_out);
-void launch_select_dt(Problem& p, double* d_dt, double* d_lastDt);
-void launch_conservation(Problem& p, double* d_out8);
-void launch_zero_derivs(Problem& p);
-// CRKSPH (crk.cu)
-int crk_prepare(Problem& p);
-void launch_crk_sum_volume(Problem& p);
-void launch_crk_volume_from_density(Problem& p);
-void launch_crk_sum_density(Problem& p);
-void launch_crk_initialize(Problem& p);
-void launch_crk_eval(Problem& p);
+// ---- batched launches -------------------------------------------------
+//
+// Every kernel runs over a set of independent problems ("members") in one
+// launch.  A member is described on the device by a Member record (its
+// buffers, sizes and parameters); the blocks of a launch are dealt to the
+// members by a block map: first[m] is the first block of member m and
+// first[nmem] the grid size.  A single problem is a batch of one member.
+
+// Slots of a member's small device scalar array (64-bit words).
+enum ScalSlot {
+  SC_HMAX = 0,         // ghost hmax of the current boundary (double bits)
+  SC_BOUNDS = 1,       // 7 ordered-bit words: lo[3], hi[3], max h
+  SC_PAIRS = 8,        // unordered pairs of the connectivity (u64)
+  SC_MAXCOUNT = 9,     // largest neighbor count (int)
+  SC_MINDT = 10,       // min dt vote before the Courant factor (double bits)
+  SC_VOTE = 11,        // cfl * min dt
+  SC_DT = 12,          // dt of the current step
+  SC_LASTDT = 13,      // dt of the previous step
+  SC_DTOUT = 14,       // sphgpu_dt result
+  SC_TOTAL = 15,       // total of the last prefix sum (i64)
+  SC_CONS = 16,        // 8 conservation sums
+  SC_MAXCOND = 24,     // largest condition number of H over the internal nodes (double bits)
+  // sizes of the current connectivity, produced and read on the device (i64)
+  SC_NTOT = 25,        // internal nodes + ghosts made so far (ghost passes)
+  SC_G = 26,           // ghosts
+  SC_NCELLS = 27,      // cells of the grid
+  SC_GRID = 28,        // lo[3], cell (doubles), dim[3] (i64)
+  NSCAL = 40
+};
+
+// Sizes and grid of the current connectivity (device side).
+__device__ __forceinline__ int64_t scalI(const double* scal, int slot) {
+  return reinterpret_cast<const int64_t*>(scal)[slot];
+}
+__device__ __forceinline__ void setScalI(double* scal, int slot, int64_t v) {
+  reinterpret_cast<int64_t*>(scal)[slot] = v;
+}
+
+struct Member {
+  Params prm;
+  double* S; double* S0; double* D; double* K;
+  double* rec; double* crec; double* mrec;
+  double* gpos; double* pacc; double* scal; double* red; double* hmaxi;
+  int32_t* groot; int32_t* cidx; int32_t* sortedIdx; int32_t* counts; int32_t* nbr; int32_t* cellFill;
+  uint32_t* gcode;
+  int64_t* offsets; int64_t* cellStart; int64_t* blockSums;
+  void* cand;
+  const float* coefF;
+  int* err;
+  int64_t n, G, ntot, gcap, E, ecap, candcap, ncells, cellcap;
+  Grid grid;
+};
+
+struct BlockMap {
+  const int32_t* first;
+  int nmem;
+};
+
+struct MemberBlock {
+  int m;            // member index
+  int64_t block;    // block index within the member
+  int blocks;       // blocks of the member in this launch
+};
+
+// The member owning this block: the largest m with first[m] <= blockIdx.x
+// (members with no blocks are skipped by construction).
+__device__ __forceinline__ MemberBlock memberBlock(const BlockMap& bm) {
+  // a single member needs no table (the launch carries no map)
+  if (bm.nmem == 1) return MemberBlock{0, (int64_t)blockIdx.x, (int)gridDim.x};
+  int lo = 0, hi = bm.nmem - 1;
+  const int b = (int)blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(bm.first + mid) <= b) lo = mid; else hi = mid - 1;
+  }
+  const int f0 = __ldg(bm.first + lo);
+  return MemberBlock{lo, (int64_t)(b - f0), __ldg(bm.first + lo + 1) - f0};
+}
+
+struct Batch {
+  std::vector<Problem*> mem;
+  cudaStream_t stream = nullptr;
+  bool ownStream = false;
+  Member* d_mem = nullptr;       // device descriptors of the latest upload
+  // Descriptor uploads rotate through kMemSlots slots (pinned host + device),
+  // so an upload never waits for the kernels that read an earlier one.
+  static constexpr int kMemSlots = 8;
+  Member* d_memRing = nullptr;
+  Member* h_memRing = nullptr;
+  int memcap = 0;                // members per slot
+  int memSlot = 0;
+  cudaEvent_t memEvents[kMemSlots] = {};
+  bool memDirty = true;
+  int32_t* d_maps = nullptr;     // block-map ring (device)
+  int32_t* h_maps = nullptr;     // pinned host side of the ring
+  int64_t mapcap = 0, mappos = 0;
+  double* d_gather = nullptr;    // gathered member scalars
+  double* h_gather = nullptr;
+  int64_t gathercap = 0;
+  int64_t launches = 0;
+  int nbrSchedule = 0;           // requested neighbor-walk schedule
+  int lastNbrSchedule = 0;
+  int evalThreads = 128;         // threads per block of the pair-loop kernels (64, 128 or 256)
+  // CUDA-graph replay of the part of the RK2 step after the connectivity
+  // (api.cu): captured once per buffer layout, replayed every step.
+  bool useGraph = false;
+  bool capturing = false;        // stream capture in progress: maps go to the arena
+  bool capacityGrids = false;    // (n + ghosts)-sized kernels sized for the buffer capacity
+  cudaGraphExec_t graphExec = nullptr;
+  uint64_t graphKey = 0;
+  int64_t graphLaunches = 0;     // kernel nodes of the captured graph
+  cudaStream_t sideStream = nullptr;
+  int32_t* d_mapArena = nullptr; // block maps referenced by the captured graph
+  int64_t mapArenaCap = 0, mapArenaPos = 0;
+  Member* d_memGraph = nullptr;  // descriptor slot read by the captured graph
+  Member* h_memGraph = nullptr;
+  int memGraphCap = 0;
+  cudaEvent_t memGraphEvent = nullptr;
+};
+
+// batch.cu
+int batch_init(Batch& b, cudaStream_t stream);
+void batch_free(Batch& b);
+int batch_upload(Batch& b);                                  // member descriptors -> device (if dirty)
+Member describe_member(const Problem& p);                    // a problem's descriptor (host)
+// block map from per-member block counts; *grid = total blocks
+int batch_map(Batch& b, const std::vector<int64_t>& blocks, BlockMap* bm, unsigned* grid);
+template<class F>
+int batch_map_items(Batch& b, F items, int threads, BlockMap* bm, unsigned* grid) {
+  std::vector<int64_t> blocks(b.mem.size());
+  for (size_t m = 0; m < b.mem.size(); ++m) {
+    const int64_t k = items(*b.mem[m]);
+    blocks[m] = k > 0 ? (k + threads - 1)/threads : 0;
+  }
+  return batch_map(b, blocks, bm, grid);
+}
+// member scalar slots -> host, out[m*nslots + s]; synchronises the stream
+int batch_gather(Batch& b, const int* slots, int nslots, std::vector<double>& out);
+void batch_count_launch(Batch& b);
+// zero (or set) one scalar slot of every member
+void batch_set_scal(Batch& b, int slot, double value);
+// exclusive prefix sums of every member (in/out chosen by `which`), totals in SC_TOTAL
+enum ScanWhich { SCAN_FLAGS = 0, SCAN_CELLS = 1, SCAN_COUNTS = 2 };
+int batch_scan(Batch& b, int which);
+
+// ---- stages (ghosts/neighbors: nbrs.cu; SPH: sph.cu; mixed: sph_mixed.cu; CRKSPH: crk.cu)
+int build_connectivity(Batch& b);     // ghosts + ConnectivityMap, device-sized
+// FP64 pair records of the members that read them next (PACK_ALL: every member)
+enum PackNeed { PACK_ALL = 0, PACK_FOR_EVAL = 1, PACK_FOR_FINALIZE = 2 };
+int pack_records(Batch& b, int need = PACK_ALL);
+int launch_gradh(Batch& b);
+int launch_eval_sph_fp64(Batch& b);
+int launch_eval_sph_mixed(Batch& b);
+int launch_sum_density(Batch& b);
+int launch_update(Batch& b, double scale, bool timeAdvanceOnly);
+int launch_compatible_energy(Batch& b, double scale);
+int launch_enforce_boundaries(Batch& b);
+int launch_eos(Batch& b);
+int launch_dt(Batch& b, int slot);                          // min dt vote bits -> slot
+int launch_select_dt(Batch& b);                             // SC_DT from the vote and SC_LASTDT
+int launch_finish_step(Batch& b);                           // SC_LASTDT = SC_DT
+int launch_conservation(Batch& b);                          // SC_CONS
+int launch_zero_derivs(Batch& b);
+int prepare_mixed(Batch& b);
+int crk_prepare(Batch& b);
+int launch_crk_sum_volume(Batch& b, bool startupOnly);      // CRKSumVolume members
+int launch_crk_volume_from_density(Batch& b, bool startupOnly);  // CRKMassOverDensity members
+int launch_crk_sum_density(Batch& b);
+int launch_crk_initialize(Batch& b);
+int launch_crk_eval(Batch& b);                              // plain FP64 CRKSPH members
+int launch_crk_eval_mixed(Batch& b);                        // mixed-precision CRKSPH members (crk_mixed.cu)
+
+// one CheapSynchronousRK2 step of every member (api.cu)
+int batch_step_rk2(Batch& b);
+// device bytes held by a problem, from its buffer capacities (api.cu)
+int64_t problem_bytes(const Problem& p);
 
 // device buffer helpers (api.cu)
 int ensure_capacity_ghosts(Problem& p, int64_t gcap);
 int ensure_capacity_entries(Problem& p, int64_t ecap);
 int ensure_block_sums(Problem& p, int64_t nblocks);
-// exclusive prefix sum of int32 counts into out[0..n] (int64), total returned on the host
-int exclusive_scan_i32(Problem& p, const int32_t* in, int64_t n, int64_t* out, int64_t* total);
 void set_error(const std::string& msg);
 int cuda_status(cudaError_t e, const char* where);
+
+#define SPH_CHECK(call)                                                 \
+  do {                                                                  \
+    const cudaError_t e__ = (call);                                     \
+    if (e__ != cudaSuccess) return cuda_status(e__, #call);             \
+  } while (0)
+
+#define SPH_TRY(expr)                                                   \
+  do {                                                                  \
+    const int rc__ = (expr);                                            \
+    if (rc__ != SPHGPU_OK) return rc__;                                 \
+  } while (0)
 
 // host TableKernel construction (table.cc)
 void build_table_kernel(int kernelType, int numPoints, std::vector<double>& coef6, std::vector<double>& nperh,
@@ -237,3 +420,7 @@ double table_kernel_value(const std::vector<double>& coef6, int n, double stepSi
                           double eta, double Hdet);
 
 }  // namespace sphgpu
+
+// Handle types of the C-ABI (include/sphgpu.h).
+struct sphgpu_problem : public sphgpu::Problem {};
+struct sphgpu_batch : public sphgpu::Batch {};

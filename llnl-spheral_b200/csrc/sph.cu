@@ -32,10 +32,7 @@ constexpr double kFltMin = 1.17549435082228750797e-38;   // FLT_MIN
 constexpr double kFltMax = 3.40282346638528859812e+38;   // FLT_MAX
 constexpr double kDblEps = 2.220446049250313e-16;
 
-inline int nblk(int64_t work, int threads) {
-  int64_t b = (work + threads - 1)/threads;
-  return (int)(b < 1 ? 1 : b);
-}
+constexpr int kConsBlocks = 148*4;   // conservation partial sums per member
 
 __device__ __forceinline__ double ldg(const double* p) { return __ldg(p); }
 
@@ -67,39 +64,50 @@ __device__ __forceinline__ Sym sels(bool c, const Sym& a, const Sym& b) {
 }
 
 // ---------------------------------------------------------------- records
-__global__ void pack_records_kernel(const double* S, int64_t n, const int32_t* groot, const uint32_t* gcode,
-                                    int64_t ntot, BoxBCs bcs, double* rec) {
-  for (int64_t k = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; k < ntot; k += (int64_t)gridDim.x*blockDim.x) {
-    const int64_t r = k < n ? k : groot[k - n];
-    V3 x{S[S_X*n + r], S[S_Y*n + r], S[S_Z*n + r]};
-    if (k >= n) x = ghostPosition(bcs, x, gcode[k - n]);
-    const Sym H{S[(S_H + 0)*n + r], S[(S_H + 1)*n + r], S[(S_H + 2)*n + r],
-                S[(S_H + 3)*n + r], S[(S_H + 4)*n + r], S[(S_H + 5)*n + r]};
-    const double m = S[S_M*n + r], rho = S[S_RHO*n + r], P = S[S_P*n + r];
-    const double somega = safeInv(S[S_OMEGA*n + r], 1.0e-30);
-    double2* q = reinterpret_cast<double2*>(rec + k*RECW);
-    q[0] = make_double2(x.x, x.y);
-    q[1] = make_double2(x.z, S[S_VX*n + r]);
-    q[2] = make_double2(S[S_VY*n + r], S[S_VZ*n + r]);
-    q[3] = make_double2(m, rho);
-    q[4] = make_double2(S[S_CS*n + r], sdet(H));
-    q[5] = make_double2(H.xx, H.xy);
-    q[6] = make_double2(H.xz, H.yy);
-    q[7] = make_double2(H.yz, H.zz);
-    q[8] = make_double2(somega*P/(rho*rho), m/rho);
-    q[9] = make_double2(P, somega);
-  }
+__global__ void __launch_bounds__(256) pack_records_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int64_t k = mb.block*blockDim.x + threadIdx.x;
+  const int64_t n = M.n;
+  if (k >= n + scalI(M.scal, SC_G)) return;
+  const double* S = M.S;
+  const int64_t r = k < n ? k : M.groot[k - n];
+  V3 x{S[S_X*n + r], S[S_Y*n + r], S[S_Z*n + r]};
+  if (k >= n) x = ghostPosition(M.prm.bcs, x, M.gcode[k - n]);
+  const Sym H{S[(S_H + 0)*n + r], S[(S_H + 1)*n + r], S[(S_H + 2)*n + r],
+              S[(S_H + 3)*n + r], S[(S_H + 4)*n + r], S[(S_H + 5)*n + r]};
+  const double m = S[S_M*n + r], rho = S[S_RHO*n + r], P = S[S_P*n + r];
+  const double somega = safeInv(S[S_OMEGA*n + r], 1.0e-30);
+  double2* q = reinterpret_cast<double2*>(M.rec + k*RECW);
+  q[0] = make_double2(x.x, x.y);
+  q[1] = make_double2(x.z, S[S_VX*n + r]);
+  q[2] = make_double2(S[S_VY*n + r], S[S_VZ*n + r]);
+  q[3] = make_double2(m, rho);
+  q[4] = make_double2(S[S_CS*n + r], sdet(H));
+  q[5] = make_double2(H.xx, H.xy);
+  q[6] = make_double2(H.xz, H.yy);
+  q[7] = make_double2(H.yz, H.zz);
+  q[8] = make_double2(somega*P/(rho*rho), m/rho);
+  q[9] = make_double2(P, somega);
 }
 
 // ---------------------------------------------------------------- derivatives
 // One directed pair (i, j) of SPHHydroBase::evaluateDerivatives, formed in
 // owner orientation, accumulated into node i.
-template<bool XSPH, bool TENSILE, bool COMPAT>
-__global__ void __launch_bounds__(128) sph_eval_fp64_kernel(Params P, const double* rec, int64_t n,
-                                                            const int64_t* offsets, const int32_t* nbr,
-                                                            double* D, double* pacc, int64_t ecap) {
-  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+template<bool XSPH, bool TENSILE, bool COMPAT, bool SOLO>
+__global__ void __launch_bounds__(128) sph_eval_fp64_kernel(const Member* mem, BlockMap bm, const Member single) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = SOLO ? single : mem[mb.m];   // one member: read from the kernel parameters
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const Params& P = MB.prm;
+  const double* rec = MB.rec;
+  const int64_t* offsets = MB.offsets;
+  const int32_t* nbr = MB.nbr;
+  double* D = MB.D;
+  double* pacc = MB.pacc;
+  const int64_t ecap = MB.ecap;
   const Rec I = loadRec(rec, i);
   double rhoSum = 0.0, norm = 0.0, wns = 0.0, maxvp = 0.0, effvp = 0.0, viscW = 0.0, DepsDt = 0.0;
   double XSPHw = 0.0;
@@ -294,11 +302,17 @@ __global__ void __launch_bounds__(128) sph_eval_fp64_kernel(Params P, const doub
 }
 
 // ---------------------------------------------------------------- grad-h
-__global__ void gradh_kernel(Params P, const double* rec, int64_t n, const int64_t* offsets, const int32_t* nbr,
-                             double* S) {
-  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) gradh_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int64_t k0 = offsets[i], k1 = offsets[i + 1];
+  const Params& P = MB.prm;
+  const double* rec = MB.rec;
+  const int32_t* nbr = MB.nbr;
+  double* S = MB.S;
+  const int64_t k0 = MB.offsets[i], k1 = MB.offsets[i + 1];
   if (k1 == k0) { S[S_OMEGA*n + i] = 1.0; return; }
   const Rec I = loadRec(rec, i);
   const double W0 = tableKernel(P.W, 0.0, I.Hdet);
@@ -320,16 +334,21 @@ __global__ void gradh_kernel(Params P, const double* rec, int64_t n, const int64
 }
 
 // ---------------------------------------------------------------- sum density
-__global__ void sum_density_kernel(Params P, const double* rec, int64_t n, const int64_t* offsets,
-                                   const int32_t* nbr, double* S) {
-  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) sum_density_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const Params& P = MB.prm;
+  const double* rec = MB.rec;
+  const int32_t* nbr = MB.nbr;
   const V3 ri{ldg(rec + i*RECW + R_X), ldg(rec + i*RECW + R_Y), ldg(rec + i*RECW + R_Z)};
   const double mi = ldg(rec + i*RECW + R_M), Hdeti = ldg(rec + i*RECW + R_HDET);
   const double W0 = tableKernel(P.W, 0.0, Hdeti);
   double rho = 0.0;
   bool selfDone = false;
-  const int64_t k0 = offsets[i], k1 = offsets[i + 1];
+  const int64_t k0 = MB.offsets[i], k1 = MB.offsets[i + 1];
   for (int64_t k = k0; k < k1; ++k) {
     const int32_t j = __ldg(nbr + k);
     if (!selfDone && j > (int32_t)i) { rho += mi*W0; selfDone = true; }
@@ -339,16 +358,23 @@ __global__ void sum_density_kernel(Params P, const double* rec, int64_t n, const
     rho += J.m*tableKernel(P.W, eta, J.Hdet);
   }
   if (!selfDone) rho += mi*W0;
-  S[S_RHO*n + i] = rho;
+  MB.S[S_RHO*n + i] = rho;
 }
 
 // ---------------------------------------------------------------- compatible energy
-__global__ void compatible_energy_kernel(int64_t n, const int64_t* offsets, const int32_t* nbr,
-                                         const int32_t* groot, const double* pacc, int64_t ecap,
-                                         const double* D, double* S, const double* d_dt, double scale) {
-  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) compatible_energy_kernel(const Member* mem, BlockMap bm, double scale) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double multiplier = scale*(*d_dt);
+  const double* D = MB.D;
+  double* S = MB.S;
+  const int32_t* nbr = MB.nbr;
+  const int32_t* groot = MB.groot;
+  const double* pacc = MB.pacc;
+  const int64_t ecap = MB.ecap;
+  const double multiplier = scale*MB.scal[SC_DT];
   const double hdt = 0.5*multiplier;
   const double weighti = fabs(D[D_DEPSDT*n + i]) + kDblEps;
   const double mi = S[S_M*n + i];
@@ -356,7 +382,7 @@ __global__ void compatible_energy_kernel(int64_t n, const int64_t* offsets, cons
   const V3 ai{D[(D_DVDT + 0)*n + i], D[(D_DVDT + 1)*n + i], D[(D_DVDT + 2)*n + i]};
   const V3 vi12 = vadd(vi, vmul(ai, hdt));
   double DepsDti = 0.0;
-  const int64_t k0 = offsets[i], k1 = offsets[i + 1];
+  const int64_t k0 = MB.offsets[i], k1 = MB.offsets[i + 1];
   for (int64_t k = k0; k < k1; ++k) {
     const int32_t j = __ldg(nbr + k);
     const int64_t r = j < n ? (int64_t)j : (int64_t)__ldg(groot + (j - n));
@@ -385,11 +411,18 @@ __device__ __forceinline__ bool hInsideBounds(const Sym& H, double hmin, double 
   return vmin(ev) > 1.0/hmax && vmax(ev) < 1.0/hmin;
 }
 
-__global__ void update_kernel(Params P, int64_t n, double* S, const double* D, const double* d_dt, double scale,
-                              int timeAdvanceOnly, int epsDone, int* err) {
-  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) update_kernel(const Member* mem, BlockMap bm, double scale,
+                                                     int timeAdvanceOnly) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double mult = scale*(*d_dt);
+  const Params& P = MB.prm;
+  double* S = MB.S;
+  const double* D = MB.D;
+  const int epsDone = (!timeAdvanceOnly && P.compatible) ? 1 : 0;
+  const double mult = scale*MB.scal[SC_DT];
   // H: IncrementBoundedState (half step / IntegrateH) or ReplaceBoundedState (IdealH)
   Sym H{S[(S_H + 0)*n + i], S[(S_H + 1)*n + i], S[(S_H + 2)*n + i],
         S[(S_H + 3)*n + i], S[(S_H + 4)*n + i], S[(S_H + 5)*n + i]};
@@ -402,7 +435,7 @@ __global__ void update_kernel(Params P, int64_t n, double* S, const double* D, c
     Hn = Sym{D[(D_HIDEAL + 0)*n + i], D[(D_HIDEAL + 1)*n + i], D[(D_HIDEAL + 2)*n + i],
              D[(D_HIDEAL + 3)*n + i], D[(D_HIDEAL + 4)*n + i], D[(D_HIDEAL + 5)*n + i]};
   }
-  if (!hInsideBounds(Hn, P.hmin, P.hmax)) atomicOr(err, DERR_H_CLAMP);
+  if (!hInsideBounds(Hn, P.hmin, P.hmax)) atomicOr(MB.err, DERR_H_CLAMP);
   S[(S_H + 0)*n + i] = Hn.xx; S[(S_H + 1)*n + i] = Hn.xy; S[(S_H + 2)*n + i] = Hn.xz;
   S[(S_H + 3)*n + i] = Hn.yy; S[(S_H + 4)*n + i] = Hn.yz; S[(S_H + 5)*n + i] = Hn.zz;
   // mass density: IncrementBoundedState
@@ -432,18 +465,28 @@ __global__ void update_kernel(Params P, int64_t n, double* S, const double* D, c
   for (int c = 0; c < 3; ++c) S[(S_VX + c)*n + i] = S[(S_VX + c)*n + i] + D[(D_DVDT + c)*n + i]*mult;
 }
 
-__global__ void eos_kernel(double gamma, int64_t n, double* S) {
-  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) eos_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
+  double* S = MB.S;
+  const double gamma = MB.prm.gamma;
   const double g1 = gamma - 1.0;
   const double rho = S[S_RHO*n + i], eps = S[S_EPS*n + i];
   S[S_P*n + i] = g1*rho*eps;
   S[S_CS*n + i] = sqrt(dmax(0.0, gamma*g1*eps));
 }
 
-__global__ void enforce_boundaries_kernel(int64_t n, double* S, BoxBCs bcs) {
-  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) enforce_boundaries_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
+  double* S = MB.S;
+  const BoxBCs& bcs = MB.prm.bcs;
   V3 r{S[S_X*n + i], S[S_Y*n + i], S[S_Z*n + i]};
   for (int pb = 0; pb < 6; pb += 2) {
     if (!bcs.periodic[pb >> 1]) continue;
@@ -464,9 +507,14 @@ __global__ void enforce_boundaries_kernel(int64_t n, double* S, BoxBCs bcs) {
 }
 
 // ---------------------------------------------------------------- dt
-__global__ void hydro_dt_kernel(Params P, int64_t n, const double* S, const double* D, const int64_t* offsets,
-                                const int32_t* nbr, const int32_t* groot, unsigned long long* out) {
-  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) hydro_dt_kernel(const Member* mem, BlockMap bm, int slot) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
+  const Params& P = MB.prm;
+  const double* S = MB.S;
+  const double* D = MB.D;
   double minDt = kFltMax;
   if (i < n) {
     const Sym H{S[(S_H + 0)*n + i], S[(S_H + 1)*n + i], S[(S_H + 2)*n + i],
@@ -482,9 +530,9 @@ __global__ void hydro_dt_kernel(Params P, int64_t n, const double* S, const doub
     const double divvDt = 1.0/(fabs(divv) + kFltMin);
     if (divvDt < minDt) minDt = divvDt;
     const V3 vi{S[S_VX*n + i], S[S_VY*n + i], S[S_VZ*n + i]};
-    for (int64_t k = offsets[i]; k < offsets[i + 1]; ++k) {
-      const int32_t j = __ldg(nbr + k);
-      const int64_t r = j < n ? (int64_t)j : (int64_t)__ldg(groot + (j - n));
+    for (int64_t k = MB.offsets[i]; k < MB.offsets[i + 1]; ++k) {
+      const int32_t j = __ldg(MB.nbr + k);
+      const int64_t r = j < n ? (int64_t)j : (int64_t)__ldg(MB.groot + (j - n));
       const V3 vj{ldg(S + S_VX*n + r), ldg(S + S_VY*n + r), ldg(S + S_VZ*n + r)};
       const double vij = mag(vsub(vi, vj));
       const double dtVelDiff = nodeScale*safeInvVar(vij, 1e-30);
@@ -499,25 +547,40 @@ __global__ void hydro_dt_kernel(Params P, int64_t n, const double* S, const doub
     }
   }
   for (int o = 16; o > 0; o >>= 1) minDt = dmin(minDt, __shfl_xor_sync(0xffffffffu, minDt, o));
-  if ((threadIdx.x & 31) == 0) atomicMin(out, (unsigned long long)__double_as_longlong(minDt));
+  if ((threadIdx.x & 31) == 0)
+    atomicMin(reinterpret_cast<unsigned long long*>(MB.scal + slot), (unsigned long long)__double_as_longlong(minDt));
 }
 
 // Integrator::selectDt on the device: dt stays resident for the step kernels.
-__global__ void select_dt_kernel(const unsigned long long* minDtBits, double cfl, double dtMin, double dtMax,
-                                 double dtGrowth, double* d_dt, double* d_lastDt, double* d_vote) {
-  const double vote = cfl*__longlong_as_double((long long)*minDtBits);
-  double dt = dtMax;
+__global__ void select_dt_kernel(const Member* mem, int nmem) {
+  const int m = blockIdx.x*blockDim.x + threadIdx.x;
+  if (m >= nmem) return;
+  const Params& P = mem[m].prm;
+  double* sc = mem[m].scal;
+  const double vote = P.cfl*sc[SC_MINDT];
+  double dt = P.dtMax;
   if (vote > 0.0 && vote < dt) dt = vote;
-  dt = dmin(dt, dtGrowth*(*d_lastDt));
-  dt = dmin(dtMax, dmax(dtMin, dt));
-  *d_dt = dt;
-  *d_vote = vote;
+  dt = dmin(dt, P.dtGrowth*sc[SC_LASTDT]);
+  dt = dmin(P.dtMax, dmax(P.dtMin, dt));
+  sc[SC_DT] = dt;
+  sc[SC_VOTE] = vote;
+}
+
+__global__ void finish_step_kernel(const Member* mem, int nmem) {
+  const int m = blockIdx.x*blockDim.x + threadIdx.x;
+  if (m < nmem) mem[m].scal[SC_LASTDT] = mem[m].scal[SC_DT];
 }
 
 // ---------------------------------------------------------------- conservation
-__global__ void conservation_partials_kernel(int64_t n, const double* S, double* partials) {
+// Fixed partition per member (grid-stride over its blocks), fixed-order
+// reduction: the sums are reproducible.
+__global__ void __launch_bounds__(256) conservation_partials_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const double* S = MB.S;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x*blockDim.x) {
+  for (int64_t i = mb.block*blockDim.x + threadIdx.x; i < n; i += (int64_t)mb.blocks*blockDim.x) {
     const double m = S[S_M*n + i];
     const V3 v{S[S_VX*n + i], S[S_VY*n + i], S[S_VZ*n + i]};
     acc[0] += m;
@@ -532,96 +595,197 @@ __global__ void conservation_partials_kernel(int64_t n, const double* S, double*
     if (threadIdx.x < s) for (int c = 0; c < 6; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + s];
     __syncthreads();
   }
-  if (threadIdx.x == 0) for (int c = 0; c < 6; ++c) partials[blockIdx.x*6 + c] = sh[c][0];
+  if (threadIdx.x == 0) for (int c = 0; c < 6; ++c) MB.red[mb.block*6 + c] = sh[c][0];
 }
 
-__global__ void conservation_final_kernel(const double* partials, int nb, double* out) {
-  if (threadIdx.x != 0) return;
+__global__ void conservation_final_kernel(const Member* mem, int nmem, const int32_t* partialBlocks, int soloBlocks) {
+  const int m = blockIdx.x*blockDim.x + threadIdx.x;
+  if (m >= nmem) return;
+  const Member& MB = mem[m];
+  const int nb = partialBlocks ? partialBlocks[m + 1] - partialBlocks[m] : soloBlocks;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int b = 0; b < nb; ++b) for (int c = 0; c < 6; ++c) acc[c] += partials[b*6 + c];
+  for (int b = 0; b < nb; ++b) for (int c = 0; c < 6; ++c) acc[c] += MB.red[b*6 + c];
+  double* out = MB.scal + SC_CONS;
   for (int c = 0; c < 6; ++c) out[c] = acc[c];
   out[6] = acc[4] + acc[5];
   out[7] = 0.0;
 }
 
+__global__ void __launch_bounds__(256) zero_derivs_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t k = mb.block*blockDim.x + threadIdx.x;
+  if (k < NDERIV*MB.n) MB.D[k] = 0.0;
+}
+
 }  // namespace
 
 // ================================================================ launchers
-void pack_records(Problem& p) {
-  const int64_t ntot = p.n + p.G;
-  int blocks = nblk(ntot, 256);
-  if (blocks > 148*64) blocks = 148*64;
-  pack_records_kernel<<<blocks, 256, 0, p.stream>>>(p.S, p.n, p.groot, p.gcode, ntot, p.prm.bcs, p.rec); ++p.launches;
+namespace {
+
+bool isSph(const Problem& p) { return p.prm.hydro == SPHGPU_HYDRO_SPH; }
+bool isFp64Sph(const Problem& p) { return isSph(p) && p.cfg.precision == SPHGPU_PRECISION_FP64; }
+
+int map_nodes(Batch& b, int threads, BlockMap* bm, unsigned* grid) {
+  return batch_map_items(b, [](const Problem& p) { return p.n; }, threads, bm, grid);
 }
 
-void launch_gradh(Problem& p) {
-  gradh_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr, p.S); ++p.launches;
+
+}  // namespace
+
+int pack_records(Batch& b, int need) {
+  if (b.memDirty) SPH_TRY(batch_upload(b));
+  // which members read the FP64 records before the next pack
+  auto wants = [need](const Problem& p) {
+    const bool crk = p.prm.hydro == SPHGPU_HYDRO_CRKSPH;
+    if (need == PACK_FOR_EVAL)       // grad-h, the FP64 pair loop, the CRKSPH moments
+      return crk || p.prm.gradh || p.cfg.precision == SPHGPU_PRECISION_FP64;
+    if (need == PACK_FOR_FINALIZE)   // the summed density, the CRKSPH volumes
+      return crk || p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM;
+    return true;
+  };
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) {
+    return wants(p) ? (b.capacityGrids ? p.candcap : p.n + p.G) : (int64_t)0; }, 256, &bm, &grid));
+  if (grid) { pack_records_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "pack_records");
 }
 
-void launch_eval_sph_fp64(Problem& p) {
-  const bool xsph = p.prm.XSPH != 0, tens = p.prm.epsTensile != 0.0, comp = p.prm.compatible != 0;
-  const int threads = 128;
-  const int blocks = nblk(p.n, threads);
-#define SPH_LAUNCH(X, T, C) \
-  sph_eval_fp64_kernel<X, T, C><<<blocks, threads, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr, p.D, p.pacc, p.ecap)
-  if (xsph) {
-    if (tens) { if (comp) SPH_LAUNCH(true, true, true); else SPH_LAUNCH(true, true, false); }
-    else      { if (comp) SPH_LAUNCH(true, false, true); else SPH_LAUNCH(true, false, false); }
-  } else {
-    if (tens) { if (comp) SPH_LAUNCH(false, true, true); else SPH_LAUNCH(false, true, false); }
-    else      { if (comp) SPH_LAUNCH(false, false, true); else SPH_LAUNCH(false, false, false); }
-  }
-  ++p.launches;
+int launch_gradh(Batch& b) {
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(batch_map_items(b, [](const Problem& p) { return isSph(p) && p.prm.gradh ? p.n : (int64_t)0; }, 128,
+                          &bm, &grid));
+  if (grid) { gradh_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "gradh");
+}
+
+int launch_eval_sph_fp64(Batch& b) {
+  auto key = [](const Problem& p) {
+    return (p.prm.XSPH ? 4 : 0) | (p.prm.epsTensile != 0.0 ? 2 : 0) | (p.prm.compatible ? 1 : 0);
+  };
+  const bool solo = b.mem.size() == 1;
+  const Member one = solo ? describe_member(*b.mem[0]) : Member{};
+  bool present[8] = {false, false, false, false, false, false, false, false};
+  for (Problem* p : b.mem) if (isFp64Sph(*p)) present[key(*p)] = true;
+  for (int v = 0; v < 8; ++v) {
+    if (!present[v]) continue;
+    BlockMap bm;
+    unsigned grid = 0;
+    SPH_TRY(batch_map_items(b, [&](const Problem& p) { return isFp64Sph(p) && key(p) == v ? p.n : (int64_t)0; },
+                            b.evalThreads, &bm, &grid));
+    if (!grid) continue;
+#define SPH_LAUNCH(X, T, C)                                                                            \
+    if (solo) sph_eval_fp64_kernel<X, T, C, true><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one);  \
+    else sph_eval_fp64_kernel<X, T, C, false><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one)
+    switch (v) {
+      case 0: SPH_LAUNCH(false, false, false); break;
+      case 1: SPH_LAUNCH(false, false, true); break;
+      case 2: SPH_LAUNCH(false, true, false); break;
+      case 3: SPH_LAUNCH(false, true, true); break;
+      case 4: SPH_LAUNCH(true, false, false); break;
+      case 5: SPH_LAUNCH(true, false, true); break;
+      case 6: SPH_LAUNCH(true, true, false); break;
+      default: SPH_LAUNCH(true, true, true); break;
+    }
 #undef SPH_LAUNCH
+    batch_count_launch(b);
+  }
+  return cuda_status(cudaGetLastError(), "evaluate (FP64)");
 }
 
-void launch_sum_density(Problem& p) {
-  sum_density_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.rec, p.n, p.offsets, p.nbr, p.S); ++p.launches;
+int launch_sum_density(Batch& b) {
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(batch_map_items(b, [](const Problem& p) {
+    return isSph(p) && p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM ? p.n : (int64_t)0; }, 128, &bm, &grid));
+  if (grid) { sum_density_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "sum density");
 }
 
-void launch_compatible_energy(Problem& p, const double* d_dt, double scale) {
-  compatible_energy_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.n, p.offsets, p.nbr, p.groot, p.pacc, p.ecap,
-                                                                 p.D, p.S, d_dt, scale); ++p.launches;
+int launch_compatible_energy(Batch& b, double scale) {
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.prm.compatible ? p.n : (int64_t)0; }, 128, &bm, &grid));
+  if (grid) { compatible_energy_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm, scale); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "compatible energy");
 }
 
-void launch_update(Problem& p, const double* d_dt, double scale, bool timeAdvanceOnly) {
-  const int epsDone = (!timeAdvanceOnly && p.prm.compatible) ? 1 : 0;
-  update_kernel<<<nblk(p.n, 256), 256, 0, p.stream>>>(p.prm, p.n, p.S, p.D, d_dt, scale,
-                                                      timeAdvanceOnly ? 1 : 0, epsDone, p.d_err); ++p.launches;
+int launch_update(Batch& b, double scale, bool timeAdvanceOnly) {
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(map_nodes(b, 256, &bm, &grid));
+  if (grid) {
+    update_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm, scale, timeAdvanceOnly ? 1 : 0);
+    batch_count_launch(b);
+  }
+  return cuda_status(cudaGetLastError(), "update");
 }
 
-void launch_eos(Problem& p) {
-  eos_kernel<<<nblk(p.n, 256), 256, 0, p.stream>>>(p.prm.gamma, p.n, p.S); ++p.launches;
+int launch_eos(Batch& b) {
+  if (b.memDirty) SPH_TRY(batch_upload(b));
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(map_nodes(b, 256, &bm, &grid));
+  if (grid) { eos_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "eos");
 }
 
-void launch_enforce_boundaries(Problem& p) {
-  enforce_boundaries_kernel<<<nblk(p.n, 256), 256, 0, p.stream>>>(p.n, p.S, p.prm.bcs); ++p.launches;
+int launch_enforce_boundaries(Batch& b) {
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(map_nodes(b, 256, &bm, &grid));
+  if (grid) { enforce_boundaries_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "enforce boundaries");
 }
 
-// d_out[0] = min dt bits (as double after the kernel), scratch in d_scal.
-void launch_dt(Problem& p, double* d_out) {
-  unsigned long long* bits = reinterpret_cast<unsigned long long*>(d_out);
-  const double init = kFltMax;
-  cudaMemcpyAsync(bits, &init, sizeof(double), cudaMemcpyHostToDevice, p.stream);
-  hydro_dt_kernel<<<nblk(p.n, 128), 128, 0, p.stream>>>(p.prm, p.n, p.S, p.D, p.offsets, p.nbr, p.groot, bits); ++p.launches;
+int launch_dt(Batch& b, int slot) {
+  if (b.memDirty) SPH_TRY(batch_upload(b));
+  batch_set_scal(b, slot, kFltMax);
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(map_nodes(b, 128, &bm, &grid));
+  if (grid) { hydro_dt_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm, slot); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "dt");
 }
 
-void launch_select_dt(Problem& p, double* d_dt, double* d_lastDt) {
-  double* minDt = p.d_scal + 10;
-  launch_dt(p, minDt);
-  select_dt_kernel<<<1, 1, 0, p.stream>>>(reinterpret_cast<unsigned long long*>(minDt), p.prm.cfl,
-                                          p.cfg.dtMin, p.cfg.dtMax, p.cfg.dtGrowth, d_dt, d_lastDt,
-                                          p.d_scal + 11); ++p.launches;
+int launch_select_dt(Batch& b) {
+  SPH_TRY(launch_dt(b, SC_MINDT));
+  const int nm = (int)b.mem.size();
+  select_dt_kernel<<<(nm + 127)/128, 128, 0, b.stream>>>(b.d_mem, nm); batch_count_launch(b);
+  return cuda_status(cudaGetLastError(), "select dt");
 }
 
-void launch_conservation(Problem& p, double* d_out8) {
-  const int nb = 148*4;
-  conservation_partials_kernel<<<nb, 256, 0, p.stream>>>(p.n, p.S, p.d_red); ++p.launches;
-  conservation_final_kernel<<<1, 32, 0, p.stream>>>(p.d_red, nb, d_out8); ++p.launches;
+int launch_finish_step(Batch& b) {
+  const int nm = (int)b.mem.size();
+  finish_step_kernel<<<(nm + 127)/128, 128, 0, b.stream>>>(b.d_mem, nm); batch_count_launch(b);
+  return cuda_status(cudaGetLastError(), "finish step");
 }
 
-void launch_zero_derivs(Problem& p) {
-  cudaMemsetAsync(p.D, 0, sizeof(double)*NDERIV*(size_t)p.n, p.stream);
+int launch_conservation(Batch& b) {
+  if (b.memDirty) SPH_TRY(batch_upload(b));
+  std::vector<int64_t> blocks(b.mem.size());
+  for (size_t m = 0; m < b.mem.size(); ++m) {
+    const int64_t k = (b.mem[m]->n + 255)/256;
+    blocks[m] = k < kConsBlocks ? k : kConsBlocks;
+  }
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(batch_map(b, blocks, &bm, &grid));
+  if (grid) { conservation_partials_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  const int nm = (int)b.mem.size();
+  conservation_final_kernel<<<(nm + 127)/128, 128, 0, b.stream>>>(b.d_mem, nm, bm.first, (int)grid); batch_count_launch(b);
+  return cuda_status(cudaGetLastError(), "conservation");
+}
+
+int launch_zero_derivs(Batch& b) {
+  if (b.memDirty) SPH_TRY(batch_upload(b));
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(batch_map_items(b, [](const Problem& p) { return (int64_t)NDERIV*p.n; }, 256, &bm, &grid));
+  if (grid) { zero_derivs_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "zero derivatives");
 }
 
 }  // namespace sphgpu

@@ -19,11 +19,6 @@ namespace sphgpu {
 
 namespace {
 
-inline int nblk(int64_t work, int threads) {
-  int64_t b = (work + threads - 1)/threads;
-  return (int)(b < 1 ? 1 : b);
-}
-
 struct Kahan {
   float s, c;
   __device__ __forceinline__ void init() { s = 0.0f; c = 0.0f; }
@@ -55,26 +50,29 @@ __device__ __forceinline__ MRec loadMRec(const double* mrec, int64_t k) {
   return R;
 }
 
-__global__ void pack_mixed_kernel(const double* S, int64_t n, const int32_t* groot, const uint32_t* gcode,
-                                  int64_t ntot, BoxBCs bcs, double* mrec) {
-  for (int64_t k = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; k < ntot; k += (int64_t)gridDim.x*blockDim.x) {
-    const int64_t r = k < n ? k : groot[k - n];
-    V3 x{S[S_X*n + r], S[S_Y*n + r], S[S_Z*n + r]};
-    if (k >= n) x = ghostPosition(bcs, x, gcode[k - n]);
-    const Sym H{S[(S_H + 0)*n + r], S[(S_H + 1)*n + r], S[(S_H + 2)*n + r],
-                S[(S_H + 3)*n + r], S[(S_H + 4)*n + r], S[(S_H + 5)*n + r]};
-    const double m = S[S_M*n + r], rho = S[S_RHO*n + r], P = S[S_P*n + r];
-    const double somega = safeInv(S[S_OMEGA*n + r], 1.0e-30);
-    double2* q = reinterpret_cast<double2*>(mrec + k*MRECW);
-    q[0] = make_double2(x.x, x.y);
-    q[1] = make_double2(x.z, S[S_VX*n + r]);
-    q[2] = make_double2(S[S_VY*n + r], S[S_VZ*n + r]);
-    float4* f = reinterpret_cast<float4*>(q + 3);
-    f[0] = make_float4((float)m, (float)rho, (float)S[S_CS*n + r], (float)sdet(H));
-    f[1] = make_float4((float)H.xx, (float)H.xy, (float)H.xz, (float)H.yy);
-    f[2] = make_float4((float)H.yz, (float)H.zz, (float)(somega*P/(rho*rho)), (float)(m/rho));
-    f[3] = make_float4((float)P, (float)somega, 0.0f, 0.0f);
-  }
+__global__ void __launch_bounds__(256) pack_mixed_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const int64_t k = mb.block*blockDim.x + threadIdx.x;
+  if (k >= n + scalI(MB.scal, SC_G)) return;
+  const double* S = MB.S;
+  const int64_t r = k < n ? k : MB.groot[k - n];
+  V3 x{S[S_X*n + r], S[S_Y*n + r], S[S_Z*n + r]};
+  if (k >= n) x = ghostPosition(MB.prm.bcs, x, MB.gcode[k - n]);
+  const Sym H{S[(S_H + 0)*n + r], S[(S_H + 1)*n + r], S[(S_H + 2)*n + r],
+              S[(S_H + 3)*n + r], S[(S_H + 4)*n + r], S[(S_H + 5)*n + r]};
+  const double m = S[S_M*n + r], rho = S[S_RHO*n + r], P = S[S_P*n + r];
+  const double somega = safeInv(S[S_OMEGA*n + r], 1.0e-30);
+  double2* q = reinterpret_cast<double2*>(MB.mrec + k*MRECW);
+  q[0] = make_double2(x.x, x.y);
+  q[1] = make_double2(x.z, S[S_VX*n + r]);
+  q[2] = make_double2(S[S_VY*n + r], S[S_VZ*n + r]);
+  float4* f = reinterpret_cast<float4*>(q + 3);
+  f[0] = make_float4((float)m, (float)rho, (float)S[S_CS*n + r], (float)sdet(H));
+  f[1] = make_float4((float)H.xx, (float)H.xy, (float)H.xz, (float)H.yy);
+  f[2] = make_float4((float)H.yz, (float)H.zz, (float)(somega*P/(rho*rho)), (float)(m/rho));
+  f[3] = make_float4((float)P, (float)somega, 0.0f, 0.0f);
 }
 
 __global__ void table_to_float_kernel(const double* coef, int n, float* out) {
@@ -106,13 +104,22 @@ __device__ __forceinline__ void tableF(const float* coef, int n, float invStep, 
   }
 }
 
-template<bool XSPH, bool TENSILE, bool COMPAT>
-__global__ void __launch_bounds__(128) sph_eval_mixed_kernel(Params P, const float* coefF, const double* mrec,
-                                                             const double* S, int64_t n, const int64_t* offsets,
-                                                             const int32_t* nbr, double* D, double* pacc,
-                                                             int64_t ecap) {
-  const int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x;
+template<bool XSPH, bool TENSILE, bool COMPAT, bool SOLO>
+__global__ void __launch_bounds__(128, 3) sph_eval_mixed_kernel(const Member* mem, BlockMap bm, const Member single) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = SOLO ? single : mem[mb.m];   // one member: read from the kernel parameters
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const Params& P = MB.prm;
+  const float* coefF = MB.coefF;
+  const double* mrec = MB.mrec;
+  const double* S = MB.S;
+  const int64_t* offsets = MB.offsets;
+  const int32_t* nbr = MB.nbr;
+  double* D = MB.D;
+  double* pacc = MB.pacc;
+  const int64_t ecap = MB.ecap;
   const MRec I = loadMRec(mrec, i);
   const float invStep = (float)(1.0/P.W.stepSize), extent = (float)P.W.extent;
   const float eps2 = (float)P.eps2;
@@ -300,47 +307,71 @@ __global__ void __launch_bounds__(128) sph_eval_mixed_kernel(Params P, const flo
 
 }  // namespace
 
-int prepare_mixed(Problem& p) {
-  if (p.coefF == nullptr) {
-    if (cudaMalloc(&p.coefF, sizeof(float)*6*(size_t)p.prm.W.n) != cudaSuccess) {
-      set_error("mixed table allocation failed");
-      return SPHGPU_ERR_NOMEM;
+int prepare_mixed(Batch& b) {
+  for (Problem* pp : b.mem) {
+    Problem& p = *pp;
+    if (p.cfg.precision != SPHGPU_PRECISION_MIXED) continue;
+    if (p.coefF == nullptr) {
+      if (cudaMalloc(&p.coefF, sizeof(float)*6*(size_t)p.prm.W.n) != cudaSuccess) {
+        set_error("mixed table allocation failed");
+        return SPHGPU_ERR_NOMEM;
+      }
+      table_to_float_kernel<<<8, 256, 0, b.stream>>>(p.prm.W.coef, p.prm.W.n, p.coefF); ++p.launches;
+      b.memDirty = true;
     }
-    table_to_float_kernel<<<8, 256, 0, p.stream>>>(p.prm.W.coef, p.prm.W.n, p.coefF); ++p.launches;
-  }
-  const int64_t need = p.candcap;
-  if (need > p.mreccap) {
-    cudaFree(p.mrec);
-    p.mrec = nullptr;
-    if (cudaMalloc(&p.mrec, sizeof(double)*MRECW*(size_t)need) != cudaSuccess) {
-      set_error("mixed record allocation failed");
-      return SPHGPU_ERR_NOMEM;
+    const int64_t need = p.candcap;
+    if (need > p.mreccap) {
+      cudaStreamSynchronize(b.stream);
+      cudaFree(p.mrec);
+      p.mrec = nullptr;
+      if (cudaMalloc(&p.mrec, sizeof(double)*(p.prm.hydro == SPHGPU_HYDRO_CRKSPH ? CMRECW : MRECW)*(size_t)need) != cudaSuccess) {
+        p.mreccap = 0;
+        set_error("mixed record allocation failed");
+        return SPHGPU_ERR_NOMEM;
+      }
+      p.mreccap = need;
+      b.memDirty = true;
     }
-    p.mreccap = need;
   }
+  if (b.memDirty) SPH_TRY(batch_upload(b));
   return SPHGPU_OK;
 }
 
-void launch_eval_sph_mixed(Problem& p) {
-  const int64_t ntot = p.n + p.G;
-  int blocks = nblk(ntot, 256);
-  if (blocks > 148*64) blocks = 148*64;
-  pack_mixed_kernel<<<blocks, 256, 0, p.stream>>>(p.S, p.n, p.groot, p.gcode, ntot, p.prm.bcs, p.mrec); ++p.launches;
-  const bool xsph = p.prm.XSPH != 0, tens = p.prm.epsTensile != 0.0, comp = p.prm.compatible != 0;
-  const int threads = 128;
-  const int nb = nblk(p.n, threads);
-#define MIX_LAUNCH(X, T, C) \
-  sph_eval_mixed_kernel<X, T, C><<<nb, threads, 0, p.stream>>>(p.prm, p.coefF, p.mrec, p.S, p.n, p.offsets, p.nbr, \
-                                                                p.D, p.pacc, p.ecap)
-  if (xsph) {
-    if (tens) { if (comp) MIX_LAUNCH(true, true, true); else MIX_LAUNCH(true, true, false); }
-    else      { if (comp) MIX_LAUNCH(true, false, true); else MIX_LAUNCH(true, false, false); }
-  } else {
-    if (tens) { if (comp) MIX_LAUNCH(false, true, true); else MIX_LAUNCH(false, true, false); }
-    else      { if (comp) MIX_LAUNCH(false, false, true); else MIX_LAUNCH(false, false, false); }
-  }
-  ++p.launches;
+int launch_eval_sph_mixed(Batch& b) {
+  auto mixed = [](const Problem& p) { return p.cfg.precision == SPHGPU_PRECISION_MIXED; };
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return mixed(p) ? (b.capacityGrids ? p.candcap : p.n + p.G) : (int64_t)0; }, 256, &bm, &grid));
+  if (grid) { pack_mixed_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  auto key = [](const Problem& p) {
+    return (p.prm.XSPH ? 4 : 0) | (p.prm.epsTensile != 0.0 ? 2 : 0) | (p.prm.compatible ? 1 : 0);
+  };
+  const bool solo = b.mem.size() == 1;
+  const Member one = solo ? describe_member(*b.mem[0]) : Member{};
+  bool present[8] = {false, false, false, false, false, false, false, false};
+  for (Problem* p : b.mem) if (mixed(*p)) present[key(*p)] = true;
+  for (int v = 0; v < 8; ++v) {
+    if (!present[v]) continue;
+    SPH_TRY(batch_map_items(b, [&](const Problem& p) { return mixed(p) && key(p) == v ? p.n : (int64_t)0; }, b.evalThreads,
+                            &bm, &grid));
+    if (!grid) continue;
+#define MIX_LAUNCH(X, T, C)                                                                             \
+    if (solo) sph_eval_mixed_kernel<X, T, C, true><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one);  \
+    else sph_eval_mixed_kernel<X, T, C, false><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one)
+    switch (v) {
+      case 0: MIX_LAUNCH(false, false, false); break;
+      case 1: MIX_LAUNCH(false, false, true); break;
+      case 2: MIX_LAUNCH(false, true, false); break;
+      case 3: MIX_LAUNCH(false, true, true); break;
+      case 4: MIX_LAUNCH(true, false, false); break;
+      case 5: MIX_LAUNCH(true, false, true); break;
+      case 6: MIX_LAUNCH(true, true, false); break;
+      default: MIX_LAUNCH(true, true, true); break;
+    }
 #undef MIX_LAUNCH
+    batch_count_launch(b);
+  }
+  return cuda_status(cudaGetLastError(), "evaluate (mixed)");
 }
 
 }  // namespace sphgpu

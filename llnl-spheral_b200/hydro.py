@@ -36,6 +36,11 @@ def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
 
 
+def _tune_report(out):
+    return {"neighbor walk": int(out[0]), "neighbor walk ms": {"thread": out[1], "warp": out[2]},
+            "pair loop": int(out[3]), "pair loop ms": {64: out[4], 128: out[5]}}
+
+
 class SPHHydro:
     """One FluidNodeList evolved by the B200 SPH hydro path.
 
@@ -139,6 +144,13 @@ class SPHHydro:
         abi.check(self.lib.sphgpu_kernel_launches(self.h, ctypes.byref(v)), self.lib)
         return v.value
 
+    def sync_time(self):
+        t = ctypes.c_double()
+        dt = ctypes.c_double()
+        abi.check(self.lib.sphgpu_time(self.h, ctypes.byref(t), ctypes.byref(dt)), self.lib)
+        self.time = t.value
+        return t.value, dt.value
+
     def set_schedule(self, stage, schedule):
         abi.check(self.lib.sphgpu_set_schedule(self.h, stage.encode(), int(schedule)), self.lib)
 
@@ -146,6 +158,12 @@ class SPHHydro:
         v = ctypes.c_int32()
         abi.check(self.lib.sphgpu_get_schedule(self.h, stage.encode(), ctypes.byref(v)), self.lib)
         return v.value
+
+    def autotune(self):
+        """Time every kernel schedule on this problem and keep the fastest."""
+        out = np.zeros(8)
+        abi.check(self.lib.sphgpu_autotune(self.h, _p(out)), self.lib)
+        return _tune_report(out)
 
     def synchronize(self):
         abi.check(self.lib.sphgpu_synchronize(self.h), self.lib)
@@ -167,3 +185,63 @@ class CheapSynchronousRK2Integrator:
 
     def advance(self, nsteps):
         return self.hydro.step(nsteps)
+
+
+class SPHBatch:
+    """Many independent problems advanced together: every stage of every call
+    is one kernel launch over all members (no counterpart in the reference,
+    whose problems run one at a time).  Members keep their own state; each
+    member's results equal those of running it alone."""
+
+    def __init__(self, members):
+        self.lib = abi.load_library()
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(self.members))(*[m.h.value for m in self.members])
+        h = ctypes.c_void_p()
+        abi.check(self.lib.sphgpu_batch_create(arr, len(self.members), ctypes.byref(h)), self.lib)
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.sphgpu_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def build_neighbors(self):
+        abi.check(self.lib.sphgpu_batch_build_neighbors(self.h), self.lib)
+
+    def evaluateDerivatives(self):
+        abi.check(self.lib.sphgpu_batch_evaluate_derivatives(self.h), self.lib)
+
+    def step(self, nsteps=1):
+        abi.check(self.lib.sphgpu_batch_step_rk2(self.h, int(nsteps)), self.lib)
+        for m in self.members:
+            m.sync_time()
+
+    def num_pairs(self):
+        v = ctypes.c_int64()
+        abi.check(self.lib.sphgpu_batch_pairs(self.h, ctypes.byref(v)), self.lib)
+        return v.value
+
+    def kernel_launches(self):
+        v = ctypes.c_int64()
+        abi.check(self.lib.sphgpu_batch_kernel_launches(self.h, ctypes.byref(v)), self.lib)
+        return v.value
+
+    def set_schedule(self, stage, schedule):
+        abi.check(self.lib.sphgpu_batch_set_schedule(self.h, stage.encode(), int(schedule)), self.lib)
+
+    def autotune(self):
+        out = np.zeros(8)
+        abi.check(self.lib.sphgpu_batch_autotune(self.h, _p(out)), self.lib)
+        return _tune_report(out)
+
+    def stream(self):
+        v = ctypes.c_void_p()
+        abi.check(self.lib.sphgpu_batch_get_stream(self.h, ctypes.byref(v)), self.lib)
+        return v.value

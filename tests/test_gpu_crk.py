@@ -84,3 +84,36 @@ def test_crk_steps(gpu_lib, pkg, oracle_mod, case):
         assert normwise(g.field(k), o.field(k)) <= 1e-12, k
     c1 = g.conservation()
     assert abs(c1[6] - c0[6]) <= 1e-12 * abs(c0[6])
+
+
+@pytest.mark.parametrize("case", ["kh", "sod"])
+def test_crk_mixed_against_fp64(gpu_lib, pkg, case):
+    """Mixed CRKSPH (FP32 pair arithmetic, Kahan sums; FP64 moments and
+    corrections): every derivative within 1e-5 normwise of plain FP64."""
+    ns, cfg = _case(pkg, case)
+    cm = cfg.copy()
+    cm.precision = pkg.abi.PRECISION_MIXED
+    f = pkg.SPHHydro(cfg, ns)
+    m = pkg.SPHHydro(cm, ns)
+    for p in (f, m):
+        p.build_neighbors()
+        p.initialize()
+        p.evaluateDerivatives()
+    for k in CRK_KEYS:
+        assert np.array_equal(m.field(k), f.field(k)), k          # the moments stay FP64
+    for k in DERIV_KEYS:
+        if k == "XSPH delta vi":
+            continue
+        assert normwise(m.field(k), f.field(k)) <= 1e-5, k
+
+
+def test_crk_mixed_energy_drift(gpu_lib, pkg):
+    ns, cfg = _case(pkg, "kh")
+    cfg.precision = pkg.abi.PRECISION_MIXED
+    g = pkg.SPHHydro(cfg, ns)
+    g.build_neighbors()
+    g.initialize()
+    g.evaluateDerivatives()
+    e0 = g.conservation()[6]
+    g.step(100)
+    assert abs(g.conservation()[6] - e0) <= 1e-6 * abs(e0)

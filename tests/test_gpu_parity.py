@@ -69,10 +69,13 @@ def test_connectivity_bitexact(gpu_lib, pkg, oracle_mod, case):
 
 @pytest.mark.parametrize("case", ["sod", "kh", "sod_x_periodic_only"])
 @pytest.mark.parametrize("schedule", [1, 2])
-def test_connectivity_every_schedule(gpu_lib, pkg, oracle_mod, case, schedule):
-    """Thread-per-node and warp-per-node neighbor walks give the same CSR."""
+@pytest.mark.parametrize("nfilter", [0, 1])
+def test_connectivity_every_schedule(gpu_lib, pkg, oracle_mod, case, schedule, nfilter):
+    """Thread-per-node and warp-per-node neighbor walks, with and without the
+    FP32 pre-test, give the same CSR."""
     g, o, ns = _pair(pkg, oracle_mod, case)
     g.set_schedule("neighbor walk", schedule)
+    g.set_schedule("neighbor filter", nfilter)
     g.build_neighbors()
     assert g.schedule("neighbor walk") == schedule
     o.build_neighbors()
@@ -201,3 +204,27 @@ def test_empty_problem_rejected(gpu_lib, pkg):
     h = ctypes.c_void_p()
     cfg = abi.make_config()
     assert gpu_lib.sphgpu_create(ctypes.byref(cfg), 0, ctypes.byref(h)) == abi.ERR_ARG
+
+
+@pytest.mark.parametrize("nfilter", [0, 1])
+def test_connectivity_anisotropic_h(gpu_lib, pkg, oracle_mod, nfilter):
+    """Anisotropic, varied H (condition numbers up to ~2) with the eta_i OR
+    eta_j predicate: many candidates sit near the support boundary."""
+    gen, abi = pkg.generators, pkg.abi
+    box = ((0.0, 0.0, 0.0), (1.0, 0.25, 0.25))
+    ns = gen.sod(nx=32, ny=8, nz=8, box=box, jitter=0.2, seed=5)
+    rng = np.random.default_rng(9)
+    ns.H[:, 0] *= rng.uniform(0.7, 1.4, ns.n)
+    ns.H[:, 3] *= rng.uniform(0.7, 1.4, ns.n)
+    ns.H[:, 5] *= rng.uniform(0.7, 1.4, ns.n)
+    ns.H[:, 1] = 0.1 * ns.H[:, 0] * rng.uniform(-1, 1, ns.n)
+    ns.H[:, 4] = 0.1 * ns.H[:, 3] * rng.uniform(-1, 1, ns.n)
+    cfg = gen.sod_config(abi, ns_box=box)
+    g = pkg.SPHHydro(cfg, ns)
+    g.set_schedule("neighbor filter", nfilter)
+    o = oracle_mod.OracleProblem(cfg, ns)
+    g.build_neighbors()
+    o.build_neighbors()
+    go, gn, gr = g.connectivity()
+    oo, on, orr = o.connectivity()
+    assert np.array_equal(go, oo) and np.array_equal(gn, on) and np.array_equal(gr, orr)

@@ -1,0 +1,34 @@
+"""Host-side serving logic on the CPU: the request trace and the admission
+footprint estimate (no device call)."""
+import numpy as np
+
+
+def test_poisson_trace_is_seeded_and_shaped(pkg):
+    s = pkg.serving
+    a = s.poisson_trace(rate=20.0, duration=60.0, seed=7)
+    b = s.poisson_trace(rate=20.0, duration=60.0, seed=7)
+    assert a == b
+    assert 900 < len(a) < 1500                        # ~ rate * duration
+    arr = np.array([r["arrival"] for r in a])
+    assert np.all(np.diff(arr) > 0) and arr[-1] <= 60.0
+    n = np.array([r["n"] for r in a])
+    assert n.min() >= 8192 and n.max() <= 1048576
+    # log-uniform: the median is near the geometric mean of the bounds
+    assert abs(np.log(np.median(n)) - 0.5 * (np.log(8192) + np.log(1048576))) < 0.3
+    kinds = [r["kind"] for r in a]
+    assert 0.4 < kinds.count("kh") / len(kinds) < 0.6
+
+
+def test_footprint_estimate_scales_with_nodes(pkg):
+    s = pkg.serving
+    est = []
+    for n in (4096, 32768, 262144):
+        ns, cfg = s.request_nodes("sod", n, 1, 1)
+        est.append(s.estimate_footprint(cfg, ns) / ns.n)
+    # bytes per node: state, derivatives, records, cell list and ~120 B-spline neighbors
+    assert all(1500 < e < 20000 for e in est), est
+    # the ghost share falls as the tube grows
+    assert est[0] > est[-1]
+    ns, cfg = s.request_nodes("kh", 32768, 1, 1)
+    kh = s.estimate_footprint(cfg, ns) / ns.n
+    assert 800 < kh < est[1]                          # ~6 Wendland neighbors: fewer CSR bytes
