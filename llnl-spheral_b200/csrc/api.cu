@@ -617,7 +617,8 @@ int64_t problem_bytes(const Problem& p) {
   b += p.candcap*(4 + 4 + 4 + 112 + 8*RECW) + 8*(p.candcap + 1);       // counts, cidx, sortedIdx, cand, rec, offsets
   b += p.ecap*(4 + (p.pacc ? 24 : 0));                                // nbr, pacc
   b += p.cellcap*(8 + 4) + 8 + 8*p.blockSumsCap;
-  b += 8*(int64_t)MRECW*p.mreccap + (p.coefF ? 4*6*(int64_t)p.prm.W.n : 0);
+  b += 8*(int64_t)(p.cfg.hydro == SPHGPU_HYDRO_CRKSPH ? CMRECW : MRECW)*p.mreccap +
+       (p.coefF ? 4*6*(int64_t)p.prm.W.n : 0);
   b += 8*(int64_t)CRECW*p.creccap + (p.K ? 8*(int64_t)NCRK*n : 0);
   return b;
 }

@@ -604,8 +604,12 @@ int plan_capacities(Batch& b) {
   for (Problem* pp : b.mem) {
     Problem& p = *pp;
     const int64_t oldg = p.gcap, oldc = p.candcap, olde = p.ecap, oldcells = p.cellcap;
-    if (p.G > 0) SPH_TRY(ensure_capacity_ghosts(p, grow(p.G)));
-    const int64_t cellsNeed = p.ncells > 0 ? grow(p.ncells) : p.candcap/2 + 64;
+    // sizes of the last build, else the caller's hints, else built-in guesses
+    const int64_t G = p.G > 0 ? p.G : p.hintG;
+    const int64_t E = p.E > 0 ? p.E : p.hintE;
+    const int64_t cells = p.ncells > 0 ? p.ncells : p.hintCells;
+    if (G > 0) SPH_TRY(ensure_capacity_ghosts(p, grow(G)));
+    const int64_t cellsNeed = cells > 0 ? grow(cells) : p.candcap/2 + 64;
     if (cellsNeed + 1 > p.cellcap) {
       cudaStreamSynchronize(b.stream);
       cudaFree(p.cellStart); cudaFree(p.cellFill);
@@ -618,8 +622,8 @@ int plan_capacities(Batch& b) {
         return SPHGPU_ERR_NOMEM;
       }
     }
-    // the first build guesses 32 entries per node; an overflow redoes it
-    SPH_TRY(ensure_capacity_entries(p, p.E > 0 ? p.E + p.E/8 : 32*p.n));
+    // without a hint the first build guesses 32 entries per node; an overflow redoes it
+    SPH_TRY(ensure_capacity_entries(p, E > 0 ? E + E/8 : 32*p.n));
     if (p.fillCap < 8) p.fillCap = p.maxCount > 0 ? p.maxCount + p.maxCount/4 + 8 : 64;
     const int64_t tiles = ((p.candcap > p.cellcap ? p.candcap : p.cellcap) + 1023)/1024 + 2;
     if (tiles > p.blockSumsCap) SPH_TRY(ensure_block_sums(p, tiles));
@@ -635,6 +639,38 @@ int plan_capacities(Batch& b) {
   b.memDirty = true;
   return SPHGPU_OK;
 }
+
+}  // namespace
+
+// Mirrors the capacity rules a new problem goes through: sphgpu_create sizes
+// the ghost and (n + ghost) buffers for n/2 + 4096 ghosts, plan_capacities
+// grows them from the planned sizes, ensure_capacity_* add their own slack,
+// and the mixed and CRKSPH records follow the (n + ghost) capacity.
+int64_t planned_bytes(const sphgpu_config& cfg, int64_t n, int64_t G, int64_t E, int64_t ncells) {
+  auto ghostCap = [](int64_t need) { return need + need/2 + 1024; };  // ensure_capacity_ghosts
+  Problem p;
+  p.cfg = cfg;
+  p.n = n;
+  p.prm.W.n = cfg.num_points;
+  p.gcap = ghostCap(n/2 + 4096);
+  if (G > 0 && grow(G) > p.gcap) p.gcap = ghostCap(grow(G));
+  p.candcap = n + p.gcap;
+  p.cellcap = (ncells > 0 ? grow(ncells) : p.candcap/2 + 64) + 1;
+  const int64_t eneed = E > 0 ? E + E/8 : 32*n;
+  p.ecap = eneed + eneed/8 + 1024;                                       // ensure_capacity_entries
+  p.blockSumsCap = ((p.candcap > p.cellcap ? p.candcap : p.cellcap) + 1023)/1024 + 2 + 64;
+  if (cfg.precision == SPHGPU_PRECISION_MIXED) p.mreccap = p.candcap;
+  if (cfg.hydro == SPHGPU_HYDRO_CRKSPH) p.creccap = p.candcap;
+  double marker = 0.0;                          // problem_bytes only tests these for null
+  if (cfg.compatibleEnergyEvolution) p.pacc = &marker;
+  if (cfg.precision == SPHGPU_PRECISION_MIXED) p.coefF = reinterpret_cast<float*>(&marker);
+  if (cfg.hydro == SPHGPU_HYDRO_CRKSPH) p.K = &marker;
+  const int64_t b = problem_bytes(p);
+  p.pacc = nullptr; p.coefF = nullptr; p.K = nullptr;
+  return b;
+}
+
+namespace {
 
 int launch_build(Batch& b) {
   cudaStream_t st = b.stream;

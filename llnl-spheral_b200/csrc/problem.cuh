@@ -137,6 +137,8 @@ struct Problem {
   bool nbrFilter = true;    // FP32 pre-test in the neighbor walk (exact either way)
   int fillCap = 0;          // neighbor-list capacity planned for the fill pass
   int fillSchedule = 0;     // schedule planned for this build (NBR_SCHEDULE_THREAD/WARP)
+  // sizes the first neighbor build plans its buffers from (0: built-in guesses)
+  int64_t hintG = 0, hintE = 0, hintCells = 0;
 
   double* S = nullptr;
   double* S0 = nullptr;
@@ -393,6 +395,10 @@ int launch_crk_eval_mixed(Batch& b);                        // mixed-precision C
 int batch_step_rk2(Batch& b);
 // device bytes held by a problem, from its buffer capacities (api.cu)
 int64_t problem_bytes(const Problem& p);
+// device bytes a new problem holds after its first neighbor build, when that
+// build is planned from G ghosts, E entries and ncells cells and needs no more
+// (the capacity rules of sphgpu_create and plan_capacities; nbrs.cu)
+int64_t planned_bytes(const sphgpu_config& cfg, int64_t n, int64_t G, int64_t E, int64_t ncells);
 
 // device buffer helpers (api.cu)
 int ensure_capacity_ghosts(Problem& p, int64_t gcap);

@@ -45,53 +45,47 @@ struct Request {
 double kernel_extent(int kernel) { return kernel == SPHGPU_KERNEL_BSPLINE ? 2.0 : 1.0; }
 
 // Footprint estimate before allocation: ghosts from the periodic layers of
-// width kappa*hmax, neighbors from the node density inside kappa*hmax, and
-// the same capacity growth rules the buffers follow.
-int64_t estimate_bytes(const Request& r) {
-  const sphgpu_config& c = r.cfg;
-  const int64_t n = r.n;
+// width kappa*hmax, neighbors from the node density inside kappa*hmax, cells
+// of side kappa*hmax over the box with its ghost layers.  The problem's first
+// neighbor build is planned from these sizes (Problem::hint*), so the bytes
+// it holds after that build are exactly planned_bytes of them, unless a size
+// turns out larger than estimated and the build grows its buffers.
+struct Estimate {
+  int64_t G = 0, E = 0, cells = 0, bytes = 0;
+};
+
+Estimate estimate_sizes(const sphgpu_config& c, int64_t n, const double* pos, const double* H) {
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
   double hmax = 0.0;
   for (int64_t i = 0; i < n; ++i) {
     for (int a = 0; a < 3; ++a) {
-      lo[a] = std::min(lo[a], r.pos[3*i + a]);
-      hi[a] = std::max(hi[a], r.pos[3*i + a]);
+      lo[a] = std::min(lo[a], pos[3*i + a]);
+      hi[a] = std::max(hi[a], pos[3*i + a]);
     }
-    const double* h = &r.H[6*i];
+    const double* h = &H[6*i];
     const double hmin = std::min(h[0], std::min(h[3], h[5]));
     if (hmin > 0.0) hmax = std::max(hmax, 1.0/hmin);
   }
   const double reach = kernel_extent(c.kernel)*hmax;
-  double vol = 1.0, ext = 1.0;
+  const double cell = reach*1.001;
+  double vol = 1.0, ext = 1.0, cells = 1.0;
   for (int a = 0; a < 3; ++a) {
     const double L = c.periodic[a] ? c.xmax[a] - c.xmin[a] : std::max(hi[a] - lo[a], reach);
     vol *= L;
     ext *= c.periodic[a] ? (L + 2.0*reach)/L : 1.0;
+    cells *= std::floor((c.periodic[a] ? L + 2.0*reach : L)/cell) + 1.0;   // the grid's cells per axis
   }
-  const int64_t G = (int64_t)(1.1*(double)n*(ext - 1.0)) + 64;
+  Estimate e;
+  e.G = (int64_t)(1.1*(double)n*(ext - 1.0)) + 64;
   const double density = (double)n/vol;
   const double nbrs = 1.3*density*(4.0/3.0)*3.14159265358979323846*reach*reach*reach + 8.0;
-  const int64_t E = (int64_t)(nbrs*(double)n);
-  Problem p;
-  p.cfg = c;
-  p.n = n;
-  p.prm.W.n = c.num_points;
-  p.gcap = std::max(G + G/2 + 1024, n/2 + 4096);
-  p.candcap = n + p.gcap;
-  p.ecap = E + E/8 + 1024;
-  const double cell = reach*1.001;
-  p.cellcap = (int64_t)(vol*ext/(cell*cell*cell)*1.25) + 64;
-  p.blockSumsCap = (std::max(p.candcap, p.cellcap) + 1023)/1024 + 64;
-  if (c.precision == SPHGPU_PRECISION_MIXED) p.mreccap = p.candcap;
-  if (c.hydro == SPHGPU_HYDRO_CRKSPH) p.creccap = p.candcap;
-  double fake = 0.0;
-  if (c.compatibleEnergyEvolution) p.pacc = &fake;            // only tested for non-null
-  if (c.precision == SPHGPU_PRECISION_MIXED) p.coefF = reinterpret_cast<float*>(&fake);
-  if (c.hydro == SPHGPU_HYDRO_CRKSPH) p.K = &fake;
-  const int64_t b = problem_bytes(p);
-  p.pacc = nullptr; p.coefF = nullptr; p.K = nullptr;
-  return b;
+  e.E = (int64_t)(nbrs*(double)n);
+  e.cells = (int64_t)(1.1*cells) + 64;
+  e.bytes = planned_bytes(c, n, e.G, e.E, e.cells);
+  return e;
 }
+
+Estimate estimate_sizes(const Request& r) { return estimate_sizes(r.cfg, r.n, r.pos.data(), r.H.data()); }
 
 }  // namespace
 }  // namespace sphgpu
@@ -122,10 +116,13 @@ void release(sphgpu_server& s, Request& r) {
   r.footprint = 0;
 }
 
-int admit(sphgpu_server& s, int64_t id) {
+int admit(sphgpu_server& s, int64_t id, const Estimate& est) {
   Request& r = s.reqs[id];
   int rc = sphgpu_create(&r.cfg, r.n, &r.prob);
   if (rc == SPHGPU_OK) {
+    r.prob->hintG = est.G;
+    r.prob->hintE = est.E;
+    r.prob->hintCells = est.cells;
     rc = sphgpu_set_state(r.prob, r.pos.data(), r.vel.data(), r.mass.data(), r.rho.data(), r.eps.data(), r.H.data());
   }
   if (rc != SPHGPU_OK) {
@@ -150,12 +147,7 @@ int sphgpu_estimate_footprint(const sphgpu_config* cfg, int64_t n, const double*
     set_error("sphgpu_estimate_footprint: bad arguments");
     return SPHGPU_ERR_ARG;
   }
-  Request r;
-  r.cfg = *cfg;
-  r.n = n;
-  r.pos.assign(position, position + 3*n);
-  r.H.assign(H, H + 6*n);
-  *bytes = estimate_bytes(r);
+  *bytes = estimate_sizes(*cfg, n, position, H).bytes;
   return SPHGPU_OK;
 }
 
@@ -220,7 +212,8 @@ int sphgpu_server_tick(sphgpu_server* s, int32_t* running, int32_t* queued) {
   while (!s->queue.empty() && (int32_t)s->running.size() < s->maxMembers) {
     const int64_t id = s->queue.front();
     Request& r = s->reqs[id];
-    const int64_t need = estimate_bytes(r);
+    const Estimate est = estimate_sizes(r);
+    const int64_t need = est.bytes;
     if (need > s->budget) {
       s->queue.pop_front();
       r.state = REQ_FAILED;
@@ -232,7 +225,7 @@ int sphgpu_server_tick(sphgpu_server* s, int32_t* running, int32_t* queued) {
     s->queue.pop_front();
     r.footprint = need;
     s->inUse += need;
-    admit(*s, id);
+    admit(*s, id, est);
   }
   s->peak = std::max(s->peak, s->inUse);
   // ---- one batched RK2 step of every running simulation
