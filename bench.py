@@ -219,6 +219,23 @@ def measure_eval(h, reps=10):
     return a.elapsed_time(b) / reps
 
 
+def measure_build(h, reps=10):
+    """Duration of one ghost + ConnectivityMap build (sphgpu_build_neighbors) on the stream."""
+    import torch
+    stream = torch.cuda.ExternalStream(h.stream())
+    h.build_neighbors()
+    h.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        h.build_neighbors()
+    b.record(stream)
+    h.synchronize()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
 def measure_e2e(pkg, ns, cfg, steps, warmup):
     """Public API with host buffers: per step the state goes host->device
     (sphgpu_set_state from pinned memory), one RK2 step runs, and the new
@@ -588,6 +605,8 @@ def run_ours(args):
     hm.lib.sphgpu_connectivity_size(hm.h, ctypes.byref(g), ctypes.byref(e))
     t_eval_mixed = measure_eval(hm)
     t_eval_plain = measure_eval(hp)
+    t_build_mixed = measure_build(hm)
+    t_build_plain = measure_build(hp)
     nodes, ghosts, entries = ns.n, g.value, e.value
     alg_bytes = (nodes + ghosts) * 152 + nodes * 576 + 4 * entries
     achieved = alg_bytes / (t_eval_mixed / 1e3) / 1e9
@@ -608,9 +627,11 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (state %.2f GB, pair records %.2f GB)" % (
                            nodes * 18 * 8 / 1e9, (nodes + ghosts) * 160 / 1e9)},
             "latency_ms": {"p50": pct(lat, 0.5), "p99": pct(lat, 0.99)},
+            "stage_ms": {"neighbor_build": t_build_mixed, "evaluate_derivatives": t_eval_mixed,
+                         "rk2_step": t_mixed / args.steps},
             "plain_fp64": {"value": plain_value, "unit": METRIC, "ms_per_step": t_plain / args.steps,
                            "latency_ms": {"p50": pct(latp, 0.5), "p99": pct(latp, 0.99)},
-                           "eval_ms": t_eval_plain},
+                           "eval_ms": t_eval_plain, "build_ms": t_build_plain},
             "mixed_over_plain": value / plain_value,
             "roofline": {"bound": "hbm", "kernel": "evaluateDerivatives (record pack + sph_eval_mixed)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",

@@ -192,7 +192,14 @@ int sphgpu_kernel_launches(sphgpu_problem* p, int64_t* launches);
  * RK2 step after the ghost/connectivity rebuild (records, dt, updates,
  * derivatives, compatible energy, sum density, boundaries) is captured once
  * as a CUDA graph and replayed every step (re-captured when a buffer moves);
- * 0 = eager launches.  sphgpu_get_schedule reports what the last call used. */
+ * 0 = eager launches.  stage "neighbor passes": 1 (default) = the counting
+ * walk also builds each node's sorted list and parks it in the
+ * pair-acceleration buffer (free until the next derivative evaluation), and
+ * a compaction moves the lists into the ConnectivityMap, so the candidates
+ * are walked once; used when the problem evolves energy compatibly (it has
+ * that buffer) and the lists fit in it, otherwise 2 = a counting walk, then
+ * a filling walk.  Both give the same ConnectivityMap.
+ * sphgpu_get_schedule reports what the last call used. */
 int sphgpu_set_schedule(sphgpu_problem* p, const char* stage, int32_t schedule);
 int sphgpu_get_schedule(sphgpu_problem* p, const char* stage, int32_t* schedule);
 /* Autotuner: times every schedule of the neighbor walk and the pair loop on

@@ -522,6 +522,14 @@ int set_schedule_impl(Batch& b, int* nbrSchedule, const char* stage, int32_t sch
     for (Problem* p : b.mem) p->nbrFilter = schedule != 0;
     return SPHGPU_OK;
   }
+  if (std::strcmp(stage, "neighbor passes") == 0) {
+    if (schedule != 1 && schedule != 2) {
+      set_error("neighbor passes is 1 (lists built in the counting walk when they fit) or 2 (count, then fill)");
+      return SPHGPU_ERR_ARG;
+    }
+    for (Problem* p : b.mem) p->nbrStash = schedule == 1;
+    return SPHGPU_OK;
+  }
   if (std::strcmp(stage, "step graph") == 0) {
     if (schedule != 0 && schedule != 1) {
       set_error("step graph is 0 (eager launches) or 1 (CUDA-graph replay)");
@@ -949,6 +957,14 @@ int sphgpu_get_schedule(sphgpu_problem* p, const char* stage, int32_t* schedule)
   }
   if (std::strcmp(stage, "step graph") == 0) {
     *schedule = p->solo->useGraph ? 1 : 0;
+    return SPHGPU_OK;
+  }
+  if (std::strcmp(stage, "neighbor passes") == 0) {
+    *schedule = p->lastNbrPasses;
+    return SPHGPU_OK;
+  }
+  if (std::strcmp(stage, "neighbor filter") == 0) {
+    *schedule = p->nbrFilter ? 1 : 0;
     return SPHGPU_OK;
   }
   set_error(std::string("unknown schedule stage: ") + stage);

@@ -39,6 +39,9 @@ namespace {
 
 constexpr int kGhostThreads = 256;
 constexpr float kFilterTol = 1.0e-3f;
+// shared memory for the per-thread lists of a 32-thread block (larger lists
+// take the warp schedule)
+constexpr size_t kMaxListSmem = 200*1024;
 
 __device__ __forceinline__ unsigned long long orderedBits(double v) {
   const unsigned long long b = (unsigned long long)__double_as_longlong(v);
@@ -403,6 +406,10 @@ __global__ void __launch_bounds__(kGhostThreads) cell_scatter_kernel(const Membe
 // indices are insertion-sorted into a per-thread shared-memory list of
 // capacity `cap` (element c of thread t at lst[c*blockDim + t], conflict
 // free) and stored ascending at offsets[i].
+// A member with a stash (Grid::stashCap > 0) builds its lists in the COUNT
+// pass too and stores them ascending in the stash, element c of sorted slot s
+// at stash[c*stashStride + s]; nbr_compact_thread_kernel then moves them to
+// offsets[i], and the FILL pass does not run for it.
 template<bool FILL>
 __global__ void __launch_bounds__(256) nbr_thread_kernel(const Member* mem, BlockMap bm, int cap, int maxNbr) {
   extern __shared__ int32_t lst[];
@@ -419,6 +426,9 @@ __global__ void __launch_bounds__(256) nbr_thread_kernel(const Member* mem, Bloc
     me = loadCand(cand + s);
     active = me.idx < n;
   }
+  // list capacity: the shared-memory list (FILL) or the member's stash (COUNT)
+  const int lcap = FILL ? cap : M.grid.stashCap;
+  const bool collect = FILL || lcap > 0;
   int count = 0, above = 0;
   if (active) {
     const Grid g = loadGrid(M);
@@ -445,8 +455,8 @@ __global__ void __launch_bounds__(256) nbr_thread_kernel(const Member* mem, Bloc
         for (int64_t k = start; k < end; ++k) {
           const NbrCand c = loadCand(cand + k);
           if (c.idx != i && neighborTest(ri, Hi, me.h, c, candH, k, kernelExtent2, g.filterTol)) {
-            if (FILL) {
-              if (count < cap) {
+            if (collect) {
+              if (count < lcap) {
                 int p = count;
                 while (p > 0) {
                   const int32_t prev = lst[(p - 1)*bd + tid];
@@ -466,6 +476,15 @@ __global__ void __launch_bounds__(256) nbr_thread_kernel(const Member* mem, Bloc
     if (!FILL) {
       M.counts[i] = count;
       if (count > maxNbr) atomicOr(M.err, DERR_NBR_CAPACITY);
+      if (lcap > 0) {
+        const int64_t stride = M.grid.stashStride;
+        if (count > lcap || s >= stride) {
+          atomicOr(M.err, DERR_LIST_CAPACITY);
+        } else {
+          int32_t* stash = reinterpret_cast<int32_t*>(M.pacc);
+          for (int c = 0; c < count; ++c) stash[c*stride + s] = lst[c*bd + tid];
+        }
+      }
     } else {
       const int64_t o = M.offsets[i];
       if (count > cap) atomicOr(M.err, DERR_LIST_CAPACITY);
@@ -477,18 +496,61 @@ __global__ void __launch_bounds__(256) nbr_thread_kernel(const Member* mem, Bloc
     int m = count;
     for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((tid & 31) == 0 && m > 0) atomicMax(reinterpret_cast<int*>(M.scal + SC_MAXCOUNT), m);
-  } else {
+  }
+  if (collect) {
     unsigned long long a = (unsigned long long)above;
     for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
     if ((tid & 31) == 0 && a) atomicAdd(reinterpret_cast<unsigned long long*>(M.scal + SC_PAIRS), a);
   }
 }
 
+// Stashed lists (thread schedule) to the CSR: thread per sorted slot.
+__global__ void __launch_bounds__(256) nbr_compact_thread_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int64_t s = mb.block*blockDim.x + threadIdx.x;
+  if (s >= allNodes(M)) return;
+  const int32_t i = M.sortedIdx[s];
+  if (i >= M.n) return;
+  const int count = M.counts[i];
+  const int64_t stride = M.grid.stashStride;
+  if (count > M.grid.stashCap || s >= stride) return;   // not stashed: the count pass flagged it
+  const int64_t o = M.offsets[i];
+  if (o + count > M.ecap) {
+    atomicOr(M.err, DERR_ENTRY_CAPACITY);
+    return;
+  }
+  const int32_t* stash = reinterpret_cast<const int32_t*>(M.pacc);
+  for (int c = 0; c < count; ++c) M.nbr[o + c] = stash[c*stride + s];
+}
+
+// Stashed lists (warp schedule) to the CSR: warp per internal node, the list
+// of node i at stash[i*stashCap : i*stashCap + count].
+__global__ void __launch_bounds__(256) nbr_compact_warp_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int lane = threadIdx.x & 31;
+  const int64_t i = (mb.block*(int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (i >= M.n) return;
+  const int count = M.counts[i];
+  if (count > M.grid.stashCap) return;       // not stashed: the count pass flagged it
+  const int64_t o = M.offsets[i];
+  if (o + count > M.ecap) {
+    if (lane == 0) atomicOr(M.err, DERR_ENTRY_CAPACITY);
+    return;
+  }
+  const int32_t* stash = reinterpret_cast<const int32_t*>(M.pacc) + i*(int64_t)M.grid.stashCap;
+  for (int t = lane; t < count; t += 32) M.nbr[o + t] = stash[t];
+}
+
 // Warp per internal node: walk the 27 neighbouring cells, apply the exact
 // ConnectivityMap predicate, count (FILL=false) or collect, sort ascending
 // and store (FILL=true) the neighbor indices.  Used when the candidate sets
 // are large (many nodes per cell), where a warp per node keeps the SMs full.
-// `cap` is the per-warp list capacity (a power of two >= 32).
+// `cap` is the per-warp list capacity (a power of two >= 32).  A member with
+// a stash (Grid::stashCap > 0) collects and sorts in the COUNT pass and
+// stores the list of node i at stash[i*stashCap]; nbr_compact_warp_kernel
+// moves it to offsets[i].
 template<bool FILL>
 __global__ void __launch_bounds__(256) nbr_walk_kernel(const Member* mem, BlockMap bm, int cap, int maxNbr) {
   extern __shared__ int32_t sbuf_all[];
@@ -496,7 +558,9 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const Member* mem, BlockM
   const Member& M = mem[mb.m];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  int32_t* sbuf = sbuf_all + (FILL ? wib*cap : 0);
+  const int scap = FILL ? 0 : M.grid.stashCap;
+  const bool collect = FILL || scap > 0;
+  int32_t* sbuf = sbuf_all + (collect ? wib*cap : 0);
   const int64_t n = M.n;
   const int64_t i = (mb.block*(int64_t)blockDim.x + threadIdx.x) >> 5;
   if (i >= n) return;
@@ -535,7 +599,7 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const Member* mem, BlockM
           pass = j != (int32_t)i && neighborTest(ri, Hi, hif, c, candH, k, kernelExtent2, g.filterTol);
         }
         const unsigned ballot = __ballot_sync(0xffffffffu, pass);
-        if (FILL && pass) {
+        if (collect && pass) {
           const int pos = count + __popc(ballot & ((1u << lane) - 1u));
           if (pos < cap) sbuf[pos] = j;
         }
@@ -549,13 +613,18 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const Member* mem, BlockM
       if (count > maxNbr) atomicOr(M.err, DERR_NBR_CAPACITY);
       atomicMax(reinterpret_cast<int*>(M.scal + SC_MAXCOUNT), count);
     }
-    return;
+    if (scap == 0) return;
+    if (count > scap) {
+      if (lane == 0) atomicOr(M.err, DERR_LIST_CAPACITY);
+      return;
+    }
   }
-  const int64_t o = M.offsets[i];
-  if (count > cap || o + count > M.ecap) {
+  const int64_t o = FILL ? M.offsets[i] : 0;
+  if (FILL && (count > cap || o + count > M.ecap)) {
     if (lane == 0) atomicOr(M.err, count > cap ? DERR_LIST_CAPACITY : DERR_ENTRY_CAPACITY);
     return;
   }
+  int32_t* out = FILL ? M.nbr + o : reinterpret_cast<int32_t*>(M.pacc) + i*(int64_t)scap;
   // bitonic sort of sbuf[0:count] (padded to a power of two)
   int size = 32;
   while (size < count) size <<= 1;
@@ -577,7 +646,7 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const Member* mem, BlockM
   int above = 0;
   for (int t = lane; t < count; t += 32) {
     const int32_t j = sbuf[t];
-    M.nbr[o + t] = j;
+    out[t] = j;
     above += (j > (int32_t)i);
   }
   for (int s = 16; s > 0; s >>= 1) above += __shfl_xor_sync(0xffffffffu, above, s);
@@ -629,12 +698,22 @@ int plan_capacities(Batch& b) {
     if (tiles > p.blockSumsCap) SPH_TRY(ensure_block_sums(p, tiles));
     if (p.gcap != oldg || p.candcap != oldc || p.ecap != olde || p.cellcap != oldcells) b.memDirty = true;
     // schedule: a warp per node once the 27-cell candidate set of the last
-    // build kept 32 lanes busy
+    // build kept 32 lanes busy, or once a thread's list would not fit in
+    // shared memory
     const double candPerNode = p.ncells > 0 ? 27.0*(double)(p.n + p.G)/(double)p.ncells : 0.0;
     const int req = p.nbrSchedule != NBR_SCHEDULE_AUTO ? p.nbrSchedule : b.nbrSchedule;
-    p.fillSchedule = (req == NBR_SCHEDULE_WARP || (req == NBR_SCHEDULE_AUTO && candPerNode > 384.0))
+    p.fillSchedule = (req == NBR_SCHEDULE_WARP || (req == NBR_SCHEDULE_AUTO && candPerNode > 384.0) ||
+                      sizeof(int32_t)*32*(size_t)p.fillCap > kMaxListSmem)
                          ? NBR_SCHEDULE_WARP : NBR_SCHEDULE_THREAD;
     p.grid.filterTol = p.nbrFilter ? kFilterTol : 0.0f;
+    // single pass: the lists go to the pair-acceleration buffer (free until
+    // the next derivative evaluation rewrites it) when they fit there
+    // (thread schedule: one row per sorted slot, internal and ghost, sized
+    // from the last build's ghosts; a slot beyond it flags the build for a redo)
+    const int64_t rows = G > 0 ? p.n + grow(G) : p.candcap;
+    p.grid.stashStride = rows < p.candcap ? rows : p.candcap;
+    const int64_t slots = p.fillSchedule == NBR_SCHEDULE_WARP ? p.n : p.grid.stashStride;
+    p.grid.stashCap = (p.pacc != nullptr && p.nbrStash && (int64_t)p.fillCap*slots <= 6*p.ecap) ? p.fillCap : 0;
   }
   b.memDirty = true;
   return SPHGPU_OK;
@@ -709,57 +788,73 @@ int launch_build(Batch& b) {
   cell_scatter_kernel<<<capGrid, kGhostThreads, 0, st>>>(b.d_mem, cap); batch_count_launch(b);
   // ---- neighbor counts, offsets, lists
   int maxNbr = 0, tcap = 1, wmax = 0;
+  bool tstash = false, wstash = false;
   for (Problem* p : b.mem) {
     maxNbr = p->maxNbr > maxNbr ? p->maxNbr : maxNbr;
-    if (p->fillSchedule == NBR_SCHEDULE_WARP) wmax = p->fillCap > wmax ? p->fillCap : wmax;
-    else tcap = p->fillCap > tcap ? p->fillCap : tcap;
-  }
-  const int wthreads = 256, tthreads = 256;
-  int fthreads = tthreads;
-  while (fthreads > 32 && sizeof(int32_t)*(size_t)fthreads*tcap > 96*1024) fthreads >>= 1;
-  if (sizeof(int32_t)*(size_t)fthreads*tcap > 200*1024) {
-    // lists too long for a thread each: these members take the warp schedule
-    for (Problem* p : b.mem) {
-      if (p->fillSchedule != NBR_SCHEDULE_WARP) {
-        p->fillSchedule = NBR_SCHEDULE_WARP;
-        wmax = p->fillCap > wmax ? p->fillCap : wmax;
-      }
+    if (p->fillSchedule == NBR_SCHEDULE_WARP) {
+      wmax = p->fillCap > wmax ? p->fillCap : wmax;
+      wstash = wstash || p->grid.stashCap > 0;
+    } else {
+      tcap = p->fillCap > tcap ? p->fillCap : tcap;
+      tstash = tstash || p->grid.stashCap > 0;
     }
   }
-  BlockMap tmap, wmap, fmap;
-  unsigned tgrid = 0, wgrid = 0, fgrid = 0;
-  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.fillSchedule == NBR_SCHEDULE_WARP ? (int64_t)0 : p.candcap; },
+  const int wthreads = 256;
+  // a thread's list lives in shared memory: fewer threads per block for long lists
+  int fthreads = 256;
+  while (fthreads > 32 && sizeof(int32_t)*(size_t)fthreads*tcap > 96*1024) fthreads >>= 1;
+  const int tthreads = tstash ? fthreads : 256;
+  // bitonic sort pads each warp's list to a power of two >= 32
+  int wcap = 32;
+  while (wcap < wmax) wcap <<= 1;
+  auto thread = [](const Problem& p) { return p.fillSchedule != NBR_SCHEDULE_WARP; };
+  BlockMap tmap, wmap, fmap, wfmap, ctmap, cwmap;
+  unsigned tgrid = 0, wgrid = 0, fgrid = 0, wfgrid = 0, ctgrid = 0, cwgrid = 0;
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return thread(p) ? p.candcap : (int64_t)0; },
                           tthreads, &tmap, &tgrid));
-  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.fillSchedule == NBR_SCHEDULE_WARP ? 32*p.n : (int64_t)0; },
-                          wthreads, &wmap, &wgrid));
-  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.fillSchedule == NBR_SCHEDULE_WARP ? (int64_t)0 : p.candcap; },
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return thread(p) ? (int64_t)0 : 32*p.n; }, wthreads, &wmap, &wgrid));
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return thread(p) && !p.grid.stashCap ? p.candcap : (int64_t)0; },
                           fthreads, &fmap, &fgrid));
-  for (Problem* p : b.mem) p->lastNbrSchedule = p->fillSchedule;
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return !thread(p) && !p.grid.stashCap ? 32*p.n : (int64_t)0; },
+                          wthreads, &wfmap, &wfgrid));
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return thread(p) && p.grid.stashCap ? p.candcap : (int64_t)0; },
+                          256, &ctmap, &ctgrid));
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return !thread(p) && p.grid.stashCap ? 32*p.n : (int64_t)0; },
+                          256, &cwmap, &cwgrid));
+  for (Problem* p : b.mem) {
+    p->lastNbrSchedule = p->fillSchedule;
+    p->lastNbrPasses = p->grid.stashCap > 0 ? 1 : 2;
+  }
   b.lastNbrSchedule = nm ? b.mem[0]->lastNbrSchedule : 0;
-  if (tgrid) { nbr_thread_kernel<false><<<tgrid, tthreads, 0, st>>>(b.d_mem, tmap, 0, maxNbr); batch_count_launch(b); }
-  if (wgrid) { nbr_walk_kernel<false><<<wgrid, wthreads, 0, st>>>(b.d_mem, wmap, 0, maxNbr); batch_count_launch(b); }
-  SPH_TRY(batch_scan(b, SCAN_COUNTS));
-  if (fgrid) {
-    const size_t smem = sizeof(int32_t)*(size_t)fthreads*tcap;
-    if (smem > 48*1024) {
-      const cudaError_t e = cudaFuncSetAttribute(nbr_thread_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
+  const size_t tsmem = sizeof(int32_t)*(size_t)fthreads*tcap;
+  const size_t wsmem = sizeof(int32_t)*(wthreads/32)*(size_t)wcap;
+  if (tsmem > 48*1024) {
+    for (auto* k : {nbr_thread_kernel<false>, nbr_thread_kernel<true>}) {
+      const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
       if (e != cudaSuccess) return cuda_status(e, "nbr smem attribute");
     }
-    nbr_thread_kernel<true><<<fgrid, fthreads, smem, st>>>(b.d_mem, fmap, tcap, maxNbr); batch_count_launch(b);
+  }
+  if (wsmem > 48*1024) {
+    for (auto* k : {nbr_walk_kernel<false>, nbr_walk_kernel<true>}) {
+      const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem);
+      if (e != cudaSuccess) return cuda_status(e, "nbr smem attribute");
+    }
+  }
+  // count pass (and the lists of members with a stash)
+  if (tgrid) {
+    nbr_thread_kernel<false><<<tgrid, tthreads, tstash ? tsmem : 0, st>>>(b.d_mem, tmap, tstash ? tcap : 0, maxNbr);
+    batch_count_launch(b);
   }
   if (wgrid) {
-    // bitonic sort pads each warp's list to a power of two >= 32
-    int wcap = 32;
-    while (wcap < wmax) wcap <<= 1;
-    const size_t smem = sizeof(int32_t)*(wthreads/32)*(size_t)wcap;
-    if (smem > 48*1024) {
-      const cudaError_t e = cudaFuncSetAttribute(nbr_walk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
-      if (e != cudaSuccess) return cuda_status(e, "nbr smem attribute");
-    }
-    nbr_walk_kernel<true><<<wgrid, wthreads, smem, st>>>(b.d_mem, wmap, wcap, maxNbr); batch_count_launch(b);
+    nbr_walk_kernel<false><<<wgrid, wthreads, wstash ? wsmem : 0, st>>>(b.d_mem, wmap, wstash ? wcap : 0, maxNbr);
+    batch_count_launch(b);
   }
+  SPH_TRY(batch_scan(b, SCAN_COUNTS));
+  // lists to the CSR: compaction of the stashes, fill pass for the rest
+  if (ctgrid) { nbr_compact_thread_kernel<<<ctgrid, 256, 0, st>>>(b.d_mem, ctmap); batch_count_launch(b); }
+  if (cwgrid) { nbr_compact_warp_kernel<<<cwgrid, 256, 0, st>>>(b.d_mem, cwmap); batch_count_launch(b); }
+  if (fgrid) { nbr_thread_kernel<true><<<fgrid, fthreads, tsmem, st>>>(b.d_mem, fmap, tcap, maxNbr); batch_count_launch(b); }
+  if (wfgrid) { nbr_walk_kernel<true><<<wfgrid, wthreads, wsmem, st>>>(b.d_mem, wfmap, wcap, maxNbr); batch_count_launch(b); }
   return cuda_status(cudaGetLastError(), "neighbor build");
 }
 

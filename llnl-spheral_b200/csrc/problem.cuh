@@ -116,6 +116,9 @@ struct Grid {
   double cell;
   int dim[3];
   float filterTol;     // relative band of the FP32 neighbor pre-test (0: exact test only)
+  int stashCap;        // lists built in the count pass, at most this long, kept in the
+                       // pair-acceleration buffer until compacted (0: separate fill pass)
+  int64_t stashStride; // thread schedule: element c of sorted slot s at c*stashStride + s
 };
 
 struct Batch;
@@ -135,6 +138,8 @@ struct Problem {
   int nbrSchedule = 0;      // NBR_SCHEDULE_* requested for the neighbor walk
   int lastNbrSchedule = 0;  // schedule the last build used
   bool nbrFilter = true;    // FP32 pre-test in the neighbor walk (exact either way)
+  bool nbrStash = true;     // single-pass neighbor walk when the lists fit the stash
+  int lastNbrPasses = 0;    // walks over the candidates the last build made (1 or 2)
   int fillCap = 0;          // neighbor-list capacity planned for the fill pass
   int fillSchedule = 0;     // schedule planned for this build (NBR_SCHEDULE_THREAD/WARP)
   // sizes the first neighbor build plans its buffers from (0: built-in guesses)

@@ -70,14 +70,18 @@ def test_connectivity_bitexact(gpu_lib, pkg, oracle_mod, case):
 @pytest.mark.parametrize("case", ["sod", "kh", "sod_x_periodic_only"])
 @pytest.mark.parametrize("schedule", [1, 2])
 @pytest.mark.parametrize("nfilter", [0, 1])
-def test_connectivity_every_schedule(gpu_lib, pkg, oracle_mod, case, schedule, nfilter):
+@pytest.mark.parametrize("passes", [1, 2])
+def test_connectivity_every_schedule(gpu_lib, pkg, oracle_mod, case, schedule, nfilter, passes):
     """Thread-per-node and warp-per-node neighbor walks, with and without the
-    FP32 pre-test, give the same CSR."""
+    FP32 pre-test, in one pass (lists parked in the pair-acceleration buffer,
+    then compacted) or two (count, then fill), give the same CSR."""
     g, o, ns = _pair(pkg, oracle_mod, case)
     g.set_schedule("neighbor walk", schedule)
     g.set_schedule("neighbor filter", nfilter)
+    g.set_schedule("neighbor passes", passes)
     g.build_neighbors()
     assert g.schedule("neighbor walk") == schedule
+    assert g.schedule("neighbor passes") == passes
     o.build_neighbors()
     go, gn, gr = g.connectivity()
     oo, on, orr = o.connectivity()
@@ -196,6 +200,21 @@ def test_large_neighbor_counts(gpu_lib, pkg, oracle_mod):
     g.evaluateDerivatives()
     o.evaluate_derivatives()
     assert np.array_equal(g.field("delta velocity hydro"), o.field("delta velocity hydro"))
+
+
+def test_single_pass_needs_the_pair_acceleration_buffer(gpu_lib, pkg, oracle_mod):
+    """Without compatible energy there is no pair-acceleration buffer to park
+    the lists in: the build counts, then fills, with the same CSR."""
+    g, o, ns = _pair(pkg, oracle_mod, "kh_noncompatible_integrate_density")
+    g.build_neighbors()
+    o.build_neighbors()
+    assert g.schedule("neighbor passes") == 2
+    go, gn, _ = g.connectivity()
+    oo, on, _ = o.connectivity()
+    assert np.array_equal(go, oo) and np.array_equal(gn, on)
+    k, ok, _ = _pair(pkg, oracle_mod, "kh")
+    k.build_neighbors()
+    assert k.schedule("neighbor passes") == 1
 
 
 def test_empty_problem_rejected(gpu_lib, pkg):
