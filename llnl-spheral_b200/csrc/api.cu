@@ -619,10 +619,10 @@ int batch_step_rk2(Batch& b) {
 int64_t problem_bytes(const Problem& p) {
   const int64_t n = p.n;
   const int stagingComps = p.cfg.hydro == SPHGPU_HYDRO_CRKSPH ? 27 : 9;
-  int64_t b = 8*(2*(int64_t)NSTATE*n + (int64_t)NDERIV*n + stagingComps*n + n + NSCAL + 148*4*8) + 16;
+  int64_t b = 8*(2*(int64_t)NSTATE*n + (int64_t)NDERIV*n + stagingComps*n + 2*n + NSCAL + 148*4*8) + 16;
   b += 8*(6 + 2)*(int64_t)p.prm.W.n;                                  // tables
   b += p.gcap*(4 + 4 + 24);                                           // groot, gcode, gpos
-  b += p.candcap*(4 + 4 + 4 + 112 + 8*RECW) + 8*(p.candcap + 1);       // counts, cidx, sortedIdx, cand, rec, offsets
+  b += p.candcap*(4 + 4 + 4 + 8*CAND_DOUBLES + 8*RECW) + 8*(p.candcap + 1);  // counts, cidx, sortedIdx, cand, rec, offsets
   b += p.ecap*(4 + (p.pacc ? 24 : 0));                                // nbr, pacc
   b += p.cellcap*(8 + 4) + 8 + 8*p.blockSumsCap;
   b += 8*(int64_t)(p.cfg.hydro == SPHGPU_HYDRO_CRKSPH ? CMRECW : MRECW)*p.mreccap +
@@ -665,7 +665,7 @@ int ensure_capacity_ghosts(Problem& p, int64_t need) {
   SPH_TRY(grow_preserve(p.cidx, 0, nc, p.stream));
   SPH_TRY(grow_preserve(p.sortedIdx, 0, nc, p.stream));
   cudaFree(p.cand);
-  SPH_TRY(dalloc(p.cand, 14*nc));          // 64-byte records + 48-byte FP64 H
+  SPH_TRY(dalloc(p.cand, CAND_DOUBLES*nc));
   cudaFree(p.rec);
   SPH_TRY(dalloc(p.rec, RECW*nc));
   p.candcap = nc;
@@ -761,7 +761,7 @@ int sphgpu_create(const sphgpu_config* cfg, int64_t n_internal, sphgpu_problem**
     // widest field: Tensor (9) for SPH, the third-rank grad m2 (27) for CRKSPH
     if ((rc = dalloc(p->staging, (cfg->hydro == SPHGPU_HYDRO_CRKSPH ? 27 : 9)*n)) != SPHGPU_OK) break;
     if ((rc = dalloc(p->d_err, 4)) != SPHGPU_OK) break;
-    if ((rc = dalloc(p->hmaxi, n)) != SPHGPU_OK) break;
+    if ((rc = dalloc(p->hmaxi, 2*n)) != SPHGPU_OK) break;
     if ((rc = dalloc(p->d_scal, NSCAL)) != SPHGPU_OK) break;
     p->redcap = 148*4*8;
     if ((rc = dalloc(p->d_red, p->redcap)) != SPHGPU_OK) break;

@@ -90,27 +90,30 @@ __global__ void build_init_kernel(const Member* mem, int nmem) {
   setScalI(s, SC_NTOT, mem[m].n);
   setScalI(s, SC_G, 0);
   s[SC_HMAX] = 0.0;
-  s[SC_MAXCOND] = 0.0;
+  s[SC_LMAXALL] = 0.0;
 }
 
-// 1/min(eig(H)) of every internal node, once per build (ghosts share their
-// root's H, so every boundary pass and the cell size read it from here), and
-// the largest condition number of H (bounds the FP32 pre-test error).
+// 1/min(eig(H)) (hmaxi[i]) and max(eig(H)) (hmaxi[n + i]) of every internal
+// node, once per build (ghosts share their root's H, so every boundary pass,
+// the cell size and the pre-test records read them from here), and the
+// largest max(eig(H)) of the problem (with the largest 1/min(eig(H)) it
+// bounds the FP32 pre-test error).
 __global__ void __launch_bounds__(kGhostThreads) node_hmax_kernel(const Member* mem, BlockMap bm) {
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
   const int64_t i = mb.block*blockDim.x + threadIdx.x;
-  double cond = 0.0;
+  double lmax = 0.0;
   if (i < M.n) {
     const V3 ev = eigenValues(nodeH(M, i));
     M.hmaxi[i] = 1.0/vmin(ev);
-    cond = vmax(ev)/vmin(ev);
-    if (!(cond < 1.0e300)) cond = 1.0e300;     // degenerate H: no FP32 pre-test
+    lmax = vmax(ev);
+    M.hmaxi[M.n + i] = lmax;
+    if (!(lmax < 1.0e300)) lmax = 1.0e300;     // degenerate H: no FP32 pre-test
   }
-  for (int o = 16; o > 0; o >>= 1) cond = dmax(cond, __shfl_xor_sync(0xffffffffu, cond, o));
-  if ((threadIdx.x & 31) == 0 && cond > 0.0)
-    atomicMax(reinterpret_cast<unsigned long long*>(M.scal + SC_MAXCOND),
-              (unsigned long long)__double_as_longlong(cond));
+  for (int o = 16; o > 0; o >>= 1) lmax = dmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+  if ((threadIdx.x & 31) == 0 && lmax > 0.0)
+    atomicMax(reinterpret_cast<unsigned long long*>(M.scal + SC_LMAXALL),
+              (unsigned long long)__double_as_longlong(lmax));
 }
 
 __device__ __forceinline__ double nodeHmax(const Member& M, int64_t k) {
@@ -243,7 +246,7 @@ __global__ void __launch_bounds__(kGhostThreads) node_bounds_kernel(const Member
 // covers the libm difference of the eigenvalue solve for anisotropic H),
 // enlarged until the cells fit the cell buffers (larger cells only widen the
 // candidate set).  Also resets the walk's counters and sets the FP32
-// pre-test tolerance: only when every H has condition number <= 100.
+// pre-test tolerance: only when max h / min h over the problem is <= 100.
 __global__ void grid_kernel(const Member* mem, int nmem) {
   const int m = blockIdx.x*blockDim.x + threadIdx.x;
   if (m >= nmem) return;
@@ -274,8 +277,9 @@ __global__ void grid_kernel(const Member* mem, int nmem) {
   s[0] = lo[0]; s[1] = lo[1]; s[2] = lo[2];
   s[3] = cell;
   for (int a = 0; a < 3; ++a) setScalI(M.scal, SC_GRID + 4 + a, dim[a]);
-  const double cond = M.scal[SC_MAXCOND];
-  s[7] = (M.grid.filterTol > 0.0f && cond > 0.0 && cond <= 100.0) ? (double)M.grid.filterTol : 0.0;
+  // largest h over smallest h of the problem (>= every node's condition number)
+  const double spread = hmaxAll*M.scal[SC_LMAXALL];
+  s[7] = (M.grid.filterTol > 0.0f && spread > 0.0 && spread <= 100.0) ? (double)M.grid.filterTol : 0.0;
   setScalI(M.scal, SC_NCELLS, ncells);
   setScalI(M.scal, SC_MAXCOUNT, 0);
   setScalI(M.scal, SC_PAIRS, 0);
@@ -308,42 +312,43 @@ __global__ void __launch_bounds__(kGhostThreads) cell_index_kernel(const Member*
   atomicAdd(M.cellFill + c, 1);
 }
 
-// Candidate record of the cell-sorted node list, 64 bytes read as four
-// 16-byte loads: FP64 position, node index, FP32 copy of H.  The FP64 H of
-// the same slot sits in a second array (48 bytes) and is read only when the
-// FP32 pre-test cannot decide.
-struct __align__(16) NbrCand {
-  double x, y, z;
-  int32_t idx;
-  float h[6];
-  float pad;
+// Cell-ordered candidate arrays (Problem::cand), one slot per node:
+//   exact   [candcap] 32 bytes: FP64 position, node index
+//   H       [candcap] 48 bytes: FP64 H
+//   pre     [candcap] float4:   FP32 offsets of the position from the lower
+//                               corner of the node's cell, FP32 min eig(H)
+//   lmax    [candcap] float:    FP32 max eig(H)
+// The walks read only `pre` for most candidates; `exact` and `H` are read
+// for the candidates the FP32 pre-test cannot decide, `lmax` when the i-side
+// test alone does not.
+struct NbrArrays {
+  const double* exact;
+  const double* H;
+  const float4* pre;
+  const float* lmax;
 };
-static_assert(sizeof(NbrCand) == 64, "candidate record is four 16-byte words");
 
-__device__ __forceinline__ NbrCand loadCand(const NbrCand* c) {
-  const double2* q = reinterpret_cast<const double2*>(c);
-  const double2 a = __ldg(q);
-  const double2 b = __ldg(q + 1);
-  const float4 f = __ldg(reinterpret_cast<const float4*>(q + 2));
-  const float4 g = __ldg(reinterpret_cast<const float4*>(q + 3));
-  NbrCand r;
-  r.x = a.x; r.y = a.y; r.z = b.x;
-  const uint64_t w = (uint64_t)__double_as_longlong(b.y);
-  r.idx = (int32_t)(uint32_t)(w & 0xffffffffu);
-  r.h[0] = __uint_as_float((uint32_t)(w >> 32));
-  r.h[1] = f.x; r.h[2] = f.y; r.h[3] = f.z; r.h[4] = f.w; r.h[5] = g.x;
-  r.pad = 0.0f;
-  return r;
+__device__ __forceinline__ NbrArrays nbrArrays(const Member& M) {
+  const double* c = static_cast<const double*>(M.cand);
+  NbrArrays a;
+  a.exact = c;
+  a.H = c + 4*M.candcap;
+  a.pre = reinterpret_cast<const float4*>(c + 10*M.candcap);
+  a.lmax = reinterpret_cast<const float*>(c + 12*M.candcap);
+  return a;
 }
 
-__device__ __forceinline__ const double* candHArray(const Member& M) {
-  return static_cast<const double*>(M.cand) + 8*M.candcap;
+__device__ __forceinline__ V3 candPos(const NbrArrays& a, int64_t k, int32_t* idx) {
+  const double2* q = reinterpret_cast<const double2*>(a.exact + 4*k);
+  const double2 u = __ldg(q), v = __ldg(q + 1);
+  if (idx) *idx = (int32_t)(uint32_t)((uint64_t)__double_as_longlong(v.y) & 0xffffffffu);
+  return V3{u.x, u.y, v.x};
 }
 
-__device__ __forceinline__ Sym loadCandH(const double* candH, int64_t k) {
-  const double2* q = reinterpret_cast<const double2*>(candH + 6*k);
-  const double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
-  return Sym{a.x, a.y, b.x, b.y, c.x, c.y};
+__device__ __forceinline__ Sym candH(const NbrArrays& a, int64_t k) {
+  const double2* q = reinterpret_cast<const double2*>(a.H + 6*k);
+  const double2 u = __ldg(q), v = __ldg(q + 1), w = __ldg(q + 2);
+  return Sym{u.x, u.y, v.x, v.y, w.x, w.y};
 }
 
 __device__ __forceinline__ float symEta2F(const float* h, float x, float y, float z) {
@@ -353,26 +358,82 @@ __device__ __forceinline__ float symEta2F(const float* h, float x, float y, floa
   return __fmaf_rn(ex, ex, __fmaf_rn(ey, ey, ez*ez));
 }
 
-// ConnectivityMap predicate |H_i r_ij|^2 <= kappa^2 || |H_j r_ij|^2 <= kappa^2.
-// A FP32 pre-test on r_ij = r_i - r_j (formed in FP64, rounded once) decides
-// every pair whose eta^2 lies outside the band kappa^2 (1 -+ tol); inside the
-// band the test is the exact FP64 one in the reference's operation order.
-// The FP32 error of eta^2 is below 1e-6 cond(H) relative, and tol is only set
-// (1e-3) when every H has cond(H) <= 100, so the result equals the exact test.
-__device__ __forceinline__ bool neighborTest(const V3& ri, const Sym& Hi, const float* hif, const NbrCand& c,
-                                             const double* candH, int64_t k, double k2, float tol) {
-  const double dx = ri.x - c.x, dy = ri.y - c.y, dz = ri.z - c.z;
-  if (tol > 0.0f) {
-    const float fx = (float)dx, fy = (float)dy, fz = (float)dz;
-    const float e2i = symEta2F(hif, fx, fy, fz);
-    const float e2j = symEta2F(c.h, fx, fy, fz);
-    const float k2f = (float)k2;
-    const float lo = k2f*(1.0f - tol), hi = k2f*(1.0f + tol);
-    if (e2i <= lo || e2j <= lo) return true;
-    if (e2i > hi && e2j > hi) return false;
+// The walking node: FP32 H and cell offsets for the pre-test, its cell and
+// its sorted slot (the exact test re-reads its FP64 position and H there).
+struct Walker {
+  float hf[6];
+  float ox, oy, oz;
+  int cx, cy, cz;
+  int64_t slot;
+  int32_t idx;
+};
+
+__device__ __forceinline__ Walker makeWalker(const NbrArrays& a, const Grid& g, int64_t s) {
+  Walker w;
+  w.slot = s;
+  const V3 r = candPos(a, s, &w.idx);
+  const Sym H = candH(a, s);
+  w.hf[0] = (float)H.xx; w.hf[1] = (float)H.xy; w.hf[2] = (float)H.xz;
+  w.hf[3] = (float)H.yy; w.hf[4] = (float)H.yz; w.hf[5] = (float)H.zz;
+  const float4 p = __ldg(a.pre + s);
+  w.ox = p.x; w.oy = p.y; w.oz = p.z;
+  w.cx = cellCoord(r.x, g.lo[0], g.cell, g.dim[0]);
+  w.cy = cellCoord(r.y, g.lo[1], g.cell, g.dim[1]);
+  w.cz = cellCoord(r.z, g.lo[2], g.cell, g.dim[2]);
+  return w;
+}
+
+// One x-row of up to three cells of the walk: its slot range and the ends of
+// its first two cells (a candidate's cell follows from its slot).
+struct Row {
+  int64_t start, end, e0, e1;
+  int x0;
+  float dyc, dzc;     // (cy' - cy)*cell, (cz' - cz)*cell in FP32
+};
+
+__device__ __forceinline__ Row loadRow(const int64_t* cellStart, const Grid& g, const Walker& w, int y, int z,
+                                       float cellf) {
+  const int x0 = w.cx > 0 ? w.cx - 1 : 0;
+  const int x1 = w.cx + 1 < g.dim[0] ? w.cx + 1 : g.dim[0] - 1;
+  const int nx = x1 - x0 + 1;
+  const int64_t* cs = cellStart + (int64_t)(z*g.dim[1] + y)*g.dim[0] + x0;
+  Row row;
+  row.start = cs[0];
+  row.e0 = cs[1];
+  row.e1 = cs[nx < 2 ? nx : 2];
+  row.end = cs[nx];
+  row.x0 = x0;
+  row.dyc = (float)(y - w.cy)*cellf;
+  row.dzc = (float)(z - w.cz)*cellf;
+  return row;
+}
+
+// ConnectivityMap predicate |H_i r_ij|^2 <= kappa^2 || |H_j r_ij|^2 <= kappa^2
+// (src/Neighbor/ConnectivityMapInline.hh:169-186) for candidate slot k.
+// With tol > 0 a FP32 pre-test decides every pair whose eta^2 lies clearly
+// outside the band kappa^2 (1 -+ tol): eta_i^2 from the FP32 H_i, eta_j^2
+// bounded by min/max eig(H_j)^2 |r_ij|^2, r_ij from the cell offsets.  The
+// pre-test error is below 1e-6 (max h/min h over the problem) relative, and
+// tol (1e-3) is only set when that ratio is <= 100, so it never decides a
+// pair the exact test would decide otherwise.  Undecided pairs take the
+// exact FP64 test in the reference's operation order.
+__device__ __forceinline__ bool candTest(const NbrArrays& a, const Walker& w, const Row& row, int64_t k,
+                                         float cellf, double k2, float k2lo, float k2hi, bool pretest) {
+  if (pretest) {
+    const float4 c = __ldg(a.pre + k);
+    const float dxc = (float)(row.x0 - w.cx + (k >= row.e0) + (k >= row.e1))*cellf;
+    const float fx = (w.ox - c.x) - dxc, fy = (w.oy - c.y) - row.dyc, fz = (w.oz - c.z) - row.dzc;
+    const float e2i = symEta2F(w.hf, fx, fy, fz);
+    if (e2i <= k2lo) return true;
+    const float r2 = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, fz*fz));
+    if (e2i > k2hi && c.w*c.w*r2 > k2hi) return false;
+    const float lm = __ldg(a.lmax + k);
+    if (lm*lm*r2 <= k2lo) return true;
   }
-  const V3 rij{dx, dy, dz};
-  return mag2(sdot(Hi, rij)) <= k2 || mag2(sdot(loadCandH(candH, k), rij)) <= k2;
+  const V3 ri = candPos(a, w.slot, nullptr);
+  const V3 rj = candPos(a, k, nullptr);
+  const V3 rij{ri.x - rj.x, ri.y - rj.y, ri.z - rj.z};
+  return mag2(sdot(candH(a, w.slot), rij)) <= k2 || mag2(sdot(candH(a, k), rij)) <= k2;
 }
 
 __global__ void __launch_bounds__(kGhostThreads) cell_scatter_kernel(const Member* mem, BlockMap bm) {
@@ -385,23 +446,30 @@ __global__ void __launch_bounds__(kGhostThreads) cell_scatter_kernel(const Membe
   M.sortedIdx[slot] = (int32_t)k;
   const V3 r = nodePos(M, k);
   const Sym H = nodeH(M, k);
-  double2* q = reinterpret_cast<double2*>(static_cast<NbrCand*>(M.cand) + slot);
-  const uint64_t w = (uint64_t)(uint32_t)k | ((uint64_t)__float_as_uint((float)H.xx) << 32);
+  const Grid g = loadGrid(M);
+  const int cx = cellCoord(r.x, g.lo[0], g.cell, g.dim[0]);
+  const int cy = cellCoord(r.y, g.lo[1], g.cell, g.dim[1]);
+  const int cz = cellCoord(r.z, g.lo[2], g.cell, g.dim[2]);
+  const int64_t root = k < M.n ? k : M.groot[k - M.n];
+  double* base = static_cast<double*>(M.cand);
+  double2* q = reinterpret_cast<double2*>(base + 4*slot);
   q[0] = make_double2(r.x, r.y);
-  q[1] = make_double2(r.z, __longlong_as_double((long long)w));
-  float4* f = reinterpret_cast<float4*>(q + 2);
-  f[0] = make_float4((float)H.xy, (float)H.xz, (float)H.yy, (float)H.yz);
-  f[1] = make_float4((float)H.zz, 0.0f, 0.0f, 0.0f);
-  double2* h = reinterpret_cast<double2*>(const_cast<double*>(candHArray(M)) + 6*slot);
+  q[1] = make_double2(r.z, __longlong_as_double((long long)(uint64_t)(uint32_t)k));
+  double2* h = reinterpret_cast<double2*>(base + 4*M.candcap + 6*slot);
   h[0] = make_double2(H.xx, H.xy);
   h[1] = make_double2(H.xz, H.yy);
   h[2] = make_double2(H.yz, H.zz);
+  float4* pre = reinterpret_cast<float4*>(base + 10*M.candcap);
+  pre[slot] = make_float4((float)(r.x - (g.lo[0] + cx*g.cell)), (float)(r.y - (g.lo[1] + cy*g.cell)),
+                          (float)(r.z - (g.lo[2] + cz*g.cell)), (float)(1.0/M.hmaxi[root]));
+  float* lmax = reinterpret_cast<float*>(base + 12*M.candcap);
+  lmax[slot] = (float)M.hmaxi[M.n + root];
 }
 
 // Thread per internal node, nodes taken in cell-sorted order so that the
 // threads of a warp share their candidate rows (L1 broadcast).  The 27
 // neighbouring cells are walked as 9 x-rows (three cells each, contiguous in
-// the sorted order) and the exact ConnectivityMap predicate is applied.
+// the sorted order) and the ConnectivityMap predicate is applied.
 // COUNT pass: per-node counts and their maximum.  FILL pass: the neighbor
 // indices are insertion-sorted into a per-thread shared-memory list of
 // capacity `cap` (element c of thread t at lst[c*blockDim + t], conflict
@@ -419,11 +487,12 @@ __global__ void __launch_bounds__(256) nbr_thread_kernel(const Member* mem, Bloc
   const int bd = blockDim.x;
   const int64_t s = mb.block*bd + tid;
   const int64_t n = M.n;
-  const NbrCand* cand = static_cast<const NbrCand*>(M.cand);
-  NbrCand me;
+  const NbrArrays a = nbrArrays(M);
+  const Grid g = loadGrid(M);
   bool active = s < allNodes(M);
+  Walker me;
   if (active) {
-    me = loadCand(cand + s);
+    me = makeWalker(a, g, s);
     active = me.idx < n;
   }
   // list capacity: the shared-memory list (FILL) or the member's stash (COUNT)
@@ -431,42 +500,34 @@ __global__ void __launch_bounds__(256) nbr_thread_kernel(const Member* mem, Bloc
   const bool collect = FILL || lcap > 0;
   int count = 0, above = 0;
   if (active) {
-    const Grid g = loadGrid(M);
-    const double kernelExtent2 = M.prm.kernelExtent*M.prm.kernelExtent;
-    const int64_t* cellStart = M.cellStart;
-    const double* candH = candHArray(M);
+    const double k2 = M.prm.kernelExtent*M.prm.kernelExtent;
+    const float k2f = (float)k2;
+    const bool pretest = g.filterTol > 0.0f;
+    const float k2lo = k2f*(1.0f - g.filterTol), k2hi = k2f*(1.0f + g.filterTol);
+    const float cellf = (float)g.cell;
     const int32_t i = me.idx;
-    const V3 ri{me.x, me.y, me.z};
-    const Sym Hi = loadCandH(candH, s);
-    const int cx = cellCoord(ri.x, g.lo[0], g.cell, g.dim[0]);
-    const int cy = cellCoord(ri.y, g.lo[1], g.cell, g.dim[1]);
-    const int cz = cellCoord(ri.z, g.lo[2], g.cell, g.dim[2]);
-    const int x0 = cx > 0 ? cx - 1 : 0;
-    const int x1 = cx + 1 < g.dim[0] ? cx + 1 : g.dim[0] - 1;
     for (int dz = -1; dz <= 1; ++dz) {
-      const int z = cz + dz;
+      const int z = me.cz + dz;
       if (z < 0 || z >= g.dim[2]) continue;
       for (int dy = -1; dy <= 1; ++dy) {
-        const int y = cy + dy;
+        const int y = me.cy + dy;
         if (y < 0 || y >= g.dim[1]) continue;
-        const int cbase = (z*g.dim[1] + y)*g.dim[0];
-        const int64_t start = cellStart[cbase + x0];
-        const int64_t end = cellStart[cbase + x1 + 1];
-        for (int64_t k = start; k < end; ++k) {
-          const NbrCand c = loadCand(cand + k);
-          if (c.idx != i && neighborTest(ri, Hi, me.h, c, candH, k, kernelExtent2, g.filterTol)) {
+        const Row row = loadRow(M.cellStart, g, me, y, z, cellf);
+        for (int64_t k = row.start; k < row.end; ++k) {
+          if (k != s && candTest(a, me, row, k, cellf, k2, k2lo, k2hi, pretest)) {
             if (collect) {
+              const int32_t j = __ldg(M.sortedIdx + k);
               if (count < lcap) {
                 int p = count;
                 while (p > 0) {
                   const int32_t prev = lst[(p - 1)*bd + tid];
-                  if (prev < c.idx) break;
+                  if (prev < j) break;
                   lst[p*bd + tid] = prev;
                   --p;
                 }
-                lst[p*bd + tid] = c.idx;
+                lst[p*bd + tid] = j;
               }
-              above += (c.idx > i);
+              above += (j > i);
             }
             ++count;
           }
@@ -498,9 +559,9 @@ __global__ void __launch_bounds__(256) nbr_thread_kernel(const Member* mem, Bloc
     if ((tid & 31) == 0 && m > 0) atomicMax(reinterpret_cast<int*>(M.scal + SC_MAXCOUNT), m);
   }
   if (collect) {
-    unsigned long long a = (unsigned long long)above;
-    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if ((tid & 31) == 0 && a) atomicAdd(reinterpret_cast<unsigned long long*>(M.scal + SC_PAIRS), a);
+    unsigned long long b = (unsigned long long)above;
+    for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(0xffffffffu, b, o);
+    if ((tid & 31) == 0 && b) atomicAdd(reinterpret_cast<unsigned long long*>(M.scal + SC_PAIRS), b);
   }
 }
 
@@ -543,14 +604,15 @@ __global__ void __launch_bounds__(256) nbr_compact_warp_kernel(const Member* mem
   for (int t = lane; t < count; t += 32) M.nbr[o + t] = stash[t];
 }
 
-// Warp per internal node: walk the 27 neighbouring cells, apply the exact
-// ConnectivityMap predicate, count (FILL=false) or collect, sort ascending
-// and store (FILL=true) the neighbor indices.  Used when the candidate sets
-// are large (many nodes per cell), where a warp per node keeps the SMs full.
-// `cap` is the per-warp list capacity (a power of two >= 32).  A member with
-// a stash (Grid::stashCap > 0) collects and sorts in the COUNT pass and
-// stores the list of node i at stash[i*stashCap]; nbr_compact_warp_kernel
-// moves it to offsets[i].
+// Warp per internal node (warps dealt over the sorted slots, ghost slots
+// idle): walk the 27 neighbouring cells, apply the ConnectivityMap
+// predicate, count (FILL=false) or collect, sort ascending and store
+// (FILL=true) the neighbor indices.  Used when the candidate sets are large
+// (many nodes per cell), where a warp per node keeps the SMs full.  `cap` is
+// the per-warp list capacity (a power of two >= 32).  A member with a stash
+// (Grid::stashCap > 0) collects and sorts in the COUNT pass and stores the
+// list of node i at stash[i*stashCap]; nbr_compact_warp_kernel moves it to
+// offsets[i].
 template<bool FILL>
 __global__ void __launch_bounds__(256) nbr_walk_kernel(const Member* mem, BlockMap bm, int cap, int maxNbr) {
   extern __shared__ int32_t sbuf_all[];
@@ -561,47 +623,34 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const Member* mem, BlockM
   const int scap = FILL ? 0 : M.grid.stashCap;
   const bool collect = FILL || scap > 0;
   int32_t* sbuf = sbuf_all + (collect ? wib*cap : 0);
-  const int64_t n = M.n;
-  const int64_t i = (mb.block*(int64_t)blockDim.x + threadIdx.x) >> 5;
-  if (i >= n) return;
-  const double* S = M.S;
+  const int64_t s = (mb.block*(int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (s >= allNodes(M)) return;
+  const NbrArrays a = nbrArrays(M);
   const Grid g = loadGrid(M);
-  const NbrCand* cand = static_cast<const NbrCand*>(M.cand);
-  const double kernelExtent2 = M.prm.kernelExtent*M.prm.kernelExtent;
-  const V3 ri{S[S_X*n + i], S[S_Y*n + i], S[S_Z*n + i]};
-  const Sym Hi{S[(S_H + 0)*n + i], S[(S_H + 1)*n + i], S[(S_H + 2)*n + i],
-               S[(S_H + 3)*n + i], S[(S_H + 4)*n + i], S[(S_H + 5)*n + i]};
-  const float hif[6] = {(float)Hi.xx, (float)Hi.xy, (float)Hi.xz, (float)Hi.yy, (float)Hi.yz, (float)Hi.zz};
-  const double* candH = candHArray(M);
-  const int cx = cellCoord(ri.x, g.lo[0], g.cell, g.dim[0]);
-  const int cy = cellCoord(ri.y, g.lo[1], g.cell, g.dim[1]);
-  const int cz = cellCoord(ri.z, g.lo[2], g.cell, g.dim[2]);
+  const Walker me = makeWalker(a, g, s);
+  if (me.idx >= M.n) return;
+  const int32_t i = me.idx;
+  const double k2 = M.prm.kernelExtent*M.prm.kernelExtent;
+  const float k2f = (float)k2;
+  const bool pretest = g.filterTol > 0.0f;
+  const float k2lo = k2f*(1.0f - g.filterTol), k2hi = k2f*(1.0f + g.filterTol);
+  const float cellf = (float)g.cell;
   int count = 0;
   for (int dz = -1; dz <= 1; ++dz) {
-    const int z = cz + dz;
+    const int z = me.cz + dz;
     if (z < 0 || z >= g.dim[2]) continue;
     for (int dy = -1; dy <= 1; ++dy) {
-      const int y = cy + dy;
+      const int y = me.cy + dy;
       if (y < 0 || y >= g.dim[1]) continue;
-      // the three x-cells of a row are contiguous in the sorted order
-      const int x0 = cx > 0 ? cx - 1 : 0;
-      const int x1 = cx + 1 < g.dim[0] ? cx + 1 : g.dim[0] - 1;
-      const int cbase = (z*g.dim[1] + y)*g.dim[0];
-      const int64_t start = M.cellStart[cbase + x0];
-      const int64_t end = M.cellStart[cbase + x1 + 1];
-      for (int64_t base = start; base < end; base += 32) {
+      // the x-cells of a row are contiguous in the sorted order
+      const Row row = loadRow(M.cellStart, g, me, y, z, cellf);
+      for (int64_t base = row.start; base < row.end; base += 32) {
         const int64_t k = base + lane;
-        bool pass = false;
-        int32_t j = -1;
-        if (k < end) {
-          const NbrCand c = loadCand(cand + k);
-          j = c.idx;
-          pass = j != (int32_t)i && neighborTest(ri, Hi, hif, c, candH, k, kernelExtent2, g.filterTol);
-        }
+        const bool pass = k < row.end && k != s && candTest(a, me, row, k, cellf, k2, k2lo, k2hi, pretest);
         const unsigned ballot = __ballot_sync(0xffffffffu, pass);
         if (collect && pass) {
           const int pos = count + __popc(ballot & ((1u << lane) - 1u));
-          if (pos < cap) sbuf[pos] = j;
+          if (pos < cap) sbuf[pos] = __ldg(M.sortedIdx + k);
         }
         count += __popc(ballot);
       }
@@ -635,9 +684,9 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const Member* mem, BlockM
       for (int t = lane; t < size; t += 32) {
         const int ixj = t ^ jj;
         if (ixj > t) {
-          const int32_t a = sbuf[t], b = sbuf[ixj];
+          const int32_t u = sbuf[t], v = sbuf[ixj];
           const bool up = (t & k) == 0;
-          if ((a > b) == up) { sbuf[t] = b; sbuf[ixj] = a; }
+          if ((u > v) == up) { sbuf[t] = v; sbuf[ixj] = u; }
         }
       }
       __syncwarp();
@@ -649,7 +698,7 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const Member* mem, BlockM
     out[t] = j;
     above += (j > (int32_t)i);
   }
-  for (int s = 16; s > 0; s >>= 1) above += __shfl_xor_sync(0xffffffffu, above, s);
+  for (int sh = 16; sh > 0; sh >>= 1) above += __shfl_xor_sync(0xffffffffu, above, sh);
   if (lane == 0 && above)
     atomicAdd(reinterpret_cast<unsigned long long*>(M.scal + SC_PAIRS), (unsigned long long)above);
 }
@@ -812,10 +861,11 @@ int launch_build(Batch& b) {
   unsigned tgrid = 0, wgrid = 0, fgrid = 0, wfgrid = 0, ctgrid = 0, cwgrid = 0;
   SPH_TRY(batch_map_items(b, [&](const Problem& p) { return thread(p) ? p.candcap : (int64_t)0; },
                           tthreads, &tmap, &tgrid));
-  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return thread(p) ? (int64_t)0 : 32*p.n; }, wthreads, &wmap, &wgrid));
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return thread(p) ? (int64_t)0 : 32*p.candcap; },
+                          wthreads, &wmap, &wgrid));
   SPH_TRY(batch_map_items(b, [&](const Problem& p) { return thread(p) && !p.grid.stashCap ? p.candcap : (int64_t)0; },
                           fthreads, &fmap, &fgrid));
-  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return !thread(p) && !p.grid.stashCap ? 32*p.n : (int64_t)0; },
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return !thread(p) && !p.grid.stashCap ? 32*p.candcap : (int64_t)0; },
                           wthreads, &wfmap, &wfgrid));
   SPH_TRY(batch_map_items(b, [&](const Problem& p) { return thread(p) && p.grid.stashCap ? p.candcap : (int64_t)0; },
                           256, &ctmap, &ctgrid));

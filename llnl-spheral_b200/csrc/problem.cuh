@@ -160,8 +160,8 @@ struct Problem {
   double* gpos = nullptr;   // [3][gcap] ghost positions during creation
 
   // cell list
-  double* cand = nullptr;       // cell order: [candcap] 64-byte records (FP64 x,y,z, index,
-                                // FP32 H) then [candcap] 48-byte FP64 H
+  double* cand = nullptr;       // cell order, CAND_DOUBLES per slot: exact records (FP64
+                                // x,y,z, index), FP64 H, FP32 pre-test records, FP32 max eig(H)
   int32_t* cidx = nullptr;      // [candcap] cell index of each node (unsorted)
   int32_t* sortedIdx = nullptr; // [candcap]
   int64_t candcap = 0;
@@ -193,7 +193,7 @@ struct Problem {
   double* d_red = nullptr;      // reduction partials
   int64_t redcap = 0;
   double* staging = nullptr;    // host<->device AoS staging, 9*n doubles
-  double* hmaxi = nullptr;      // [n] 1/min(eig(H)) of each internal node, per build
+  double* hmaxi = nullptr;      // [2][n] 1/min(eig(H)), max(eig(H)) of each internal node, per build
   double* pinned = nullptr;     // pinned host staging for get/set
   int64_t pinnedcap = 0;
 
@@ -233,6 +233,11 @@ enum NbrSchedule {
 // first[nmem] the grid size.  A single problem is a batch of one member.
 
 // Slots of a member's small device scalar array (64-bit words).
+// Doubles per slot of the cell-ordered candidate arrays (Problem::cand):
+// 32-byte exact record + 48-byte FP64 H + 16-byte pre-test record + 4-byte
+// FP32 max eig(H), rounded up.
+constexpr int CAND_DOUBLES = 13;
+
 enum ScalSlot {
   SC_HMAX = 0,         // ghost hmax of the current boundary (double bits)
   SC_BOUNDS = 1,       // 7 ordered-bit words: lo[3], hi[3], max h
@@ -245,7 +250,7 @@ enum ScalSlot {
   SC_DTOUT = 14,       // sphgpu_dt result
   SC_TOTAL = 15,       // total of the last prefix sum (i64)
   SC_CONS = 16,        // 8 conservation sums
-  SC_MAXCOND = 24,     // largest condition number of H over the internal nodes (double bits)
+  SC_LMAXALL = 24,     // largest eigenvalue of H over the internal nodes (double bits)
   // sizes of the current connectivity, produced and read on the device (i64)
   SC_NTOT = 25,        // internal nodes + ghosts made so far (ghost passes)
   SC_G = 26,           // ghosts
