@@ -244,23 +244,6 @@ int batch_check_errors(Batch& b, const char* where) {
   return rc;
 }
 
-__global__ void __launch_bounds__(256) copy_state_kernel(const Member* mem, BlockMap bm, int toStart) {
-  const MemberBlock mb = memberBlock(bm);
-  const Member& M = mem[mb.m];
-  const int64_t k = mb.block*blockDim.x + threadIdx.x;
-  if (k >= NSTATE*M.n) return;
-  if (toStart) M.S0[k] = M.S[k];
-  else M.S[k] = M.S0[k];
-}
-
-int copy_state(Batch& b, bool toStart) {
-  BlockMap bm;
-  unsigned grid = 0;
-  SPH_TRY(batch_map_items(b, [](const Problem& p) { return (int64_t)NSTATE*p.n; }, 256, &bm, &grid));
-  if (grid) { copy_state_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm, toStart ? 1 : 0); batch_count_launch(b); }
-  return cuda_status(cudaGetLastError(), "state copy");
-}
-
 int set_state_impl(Problem& p, const double* pos, const double* vel, const double* mass, const double* rho,
                    const double* eps, const double* H, bool device) {
   SPH_TRY(upload_aos(p, pos, 3, S_X, device));
@@ -335,6 +318,7 @@ int finalize_impl(Batch& b) {
     SPH_TRY(launch_crk_sum_density(b));
   }
   SPH_TRY(launch_sum_density(b));
+  if (anyMember(b, isMixedSph)) SPH_TRY(launch_sum_density_mixed(b));
   return SPHGPU_OK;
 }
 
@@ -368,17 +352,17 @@ int step_after_connectivity(Batch& b) {
   // selectDt with the previous derivatives, state at the step start
   // (reads the state and derivatives directly: no records needed yet).
   SPH_TRY(launch_select_dt(b));
-  SPH_TRY(copy_state(b, true));                  // state0
-  // trial advance to the mid point (updateAsIncrement for every policy)
-  SPH_TRY(launch_update(b, 0.5, true));
+  // state0 = state; trial advance to the mid point (updateAsIncrement for
+  // every policy), one kernel
+  SPH_TRY(launch_update(b, 0.5, true, 1));
   SPH_TRY(pack_records(b, PACK_FOR_EVAL));
   // initializeDerivatives + derivs.Zero + evaluateDerivatives at the mid point
   SPH_TRY(initialize_impl(b));
   SPH_TRY(launch_eval(b));
-  // full step from state0 with the mid-point derivatives
-  SPH_TRY(copy_state(b, false));
+  // full step from state0 with the mid-point derivatives (the restore of
+  // state0 is folded into the compatible-energy and update kernels)
   SPH_TRY(launch_compatible_energy(b, 1.0));
-  SPH_TRY(launch_update(b, 1.0, false));
+  SPH_TRY(launch_update(b, 1.0, false, 2));
   // applyGhostBoundaries; postStepFinalize (sum density); enforceBoundaries
   SPH_TRY(pack_records(b, PACK_FOR_FINALIZE));
   SPH_TRY(finalize_impl(b));

@@ -382,8 +382,10 @@ int pack_records(Batch& b, int need = PACK_ALL);
 int launch_gradh(Batch& b);
 int launch_eval_sph_fp64(Batch& b);
 int launch_eval_sph_mixed(Batch& b);
-int launch_sum_density(Batch& b);
-int launch_update(Batch& b, double scale, bool timeAdvanceOnly);
+int launch_sum_density(Batch& b);          // plain FP64 SPH members
+int launch_sum_density_mixed(Batch& b);    // mixed-precision SPH members (sph_mixed.cu)
+// mode: 0 in place, 1 save state0 first (mid point), 2 from state0 (full step)
+int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode);
 int launch_compatible_energy(Batch& b, double scale);
 int launch_enforce_boundaries(Batch& b);
 int launch_eos(Batch& b);

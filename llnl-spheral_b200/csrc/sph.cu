@@ -362,6 +362,9 @@ __global__ void __launch_bounds__(128) sum_density_kernel(const Member* mem, Blo
 }
 
 // ---------------------------------------------------------------- compatible energy
+// Runs in the full step after the mid-point evaluation, where the reference
+// first restores state0: it reads the start-of-step state S0 and writes the
+// new specific thermal energy to S.
 __global__ void __launch_bounds__(128) compatible_energy_kernel(const Member* mem, BlockMap bm, double scale) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = mem[mb.m];
@@ -377,8 +380,9 @@ __global__ void __launch_bounds__(128) compatible_energy_kernel(const Member* me
   const double multiplier = scale*MB.scal[SC_DT];
   const double hdt = 0.5*multiplier;
   const double weighti = fabs(D[D_DEPSDT*n + i]) + kDblEps;
-  const double mi = S[S_M*n + i];
-  const V3 vi{S[S_VX*n + i], S[S_VY*n + i], S[S_VZ*n + i]};
+  const double* S0 = MB.S0;
+  const double mi = S0[S_M*n + i];
+  const V3 vi{S0[S_VX*n + i], S0[S_VY*n + i], S0[S_VZ*n + i]};
   const V3 ai{D[(D_DVDT + 0)*n + i], D[(D_DVDT + 1)*n + i], D[(D_DVDT + 2)*n + i]};
   const V3 vi12 = vadd(vi, vmul(ai, hdt));
   double DepsDti = 0.0;
@@ -387,8 +391,8 @@ __global__ void __launch_bounds__(128) compatible_energy_kernel(const Member* me
     const int32_t j = __ldg(nbr + k);
     const int64_t r = j < n ? (int64_t)j : (int64_t)__ldg(groot + (j - n));
     const double weightj = fabs(ldg(D + D_DEPSDT*n + r)) + kDblEps;
-    const double mj = ldg(S + S_M*n + r);
-    const V3 vj{ldg(S + S_VX*n + r), ldg(S + S_VY*n + r), ldg(S + S_VZ*n + r)};
+    const double mj = ldg(S0 + S_M*n + r);
+    const V3 vj{ldg(S0 + S_VX*n + r), ldg(S0 + S_VY*n + r), ldg(S0 + S_VZ*n + r)};
     const V3 aj{ldg(D + (D_DVDT + 0)*n + r), ldg(D + (D_DVDT + 1)*n + r), ldg(D + (D_DVDT + 2)*n + r)};
     const V3 vj12 = vadd(vj, vmul(aj, hdt));
     const V3 pa{ldg(pacc + k), ldg(pacc + ecap + k), ldg(pacc + 2*ecap + k)};   // owner's pair acceleration
@@ -402,7 +406,7 @@ __global__ void __launch_bounds__(128) compatible_energy_kernel(const Member* me
       DepsDti += (1.0 - wj)*duji*mj/mi;
     }
   }
-  S[S_EPS*n + i] += DepsDti*multiplier;
+  S[S_EPS*n + i] = S0[S_EPS*n + i] + DepsDti*multiplier;
 }
 
 // ---------------------------------------------------------------- policies
@@ -411,8 +415,17 @@ __device__ __forceinline__ bool hInsideBounds(const Sym& H, double hmin, double 
   return vmin(ev) > 1.0/hmax && vmax(ev) < 1.0/hmin;
 }
 
+// State::update of every policy, f = f_src + scale*dt*df, into S.
+// UPDATE_IN_PLACE: the source is S.  UPDATE_SAVE_START: the source is S and
+// every state field is first copied to S0 (state0 = state.copyState()).
+// UPDATE_FROM_START: the source is S0 (state.assign(state0) fused into the
+// update); the fields no policy updates are copied from S0, and with
+// compatible energy the specific thermal energy already written to S by
+// compatible_energy_kernel is kept.
+enum UpdateMode { UPDATE_IN_PLACE = 0, UPDATE_SAVE_START = 1, UPDATE_FROM_START = 2 };
+
 __global__ void __launch_bounds__(256) update_kernel(const Member* mem, BlockMap bm, double scale,
-                                                     int timeAdvanceOnly) {
+                                                     int timeAdvanceOnly, int mode) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = mem[mb.m];
   const int64_t n = MB.n;
@@ -420,12 +433,20 @@ __global__ void __launch_bounds__(256) update_kernel(const Member* mem, BlockMap
   if (i >= n) return;
   const Params& P = MB.prm;
   double* S = MB.S;
+  const double* Src = mode == UPDATE_FROM_START ? MB.S0 : MB.S;
   const double* D = MB.D;
+  if (mode == UPDATE_SAVE_START) {
+    for (int f = 0; f < NSTATE; ++f) MB.S0[f*n + i] = S[f*n + i];
+  } else if (mode == UPDATE_FROM_START) {
+    S[S_M*n + i] = Src[S_M*n + i];
+    S[S_OMEGA*n + i] = Src[S_OMEGA*n + i];
+    if (P.hydro != SPHGPU_HYDRO_CRKSPH) S[S_VOL*n + i] = Src[S_VOL*n + i];
+  }
   const int epsDone = (!timeAdvanceOnly && P.compatible) ? 1 : 0;
   const double mult = scale*MB.scal[SC_DT];
   // H: IncrementBoundedState (half step / IntegrateH) or ReplaceBoundedState (IdealH)
-  Sym H{S[(S_H + 0)*n + i], S[(S_H + 1)*n + i], S[(S_H + 2)*n + i],
-        S[(S_H + 3)*n + i], S[(S_H + 4)*n + i], S[(S_H + 5)*n + i]};
+  Sym H{Src[(S_H + 0)*n + i], Src[(S_H + 1)*n + i], Src[(S_H + 2)*n + i],
+        Src[(S_H + 3)*n + i], Src[(S_H + 4)*n + i], Src[(S_H + 5)*n + i]};
   Sym Hn;
   if (timeAdvanceOnly || P.HUpdate == SPHGPU_H_INTEGRATE) {
     const Sym dH{D[(D_DHDT + 0)*n + i], D[(D_DHDT + 1)*n + i], D[(D_DHDT + 2)*n + i],
@@ -439,30 +460,32 @@ __global__ void __launch_bounds__(256) update_kernel(const Member* mem, BlockMap
   S[(S_H + 0)*n + i] = Hn.xx; S[(S_H + 1)*n + i] = Hn.xy; S[(S_H + 2)*n + i] = Hn.xz;
   S[(S_H + 3)*n + i] = Hn.yy; S[(S_H + 4)*n + i] = Hn.yz; S[(S_H + 5)*n + i] = Hn.zz;
   // mass density: IncrementBoundedState
-  const double rho = dmin(P.rhoMax, dmax(P.rhoMin, S[S_RHO*n + i] + mult*(D[D_DRHODT*n + i])));
+  const double rho = dmin(P.rhoMax, dmax(P.rhoMin, Src[S_RHO*n + i] + mult*(D[D_DRHODT*n + i])));
   S[S_RHO*n + i] = rho;
   // position: IncrementFieldList
-  for (int c = 0; c < 3; ++c) S[(S_X + c)*n + i] = S[(S_X + c)*n + i] + D[(D_DXDT + c)*n + i]*mult;
+  for (int c = 0; c < 3; ++c) S[(S_X + c)*n + i] = Src[(S_X + c)*n + i] + D[(D_DXDT + c)*n + i]*mult;
   // CRKSPH node volume: ContinuityVolumePolicy (after mass density and H)
   if (P.hydro == SPHGPU_HYDRO_CRKSPH) {
-    const double m = S[S_M*n + i];
+    const double m = Src[S_M*n + i];
     const double volMin = 0.5*m*safeInvVar(rho);
     const double volMax = 4.0*3.14159265358979323846/(3.0*sdet(Hn));
     const double dVdt = -m*safeInvVar(rho*rho)*D[D_DRHODT*n + i];
-    S[S_VOL*n + i] = dmax(volMin, dmin(volMax, S[S_VOL*n + i] + mult*dVdt));
+    S[S_VOL*n + i] = dmax(volMin, dmin(volMax, Src[S_VOL*n + i] + mult*dVdt));
   }
   // specific thermal energy: IncrementFieldList (or the compatible policy, already applied)
-  double eps = S[S_EPS*n + i];
+  double eps;
   if (!epsDone) {
-    eps = eps + mult*(D[D_DEPSDT*n + i]);
+    eps = Src[S_EPS*n + i] + mult*(D[D_DEPSDT*n + i]);
     S[S_EPS*n + i] = eps;
+  } else {
+    eps = S[S_EPS*n + i];
   }
   // pressure, sound speed (GammaLawGas, no active pressure limits)
   const double g1 = P.gamma - 1.0;
   S[S_P*n + i] = g1*rho*eps;
   S[S_CS*n + i] = sqrt(dmax(0.0, P.gamma*g1*eps));
   // velocity: IncrementFieldList (after the energy it depends on)
-  for (int c = 0; c < 3; ++c) S[(S_VX + c)*n + i] = S[(S_VX + c)*n + i] + D[(D_DVDT + c)*n + i]*mult;
+  for (int c = 0; c < 3; ++c) S[(S_VX + c)*n + i] = Src[(S_VX + c)*n + i] + D[(D_DVDT + c)*n + i]*mult;
 }
 
 __global__ void __launch_bounds__(256) eos_kernel(const Member* mem, BlockMap bm) {
@@ -640,8 +663,9 @@ int pack_records(Batch& b, int need) {
     const bool crk = p.prm.hydro == SPHGPU_HYDRO_CRKSPH;
     if (need == PACK_FOR_EVAL)       // grad-h, the FP64 pair loop, the CRKSPH moments
       return crk || p.prm.gradh || p.cfg.precision == SPHGPU_PRECISION_FP64;
-    if (need == PACK_FOR_FINALIZE)   // the summed density, the CRKSPH volumes
-      return crk || p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM;
+    if (need == PACK_FOR_FINALIZE)   // the FP64 summed density, the CRKSPH volumes
+      return crk || (p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM &&
+                     p.cfg.precision == SPHGPU_PRECISION_FP64);
     return true;
   };
   BlockMap bm;
@@ -699,7 +723,7 @@ int launch_sum_density(Batch& b) {
   BlockMap bm;
   unsigned grid = 0;
   SPH_TRY(batch_map_items(b, [](const Problem& p) {
-    return isSph(p) && p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM ? p.n : (int64_t)0; }, 128, &bm, &grid));
+    return isFp64Sph(p) && p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM ? p.n : (int64_t)0; }, 128, &bm, &grid));
   if (grid) { sum_density_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
   return cuda_status(cudaGetLastError(), "sum density");
 }
@@ -712,12 +736,12 @@ int launch_compatible_energy(Batch& b, double scale) {
   return cuda_status(cudaGetLastError(), "compatible energy");
 }
 
-int launch_update(Batch& b, double scale, bool timeAdvanceOnly) {
+int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode) {
   BlockMap bm;
   unsigned grid = 0;
   SPH_TRY(map_nodes(b, 256, &bm, &grid));
   if (grid) {
-    update_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm, scale, timeAdvanceOnly ? 1 : 0);
+    update_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm, scale, timeAdvanceOnly ? 1 : 0, mode);
     batch_count_launch(b);
   }
   return cuda_status(cudaGetLastError(), "update");

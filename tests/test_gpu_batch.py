@@ -165,6 +165,25 @@ def test_graph_replayed_steps_match_eager(gpu_lib, pkg):
         assert np.array_equal(a.field(k), g.field(k)), k
 
 
+def test_batch_of_mixed_sph_and_mixed_crk_members(gpu_lib, pkg):
+    """Mixed-form SPH and CRKSPH members in one batch keep their own record
+    layouts and kernels: each equals its solo run bit for bit."""
+    abi = pkg.abi
+    specs = [_sod_member(pkg, 48, 1.4, 3.0, abi.PRECISION_MIXED, 21),
+             _kh_member(pkg, abi.PRECISION_MIXED, hydro=abi.HYDRO_CRKSPH),
+             _kh_member(pkg, abi.PRECISION_MIXED),
+             _sod_member(pkg, 40, 5.0 / 3.0, 2.0, abi.PRECISION_FP64, 22)]
+    solo = [pkg.SPHHydro(cfg, ns) for ns, cfg in specs]
+    mem = [pkg.SPHHydro(cfg, ns) for ns, cfg in specs]
+    for s in solo:
+        s.step(3)
+    batch = pkg.SPHBatch(mem)
+    batch.step(3)
+    for s, m in zip(solo, mem):
+        for k in STATE_KEYS:
+            assert np.array_equal(s.field(k), m.field(k)), k
+
+
 def test_batch_rejects_duplicates(gpu_lib, pkg):
     ns, cfg = _sod_member(pkg, 32, 5.0 / 3.0, 4.0, pkg.abi.PRECISION_FP64, 5)
     a = pkg.SPHHydro(cfg, ns)

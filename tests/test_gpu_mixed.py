@@ -66,3 +66,30 @@ def test_mixed_energy_drift_200_steps(gpu_lib, pkg):
     m.step(200)
     e1 = m.conservation()[6]
     assert abs(e1 - e0) / abs(e0) <= 1e-6
+
+
+@pytest.mark.parametrize("which", ["sod", "kh"])
+def test_mixed_summed_density_and_states_after_steps(gpu_lib, pkg, which):
+    """The mixed form also sums the density (RigorousSumDensity) with FP32
+    pair terms and a Kahan sum: after a few RK2 steps the states stay within
+    1e-5 of the FP64 path, and finalize() alone gives the density within it."""
+    gen, abi = pkg.generators, pkg.abi
+    if which == "sod":
+        box = ((0.0, 0.0, 0.0), (1.0, 0.125, 0.125))
+        ns = gen.sod(nx=64, ny=8, nz=8, box=box)
+        cfg = gen.sod_config(abi, ns_box=box)
+    else:
+        ns = gen.kelvin_helmholtz(nx=32, ny=32, nz=16, box=((0, 0, 0), (1.0, 1.0, 0.5)))
+        cfg = gen.kh_config(abi, xmax=(1.0, 1.0, 0.5))
+    cm = cfg.copy()
+    cm.precision = abi.PRECISION_MIXED
+    f = pkg.SPHHydro(cfg, ns)
+    m = pkg.SPHHydro(cm, ns)
+    for p in (f, m):
+        p.build_neighbors()
+        p.finalize()
+    assert normwise(m.field("mass density"), f.field("mass density")) <= 1e-6
+    for p in (f, m):
+        p.step(5)
+    for k in ("mass density", "position", "velocity", "specific thermal energy", "H"):
+        assert normwise(m.field(k), f.field(k)) <= 1e-5, k
