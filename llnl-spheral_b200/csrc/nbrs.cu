@@ -91,29 +91,68 @@ __global__ void build_init_kernel(const Member* mem, int nmem) {
   setScalI(s, SC_G, 0);
   s[SC_HMAX] = 0.0;
   s[SC_LMAXALL] = 0.0;
+  unsigned long long* bb = reinterpret_cast<unsigned long long*>(s + SC_BOUNDS);
+  for (int a = 0; a < 3; ++a) { bb[a] = ~0ULL; bb[3 + a] = 0ULL; }
+  bb[6] = 0ULL;
 }
 
 // 1/min(eig(H)) (hmaxi[i]) and max(eig(H)) (hmaxi[n + i]) of every internal
 // node, once per build (ghosts share their root's H, so every boundary pass,
-// the cell size and the pre-test records read them from here), and the
+// the cell size and the pre-test records read them from here); the bounding
+// box of the internal nodes and the largest 1/min(eig(H)) (SC_BOUNDS); the
 // largest max(eig(H)) of the problem (with the largest 1/min(eig(H)) it
 // bounds the FP32 pre-test error).
 __global__ void __launch_bounds__(kGhostThreads) node_hmax_kernel(const Member* mem, BlockMap bm) {
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
   const int64_t i = mb.block*blockDim.x + threadIdx.x;
-  double lmax = 0.0;
+  double lmax = 0.0, h = 0.0;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
   if (i < M.n) {
     const V3 ev = eigenValues(nodeH(M, i));
-    M.hmaxi[i] = 1.0/vmin(ev);
+    h = 1.0/vmin(ev);
+    M.hmaxi[i] = h;
     lmax = vmax(ev);
     M.hmaxi[M.n + i] = lmax;
     if (!(lmax < 1.0e300)) lmax = 1.0e300;     // degenerate H: no FP32 pre-test
+    const V3 r = nodePos(M, i);
+    lo[0] = r.x; lo[1] = r.y; lo[2] = r.z;
+    hi[0] = r.x; hi[1] = r.y; hi[2] = r.z;
   }
-  for (int o = 16; o > 0; o >>= 1) lmax = dmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-  if ((threadIdx.x & 31) == 0 && lmax > 0.0)
-    atomicMax(reinterpret_cast<unsigned long long*>(M.scal + SC_LMAXALL),
-              (unsigned long long)__double_as_longlong(lmax));
+  for (int o = 16; o > 0; o >>= 1) {
+    lmax = dmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    h = fmax(h, __shfl_xor_sync(0xffffffffu, h, o));
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+      hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+    }
+  }
+  __shared__ double sh[kGhostThreads/32][8];
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    for (int a = 0; a < 3; ++a) { sh[w][a] = lo[a]; sh[w][3 + a] = hi[a]; }
+    sh[w][6] = h;
+    sh[w][7] = lmax;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int ww = 1; ww < (int)(blockDim.x >> 5); ++ww) {
+      for (int a = 0; a < 3; ++a) { lo[a] = fmin(lo[a], sh[ww][a]); hi[a] = fmax(hi[a], sh[ww][3 + a]); }
+      h = fmax(h, sh[ww][6]);
+      lmax = dmax(lmax, sh[ww][7]);
+    }
+    unsigned long long* out = reinterpret_cast<unsigned long long*>(M.scal + SC_BOUNDS);
+    if (h > 0.0) {
+      for (int a = 0; a < 3; ++a) {
+        atomicMin(out + a, orderedBits(lo[a]));
+        atomicMax(out + 3 + a, orderedBits(hi[a]));
+      }
+      atomicMax(out + 6, orderedBits(h));
+    }
+    if (lmax > 0.0)
+      atomicMax(reinterpret_cast<unsigned long long*>(M.scal + SC_LMAXALL),
+                (unsigned long long)__double_as_longlong(lmax));
+  }
 }
 
 __device__ __forceinline__ double nodeHmax(const Member& M, int64_t k) {
@@ -194,54 +233,6 @@ __global__ void ghost_advance_kernel(const Member* mem, int nmem) {
 }
 
 // ---------------------------------------------------------------- cells
-__global__ void bounds_init_kernel(const Member* mem, int nmem) {
-  const int m = blockIdx.x*blockDim.x + threadIdx.x;
-  if (m >= nmem) return;
-  unsigned long long* bb = reinterpret_cast<unsigned long long*>(mem[m].scal + SC_BOUNDS);
-  for (int a = 0; a < 3; ++a) { bb[a] = ~0ULL; bb[3 + a] = 0ULL; }
-  bb[6] = 0ULL;
-}
-
-// Bounding box of all nodes and max of 1/min(eig(H)) (cell size).
-__global__ void __launch_bounds__(kGhostThreads) node_bounds_kernel(const Member* mem, BlockMap bm) {
-  const MemberBlock mb = memberBlock(bm);
-  const Member& M = mem[mb.m];
-  const int64_t k = mb.block*blockDim.x + threadIdx.x;
-  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300}, h = 0.0;
-  if (k < allNodes(M)) {
-    const V3 r = nodePos(M, k);
-    lo[0] = r.x; lo[1] = r.y; lo[2] = r.z;
-    hi[0] = r.x; hi[1] = r.y; hi[2] = r.z;
-    if (k < M.n) h = M.hmaxi[k];
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    for (int a = 0; a < 3; ++a) {
-      lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
-      hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
-    }
-    h = fmax(h, __shfl_xor_sync(0xffffffffu, h, o));
-  }
-  __shared__ double sh[kGhostThreads/32][7];
-  const int w = threadIdx.x >> 5;
-  if ((threadIdx.x & 31) == 0) {
-    for (int a = 0; a < 3; ++a) { sh[w][a] = lo[a]; sh[w][3 + a] = hi[a]; }
-    sh[w][6] = h;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int ww = 1; ww < (int)(blockDim.x >> 5); ++ww) {
-      for (int a = 0; a < 3; ++a) { lo[a] = fmin(lo[a], sh[ww][a]); hi[a] = fmax(hi[a], sh[ww][3 + a]); }
-      h = fmax(h, sh[ww][6]);
-    }
-    unsigned long long* out = reinterpret_cast<unsigned long long*>(M.scal + SC_BOUNDS);
-    for (int a = 0; a < 3; ++a) {
-      atomicMin(out + a, orderedBits(lo[a]));
-      atomicMax(out + 3 + a, orderedBits(hi[a]));
-    }
-    atomicMax(out + 6, orderedBits(h));
-  }
-}
-
 // Uniform grid of cells of edge >= kappa*max(1/lambda_min(H)) (the margin
 // covers the libm difference of the eigenvalue solve for anisotropic H),
 // enlarged until the cells fit the cell buffers (larger cells only widen the
@@ -255,6 +246,16 @@ __global__ void grid_kernel(const Member* mem, int nmem) {
   double lo[3], hi[3];
   for (int a = 0; a < 3; ++a) { lo[a] = fromOrderedBits(bb[a]); hi[a] = fromOrderedBits(bb[3 + a]); }
   const double hmaxAll = fromOrderedBits(bb[6]);
+  // ghosts lie within kappa*hmax (<= kappa*hmaxAll) beyond the periodic
+  // planes; elsewhere they share their root's coordinates
+  const double reach = M.prm.kernelExtent*hmaxAll*1.001 + 1.0e-300;
+  for (int a = 0; a < 3; ++a) {
+    if (!M.prm.bcs.periodic[a]) continue;
+    const PlanarBC& bc = M.prm.bcs.bc[2*a];
+    const double p0 = (&bc.enter.point.x)[a], p1 = (&bc.exit.point.x)[a];
+    lo[a] = fmin(lo[a], fmin(p0, p1) - reach);
+    hi[a] = fmax(hi[a], fmax(p0, p1) + reach);
+  }
   double cell = M.prm.kernelExtent*hmaxAll*1.001;
   if (!(cell > 0.0) || !(cell < 1.0e300)) {
     atomicOr(M.err, DERR_NONPOSITIVE);
@@ -313,17 +314,14 @@ __global__ void __launch_bounds__(kGhostThreads) cell_index_kernel(const Member*
 }
 
 // Cell-ordered candidate arrays (Problem::cand), one slot per node:
-//   exact   [candcap] 32 bytes: FP64 position, node index
-//   H       [candcap] 48 bytes: FP64 H
 //   pre     [candcap] float4:   FP32 offsets of the position from the lower
 //                               corner of the node's cell, FP32 min eig(H)
 //   lmax    [candcap] float:    FP32 max eig(H)
-// The walks read only `pre` for most candidates; `exact` and `H` are read
-// for the candidates the FP32 pre-test cannot decide, `lmax` when the i-side
-// test alone does not.
+// and sortedIdx[slot], the node of each slot.  The walks read only `pre` for
+// most candidates; `lmax` when the i-side test alone does not decide, and
+// the FP64 position and H of the node (state, ghost positions) for the
+// candidates the FP32 pre-test cannot decide.
 struct NbrArrays {
-  const double* exact;
-  const double* H;
   const float4* pre;
   const float* lmax;
 };
@@ -331,24 +329,9 @@ struct NbrArrays {
 __device__ __forceinline__ NbrArrays nbrArrays(const Member& M) {
   const double* c = static_cast<const double*>(M.cand);
   NbrArrays a;
-  a.exact = c;
-  a.H = c + 4*M.candcap;
-  a.pre = reinterpret_cast<const float4*>(c + 10*M.candcap);
-  a.lmax = reinterpret_cast<const float*>(c + 12*M.candcap);
+  a.pre = reinterpret_cast<const float4*>(c);
+  a.lmax = reinterpret_cast<const float*>(c + 2*M.candcap);
   return a;
-}
-
-__device__ __forceinline__ V3 candPos(const NbrArrays& a, int64_t k, int32_t* idx) {
-  const double2* q = reinterpret_cast<const double2*>(a.exact + 4*k);
-  const double2 u = __ldg(q), v = __ldg(q + 1);
-  if (idx) *idx = (int32_t)(uint32_t)((uint64_t)__double_as_longlong(v.y) & 0xffffffffu);
-  return V3{u.x, u.y, v.x};
-}
-
-__device__ __forceinline__ Sym candH(const NbrArrays& a, int64_t k) {
-  const double2* q = reinterpret_cast<const double2*>(a.H + 6*k);
-  const double2 u = __ldg(q), v = __ldg(q + 1), w = __ldg(q + 2);
-  return Sym{u.x, u.y, v.x, v.y, w.x, w.y};
 }
 
 __device__ __forceinline__ float symEta2F(const float* h, float x, float y, float z) {
@@ -358,8 +341,8 @@ __device__ __forceinline__ float symEta2F(const float* h, float x, float y, floa
   return __fmaf_rn(ex, ex, __fmaf_rn(ey, ey, ez*ez));
 }
 
-// The walking node: FP32 H and cell offsets for the pre-test, its cell and
-// its sorted slot (the exact test re-reads its FP64 position and H there).
+// The walking node: FP32 H and cell offsets for the pre-test, its cell, its
+// sorted slot and node index (the exact test re-reads its FP64 state).
 struct Walker {
   float hf[6];
   float ox, oy, oz;
@@ -368,11 +351,14 @@ struct Walker {
   int32_t idx;
 };
 
-__device__ __forceinline__ Walker makeWalker(const NbrArrays& a, const Grid& g, int64_t s) {
+// Walker of sorted slot s; idx >= n marks a ghost slot (no walk).
+__device__ __forceinline__ Walker makeWalker(const Member& M, const NbrArrays& a, const Grid& g, int64_t s) {
   Walker w;
   w.slot = s;
-  const V3 r = candPos(a, s, &w.idx);
-  const Sym H = candH(a, s);
+  w.idx = __ldg(M.sortedIdx + s);
+  if (w.idx >= M.n) return w;
+  const V3 r = nodePos(M, w.idx);
+  const Sym H = nodeH(M, w.idx);
   w.hf[0] = (float)H.xx; w.hf[1] = (float)H.xy; w.hf[2] = (float)H.xz;
   w.hf[3] = (float)H.yy; w.hf[4] = (float)H.yz; w.hf[5] = (float)H.zz;
   const float4 p = __ldg(a.pre + s);
@@ -408,6 +394,19 @@ __device__ __forceinline__ Row loadRow(const int64_t* cellStart, const Grid& g, 
   return row;
 }
 
+// The exact FP64 predicate for nodes i and j (the walks reach it for the
+// few candidates the pre-test leaves undecided).
+__device__ __forceinline__ bool exactTest(const Member& M, int32_t i, int32_t j, double k2) {
+  const int64_t n = M.n;
+  const double* S = M.S;
+  const V3 ri{S[S_X*n + i], S[S_Y*n + i], S[S_Z*n + i]};     // the walker is an internal node
+  const V3 rj = nodePos(M, j);
+  const V3 rij{ri.x - rj.x, ri.y - rj.y, ri.z - rj.z};
+  const Sym Hi{S[(S_H + 0)*n + i], S[(S_H + 1)*n + i], S[(S_H + 2)*n + i],
+               S[(S_H + 3)*n + i], S[(S_H + 4)*n + i], S[(S_H + 5)*n + i]};
+  return mag2(sdot(Hi, rij)) <= k2 || mag2(sdot(nodeH(M, j), rij)) <= k2;
+}
+
 // ConnectivityMap predicate |H_i r_ij|^2 <= kappa^2 || |H_j r_ij|^2 <= kappa^2
 // (src/Neighbor/ConnectivityMapInline.hh:169-186) for candidate slot k.
 // With tol > 0 a FP32 pre-test decides every pair whose eta^2 lies clearly
@@ -417,8 +416,8 @@ __device__ __forceinline__ Row loadRow(const int64_t* cellStart, const Grid& g, 
 // tol (1e-3) is only set when that ratio is <= 100, so it never decides a
 // pair the exact test would decide otherwise.  Undecided pairs take the
 // exact FP64 test in the reference's operation order.
-__device__ __forceinline__ bool candTest(const NbrArrays& a, const Walker& w, const Row& row, int64_t k,
-                                         float cellf, double k2, float k2lo, float k2hi, bool pretest) {
+__device__ __forceinline__ bool candTest(const Member& M, const NbrArrays& a, const Walker& w, const Row& row,
+                                         int64_t k, float cellf, double k2, float k2lo, float k2hi, bool pretest) {
   if (pretest) {
     const float4 c = __ldg(a.pre + k);
     const float dxc = (float)(row.x0 - w.cx + (k >= row.e0) + (k >= row.e1))*cellf;
@@ -430,10 +429,7 @@ __device__ __forceinline__ bool candTest(const NbrArrays& a, const Walker& w, co
     const float lm = __ldg(a.lmax + k);
     if (lm*lm*r2 <= k2lo) return true;
   }
-  const V3 ri = candPos(a, w.slot, nullptr);
-  const V3 rj = candPos(a, k, nullptr);
-  const V3 rij{ri.x - rj.x, ri.y - rj.y, ri.z - rj.z};
-  return mag2(sdot(candH(a, w.slot), rij)) <= k2 || mag2(sdot(candH(a, k), rij)) <= k2;
+  return exactTest(M, w.idx, __ldg(M.sortedIdx + k), k2);
 }
 
 __global__ void __launch_bounds__(kGhostThreads) cell_scatter_kernel(const Member* mem, BlockMap bm) {
@@ -445,24 +441,16 @@ __global__ void __launch_bounds__(kGhostThreads) cell_scatter_kernel(const Membe
   const int64_t slot = M.cellStart[c] + atomicAdd(M.cellFill + c, 1);
   M.sortedIdx[slot] = (int32_t)k;
   const V3 r = nodePos(M, k);
-  const Sym H = nodeH(M, k);
   const Grid g = loadGrid(M);
   const int cx = cellCoord(r.x, g.lo[0], g.cell, g.dim[0]);
   const int cy = cellCoord(r.y, g.lo[1], g.cell, g.dim[1]);
   const int cz = cellCoord(r.z, g.lo[2], g.cell, g.dim[2]);
   const int64_t root = k < M.n ? k : M.groot[k - M.n];
   double* base = static_cast<double*>(M.cand);
-  double2* q = reinterpret_cast<double2*>(base + 4*slot);
-  q[0] = make_double2(r.x, r.y);
-  q[1] = make_double2(r.z, __longlong_as_double((long long)(uint64_t)(uint32_t)k));
-  double2* h = reinterpret_cast<double2*>(base + 4*M.candcap + 6*slot);
-  h[0] = make_double2(H.xx, H.xy);
-  h[1] = make_double2(H.xz, H.yy);
-  h[2] = make_double2(H.yz, H.zz);
-  float4* pre = reinterpret_cast<float4*>(base + 10*M.candcap);
+  float4* pre = reinterpret_cast<float4*>(base);
   pre[slot] = make_float4((float)(r.x - (g.lo[0] + cx*g.cell)), (float)(r.y - (g.lo[1] + cy*g.cell)),
                           (float)(r.z - (g.lo[2] + cz*g.cell)), (float)(1.0/M.hmaxi[root]));
-  float* lmax = reinterpret_cast<float*>(base + 12*M.candcap);
+  float* lmax = reinterpret_cast<float*>(base + 2*M.candcap);
   lmax[slot] = (float)M.hmaxi[M.n + root];
 }
 
@@ -492,7 +480,7 @@ __global__ void __launch_bounds__(256) nbr_thread_kernel(const Member* mem, Bloc
   bool active = s < allNodes(M);
   Walker me;
   if (active) {
-    me = makeWalker(a, g, s);
+    me = makeWalker(M, a, g, s);
     active = me.idx < n;
   }
   // list capacity: the shared-memory list (FILL) or the member's stash (COUNT)
@@ -514,7 +502,7 @@ __global__ void __launch_bounds__(256) nbr_thread_kernel(const Member* mem, Bloc
         if (y < 0 || y >= g.dim[1]) continue;
         const Row row = loadRow(M.cellStart, g, me, y, z, cellf);
         for (int64_t k = row.start; k < row.end; ++k) {
-          if (k != s && candTest(a, me, row, k, cellf, k2, k2lo, k2hi, pretest)) {
+          if (k != s && candTest(M, a, me, row, k, cellf, k2, k2lo, k2hi, pretest)) {
             if (collect) {
               const int32_t j = __ldg(M.sortedIdx + k);
               if (count < lcap) {
@@ -627,7 +615,7 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const Member* mem, BlockM
   if (s >= allNodes(M)) return;
   const NbrArrays a = nbrArrays(M);
   const Grid g = loadGrid(M);
-  const Walker me = makeWalker(a, g, s);
+  const Walker me = makeWalker(M, a, g, s);
   if (me.idx >= M.n) return;
   const int32_t i = me.idx;
   const double k2 = M.prm.kernelExtent*M.prm.kernelExtent;
@@ -646,7 +634,7 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const Member* mem, BlockM
       const Row row = loadRow(M.cellStart, g, me, y, z, cellf);
       for (int64_t base = row.start; base < row.end; base += 32) {
         const int64_t k = base + lane;
-        const bool pass = k < row.end && k != s && candTest(a, me, row, k, cellf, k2, k2lo, k2hi, pretest);
+        const bool pass = k < row.end && k != s && candTest(M, a, me, row, k, cellf, k2, k2lo, k2hi, pretest);
         const unsigned ballot = __ballot_sync(0xffffffffu, pass);
         if (collect && pass) {
           const int pos = count + __popc(ballot & ((1u << lane) - 1u));
@@ -824,8 +812,6 @@ int launch_build(Batch& b) {
     ghost_advance_kernel<<<(nm + 127)/128, 128, 0, st>>>(b.d_mem, nm); batch_count_launch(b);
   }
   // ---- cell grid and counting sort of all nodes by cell
-  bounds_init_kernel<<<(nm + 127)/128, 128, 0, st>>>(b.d_mem, nm); batch_count_launch(b);
-  node_bounds_kernel<<<capGrid, kGhostThreads, 0, st>>>(b.d_mem, cap); batch_count_launch(b);
   grid_kernel<<<(nm + 127)/128, 128, 0, st>>>(b.d_mem, nm); batch_count_launch(b);
   BlockMap cm;
   unsigned cgrid = 0;

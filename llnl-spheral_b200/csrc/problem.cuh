@@ -160,8 +160,8 @@ struct Problem {
   double* gpos = nullptr;   // [3][gcap] ghost positions during creation
 
   // cell list
-  double* cand = nullptr;       // cell order, CAND_DOUBLES per slot: exact records (FP64
-                                // x,y,z, index), FP64 H, FP32 pre-test records, FP32 max eig(H)
+  double* cand = nullptr;       // cell order, CAND_DOUBLES per slot: FP32 pre-test records
+                                // (cell offsets, min eig(H)), FP32 max eig(H)
   int32_t* cidx = nullptr;      // [candcap] cell index of each node (unsorted)
   int32_t* sortedIdx = nullptr; // [candcap]
   int64_t candcap = 0;
@@ -234,9 +234,8 @@ enum NbrSchedule {
 
 // Slots of a member's small device scalar array (64-bit words).
 // Doubles per slot of the cell-ordered candidate arrays (Problem::cand):
-// 32-byte exact record + 48-byte FP64 H + 16-byte pre-test record + 4-byte
-// FP32 max eig(H), rounded up.
-constexpr int CAND_DOUBLES = 13;
+// 16-byte pre-test record + 4-byte FP32 max eig(H), rounded up.
+constexpr int CAND_DOUBLES = 3;
 
 enum ScalSlot {
   SC_HMAX = 0,         // ghost hmax of the current boundary (double bits)
