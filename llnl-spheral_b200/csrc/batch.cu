@@ -17,6 +17,7 @@ namespace {
 constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = 4;
 constexpr int SCAN_TILE = SCAN_THREADS*SCAN_ITEMS;
+
 constexpr int64_t kMapRing = 1 << 20;
 
 Member member_of(const Problem& p) {
@@ -57,9 +58,23 @@ __global__ void set_scal_kernel(const Member* mem, int nmem, int slot, double v)
 __device__ __forceinline__ void scanIO(const Member& M, int which, const int32_t*& in, int64_t& n,
                                        int64_t*& out) {
   // lengths from the device-side sizes of the build in progress
-  if (which == SCAN_FLAGS) { in = M.counts; n = scalI(M.scal, SC_NTOT); out = M.offsets; }
+  if (which == SCAN_FLAGS) {
+    // a boundary pass: the near-plane internal nodes, then the ghosts so far
+    in = M.counts; n = scalI(M.scal, SC_NNEAR) + scalI(M.scal, SC_NTOT) - M.n; out = M.offsets;
+  }
   else if (which == SCAN_CELLS) { in = M.cellFill; n = scalI(M.scal, SC_NCELLS); out = M.cellStart; }
   else { in = M.counts; n = M.n; out = M.offsets; }
+}
+
+// Upper bound of a scan's length (host and device).
+__host__ __device__ __forceinline__ int64_t scanCapacity(int64_t n, int64_t candcap, int64_t cellcap, int which) {
+  return which == SCAN_FLAGS ? candcap : (which == SCAN_CELLS ? cellcap : n);
+}
+
+// Blocks of a member's scan: one per tile up to kScanBlocks.
+__host__ __device__ __forceinline__ int scanBlocks(int64_t cap) {
+  const int64_t t = (cap + SCAN_TILE - 1)/SCAN_TILE;
+  return (int)(t < 1 ? 1 : (t > kScanBlocks ? kScanBlocks : t));
 }
 
 __device__ __forceinline__ int64_t warp_incl_scan(int64_t v) {
@@ -90,37 +105,47 @@ __device__ __forceinline__ int64_t block_excl_scan(int64_t v, int64_t* total) {
   return before;
 }
 
-// Pass 1: the sum of each tile of SCAN_TILE counts.
+// Tile range [t0, t1) of block `blk` of `nblk` over a scan of length n.
+__device__ __forceinline__ void blockTiles(int64_t n, int blk, int nblk, int64_t& t0, int64_t& t1) {
+  const int64_t tiles = (n + SCAN_TILE - 1)/SCAN_TILE;
+  const int64_t per = (tiles + nblk - 1)/nblk;
+  t0 = (int64_t)blk*per;
+  t1 = t0 + per < tiles ? t0 + per : tiles;
+}
+
+// Pass 1: the sum of each block's run of tiles.
 __global__ void __launch_bounds__(SCAN_THREADS) scan_tile_sums_kernel(const Member* mem, BlockMap bm, int which) {
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
   const int32_t* in; int64_t n; int64_t* out;
   scanIO(M, which, in, n, out);
-  const int64_t base = mb.block*SCAN_TILE;
+  int64_t t0, t1;
+  blockTiles(n, (int)mb.block, mb.blocks, t0, t1);
   int64_t s = 0;
-  for (int k = 0; k < SCAN_ITEMS; ++k) {
-    const int64_t idx = base + (int64_t)threadIdx.x*SCAN_ITEMS + k;
-    if (idx < n) s += in[idx];
+  for (int64_t t = t0; t < t1; ++t) {
+    const int64_t base = t*SCAN_TILE + (int64_t)threadIdx.x*SCAN_ITEMS;
+    for (int k = 0; k < SCAN_ITEMS; ++k)
+      if (base + k < n) s += in[base + k];
   }
   int64_t total;
   block_excl_scan(s, &total);
   if (threadIdx.x == 0) M.blockSums[mb.block] = total;
 }
 
-// Pass 2: one block per member scans its tile sums; writes out[n] and the total.
+// Pass 2: one block per member scans its block sums; writes out[n] and the total.
 __global__ void __launch_bounds__(SCAN_THREADS) scan_sums_kernel(const Member* mem, BlockMap bm, int which) {
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
   const int32_t* in; int64_t n; int64_t* out;
   scanIO(M, which, in, n, out);
-  const int64_t ntiles = (n + SCAN_TILE - 1)/SCAN_TILE;
+  const int nblk = scanBlocks(scanCapacity(M.n, M.candcap, M.cellcap, which));
   int64_t carry = 0;
-  for (int64_t base = 0; base < ntiles; base += SCAN_THREADS) {
-    const int64_t idx = base + threadIdx.x;
-    const int64_t v = idx < ntiles ? M.blockSums[idx] : 0;
+  for (int base = 0; base < nblk; base += SCAN_THREADS) {
+    const int idx = base + threadIdx.x;
+    const int64_t v = idx < nblk ? M.blockSums[idx] : 0;
     int64_t total;
     const int64_t ex = block_excl_scan(v, &total);
-    if (idx < ntiles) M.blockSums[idx] = carry + ex;
+    if (idx < nblk) M.blockSums[idx] = carry + ex;
     carry += total;
   }
   if (threadIdx.x == 0) {
@@ -129,33 +154,35 @@ __global__ void __launch_bounds__(SCAN_THREADS) scan_sums_kernel(const Member* m
   }
 }
 
-// Pass 3: block-local exclusive scan plus the tile's offset.
+// Pass 3: each block rescans its run of tiles from its block's offset.
 __global__ void __launch_bounds__(SCAN_THREADS) scan_apply_kernel(const Member* mem, BlockMap bm, int which) {
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
   const int32_t* in; int64_t n; int64_t* out;
   scanIO(M, which, in, n, out);
-  const int64_t base = mb.block*SCAN_TILE;
-  int32_t v[SCAN_ITEMS];
-  int64_t s = 0;
-  for (int k = 0; k < SCAN_ITEMS; ++k) {
-    const int64_t idx = base + (int64_t)threadIdx.x*SCAN_ITEMS + k;
-    v[k] = idx < n ? in[idx] : 0;
-    s += v[k];
-  }
-  int64_t total;
-  int64_t run = block_excl_scan(s, &total) + M.blockSums[mb.block];
-  for (int k = 0; k < SCAN_ITEMS; ++k) {
-    const int64_t idx = base + (int64_t)threadIdx.x*SCAN_ITEMS + k;
-    if (idx < n) out[idx] = run;
-    run += v[k];
+  int64_t t0, t1;
+  blockTiles(n, (int)mb.block, mb.blocks, t0, t1);
+  int64_t carry = M.blockSums[mb.block];
+  for (int64_t t = t0; t < t1; ++t) {
+    const int64_t base = t*SCAN_TILE + (int64_t)threadIdx.x*SCAN_ITEMS;
+    int32_t v[SCAN_ITEMS];
+    int64_t s = 0;
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+      v[k] = base + k < n ? in[base + k] : 0;
+      s += v[k];
+    }
+    int64_t total;
+    int64_t run = block_excl_scan(s, &total) + carry;
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+      if (base + k < n) out[base + k] = run;
+      run += v[k];
+    }
+    carry += total;
   }
 }
 
 // Launch sizes: the capacities bound the device-side lengths.
-int64_t scan_items(const Problem& p, int which) {
-  return which == SCAN_FLAGS ? p.candcap : (which == SCAN_CELLS ? p.cellcap : p.n);
-}
+int64_t scan_items(const Problem& p, int which) { return scanCapacity(p.n, p.candcap, p.cellcap, which); }
 
 }  // namespace
 
@@ -332,9 +359,9 @@ int batch_scan(Batch& b, int which) {
   std::vector<int64_t> tiles(b.mem.size()), ones(b.mem.size(), 1);
   for (size_t m = 0; m < b.mem.size(); ++m) {
     Problem& p = *b.mem[m];
-    tiles[m] = (scan_items(p, which) + SCAN_TILE - 1)/SCAN_TILE;
+    tiles[m] = scanBlocks(scan_items(p, which));
     if (tiles[m] + 1 > p.blockSumsCap) {
-      const int rc = ensure_block_sums(p, tiles[m] + 1);
+      const int rc = ensure_block_sums(p, kScanBlocks + 1);
       if (rc) return rc;
       b.memDirty = true;
     }

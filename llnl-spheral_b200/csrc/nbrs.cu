@@ -38,6 +38,8 @@ namespace sphgpu {
 namespace {
 
 constexpr int kGhostThreads = 256;
+// blocks per member of the streaming passes (member-local grid stride)
+constexpr int64_t kStreamBlocks = 148*4;
 constexpr float kFilterTol = 1.0e-3f;
 // shared memory for the per-thread lists of a 32-thread block (larger lists
 // take the warp schedule)
@@ -159,18 +161,67 @@ __device__ __forceinline__ double nodeHmax(const Member& M, int64_t k) {
   return M.hmaxi[k < M.n ? k : M.groot[k - M.n]];
 }
 
+// Items of a member in a fixed grid: member-local grid stride.
+#define FOR_ITEMS(t, count) \
+  for (int64_t t = mb.block*(int64_t)blockDim.x + threadIdx.x; t < (count); t += (int64_t)mb.blocks*blockDim.x)
+
+// Internal nodes within kernelExtent*max(1/min(eig(H))) of a periodic plane
+// (with a relative margin): the only internal nodes a boundary pass can
+// image or count into its hmax.  Flags into counts[0:n].
+__global__ void __launch_bounds__(kGhostThreads) near_flag_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const unsigned long long* bb = reinterpret_cast<const unsigned long long*>(M.scal + SC_BOUNDS);
+  const double reach = M.prm.kernelExtent*fromOrderedBits(bb[6])*(1.0 + 1.0e-6);
+  FOR_ITEMS(i, M.n) {
+    const V3 r = nodePos(M, i);
+    int f = 0;
+    for (int a = 0; a < 3; ++a) {
+      if (!M.prm.bcs.periodic[a]) continue;
+      const PlanarBC& bc = M.prm.bcs.bc[2*a];
+      if (dmin(minimumDistance(bc.exit, r), minimumDistance(bc.enter, r)) <= reach) f = 1;
+    }
+    M.counts[i] = f;
+  }
+}
+
+// The near-plane list, ascending, into cidx[0:nnear] (cidx is free until
+// the cell pass), and its length.
+__global__ void __launch_bounds__(kGhostThreads) near_list_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  FOR_ITEMS(i, M.n) {
+    if (M.counts[i]) M.cidx[M.offsets[i]] = (int32_t)i;
+  }
+  if (mb.block == 0 && threadIdx.x == 0) setScalI(M.scal, SC_NNEAR, M.offsets[M.n]);
+}
+
+// Item t of a boundary pass: the near-plane internal nodes in ascending
+// order, then the ghosts made so far in creation order (the order in which
+// the reference visits a NodeList's nodes).
+__device__ __forceinline__ int64_t passItems(const Member& M) {
+  return scalI(M.scal, SC_NNEAR) + scalI(M.scal, SC_NTOT) - M.n;
+}
+__device__ __forceinline__ int64_t passNode(const Member& M, int64_t t, int64_t nnear) {
+  return t < nnear ? (int64_t)M.cidx[t] : M.n + (t - nnear);
+}
+
 // hmax of PlanarBoundary::setGhostNodes: max 1/min(eig(H)) over nodes within
 // kernelExtent*hmaxi of either plane.
 __global__ void __launch_bounds__(kGhostThreads) ghost_hmax_kernel(const Member* mem, BlockMap bm, int b) {
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
-  const int64_t k = mb.block*blockDim.x + threadIdx.x;
   double best = 0.0;
-  if (k < scalI(M.scal, SC_NTOT) && M.prm.bcs.periodic[b >> 1]) {
+  if (M.prm.bcs.periodic[b >> 1]) {
     const PlanarBC& bc = M.prm.bcs.bc[b];
-    const V3 r = nodePos(M, k);
-    const double hmaxi = nodeHmax(M, k);
-    if (dmin(minimumDistance(bc.exit, r), minimumDistance(bc.enter, r)) < M.prm.kernelExtent*hmaxi) best = hmaxi;
+    const int64_t nnear = scalI(M.scal, SC_NNEAR);
+    FOR_ITEMS(t, passItems(M)) {
+      const int64_t k = passNode(M, t, nnear);
+      const V3 r = nodePos(M, k);
+      const double hmaxi = nodeHmax(M, k);
+      if (dmin(minimumDistance(bc.exit, r), minimumDistance(bc.enter, r)) < M.prm.kernelExtent*hmaxi)
+        best = dmax(best, hmaxi);
+    }
   }
   for (int o = 16; o > 0; o >>= 1) best = dmax(best, __shfl_xor_sync(0xffffffffu, best, o));
   if ((threadIdx.x & 31) == 0 && best > 0.0)
@@ -180,40 +231,45 @@ __global__ void __launch_bounds__(kGhostThreads) ghost_hmax_kernel(const Member*
 __global__ void __launch_bounds__(kGhostThreads) ghost_flag_kernel(const Member* mem, BlockMap bm, int b) {
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
-  const int64_t k = mb.block*blockDim.x + threadIdx.x;
-  if (k >= scalI(M.scal, SC_NTOT)) return;
-  int f = 0;
   const double hmax = M.scal[SC_HMAX];
-  if (M.prm.bcs.periodic[b >> 1] && hmax > 0.0) {
-    const V3 r = nodePos(M, k);
-    const double disti = signedDistance(M.prm.bcs.bc[b].exit, r)/hmax;
-    f = (disti >= 0.0 && disti <= M.prm.kernelExtent) ? 1 : 0;
+  const bool on = M.prm.bcs.periodic[b >> 1] && hmax > 0.0;
+  const int64_t nnear = scalI(M.scal, SC_NNEAR);
+  FOR_ITEMS(t, passItems(M)) {
+    int f = 0;
+    if (on) {
+      const V3 r = nodePos(M, passNode(M, t, nnear));
+      const double disti = signedDistance(M.prm.bcs.bc[b].exit, r)/hmax;
+      f = (disti >= 0.0 && disti <= M.prm.kernelExtent) ? 1 : 0;
+    }
+    M.counts[t] = f;
   }
-  M.counts[k] = f;
 }
 
 __global__ void __launch_bounds__(kGhostThreads) ghost_scatter_kernel(const Member* mem, BlockMap bm, int b) {
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
-  const int64_t k = mb.block*blockDim.x + threadIdx.x;
-  const int64_t ntot = scalI(M.scal, SC_NTOT);
-  if (k >= ntot || !M.counts[k]) return;
   const int64_t n = M.n;
-  const int64_t g = (ntot - n) + M.offsets[k];     // ghost index of the new image
-  if (g >= M.gcap) {
-    atomicOr(M.err, DERR_GHOST_CAPACITY);
-    return;
-  }
+  const int64_t ntot = scalI(M.scal, SC_NTOT);
+  const int64_t nnear = scalI(M.scal, SC_NNEAR);
   const PlanarBC& bc = M.prm.bcs.bc[b];
-  const V3 gp = mapPositionThroughPlanes(nodePos(M, k), bc.exit, bc.enter);
-  const int32_t root = k < n ? (int32_t)k : M.groot[k - n];
-  uint32_t code = k < n ? 0u : M.gcode[k - n];
   const int axis = b >> 1;
-  if ((code >> (2*axis)) & 3u) atomicOr(M.err, DERR_GHOST_CHAIN);
-  code |= (uint32_t)((b & 1) + 1) << (2*axis);
-  M.groot[g] = root;
-  M.gcode[g] = code;
-  M.gpos[g] = gp.x; M.gpos[M.gcap + g] = gp.y; M.gpos[2*M.gcap + g] = gp.z;
+  FOR_ITEMS(t, passItems(M)) {
+    if (!M.counts[t]) continue;
+    const int64_t k = passNode(M, t, nnear);
+    const int64_t g = (ntot - n) + M.offsets[t];     // ghost index of the new image
+    if (g >= M.gcap) {
+      atomicOr(M.err, DERR_GHOST_CAPACITY);
+      continue;
+    }
+    const V3 gp = mapPositionThroughPlanes(nodePos(M, k), bc.exit, bc.enter);
+    const int32_t root = k < n ? (int32_t)k : M.groot[k - n];
+    uint32_t code = k < n ? 0u : M.gcode[k - n];
+    if ((code >> (2*axis)) & 3u) atomicOr(M.err, DERR_GHOST_CHAIN);
+    code |= (uint32_t)((b & 1) + 1) << (2*axis);
+    M.groot[g] = root;
+    M.gcode[g] = code;
+    M.gpos[g] = gp.x; M.gpos[M.gcap + g] = gp.y; M.gpos[2*M.gcap + g] = gp.z;
+  }
 }
 
 // After a boundary pass: the new images join the node set (at most up to the
@@ -294,23 +350,22 @@ __device__ __forceinline__ int cellCoord(double x, double lo, double cell, int d
 __global__ void __launch_bounds__(kGhostThreads) cell_zero_kernel(const Member* mem, BlockMap bm) {
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
-  const int64_t c = mb.block*blockDim.x + threadIdx.x;
-  if (c < scalI(M.scal, SC_NCELLS)) M.cellFill[c] = 0;
+  FOR_ITEMS(c, scalI(M.scal, SC_NCELLS)) M.cellFill[c] = 0;
 }
 
 __global__ void __launch_bounds__(kGhostThreads) cell_index_kernel(const Member* mem, BlockMap bm) {
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
-  const int64_t k = mb.block*blockDim.x + threadIdx.x;
-  if (k >= allNodes(M)) return;
   const Grid g = loadGrid(M);
-  const V3 r = nodePos(M, k);
-  const int cx = cellCoord(r.x, g.lo[0], g.cell, g.dim[0]);
-  const int cy = cellCoord(r.y, g.lo[1], g.cell, g.dim[1]);
-  const int cz = cellCoord(r.z, g.lo[2], g.cell, g.dim[2]);
-  const int c = (cz*g.dim[1] + cy)*g.dim[0] + cx;
-  M.cidx[k] = c;
-  atomicAdd(M.cellFill + c, 1);
+  FOR_ITEMS(k, allNodes(M)) {
+    const V3 r = nodePos(M, k);
+    const int cx = cellCoord(r.x, g.lo[0], g.cell, g.dim[0]);
+    const int cy = cellCoord(r.y, g.lo[1], g.cell, g.dim[1]);
+    const int cz = cellCoord(r.z, g.lo[2], g.cell, g.dim[2]);
+    const int c = (cz*g.dim[1] + cy)*g.dim[0] + cx;
+    M.cidx[k] = c;
+    atomicAdd(M.cellFill + c, 1);
+  }
 }
 
 // Cell-ordered candidate arrays (Problem::cand), one slot per node:
@@ -435,23 +490,23 @@ __device__ __forceinline__ bool candTest(const Member& M, const NbrArrays& a, co
 __global__ void __launch_bounds__(kGhostThreads) cell_scatter_kernel(const Member* mem, BlockMap bm) {
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
-  const int64_t k = mb.block*blockDim.x + threadIdx.x;
-  if (k >= allNodes(M)) return;
-  const int c = M.cidx[k];
-  const int64_t slot = M.cellStart[c] + atomicAdd(M.cellFill + c, 1);
-  M.sortedIdx[slot] = (int32_t)k;
-  const V3 r = nodePos(M, k);
   const Grid g = loadGrid(M);
-  const int cx = cellCoord(r.x, g.lo[0], g.cell, g.dim[0]);
-  const int cy = cellCoord(r.y, g.lo[1], g.cell, g.dim[1]);
-  const int cz = cellCoord(r.z, g.lo[2], g.cell, g.dim[2]);
-  const int64_t root = k < M.n ? k : M.groot[k - M.n];
   double* base = static_cast<double*>(M.cand);
   float4* pre = reinterpret_cast<float4*>(base);
-  pre[slot] = make_float4((float)(r.x - (g.lo[0] + cx*g.cell)), (float)(r.y - (g.lo[1] + cy*g.cell)),
-                          (float)(r.z - (g.lo[2] + cz*g.cell)), (float)(1.0/M.hmaxi[root]));
   float* lmax = reinterpret_cast<float*>(base + 2*M.candcap);
-  lmax[slot] = (float)M.hmaxi[M.n + root];
+  FOR_ITEMS(k, allNodes(M)) {
+    const int c = M.cidx[k];
+    const int64_t slot = M.cellStart[c] + atomicAdd(M.cellFill + c, 1);
+    M.sortedIdx[slot] = (int32_t)k;
+    const V3 r = nodePos(M, k);
+    const int cx = cellCoord(r.x, g.lo[0], g.cell, g.dim[0]);
+    const int cy = cellCoord(r.y, g.lo[1], g.cell, g.dim[1]);
+    const int cz = cellCoord(r.z, g.lo[2], g.cell, g.dim[2]);
+    const int64_t root = k < M.n ? k : M.groot[k - M.n];
+    pre[slot] = make_float4((float)(r.x - (g.lo[0] + cx*g.cell)), (float)(r.y - (g.lo[1] + cy*g.cell)),
+                            (float)(r.z - (g.lo[2] + cz*g.cell)), (float)(1.0/M.hmaxi[root]));
+    lmax[slot] = (float)M.hmaxi[M.n + root];
+  }
 }
 
 // Thread per internal node, nodes taken in cell-sorted order so that the
@@ -731,8 +786,7 @@ int plan_capacities(Batch& b) {
     // without a hint the first build guesses 32 entries per node; an overflow redoes it
     SPH_TRY(ensure_capacity_entries(p, E > 0 ? E + E/8 : 32*p.n));
     if (p.fillCap < 8) p.fillCap = p.maxCount > 0 ? p.maxCount + p.maxCount/4 + 8 : 64;
-    const int64_t tiles = ((p.candcap > p.cellcap ? p.candcap : p.cellcap) + 1023)/1024 + 2;
-    if (tiles > p.blockSumsCap) SPH_TRY(ensure_block_sums(p, tiles));
+    if (kScanBlocks + 1 > p.blockSumsCap) SPH_TRY(ensure_block_sums(p, kScanBlocks + 1));
     if (p.gcap != oldg || p.candcap != oldc || p.ecap != olde || p.cellcap != oldcells) b.memDirty = true;
     // schedule: a warp per node once the 27-cell candidate set of the last
     // build kept 32 lanes busy, or once a thread's list would not fit in
@@ -774,7 +828,7 @@ int64_t planned_bytes(const sphgpu_config& cfg, int64_t n, int64_t G, int64_t E,
   p.cellcap = (ncells > 0 ? grow(ncells) : p.candcap/2 + 64) + 1;
   const int64_t eneed = E > 0 ? E + E/8 : 32*n;
   p.ecap = eneed + eneed/8 + 1024;                                       // ensure_capacity_entries
-  p.blockSumsCap = ((p.candcap > p.cellcap ? p.candcap : p.cellcap) + 1023)/1024 + 2 + 64;
+  p.blockSumsCap = kScanBlocks + 1 + 64;                                // ensure_block_sums
   if (cfg.precision == SPHGPU_PRECISION_MIXED) p.mreccap = p.candcap;
   if (cfg.hydro == SPHGPU_HYDRO_CRKSPH) p.creccap = p.candcap;
   double marker = 0.0;                          // problem_bytes only tests these for null
@@ -798,9 +852,20 @@ int launch_build(Batch& b) {
   build_init_kernel<<<(nm + 127)/128, 128, 0, st>>>(b.d_mem, nm); batch_count_launch(b);
   SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.n; }, kGhostThreads, &bm, &grid));
   if (grid) { node_hmax_kernel<<<grid, kGhostThreads, 0, st>>>(b.d_mem, bm); batch_count_launch(b); }
-  BlockMap cap;
-  unsigned capGrid = 0;
-  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.candcap; }, kGhostThreads, &cap, &capGrid));
+  // fixed grids: at most kStreamBlocks blocks per member, member-local stride
+  auto fixedItems = [](int64_t cap) { return cap < kStreamBlocks*kGhostThreads ? cap : kStreamBlocks*kGhostThreads; };
+  BlockMap nmap, cap;
+  unsigned ngrid = 0, capGrid = 0;
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return fixedItems(p.n); }, kGhostThreads, &nmap, &ngrid));
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return fixedItems(p.candcap); }, kGhostThreads, &cap, &capGrid));
+  bool anyPeriodic = false;
+  for (Problem* p : b.mem) for (int a = 0; a < 3; ++a) anyPeriodic = anyPeriodic || p->prm.bcs.periodic[a];
+  if (anyPeriodic) {
+    // the boundary passes visit only the internal nodes near a periodic plane
+    near_flag_kernel<<<ngrid, kGhostThreads, 0, st>>>(b.d_mem, nmap); batch_count_launch(b);
+    SPH_TRY(batch_scan(b, SCAN_COUNTS));
+    near_list_kernel<<<ngrid, kGhostThreads, 0, st>>>(b.d_mem, nmap); batch_count_launch(b);
+  }
   for (int bnd = 0; bnd < 6; ++bnd) {
     bool any = false;
     for (Problem* p : b.mem) any = any || p->prm.bcs.periodic[bnd >> 1];
@@ -815,7 +880,7 @@ int launch_build(Batch& b) {
   grid_kernel<<<(nm + 127)/128, 128, 0, st>>>(b.d_mem, nm); batch_count_launch(b);
   BlockMap cm;
   unsigned cgrid = 0;
-  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.cellcap; }, kGhostThreads, &cm, &cgrid));
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return fixedItems(p.cellcap); }, kGhostThreads, &cm, &cgrid));
   cell_zero_kernel<<<cgrid, kGhostThreads, 0, st>>>(b.d_mem, cm); batch_count_launch(b);
   cell_index_kernel<<<capGrid, kGhostThreads, 0, st>>>(b.d_mem, cap); batch_count_launch(b);
   SPH_TRY(batch_scan(b, SCAN_CELLS));

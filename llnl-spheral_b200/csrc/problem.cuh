@@ -254,7 +254,8 @@ enum ScalSlot {
   SC_NTOT = 25,        // internal nodes + ghosts made so far (ghost passes)
   SC_G = 26,           // ghosts
   SC_NCELLS = 27,      // cells of the grid
-  SC_GRID = 28,        // lo[3], cell (doubles), dim[3] (i64)
+  SC_GRID = 28,        // lo[3], cell (doubles), dim[3] (i64), pre-test tolerance
+  SC_NNEAR = 36,       // internal nodes near a periodic plane (the boundary passes' list)
   NSCAL = 40
 };
 
@@ -371,6 +372,10 @@ void batch_count_launch(Batch& b);
 void batch_set_scal(Batch& b, int slot, double value);
 // exclusive prefix sums of every member (in/out chosen by `which`), totals in SC_TOTAL
 enum ScanWhich { SCAN_FLAGS = 0, SCAN_CELLS = 1, SCAN_COUNTS = 2 };
+// A scan runs on at most kScanBlocks blocks per member, each over a
+// contiguous run of tiles, so its grid does not grow with the capacity
+// (blockSums holds kScanBlocks + 1 entries).
+constexpr int kScanBlocks = 148*2;
 int batch_scan(Batch& b, int which);
 
 // ---- stages (ghosts/neighbors: nbrs.cu; SPH: sph.cu; mixed: sph_mixed.cu; CRKSPH: crk.cu)
