@@ -853,7 +853,7 @@ int sphgpu_evaluate_derivatives(sphgpu_problem* p, double time, double dt) {
   if (p == nullptr) return SPHGPU_ERR_ARG;
   (void)time; (void)dt;
   SPH_TRY(require_nbrs(solo(p)));
-  SPH_TRY(pack_records(solo(p)));
+  SPH_TRY(pack_records(solo(p), PACK_FOR_EVAL));   // the mixed form packs its own records
   SPH_TRY(launch_eval(solo(p)));
   p->haveDerivs = true;
   return SPHGPU_OK;
@@ -876,7 +876,7 @@ int sphgpu_finalize(sphgpu_problem* p, double time, double dt) {
 int sphgpu_dt(sphgpu_problem* p, double* dt_out) {
   if (p == nullptr || dt_out == nullptr) return SPHGPU_ERR_ARG;
   SPH_TRY(require_nbrs(solo(p)));
-  SPH_TRY(launch_dt(solo(p), SC_DTOUT));
+  SPH_TRY(launch_dt(solo(p), SC_DTOUT, false));
   const int slot = SC_DTOUT;
   std::vector<double> v;
   SPH_TRY(batch_gather(solo(p), &slot, 1, v));

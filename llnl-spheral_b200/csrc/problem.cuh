@@ -393,7 +393,7 @@ int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode);
 int launch_compatible_energy(Batch& b, double scale);
 int launch_enforce_boundaries(Batch& b);
 int launch_eos(Batch& b);
-int launch_dt(Batch& b, int slot);                          // min dt vote bits -> slot
+int launch_dt(Batch& b, int slot, bool cachedEig);          // min dt vote bits -> slot
 int launch_select_dt(Batch& b);                             // SC_DT from the vote and SC_LASTDT
 int launch_finish_step(Batch& b);                           // SC_LASTDT = SC_DT
 int launch_conservation(Batch& b);                          // SC_CONS

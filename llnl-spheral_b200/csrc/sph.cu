@@ -410,7 +410,15 @@ __global__ void __launch_bounds__(128) compatible_energy_kernel(const Member* me
 }
 
 // ---------------------------------------------------------------- policies
+// eig(H) strictly inside (1/hmax, 1/hmin), where the eigenvalue clamp of the
+// bounded H policies is inactive.  Gershgorin discs bound the eigenvalues;
+// when they lie inside with a relative margin far above the eigen solve's
+// rounding, the solve is skipped (the answer cannot differ).
 __device__ __forceinline__ bool hInsideBounds(const Sym& H, double hmin, double hmax) {
+  const double rx = dabs(H.xy) + dabs(H.xz), ry = dabs(H.xy) + dabs(H.yz), rz = dabs(H.xz) + dabs(H.yz);
+  const double glo = dmin(H.xx - rx, dmin(H.yy - ry, H.zz - rz));
+  const double ghi = dmax(H.xx + rx, dmax(H.yy + ry, H.zz + rz));
+  if (glo > (1.0/hmax)*(1.0 + 1.0e-12) && ghi < (1.0/hmin)*(1.0 - 1.0e-12)) return true;
   const V3 ev = eigenValues(H);
   return vmin(ev) > 1.0/hmax && vmax(ev) < 1.0/hmin;
 }
@@ -530,7 +538,10 @@ __global__ void __launch_bounds__(256) enforce_boundaries_kernel(const Member* m
 }
 
 // ---------------------------------------------------------------- dt
-__global__ void __launch_bounds__(128) hydro_dt_kernel(const Member* mem, BlockMap bm, int slot) {
+// cachedEig: max eig(H) of each node is the one the neighbor build stored
+// (hmaxi[n + i]), valid when H has not changed since that build (the step's
+// selectDt, which follows the build); otherwise it is solved here.
+__global__ void __launch_bounds__(128) hydro_dt_kernel(const Member* mem, BlockMap bm, int slot, int cachedEig) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = mem[mb.m];
   const int64_t n = MB.n;
@@ -540,9 +551,15 @@ __global__ void __launch_bounds__(128) hydro_dt_kernel(const Member* mem, BlockM
   const double* D = MB.D;
   double minDt = kFltMax;
   if (i < n) {
-    const Sym H{S[(S_H + 0)*n + i], S[(S_H + 1)*n + i], S[(S_H + 2)*n + i],
-                S[(S_H + 3)*n + i], S[(S_H + 4)*n + i], S[(S_H + 5)*n + i]};
-    const double nodeScale = 1.0/vmax(eigenValues(H))/P.nPerh;
+    double lmax;
+    if (cachedEig) {
+      lmax = MB.hmaxi[n + i];
+    } else {
+      const Sym H{S[(S_H + 0)*n + i], S[(S_H + 1)*n + i], S[(S_H + 2)*n + i],
+                  S[(S_H + 3)*n + i], S[(S_H + 4)*n + i], S[(S_H + 5)*n + i]};
+      lmax = vmax(eigenValues(H));
+    }
+    const double nodeScale = 1.0/lmax/P.nPerh;
     const double cs = S[S_CS*n + i], rho = S[S_RHO*n + i];
     const double csDt = nodeScale/(cs + kFltMin);
     if (csDt < minDt) minDt = csDt;
@@ -764,18 +781,18 @@ int launch_enforce_boundaries(Batch& b) {
   return cuda_status(cudaGetLastError(), "enforce boundaries");
 }
 
-int launch_dt(Batch& b, int slot) {
+int launch_dt(Batch& b, int slot, bool cachedEig) {
   if (b.memDirty) SPH_TRY(batch_upload(b));
   batch_set_scal(b, slot, kFltMax);
   BlockMap bm;
   unsigned grid = 0;
   SPH_TRY(map_nodes(b, 128, &bm, &grid));
-  if (grid) { hydro_dt_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm, slot); batch_count_launch(b); }
+  if (grid) { hydro_dt_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm, slot, cachedEig ? 1 : 0); batch_count_launch(b); }
   return cuda_status(cudaGetLastError(), "dt");
 }
 
 int launch_select_dt(Batch& b) {
-  SPH_TRY(launch_dt(b, SC_MINDT));
+  SPH_TRY(launch_dt(b, SC_MINDT, true));      // right after the build: H unchanged
   const int nm = (int)b.mem.size();
   select_dt_kernel<<<(nm + 127)/128, 128, 0, b.stream>>>(b.d_mem, nm); batch_count_launch(b);
   return cuda_status(cudaGetLastError(), "select dt");
