@@ -123,9 +123,9 @@ const FieldSpec kFields[] = {
     {"delta H", 1, D_DHDT, 6},
     {"new H", 1, D_HIDEAL, 6},
     {"velocity gradient", 1, D_DVDX, 9},
-    {"internal velocity gradient", 1, D_LDVDX, 9},
+    {"internal velocity gradient", 1, D_DVDX, 9},
     {"M SPH gradient correction", 1, D_M, 9},
-    {"local M SPH gradient correction", 1, D_LM, 9},
+    {"local M SPH gradient correction", 1, D_M, 9},
     {"new mass density", 1, D_RHOSUM, 1},
     {"normalization", 1, D_NORM, 1},
     {"weighted neighbor sum", 1, D_WNS, 1},
@@ -177,7 +177,8 @@ void free_problem(Problem* p) {
   if (p == nullptr) return;
   void* ptrs[] = {p->S, p->S0, p->D, p->rec, p->groot, p->gcode, p->gpos, p->cand, p->cidx, p->sortedIdx,
                   p->cellStart, p->cellFill, p->counts, p->offsets, p->nbr, p->pacc, p->tableCoef, p->nperhTab,
-                  p->wsumTab, p->blockSums, p->d_err, p->d_scal, p->d_red, p->staging, p->coefF, p->mrec, p->K, p->crec, p->hmaxi};
+                  p->wsumTab, p->blockSums, p->d_err, p->d_scal, p->d_red, p->staging, p->coefF, p->mrec, p->K, p->crec, p->hmaxi,
+                  p->wsumBinsTab};
   for (void* q : ptrs) if (q) cudaFree(q);
   if (p->pinned) cudaFreeHost(p->pinned);
   if (p->solo) { batch_free(*p->solo); delete p->solo; p->solo = nullptr; }
@@ -604,7 +605,7 @@ int64_t problem_bytes(const Problem& p) {
   const int64_t n = p.n;
   const int stagingComps = p.cfg.hydro == SPHGPU_HYDRO_CRKSPH ? 27 : 9;
   int64_t b = 8*(2*(int64_t)NSTATE*n + (int64_t)NDERIV*n + stagingComps*n + 2*n + NSCAL + 148*4*8) + 16;
-  b += 8*(6 + 2)*(int64_t)p.prm.W.n;                                  // tables
+  b += 8*(6 + 2)*(int64_t)p.prm.W.n + 4*(kWsumBins + 1);              // tables
   b += p.gcap*(4 + 4 + 24);                                           // groot, gcode, gpos
   b += p.candcap*(4 + 4 + 4 + 8*CAND_DOUBLES + 8*RECW) + 8*(p.candcap + 1);  // counts, cidx, sortedIdx, cand, rec, offsets
   b += p.ecap*(4 + (p.pacc ? 24 : 0));                                // nbr, pacc
@@ -709,6 +710,27 @@ int sphgpu_create(const sphgpu_config* cfg, int64_t n_internal, sphgpu_problem**
     cudaMemcpy(p->tableCoef, coef6.data(), sizeof(double)*coef6.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(p->nperhTab, nperh.data(), sizeof(double)*nt, cudaMemcpyHostToDevice);
     cudaMemcpy(p->wsumTab, wsum.data(), sizeof(double)*nt, cudaMemcpyHostToDevice);
+    // bracket table of the Wsum bisection (ascending Wsum)
+    if (nt >= 2 && wsum[nt - 1] > wsum[0]) {
+      std::vector<int32_t> bins(kWsumBins + 1);
+      const double w0 = wsum[0], width = (wsum[nt - 1] - wsum[0])/kWsumBins;
+      int j = -1;
+      for (int b = 0; b <= kWsumBins; ++b) {
+        const double edge = b == kWsumBins ? wsum[nt - 1] : w0 + b*width;
+        while (j + 1 < nt && wsum[j + 1] <= edge) ++j;
+        bins[b] = j;
+      }
+      bool ascending = true;
+      for (int k = 1; k < nt; ++k) ascending = ascending && wsum[k] >= wsum[k - 1];
+      if (ascending) {
+        if ((rc = dalloc(p->wsumBinsTab, kWsumBins + 1)) != SPHGPU_OK) break;
+        cudaMemcpy(p->wsumBinsTab, bins.data(), sizeof(int32_t)*(kWsumBins + 1), cudaMemcpyHostToDevice);
+        p->prm.wsumBins = p->wsumBinsTab;
+        p->prm.wsumNbins = kWsumBins;
+        p->prm.wsumBin0 = w0;
+        p->prm.wsumBinInv = 1.0/width;
+      }
+    }
     Params& P = p->prm;
     P.W.coef = p->tableCoef;
     P.W.n = nt;

@@ -413,20 +413,7 @@ __global__ void __launch_bounds__(128) crk_eval_kernel(const Member* mem, BlockM
   if (fuzzyEqual(wns, 0.0)) {
     nPerhCur = 0.5*P.nPerh;
   } else {
-    const int nt = P.W.n;
-    const bool ascnd = ldg(P.wsum + nt - 1) >= ldg(P.wsum);
-    int jl = -1, ju = nt;
-    while (ju - jl > 1) {
-      const int jm = (ju + jl)/2;
-      if ((wns >= ldg(P.wsum + jm)) == ascnd) jl = jm; else ju = jm;
-    }
-    if (jl == -1) nPerhCur = ldg(P.nperh);
-    else if (jl + 1 == nt) nPerhCur = ldg(P.nperh + nt - 1);
-    else {
-      const double nl = ldg(P.nperh + jl), nu = ldg(P.nperh + jl + 1);
-      const double wl = ldg(P.wsum + jl), wu = ldg(P.wsum + jl + 1);
-      nPerhCur = dmin(nu, dmax(nl, nl + (wns - wl)/(wu - wl)*(nu - nl)));
-    }
+    nPerhCur = equivalentNodesPerSmoothingScale(P, wns);
   }
   const double s = dmin(4.0, dmax(0.25, P.nPerh/(nPerhCur + 1.0e-30)));
   const double a = s < 1.0 ? 0.4*(1.0 + s*s) : 0.4*(1.0 + 1.0/(s*s*s));
@@ -446,7 +433,6 @@ __global__ void __launch_bounds__(128) crk_eval_kernel(const Member* mem, BlockM
 #pragma unroll
   for (int c = 0; c < 9; ++c) {
     d[(D_DVDX + c)*n] = dv[c];
-    d[(D_LDVDX + c)*n] = dv[c];
   }
   d[D_WNS*n] = wns;
   d[(D_M2 + 0)*n] = m2.xx; d[(D_M2 + 1)*n] = m2.xy; d[(D_M2 + 2)*n] = m2.xz;

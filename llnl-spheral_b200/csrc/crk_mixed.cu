@@ -253,20 +253,7 @@ __global__ void __launch_bounds__(128, 3) crk_eval_mixed_kernel(const Member* me
   if (fuzzyEqual(w, 0.0)) {
     nPerhCur = 0.5*P.nPerh;
   } else {
-    const int nt = P.W.n;
-    const bool ascnd = __ldg(P.wsum + nt - 1) >= __ldg(P.wsum);
-    int jl = -1, ju = nt;
-    while (ju - jl > 1) {
-      const int jm = (ju + jl)/2;
-      if ((w >= __ldg(P.wsum + jm)) == ascnd) jl = jm; else ju = jm;
-    }
-    if (jl == -1) nPerhCur = __ldg(P.nperh);
-    else if (jl + 1 == nt) nPerhCur = __ldg(P.nperh + nt - 1);
-    else {
-      const double nl = __ldg(P.nperh + jl), nu = __ldg(P.nperh + jl + 1);
-      const double wl = __ldg(P.wsum + jl), wu = __ldg(P.wsum + jl + 1);
-      nPerhCur = dmin(nu, dmax(nl, nl + (w - wl)/(wu - wl)*(nu - nl)));
-    }
+    nPerhCur = equivalentNodesPerSmoothingScale(P, w);
   }
   const double s = dmin(4.0, dmax(0.25, P.nPerh/(nPerhCur + 1.0e-30)));
   const double a = s < 1.0 ? 0.4*(1.0 + s*s) : 0.4*(1.0 + 1.0/(s*s*s));
@@ -286,7 +273,6 @@ __global__ void __launch_bounds__(128, 3) crk_eval_mixed_kernel(const Member* me
 #pragma unroll
   for (int c = 0; c < 9; ++c) {
     d[(D_DVDX + c)*n] = dvdx[c];
-    d[(D_LDVDX + c)*n] = dvdx[c];
   }
   d[D_WNS*n] = w;
 #pragma unroll

@@ -59,6 +59,10 @@ enum CrkRecField {
   CRECW = 34           // 272 bytes
 };
 
+// StateDerivatives of the internal nodes.  With one NodeList the reference's
+// "internal velocity gradient" and "local M SPH gradient correction" equal
+// the velocity gradient and M (every pair is internal to the material), so
+// those two keys read D_DVDX and D_M.
 enum DerivField {
   D_DXDT = 0,          // 3  "delta position"
   D_DVDT = 3,          // 3  "delta velocity hydro"
@@ -66,20 +70,18 @@ enum DerivField {
   D_DEPSDT = 7,        // 1  "delta specific thermal energy"
   D_DHDT = 8,          // 6  "delta H"
   D_HIDEAL = 14,       // 6  "new H"
-  D_DVDX = 20,         // 9  "velocity gradient"
-  D_LDVDX = 29,        // 9  "internal velocity gradient"
-  D_M = 38,            // 9  "M SPH gradient correction"
-  D_LM = 47,           // 9  "local M SPH gradient correction"
-  D_RHOSUM = 56,       // 1  "new mass density"
-  D_NORM = 57,         // 1  "normalization"
-  D_WNS = 58,          // 1  "weighted neighbor sum"
-  D_M2 = 59,           // 6  "mass second moment"
-  D_XSPHW = 65,        // 1  "XSPH weight sum"
-  D_XSPHDV = 66,       // 3  "XSPH delta vi"
-  D_MAXVP = 69,        // 1  "max viscous pressure"
-  D_EFFVP = 70,        // 1  "effective viscous pressure"
-  D_VISCW = 71,        // 1  "viscous work rate"
-  NDERIV = 72
+  D_DVDX = 20,         // 9  "velocity gradient", "internal velocity gradient"
+  D_M = 29,            // 9  "M SPH gradient correction", "local M SPH gradient correction"
+  D_RHOSUM = 38,       // 1  "new mass density"
+  D_NORM = 39,         // 1  "normalization"
+  D_WNS = 40,          // 1  "weighted neighbor sum"
+  D_M2 = 41,           // 6  "mass second moment"
+  D_XSPHW = 47,        // 1  "XSPH weight sum"
+  D_XSPHDV = 48,       // 3  "XSPH delta vi"
+  D_MAXVP = 51,        // 1  "max viscous pressure"
+  D_EFFVP = 52,        // 1  "effective viscous pressure"
+  D_VISCW = 53,        // 1  "viscous work rate"
+  NDERIV = 54
 };
 
 // Packed pair record: everything one side of a pair needs.
@@ -98,6 +100,11 @@ struct Params {
   TableDev W;
   const double* nperh;     // TableKernel nPerh table
   const double* wsum;      // TableKernel Wsum table
+  // Bracket table of the Wsum bisection (ascending tables only, else null):
+  // wsumBins[b] = last index j with wsum[j] <= wsumBin0 + b/wsumBinInv.
+  const int32_t* wsumBins;
+  int wsumNbins;
+  double wsumBin0, wsumBinInv;
   double W0;               // W.kernelValue(0, 1)
   double WnPerh;           // W.kernelValue(1/nPerh, 1)
   double nPerh, Cl, Cq, eps2, epsTensile, gamma, cfl;
@@ -182,6 +189,7 @@ struct Problem {
   double* mrec = nullptr;       // [n+G][MRECW] mixed-precision records
   int64_t mreccap = 0;
   double* nperhTab = nullptr;
+  int32_t* wsumBinsTab = nullptr;   // [kWsumBins + 1] Params::wsumBins
   double* wsumTab = nullptr;
   Params prm{};
 
@@ -409,6 +417,34 @@ int launch_crk_eval_mixed(Batch& b);                        // mixed-precision C
 
 // one CheapSynchronousRK2 step of every member (api.cu)
 int batch_step_rk2(Batch& b);
+// TableKernel::equivalentNodesPerSmoothingScale (src/Kernel/TableKernel.cc:
+// 402-430): bisectSearch of the Wsum table, then linear interpolation of the
+// nPerh table.  The bisection starts from the bracket table's interval for w
+// (a few entries) instead of the whole table; every bracket satisfies the
+// bisection's invariant wsum[jl] <= w < wsum[ju], so it ends on the same
+// index as the full search.
+constexpr int kWsumBins = 4096;
+__device__ __forceinline__ double equivalentNodesPerSmoothingScale(const Params& P, double w) {
+  const int nt = P.W.n;
+  const bool ascnd = __ldg(P.wsum + nt - 1) >= __ldg(P.wsum);
+  int jl = -1, ju = nt;
+  if (P.wsumBins != nullptr && w >= P.wsumBin0) {
+    const double q = (w - P.wsumBin0)*P.wsumBinInv;
+    const int b = q < (double)(P.wsumNbins - 1) ? (int)q : P.wsumNbins - 1;
+    jl = b >= 1 ? __ldg(P.wsumBins + b - 1) : -1;
+    ju = __ldg(P.wsumBins + (b + 2 < P.wsumNbins ? b + 2 : P.wsumNbins)) + 1;
+  }
+  while (ju - jl > 1) {
+    const int jm = (ju + jl)/2;
+    if ((w >= __ldg(P.wsum + jm)) == ascnd) jl = jm; else ju = jm;
+  }
+  if (jl == -1) return __ldg(P.nperh);
+  if (jl + 1 == nt) return __ldg(P.nperh + nt - 1);
+  const double nl = __ldg(P.nperh + jl), nu = __ldg(P.nperh + jl + 1);
+  const double wl = __ldg(P.wsum + jl), wu = __ldg(P.wsum + jl + 1);
+  return dmin(nu, dmax(nl, nl + (w - wl)/(wu - wl)*(nu - nl)));
+}
+
 // device bytes held by a problem, from its buffer capacities (api.cu)
 int64_t problem_bytes(const Problem& p);
 // device bytes a new problem holds after its first neighbor build, when that

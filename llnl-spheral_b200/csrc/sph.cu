@@ -247,22 +247,7 @@ __global__ void __launch_bounds__(128) sph_eval_fp64_kernel(const Member* mem, B
   if (fuzzyEqual(wns, 0.0)) {
     nPerhCur = 0.5*P.nPerh;
   } else {
-    // TableKernel::equivalentNodesPerSmoothingScale with bisectSearch
-    const int nt = P.W.n;
-    const bool ascnd = ldg(P.wsum + nt - 1) >= ldg(P.wsum);
-    int jl = -1, ju = nt;
-    while (ju - jl > 1) {
-      const int jm = (ju + jl)/2;
-      if ((wns >= ldg(P.wsum + jm)) == ascnd) jl = jm; else ju = jm;
-    }
-    const int lb = jl, ub = lb + 1;
-    if (lb == -1) nPerhCur = ldg(P.nperh);
-    else if (ub == nt) nPerhCur = ldg(P.nperh + nt - 1);
-    else {
-      const double nl = ldg(P.nperh + lb), nu = ldg(P.nperh + ub);
-      const double wl = ldg(P.wsum + lb), wu = ldg(P.wsum + ub);
-      nPerhCur = dmin(nu, dmax(nl, nl + (wns - wl)/(wu - wl)*(nu - nl)));
-    }
+    nPerhCur = equivalentNodesPerSmoothingScale(P, wns);
   }
   const double s = dmin(4.0, dmax(0.25, P.nPerh/(nPerhCur + 1.0e-30)));
   const double a = s < 1.0 ? 0.4*(1.0 + s*s) : 0.4*(1.0 + 1.0/(s*s*s));
@@ -285,9 +270,7 @@ __global__ void __launch_bounds__(128) sph_eval_fp64_kernel(const Member* mem, B
 #pragma unroll
   for (int c = 0; c < 9; ++c) {
     d[(D_DVDX + c)*n] = dv[c];
-    d[(D_LDVDX + c)*n] = dv[c];     // localDvDx: same material everywhere
     d[(D_M + c)*n] = mm[c];
-    d[(D_LM + c)*n] = mm[c];
   }
   d[D_RHOSUM*n] = rhoSum;
   d[D_NORM*n] = norm;
