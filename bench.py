@@ -465,6 +465,7 @@ def measure_batch(pkg, count, steps, warmup):
             "batched_over_loop": (pairs / t_batch) / (lpairs / t_loop),
             "kernel_launches_per_step": launches / steps,
             "autotuned": {"neighbor walk": ["auto", "thread per node", "warp per node"][tune["neighbor walk"]],
+                          "neighbor cells per kernel reach": tune["neighbor cells"],
                           "pair loop threads": tune["pair loop"]},
             "config": {"workload": "%d Sod-type tubes, n log-uniform in [4096, 262144] (8k x k x k), "
                                    "gamma ~ U[1.3, 1.67], density ratio ~ U[2, 8], cubic B-spline nPerh 1.51, "

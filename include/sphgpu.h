@@ -198,17 +198,23 @@ int sphgpu_kernel_launches(sphgpu_problem* p, int64_t* launches);
  * a compaction moves the lists into the ConnectivityMap, so the candidates
  * are walked once; used when the problem evolves energy compatibly (it has
  * that buffer) and the lists fit in it, otherwise 2 = a counting walk, then
- * a filling walk.  Both give the same ConnectivityMap.
+ * a filling walk.  Both give the same ConnectivityMap.  stage "neighbor
+ * cells": cells per kernel reach of the walk's grid, 0 = automatic (1),
+ * 1 = cells of one reach (27-cell window), 2 = cells of half a reach
+ * (125-cell window, rows and cells beyond the reach skipped).  Same
+ * ConnectivityMap either way.
  * sphgpu_get_schedule reports what the last call used. */
 int sphgpu_set_schedule(sphgpu_problem* p, const char* stage, int32_t schedule);
 int sphgpu_get_schedule(sphgpu_problem* p, const char* stage, int32_t* schedule);
-/* Autotuner: times every schedule of the neighbor walk and the pair loop on
+/* Autotuner: times every schedule of the neighbor walk (thread or warp per
+ * node, then cells of one or half a kernel reach) and of the pair loop on
  * the problem's own data (CUDA events, median of three) and keeps the
  * fastest.  Results do not depend on the schedule; the call leaves the
  * connectivity rebuilt and the derivatives evaluated at the current state (as
  * sphgpu_build_neighbors, sphgpu_initialize and sphgpu_evaluate_derivatives
  * do).  report (may be NULL) = {neighbor schedule, ms thread, ms warp,
- * pair-loop threads, ms 64, ms 128, 0, 0}. */
+ * pair-loop threads, ms 64, ms 128, cells per kernel reach, ms with
+ * half-reach cells}. */
 int sphgpu_autotune(sphgpu_problem* p, double report[8]);
 /* ---- batches (no counterpart in the reference, which advances one problem
  * at a time).  A batch advances many independent problems together: each

@@ -482,7 +482,15 @@ int step_impl(Batch& b) {
   return SPHGPU_OK;
 }
 
-int set_schedule_impl(Batch& b, int* nbrSchedule, const char* stage, int32_t schedule) {
+int set_schedule_impl(Batch& b, int* nbrSchedule, int* nbrCells, const char* stage, int32_t schedule) {
+  if (std::strcmp(stage, "neighbor cells") == 0) {
+    if (schedule < 0 || schedule > 2) {
+      set_error("neighbor cells is 0 (auto), 1 (cells of one kernel reach) or 2 (half a reach)");
+      return SPHGPU_ERR_ARG;
+    }
+    *nbrCells = schedule;
+    return SPHGPU_OK;
+  }
   if (std::strcmp(stage, "neighbor walk") == 0) {
     if (schedule < NBR_SCHEDULE_AUTO || schedule > NBR_SCHEDULE_WARP) {
       set_error("neighbor walk schedule must be 0 (auto), 1 (thread per node) or 2 (warp per node)");
@@ -531,7 +539,8 @@ int set_schedule_impl(Batch& b, int* nbrSchedule, const char* stage, int32_t sch
 // data and timed with CUDA events on the batch stream (one warm run, then the
 // median of three); the fastest is kept.  All schedules give bit-identical
 // results, so tuning changes speed only.  report = {neighbor schedule,
-// ms thread, ms warp, pair-loop threads, ms 64, ms 128, 0, 0}.
+// ms thread, ms warp, pair-loop threads, ms 64, ms 128, cells per kernel
+// reach, ms with half-reach cells}.
 int autotune_impl(Batch& b, double* report) {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   SPH_CHECK(cudaEventCreate(&e0));
@@ -569,6 +578,13 @@ int autotune_impl(Batch& b, double* report) {
     if (rc != SPHGPU_OK) break;
     b.nbrSchedule = bestS;
     out[0] = bestS;
+    // cells of one kernel reach (the times above) vs half a reach
+    b.nbrCells = 2;
+    double ms2 = 0.0;
+    if ((rc = timeit([&]() { return build_neighbors_impl(b); }, &ms2)) != SPHGPU_OK) break;
+    b.nbrCells = ms2 < best ? 2 : 1;
+    out[6] = b.nbrCells;
+    out[7] = ms2;
     if ((rc = build_neighbors_impl(b)) != SPHGPU_OK) break;
     if ((rc = pack_records(b)) != SPHGPU_OK) break;
     if ((rc = initialize_impl(b)) != SPHGPU_OK) break;
@@ -948,7 +964,7 @@ int sphgpu_kernel_launches(sphgpu_problem* p, int64_t* launches) {
 
 int sphgpu_set_schedule(sphgpu_problem* p, const char* stage, int32_t schedule) {
   if (p == nullptr || stage == nullptr) return SPHGPU_ERR_ARG;
-  return set_schedule_impl(*p->solo, &p->nbrSchedule, stage, schedule);
+  return set_schedule_impl(*p->solo, &p->nbrSchedule, &p->nbrCells, stage, schedule);
 }
 
 int sphgpu_get_schedule(sphgpu_problem* p, const char* stage, int32_t* schedule) {
@@ -967,6 +983,10 @@ int sphgpu_get_schedule(sphgpu_problem* p, const char* stage, int32_t* schedule)
   }
   if (std::strcmp(stage, "neighbor passes") == 0) {
     *schedule = p->lastNbrPasses;
+    return SPHGPU_OK;
+  }
+  if (std::strcmp(stage, "neighbor cells") == 0) {
+    *schedule = p->lastNbrCells;
     return SPHGPU_OK;
   }
   if (std::strcmp(stage, "neighbor filter") == 0) {
@@ -1105,7 +1125,7 @@ int sphgpu_batch_kernel_launches(sphgpu_batch* b, int64_t* launches) {
 
 int sphgpu_batch_set_schedule(sphgpu_batch* b, const char* stage, int32_t schedule) {
   if (b == nullptr || stage == nullptr) return SPHGPU_ERR_ARG;
-  return set_schedule_impl(*b, &b->nbrSchedule, stage, schedule);
+  return set_schedule_impl(*b, &b->nbrSchedule, &b->nbrCells, stage, schedule);
 }
 
 int sphgpu_batch_autotune(sphgpu_batch* b, double report[8]) {

@@ -80,6 +80,7 @@ __device__ __forceinline__ Grid loadGrid(const Member& M) {
   g.dim[1] = (int)scalI(M.scal, SC_GRID + 5);
   g.dim[2] = (int)scalI(M.scal, SC_GRID + 6);
   g.filterTol = (float)s[7];
+  g.reach = (float)M.scal[SC_REACH];
   return g;
 }
 
@@ -312,13 +313,20 @@ __global__ void grid_kernel(const Member* mem, int nmem) {
     lo[a] = fmin(lo[a], fmin(p0, p1) - reach);
     hi[a] = fmax(hi[a], fmax(p0, p1) + reach);
   }
-  double cell = M.prm.kernelExtent*hmaxAll*1.001;
+  const int sub = M.grid.sub > 1 ? M.grid.sub : 1;
+  double cell = M.prm.kernelExtent*hmaxAll*1.001/sub;
   if (!(cell > 0.0) || !(cell < 1.0e300)) {
     atomicOr(M.err, DERR_NONPOSITIVE);
     cell = 1.0;
   }
   const int64_t maxCells = M.cellcap < ((int64_t)1 << 26) ? M.cellcap : ((int64_t)1 << 26);
   int64_t dim[3] = {1, 1, 1}, ncells = 1;
+  {
+    // cells at the natural size, for the next build's capacity
+    double want = 1.0;
+    for (int a = 0; a < 3; ++a) want *= fmin((hi[a] - lo[a])/cell + 1.0, (double)(1 << 20));
+    setScalI(M.scal, SC_CELLSWANTED, want < 1.0e15 ? (int64_t)want : (int64_t)1 << 50);
+  }
   for (int attempt = 0; attempt < 200; ++attempt) {
     ncells = 1;
     for (int a = 0; a < 3; ++a) {
@@ -337,6 +345,8 @@ __global__ void grid_kernel(const Member* mem, int nmem) {
   // largest h over smallest h of the problem (>= every node's condition number)
   const double spread = hmaxAll*M.scal[SC_LMAXALL];
   s[7] = (M.grid.filterTol > 0.0f && spread > 0.0 && spread <= 100.0) ? (double)M.grid.filterTol : 0.0;
+  // the largest kernel reach in cells (<= sub), for the walks' pruning
+  M.scal[SC_REACH] = M.prm.kernelExtent*hmaxAll/cell;
   setScalI(M.scal, SC_NCELLS, ncells);
   setScalI(M.scal, SC_MAXCOUNT, 0);
   setScalI(M.scal, SC_PAIRS, 0);
@@ -424,29 +434,51 @@ __device__ __forceinline__ Walker makeWalker(const Member& M, const NbrArrays& a
   return w;
 }
 
-// One x-row of up to three cells of the walk: its slot range and the ends of
-// its first two cells (a candidate's cell follows from its slot).
+// Distance, in cells, from a walker at fraction f of its cell to the cell d
+// cells away along one axis (0 for its own cell); a lower bound for every
+// node of that cell.
+__device__ __forceinline__ float axisGap(int d, float f) {
+  return d > 0 ? fmaxf(0.0f, (float)d - f) : (d < 0 ? fmaxf(0.0f, (float)(-d - 1) + f) : 0.0f);
+}
+
+// One x-row of the walk window: the candidate slot range [start, end) of its
+// cells x0..x1 (contiguous in the sorted order), trimmed with SUB > 1 to
+// the cells within the kernel reach, and the ends of its first cells (a
+// candidate's cell follows from its slot).
+template<int SUB>
 struct Row {
-  int64_t start, end, e0, e1;
+  int64_t start, end;
+  int64_t e[2*SUB];
   int x0;
-  float dyc, dzc;     // (cy' - cy)*cell, (cz' - cz)*cell in FP32
 };
 
-__device__ __forceinline__ Row loadRow(const int64_t* cellStart, const Grid& g, const Walker& w, int y, int z,
-                                       float cellf) {
-  const int x0 = w.cx > 0 ? w.cx - 1 : 0;
-  const int x1 = w.cx + 1 < g.dim[0] ? w.cx + 1 : g.dim[0] - 1;
+template<int SUB>
+__device__ __forceinline__ Row<SUB> loadRow(const Member& M, const Grid& g, const Walker& w, int y, int z,
+                                            float fx, float gyz, float rc2) {
+  int x0 = w.cx - SUB > 0 ? w.cx - SUB : 0;
+  int x1 = w.cx + SUB < g.dim[0] - 1 ? w.cx + SUB : g.dim[0] - 1;
+  if (SUB > 1) {
+    // the gaps grow with |x - cx|: trim the far cells at both ends
+    while (x0 < w.cx) { const float gx = axisGap(x0 - w.cx, fx); if (gx*gx + gyz <= rc2) break; ++x0; }
+    while (x1 > w.cx) { const float gx = axisGap(x1 - w.cx, fx); if (gx*gx + gyz <= rc2) break; --x1; }
+  }
+  const int64_t* cs = M.cellStart + (int64_t)(z*g.dim[1] + y)*g.dim[0] + x0;
   const int nx = x1 - x0 + 1;
-  const int64_t* cs = cellStart + (int64_t)(z*g.dim[1] + y)*g.dim[0] + x0;
-  Row row;
-  row.start = cs[0];
-  row.e0 = cs[1];
-  row.e1 = cs[nx < 2 ? nx : 2];
-  row.end = cs[nx];
-  row.x0 = x0;
-  row.dyc = (float)(y - w.cy)*cellf;
-  row.dzc = (float)(z - w.cz)*cellf;
-  return row;
+  Row<SUB> r;
+  r.x0 = x0;
+  r.start = cs[0];
+  r.end = cs[nx];
+#pragma unroll
+  for (int c = 0; c < 2*SUB; ++c) r.e[c] = c + 1 < nx ? cs[c + 1] : r.end;
+  return r;
+}
+
+template<int SUB>
+__device__ __forceinline__ float rowDxc(const Row<SUB>& r, const Walker& w, int64_t k, float cellf) {
+  int xc = r.x0 - w.cx;
+#pragma unroll
+  for (int c = 0; c < 2*SUB; ++c) xc += (k >= r.e[c]);
+  return (float)xc*cellf;
 }
 
 // The exact FP64 predicate for nodes i and j (the walks reach it for the
@@ -463,7 +495,8 @@ __device__ __forceinline__ bool exactTest(const Member& M, int32_t i, int32_t j,
 }
 
 // ConnectivityMap predicate |H_i r_ij|^2 <= kappa^2 || |H_j r_ij|^2 <= kappa^2
-// (src/Neighbor/ConnectivityMapInline.hh:169-186) for candidate slot k.
+// (src/Neighbor/ConnectivityMapInline.hh:169-186) for candidate slot k, whose
+// cell corner lies at (dxc, dyc, dzc) from the walker's (FP32).
 // With tol > 0 a FP32 pre-test decides every pair whose eta^2 lies clearly
 // outside the band kappa^2 (1 -+ tol): eta_i^2 from the FP32 H_i, eta_j^2
 // bounded by min/max eig(H_j)^2 |r_ij|^2, r_ij from the cell offsets.  The
@@ -471,12 +504,12 @@ __device__ __forceinline__ bool exactTest(const Member& M, int32_t i, int32_t j,
 // tol (1e-3) is only set when that ratio is <= 100, so it never decides a
 // pair the exact test would decide otherwise.  Undecided pairs take the
 // exact FP64 test in the reference's operation order.
-__device__ __forceinline__ bool candTest(const Member& M, const NbrArrays& a, const Walker& w, const Row& row,
-                                         int64_t k, float cellf, double k2, float k2lo, float k2hi, bool pretest) {
+__device__ __forceinline__ bool candTest(const Member& M, const NbrArrays& a, const Walker& w, int64_t k,
+                                         float dxc, float dyc, float dzc, double k2, float k2lo, float k2hi,
+                                         bool pretest) {
   if (pretest) {
     const float4 c = __ldg(a.pre + k);
-    const float dxc = (float)(row.x0 - w.cx + (k >= row.e0) + (k >= row.e1))*cellf;
-    const float fx = (w.ox - c.x) - dxc, fy = (w.oy - c.y) - row.dyc, fz = (w.oz - c.z) - row.dzc;
+    const float fx = (w.ox - c.x) - dxc, fy = (w.oy - c.y) - dyc, fz = (w.oz - c.z) - dzc;
     const float e2i = symEta2F(w.hf, fx, fy, fz);
     if (e2i <= k2lo) return true;
     const float r2 = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, fz*fz));
@@ -521,8 +554,8 @@ __global__ void __launch_bounds__(kGhostThreads) cell_scatter_kernel(const Membe
 // pass too and stores them ascending in the stash, element c of sorted slot s
 // at stash[c*stashStride + s]; nbr_compact_thread_kernel then moves them to
 // offsets[i], and the FILL pass does not run for it.
-template<bool FILL>
-__global__ void __launch_bounds__(256) nbr_thread_kernel(const Member* mem, BlockMap bm, int cap, int maxNbr) {
+template<bool FILL, int SUB>
+__global__ void __launch_bounds__(256, SUB == 1 ? 3 : 1) nbr_thread_kernel(const Member* mem, BlockMap bm, int cap, int maxNbr) {
   extern __shared__ int32_t lst[];
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
@@ -549,15 +582,26 @@ __global__ void __launch_bounds__(256) nbr_thread_kernel(const Member* mem, Bloc
     const float k2lo = k2f*(1.0f - g.filterTol), k2hi = k2f*(1.0f + g.filterTol);
     const float cellf = (float)g.cell;
     const int32_t i = me.idx;
-    for (int dz = -1; dz <= 1; ++dz) {
+    // window of +-SUB cells; with SUB > 1 the rows and cells farther than the
+    // largest kernel reach (in cells, with a margin) are skipped
+    const float rc2 = g.reach*g.reach*1.0001f;
+    const float fx = me.ox/cellf, fy = me.oy/cellf, fz = me.oz/cellf;
+    for (int dz = -SUB; dz <= SUB; ++dz) {
       const int z = me.cz + dz;
       if (z < 0 || z >= g.dim[2]) continue;
-      for (int dy = -1; dy <= 1; ++dy) {
+      const float gz = axisGap(dz, fz);
+      const float dzc = (float)dz*cellf;
+      for (int dy = -SUB; dy <= SUB; ++dy) {
         const int y = me.cy + dy;
         if (y < 0 || y >= g.dim[1]) continue;
-        const Row row = loadRow(M.cellStart, g, me, y, z, cellf);
-        for (int64_t k = row.start; k < row.end; ++k) {
-          if (k != s && candTest(M, a, me, row, k, cellf, k2, k2lo, k2hi, pretest)) {
+        const float gy = axisGap(dy, fy);
+        const float gyz = gy*gy + gz*gz;
+        if (SUB > 1 && gyz > rc2) continue;
+        const float dyc = (float)dy*cellf;
+        const Row<SUB> row = loadRow<SUB>(M, g, me, y, z, fx, gyz, rc2);
+        {
+          for (int64_t k = row.start; k < row.end; ++k) {
+          if (k != s && candTest(M, a, me, k, rowDxc<SUB>(row, me, k, cellf), dyc, dzc, k2, k2lo, k2hi, pretest)) {
             if (collect) {
               const int32_t j = __ldg(M.sortedIdx + k);
               if (count < lcap) {
@@ -573,6 +617,7 @@ __global__ void __launch_bounds__(256) nbr_thread_kernel(const Member* mem, Bloc
               above += (j > i);
             }
             ++count;
+          }
           }
         }
       }
@@ -656,8 +701,8 @@ __global__ void __launch_bounds__(256) nbr_compact_warp_kernel(const Member* mem
 // (Grid::stashCap > 0) collects and sorts in the COUNT pass and stores the
 // list of node i at stash[i*stashCap]; nbr_compact_warp_kernel moves it to
 // offsets[i].
-template<bool FILL>
-__global__ void __launch_bounds__(256) nbr_walk_kernel(const Member* mem, BlockMap bm, int cap, int maxNbr) {
+template<bool FILL, int SUB>
+__global__ void __launch_bounds__(256, SUB == 1 ? 3 : 1) nbr_walk_kernel(const Member* mem, BlockMap bm, int cap, int maxNbr) {
   extern __shared__ int32_t sbuf_all[];
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
@@ -678,18 +723,26 @@ __global__ void __launch_bounds__(256) nbr_walk_kernel(const Member* mem, BlockM
   const bool pretest = g.filterTol > 0.0f;
   const float k2lo = k2f*(1.0f - g.filterTol), k2hi = k2f*(1.0f + g.filterTol);
   const float cellf = (float)g.cell;
+  const float rc2 = g.reach*g.reach*1.0001f;
+  const float fx = me.ox/cellf, fy = me.oy/cellf, fz = me.oz/cellf;
   int count = 0;
-  for (int dz = -1; dz <= 1; ++dz) {
+  for (int dz = -SUB; dz <= SUB; ++dz) {
     const int z = me.cz + dz;
     if (z < 0 || z >= g.dim[2]) continue;
-    for (int dy = -1; dy <= 1; ++dy) {
+    const float gz = axisGap(dz, fz);
+    const float dzc = (float)dz*cellf;
+    for (int dy = -SUB; dy <= SUB; ++dy) {
       const int y = me.cy + dy;
       if (y < 0 || y >= g.dim[1]) continue;
-      // the x-cells of a row are contiguous in the sorted order
-      const Row row = loadRow(M.cellStart, g, me, y, z, cellf);
+      const float gy = axisGap(dy, fy);
+      const float gyz = gy*gy + gz*gz;
+      if (SUB > 1 && gyz > rc2) continue;
+      const float dyc = (float)dy*cellf;
+      const Row<SUB> row = loadRow<SUB>(M, g, me, y, z, fx, gyz, rc2);
       for (int64_t base = row.start; base < row.end; base += 32) {
         const int64_t k = base + lane;
-        const bool pass = k < row.end && k != s && candTest(M, a, me, row, k, cellf, k2, k2lo, k2hi, pretest);
+        const bool pass = k < row.end && k != s &&
+                          candTest(M, a, me, k, rowDxc<SUB>(row, me, k, cellf), dyc, dzc, k2, k2lo, k2hi, pretest);
         const unsigned ballot = __ballot_sync(0xffffffffu, pass);
         if (collect && pass) {
           const int pos = count + __popc(ballot & ((1u << lane) - 1u));
@@ -768,10 +821,28 @@ int plan_capacities(Batch& b) {
     // sizes of the last build, else the caller's hints, else built-in guesses
     const int64_t G = p.G > 0 ? p.G : p.hintG;
     const int64_t E = p.E > 0 ? p.E : p.hintE;
-    const int64_t cells = p.ncells > 0 ? p.ncells : p.hintCells;
     if (G > 0) SPH_TRY(ensure_capacity_ghosts(p, grow(G)));
+    // schedule: a warp per node once the 27-cell candidate set of the last
+    // build kept 32 lanes busy, or once a thread's list would not fit in
+    // shared memory
+    const int lastSub = p.lastNbrCells > 0 ? p.lastNbrCells : 1;
+    const double cells1 = p.cellsWanted > 0 ? (double)p.cellsWanted/(double)(lastSub*lastSub*lastSub) : 0.0;
+    const double candPerNode = cells1 > 0.0 ? 27.0*(double)(p.n + p.G)/cells1 : 0.0;
+    const int req = p.nbrSchedule != NBR_SCHEDULE_AUTO ? p.nbrSchedule : b.nbrSchedule;
+    p.fillSchedule = (req == NBR_SCHEDULE_WARP || (req == NBR_SCHEDULE_AUTO && candPerNode > 384.0) ||
+                      sizeof(int32_t)*32*(size_t)(p.fillCap > 8 ? p.fillCap : 64) > kMaxListSmem)
+                         ? NBR_SCHEDULE_WARP : NBR_SCHEDULE_THREAD;
+    // cells per kernel reach: one unless requested (half-reach cells test
+    // fewer candidates but walk more rows; the autotuner measures both)
+    const int reqCells = p.nbrCells != 0 ? p.nbrCells : b.nbrCells;
+    p.grid.sub = reqCells != 0 ? reqCells : 1;
+    const int sub = p.grid.sub;
+    // cells the grid wants at this subdivision (the last build's, rescaled), else the hint
+    const int64_t cells = cells1 > 0.0 ? (int64_t)(cells1*sub*sub*sub) + 1 : p.hintCells;
+    // grow (with slack) only when the buffers hold less than the wanted cells
     const int64_t cellsNeed = cells > 0 ? grow(cells) : p.candcap/2 + 64;
-    if (cellsNeed + 1 > p.cellcap) {
+    const int64_t cellsMin = cells > 0 ? cells + cells/32 + 64 : cellsNeed;
+    if (cellsMin + 1 > p.cellcap) {
       cudaStreamSynchronize(b.stream);
       cudaFree(p.cellStart); cudaFree(p.cellFill);
       p.cellStart = nullptr; p.cellFill = nullptr;
@@ -788,14 +859,8 @@ int plan_capacities(Batch& b) {
     if (p.fillCap < 8) p.fillCap = p.maxCount > 0 ? p.maxCount + p.maxCount/4 + 8 : 64;
     if (kScanBlocks + 1 > p.blockSumsCap) SPH_TRY(ensure_block_sums(p, kScanBlocks + 1));
     if (p.gcap != oldg || p.candcap != oldc || p.ecap != olde || p.cellcap != oldcells) b.memDirty = true;
-    // schedule: a warp per node once the 27-cell candidate set of the last
-    // build kept 32 lanes busy, or once a thread's list would not fit in
-    // shared memory
-    const double candPerNode = p.ncells > 0 ? 27.0*(double)(p.n + p.G)/(double)p.ncells : 0.0;
-    const int req = p.nbrSchedule != NBR_SCHEDULE_AUTO ? p.nbrSchedule : b.nbrSchedule;
-    p.fillSchedule = (req == NBR_SCHEDULE_WARP || (req == NBR_SCHEDULE_AUTO && candPerNode > 384.0) ||
-                      sizeof(int32_t)*32*(size_t)p.fillCap > kMaxListSmem)
-                         ? NBR_SCHEDULE_WARP : NBR_SCHEDULE_THREAD;
+    if (p.fillSchedule == NBR_SCHEDULE_THREAD && sizeof(int32_t)*32*(size_t)p.fillCap > kMaxListSmem)
+      p.fillSchedule = NBR_SCHEDULE_WARP;
     p.grid.filterTol = p.nbrFilter ? kFilterTol : 0.0f;
     // single pass: the lists go to the pair-acceleration buffer (free until
     // the next derivative evaluation rewrites it) when they fit there
@@ -903,25 +968,10 @@ int launch_build(Batch& b) {
   // a thread's list lives in shared memory: fewer threads per block for long lists
   int fthreads = 256;
   while (fthreads > 32 && sizeof(int32_t)*(size_t)fthreads*tcap > 96*1024) fthreads >>= 1;
-  const int tthreads = tstash ? fthreads : 256;
   // bitonic sort pads each warp's list to a power of two >= 32
   int wcap = 32;
   while (wcap < wmax) wcap <<= 1;
   auto thread = [](const Problem& p) { return p.fillSchedule != NBR_SCHEDULE_WARP; };
-  BlockMap tmap, wmap, fmap, wfmap, ctmap, cwmap;
-  unsigned tgrid = 0, wgrid = 0, fgrid = 0, wfgrid = 0, ctgrid = 0, cwgrid = 0;
-  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return thread(p) ? p.candcap : (int64_t)0; },
-                          tthreads, &tmap, &tgrid));
-  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return thread(p) ? (int64_t)0 : 32*p.candcap; },
-                          wthreads, &wmap, &wgrid));
-  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return thread(p) && !p.grid.stashCap ? p.candcap : (int64_t)0; },
-                          fthreads, &fmap, &fgrid));
-  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return !thread(p) && !p.grid.stashCap ? 32*p.candcap : (int64_t)0; },
-                          wthreads, &wfmap, &wfgrid));
-  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return thread(p) && p.grid.stashCap ? p.candcap : (int64_t)0; },
-                          256, &ctmap, &ctgrid));
-  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return !thread(p) && p.grid.stashCap ? 32*p.n : (int64_t)0; },
-                          256, &cwmap, &cwgrid));
   for (Problem* p : b.mem) {
     p->lastNbrSchedule = p->fillSchedule;
     p->lastNbrPasses = p->grid.stashCap > 0 ? 1 : 2;
@@ -929,33 +979,69 @@ int launch_build(Batch& b) {
   b.lastNbrSchedule = nm ? b.mem[0]->lastNbrSchedule : 0;
   const size_t tsmem = sizeof(int32_t)*(size_t)fthreads*tcap;
   const size_t wsmem = sizeof(int32_t)*(wthreads/32)*(size_t)wcap;
-  if (tsmem > 48*1024) {
-    for (auto* k : {nbr_thread_kernel<false>, nbr_thread_kernel<true>}) {
-      const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
-      if (e != cudaSuccess) return cuda_status(e, "nbr smem attribute");
+  auto smemAttr = [](auto* kernel, size_t bytes) -> int {
+    if (bytes <= 48*1024) return SPHGPU_OK;
+    return cuda_status(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+                       "nbr smem attribute");
+  };
+  SPH_TRY(smemAttr(nbr_thread_kernel<false, 1>, tsmem)); SPH_TRY(smemAttr(nbr_thread_kernel<true, 1>, tsmem));
+  SPH_TRY(smemAttr(nbr_thread_kernel<false, 2>, tsmem)); SPH_TRY(smemAttr(nbr_thread_kernel<true, 2>, tsmem));
+  SPH_TRY(smemAttr(nbr_walk_kernel<false, 1>, wsmem)); SPH_TRY(smemAttr(nbr_walk_kernel<true, 1>, wsmem));
+  SPH_TRY(smemAttr(nbr_walk_kernel<false, 2>, wsmem)); SPH_TRY(smemAttr(nbr_walk_kernel<true, 2>, wsmem));
+  // One walk launch per (schedule, cell subdivision) present.  pass 0: count
+  // (and the lists of members with a stash); pass 1: fill (members without).
+  auto walk = [&](bool threadSched, int sub, bool fill) -> int {
+    BlockMap map;
+    unsigned grid = 0;
+    const int threads = threadSched ? (fill || tstash ? fthreads : 256) : wthreads;
+    SPH_TRY(batch_map_items(b, [&](const Problem& p) {
+      if (thread(p) != threadSched || p.grid.sub != sub || (fill && p.grid.stashCap)) return (int64_t)0;
+      return threadSched ? p.candcap : 32*p.candcap; }, threads, &map, &grid));
+    if (!grid) return SPHGPU_OK;
+    if (threadSched) {
+      const bool lists = fill || tstash;
+      const size_t smem = lists ? tsmem : 0;
+      const int c = lists ? tcap : 0;
+      if (sub == 1) {
+        if (fill) nbr_thread_kernel<true, 1><<<grid, threads, smem, st>>>(b.d_mem, map, c, maxNbr);
+        else nbr_thread_kernel<false, 1><<<grid, threads, smem, st>>>(b.d_mem, map, c, maxNbr);
+      } else {
+        if (fill) nbr_thread_kernel<true, 2><<<grid, threads, smem, st>>>(b.d_mem, map, c, maxNbr);
+        else nbr_thread_kernel<false, 2><<<grid, threads, smem, st>>>(b.d_mem, map, c, maxNbr);
+      }
+    } else {
+      const bool lists = fill || wstash;
+      const size_t smem = lists ? wsmem : 0;
+      const int c = lists ? wcap : 0;
+      if (sub == 1) {
+        if (fill) nbr_walk_kernel<true, 1><<<grid, threads, smem, st>>>(b.d_mem, map, c, maxNbr);
+        else nbr_walk_kernel<false, 1><<<grid, threads, smem, st>>>(b.d_mem, map, c, maxNbr);
+      } else {
+        if (fill) nbr_walk_kernel<true, 2><<<grid, threads, smem, st>>>(b.d_mem, map, c, maxNbr);
+        else nbr_walk_kernel<false, 2><<<grid, threads, smem, st>>>(b.d_mem, map, c, maxNbr);
+      }
     }
-  }
-  if (wsmem > 48*1024) {
-    for (auto* k : {nbr_walk_kernel<false>, nbr_walk_kernel<true>}) {
-      const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem);
-      if (e != cudaSuccess) return cuda_status(e, "nbr smem attribute");
-    }
-  }
-  // count pass (and the lists of members with a stash)
-  if (tgrid) {
-    nbr_thread_kernel<false><<<tgrid, tthreads, tstash ? tsmem : 0, st>>>(b.d_mem, tmap, tstash ? tcap : 0, maxNbr);
     batch_count_launch(b);
-  }
-  if (wgrid) {
-    nbr_walk_kernel<false><<<wgrid, wthreads, wstash ? wsmem : 0, st>>>(b.d_mem, wmap, wstash ? wcap : 0, maxNbr);
-    batch_count_launch(b);
+    return SPHGPU_OK;
+  };
+  for (int sub = 1; sub <= 2; ++sub) {
+    SPH_TRY(walk(true, sub, false));
+    SPH_TRY(walk(false, sub, false));
   }
   SPH_TRY(batch_scan(b, SCAN_COUNTS));
   // lists to the CSR: compaction of the stashes, fill pass for the rest
+  BlockMap ctmap, cwmap;
+  unsigned ctgrid = 0, cwgrid = 0;
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return thread(p) && p.grid.stashCap ? p.candcap : (int64_t)0; },
+                          256, &ctmap, &ctgrid));
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return !thread(p) && p.grid.stashCap ? 32*p.n : (int64_t)0; },
+                          256, &cwmap, &cwgrid));
   if (ctgrid) { nbr_compact_thread_kernel<<<ctgrid, 256, 0, st>>>(b.d_mem, ctmap); batch_count_launch(b); }
   if (cwgrid) { nbr_compact_warp_kernel<<<cwgrid, 256, 0, st>>>(b.d_mem, cwmap); batch_count_launch(b); }
-  if (fgrid) { nbr_thread_kernel<true><<<fgrid, fthreads, tsmem, st>>>(b.d_mem, fmap, tcap, maxNbr); batch_count_launch(b); }
-  if (wfgrid) { nbr_walk_kernel<true><<<wfgrid, wthreads, wsmem, st>>>(b.d_mem, wfmap, wcap, maxNbr); batch_count_launch(b); }
+  for (int sub = 1; sub <= 2; ++sub) {
+    SPH_TRY(walk(true, sub, true));
+    SPH_TRY(walk(false, sub, true));
+  }
   return cuda_status(cudaGetLastError(), "neighbor build");
 }
 
@@ -972,19 +1058,21 @@ int build_connectivity(Batch& b) {
   for (int attempt = 0; attempt < 6; ++attempt) {
     SPH_TRY(plan_capacities(b));
     SPH_TRY(launch_build(b));
-    const int slots[6] = {SC_G, SC_TOTAL, SC_MAXCOUNT, SC_PAIRS, SC_NCELLS, -1};
+    const int slots[7] = {SC_G, SC_TOTAL, SC_MAXCOUNT, SC_PAIRS, SC_NCELLS, SC_CELLSWANTED, -1};
     std::vector<double> r;
-    SPH_TRY(batch_gather(b, slots, 6, r));
+    SPH_TRY(batch_gather(b, slots, 7, r));
     bool redo = false;
     for (int m = 0; m < nm; ++m) {
       Problem& p = *b.mem[m];
-      const int herr = (int)r[m*6 + 5];
-      p.G = asI64(r[m*6]);
+      const int herr = (int)r[m*7 + 6];
+      p.G = asI64(r[m*7]);
       p.ntot = p.n + p.G;
-      p.E = asI64(r[m*6 + 1]);
-      p.maxCount = asI32(r[m*6 + 2]);
-      p.pairs = asI64(r[m*6 + 3]);
-      p.ncells = asI64(r[m*6 + 4]);
+      p.E = asI64(r[m*7 + 1]);
+      p.maxCount = asI32(r[m*7 + 2]);
+      p.pairs = asI64(r[m*7 + 3]);
+      p.ncells = asI64(r[m*7 + 4]);
+      p.cellsWanted = asI64(r[m*7 + 5]);
+      p.lastNbrCells = p.grid.sub;
       if (herr) cudaMemsetAsync(p.d_err, 0, sizeof(int), b.stream);
       if ((herr & DERR_NBR_CAPACITY) || p.maxCount > p.maxNbr) {
         set_error("a node has more neighbors than max_neighbors");

@@ -126,6 +126,8 @@ struct Grid {
   int stashCap;        // lists built in the count pass, at most this long, kept in the
                        // pair-acceleration buffer until compacted (0: separate fill pass)
   int64_t stashStride; // thread schedule: element c of sorted slot s at c*stashStride + s
+  int sub;             // cells per kernel reach (1: 27-cell walk, 2: 125-cell walk with pruning)
+  float reach;         // kernel reach kappa*max(1/min(eig(H))) in cells (device-side, per build)
 };
 
 struct Batch;
@@ -146,6 +148,8 @@ struct Problem {
   int lastNbrSchedule = 0;  // schedule the last build used
   bool nbrFilter = true;    // FP32 pre-test in the neighbor walk (exact either way)
   bool nbrStash = true;     // single-pass neighbor walk when the lists fit the stash
+  int nbrCells = 0;         // cells per kernel reach requested (0 auto, 1, 2)
+  int lastNbrCells = 0;     // cells per kernel reach of the last build
   int lastNbrPasses = 0;    // walks over the candidates the last build made (1 or 2)
   int fillCap = 0;          // neighbor-list capacity planned for the fill pass
   int fillSchedule = 0;     // schedule planned for this build (NBR_SCHEDULE_THREAD/WARP)
@@ -176,6 +180,7 @@ struct Problem {
   int32_t* cellFill = nullptr;  // [ncells]
   int64_t cellcap = 0;
   int64_t ncells = 0;
+  int64_t cellsWanted = 0;      // cells of the last grid at its natural size
   int64_t ntot = 0;             // n + ghosts created so far (ghost passes)
   Grid grid{};
 
@@ -264,6 +269,8 @@ enum ScalSlot {
   SC_NCELLS = 27,      // cells of the grid
   SC_GRID = 28,        // lo[3], cell (doubles), dim[3] (i64), pre-test tolerance
   SC_NNEAR = 36,       // internal nodes near a periodic plane (the boundary passes' list)
+  SC_REACH = 37,       // kernel reach in cells of the current grid
+  SC_CELLSWANTED = 38, // cells of the grid at its natural cell size (i64)
   NSCAL = 40
 };
 
@@ -338,6 +345,7 @@ struct Batch {
   int64_t gathercap = 0;
   int64_t launches = 0;
   int nbrSchedule = 0;           // requested neighbor-walk schedule
+  int nbrCells = 0;              // requested cells per kernel reach (0 auto)
   int lastNbrSchedule = 0;
   int evalThreads = 128;         // threads per block of the pair-loop kernels (64, 128 or 256)
   // CUDA-graph replay of the part of the RK2 step after the connectivity

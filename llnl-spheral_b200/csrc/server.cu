@@ -67,7 +67,8 @@ Estimate estimate_sizes(const sphgpu_config& c, int64_t n, const double* pos, co
     if (hmin > 0.0) hmax = std::max(hmax, 1.0/hmin);
   }
   const double reach = kernel_extent(c.kernel)*hmax;
-  const double cell = reach*1.001;
+  // cells of half a kernel reach (the finest subdivision the neighbor walk uses)
+  const double cell = reach*1.001/2.0;
   double vol = 1.0, ext = 1.0, cells = 1.0;
   for (int a = 0; a < 3; ++a) {
     const double L = c.periodic[a] ? c.xmax[a] - c.xmin[a] : std::max(hi[a] - lo[a], reach);

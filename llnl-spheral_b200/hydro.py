@@ -37,7 +37,9 @@ def _p(a):
 
 
 def _tune_report(out):
+    best = min(out[1], out[2])
     return {"neighbor walk": int(out[0]), "neighbor walk ms": {"thread": out[1], "warp": out[2]},
+            "neighbor cells": int(out[6]), "neighbor cells ms": {1: best, 2: out[7]},
             "pair loop": int(out[3]), "pair loop ms": {64: out[4], 128: out[5]}}
 
 

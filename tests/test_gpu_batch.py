@@ -120,6 +120,7 @@ def test_autotune_keeps_results(gpu_lib, pkg):
     batch.build_neighbors()
     rep = batch.autotune()
     assert rep["neighbor walk"] in (1, 2) and rep["pair loop"] in (64, 128, 256)
+    assert rep["neighbor cells"] in (1, 2) and rep["neighbor cells ms"][2] > 0
     assert all(v > 0 for v in rep["neighbor walk ms"].values())
     batch.step(2)
     for s in solo:

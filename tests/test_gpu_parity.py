@@ -71,17 +71,22 @@ def test_connectivity_bitexact(gpu_lib, pkg, oracle_mod, case):
 @pytest.mark.parametrize("schedule", [1, 2])
 @pytest.mark.parametrize("nfilter", [0, 1])
 @pytest.mark.parametrize("passes", [1, 2])
-def test_connectivity_every_schedule(gpu_lib, pkg, oracle_mod, case, schedule, nfilter, passes):
+@pytest.mark.parametrize("cells", [1, 2])
+def test_connectivity_every_schedule(gpu_lib, pkg, oracle_mod, case, schedule, nfilter, passes, cells):
     """Thread-per-node and warp-per-node neighbor walks, with and without the
     FP32 pre-test, in one pass (lists parked in the pair-acceleration buffer,
-    then compacted) or two (count, then fill), give the same CSR."""
+    then compacted) or two (count, then fill), over cells of one kernel reach
+    (27-cell window) or half a reach (125-cell window with distance pruning),
+    give the same CSR."""
     g, o, ns = _pair(pkg, oracle_mod, case)
     g.set_schedule("neighbor walk", schedule)
     g.set_schedule("neighbor filter", nfilter)
     g.set_schedule("neighbor passes", passes)
+    g.set_schedule("neighbor cells", cells)
     g.build_neighbors()
     assert g.schedule("neighbor walk") == schedule
     assert g.schedule("neighbor passes") == passes
+    assert g.schedule("neighbor cells") == cells
     o.build_neighbors()
     go, gn, gr = g.connectivity()
     oo, on, orr = o.connectivity()
@@ -226,7 +231,8 @@ def test_empty_problem_rejected(gpu_lib, pkg):
 
 
 @pytest.mark.parametrize("nfilter", [0, 1])
-def test_connectivity_anisotropic_h(gpu_lib, pkg, oracle_mod, nfilter):
+@pytest.mark.parametrize("cells", [1, 2])
+def test_connectivity_anisotropic_h(gpu_lib, pkg, oracle_mod, nfilter, cells):
     """Anisotropic, varied H (condition numbers up to ~2) with the eta_i OR
     eta_j predicate: many candidates sit near the support boundary."""
     gen, abi = pkg.generators, pkg.abi
@@ -241,6 +247,7 @@ def test_connectivity_anisotropic_h(gpu_lib, pkg, oracle_mod, nfilter):
     cfg = gen.sod_config(abi, ns_box=box)
     g = pkg.SPHHydro(cfg, ns)
     g.set_schedule("neighbor filter", nfilter)
+    g.set_schedule("neighbor cells", cells)
     o = oracle_mod.OracleProblem(cfg, ns)
     g.build_neighbors()
     o.build_neighbors()
