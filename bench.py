@@ -62,6 +62,25 @@ def parse():
     return ap.parse_args()
 
 
+# Algorithmic bytes of one mixed-form evaluateDerivatives (record pack + pair
+# kernel): the pack reads 136 B of state per internal node (position,
+# velocity, m, rho, cs, P, omega, H) and writes a 112-byte record per node and
+# ghost; the pair kernel reads those records, writes 54 derivative doubles
+# per internal node (432 B; the reference's "internal velocity gradient" and
+# "local M" equal the velocity gradient and M for one NodeList and are not
+# stored twice), reads 4 B of CSR index and writes 24 B of pair acceleration
+# per directed entry.
+def eval_alg_bytes(nodes, ghosts, entries):
+    return nodes * 136 + 2 * (nodes + ghosts) * 112 + nodes * 432 + 28 * entries
+
+
+# DRAM traffic (read + write) of pack_mixed_kernel + sph_eval_mixed_kernel
+# measured by ncu on Kelvin-Helmholtz 96^3 (884,736 nodes, 56,456 ghosts,
+# 5,363,712 entries); scaled to other sizes by the algorithmic bytes.
+EVAL_TRAFFIC_96 = 157972224 + 74632448 + 204818688 + 463323136
+EVAL_UNITS_96 = (884736, 56456, 5363712)
+
+
 def kh_problem(pkg, nx, nz=None, seed=20261203):
     gen, abi = pkg.generators, pkg.abi
     nz = nz or nx
@@ -609,8 +628,9 @@ def run_ours(args):
     t_build_mixed = measure_build(hm)
     t_build_plain = measure_build(hp)
     nodes, ghosts, entries = ns.n, g.value, e.value
-    alg_bytes = (nodes + ghosts) * 152 + nodes * 576 + 4 * entries
+    alg_bytes = eval_alg_bytes(nodes, ghosts, entries)
     achieved = alg_bytes / (t_eval_mixed / 1e3) / 1e9
+    traffic = EVAL_TRAFFIC_96 * alg_bytes / eval_alg_bytes(*EVAL_UNITS_96)
     result = None
     if rank == 0:
         lat = sorted(rm["per_step_ms"])
@@ -636,7 +656,10 @@ def run_ours(args):
             "mixed_over_plain": value / plain_value,
             "roofline": {"bound": "hbm", "kernel": "evaluateDerivatives (record pack + sph_eval_mixed)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": traffic,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of pack_mixed_kernel + "
+                                           "sph_eval_mixed_kernel on Kelvin-Helmholtz 96^3, scaled by the "
+                                           "algorithmic bytes",
                          "algorithmic_bytes": alg_bytes, "eval_ms": t_eval_mixed},
             "gpu_launches": rm["launches"],
             "clocks": rm["clocks"],

@@ -2,9 +2,10 @@
  * sphgpu.h -- C ABI of the B200 SPH/CRKSPH hydro derivative path.
  *
  * This is the drop-in boundary for Spheral's fluid-hydro hot path.  A thin
- * C++ adapter (GpuSPHHydroBase<Dim<3>>, shown in INTEGRATION.md) implements
- * the Physics<Dim<3>> virtuals of the reference by calling these entry
- * points, so the reference's integrators and drivers keep working unchanged.
+ * C++ adapter (a GpuSPHHydroBase<Dim<3>> derived from GenericHydro<Dim<3>>)
+ * implements the Physics<Dim<3>> virtuals of the reference by calling these
+ * entry points, so the reference's integrators and drivers keep working
+ * unchanged.
  *
  * Conventions (all entry points):
  *   - every call returns SPHGPU_OK (0) or a negative SPHGPU_ERR_* code; no
