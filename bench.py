@@ -439,34 +439,49 @@ def batch_specs(pkg, count, seed=20261203, nmin=4096, nmax=262144):
     return out
 
 
-def measure_batch(pkg, count, steps, warmup):
+def measure_batch(pkg, count, steps, warmup, rank=0, world=1):
     """Batched ensemble: every stage one launch over all members (autotuned),
     against the same problems stepped one at a time (one launch per problem
-    per stage)."""
+    per stage).  With N GPUs the tubes are placed by size (longest first onto
+    the least-loaded rank; no exchange on the data path); each rank times
+    its batch with CUDA events on the batch stream, and the line takes the
+    max over ranks and the sum of the pairs."""
     import torch
     specs = batch_specs(pkg, count)
+    place = pkg.sharding.partition_by_cost([ns.n for ns, _ in specs], world)
+    mine = pkg.sharding.local_items(place, rank)
+    specs = [specs[k] for k in mine]
     probs = [pkg.SPHHydro(cfg, ns) for ns, cfg in specs]
-    nodes = sum(ns.n for ns, _ in specs)
+    nodes = allsum(sum(ns.n for ns, _ in specs), world)
     batch = pkg.SPHBatch(probs)
     batch.build_neighbors()
     batch.evaluateDerivatives()
     tune = batch.autotune()
+    stream = torch.cuda.ExternalStream(batch.stream())
     for _ in range(warmup):
         batch.step(1)
     torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     l0 = batch.kernel_launches()
-    t0 = time.perf_counter()
+    e0.record(stream)
     pairs = 0
     for _ in range(steps):
         batch.step(1)
         pairs += batch.num_pairs()
+    e1.record(stream)
     torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
+    barrier(world)
+    t_batch = allmax(e0.elapsed_time(e1) / 1e3, world)
+    pairs = allsum(pairs, world)
     launches = batch.kernel_launches() - l0
+    # one launch sequence per problem, each on its own stream: host clock
+    # around device synchronisation
     for _ in range(warmup):
         for p in probs:
             p.step(1)
     torch.cuda.synchronize()
+    barrier(world)
     t0 = time.perf_counter()
     lpairs = 0
     for _ in range(steps):
@@ -474,7 +489,8 @@ def measure_batch(pkg, count, steps, warmup):
             p.step(1)
             lpairs += p.num_pairs()
     torch.cuda.synchronize()
-    t_loop = time.perf_counter() - t0
+    t_loop = allmax(time.perf_counter() - t0, world)
+    lpairs = allsum(lpairs, world)
     batch.close()
     for p in probs:
         p.close()
@@ -489,26 +505,45 @@ def measure_batch(pkg, count, steps, warmup):
             "config": {"workload": "%d Sod-type tubes, n log-uniform in [4096, 262144] (8k x k x k), "
                                    "gamma ~ U[1.3, 1.67], density ratio ~ U[2, 8], cubic B-spline nPerh 1.51, "
                                    "mixed form, fixed dt 1e-4" % count,
-                       "nodes": nodes, "steps": steps, "warmup": warmup}}
+                       "nodes": nodes, "steps": steps, "warmup": warmup,
+                       "placement": "tubes placed on %d GPU(s) by size, no data-path exchange" % world}}
 
 
-def measure_serving(pkg, duration, nsteps, rate=20.0, budget=150e9):
+def measure_serving(pkg, duration, nsteps, rate=20.0, budget=150e9, rank=0, world=1):
     """Continuous-batching request loop on a seeded Poisson trace, mixed form
-    and plain FP64 on the same trace."""
+    and plain FP64 on the same trace.  With N GPUs every rank routes the
+    trace identically (least outstanding estimated work at arrival) and
+    serves its share; times to completion and pairs are gathered to rank 0."""
     s = pkg.serving
     trace = s.poisson_trace(rate=rate, duration=duration, nsteps=nsteps)
+    route = pkg.sharding.route_requests([r["arrival"] for r in trace],
+                                        [r["n"] * r["nsteps"] * 1.0e-8 for r in trace], world)
+    mine = [trace[k] for k in pkg.sharding.local_items(route, rank)]
     out = {}
     for name, prec in (("mixed", pkg.abi.PRECISION_MIXED), ("plain_fp64", pkg.abi.PRECISION_FP64)):
-        ttc, makespan, stats = s.serve(trace, prec, budget_bytes=budget)
-        t = np.array(ttc)
+        barrier(world)
+        ttc, makespan, stats = s.serve(mine, prec, budget_bytes=budget) if mine else ([], 0.0, None)
+        local = {"ttc": ttc, "makespan": makespan,
+                 "pairs": stats["pair_interactions"] if stats else 0.0,
+                 "completed": int(stats["completed"]) if stats else 0,
+                 "peak": stats["peak_bytes"] if stats else 0.0,
+                 "ticks": int(stats["ticks"]) if stats else 0}
+        parts = [local]
+        if world > 1:
+            import torch.distributed as dist
+            parts = [None] * world
+            dist.all_gather_object(parts, local)
+        t = np.array([x for p in parts for x in p["ttc"]])
+        span = max(p["makespan"] for p in parts)
         out[name] = {"ttc_p50_s": float(np.percentile(t, 50)), "ttc_p99_s": float(np.percentile(t, 99)),
-                     "pair_interactions_per_s": stats["pair_interactions"] / makespan, "makespan_s": makespan,
-                     "completed": int(stats["completed"]), "peak_device_gb": stats["peak_bytes"] / 1e9,
-                     "batched_steps": int(stats["ticks"])}
+                     "pair_interactions_per_s": sum(p["pairs"] for p in parts) / span, "makespan_s": span,
+                     "completed": sum(p["completed"] for p in parts),
+                     "peak_device_gb": max(p["peak"] for p in parts) / 1e9,
+                     "batched_steps": sum(p["ticks"] for p in parts)}
     out["config"] = {"trace": "Poisson arrivals at %.0f/s for %.1f s (%d requests, seeded), 50/50 "
                               "Kelvin-Helmholtz / Sod-type, n log-uniform in [8192, 1048576], %d RK2 steps each, "
-                              "admission by device footprint under %.0f GB" % (rate, duration, len(trace), nsteps,
-                                                                              budget / 1e9)}
+                              "admission by device footprint under %.0f GB per GPU, routed to %d GPU(s)"
+                              % (rate, duration, len(trace), nsteps, budget / 1e9, world)}
     return out
 
 
@@ -683,11 +718,11 @@ def run_ours(args):
             result["sod_fp64"] = rsod
             result["crk_kh"] = rcrk
     if args.batch > 0:
-        rb = measure_batch(pkg, args.batch, max(2, args.steps // 3), 1)
+        rb = measure_batch(pkg, args.batch, max(2, args.steps // 3), 1, rank, world)
         if rank == 0:
             result["batch"] = rb
     if args.serving > 0:
-        rs = measure_serving(pkg, args.serving, args.serving_steps)
+        rs = measure_serving(pkg, args.serving, args.serving_steps, rank=rank, world=world)
         if rank == 0:
             result["serving"] = rs
     if world > 1:
