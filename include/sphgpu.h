@@ -155,6 +155,29 @@ int sphgpu_dt(sphgpu_problem* p, double* dt_out);
 int sphgpu_step_rk2(sphgpu_problem* p, double* time, int64_t nsteps, double* last_dt);
 /* Integrator::currentTime and lastDt (src/Integrator/Integrator.hh) of the problem. */
 int sphgpu_time(sphgpu_problem* p, double* time, double* last_dt);
+/* iterateIdealH (src/Utilities/iterateIdealH.cc:26-349) as the reference's
+ * controller calls it at start-up (SpheralController.iterateIdealH: at most
+ * max_iterations iterations, tolerance on the relative change of H, no
+ * nPerh rescaling, no spherical start, no fixed determinant) with
+ * SPHSmoothingScale.  Each iteration rebuilds the ghosts and the
+ * ConnectivityMap from the current H and replaces the H of every node not
+ * yet converged by its ideal H.  Returns the iterations done and the
+ * largest change of the last one; the connectivity must be rebuilt
+ * afterwards (sphgpu_build_neighbors or the next step). */
+int sphgpu_iterate_ideal_h(sphgpu_problem* p, int32_t max_iterations, double tolerance, int32_t* iterations,
+                           double* max_delta_h);
+/* Checkpoint and restart (SPHHydroBase::dumpState/restoreState,
+ * src/SPH/SPHHydroBase.cc:1283-1357, with the NodeList state and the
+ * integrator's time, last dt and cycle).  The image is a self-describing
+ * byte buffer: a header (format tag, node count, hydro form, precision, field
+ * counts, time, last dt, cycle) followed by the FP64 state, the
+ * StateDerivatives and, for CRKSPH, the corrections and moments.  Restoring
+ * it into a problem created with the same configuration and node count
+ * continues the run bit for bit (the next step rebuilds the connectivity, as
+ * every step does).  A size, tag or layout mismatch returns SPHGPU_ERR_ARG. */
+int sphgpu_checkpoint_size(sphgpu_problem* p, int64_t* bytes);
+int sphgpu_checkpoint_save(sphgpu_problem* p, void* buffer, int64_t bytes);
+int sphgpu_checkpoint_load(sphgpu_problem* p, const void* buffer, int64_t bytes);
 /* SpheralConservation (src/SimulationControl/SpheralConservation.py:27-63):
  * out = {mass, px, py, pz, kinetic E, thermal E, total E, 0}, FP64 on device. */
 int sphgpu_conservation(sphgpu_problem* p, double out[8]);

@@ -146,6 +146,11 @@ def load_library(path=None):
     lib.sphgpu_dt.argtypes = [P, D]
     lib.sphgpu_step_rk2.argtypes = [P, D, I64, D]
     lib.sphgpu_conservation.argtypes = [P, P]
+    lib.sphgpu_iterate_ideal_h.argtypes = [P, ctypes.c_int32, ctypes.c_double, ctypes.POINTER(ctypes.c_int32),
+                                           ctypes.POINTER(ctypes.c_double)]
+    lib.sphgpu_checkpoint_size.argtypes = [P, ctypes.POINTER(I64)]
+    lib.sphgpu_checkpoint_save.argtypes = [P, P, I64]
+    lib.sphgpu_checkpoint_load.argtypes = [P, P, I64]
     lib.sphgpu_num_pairs.argtypes = [P, ctypes.POINTER(I64)]
     lib.sphgpu_kernel_launches.argtypes = [P, ctypes.POINTER(I64)]
     lib.sphgpu_time.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]

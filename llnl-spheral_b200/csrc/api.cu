@@ -938,6 +938,126 @@ int sphgpu_time(sphgpu_problem* p, double* time, double* last_dt) {
   return SPHGPU_OK;
 }
 
+namespace {
+// Checkpoint image header; the arrays follow in this order: S, D, K (CRKSPH).
+struct CheckpointHeader {
+  char tag[8];                 // "SPHGPUC1"
+  int64_t n;
+  int32_t hydro, precision, nstate, nderiv, ncrk, haveDerivs, crkVolumeReady, pad;
+  double time, lastDt;
+  int64_t cycle;
+};
+constexpr char kCheckpointTag[8] = {'S', 'P', 'H', 'G', 'P', 'U', 'C', '1'};
+
+int64_t checkpoint_bytes(const Problem& p) {
+  const int64_t ncrk = p.cfg.hydro == SPHGPU_HYDRO_CRKSPH ? NCRK : 0;
+  return (int64_t)sizeof(CheckpointHeader) + 8*p.n*((int64_t)NSTATE + NDERIV + ncrk);
+}
+}  // namespace
+
+int sphgpu_iterate_ideal_h(sphgpu_problem* p, int32_t max_iterations, double tolerance, int32_t* iterations,
+                           double* max_delta_h) {
+  if (p == nullptr || max_iterations < 0 || !(tolerance >= 0.0)) return SPHGPU_ERR_ARG;
+  Batch& b = solo(p);
+  // per-node change of H: the staging buffer (free between calls), start 2*tolerance
+  double* deltaH = p->staging;
+  fill_kernel<<<grid1(p->n), 256, 0, b.stream>>>(deltaH, p->n, 2.0*tolerance);
+  batch_count_launch(b);
+  int itr = 0;
+  double maxDeltaH = 2.0*tolerance;
+  while (itr < max_iterations && maxDeltaH > tolerance) {
+    ++itr;
+    SPH_TRY(build_neighbors_impl(b));
+    SPH_TRY(launch_ideal_h_iteration(b, tolerance, deltaH));
+    const int slot = SC_DELTAH;
+    std::vector<double> v;
+    SPH_TRY(batch_gather(b, &slot, 1, v));
+    maxDeltaH = v[0];
+  }
+  // the connectivity of the last iteration belongs to the previous H
+  p->haveNbrs = false;
+  p->haveDerivs = false;
+  if (iterations) *iterations = itr;
+  if (max_delta_h) *max_delta_h = maxDeltaH;
+  return batch_check_errors(b, "iterate ideal H");
+}
+
+int sphgpu_checkpoint_size(sphgpu_problem* p, int64_t* bytes) {
+  if (p == nullptr || bytes == nullptr) return SPHGPU_ERR_ARG;
+  *bytes = checkpoint_bytes(*p);
+  return SPHGPU_OK;
+}
+
+int sphgpu_checkpoint_save(sphgpu_problem* p, void* buffer, int64_t bytes) {
+  if (p == nullptr || buffer == nullptr) return SPHGPU_ERR_ARG;
+  if (bytes < checkpoint_bytes(*p)) { set_error("checkpoint buffer too small"); return SPHGPU_ERR_ARG; }
+  SPH_CHECK(cudaStreamSynchronize(p->stream));
+  CheckpointHeader h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.tag, kCheckpointTag, sizeof(h.tag));
+  h.n = p->n;
+  h.hydro = p->cfg.hydro;
+  h.precision = p->cfg.precision;
+  h.nstate = NSTATE;
+  h.nderiv = NDERIV;
+  h.ncrk = p->cfg.hydro == SPHGPU_HYDRO_CRKSPH ? NCRK : 0;
+  h.haveDerivs = p->haveDerivs ? 1 : 0;
+  h.crkVolumeReady = p->crkVolumeReady ? 1 : 0;
+  h.time = p->time;
+  h.lastDt = p->lastDt;
+  h.cycle = p->cycle;
+  char* out = static_cast<char*>(buffer);
+  std::memcpy(out, &h, sizeof(h));
+  double* d = reinterpret_cast<double*>(out + sizeof(h));
+  SPH_CHECK(cudaMemcpy(d, p->S, sizeof(double)*NSTATE*(size_t)p->n, cudaMemcpyDeviceToHost));
+  SPH_CHECK(cudaMemcpy(d + NSTATE*p->n, p->D, sizeof(double)*NDERIV*(size_t)p->n, cudaMemcpyDeviceToHost));
+  if (h.ncrk) {
+    if (p->K) {
+      SPH_CHECK(cudaMemcpy(d + (NSTATE + NDERIV)*p->n, p->K, sizeof(double)*NCRK*(size_t)p->n,
+                           cudaMemcpyDeviceToHost));
+    } else {
+      std::memset(d + (NSTATE + NDERIV)*p->n, 0, sizeof(double)*NCRK*(size_t)p->n);
+    }
+  }
+  return SPHGPU_OK;
+}
+
+int sphgpu_checkpoint_load(sphgpu_problem* p, const void* buffer, int64_t bytes) {
+  if (p == nullptr || buffer == nullptr) return SPHGPU_ERR_ARG;
+  if (bytes < (int64_t)sizeof(CheckpointHeader)) { set_error("checkpoint image too small"); return SPHGPU_ERR_ARG; }
+  CheckpointHeader h;
+  std::memcpy(&h, buffer, sizeof(h));
+  if (std::memcmp(h.tag, kCheckpointTag, sizeof(h.tag)) != 0) { set_error("not a checkpoint image"); return SPHGPU_ERR_ARG; }
+  const int32_t ncrk = p->cfg.hydro == SPHGPU_HYDRO_CRKSPH ? NCRK : 0;
+  if (h.n != p->n || h.hydro != p->cfg.hydro || h.nstate != NSTATE || h.nderiv != NDERIV || h.ncrk != ncrk) {
+    set_error("checkpoint image does not match the problem (node count, hydro form or field layout)");
+    return SPHGPU_ERR_ARG;
+  }
+  if (bytes < checkpoint_bytes(*p)) { set_error("checkpoint image truncated"); return SPHGPU_ERR_ARG; }
+  SPH_CHECK(cudaStreamSynchronize(p->stream));
+  const double* d = reinterpret_cast<const double*>(static_cast<const char*>(buffer) + sizeof(h));
+  SPH_CHECK(cudaMemcpy(p->S, d, sizeof(double)*NSTATE*(size_t)p->n, cudaMemcpyHostToDevice));
+  SPH_CHECK(cudaMemcpy(p->D, d + NSTATE*p->n, sizeof(double)*NDERIV*(size_t)p->n, cudaMemcpyHostToDevice));
+  if (ncrk) {
+    if (p->K == nullptr && cudaMalloc(&p->K, sizeof(double)*NCRK*(size_t)p->n) != cudaSuccess) {
+      p->K = nullptr;
+      set_error("CRKSPH field allocation failed");
+      return SPHGPU_ERR_NOMEM;
+    }
+    SPH_CHECK(cudaMemcpy(p->K, d + (NSTATE + NDERIV)*p->n, sizeof(double)*NCRK*(size_t)p->n,
+                         cudaMemcpyHostToDevice));
+  }
+  p->time = h.time;
+  p->lastDt = h.lastDt;
+  p->cycle = h.cycle;
+  p->haveDerivs = h.haveDerivs != 0;
+  p->crkVolumeReady = h.crkVolumeReady != 0;
+  p->haveNbrs = false;
+  SPH_CHECK(cudaMemcpy(p->d_scal + SC_LASTDT, &p->lastDt, sizeof(double), cudaMemcpyHostToDevice));
+  solo(p).memDirty = true;
+  return SPHGPU_OK;
+}
+
 int sphgpu_conservation(sphgpu_problem* p, double out[8]) {
   if (p == nullptr || out == nullptr) return SPHGPU_ERR_ARG;
   SPH_TRY(launch_conservation(solo(p)));

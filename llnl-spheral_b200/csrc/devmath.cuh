@@ -76,6 +76,16 @@ SPH_HD Sym sneg(const Sym& a) { return Sym{-a.xx, -a.xy, -a.xz, -a.yy, -a.yz, -a
 SPH_HD Sym selfdyad(const V3& a) {
   return Sym{a.x*a.x, a.x*a.y, a.x*a.z, a.y*a.y, a.y*a.z, a.z*a.z};
 }
+// GeomSymmetricTensor<3>::Inverse (cofactors over the determinant).
+SPH_HD Sym sinverse(const Sym& s) {
+  const Sym c{s.yy*s.zz - s.yz*s.yz,
+              s.yz*s.xz - s.xy*s.zz,
+              s.xy*s.yz - s.yy*s.xz,
+              s.xx*s.zz - s.xz*s.xz,
+              s.xy*s.xz - s.xx*s.yz,
+              s.xx*s.yy - s.xy*s.xy};
+  return sdiv(c, sdet(s));
+}
 SPH_HD double smaxAbs(const Sym& s) {
   return dmax(dabs(s.xx), dmax(dabs(s.xy), dmax(dabs(s.xz), dmax(dabs(s.yy), dmax(dabs(s.yz), dabs(s.zz))))));
 }

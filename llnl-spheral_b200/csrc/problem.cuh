@@ -271,6 +271,7 @@ enum ScalSlot {
   SC_NNEAR = 36,       // internal nodes near a periodic plane (the boundary passes' list)
   SC_REACH = 37,       // kernel reach in cells of the current grid
   SC_CELLSWANTED = 38, // cells of the grid at its natural cell size (i64)
+  SC_DELTAH = 39,      // largest H change of an iterateIdealH iteration (double bits)
   NSCAL = 40
 };
 
@@ -409,7 +410,9 @@ int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode);
 int launch_compatible_energy(Batch& b, double scale);
 int launch_enforce_boundaries(Batch& b);
 int launch_eos(Batch& b);
-int launch_dt(Batch& b, int slot, bool cachedEig);          // min dt vote bits -> slot
+int launch_dt(Batch& b, int slot, bool cachedEig);
+// one iterateIdealH iteration of a single problem; deltaH[n] per-node changes
+int launch_ideal_h_iteration(Batch& b, double tolerance, double* deltaH);          // min dt vote bits -> slot
 int launch_select_dt(Batch& b);                             // SC_DT from the vote and SC_LASTDT
 int launch_finish_step(Batch& b);                           // SC_LASTDT = SC_DT
 int launch_conservation(Batch& b);                          // SC_CONS

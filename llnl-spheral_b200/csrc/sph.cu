@@ -520,6 +520,69 @@ __global__ void __launch_bounds__(256) enforce_boundaries_kernel(const Member* m
   S[S_X*n + i] = r.x; S[S_Y*n + i] = r.y; S[S_Z*n + i] = r.z;
 }
 
+// ---------------------------------------------------------------- iterateIdealH
+// One iteration of iterateIdealH (src/Utilities/iterateIdealH.cc:26-349, the
+// drivers' arguments: nPerhForIteration 0, no spherical start, no fixed
+// determinant) with SPHSmoothingScale::idealSmoothingScale
+// (src/NodeList/SPHSmoothingScale.cc:102-225), one thread per internal node
+// over its ascending CSR row.  Nodes whose last change was within the
+// tolerance keep their H.  H is replaced in place: the moment of node i
+// reads only its own H and the positions.  deltaH[i] receives
+// max |eig((H1^1/2 Hi^-1 H1^1/2).Symmetric()) - 1|; H1 = c I, whose square
+// root the reference takes from a diagonal eigen decomposition (eigenvalue
+// (c*(1/c))*c, identity eigenvectors).  The largest change goes to
+// SC_DELTAH.
+__global__ void __launch_bounds__(128) ideal_h_iter_kernel(const Member* mem, BlockMap bm, double tolerance,
+                                                            double* deltaH) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
+  double dHi = 0.0;
+  if (i < n && deltaH[i] > tolerance) {
+    const Params& P = MB.prm;
+    double* S = MB.S;
+    const V3 ri{S[S_X*n + i], S[S_Y*n + i], S[S_Z*n + i]};
+    const Sym Hi{S[(S_H + 0)*n + i], S[(S_H + 1)*n + i], S[(S_H + 2)*n + i],
+                 S[(S_H + 3)*n + i], S[(S_H + 4)*n + i], S[(S_H + 5)*n + i]};
+    double zerothMoment = 0.0;
+    const int64_t k0 = MB.offsets[i], k1 = MB.offsets[i + 1];
+    for (int64_t k = k0; k < k1; ++k) {
+      const int32_t j = __ldg(MB.nbr + k);
+      V3 rj;
+      if (j < n) rj = V3{ldg(S + S_X*n + j), ldg(S + S_Y*n + j), ldg(S + S_Z*n + j)};
+      else rj = V3{ldg(MB.gpos + (j - n)), ldg(MB.gpos + MB.gcap + (j - n)), ldg(MB.gpos + 2*MB.gcap + (j - n))};
+      const V3 xij = vsub(ri, rj);
+      const double etai = mag(sdot(Hi, xij));
+      double W, gW;
+      tableKernelAndGrad(P.W, etai, 1.0, W, gW);
+      zerothMoment += dabs(gW);
+    }
+    zerothMoment = sgn(zerothMoment)*pow(dabs(zerothMoment), 0.3333333333333333);   // Dim<3>::rootnu
+    double nPerhCur;
+    if (fuzzyEqual(zerothMoment, 0.0)) nPerhCur = 0.5*P.nPerh;
+    else nPerhCur = equivalentNodesPerSmoothingScale(P, zerothMoment);
+    const double s = dmin(4.0, dmax(0.25, P.nPerh/(nPerhCur + 1.0e-30)));
+    const double a = s < 1.0 ? 0.4*(1.0 + s*s) : 0.4*(1.0 + 1.0/(s*s*s));
+    const double hi0 = 1.0/Hi.xx;
+    const double hi1 = dmin(P.hmax, dmax(P.hmin, hi0*(1.0 - a + a*s)));
+    const double inv = 1.0/hi1;
+    const Sym H1{1.0*inv, 0.0*inv, 0.0*inv, 1.0*inv, 0.0*inv, 1.0*inv};
+    const double fscale = dmax(10.0*kDblEps, smaxAbs(H1));
+    const double r = sqrt((inv*(1.0/fscale))*fscale);
+    const Sym Hinv = sinverse(Hi);
+    const Sym T{r*(r*Hinv.xx), r*(r*Hinv.xy), r*(r*Hinv.xz), r*(r*Hinv.yy), r*(r*Hinv.yz), r*(r*Hinv.zz)};
+    const V3 phi = eigenValues(T);
+    dHi = dmax(dabs(vmin(phi) - 1.0), dabs(vmax(phi) - 1.0));
+    deltaH[i] = dHi;
+    S[(S_H + 0)*n + i] = H1.xx; S[(S_H + 1)*n + i] = H1.xy; S[(S_H + 2)*n + i] = H1.xz;
+    S[(S_H + 3)*n + i] = H1.yy; S[(S_H + 4)*n + i] = H1.yz; S[(S_H + 5)*n + i] = H1.zz;
+  }
+  for (int o = 16; o > 0; o >>= 1) dHi = dmax(dHi, __shfl_xor_sync(0xffffffffu, dHi, o));
+  if ((threadIdx.x & 31) == 0 && dHi > 0.0)
+    atomicMax(reinterpret_cast<unsigned long long*>(MB.scal + SC_DELTAH), (unsigned long long)__double_as_longlong(dHi));
+}
+
 // ---------------------------------------------------------------- dt
 // cachedEig: max eig(H) of each node is the one the neighbor build stored
 // (hmaxi[n + i]), valid when H has not changed since that build (the step's
@@ -762,6 +825,16 @@ int launch_enforce_boundaries(Batch& b) {
   SPH_TRY(map_nodes(b, 256, &bm, &grid));
   if (grid) { enforce_boundaries_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
   return cuda_status(cudaGetLastError(), "enforce boundaries");
+}
+
+int launch_ideal_h_iteration(Batch& b, double tolerance, double* deltaH) {
+  if (b.memDirty) SPH_TRY(batch_upload(b));
+  batch_set_scal(b, SC_DELTAH, 0.0);
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(map_nodes(b, 128, &bm, &grid));
+  if (grid) { ideal_h_iter_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm, tolerance, deltaH); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "ideal H iteration");
 }
 
 int launch_dt(Batch& b, int slot, bool cachedEig) {

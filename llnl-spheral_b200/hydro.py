@@ -141,6 +141,40 @@ class SPHHydro:
         abi.check(self.lib.sphgpu_conservation(self.h, _p(out)), self.lib)
         return out
 
+    def iterateIdealH(self, maxIdealHIterations=50, idealHTolerance=1.0e-4):
+        """SpheralController.iterateIdealH: relax H to the ideal smoothing
+        scale before the run.  Returns (iterations, last max change of H)."""
+        itr = ctypes.c_int32()
+        dh = ctypes.c_double()
+        abi.check(self.lib.sphgpu_iterate_ideal_h(self.h, int(maxIdealHIterations), float(idealHTolerance),
+                                                  ctypes.byref(itr), ctypes.byref(dh)), self.lib)
+        return itr.value, dh.value
+
+    def checkpoint(self):
+        """Checkpoint image (bytes) of the state, derivatives, time, last dt
+        and cycle: SPHHydroBase::dumpState plus the NodeList and integrator
+        state."""
+        size = ctypes.c_int64()
+        abi.check(self.lib.sphgpu_checkpoint_size(self.h, ctypes.byref(size)), self.lib)
+        buf = np.empty(size.value, dtype=np.uint8)
+        abi.check(self.lib.sphgpu_checkpoint_save(self.h, _p(buf), size.value), self.lib)
+        return buf.tobytes()
+
+    def restore(self, image):
+        """SPHHydroBase::restoreState from a checkpoint image of a problem
+        with the same configuration and node count."""
+        buf = np.frombuffer(image, dtype=np.uint8)
+        abi.check(self.lib.sphgpu_checkpoint_load(self.h, _p(buf), buf.size), self.lib)
+        self.sync_time()
+
+    def dumpState(self, path):
+        with open(path, "wb") as f:
+            f.write(self.checkpoint())
+
+    def restoreState(self, path):
+        with open(path, "rb") as f:
+            self.restore(f.read())
+
     def kernel_launches(self):
         v = ctypes.c_int64()
         abi.check(self.lib.sphgpu_kernel_launches(self.h, ctypes.byref(v)), self.lib)

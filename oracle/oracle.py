@@ -42,6 +42,7 @@ def lib():
         L.orc_dt.argtypes = [P]
         L.orc_dt.restype = ctypes.c_double
         L.orc_step_rk2.argtypes = [P, ctypes.c_int, P, P]
+        L.orc_iterate_ideal_h.argtypes = [P, ctypes.c_int, ctypes.c_double, P]
         L.orc_get_field.argtypes = [P, ctypes.c_char_p, P]
         L.orc_get_pair_accelerations.argtypes = [P, P]
         L.orc_conservation.argtypes = [P, P]
@@ -134,6 +135,11 @@ class OracleProblem:
         if rc != 0:
             raise RuntimeError("oracle step failed: %s" % self.L.orc_last_error().decode())
         return t.value, dt.value
+
+    def iterate_ideal_h(self, max_iterations=50, tolerance=1.0e-4):
+        dh = ctypes.c_double()
+        itr = self.L.orc_iterate_ideal_h(self.h, int(max_iterations), float(tolerance), ctypes.byref(dh))
+        return itr, dh.value
 
     def field(self, key):
         c = FIELD_COMPONENTS[key]

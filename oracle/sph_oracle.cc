@@ -1056,6 +1056,69 @@ bool crkStepRK2(Problem& p, double& dtOut) {
 }  // namespace
 
 // ============================================================== C API
+// iterateIdealH (src/Utilities/iterateIdealH.cc:26-349) with the drivers'
+// arguments (SpheralController.iterateIdealH: nPerhForIteration = 0,
+// sphericalStart = false, fixDeterminant = false) and SPHSmoothingScale
+// (src/NodeList/SPHSmoothingScale.cc:102-225).  One NodeList, so every
+// neighbor weight fweightij is 1 and the second moment (unused by the SPH
+// smoothing scale) is not formed.  Each iteration rebuilds the ghosts and
+// the ConnectivityMap from the current H; nodes whose last change was within
+// the tolerance keep their H.  The change of H is measured as the reference
+// does: phi = eig((H1^1/2 Hi^-1 H1^1/2).Symmetric()), with H1 = c I from the
+// ideal smoothing scale, whose square root comes from a diagonal eigen
+// decomposition (eigenvalue (c*(1/c))*c, identity eigenvectors).
+int iterateIdealH(Problem& p, int maxIterations, double tolerance, double* maxDeltaHOut) {
+  const int nInt = p.nInt;
+  std::vector<double> deltaH(nInt, 2.0*tolerance);
+  const double nPerh = p.cfg.nPerh;
+  int itr = 0;
+  double maxDeltaH = 2.0*tolerance;
+  while (itr < maxIterations && maxDeltaH > tolerance) {
+    ++itr;
+    maxDeltaH = 0.0;
+    preStepInitialize(p);
+    std::vector<Sym> H1(p.H.begin(), p.H.begin() + nInt);
+    for (int i = 0; i < nInt; ++i) {
+      if (deltaH[i] <= tolerance) continue;
+      const V3& posi = p.pos[i];
+      const Sym& Hi = p.H[i];
+      double zerothMoment = 0.0;
+      for (int j : p.conn[i]) {
+        const V3 xij = vsub(posi, p.pos[j]);
+        const double etai = mag(sdot(Hi, xij));
+        const double Wi = std::abs(p.W.gradValue(etai, 1.0));
+        zerothMoment += Wi;
+      }
+      zerothMoment = CubeRootHalley2(zerothMoment);        // Dim<3>::rootnu
+      double currentNodesPerSmoothingScale;
+      if (fuzzyEqual(zerothMoment, 0.0)) currentNodesPerSmoothingScale = 0.5*nPerh;
+      else currentNodesPerSmoothingScale = p.W.equivalentNodesPerSmoothingScale(zerothMoment);
+      const double s = std::min(4.0, std::max(0.25, nPerh/(currentNodesPerSmoothingScale + 1.0e-30)));
+      double a;
+      if (s < 1.0) a = 0.4*(1.0 + s*s);
+      else a = 0.4*(1.0 + 1.0/(s*s*s));
+      const double hi0 = 1.0/Hi.xx;
+      const double hi1 = std::min(p.cfg.hmax, std::max(p.cfg.hmin, hi0*(1.0 - a + a*s)));
+      const double inv = 1.0/hi1;
+      H1[i] = Sym{1.0*inv, 0.0*inv, 0.0*inv, 1.0*inv, 0.0*inv, 1.0*inv};
+      // H1.sqrt(): eigen decomposition of the scaled diagonal tensor
+      const double fscale = std::max(10.0*2.220446049250313e-16, smaxAbsElement(H1[i]));
+      const double lam = (inv*(1.0/fscale))*fscale;
+      const double r = std::sqrt(lam);
+      const Sym Hinv = sinverse(Hi);
+      const Sym S{r*(r*Hinv.xx), r*(r*Hinv.xy), r*(r*Hinv.xz), r*(r*Hinv.yy), r*(r*Hinv.yz), r*(r*Hinv.zz)};
+      const V3 phi = eigenValues(S);
+      const double deltaHi = std::max(std::abs(minElement(phi) - 1.0), std::abs(maxElement(phi) - 1.0));
+      deltaH[i] = deltaHi;
+      maxDeltaH = std::max(maxDeltaH, deltaHi);
+    }
+    for (int i = 0; i < nInt; ++i) p.H[i] = H1[i];
+  }
+  p.haveConn = false;
+  if (maxDeltaHOut) *maxDeltaHOut = maxDeltaH;
+  return itr;
+}
+
 extern "C" {
 
 const char* orc_last_error() { return g_err.c_str(); }
@@ -1099,6 +1162,11 @@ int orc_build_neighbors(void* h) {
     ghostCopy(p, p.vol);
   }
   return 0;
+}
+
+int orc_iterate_ideal_h(void* h, int maxIterations, double tolerance, double* maxDeltaH) {
+  Problem& p = *static_cast<Problem*>(h);
+  return iterateIdealH(p, maxIterations, tolerance, maxDeltaH);
 }
 
 int orc_num_ghosts(void* h) { Problem& p = *static_cast<Problem*>(h); return numNodes(p) - p.nInt; }
