@@ -58,6 +58,11 @@ extern "C" {
 #define SPHGPU_CRK_SUMVOLUME      0  /* CRKVolumeType::CRKSumVolume       */
 #define SPHGPU_CRK_MASSOVERDENSITY 1 /* CRKVolumeType::CRKMassOverDensity */
 
+#define SPHGPU_Q_MONAGHAN_GINGOLD 0  /* MonaghanGingoldViscosity (src/ArtificialViscosity/MonaghanGingoldViscosity.cc) */
+#define SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD 1 /* CRKSPHMonaghanGingoldViscosity: limited, gradient-reconstructed
+                                       (src/ArtificialViscosity/CRKSPHMonaghanGingoldViscosity.cc:60-313);
+                                       CRKSPH problems only */
+
 /* Problem configuration: every physics switch of SPHHydroBase's constructor
  * (src/SPH/SPHHydroBase.cc:82-141), MonaghanGingoldViscosity
  * (src/ArtificialViscosity/MonaghanGingoldViscosity.cc:43-50), GammaLawGas,
@@ -90,6 +95,10 @@ typedef struct sphgpu_config {
   int32_t periodic[3];           /* 1 = PeriodicBoundary along that axis */
   int32_t max_neighbors;         /* per-node neighbor capacity (0 = 1024) */
   double  dtMin, dtMax, dtGrowth, lastDt;  /* Integrator controls       */
+  int32_t qType;                 /* SPHGPU_Q_*                           */
+  int32_t qPad;
+  double  etaCritFrac, etaFoldFrac;  /* CRKSPH Q: full Q below etaCritFrac/nPerh,
+                                        fold width etaFoldFrac/nPerh (defaults 1, 0.2) */
 } sphgpu_config;
 
 typedef struct sphgpu_problem sphgpu_problem;

@@ -21,6 +21,7 @@ DENSITY_RIGOROUS_SUM, DENSITY_INTEGRATE = 0, 1
 H_IDEAL, H_INTEGRATE = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 CRK_SUMVOLUME, CRK_MASSOVERDENSITY = 0, 1
+Q_MONAGHAN_GINGOLD, Q_CRKSPH_MONAGHAN_GINGOLD = 0, 1
 
 
 class SphConfig(ctypes.Structure):
@@ -61,6 +62,10 @@ class SphConfig(ctypes.Structure):
         ("dtMax", ctypes.c_double),
         ("dtGrowth", ctypes.c_double),
         ("lastDt", ctypes.c_double),
+        ("qType", ctypes.c_int32),
+        ("qPad", ctypes.c_int32),
+        ("etaCritFrac", ctypes.c_double),
+        ("etaFoldFrac", ctypes.c_double),
     ]
 
     def copy(self):
@@ -103,6 +108,10 @@ def make_config(**kw):
         c.xmin[a], c.xmax[a], c.periodic[a] = 0.0, 1.0, 1
     c.max_neighbors = 0
     c.dtMin, c.dtMax, c.dtGrowth, c.lastDt = 0.0, 0.1, 2.0, 1.0e-5
+    # CRKSPHMonaghanGingoldViscosity constructor defaults
+    # (src/PBGWraps/ArtificialViscosity/ArtificialViscosityModule.py:209-214)
+    c.qType = Q_MONAGHAN_GINGOLD
+    c.etaCritFrac, c.etaFoldFrac = 1.0, 0.2
     for k, v in kw.items():
         if k in ("xmin", "xmax", "periodic"):
             for a in range(3):

@@ -170,6 +170,15 @@ int validate_config(const sphgpu_config& c) {
   if (c.HUpdate != SPHGPU_H_IDEAL && c.HUpdate != SPHGPU_H_INTEGRATE) { set_error("unknown HUpdate"); return SPHGPU_ERR_ARG; }
   for (int a = 0; a < 3; ++a) if (c.periodic[a] && !(c.xmax[a] > c.xmin[a])) { set_error("empty periodic box"); return SPHGPU_ERR_ARG; }
   if (c.max_neighbors < 0 || c.max_neighbors > 4096) { set_error("max_neighbors must be in [0, 4096]"); return SPHGPU_ERR_ARG; }
+  if (c.qType != SPHGPU_Q_MONAGHAN_GINGOLD && c.qType != SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD) {
+    set_error("unknown qType"); return SPHGPU_ERR_ARG;
+  }
+  if (c.qType == SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD && c.hydro != SPHGPU_HYDRO_CRKSPH) {
+    set_error("the CRKSPH Monaghan-Gingold Q is implemented for CRKSPH problems"); return SPHGPU_ERR_UNSUPPORTED;
+  }
+  if (c.qType == SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD && !(c.etaCritFrac >= 0.0 && c.etaFoldFrac > 0.0)) {
+    set_error("etaCritFrac must be >= 0 and etaFoldFrac > 0"); return SPHGPU_ERR_ARG;
+  }
   return SPHGPU_OK;
 }
 
@@ -178,7 +187,7 @@ void free_problem(Problem* p) {
   void* ptrs[] = {p->S, p->S0, p->D, p->rec, p->groot, p->gcode, p->gpos, p->cand, p->cidx, p->sortedIdx,
                   p->cellStart, p->cellFill, p->counts, p->offsets, p->nbr, p->pacc, p->tableCoef, p->nperhTab,
                   p->wsumTab, p->blockSums, p->d_err, p->d_scal, p->d_red, p->staging, p->coefF, p->mrec, p->K, p->crec, p->hmaxi,
-                  p->wsumBinsTab};
+                  p->wsumBinsTab, p->qgrad};
   for (void* q : ptrs) if (q) cudaFree(q);
   if (p->pinned) cudaFreeHost(p->pinned);
   if (p->solo) { batch_free(*p->solo); delete p->solo; p->solo = nullptr; }
@@ -629,6 +638,7 @@ int64_t problem_bytes(const Problem& p) {
   b += 8*(int64_t)(p.cfg.hydro == SPHGPU_HYDRO_CRKSPH ? CMRECW : MRECW)*p.mreccap +
        (p.coefF ? 4*6*(int64_t)p.prm.W.n : 0);
   b += 8*(int64_t)CRECW*p.creccap + (p.K ? 8*(int64_t)NCRK*n : 0);
+  b += p.cfg.qType == SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD ? 8*(int64_t)QGRADW*n : 0;
   return b;
 }
 
@@ -765,6 +775,9 @@ int sphgpu_create(const sphgpu_config* cfg, int64_t n_internal, sphgpu_problem**
     P.useVelMagDt = cfg->useVelocityMagnitudeForDt; P.HUpdate = cfg->HUpdate; P.densityUpdate = cfg->densityUpdate;
     P.gradh = cfg->gradhCorrection;
     P.hydro = cfg->hydro;
+    P.qType = cfg->qType;
+    P.etaCrit = cfg->etaCritFrac/cfg->nPerh;
+    P.etaFold = cfg->etaFoldFrac/cfg->nPerh;
     P.dtMin = cfg->dtMin; P.dtMax = cfg->dtMax; P.dtGrowth = cfg->dtGrowth;
     // periodic planes: PeriodicBoundary(plane1 = (xmin, +e_a), plane2 = (xmax, -e_a))
     for (int a = 0; a < 3; ++a) {

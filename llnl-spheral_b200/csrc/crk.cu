@@ -323,7 +323,58 @@ __device__ __forceinline__ void crkKernel(const TableDev& T, const V3& rij, cons
   }
 }
 
-template<bool XSPH, bool COMPAT, bool SOLO>
+// CRKSPHMonaghanGingoldViscosity::Piij
+// (src/ArtificialViscosity/CRKSPHMonaghanGingoldViscosity.cc:188-262): the
+// velocity difference the Q sees.  The cached velocity gradients of both
+// nodes are projected onto half the separation; their ratio feeds the van
+// Leer limiter, which is released toward the full Q for pairs closer than
+// etaCrit.  The velocities are then reconstructed to the midpoint.  Every
+// term is even under i <-> j or flips sign exactly with it, so forming it
+// from node i's side gives the owner-oriented value of the reference, up to
+// the sign that the orientation-invariant mu absorbs.
+__device__ __forceinline__ double limiterVL(double x) {
+  return x > 0.0 ? 2.0/(1.0 + x)*2.0*x/(1.0 + x) : 0.0;                   // van Leer
+}
+
+__device__ __forceinline__ T9 loadQGrad(const double* qgrad, int64_t r) {
+  const double2* q = reinterpret_cast<const double2*>(qgrad + r*QGRADW);
+  const double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3), e = __ldg(q + 4);
+  return T9{a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x};
+}
+
+__device__ __forceinline__ V3 crkQVelocityDifference(const Params& P, const T9& Gi, const T9& Gj, const V3& ri,
+                                                     const V3& rj, const V3& vi, const V3& vj, const V3& etai,
+                                                     const V3& etaj) {
+  const V3 xij = vmul(vsub(ri, rj), 0.5);
+  const double gradi = dot(tvdot(Gi, xij), xij);
+  const double gradj = dot(tvdot(Gj, xij), xij);
+  const double rI = gradi/(sgn(gradj)*dmax(1.0e-30, dabs(gradj)));
+  const double rJ = gradj/(sgn(gradi)*dmax(1.0e-30, dabs(gradi)));
+  double phi = limiterVL(dmin(rI, rJ));
+  const double etaij = dmin(mag(etai), mag(etaj));
+  if (etaij < P.etaCrit) {
+    const double y = (etaij - P.etaCrit)/P.etaFold;
+    phi *= exp(-(y*y));
+  }
+  const V3 vi1 = vsub(vi, tvdot(tmul(Gi, phi), xij));
+  const V3 vj1 = vadd(vj, tvdot(tmul(Gj, phi), xij));
+  return vsub(vi1, vj1);
+}
+
+// The velocity gradient the CRKSPH Q caches at initialize (the previous
+// evaluation's), as [n][QGRADW] records.
+__global__ void __launch_bounds__(256) crk_qgrad_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
+  if (i >= M.n) return;
+  double* q = M.qgrad + i*QGRADW;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) q[c] = M.D[(D_DVDX + c)*M.n + i];
+  q[9] = 0.0;
+}
+
+template<bool XSPH, bool COMPAT, bool SOLO, bool QCRK>
 __global__ void __launch_bounds__(128) crk_eval_kernel(const Member* mem, BlockMap bm, const Member single) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = SOLO ? single : mem[mb.m];   // one member: read from the kernel parameters
@@ -354,6 +405,12 @@ __global__ void __launch_bounds__(128) crk_eval_kernel(const Member* mem, BlockM
     const V3 etai = sdot(I.H, rij);
     const V3 etaj = sdot(J.H, rij);
     const V3 vij = vsub(I.v, J.v);
+    V3 vQ = vij;
+    if (QCRK) {
+      const int64_t rootj = j < n ? (int64_t)j : (int64_t)__ldg(MB.groot + (j - n));
+      vQ = crkQVelocityDifference(P, loadQGrad(MB.qgrad, i), loadQGrad(MB.qgrad, rootj), I.r, J.r, I.v, J.v,
+                                  etai, etaj);
+    }
     double Wj, gWj, Wi, gWi;
     V3 gradWj, gradWi;
     crkKernel(P.W, rij, etai, I.H, I.Hdet, etaj, J.H, J.Hdet, I.A, I.B, I.gA, I.gB, Wj, gWj, gradWj);
@@ -371,8 +428,8 @@ __global__ void __launch_bounds__(128) crk_eval_kernel(const Member* mem, BlockM
       m2 = sadd(m2, smul(thpt, 1.0*mag2(gradWSPHi)));
     }
     // Monaghan-Gingold Pi (orientation-invariant mu)
-    const double mui = dot(vij, etai)/(mag2(etai) + P.eps2);
-    const double muj = dot(vij, etaj)/(mag2(etaj) + P.eps2);
+    const double mui = dot(vQ, etai)/(mag2(etai) + P.eps2);
+    const double muj = dot(vQ, etaj)/(mag2(etaj) + P.eps2);
     const double mi0 = dmin(0.0, mui), mj0 = dmin(0.0, muj);
     const double ei = -Cl*I.cs*(P.linearInExp ? mui : mi0) + Cq*(P.quadInExp ? -sgn(mui)*mui*mui : mi0*mi0);
     const double ej = -Cl*J.cs*(P.linearInExp ? muj : mj0) + Cq*(P.quadInExp ? -sgn(muj)*muj*muj : mj0*mj0);
@@ -460,6 +517,15 @@ int crk_prepare(Batch& b) {
       cudaMemsetAsync(p.K, 0, sizeof(double)*NCRK*(size_t)p.n, b.stream);
       b.memDirty = true;
     }
+    if (p.prm.qType == SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD && p.qgrad == nullptr) {
+      if (cudaMalloc(&p.qgrad, sizeof(double)*QGRADW*(size_t)p.n) != cudaSuccess) {
+        p.qgrad = nullptr;
+        set_error("CRKSPH Q gradient allocation failed");
+        return SPHGPU_ERR_NOMEM;
+      }
+      cudaMemsetAsync(p.qgrad, 0, sizeof(double)*QGRADW*(size_t)p.n, b.stream);
+      b.memDirty = true;
+    }
     if (p.candcap > p.creccap) {
       cudaStreamSynchronize(b.stream);
       cudaFree(p.crec);
@@ -489,6 +555,7 @@ int crk_nodes(Batch& b, int threads, BlockMap* bm, unsigned* grid, bool (*pred)(
 bool crkSumVolume(const Problem& p) { return isCrk(p) && p.cfg.crkVolumeType == SPHGPU_CRK_SUMVOLUME; }
 bool crkMassOverDensity(const Problem& p) { return isCrk(p) && p.cfg.crkVolumeType != SPHGPU_CRK_SUMVOLUME; }
 bool crkSumDensity(const Problem& p) { return isCrk(p) && p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM; }
+bool crkQ(const Problem& p) { return isCrk(p) && p.prm.qType == SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD; }
 
 }  // namespace
 
@@ -523,6 +590,9 @@ int launch_crk_initialize(Batch& b) {
   unsigned grid = 0;
   SPH_TRY(crk_nodes(b, 128, &bm, &grid, isCrk));
   if (grid) { crk_moments_corrections_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  // CRKSPHMonaghanGingoldViscosity::initialize caches the last velocity gradient
+  SPH_TRY(crk_nodes(b, 256, &bm, &grid, crkQ));
+  if (grid) { crk_qgrad_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
   return cuda_status(cudaGetLastError(), "CRK moments");
 }
 
@@ -531,24 +601,30 @@ int launch_crk_eval(Batch& b) {
   unsigned grid = 0;
   SPH_TRY(batch_map_items(b, [&](const Problem& p) { return isCrkFp64(p) ? (b.capacityGrids ? p.candcap : p.n + p.G) : (int64_t)0; }, 256, &bm, &grid));
   if (grid) { pack_crk_records_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
-  auto key = [](const Problem& p) { return (p.prm.XSPH ? 2 : 0) | (p.prm.compatible ? 1 : 0); };
+  auto key = [](const Problem& p) {
+    return (crkQ(p) ? 4 : 0) | (p.prm.XSPH ? 2 : 0) | (p.prm.compatible ? 1 : 0);
+  };
   const bool solo = b.mem.size() == 1;
   const Member one = solo ? describe_member(*b.mem[0]) : Member{};
-  bool present[4] = {false, false, false, false};
+  bool present[8] = {false, false, false, false, false, false, false, false};
   for (Problem* p : b.mem) if (isCrkFp64(*p)) present[key(*p)] = true;
-  for (int v = 0; v < 4; ++v) {
+  for (int v = 0; v < 8; ++v) {
     if (!present[v]) continue;
     SPH_TRY(batch_map_items(b, [&](const Problem& p) { return isCrkFp64(p) && key(p) == v ? p.n : (int64_t)0; }, b.evalThreads,
                             &bm, &grid));
     if (!grid) continue;
-#define CRK_LAUNCH(X, C)                                                                               \
-    if (solo) crk_eval_kernel<X, C, true><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one);     \
-    else crk_eval_kernel<X, C, false><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one)
+#define CRK_LAUNCH(X, C, Q)                                                                            \
+    if (solo) crk_eval_kernel<X, C, true, Q><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one);  \
+    else crk_eval_kernel<X, C, false, Q><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one)
     switch (v) {
-      case 0: CRK_LAUNCH(false, false); break;
-      case 1: CRK_LAUNCH(false, true); break;
-      case 2: CRK_LAUNCH(true, false); break;
-      default: CRK_LAUNCH(true, true); break;
+      case 0: CRK_LAUNCH(false, false, false); break;
+      case 1: CRK_LAUNCH(false, true, false); break;
+      case 2: CRK_LAUNCH(true, false, false); break;
+      case 3: CRK_LAUNCH(true, true, false); break;
+      case 4: CRK_LAUNCH(false, false, true); break;
+      case 5: CRK_LAUNCH(false, true, true); break;
+      case 6: CRK_LAUNCH(true, false, true); break;
+      default: CRK_LAUNCH(true, true, true); break;
     }
 #undef CRK_LAUNCH
     batch_count_launch(b);

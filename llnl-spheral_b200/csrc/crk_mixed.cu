@@ -134,7 +134,42 @@ __device__ __forceinline__ void crkKernelF(const F3& rij, float Wij, const F3& g
   gradWCRK.z = gradWij.z*corr + B[2]*AW + gA[2]*gAW + AW*(gB[2]*rij.x + gB[5]*rij.y + gB[8]*rij.z);
 }
 
-template<bool XSPH, bool COMPAT, bool SOLO>
+// CRKSPHMonaghanGingoldViscosity velocity reconstruction in FP32 (see
+// crkQVelocityDifference in crk.cu): the cached velocity gradients projected
+// on half the separation, van Leer limited, released near etaCrit.
+__device__ __forceinline__ void loadQGradF(const double* qgrad, int64_t r, float* g) {
+  const double2* q = reinterpret_cast<const double2*>(qgrad + r*QGRADW);
+#pragma unroll
+  for (int c = 0; c < 5; ++c) {
+    const double2 v = __ldg(q + c);
+    g[2*c] = (float)v.x;
+    if (2*c + 1 < 9) g[2*c + 1] = (float)v.y;
+  }
+}
+
+__device__ __forceinline__ F3 crkQVelocityDifferenceF(const Params& P, const double* qgrad, int64_t i, int64_t rj,
+                                                      const F3& rij, const F3& vij, const F3& etai, const F3& etaj) {
+  float gi[9], gj[9];
+  loadQGradF(qgrad, i, gi);
+  loadQGradF(qgrad, rj, gj);
+  const F3 x{0.5f*rij.x, 0.5f*rij.y, 0.5f*rij.z};
+  const F3 ti{gi[0]*x.x + gi[1]*x.y + gi[2]*x.z, gi[3]*x.x + gi[4]*x.y + gi[5]*x.z, gi[6]*x.x + gi[7]*x.y + gi[8]*x.z};
+  const F3 tj{gj[0]*x.x + gj[1]*x.y + gj[2]*x.z, gj[3]*x.x + gj[4]*x.y + gj[5]*x.z, gj[6]*x.x + gj[7]*x.y + gj[8]*x.z};
+  const float gradi = dotF(ti, x), gradj = dotF(tj, x);
+  const float rI = gradi/(copysignf(1.0f, gradj)*fmaxf(1.0e-30f, fabsf(gradj)));
+  const float rJ = gradj/(copysignf(1.0f, gradi)*fmaxf(1.0e-30f, fabsf(gradi)));
+  const float r = fminf(rI, rJ);
+  float phi = r > 0.0f ? 2.0f/(1.0f + r)*2.0f*r/(1.0f + r) : 0.0f;
+  const float etaij = fminf(sqrtf(dotF(etai, etai)), sqrtf(dotF(etaj, etaj)));
+  const float etaCrit = (float)P.etaCrit;
+  if (etaij < etaCrit) {
+    const float y = (etaij - etaCrit)/(float)P.etaFold;
+    phi *= expf(-(y*y));
+  }
+  return F3{vij.x - phi*(ti.x + tj.x), vij.y - phi*(ti.y + tj.y), vij.z - phi*(ti.z + tj.z)};
+}
+
+template<bool XSPH, bool COMPAT, bool SOLO, bool QCRK>
 __global__ void __launch_bounds__(128, 3) crk_eval_mixed_kernel(const Member* mem, BlockMap bm, const Member single) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = SOLO ? single : mem[mb.m];   // one member: read from the kernel parameters
@@ -196,9 +231,14 @@ __global__ void __launch_bounds__(128, 3) crk_eval_mixed_kernel(const Member* me
       m2[0].add(rij.x*rij.x*g2); m2[1].add(rij.x*rij.y*g2); m2[2].add(rij.x*rij.z*g2);
       m2[3].add(rij.y*rij.y*g2); m2[4].add(rij.y*rij.z*g2); m2[5].add(rij.z*rij.z*g2);
     }
-    // Monaghan-Gingold Pi
-    const float mui = __fdividef(dotF(vij, etai), dotF(etai, etai) + eps2);
-    const float muj = __fdividef(dotF(vij, etaj), dotF(etaj, etaj) + eps2);
+    // Monaghan-Gingold Pi (the CRKSPH Q sees the reconstructed velocities)
+    F3 vQ = vij;
+    if (QCRK) {
+      const int64_t rootj = j < n ? (int64_t)j : (int64_t)__ldg(MB.groot + (j - n));
+      vQ = crkQVelocityDifferenceF(P, MB.qgrad, i, rootj, rij, vij, etai, etaj);
+    }
+    const float mui = __fdividef(dotF(vQ, etai), dotF(etai, etai) + eps2);
+    const float muj = __fdividef(dotF(vQ, etaj), dotF(etaj, etaj) + eps2);
     const float mi0 = fminf(0.0f, mui), mj0 = fminf(0.0f, muj);
     const float ei = -Cl*I.cs*(P.linearInExp ? mui : mi0) + Cq*(P.quadInExp ? -copysignf(1.0f, mui)*mui*mui : mi0*mi0);
     const float ej = -Cl*J.cs*(P.linearInExp ? muj : mj0) + Cq*(P.quadInExp ? -copysignf(1.0f, muj)*muj*muj : mj0*mj0);
@@ -299,24 +339,31 @@ int launch_crk_eval_mixed(Batch& b) {
   SPH_TRY(batch_map_items(b, [&](const Problem& p) { return isCrkMixed(p) ? (b.capacityGrids ? p.candcap : p.n + p.G) : (int64_t)0; }, 256, &bm,
                           &grid));
   if (grid) { pack_crk_mixed_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
-  auto key = [](const Problem& p) { return (p.prm.XSPH ? 2 : 0) | (p.prm.compatible ? 1 : 0); };
+  auto key = [](const Problem& p) {
+    return (p.prm.qType == SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD ? 4 : 0) | (p.prm.XSPH ? 2 : 0) |
+           (p.prm.compatible ? 1 : 0);
+  };
   const bool solo = b.mem.size() == 1;
   const Member one = solo ? describe_member(*b.mem[0]) : Member{};
-  bool present[4] = {false, false, false, false};
+  bool present[8] = {false, false, false, false, false, false, false, false};
   for (Problem* p : b.mem) if (isCrkMixed(*p)) present[key(*p)] = true;
-  for (int v = 0; v < 4; ++v) {
+  for (int v = 0; v < 8; ++v) {
     if (!present[v]) continue;
     SPH_TRY(batch_map_items(b, [&](const Problem& p) { return isCrkMixed(p) && key(p) == v ? p.n : (int64_t)0; },
                             b.evalThreads, &bm, &grid));
     if (!grid) continue;
-#define CRKM_LAUNCH(X, C)                                                                                  \
-    if (solo) crk_eval_mixed_kernel<X, C, true><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one);   \
-    else crk_eval_mixed_kernel<X, C, false><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one)
+#define CRKM_LAUNCH(X, C, Q)                                                                                 \
+    if (solo) crk_eval_mixed_kernel<X, C, true, Q><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one);  \
+    else crk_eval_mixed_kernel<X, C, false, Q><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one)
     switch (v) {
-      case 0: CRKM_LAUNCH(false, false); break;
-      case 1: CRKM_LAUNCH(false, true); break;
-      case 2: CRKM_LAUNCH(true, false); break;
-      default: CRKM_LAUNCH(true, true); break;
+      case 0: CRKM_LAUNCH(false, false, false); break;
+      case 1: CRKM_LAUNCH(false, true, false); break;
+      case 2: CRKM_LAUNCH(true, false, false); break;
+      case 3: CRKM_LAUNCH(true, true, false); break;
+      case 4: CRKM_LAUNCH(false, false, true); break;
+      case 5: CRKM_LAUNCH(false, true, true); break;
+      case 6: CRKM_LAUNCH(true, false, true); break;
+      default: CRKM_LAUNCH(true, true, true); break;
     }
 #undef CRKM_LAUNCH
     batch_count_launch(b);

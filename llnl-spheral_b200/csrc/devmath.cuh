@@ -118,6 +118,12 @@ SPH_HD V3 eigenValues(const Sym& s) {
 SPH_HD T9 dyad(const V3& a, const V3& b) {
   return T9{a.x*b.x, a.x*b.y, a.x*b.z, a.y*b.x, a.y*b.y, a.y*b.z, a.z*b.x, a.z*b.y, a.z*b.z};
 }
+// Tensor.dot(Vector)
+SPH_HD V3 tvdot(const T9& t, const V3& r) {
+  return V3{t.xx*r.x + t.xy*r.y + t.xz*r.z,
+            t.yx*r.x + t.yy*r.y + t.yz*r.z,
+            t.zx*r.x + t.zy*r.y + t.zz*r.z};
+}
 SPH_HD T9 tmul(const T9& t, double s) {
   return T9{t.xx*s, t.xy*s, t.xz*s, t.yx*s, t.yy*s, t.yz*s, t.zx*s, t.zy*s, t.zz*s};
 }

@@ -113,6 +113,8 @@ struct Params {
   int compatible, XSPH, correctVelGrad, linearInExp, quadInExp, useVelMagDt;
   int HUpdate, densityUpdate, gradh;
   int hydro;               // SPHGPU_HYDRO_*
+  int qType;               // SPHGPU_Q_*
+  double etaCrit, etaFold; // CRKSPH Q: etaCritFrac/nPerh, etaFoldFrac/nPerh
   double dtMin, dtMax, dtGrowth;   // Integrator time-step controls
   BoxBCs bcs;
 };
@@ -160,6 +162,7 @@ struct Problem {
   double* S0 = nullptr;
   double* D = nullptr;
   double* K = nullptr;          // [NCRK][n] CRKSPH fields (CRKSPH problems only)
+  double* qgrad = nullptr;      // [n][QGRADW] velocity gradient cached by the CRKSPH Q's initialize
   double* crec = nullptr;       // [n+G][CRECW] CRKSPH pair records
   int64_t creccap = 0;
   bool crkVolumeReady = false;
@@ -246,6 +249,10 @@ enum NbrSchedule {
 // first[nmem] the grid size.  A single problem is a batch of one member.
 
 // Slots of a member's small device scalar array (64-bit words).
+// Doubles per node of the CRKSPH Q's cached velocity gradient (9, padded
+// to 80 bytes for 16-byte loads).
+constexpr int QGRADW = 10;
+
 // Doubles per slot of the cell-ordered candidate arrays (Problem::cand):
 // 16-byte pre-test record + 4-byte FP32 max eig(H), rounded up.
 constexpr int CAND_DOUBLES = 3;
@@ -287,7 +294,7 @@ struct Member {
   Params prm;
   double* S; double* S0; double* D; double* K;
   double* rec; double* crec; double* mrec;
-  double* gpos; double* pacc; double* scal; double* red; double* hmaxi;
+  double* gpos; double* pacc; double* scal; double* red; double* hmaxi; double* qgrad;
   int32_t* groot; int32_t* cidx; int32_t* sortedIdx; int32_t* counts; int32_t* nbr; int32_t* cellFill;
   uint32_t* gcode;
   int64_t* offsets; int64_t* cellStart; int64_t* blockSums;

@@ -79,6 +79,7 @@ struct Problem {
   std::vector<double> vol, A, m0;
   std::vector<V3> B, gradA, m1, gradm0, gradRho;
   std::vector<T9> gradB, gradm1;
+  std::vector<T9> qGradVel;   // CRKSPHMonaghanGingoldViscosity::mGradVel (internal + ghosts)
   std::vector<Sym> cm2;                      // CRK second moment (m2 above is the ideal-H one)
   std::vector<std::array<double, 27>> gradm2;
   double time = 0.0, lastDt = 1e-5;
@@ -906,6 +907,33 @@ void crkKernel(const TableKernel& W, const V3& rij, const V3& etai, const Sym& H
   }
 }
 
+// CRKSPHMonaghanGingoldViscosity::Piij velocity reconstruction
+// (src/ArtificialViscosity/CRKSPHMonaghanGingoldViscosity.cc:223-247), pair
+// (i, j) in the reference's orientation; the limited velocities then enter
+// the Monaghan-Gingold mu.
+inline double limiterVL(const double x) {
+  if (x > 0.0) return 2.0/(1.0 + x)*2.0*x/(1.0 + x);
+  return 0.0;
+}
+void crkQVelocities(const Problem& p, int i, int j, const V3& etai, const V3& etaj, V3& vi1, V3& vj1) {
+  const T9& DvDxi = p.qGradVel[i];
+  const T9& DvDxj = p.qGradVel[j];
+  const V3 xij = vmul(vsub(p.pos[i], p.pos[j]), 0.5);
+  const double gradi = dot(tvdot(DvDxi, xij), xij);
+  const double gradj = dot(tvdot(DvDxj, xij), xij);
+  const double ri = gradi/(sgn(gradj)*std::max(1.0e-30, std::abs(gradj)));
+  const double rj = gradj/(sgn(gradi)*std::max(1.0e-30, std::abs(gradi)));
+  double phi = limiterVL(std::min(ri, rj));
+  const double etaCrit = p.cfg.etaCritFrac/p.cfg.nPerh, etaFold = p.cfg.etaFoldFrac/p.cfg.nPerh;
+  const double etaij = std::min(mag(etai), mag(etaj));
+  if (etaij < etaCrit) {
+    const double y = (etaij - etaCrit)/etaFold;
+    phi *= std::exp(-(y*y));
+  }
+  vi1 = vsub(p.vel[i], tvdot(tmul(DvDxi, phi), xij));
+  vj1 = vadd(p.vel[j], tvdot(tmul(DvDxj, phi), xij));
+}
+
 void crkEvaluateDerivatives(Problem& p) {
   zeroDerivs(p);
   const int n = numNodes(p);
@@ -948,7 +976,13 @@ void crkEvaluateDerivatives(Problem& p) {
         p.m2[j] = sadd(p.m2[j], smul(thpt, 1.0/fweightij*mag2(gradWSPHj)));
       }
       T9 QPi, QPj;
-      Piij(p, etai, vi, rhoi, ci, etaj, vj, rhoj, cj, QPi, QPj);
+      if (p.cfg.qType == SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD) {
+        V3 vi1, vj1;
+        crkQVelocities(p, i, j, etai, etaj, vi1, vj1);
+        Piij(p, etai, vi1, rhoi, ci, etaj, vj1, rhoj, cj, QPi, QPj);
+      } else {
+        Piij(p, etai, vi, rhoi, ci, etaj, vj, rhoj, cj, QPi, QPj);
+      }
       T9 Qsum = tmul(QPi, rhoi*rhoi);
       taddto(Qsum, tmul(QPj, rhoj*rhoj));
       const V3 Qaccij = tvdot(Qsum, deltagrad);
@@ -1018,7 +1052,17 @@ void crkVolumeUpdate(Problem& p, double multiplier) {
 void crkInitialize(Problem& p) {
   crkMoments(p);
   crkCorrections(p);
+  // CRKSPHMonaghanGingoldViscosity::initialize
+  // (src/ArtificialViscosity/CRKSPHMonaghanGingoldViscosity.cc:119-150): cache
+  // the last velocity gradient, ghosts by the boundary copies.
+  if (p.cfg.qType == SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD) {
+    p.qGradVel.assign(numNodes(p), tzero());
+    for (int i = 0; i < p.nInt && i < int(p.DvDx.size()); ++i) p.qGradVel[i] = p.DvDx[i];
+    ghostCopy(p, p.qGradVel);
+  }
 }
+
+
 
 bool crkStepRK2(Problem& p, double& dtOut) {
   const double t = p.time;

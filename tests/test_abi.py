@@ -5,6 +5,10 @@ import glob
 import importlib
 import os
 import re
+import shutil
+import subprocess
+
+import pytest
 
 ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 
@@ -34,12 +38,25 @@ def test_library_exports_all_declared_symbols():
     assert not missing, missing
 
 
-def test_config_struct_layout_matches_header():
+def test_config_struct_layout_matches_header(tmp_path):
+    """The ctypes mirror has the C struct's size and every field's offset
+    (the C side measured by compiling the header with the host compiler)."""
     abi = importlib.import_module("llnl-spheral_b200.abi")
-    # 4 ints, 1 double, 3 doubles, 2 ints, 1 + 2 + 3 + 2 + 1 doubles, 8 ints,
-    # 6 doubles, 4 ints, 4 doubles
-    expect = 4 * 4 + 8 + 24 + 8 + 8 + 16 + 24 + 16 + 8 + 32 + 48 + 16 + 32
-    assert ctypes.sizeof(abi.SphConfig) == expect
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    names = [f[0] for f in abi.SphConfig._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "sphgpu.h"\nint main(void) {\n'
+                   '  printf("%zu\\n", sizeof(sphgpu_config));\n' +
+                   "".join('  printf("%%zu\\n", offsetof(sphgpu_config, %s));\n' % n for n in names) +
+                   "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.check_call([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    out = [int(x) for x in subprocess.check_output([str(exe)]).split()]
+    assert ctypes.sizeof(abi.SphConfig) == out[0]
+    for name, off in zip(names, out[1:]):
+        assert getattr(abi.SphConfig, name).offset == off, name
 
 
 def test_error_codes_without_gpu_calls():

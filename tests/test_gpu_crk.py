@@ -117,3 +117,66 @@ def test_crk_mixed_energy_drift(gpu_lib, pkg):
     e0 = g.conservation()[6]
     g.step(100)
     assert abs(g.conservation()[6] - e0) <= 1e-6 * abs(e0)
+
+
+@pytest.mark.parametrize("case", ["kh", "sod"])
+def test_crk_q_limited_viscosity(gpu_lib, pkg, oracle_mod, case):
+    """CRKSPHMonaghanGingoldViscosity: the Q sees velocities reconstructed from
+    the last velocity gradient (van Leer limited, released near etaCrit).
+    After a few steps the cached gradients are non-zero; states and the next
+    derivatives match the oracle within 1e-12 (CUDA and glibc exp may differ
+    by an ulp, so not bit for bit) and differ from the plain Q."""
+    ns, cfg = _case(pkg, case)
+    cq = cfg.copy()
+    cq.qType = pkg.abi.Q_CRKSPH_MONAGHAN_GINGOLD
+    g = pkg.SPHHydro(cq, ns)
+    o = oracle_mod.OracleProblem(cq, ns)
+    plain = pkg.SPHHydro(cfg, ns)
+    for p in (g, plain):
+        p.build_neighbors()
+        p.initialize()
+        p.evaluateDerivatives()
+    o.build_neighbors()
+    o.initialize()
+    o.evaluate_derivatives()
+    for _ in range(4):
+        g.step(1)
+        o.step(1)
+        plain.step(1)
+    for k in ("position", "velocity", "mass density", "specific thermal energy", "H"):
+        assert normwise(g.field(k), o.field(k)) <= 1e-12, k
+    g.build_neighbors()
+    o.build_neighbors()
+    g.initialize()
+    o.initialize()
+    g.evaluateDerivatives()
+    o.evaluate_derivatives()
+    for k in DERIV_KEYS:
+        assert normwise(g.field(k), o.field(k)) <= 1e-12, k
+    assert not np.array_equal(g.field("max viscous pressure"), plain.field("max viscous pressure"))
+
+
+def test_crk_q_mixed_against_fp64(gpu_lib, pkg):
+    ns, cfg = _case(pkg, "sod")
+    cfg.qType = pkg.abi.Q_CRKSPH_MONAGHAN_GINGOLD
+    cm = cfg.copy()
+    cm.precision = pkg.abi.PRECISION_MIXED
+    f = pkg.SPHHydro(cfg, ns)
+    m = pkg.SPHHydro(cm, ns)
+    for p in (f, m):
+        p.build_neighbors()
+        p.initialize()
+        p.evaluateDerivatives()
+        p.step(3)
+    for k in ("position", "velocity", "mass density", "specific thermal energy"):
+        assert normwise(m.field(k), f.field(k)) <= 1e-5, k
+
+
+def test_crk_q_rejected_for_sph(gpu_lib, pkg):
+    gen, abi = pkg.generators, pkg.abi
+    box = ((0.0, 0.0, 0.0), (1.0, 0.25, 0.25))
+    ns = gen.sod(nx=16, ny=4, nz=4, box=box)
+    cfg = gen.sod_config(abi, ns_box=box)
+    cfg.qType = abi.Q_CRKSPH_MONAGHAN_GINGOLD
+    with pytest.raises(RuntimeError, match="CRKSPH"):
+        pkg.SPHHydro(cfg, ns)
