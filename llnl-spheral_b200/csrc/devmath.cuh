@@ -76,6 +76,11 @@ SPH_HD Sym sneg(const Sym& a) { return Sym{-a.xx, -a.xy, -a.xz, -a.yy, -a.yz, -a
 SPH_HD Sym selfdyad(const V3& a) {
   return Sym{a.x*a.x, a.x*a.y, a.x*a.z, a.y*a.y, a.y*a.z, a.z*a.z};
 }
+// H = h I exactly: then H.dot(r) = r*h bit for bit (the off-diagonal
+// products are exact zeros).
+SPH_HD bool isoSym(const Sym& s) {
+  return s.xy == 0.0 && s.xz == 0.0 && s.yz == 0.0 && s.xx == s.yy && s.xx == s.zz;
+}
 // GeomSymmetricTensor<3>::Inverse (cofactors over the determinant).
 SPH_HD Sym sinverse(const Sym& s) {
   const Sym c{s.yy*s.zz - s.yz*s.yz,

@@ -410,6 +410,8 @@ __device__ __forceinline__ float symEta2F(const float* h, float x, float y, floa
 // sorted slot and node index (the exact test re-reads its FP64 state).
 struct Walker {
   float hf[6];
+  float lam2;          // isotropic H = lam I: lam^2 (then eta_i^2 = lam^2 |r|^2)
+  bool iso;
   float ox, oy, oz;
   int cx, cy, cz;
   int64_t slot;
@@ -426,6 +428,8 @@ __device__ __forceinline__ Walker makeWalker(const Member& M, const NbrArrays& a
   const Sym H = nodeH(M, w.idx);
   w.hf[0] = (float)H.xx; w.hf[1] = (float)H.xy; w.hf[2] = (float)H.xz;
   w.hf[3] = (float)H.yy; w.hf[4] = (float)H.yz; w.hf[5] = (float)H.zz;
+  w.iso = H.xy == 0.0 && H.xz == 0.0 && H.yz == 0.0 && H.xx == H.yy && H.xx == H.zz;
+  w.lam2 = w.hf[0]*w.hf[0];
   const float4 p = __ldg(a.pre + s);
   w.ox = p.x; w.oy = p.y; w.oz = p.z;
   w.cx = cellCoord(r.x, g.lo[0], g.cell, g.dim[0]);
@@ -510,9 +514,11 @@ __device__ __forceinline__ bool candTest(const Member& M, const NbrArrays& a, co
   if (pretest) {
     const float4 c = __ldg(a.pre + k);
     const float fx = (w.ox - c.x) - dxc, fy = (w.oy - c.y) - dyc, fz = (w.oz - c.z) - dzc;
-    const float e2i = symEta2F(w.hf, fx, fy, fz);
-    if (e2i <= k2lo) return true;
     const float r2 = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, fz*fz));
+    float e2i;
+    if (w.iso) e2i = w.lam2*r2;          // the common case: H = lam I
+    else e2i = symEta2F(w.hf, fx, fy, fz);
+    if (e2i <= k2lo) return true;
     if (e2i > k2hi && c.w*c.w*r2 > k2hi) return false;
     const float lm = __ldg(a.lmax + k);
     if (lm*lm*r2 <= k2lo) return true;

@@ -109,6 +109,7 @@ __global__ void __launch_bounds__(128) sph_eval_fp64_kernel(const Member* mem, B
   double* pacc = MB.pacc;
   const int64_t ecap = MB.ecap;
   const Rec I = loadRec(rec, i);
+  const bool isoI = isoSym(I.H);
   double rhoSum = 0.0, norm = 0.0, wns = 0.0, maxvp = 0.0, effvp = 0.0, viscW = 0.0, DepsDt = 0.0;
   double XSPHw = 0.0;
   V3 DvDt{0.0, 0.0, 0.0}, XSPHdv{0.0, 0.0, 0.0};
@@ -132,12 +133,15 @@ __global__ void __launch_bounds__(128) sph_eval_fp64_kernel(const Member* mem, B
     const double mrhoA = own ? I.mrho : J.mrho, mrhoB = own ? J.mrho : I.mrho;
 
     const V3 rij = vsub(rA, rB);
-    const V3 etaA = sdot(HA, rij);
-    const V3 etaB = sdot(HB, rij);
+    // H = h I (the common case): every H product reduces to a scaling with
+    // the same bits (the off-diagonal terms add exact zeros)
+    const bool iso = isoI && isoSym(J.H);
+    const V3 etaA = iso ? vmul(rij, HA.xx) : sdot(HA, rij);
+    const V3 etaB = iso ? vmul(rij, HB.xx) : sdot(HB, rij);
     const double etaMagA = mag(etaA);
     const double etaMagB = mag(etaB);
-    const V3 HetaA = sdot(HA, unitVector(etaA));
-    const V3 HetaB = sdot(HB, unitVector(etaB));
+    const V3 HetaA = iso ? vmul(unitVector(etaA), HA.xx) : sdot(HA, unitVector(etaA));
+    const V3 HetaB = iso ? vmul(unitVector(etaB), HB.xx) : sdot(HB, unitVector(etaB));
     double WA, gWA, WB, gWB;
     tableKernelAndGrad(P.W, etaMagA, HdetA, WA, gWA);
     tableKernelAndGrad(P.W, etaMagB, HdetB, WB, gWB);
@@ -337,7 +341,7 @@ __global__ void __launch_bounds__(128) sum_density_kernel(const Member* mem, Blo
     if (!selfDone && j > (int32_t)i) { rho += mi*W0; selfDone = true; }
     const Rec J = loadRec(rec, j);
     const V3 rij = vsub(ri, J.r);
-    const double eta = mag(sdot(J.H, rij));
+    const double eta = mag(isoSym(J.H) ? vmul(rij, J.H.xx) : sdot(J.H, rij));
     rho += J.m*tableKernel(P.W, eta, J.Hdet);
   }
   if (!selfDone) rho += mi*W0;

@@ -34,6 +34,7 @@ struct Kahan {
 struct MRec {
   double x, y, z, vx, vy, vz;
   float m, rho, cs, Hdet, hxx, hxy, hxz, hyy, hyz, hzz, Prho, mrho, P, somega;
+  float iso;           // 1: H = hxx I (the symmetric products reduce to scalings)
 };
 
 __device__ __forceinline__ MRec loadMRec(const double* mrec, int64_t k) {
@@ -46,7 +47,7 @@ __device__ __forceinline__ MRec loadMRec(const double* mrec, int64_t k) {
   R.m = b0.x; R.rho = b0.y; R.cs = b0.z; R.Hdet = b0.w;
   R.hxx = b1.x; R.hxy = b1.y; R.hxz = b1.z; R.hyy = b1.w;
   R.hyz = b2.x; R.hzz = b2.y; R.Prho = b2.z; R.mrho = b2.w;
-  R.P = b3.x; R.somega = b3.y;
+  R.P = b3.x; R.somega = b3.y; R.iso = b3.z;
   return R;
 }
 
@@ -72,7 +73,8 @@ __global__ void __launch_bounds__(256) pack_mixed_kernel(const Member* mem, Bloc
   f[0] = make_float4((float)m, (float)rho, (float)S[S_CS*n + r], (float)sdet(H));
   f[1] = make_float4((float)H.xx, (float)H.xy, (float)H.xz, (float)H.yy);
   f[2] = make_float4((float)H.yz, (float)H.zz, (float)(somega*P/(rho*rho)), (float)(m/rho));
-  f[3] = make_float4((float)P, (float)somega, 0.0f, 0.0f);
+  const bool iso = H.xy == 0.0 && H.xz == 0.0 && H.yz == 0.0 && H.xx == H.yy && H.xx == H.zz;
+  f[3] = make_float4((float)P, (float)somega, iso ? 1.0f : 0.0f, 0.0f);
 }
 
 __global__ void table_to_float_kernel(const double* coef, int n, float* out) {
@@ -185,8 +187,16 @@ __global__ void __launch_bounds__(128, 3) sph_eval_mixed_kernel(const Member* me
     // FP64 differences, rounded once
     const F3 rij{(float)(I.x - J.x), (float)(I.y - J.y), (float)(I.z - J.z)};
     const F3 vij{(float)(I.vx - J.vx), (float)(I.vy - J.vy), (float)(I.vz - J.vz)};
-    const F3 etai = symdot(I.hxx, I.hxy, I.hxz, I.hyy, I.hyz, I.hzz, rij);
-    const F3 etaj = symdot(J.hxx, J.hxy, J.hxz, J.hyy, J.hyz, J.hzz, rij);
+    // isotropic H (the common case): H r = hxx r, bit-identical to the full product
+    const bool isoPair = I.iso != 0.0f && J.iso != 0.0f;
+    F3 etai, etaj;
+    if (isoPair) {
+      etai = F3{I.hxx*rij.x, I.hxx*rij.y, I.hxx*rij.z};
+      etaj = F3{J.hxx*rij.x, J.hxx*rij.y, J.hxx*rij.z};
+    } else {
+      etai = symdot(I.hxx, I.hxy, I.hxz, I.hyy, I.hyz, I.hzz, rij);
+      etaj = symdot(J.hxx, J.hxy, J.hxz, J.hyy, J.hyz, J.hzz, rij);
+    }
     const float e2i = etai.x*etai.x + etai.y*etai.y + etai.z*etai.z;
     const float e2j = etaj.x*etaj.x + etaj.y*etaj.y + etaj.z*etaj.z;
     const float rinvi = e2i > 0.0f ? __frsqrt_rn(e2i) : 0.0f;
@@ -194,8 +204,14 @@ __global__ void __launch_bounds__(128, 3) sph_eval_mixed_kernel(const Member* me
     const float etaMagi = e2i*rinvi, etaMagj = e2j*rinvj;
     const F3 ui = e2i > 0.0f ? F3{etai.x*rinvi, etai.y*rinvi, etai.z*rinvi} : F3{1.0f, 0.0f, 0.0f};
     const F3 uj = e2j > 0.0f ? F3{etaj.x*rinvj, etaj.y*rinvj, etaj.z*rinvj} : F3{1.0f, 0.0f, 0.0f};
-    const F3 Hetai = symdot(I.hxx, I.hxy, I.hxz, I.hyy, I.hyz, I.hzz, ui);
-    const F3 Hetaj = symdot(J.hxx, J.hxy, J.hxz, J.hyy, J.hyz, J.hzz, uj);
+    F3 Hetai, Hetaj;
+    if (isoPair) {
+      Hetai = F3{I.hxx*ui.x, I.hxx*ui.y, I.hxx*ui.z};
+      Hetaj = F3{J.hxx*uj.x, J.hxx*uj.y, J.hxx*uj.z};
+    } else {
+      Hetai = symdot(I.hxx, I.hxy, I.hxz, I.hyy, I.hyz, I.hzz, ui);
+      Hetaj = symdot(J.hxx, J.hxy, J.hxz, J.hyy, J.hyz, J.hzz, uj);
+    }
     float Wi, gWi, Wj, gWj;
     tableF(coefF, P.W.n, invStep, extent, etaMagi, I.Hdet, Wi, gWi);
     tableF(coefF, P.W.n, invStep, extent, etaMagj, J.Hdet, Wj, gWj);
