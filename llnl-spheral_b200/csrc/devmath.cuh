@@ -110,8 +110,14 @@ SPH_HD V3 eigenValues(const Sym& s) {
   const double c2Div3 = c2*onethird;
   const double aDiv3 = dmin(0.0, onethird*(c1 - c2*c2Div3));
   const double mbDiv2 = 0.5*(c0 + c2Div3*(2.0*c2Div3*c2Div3 - c1));
-  const double q = dmin(0.0, mbDiv2*mbDiv2 + aDiv3*aDiv3*aDiv3);
   const double m = sqrt(-aDiv3);
+  // m == +-0 (every isotropic H): the cos/sin terms are multiplied by a zero,
+  // so all three eigenvalues are fscale*c2Div3 bit for bit; skip the solve
+  if (m == 0.0) {
+    const double e = fscale*c2Div3;
+    return V3{e, e, e};
+  }
+  const double q = dmin(0.0, mbDiv2*mbDiv2 + aDiv3*aDiv3*aDiv3);
   const double angle = atan2(sqrt(-q), mbDiv2)*onethird;
   const double cs = cos(angle);
   const double sn = sin(angle);
