@@ -199,6 +199,7 @@ void free_problem(Problem* p) {
 // call: another batch holding the same problem may have moved its buffers.
 Batch& solo(Problem* p) {
   p->solo->memDirty = true;
+  p->solo->packedByUpdate = 0;      // records written by an update belong to that step only
   return *p->solo;
 }
 
@@ -362,20 +363,25 @@ int step_after_connectivity(Batch& b) {
   // selectDt with the previous derivatives, state at the step start
   // (reads the state and derivatives directly: no records needed yet).
   SPH_TRY(launch_select_dt(b));
+  if (anyMember(b, isMixedSph)) SPH_TRY(prepare_mixed(b));   // the update writes mixed records
   // state0 = state; trial advance to the mid point (updateAsIncrement for
-  // every policy), one kernel
-  SPH_TRY(launch_update(b, 0.5, true, 1));
+  // every policy) and the internal nodes' pair records, one kernel; the
+  // record passes then cover the ghosts (and the members the update does
+  // not pack)
+  SPH_TRY(launch_update(b, 0.5, true, 1, PACK_FOR_EVAL));
   SPH_TRY(pack_records(b, PACK_FOR_EVAL));
   // initializeDerivatives + derivs.Zero + evaluateDerivatives at the mid point
   SPH_TRY(initialize_impl(b));
   SPH_TRY(launch_eval(b));
   // full step from state0 with the mid-point derivatives (the restore of
-  // state0 is folded into the compatible-energy and update kernels)
+  // state0 is folded into the compatible-energy and update kernels), with
+  // the records of the summed density
   SPH_TRY(launch_compatible_energy(b, 1.0));
-  SPH_TRY(launch_update(b, 1.0, false, 2));
+  SPH_TRY(launch_update(b, 1.0, false, 2, PACK_FOR_FINALIZE));
   // applyGhostBoundaries; postStepFinalize (sum density); enforceBoundaries
   SPH_TRY(pack_records(b, PACK_FOR_FINALIZE));
   SPH_TRY(finalize_impl(b));
+  b.packedByUpdate = 0;
   SPH_TRY(launch_enforce_boundaries(b));
   SPH_TRY(launch_finish_step(b));
   return SPHGPU_OK;
@@ -776,6 +782,7 @@ int sphgpu_create(const sphgpu_config* cfg, int64_t n_internal, sphgpu_problem**
     P.gradh = cfg->gradhCorrection;
     P.hydro = cfg->hydro;
     P.qType = cfg->qType;
+    P.precision = cfg->precision;
     P.etaCrit = cfg->etaCritFrac/cfg->nPerh;
     P.etaFold = cfg->etaFoldFrac/cfg->nPerh;
     P.dtMin = cfg->dtMin; P.dtMax = cfg->dtMax; P.dtGrowth = cfg->dtGrowth;
@@ -1165,6 +1172,7 @@ namespace {
 int batch_begin(Batch& b) {
   // members' buffers may have moved under their own calls since the last upload
   b.memDirty = true;
+  b.packedByUpdate = 0;
   for (Problem* p : b.mem) SPH_CHECK(cudaStreamSynchronize(p->stream));
   return SPHGPU_OK;
 }

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include "devmath.cuh"
+#include "mixed.cuh"
 #include "../../include/sphgpu.h"
 
 namespace sphgpu {
@@ -95,6 +96,43 @@ enum RecField {
   RECW = 20
 };
 
+// The pair records of one node, from its state.  Written by the record
+// pack kernels and by the update kernel (which packs the internal nodes as
+// it advances them); every writer is compiled in the same translation unit
+// (sph.cu, -fmad=false), so a node's record has the same bits whoever wrote it.
+__device__ __forceinline__ void writeRecord(double* rec, int64_t k, const V3& x, const V3& v, double m, double rho,
+                                            double cs, double P, double omega, const Sym& H) {
+  const double somega = safeInv(omega, 1.0e-30);
+  double2* q = reinterpret_cast<double2*>(rec + k*RECW);
+  q[0] = make_double2(x.x, x.y);
+  q[1] = make_double2(x.z, v.x);
+  q[2] = make_double2(v.y, v.z);
+  q[3] = make_double2(m, rho);
+  q[4] = make_double2(cs, sdet(H));
+  q[5] = make_double2(H.xx, H.xy);
+  q[6] = make_double2(H.xz, H.yy);
+  q[7] = make_double2(H.yz, H.zz);
+  q[8] = make_double2(somega*P/(rho*rho), m/rho);
+  q[9] = make_double2(P, somega);
+}
+
+// Mixed-precision record (MRECW doubles): FP64 position and velocity, FP32
+// m, rho, cs, det H, H, P/rho^2 term, m/rho, P, safeOmega, isotropy flag.
+__device__ __forceinline__ void writeMixedRecord(double* mrec, int64_t k, const V3& x, const V3& v, double m,
+                                                 double rho, double cs, double P, double omega, const Sym& H) {
+  const double somega = safeInv(omega, 1.0e-30);
+  double2* q = reinterpret_cast<double2*>(mrec + k*MRECW);
+  q[0] = make_double2(x.x, x.y);
+  q[1] = make_double2(x.z, v.x);
+  q[2] = make_double2(v.y, v.z);
+  float4* f = reinterpret_cast<float4*>(q + 3);
+  f[0] = make_float4((float)m, (float)rho, (float)cs, (float)sdet(H));
+  f[1] = make_float4((float)H.xx, (float)H.xy, (float)H.xz, (float)H.yy);
+  f[2] = make_float4((float)H.yz, (float)H.zz, (float)(somega*P/(rho*rho)), (float)(m/rho));
+  const bool iso = H.xy == 0.0 && H.xz == 0.0 && H.yz == 0.0 && H.xx == H.yy && H.xx == H.zz;
+  f[3] = make_float4((float)P, (float)somega, iso ? 1.0f : 0.0f, 0.0f);
+}
+
 // Read-only physics parameters of one problem (in its Member descriptor).
 struct Params {
   TableDev W;
@@ -114,6 +152,7 @@ struct Params {
   int HUpdate, densityUpdate, gradh;
   int hydro;               // SPHGPU_HYDRO_*
   int qType;               // SPHGPU_Q_*
+  int precision;           // SPHGPU_PRECISION_*
   double etaCrit, etaFold; // CRKSPH Q: etaCritFrac/nPerh, etaFoldFrac/nPerh
   double dtMin, dtMax, dtGrowth;   // Integrator time-step controls
   BoxBCs bcs;
@@ -356,6 +395,7 @@ struct Batch {
   int nbrCells = 0;              // requested cells per kernel reach (0 auto)
   int lastNbrSchedule = 0;
   int evalThreads = 128;         // threads per block of the pair-loop kernels (64, 128 or 256)
+  int packedByUpdate = 0;        // records the last update kernel wrote (PackNeed), 0: none
   // CUDA-graph replay of the part of the RK2 step after the connectivity
   // (api.cu): captured once per buffer layout, replayed every step.
   bool useGraph = false;
@@ -407,13 +447,22 @@ int build_connectivity(Batch& b);     // ghosts + ConnectivityMap, device-sized
 // FP64 pair records of the members that read them next (PACK_ALL: every member)
 enum PackNeed { PACK_ALL = 0, PACK_FOR_EVAL = 1, PACK_FOR_FINALIZE = 2 };
 int pack_records(Batch& b, int need = PACK_ALL);
+// mixed records of the mixed-form SPH members (of those with a summed
+// density only, for finalize); sph.cu
+int pack_mixed(Batch& b, bool rigorousSumOnly);
+// members whose internal records the last update kernel wrote (packMode 1:
+// mid-point evaluation, 2: end-of-step summed density); their packs then
+// cover the ghosts only
+bool packedByUpdate(const Problem& p, int packMode);
 int launch_gradh(Batch& b);
 int launch_eval_sph_fp64(Batch& b);
 int launch_eval_sph_mixed(Batch& b);
 int launch_sum_density(Batch& b);          // plain FP64 SPH members
 int launch_sum_density_mixed(Batch& b);    // mixed-precision SPH members (sph_mixed.cu)
-// mode: 0 in place, 1 save state0 first (mid point), 2 from state0 (full step)
-int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode);
+// mode: 0 in place, 1 save state0 first (mid point), 2 from state0 (full step);
+// packMode (PackNeed): also write the internal nodes' records for the next
+// evaluation (1) or summed density (2), 0: none
+int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode, int packMode = 0);
 int launch_compatible_energy(Batch& b, double scale);
 int launch_enforce_boundaries(Batch& b);
 int launch_eos(Batch& b);

@@ -64,31 +64,40 @@ __device__ __forceinline__ Sym sels(bool c, const Sym& a, const Sym& b) {
 }
 
 // ---------------------------------------------------------------- records
-__global__ void __launch_bounds__(256) pack_records_kernel(const Member* mem, BlockMap bm) {
+// Pair records of the nodes [first, n + G): every node, or only the ghosts
+// when the update kernel has already packed the internal nodes.  A ghost's
+// record is its root's with the position mapped through the periodic planes.
+__device__ __forceinline__ void nodeRecordState(const Member& M, int64_t k, V3& x, V3& v, double& m, double& rho,
+                                                double& cs, double& P, double& omega, Sym& H) {
+  const double* S = M.S;
+  const int64_t n = M.n;
+  const int64_t r = k < n ? k : M.groot[k - n];
+  x = V3{S[S_X*n + r], S[S_Y*n + r], S[S_Z*n + r]};
+  if (k >= n) x = ghostPosition(M.prm.bcs, x, M.gcode[k - n]);
+  v = V3{S[S_VX*n + r], S[S_VY*n + r], S[S_VZ*n + r]};
+  H = Sym{S[(S_H + 0)*n + r], S[(S_H + 1)*n + r], S[(S_H + 2)*n + r],
+          S[(S_H + 3)*n + r], S[(S_H + 4)*n + r], S[(S_H + 5)*n + r]};
+  m = S[S_M*n + r]; rho = S[S_RHO*n + r]; cs = S[S_CS*n + r]; P = S[S_P*n + r]; omega = S[S_OMEGA*n + r];
+}
+
+__global__ void __launch_bounds__(256) pack_records_kernel(const Member* mem, BlockMap bm, int ghostsOnly) {
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
-  const int64_t k = mb.block*blockDim.x + threadIdx.x;
-  const int64_t n = M.n;
-  if (k >= n + scalI(M.scal, SC_G)) return;
-  const double* S = M.S;
-  const int64_t r = k < n ? k : M.groot[k - n];
-  V3 x{S[S_X*n + r], S[S_Y*n + r], S[S_Z*n + r]};
-  if (k >= n) x = ghostPosition(M.prm.bcs, x, M.gcode[k - n]);
-  const Sym H{S[(S_H + 0)*n + r], S[(S_H + 1)*n + r], S[(S_H + 2)*n + r],
-              S[(S_H + 3)*n + r], S[(S_H + 4)*n + r], S[(S_H + 5)*n + r]};
-  const double m = S[S_M*n + r], rho = S[S_RHO*n + r], P = S[S_P*n + r];
-  const double somega = safeInv(S[S_OMEGA*n + r], 1.0e-30);
-  double2* q = reinterpret_cast<double2*>(M.rec + k*RECW);
-  q[0] = make_double2(x.x, x.y);
-  q[1] = make_double2(x.z, S[S_VX*n + r]);
-  q[2] = make_double2(S[S_VY*n + r], S[S_VZ*n + r]);
-  q[3] = make_double2(m, rho);
-  q[4] = make_double2(S[S_CS*n + r], sdet(H));
-  q[5] = make_double2(H.xx, H.xy);
-  q[6] = make_double2(H.xz, H.yy);
-  q[7] = make_double2(H.yz, H.zz);
-  q[8] = make_double2(somega*P/(rho*rho), m/rho);
-  q[9] = make_double2(P, somega);
+  const int64_t k = (ghostsOnly ? M.n : 0) + mb.block*blockDim.x + threadIdx.x;
+  if (k >= M.n + scalI(M.scal, SC_G)) return;
+  V3 x, v; double m, rho, cs, P, omega; Sym H;
+  nodeRecordState(M, k, x, v, m, rho, cs, P, omega, H);
+  writeRecord(M.rec, k, x, v, m, rho, cs, P, omega, H);
+}
+
+__global__ void __launch_bounds__(256) pack_mixed_kernel(const Member* mem, BlockMap bm, int ghostsOnly) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int64_t k = (ghostsOnly ? M.n : 0) + mb.block*blockDim.x + threadIdx.x;
+  if (k >= M.n + scalI(M.scal, SC_G)) return;
+  V3 x, v; double m, rho, cs, P, omega; Sym H;
+  nodeRecordState(M, k, x, v, m, rho, cs, P, omega, H);
+  writeMixedRecord(M.mrec, k, x, v, m, rho, cs, P, omega, H);
 }
 
 // ---------------------------------------------------------------- derivatives
@@ -368,7 +377,7 @@ __global__ void __launch_bounds__(128) compatible_energy_kernel(const Member* me
   const double hdt = 0.5*multiplier;
   const double weighti = fabs(D[D_DEPSDT*n + i]) + kDblEps;
   const double* S0 = MB.S0;
-  const double mi = S0[S_M*n + i];
+  const double mi = S[S_M*n + i];                // mass is constant within the step
   const V3 vi{S0[S_VX*n + i], S0[S_VY*n + i], S0[S_VZ*n + i]};
   const V3 ai{D[(D_DVDT + 0)*n + i], D[(D_DVDT + 1)*n + i], D[(D_DVDT + 2)*n + i]};
   const V3 vi12 = vadd(vi, vmul(ai, hdt));
@@ -378,7 +387,7 @@ __global__ void __launch_bounds__(128) compatible_energy_kernel(const Member* me
     const int32_t j = __ldg(nbr + k);
     const int64_t r = j < n ? (int64_t)j : (int64_t)__ldg(groot + (j - n));
     const double weightj = fabs(ldg(D + D_DEPSDT*n + r)) + kDblEps;
-    const double mj = ldg(S0 + S_M*n + r);
+    const double mj = ldg(S + S_M*n + r);
     const V3 vj{ldg(S0 + S_VX*n + r), ldg(S0 + S_VY*n + r), ldg(S0 + S_VZ*n + r)};
     const V3 aj{ldg(D + (D_DVDT + 0)*n + r), ldg(D + (D_DVDT + 1)*n + r), ldg(D + (D_DVDT + 2)*n + r)};
     const V3 vj12 = vadd(vj, vmul(aj, hdt));
@@ -411,16 +420,21 @@ __device__ __forceinline__ bool hInsideBounds(const Sym& H, double hmin, double 
 }
 
 // State::update of every policy, f = f_src + scale*dt*df, into S.
-// UPDATE_IN_PLACE: the source is S.  UPDATE_SAVE_START: the source is S and
-// every state field is first copied to S0 (state0 = state.copyState()).
-// UPDATE_FROM_START: the source is S0 (state.assign(state0) fused into the
-// update); the fields no policy updates are copied from S0, and with
-// compatible energy the specific thermal energy already written to S by
-// compatible_energy_kernel is kept.
+// UPDATE_IN_PLACE: the source is S.  UPDATE_SAVE_START: the source is S,
+// saved to S0 first (state0 = state.copyState()).  UPDATE_FROM_START: the
+// source is S0 (state.assign(state0) fused into the update); with
+// compatible energy the specific thermal energy compatible_energy_kernel
+// wrote to S is kept.  S0 holds only what the rest of the step reads from
+// it: position, velocity, density, energy, H, plus omega with grad-h (the
+// mid-point initialize changes it) and the CRKSPH volume.  Mass is constant
+// and pressure and sound speed are recomputed, so S0 skips them.
+// packMode 1 / 2 also writes the node's pair record for the mid-point
+// evaluation / the end-of-step summed density (SPH members, see
+// packedByUpdate).
 enum UpdateMode { UPDATE_IN_PLACE = 0, UPDATE_SAVE_START = 1, UPDATE_FROM_START = 2 };
 
 __global__ void __launch_bounds__(256) update_kernel(const Member* mem, BlockMap bm, double scale,
-                                                     int timeAdvanceOnly, int mode) {
+                                                     int timeAdvanceOnly, int mode, int packMode) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = mem[mb.m];
   const int64_t n = MB.n;
@@ -428,20 +442,33 @@ __global__ void __launch_bounds__(256) update_kernel(const Member* mem, BlockMap
   if (i >= n) return;
   const Params& P = MB.prm;
   double* S = MB.S;
-  const double* Src = mode == UPDATE_FROM_START ? MB.S0 : MB.S;
+  double* S0 = MB.S0;
+  const double* Src = mode == UPDATE_FROM_START ? S0 : S;
   const double* D = MB.D;
+  const bool crk = P.hydro == SPHGPU_HYDRO_CRKSPH;
+  // the source state of the updated fields
+  V3 x{Src[S_X*n + i], Src[S_Y*n + i], Src[S_Z*n + i]};
+  V3 v{Src[S_VX*n + i], Src[S_VY*n + i], Src[S_VZ*n + i]};
+  const double rho0 = Src[S_RHO*n + i];
+  const double eps0 = Src[S_EPS*n + i];
+  const Sym H{Src[(S_H + 0)*n + i], Src[(S_H + 1)*n + i], Src[(S_H + 2)*n + i],
+              Src[(S_H + 3)*n + i], Src[(S_H + 4)*n + i], Src[(S_H + 5)*n + i]};
+  const double vol0 = crk ? Src[S_VOL*n + i] : 0.0;
   if (mode == UPDATE_SAVE_START) {
-    for (int f = 0; f < NSTATE; ++f) MB.S0[f*n + i] = S[f*n + i];
-  } else if (mode == UPDATE_FROM_START) {
-    S[S_M*n + i] = Src[S_M*n + i];
-    S[S_OMEGA*n + i] = Src[S_OMEGA*n + i];
-    if (P.hydro != SPHGPU_HYDRO_CRKSPH) S[S_VOL*n + i] = Src[S_VOL*n + i];
+    S0[S_X*n + i] = x.x; S0[S_Y*n + i] = x.y; S0[S_Z*n + i] = x.z;
+    S0[S_VX*n + i] = v.x; S0[S_VY*n + i] = v.y; S0[S_VZ*n + i] = v.z;
+    S0[S_RHO*n + i] = rho0;
+    S0[S_EPS*n + i] = eps0;
+    S0[(S_H + 0)*n + i] = H.xx; S0[(S_H + 1)*n + i] = H.xy; S0[(S_H + 2)*n + i] = H.xz;
+    S0[(S_H + 3)*n + i] = H.yy; S0[(S_H + 4)*n + i] = H.yz; S0[(S_H + 5)*n + i] = H.zz;
+    if (P.gradh) S0[S_OMEGA*n + i] = S[S_OMEGA*n + i];
+    if (crk) S0[S_VOL*n + i] = vol0;
+  } else if (mode == UPDATE_FROM_START && P.gradh) {
+    S[S_OMEGA*n + i] = S0[S_OMEGA*n + i];
   }
   const int epsDone = (!timeAdvanceOnly && P.compatible) ? 1 : 0;
   const double mult = scale*MB.scal[SC_DT];
   // H: IncrementBoundedState (half step / IntegrateH) or ReplaceBoundedState (IdealH)
-  Sym H{Src[(S_H + 0)*n + i], Src[(S_H + 1)*n + i], Src[(S_H + 2)*n + i],
-        Src[(S_H + 3)*n + i], Src[(S_H + 4)*n + i], Src[(S_H + 5)*n + i]};
   Sym Hn;
   if (timeAdvanceOnly || P.HUpdate == SPHGPU_H_INTEGRATE) {
     const Sym dH{D[(D_DHDT + 0)*n + i], D[(D_DHDT + 1)*n + i], D[(D_DHDT + 2)*n + i],
@@ -455,32 +482,45 @@ __global__ void __launch_bounds__(256) update_kernel(const Member* mem, BlockMap
   S[(S_H + 0)*n + i] = Hn.xx; S[(S_H + 1)*n + i] = Hn.xy; S[(S_H + 2)*n + i] = Hn.xz;
   S[(S_H + 3)*n + i] = Hn.yy; S[(S_H + 4)*n + i] = Hn.yz; S[(S_H + 5)*n + i] = Hn.zz;
   // mass density: IncrementBoundedState
-  const double rho = dmin(P.rhoMax, dmax(P.rhoMin, Src[S_RHO*n + i] + mult*(D[D_DRHODT*n + i])));
+  const double drho = D[D_DRHODT*n + i];
+  const double rho = dmin(P.rhoMax, dmax(P.rhoMin, rho0 + mult*(drho)));
   S[S_RHO*n + i] = rho;
   // position: IncrementFieldList
-  for (int c = 0; c < 3; ++c) S[(S_X + c)*n + i] = Src[(S_X + c)*n + i] + D[(D_DXDT + c)*n + i]*mult;
+  x = V3{x.x + D[(D_DXDT + 0)*n + i]*mult, x.y + D[(D_DXDT + 1)*n + i]*mult, x.z + D[(D_DXDT + 2)*n + i]*mult};
+  S[S_X*n + i] = x.x; S[S_Y*n + i] = x.y; S[S_Z*n + i] = x.z;
+  const double m = S[S_M*n + i];                     // constant within the step
   // CRKSPH node volume: ContinuityVolumePolicy (after mass density and H)
-  if (P.hydro == SPHGPU_HYDRO_CRKSPH) {
-    const double m = Src[S_M*n + i];
+  if (crk) {
     const double volMin = 0.5*m*safeInvVar(rho);
     const double volMax = 4.0*3.14159265358979323846/(3.0*sdet(Hn));
-    const double dVdt = -m*safeInvVar(rho*rho)*D[D_DRHODT*n + i];
-    S[S_VOL*n + i] = dmax(volMin, dmin(volMax, Src[S_VOL*n + i] + mult*dVdt));
+    const double dVdt = -m*safeInvVar(rho*rho)*drho;
+    S[S_VOL*n + i] = dmax(volMin, dmin(volMax, vol0 + mult*dVdt));
   }
   // specific thermal energy: IncrementFieldList (or the compatible policy, already applied)
   double eps;
   if (!epsDone) {
-    eps = Src[S_EPS*n + i] + mult*(D[D_DEPSDT*n + i]);
+    eps = eps0 + mult*(D[D_DEPSDT*n + i]);
     S[S_EPS*n + i] = eps;
   } else {
     eps = S[S_EPS*n + i];
   }
   // pressure, sound speed (GammaLawGas, no active pressure limits)
   const double g1 = P.gamma - 1.0;
-  S[S_P*n + i] = g1*rho*eps;
-  S[S_CS*n + i] = sqrt(dmax(0.0, P.gamma*g1*eps));
+  const double Pn = g1*rho*eps;
+  const double csn = sqrt(dmax(0.0, P.gamma*g1*eps));
+  S[S_P*n + i] = Pn;
+  S[S_CS*n + i] = csn;
   // velocity: IncrementFieldList (after the energy it depends on)
-  for (int c = 0; c < 3; ++c) S[(S_VX + c)*n + i] = Src[(S_VX + c)*n + i] + D[(D_DVDT + c)*n + i]*mult;
+  v = V3{v.x + D[(D_DVDT + 0)*n + i]*mult, v.y + D[(D_DVDT + 1)*n + i]*mult, v.z + D[(D_DVDT + 2)*n + i]*mult};
+  S[S_VX*n + i] = v.x; S[S_VY*n + i] = v.y; S[S_VZ*n + i] = v.z;
+  // the internal node's record for the next pair loop, from the new state
+  const bool pack = packMode != 0 && !crk &&
+                    (packMode == 1 ? !P.gradh : P.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM);
+  if (pack) {
+    const double omega = S[S_OMEGA*n + i];
+    if (P.precision == SPHGPU_PRECISION_MIXED) writeMixedRecord(MB.mrec, i, x, v, m, rho, csn, Pn, omega, Hn);
+    else writeRecord(MB.rec, i, x, v, m, rho, csn, Pn, omega, Hn);
+  }
 }
 
 __global__ void __launch_bounds__(256) eos_kernel(const Member* mem, BlockMap bm) {
@@ -723,6 +763,35 @@ int map_nodes(Batch& b, int threads, BlockMap* bm, unsigned* grid) {
 
 }  // namespace
 
+bool packedByUpdate(const Problem& p, int packMode) {
+  if (p.prm.hydro != SPHGPU_HYDRO_SPH) return false;
+  if (packMode == PACK_FOR_EVAL) return !p.prm.gradh;               // grad-h changes omega after the update
+  if (packMode == PACK_FOR_FINALIZE) return p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM;
+  return false;
+}
+
+namespace {
+
+// Records of every node (full) or of the ghosts only, one launch each.
+template<class Want, class Ghosts>
+int launch_pack(Batch& b, Want want, Ghosts ghostsOnly, bool mixed) {
+  for (int g = 0; g < 2; ++g) {
+    BlockMap bm;
+    unsigned grid = 0;
+    SPH_TRY(batch_map_items(b, [&](const Problem& p) {
+      if (!want(p) || ghostsOnly(p) != (g == 1)) return (int64_t)0;
+      if (g == 1) return b.capacityGrids ? p.gcap : p.G;
+      return b.capacityGrids ? p.candcap : p.n + p.G; }, 256, &bm, &grid));
+    if (!grid) continue;
+    if (mixed) pack_mixed_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm, g);
+    else pack_records_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm, g);
+    batch_count_launch(b);
+  }
+  return cuda_status(cudaGetLastError(), mixed ? "pack mixed records" : "pack_records");
+}
+
+}  // namespace
+
 int pack_records(Batch& b, int need) {
   if (b.memDirty) SPH_TRY(batch_upload(b));
   // which members read the FP64 records before the next pack
@@ -735,12 +804,23 @@ int pack_records(Batch& b, int need) {
                      p.cfg.precision == SPHGPU_PRECISION_FP64);
     return true;
   };
-  BlockMap bm;
-  unsigned grid = 0;
-  SPH_TRY(batch_map_items(b, [&](const Problem& p) {
-    return wants(p) ? (b.capacityGrids ? p.candcap : p.n + p.G) : (int64_t)0; }, 256, &bm, &grid));
-  if (grid) { pack_records_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
-  return cuda_status(cudaGetLastError(), "pack_records");
+  // internal records the update kernel already wrote (FP64 members)
+  auto ghosts = [&](const Problem& p) {
+    return need != PACK_ALL && b.packedByUpdate == need && p.cfg.precision == SPHGPU_PRECISION_FP64 &&
+           packedByUpdate(p, need);
+  };
+  return launch_pack(b, wants, ghosts, false);
+}
+
+int pack_mixed(Batch& b, bool rigorousSumOnly) {
+  if (b.memDirty) SPH_TRY(batch_upload(b));
+  const int need = rigorousSumOnly ? PACK_FOR_FINALIZE : PACK_FOR_EVAL;
+  auto wants = [&](const Problem& p) {
+    return p.cfg.precision == SPHGPU_PRECISION_MIXED && p.prm.hydro == SPHGPU_HYDRO_SPH &&
+           (!rigorousSumOnly || p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM);
+  };
+  auto ghosts = [&](const Problem& p) { return b.packedByUpdate == need && packedByUpdate(p, need); };
+  return launch_pack(b, wants, ghosts, true);
 }
 
 int launch_gradh(Batch& b) {
@@ -803,12 +883,13 @@ int launch_compatible_energy(Batch& b, double scale) {
   return cuda_status(cudaGetLastError(), "compatible energy");
 }
 
-int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode) {
+int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode, int packMode) {
   BlockMap bm;
   unsigned grid = 0;
   SPH_TRY(map_nodes(b, 256, &bm, &grid));
+  b.packedByUpdate = packMode;
   if (grid) {
-    update_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm, scale, timeAdvanceOnly ? 1 : 0, mode);
+    update_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm, scale, timeAdvanceOnly ? 1 : 0, mode, packMode);
     batch_count_launch(b);
   }
   return cuda_status(cudaGetLastError(), "update");

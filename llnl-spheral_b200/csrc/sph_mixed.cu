@@ -51,32 +51,6 @@ __device__ __forceinline__ MRec loadMRec(const double* mrec, int64_t k) {
   return R;
 }
 
-__global__ void __launch_bounds__(256) pack_mixed_kernel(const Member* mem, BlockMap bm) {
-  const MemberBlock mb = memberBlock(bm);
-  const Member& MB = mem[mb.m];
-  const int64_t n = MB.n;
-  const int64_t k = mb.block*blockDim.x + threadIdx.x;
-  if (k >= n + scalI(MB.scal, SC_G)) return;
-  const double* S = MB.S;
-  const int64_t r = k < n ? k : MB.groot[k - n];
-  V3 x{S[S_X*n + r], S[S_Y*n + r], S[S_Z*n + r]};
-  if (k >= n) x = ghostPosition(MB.prm.bcs, x, MB.gcode[k - n]);
-  const Sym H{S[(S_H + 0)*n + r], S[(S_H + 1)*n + r], S[(S_H + 2)*n + r],
-              S[(S_H + 3)*n + r], S[(S_H + 4)*n + r], S[(S_H + 5)*n + r]};
-  const double m = S[S_M*n + r], rho = S[S_RHO*n + r], P = S[S_P*n + r];
-  const double somega = safeInv(S[S_OMEGA*n + r], 1.0e-30);
-  double2* q = reinterpret_cast<double2*>(MB.mrec + k*MRECW);
-  q[0] = make_double2(x.x, x.y);
-  q[1] = make_double2(x.z, S[S_VX*n + r]);
-  q[2] = make_double2(S[S_VY*n + r], S[S_VZ*n + r]);
-  float4* f = reinterpret_cast<float4*>(q + 3);
-  f[0] = make_float4((float)m, (float)rho, (float)S[S_CS*n + r], (float)sdet(H));
-  f[1] = make_float4((float)H.xx, (float)H.xy, (float)H.xz, (float)H.yy);
-  f[2] = make_float4((float)H.yz, (float)H.zz, (float)(somega*P/(rho*rho)), (float)(m/rho));
-  const bool iso = H.xy == 0.0 && H.xz == 0.0 && H.yz == 0.0 && H.xx == H.yy && H.xx == H.zz;
-  f[3] = make_float4((float)P, (float)somega, iso ? 1.0f : 0.0f, 0.0f);
-}
-
 __global__ void table_to_float_kernel(const double* coef, int n, float* out) {
   for (int t = blockIdx.x*blockDim.x + threadIdx.x; t < 6*n; t += gridDim.x*blockDim.x) out[t] = (float)coef[t];
 }
@@ -387,16 +361,6 @@ int prepare_mixed(Batch& b) {
 // own records and kernels, crk_mixed.cu)
 bool mixedSph(const Problem& p) {
   return p.cfg.precision == SPHGPU_PRECISION_MIXED && p.prm.hydro == SPHGPU_HYDRO_SPH;
-}
-
-int pack_mixed(Batch& b, bool rigorousSumOnly) {
-  BlockMap bm;
-  unsigned grid = 0;
-  SPH_TRY(batch_map_items(b, [&](const Problem& p) {
-    const bool want = mixedSph(p) && (!rigorousSumOnly || p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM);
-    return want ? (b.capacityGrids ? p.candcap : p.n + p.G) : (int64_t)0; }, 256, &bm, &grid));
-  if (grid) { pack_mixed_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
-  return cuda_status(cudaGetLastError(), "pack mixed records");
 }
 
 int launch_sum_density_mixed(Batch& b) {
