@@ -323,13 +323,15 @@ int initialize_impl(Batch& b) {
 }
 
 // Physics::finalize: CRK volumes then the summed density, or the SPH sum.
-int finalize_impl(Batch& b) {
+// enforce: the step's enforceBoundaries follows; the summed-density
+// kernels apply it to their members
+int finalize_impl(Batch& b, bool enforce) {
   if (anyMember(b, isCrkP)) {
     SPH_TRY(crk_volume(b, false));
     SPH_TRY(launch_crk_sum_density(b));
   }
-  SPH_TRY(launch_sum_density(b));
-  if (anyMember(b, isMixedSph)) SPH_TRY(launch_sum_density_mixed(b));
+  SPH_TRY(launch_sum_density(b, enforce));
+  if (anyMember(b, isMixedSph)) SPH_TRY(launch_sum_density_mixed(b, enforce));
   return SPHGPU_OK;
 }
 
@@ -380,9 +382,9 @@ int step_after_connectivity(Batch& b) {
   SPH_TRY(launch_update(b, 1.0, false, 2, PACK_FOR_FINALIZE));
   // applyGhostBoundaries; postStepFinalize (sum density); enforceBoundaries
   SPH_TRY(pack_records(b, PACK_FOR_FINALIZE));
-  SPH_TRY(finalize_impl(b));
+  SPH_TRY(finalize_impl(b, true));
   b.packedByUpdate = 0;
-  SPH_TRY(launch_enforce_boundaries(b));
+  SPH_TRY(launch_enforce_boundaries(b, true));
   SPH_TRY(launch_finish_step(b));
   return SPHGPU_OK;
 }
@@ -928,7 +930,7 @@ int sphgpu_finalize(sphgpu_problem* p, double time, double dt) {
   (void)time; (void)dt;
   SPH_TRY(require_nbrs(solo(p)));
   SPH_TRY(pack_records(solo(p)));
-  return finalize_impl(solo(p));
+  return finalize_impl(solo(p), false);
 }
 
 int sphgpu_dt(sphgpu_problem* p, double* dt_out) {

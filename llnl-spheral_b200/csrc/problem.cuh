@@ -457,14 +457,17 @@ bool packedByUpdate(const Problem& p, int packMode);
 int launch_gradh(Batch& b);
 int launch_eval_sph_fp64(Batch& b);
 int launch_eval_sph_mixed(Batch& b);
-int launch_sum_density(Batch& b);          // plain FP64 SPH members
-int launch_sum_density_mixed(Batch& b);    // mixed-precision SPH members (sph_mixed.cu)
+// summed density of the plain FP64 / mixed-precision SPH members; enforce:
+// also apply the step's periodic wrap to those members' positions
+int launch_sum_density(Batch& b, bool enforce = false);
+int launch_sum_density_mixed(Batch& b, bool enforce = false);
 // mode: 0 in place, 1 save state0 first (mid point), 2 from state0 (full step);
 // packMode (PackNeed): also write the internal nodes' records for the next
 // evaluation (1) or summed density (2), 0: none
 int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode, int packMode = 0);
 int launch_compatible_energy(Batch& b, double scale);
-int launch_enforce_boundaries(Batch& b);
+// skipSummed: leave out the SPH members whose summed density already wrapped them
+int launch_enforce_boundaries(Batch& b, bool skipSummed = false);
 int launch_eos(Batch& b);
 int launch_dt(Batch& b, int slot, bool cachedEig);
 // one iterateIdealH iteration of a single problem; deltaH[n] per-node changes

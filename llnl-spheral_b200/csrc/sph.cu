@@ -330,7 +330,38 @@ __global__ void __launch_bounds__(128) gradh_kernel(const Member* mem, BlockMap 
 }
 
 // ---------------------------------------------------------------- sum density
-__global__ void __launch_bounds__(128) sum_density_kernel(const Member* mem, BlockMap bm) {
+// PeriodicBoundary::enforceBoundary (src/Boundary/PeriodicBoundary.cc:145-203)
+// for one internal node's position.
+__device__ __forceinline__ V3 enforcedPosition(const BoxBCs& bcs, V3 r) {
+  for (int pb = 0; pb < 6; pb += 2) {
+    if (!bcs.periodic[pb >> 1]) continue;
+    for (int sub = 0; sub < 2; ++sub) {
+      const PlanarBC& bc = bcs.bc[pb + sub];
+      if (planeCompare(bc.enter, r) == 1) r = mapPositionThroughPlanes(r, bc.enter, bc.exit);
+    }
+    const PlaneD& plane1 = bcs.bc[pb].enter;
+    const PlaneD& plane2 = bcs.bc[pb].exit;
+    if (planeCompare(plane1, r) == 1 || planeCompare(plane2, r) == 1) {
+      const double L = minimumDistance(plane1, plane2.point);
+      const V3 p0 = vadd(r, vmul(plane1.normal, dot(vsub(plane1.point, r), plane1.normal)));
+      const double f = dmax(-1.0, dmin(1.0, fmod(signedDistance(plane1, r)/L, 1.0)));
+      r = vadd(p0, vmul(plane1.normal, f*L));
+    }
+  }
+  return r;
+}
+
+__device__ __forceinline__ void enforceNode(const Member& MB, int64_t i) {
+  double* S = MB.S;
+  const int64_t n = MB.n;
+  const V3 r = enforcedPosition(MB.prm.bcs, V3{S[S_X*n + i], S[S_Y*n + i], S[S_Z*n + i]});
+  S[S_X*n + i] = r.x; S[S_Y*n + i] = r.y; S[S_Z*n + i] = r.z;
+}
+
+// enforce: also wrap the node's position through the periodic planes (the
+// step's enforceBoundaries, which follows the summed density; the pair
+// terms read positions from the records, never from the state)
+__global__ void __launch_bounds__(128) sum_density_kernel(const Member* mem, BlockMap bm, int enforce) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = mem[mb.m];
   const int64_t n = MB.n;
@@ -355,6 +386,76 @@ __global__ void __launch_bounds__(128) sum_density_kernel(const Member* mem, Blo
   }
   if (!selfDone) rho += mi*W0;
   MB.S[S_RHO*n + i] = rho;
+  if (enforce) enforceNode(MB, i);
+}
+
+// ---------------------------------------------------------------- summed density, mixed form
+struct KahanSum {
+  float s, c;
+  __device__ __forceinline__ void add(float x) {
+    const float y = x - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+// FP32 TableKernel value (the FP32 copy of the coefficient table).
+__device__ __forceinline__ float tableW32(const float* coef, int n, float invStep, float extent, float eta,
+                                          float Hdet) {
+  if (!(eta < extent)) return 0.0f;
+  const float q = eta*invStep;
+  int lb = (int)q;
+  lb = lb < n - 1 ? lb : n - 1;
+  const int i0 = lb < n - 3 ? lb : n - 3;
+  const float x = q - (float)i0;
+  const float2* c = reinterpret_cast<const float2*>(coef + 6*(i0 + 1));
+  const float2 c01 = __ldg(c), c23 = __ldg(c + 1);
+  return Hdet*(c01.x + x*(c01.y + x*c23.x));
+}
+
+// computeSPHSumMassDensity (src/SPH/computeSPHSumMassDensity.cc:27-111),
+// RigorousSumDensity, mixed form: rho_i = m_i W(0) + sum_j m_j W(|H_j r_ij|)
+// with the pair terms in FP32 (r_ij formed in FP64, rounded once) and a
+// Kahan-compensated FP32 sum, from the mixed records of the end-of-step
+// state.  enforce as for sum_density_kernel.
+__global__ void __launch_bounds__(128) sum_density_mixed_kernel(const Member* mem, BlockMap bm, int enforce) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& MB = mem[mb.m];
+  const int64_t n = MB.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Params& P = MB.prm;
+  const float* coefF = MB.coefF;
+  const double* mrec = MB.mrec;
+  const int32_t* nbr = MB.nbr;
+  const float invStep = (float)(1.0/P.W.stepSize), extent = (float)P.W.extent;
+  const double2* qi = reinterpret_cast<const double2*>(mrec + i*MRECW);
+  const double2 a0 = __ldg(qi), a1 = __ldg(qi + 1);
+  const float4 bi = __ldg(reinterpret_cast<const float4*>(qi + 3));
+  const float W0 = tableW32(coefF, P.W.n, invStep, extent, 0.0f, bi.w);
+  KahanSum rho{0.0f, 0.0f};
+  bool selfDone = false;
+  const int64_t k0 = MB.offsets[i], k1 = MB.offsets[i + 1];
+  for (int64_t k = k0; k < k1; ++k) {
+    const int32_t j = __ldg(nbr + k);
+    if (!selfDone && j > (int32_t)i) { rho.add(bi.x*W0); selfDone = true; }
+    const double2* q = reinterpret_cast<const double2*>(mrec + (int64_t)j*MRECW);
+    const double2 c0 = __ldg(q), c1 = __ldg(q + 1);
+    const float4* f = reinterpret_cast<const float4*>(q + 3);
+    const float4 f0 = __ldg(f), f1 = __ldg(f + 1);
+    const float2 f2 = __ldg(reinterpret_cast<const float2*>(f + 2));
+    const float rx = (float)(a0.x - c0.x), ry = (float)(a0.y - c0.y), rz = (float)(a1.x - c1.x);
+    const float ex = f1.x*rx + f1.y*ry + f1.z*rz;
+    const float ey = f1.y*rx + f1.w*ry + f2.x*rz;
+    const float ez = f1.z*rx + f2.x*ry + f2.y*rz;
+    const float eta = sqrtf(ex*ex + ey*ey + ez*ez);
+    rho.add(f0.x*tableW32(coefF, P.W.n, invStep, extent, eta, f0.w));
+  }
+  if (!selfDone) rho.add(bi.x*W0);
+  MB.S[S_RHO*n + i] = rho.value();
+  if (enforce) enforceNode(MB, i);
 }
 
 // ---------------------------------------------------------------- compatible energy
@@ -537,31 +638,13 @@ __global__ void __launch_bounds__(256) eos_kernel(const Member* mem, BlockMap bm
   S[S_CS*n + i] = sqrt(dmax(0.0, gamma*g1*eps));
 }
 
+// PeriodicBoundary::enforceBoundary over every internal node of the members
 __global__ void __launch_bounds__(256) enforce_boundaries_kernel(const Member* mem, BlockMap bm) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = mem[mb.m];
-  const int64_t n = MB.n;
   const int64_t i = mb.block*blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double* S = MB.S;
-  const BoxBCs& bcs = MB.prm.bcs;
-  V3 r{S[S_X*n + i], S[S_Y*n + i], S[S_Z*n + i]};
-  for (int pb = 0; pb < 6; pb += 2) {
-    if (!bcs.periodic[pb >> 1]) continue;
-    for (int sub = 0; sub < 2; ++sub) {
-      const PlanarBC& bc = bcs.bc[pb + sub];
-      if (planeCompare(bc.enter, r) == 1) r = mapPositionThroughPlanes(r, bc.enter, bc.exit);
-    }
-    const PlaneD& plane1 = bcs.bc[pb].enter;
-    const PlaneD& plane2 = bcs.bc[pb].exit;
-    if (planeCompare(plane1, r) == 1 || planeCompare(plane2, r) == 1) {
-      const double L = minimumDistance(plane1, plane2.point);
-      const V3 p0 = vadd(r, vmul(plane1.normal, dot(vsub(plane1.point, r), plane1.normal)));
-      const double f = dmax(-1.0, dmin(1.0, fmod(signedDistance(plane1, r)/L, 1.0)));
-      r = vadd(p0, vmul(plane1.normal, f*L));
-    }
-  }
-  S[S_X*n + i] = r.x; S[S_Y*n + i] = r.y; S[S_Z*n + i] = r.z;
+  if (i >= MB.n) return;
+  enforceNode(MB, i);
 }
 
 // ---------------------------------------------------------------- iterateIdealH
@@ -866,13 +949,26 @@ int launch_eval_sph_fp64(Batch& b) {
   return cuda_status(cudaGetLastError(), "evaluate (FP64)");
 }
 
-int launch_sum_density(Batch& b) {
+bool summedSph(const Problem& p) { return isSph(p) && p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM; }
+
+int launch_sum_density(Batch& b, bool enforce) {
   BlockMap bm;
   unsigned grid = 0;
   SPH_TRY(batch_map_items(b, [](const Problem& p) {
-    return isFp64Sph(p) && p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM ? p.n : (int64_t)0; }, 128, &bm, &grid));
-  if (grid) { sum_density_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+    return isFp64Sph(p) && summedSph(p) ? p.n : (int64_t)0; }, 128, &bm, &grid));
+  if (grid) { sum_density_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm, enforce ? 1 : 0); batch_count_launch(b); }
   return cuda_status(cudaGetLastError(), "sum density");
+}
+
+int launch_sum_density_mixed(Batch& b, bool enforce) {
+  SPH_TRY(prepare_mixed(b));
+  SPH_TRY(pack_mixed(b, true));
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(batch_map_items(b, [](const Problem& p) {
+    return p.cfg.precision == SPHGPU_PRECISION_MIXED && summedSph(p) ? p.n : (int64_t)0; }, 128, &bm, &grid));
+  if (grid) { sum_density_mixed_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm, enforce ? 1 : 0); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "sum density (mixed)");
 }
 
 int launch_compatible_energy(Batch& b, double scale) {
@@ -904,10 +1000,11 @@ int launch_eos(Batch& b) {
   return cuda_status(cudaGetLastError(), "eos");
 }
 
-int launch_enforce_boundaries(Batch& b) {
+int launch_enforce_boundaries(Batch& b, bool skipSummed) {
   BlockMap bm;
   unsigned grid = 0;
-  SPH_TRY(map_nodes(b, 256, &bm, &grid));
+  SPH_TRY(batch_map_items(b, [&](const Problem& p) { return skipSummed && summedSph(p) ? (int64_t)0 : p.n; },
+                          256, &bm, &grid));
   if (grid) { enforce_boundaries_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
   return cuda_status(cudaGetLastError(), "enforce boundaries");
 }

@@ -80,50 +80,6 @@ __device__ __forceinline__ void tableF(const float* coef, int n, float invStep, 
   }
 }
 
-// computeSPHSumMassDensity (src/SPH/computeSPHSumMassDensity.cc:27-111),
-// RigorousSumDensity, mixed form: rho_i = m_i W(0) + sum_j m_j W(|H_j r_ij|)
-// with the pair terms in FP32 (r_ij formed in FP64, rounded once) and a
-// Kahan-compensated FP32 sum.  Reads the mixed records, packed at the
-// end-of-step state.
-__global__ void __launch_bounds__(128) sum_density_mixed_kernel(const Member* mem, BlockMap bm) {
-  const MemberBlock mb = memberBlock(bm);
-  const Member& MB = mem[mb.m];
-  const int64_t n = MB.n;
-  const int64_t i = mb.block*blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const Params& P = MB.prm;
-  const float* coefF = MB.coefF;
-  const double* mrec = MB.mrec;
-  const int32_t* nbr = MB.nbr;
-  const float invStep = (float)(1.0/P.W.stepSize), extent = (float)P.W.extent;
-  const double2* qi = reinterpret_cast<const double2*>(mrec + i*MRECW);
-  const double2 a0 = __ldg(qi), a1 = __ldg(qi + 1);
-  const float4 bi = __ldg(reinterpret_cast<const float4*>(qi + 3));
-  float W0, gW0;
-  tableF(coefF, P.W.n, invStep, extent, 0.0f, bi.w, W0, gW0);
-  Kahan rho;
-  rho.init();
-  bool selfDone = false;
-  const int64_t k0 = MB.offsets[i], k1 = MB.offsets[i + 1];
-  for (int64_t k = k0; k < k1; ++k) {
-    const int32_t j = __ldg(nbr + k);
-    if (!selfDone && j > (int32_t)i) { rho.add(bi.x*W0); selfDone = true; }
-    const double2* q = reinterpret_cast<const double2*>(mrec + (int64_t)j*MRECW);
-    const double2 c0 = __ldg(q), c1 = __ldg(q + 1);
-    const float4* f = reinterpret_cast<const float4*>(q + 3);
-    const float4 f0 = __ldg(f), f1 = __ldg(f + 1);
-    const float2 f2 = __ldg(reinterpret_cast<const float2*>(f + 2));
-    const F3 r{(float)(a0.x - c0.x), (float)(a0.y - c0.y), (float)(a1.x - c1.x)};
-    const F3 e = symdot(f1.x, f1.y, f1.z, f1.w, f2.x, f2.y, r);
-    const float eta = sqrtf(e.x*e.x + e.y*e.y + e.z*e.z);
-    float W, gW;
-    tableF(coefF, P.W.n, invStep, extent, eta, f0.w, W, gW);
-    rho.add(f0.x*W);
-  }
-  if (!selfDone) rho.add(bi.x*W0);
-  MB.S[S_RHO*n + i] = rho.value();
-}
-
 template<bool XSPH, bool TENSILE, bool COMPAT, bool SOLO>
 __global__ void __launch_bounds__(128, 3) sph_eval_mixed_kernel(const Member* mem, BlockMap bm, const Member single) {
   const MemberBlock mb = memberBlock(bm);
@@ -361,17 +317,6 @@ int prepare_mixed(Batch& b) {
 // own records and kernels, crk_mixed.cu)
 bool mixedSph(const Problem& p) {
   return p.cfg.precision == SPHGPU_PRECISION_MIXED && p.prm.hydro == SPHGPU_HYDRO_SPH;
-}
-
-int launch_sum_density_mixed(Batch& b) {
-  SPH_TRY(prepare_mixed(b));
-  SPH_TRY(pack_mixed(b, true));
-  BlockMap bm;
-  unsigned grid = 0;
-  SPH_TRY(batch_map_items(b, [](const Problem& p) {
-    return mixedSph(p) && p.prm.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM ? p.n : (int64_t)0; }, 128, &bm, &grid));
-  if (grid) { sum_density_mixed_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
-  return cuda_status(cudaGetLastError(), "sum density (mixed)");
 }
 
 int launch_eval_sph_mixed(Batch& b) {
