@@ -411,15 +411,16 @@ __device__ __forceinline__ float symEta2F(const float* h, float x, float y, floa
 struct Walker {
   float hf[6];
   float lam2;          // isotropic H = lam I: lam^2 (then eta_i^2 = lam^2 |r|^2)
+  float lmin;          // min eig(H)
   bool iso;
   float ox, oy, oz;
   int cx, cy, cz;
-  int64_t slot;
+  int32_t slot;
   int32_t idx;
 };
 
 // Walker of sorted slot s; idx >= n marks a ghost slot (no walk).
-__device__ __forceinline__ Walker makeWalker(const Member& M, const NbrArrays& a, const Grid& g, int64_t s) {
+__device__ __forceinline__ Walker makeWalker(const Member& M, const NbrArrays& a, const Grid& g, int32_t s) {
   Walker w;
   w.slot = s;
   w.idx = __ldg(M.sortedIdx + s);
@@ -432,6 +433,7 @@ __device__ __forceinline__ Walker makeWalker(const Member& M, const NbrArrays& a
   w.lam2 = w.hf[0]*w.hf[0];
   const float4 p = __ldg(a.pre + s);
   w.ox = p.x; w.oy = p.y; w.oz = p.z;
+  w.lmin = p.w;
   w.cx = cellCoord(r.x, g.lo[0], g.cell, g.dim[0]);
   w.cy = cellCoord(r.y, g.lo[1], g.cell, g.dim[1]);
   w.cz = cellCoord(r.z, g.lo[2], g.cell, g.dim[2]);
@@ -451,8 +453,8 @@ __device__ __forceinline__ float axisGap(int d, float f) {
 // candidate's cell follows from its slot).
 template<int SUB>
 struct Row {
-  int64_t start, end;
-  int64_t e[2*SUB];
+  int32_t start, end;  // slots (every slot index fits in 32 bits)
+  int32_t e[2*SUB];
   int x0;
 };
 
@@ -470,15 +472,15 @@ __device__ __forceinline__ Row<SUB> loadRow(const Member& M, const Grid& g, cons
   const int nx = x1 - x0 + 1;
   Row<SUB> r;
   r.x0 = x0;
-  r.start = cs[0];
-  r.end = cs[nx];
+  r.start = (int32_t)cs[0];
+  r.end = (int32_t)cs[nx];
 #pragma unroll
-  for (int c = 0; c < 2*SUB; ++c) r.e[c] = c + 1 < nx ? cs[c + 1] : r.end;
+  for (int c = 0; c < 2*SUB; ++c) r.e[c] = c + 1 < nx ? (int32_t)cs[c + 1] : r.end;
   return r;
 }
 
 template<int SUB>
-__device__ __forceinline__ float rowDxc(const Row<SUB>& r, const Walker& w, int64_t k, float cellf) {
+__device__ __forceinline__ float rowDxc(const Row<SUB>& r, const Walker& w, int32_t k, float cellf) {
   int xc = r.x0 - w.cx;
 #pragma unroll
   for (int c = 0; c < 2*SUB; ++c) xc += (k >= r.e[c]);
@@ -507,14 +509,19 @@ __device__ __forceinline__ bool exactTest(const Member& M, int32_t i, int32_t j,
 // pre-test error is below 1e-6 (max h/min h over the problem) relative, and
 // tol (1e-3) is only set when that ratio is <= 100, so it never decides a
 // pair the exact test would decide otherwise.  Undecided pairs take the
-// exact FP64 test in the reference's operation order.
-__device__ __forceinline__ bool candTest(const Member& M, const NbrArrays& a, const Walker& w, int64_t k,
+// exact FP64 test in the reference's operation order.  eta^2 of either node
+// lies in [min eig(H)^2 r^2, max eig(H)^2 r^2]: a candidate beyond the band
+// for the smaller of the two minimum eigenvalues is rejected from r^2 alone
+// (most candidates of the window).
+__device__ __forceinline__ bool candTest(const Member& M, const NbrArrays& a, const Walker& w, int32_t k,
                                          float dxc, float dyc, float dzc, double k2, float k2lo, float k2hi,
                                          bool pretest) {
   if (pretest) {
     const float4 c = __ldg(a.pre + k);
     const float fx = (w.ox - c.x) - dxc, fy = (w.oy - c.y) - dyc, fz = (w.oz - c.z) - dzc;
     const float r2 = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, fz*fz));
+    const float lo = fminf(w.lmin, c.w);
+    if (lo*lo*r2 > k2hi) return false;
     float e2i;
     if (w.iso) e2i = w.lam2*r2;          // the common case: H = lam I
     else e2i = symEta2F(w.hf, fx, fy, fz);
@@ -574,7 +581,7 @@ __global__ void __launch_bounds__(256, SUB == 1 ? 3 : 1) nbr_thread_kernel(const
   bool active = s < allNodes(M);
   Walker me;
   if (active) {
-    me = makeWalker(M, a, g, s);
+    me = makeWalker(M, a, g, (int32_t)s);
     active = me.idx < n;
   }
   // list capacity: the shared-memory list (FILL) or the member's stash (COUNT)
@@ -606,7 +613,7 @@ __global__ void __launch_bounds__(256, SUB == 1 ? 3 : 1) nbr_thread_kernel(const
         const float dyc = (float)dy*cellf;
         const Row<SUB> row = loadRow<SUB>(M, g, me, y, z, fx, gyz, rc2);
         {
-          for (int64_t k = row.start; k < row.end; ++k) {
+          for (int32_t k = row.start; k < row.end; ++k) {
           if (k != s && candTest(M, a, me, k, rowDxc<SUB>(row, me, k, cellf), dyc, dzc, k2, k2lo, k2hi, pretest)) {
             if (collect) {
               const int32_t j = __ldg(M.sortedIdx + k);
@@ -721,7 +728,7 @@ __global__ void __launch_bounds__(256, SUB == 1 ? 3 : 1) nbr_walk_kernel(const M
   if (s >= allNodes(M)) return;
   const NbrArrays a = nbrArrays(M);
   const Grid g = loadGrid(M);
-  const Walker me = makeWalker(M, a, g, s);
+  const Walker me = makeWalker(M, a, g, (int32_t)s);
   if (me.idx >= M.n) return;
   const int32_t i = me.idx;
   const double k2 = M.prm.kernelExtent*M.prm.kernelExtent;
@@ -745,8 +752,8 @@ __global__ void __launch_bounds__(256, SUB == 1 ? 3 : 1) nbr_walk_kernel(const M
       if (SUB > 1 && gyz > rc2) continue;
       const float dyc = (float)dy*cellf;
       const Row<SUB> row = loadRow<SUB>(M, g, me, y, z, fx, gyz, rc2);
-      for (int64_t base = row.start; base < row.end; base += 32) {
-        const int64_t k = base + lane;
+      for (int32_t base = row.start; base < row.end; base += 32) {
+        const int32_t k = base + lane;
         const bool pass = k < row.end && k != s &&
                           candTest(M, a, me, k, rowDxc<SUB>(row, me, k, cellf), dyc, dzc, k2, k2lo, k2hi, pretest);
         const unsigned ballot = __ballot_sync(0xffffffffu, pass);
@@ -1095,7 +1102,7 @@ int build_connectivity(Batch& b) {
       if (herr & DERR_GHOST_CAPACITY) { p.G = 2*p.gcap; redo = true; }        // ghost count unknown: double
       if (herr & DERR_ENTRY_CAPACITY) redo = true;                           // p.E is the true entry count
       if (herr & DERR_LIST_CAPACITY) { p.fillCap = p.maxCount + p.maxCount/4 + 8; redo = true; }
-      else if (p.fillCap > 2*p.maxCount + 64) p.fillCap = 0;                 // re-plan a tighter list
+      else if (p.fillCap > p.maxCount + p.maxCount/2 + 16) p.fillCap = 0;   // re-plan a tighter list
     }
     if (!redo) return SPHGPU_OK;
     SPH_CHECK(cudaStreamSynchronize(b.stream));
