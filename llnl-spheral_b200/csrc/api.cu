@@ -376,9 +376,8 @@ int step_after_connectivity(Batch& b) {
   SPH_TRY(initialize_impl(b));
   SPH_TRY(launch_eval(b));
   // full step from state0 with the mid-point derivatives (the restore of
-  // state0 is folded into the compatible-energy and update kernels), with
-  // the records of the summed density
-  SPH_TRY(launch_compatible_energy(b, 1.0));
+  // state0 and the compatible energy are folded into the update kernel),
+  // with the records of the summed density
   SPH_TRY(launch_update(b, 1.0, false, 2, PACK_FOR_FINALIZE));
   // applyGhostBoundaries; postStepFinalize (sum density); enforceBoundaries
   SPH_TRY(pack_records(b, PACK_FOR_FINALIZE));

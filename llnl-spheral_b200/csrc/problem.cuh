@@ -465,7 +465,6 @@ int launch_sum_density_mixed(Batch& b, bool enforce = false);
 // packMode (PackNeed): also write the internal nodes' records for the next
 // evaluation (1) or summed density (2), 0: none
 int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode, int packMode = 0);
-int launch_compatible_energy(Batch& b, double scale);
 // skipSummed: leave out the SPH members whose summed density already wrapped them
 int launch_enforce_boundaries(Batch& b, bool skipSummed = false);
 int launch_eos(Batch& b);

@@ -459,25 +459,21 @@ __global__ void __launch_bounds__(128) sum_density_mixed_kernel(const Member* me
 }
 
 // ---------------------------------------------------------------- compatible energy
-// Runs in the full step after the mid-point evaluation, where the reference
-// first restores state0: it reads the start-of-step state S0 and writes the
-// new specific thermal energy to S.
-__global__ void __launch_bounds__(128) compatible_energy_kernel(const Member* mem, BlockMap bm, double scale) {
-  const MemberBlock mb = memberBlock(bm);
-  const Member& MB = mem[mb.m];
+// SpecificThermalEnergyPolicy::update (src/Hydro/SpecificThermalEnergyPolicy.cc:66-189,
+// compatible energy) for internal node i: the energy increment rate from the
+// owner-oriented pair accelerations, with the half-step velocities
+// v + a dt/2 of the start-of-step state S0 and the weights |DepsDt| + eps.
+// Evaluated in the full RK2 update, where the reference has restored state0.
+__device__ __forceinline__ double compatibleDepsDt(const Member& MB, int64_t i, double hdt) {
   const int64_t n = MB.n;
-  const int64_t i = mb.block*blockDim.x + threadIdx.x;
-  if (i >= n) return;
   const double* D = MB.D;
-  double* S = MB.S;
+  const double* S = MB.S;
+  const double* S0 = MB.S0;
   const int32_t* nbr = MB.nbr;
   const int32_t* groot = MB.groot;
   const double* pacc = MB.pacc;
   const int64_t ecap = MB.ecap;
-  const double multiplier = scale*MB.scal[SC_DT];
-  const double hdt = 0.5*multiplier;
   const double weighti = fabs(D[D_DEPSDT*n + i]) + kDblEps;
-  const double* S0 = MB.S0;
   const double mi = S[S_M*n + i];                // mass is constant within the step
   const V3 vi{S0[S_VX*n + i], S0[S_VY*n + i], S0[S_VZ*n + i]};
   const V3 ai{D[(D_DVDT + 0)*n + i], D[(D_DVDT + 1)*n + i], D[(D_DVDT + 2)*n + i]};
@@ -503,7 +499,7 @@ __global__ void __launch_bounds__(128) compatible_energy_kernel(const Member* me
       DepsDti += (1.0 - wj)*duji*mj/mi;
     }
   }
-  S[S_EPS*n + i] = S0[S_EPS*n + i] + DepsDti*multiplier;
+  return DepsDti;
 }
 
 // ---------------------------------------------------------------- policies
@@ -524,8 +520,9 @@ __device__ __forceinline__ bool hInsideBounds(const Sym& H, double hmin, double 
 // UPDATE_IN_PLACE: the source is S.  UPDATE_SAVE_START: the source is S,
 // saved to S0 first (state0 = state.copyState()).  UPDATE_FROM_START: the
 // source is S0 (state.assign(state0) fused into the update); with
-// compatible energy the specific thermal energy compatible_energy_kernel
-// wrote to S is kept.  S0 holds only what the rest of the step reads from
+// compatible energy the specific thermal energy comes from
+// compatibleDepsDt (its pair loop reads S0 and the derivatives only, which
+// no thread of this launch writes).  S0 holds only what the rest of the step reads from
 // it: position, velocity, density, energy, H, plus omega with grad-h (the
 // mid-point initialize changes it) and the CRKSPH volume.  Mass is constant
 // and pressure and sound speed are recomputed, so S0 skips them.
@@ -534,7 +531,12 @@ __device__ __forceinline__ bool hInsideBounds(const Sym& H, double hmin, double 
 // packedByUpdate).
 enum UpdateMode { UPDATE_IN_PLACE = 0, UPDATE_SAVE_START = 1, UPDATE_FROM_START = 2 };
 
-__global__ void __launch_bounds__(256) update_kernel(const Member* mem, BlockMap bm, double scale,
+// COMPAT: the launch applies the compatible energy of its compatible members
+// (only from the start-of-step state: mode UPDATE_FROM_START, the full update
+// of the RK2 step); a separate instance keeps the pair loop's registers out of
+// the other updates.
+template<bool COMPAT>
+__global__ void __launch_bounds__(128, 6) update_kernel(const Member* mem, BlockMap bm, double scale,
                                                      int timeAdvanceOnly, int mode, int packMode) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = mem[mb.m];
@@ -542,6 +544,10 @@ __global__ void __launch_bounds__(256) update_kernel(const Member* mem, BlockMap
   const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Params& P = MB.prm;
+  const double mult = scale*MB.scal[SC_DT];
+  // the compatible energy's pair loop first, before the node's fields are live
+  const bool compatible = COMPAT && P.compatible;
+  const double compatDeps = compatible ? compatibleDepsDt(MB, i, 0.5*mult) : 0.0;
   double* S = MB.S;
   double* S0 = MB.S0;
   const double* Src = mode == UPDATE_FROM_START ? S0 : S;
@@ -567,8 +573,6 @@ __global__ void __launch_bounds__(256) update_kernel(const Member* mem, BlockMap
   } else if (mode == UPDATE_FROM_START && P.gradh) {
     S[S_OMEGA*n + i] = S0[S_OMEGA*n + i];
   }
-  const int epsDone = (!timeAdvanceOnly && P.compatible) ? 1 : 0;
-  const double mult = scale*MB.scal[SC_DT];
   // H: IncrementBoundedState (half step / IntegrateH) or ReplaceBoundedState (IdealH)
   Sym Hn;
   if (timeAdvanceOnly || P.HUpdate == SPHGPU_H_INTEGRATE) {
@@ -597,14 +601,10 @@ __global__ void __launch_bounds__(256) update_kernel(const Member* mem, BlockMap
     const double dVdt = -m*safeInvVar(rho*rho)*drho;
     S[S_VOL*n + i] = dmax(volMin, dmin(volMax, vol0 + mult*dVdt));
   }
-  // specific thermal energy: IncrementFieldList (or the compatible policy, already applied)
-  double eps;
-  if (!epsDone) {
-    eps = eps0 + mult*(D[D_DEPSDT*n + i]);
-    S[S_EPS*n + i] = eps;
-  } else {
-    eps = S[S_EPS*n + i];
-  }
+  // specific thermal energy: IncrementFieldList, or the compatible policy
+  // (from the start-of-step state: only in the full update)
+  const double eps = compatible ? eps0 + compatDeps*mult : eps0 + mult*(D[D_DEPSDT*n + i]);
+  S[S_EPS*n + i] = eps;
   // pressure, sound speed (GammaLawGas, no active pressure limits)
   const double g1 = P.gamma - 1.0;
   const double Pn = g1*rho*eps;
@@ -971,21 +971,16 @@ int launch_sum_density_mixed(Batch& b, bool enforce) {
   return cuda_status(cudaGetLastError(), "sum density (mixed)");
 }
 
-int launch_compatible_energy(Batch& b, double scale) {
-  BlockMap bm;
-  unsigned grid = 0;
-  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.prm.compatible ? p.n : (int64_t)0; }, 128, &bm, &grid));
-  if (grid) { compatible_energy_kernel<<<grid, 128, 0, b.stream>>>(b.d_mem, bm, scale); batch_count_launch(b); }
-  return cuda_status(cudaGetLastError(), "compatible energy");
-}
-
 int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode, int packMode) {
   BlockMap bm;
   unsigned grid = 0;
-  SPH_TRY(map_nodes(b, 256, &bm, &grid));
+  SPH_TRY(map_nodes(b, 128, &bm, &grid));
   b.packedByUpdate = packMode;
   if (grid) {
-    update_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm, scale, timeAdvanceOnly ? 1 : 0, mode, packMode);
+    bool compat = false;
+    if (!timeAdvanceOnly && mode == UPDATE_FROM_START) for (const Problem* p : b.mem) compat = compat || p->prm.compatible;
+    if (compat) update_kernel<true><<<grid, 128, 0, b.stream>>>(b.d_mem, bm, scale, 0, mode, packMode);
+    else update_kernel<false><<<grid, 128, 0, b.stream>>>(b.d_mem, bm, scale, timeAdvanceOnly ? 1 : 0, mode, packMode);
     batch_count_launch(b);
   }
   return cuda_status(cudaGetLastError(), "update");
