@@ -743,12 +743,20 @@ __global__ void __launch_bounds__(128) hydro_dt_kernel(const Member* mem, BlockM
     const double divvDt = 1.0/(fabs(divv) + kFltMin);
     if (divvDt < minDt) minDt = divvDt;
     const V3 vi{S[S_VX*n + i], S[S_VY*n + i], S[S_VZ*n + i]};
+    // min over the neighbors of nodeScale*safeInvVar(|vi - vj|): sqrt and the
+    // division are correctly rounded and monotone, so it is the term of the
+    // largest |vi - vj|^2, one sqrt and one division per node (bit-identical)
+    double v2max = -1.0;
     for (int64_t k = MB.offsets[i]; k < MB.offsets[i + 1]; ++k) {
       const int32_t j = __ldg(MB.nbr + k);
       const int64_t r = j < n ? (int64_t)j : (int64_t)__ldg(MB.groot + (j - n));
       const V3 vj{ldg(S + S_VX*n + r), ldg(S + S_VY*n + r), ldg(S + S_VZ*n + r)};
-      const double vij = mag(vsub(vi, vj));
-      const double dtVelDiff = nodeScale*safeInvVar(vij, 1e-30);
+      const V3 d = vsub(vi, vj);
+      const double v2 = d.x*d.x + d.y*d.y + d.z*d.z;
+      if (v2 > v2max) v2max = v2;
+    }
+    if (v2max >= 0.0) {
+      const double dtVelDiff = nodeScale*safeInvVar(sqrt(v2max), 1e-30);
       if (dtVelDiff < minDt) minDt = dtVelDiff;
     }
     const V3 a{D[(D_DVDT + 0)*n + i], D[(D_DVDT + 1)*n + i], D[(D_DVDT + 2)*n + i]};
