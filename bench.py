@@ -71,7 +71,9 @@ def parse():
 # stored twice), reads 4 B of CSR index and writes 24 B of pair acceleration
 # per directed entry.
 def eval_alg_bytes(nodes, ghosts, entries):
-    return nodes * 136 + 2 * (nodes + ghosts) * 112 + nodes * 432 + 28 * entries
+    # pack (state in, records out), pair kernel (records in, 54 derivative
+    # doubles out, CSR index in, FP32 pair accelerations out)
+    return nodes * 136 + 2 * (nodes + ghosts) * 112 + nodes * 432 + 16 * entries
 
 
 # DRAM traffic (read + write) of pack_mixed_kernel + sph_eval_mixed_kernel

@@ -261,11 +261,13 @@ __global__ void __launch_bounds__(128, 3) crk_eval_mixed_kernel(const Member* me
                    (deltagrad.z*Psum + deltagrad.z*qsum)*f};
     DvDt[0].add(-force.x*invmi); DvDt[1].add(-force.y*invmi); DvDt[2].add(-force.z*invmi);
     if (COMPAT) {
-      // owner's pair acceleration (-force_owner/m_owner)
+      // owner's pair acceleration (-force_owner/m_owner), FP32 in the mixed
+      // form (both nodes of the pair read the same value)
       const double s = own ? -1.0/(double)I.m : 1.0/(double)J.m;
-      pacc[k] = s*(double)force.x;
-      pacc[ecap + k] = s*(double)force.y;
-      pacc[2*ecap + k] = s*(double)force.z;
+      float* pf = reinterpret_cast<float*>(pacc);
+      pf[k] = (float)(s*(double)force.x);
+      pf[ecap + k] = (float)(s*(double)force.y);
+      pf[2*ecap + k] = (float)(s*(double)force.z);
     }
     DepsDt.add(f*(J.P*dotF(vij, deltagrad) + workQi)*invmi);
     if (XSPH) {

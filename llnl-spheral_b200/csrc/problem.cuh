@@ -9,7 +9,8 @@
 //   groot/gcode [G]       ghost -> internal root node, per-axis image code
 //   offsets [n+1] (i64), nbr [E] (i32)   ConnectivityMap as CSR, ascending j
 //   pacc [3][E]           owner-oriented pair acceleration per CSR entry
-//                         (the reference's "pair-wise accelerations")
+//                         (the reference's "pair-wise accelerations"); FP32
+//                         in the mixed form
 // Ghost nodes are never stored as state: every ghost quantity is read from
 // its root, positions are re-mapped through the periodic planes.
 #pragma once

@@ -472,6 +472,8 @@ __device__ __forceinline__ double compatibleDepsDt(const Member& MB, int64_t i, 
   const int32_t* nbr = MB.nbr;
   const int32_t* groot = MB.groot;
   const double* pacc = MB.pacc;
+  const float* paccF = reinterpret_cast<const float*>(MB.pacc);
+  const bool mixed = MB.prm.precision == SPHGPU_PRECISION_MIXED;
   const int64_t ecap = MB.ecap;
   const double weighti = fabs(D[D_DEPSDT*n + i]) + kDblEps;
   const double mi = S[S_M*n + i];                // mass is constant within the step
@@ -488,7 +490,9 @@ __device__ __forceinline__ double compatibleDepsDt(const Member& MB, int64_t i, 
     const V3 vj{ldg(S0 + S_VX*n + r), ldg(S0 + S_VY*n + r), ldg(S0 + S_VZ*n + r)};
     const V3 aj{ldg(D + (D_DVDT + 0)*n + r), ldg(D + (D_DVDT + 1)*n + r), ldg(D + (D_DVDT + 2)*n + r)};
     const V3 vj12 = vadd(vj, vmul(aj, hdt));
-    const V3 pa{ldg(pacc + k), ldg(pacc + ecap + k), ldg(pacc + 2*ecap + k)};   // owner's pair acceleration
+    // owner's pair acceleration (FP32 in the mixed form)
+    const V3 pa = mixed ? V3{(double)__ldg(paccF + k), (double)__ldg(paccF + ecap + k), (double)__ldg(paccF + 2*ecap + k)}
+                        : V3{ldg(pacc + k), ldg(pacc + ecap + k), ldg(pacc + 2*ecap + k)};
     if (j > (int32_t)i) {
       const double duij = dot(vsub(vj12, vi12), pa);
       const double wi = weighti/(weighti + weightj);

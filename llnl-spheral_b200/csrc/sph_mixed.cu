@@ -189,11 +189,13 @@ __global__ void __launch_bounds__(128, 3) sph_eval_mixed_kernel(const Member* me
     DepsDt.add(J.m*(Prhoi*(vij.x*gradWi.x + vij.y*gradWi.y + vij.z*gradWi.z) + workQi));
     if (COMPAT) {
       // the owner's pair acceleration: -m_other*deltaDvDt in owner orientation
+      // (FP32 in the mixed form; both nodes of the pair read the same value)
       const bool own = j > (int32_t)i;
-      const double s = own ? -(double)J.m : (double)I.m;
-      pacc[k] = s*(double)dd.x;
-      pacc[ecap + k] = s*(double)dd.y;
-      pacc[2*ecap + k] = s*(double)dd.z;
+      const float s = own ? -J.m : I.m;
+      float* pf = reinterpret_cast<float*>(pacc);
+      pf[k] = s*dd.x;
+      pf[ecap + k] = s*dd.y;
+      pf[2*ecap + k] = s*dd.z;
     }
     const float mj = J.m;
     const F3 mg{mj*gradWi.x, mj*gradWi.y, mj*gradWi.z};
