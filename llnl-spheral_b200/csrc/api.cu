@@ -200,6 +200,7 @@ void free_problem(Problem* p) {
 Batch& solo(Problem* p) {
   p->solo->memDirty = true;
   p->solo->packedByUpdate = 0;      // records written by an update belong to that step only
+  p->solo->midInS0 = false;
   return *p->solo;
 }
 
@@ -370,7 +371,7 @@ int step_after_connectivity(Batch& b) {
   // every policy) and the internal nodes' pair records, one kernel; the
   // record passes then cover the ghosts (and the members the update does
   // not pack)
-  SPH_TRY(launch_update(b, 0.5, true, 1, PACK_FOR_EVAL));
+  SPH_TRY(launch_update(b, 0.5, true, 1, PACK_FOR_EVAL, true));
   SPH_TRY(pack_records(b, PACK_FOR_EVAL));
   // initializeDerivatives + derivs.Zero + evaluateDerivatives at the mid point
   SPH_TRY(initialize_impl(b));
@@ -378,7 +379,7 @@ int step_after_connectivity(Batch& b) {
   // full step from state0 with the mid-point derivatives (the restore of
   // state0 and the compatible energy are folded into the update kernel),
   // with the records of the summed density
-  SPH_TRY(launch_update(b, 1.0, false, 2, PACK_FOR_FINALIZE));
+  SPH_TRY(launch_update(b, 1.0, false, 2, PACK_FOR_FINALIZE, true));
   // applyGhostBoundaries; postStepFinalize (sum density); enforceBoundaries
   SPH_TRY(pack_records(b, PACK_FOR_FINALIZE));
   SPH_TRY(finalize_impl(b, true));
@@ -1174,6 +1175,7 @@ int batch_begin(Batch& b) {
   // members' buffers may have moved under their own calls since the last upload
   b.memDirty = true;
   b.packedByUpdate = 0;
+  b.midInS0 = false;
   for (Problem* p : b.mem) SPH_CHECK(cudaStreamSynchronize(p->stream));
   return SPHGPU_OK;
 }

@@ -397,6 +397,8 @@ struct Batch {
   int lastNbrSchedule = 0;
   int evalThreads = 128;         // threads per block of the pair-loop kernels (64, 128 or 256)
   int packedByUpdate = 0;        // records the last update kernel wrote (PackNeed), 0: none
+  bool midInS0 = false;          // a record-only mid-point update ran: its packed SPH
+                                 // members' mid-point H and mass density are in S0
   // CUDA-graph replay of the part of the RK2 step after the connectivity
   // (api.cu): captured once per buffer layout, replayed every step.
   bool useGraph = false;
@@ -464,8 +466,10 @@ int launch_sum_density(Batch& b, bool enforce = false);
 int launch_sum_density_mixed(Batch& b, bool enforce = false);
 // mode: 0 in place, 1 save state0 first (mid point), 2 from state0 (full step);
 // packMode (PackNeed): also write the internal nodes' records for the next
-// evaluation (1) or summed density (2), 0: none
-int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode, int packMode = 0);
+// evaluation (1) or summed density (2), 0: none; recordMid: the RK2 step's
+// record-only mid point for the members the update packs (update_kernel)
+int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode, int packMode = 0,
+                  bool recordMid = false);
 // skipSummed: leave out the SPH members whose summed density already wrapped them
 int launch_enforce_boundaries(Batch& b, bool skipSummed = false);
 int launch_eos(Batch& b);

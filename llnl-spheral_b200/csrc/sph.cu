@@ -80,11 +80,32 @@ __device__ __forceinline__ void nodeRecordState(const Member& M, int64_t k, V3& 
   m = S[S_M*n + r]; rho = S[S_RHO*n + r]; cs = S[S_CS*n + r]; P = S[S_P*n + r]; omega = S[S_OMEGA*n + r];
 }
 
+// A ghost's record from its root's record (written by the update kernel):
+// every field but the position is the root's, the position is mapped
+// through the periodic planes, so the record equals the one packed from the
+// root's state.  W doubles per record, position in the first three.
+template<int W>
+__device__ __forceinline__ void ghostFromRoot(const Member& M, double* recs, int64_t k) {
+  const int64_t r = M.groot[k - M.n];
+  const double2* src = reinterpret_cast<const double2*>(recs + r*W);
+  double2* dst = reinterpret_cast<double2*>(recs + k*W);
+  const double2 p01 = src[0], p2v = src[1];
+  const V3 x = ghostPosition(M.prm.bcs, V3{p01.x, p01.y, p2v.x}, M.gcode[k - M.n]);
+  dst[0] = make_double2(x.x, x.y);
+  dst[1] = make_double2(x.z, p2v.y);
+#pragma unroll
+  for (int c = 2; c < W/2; ++c) dst[c] = src[c];
+}
+
+// ghostsOnly: the update kernel wrote the internal nodes' records (in the
+// RK2 step the state may then hold the start of the step, not the records'
+// mid point), so the ghosts copy their roots' records.
 __global__ void __launch_bounds__(256) pack_records_kernel(const Member* mem, BlockMap bm, int ghostsOnly) {
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
   const int64_t k = (ghostsOnly ? M.n : 0) + mb.block*blockDim.x + threadIdx.x;
   if (k >= M.n + scalI(M.scal, SC_G)) return;
+  if (ghostsOnly) { ghostFromRoot<RECW>(M, M.rec, k); return; }
   V3 x, v; double m, rho, cs, P, omega; Sym H;
   nodeRecordState(M, k, x, v, m, rho, cs, P, omega, H);
   writeRecord(M.rec, k, x, v, m, rho, cs, P, omega, H);
@@ -95,6 +116,7 @@ __global__ void __launch_bounds__(256) pack_mixed_kernel(const Member* mem, Bloc
   const Member& M = mem[mb.m];
   const int64_t k = (ghostsOnly ? M.n : 0) + mb.block*blockDim.x + threadIdx.x;
   if (k >= M.n + scalI(M.scal, SC_G)) return;
+  if (ghostsOnly) { ghostFromRoot<MRECW>(M, M.mrec, k); return; }
   V3 x, v; double m, rho, cs, P, omega; Sym H;
   nodeRecordState(M, k, x, v, m, rho, cs, P, omega, H);
   writeMixedRecord(M.mrec, k, x, v, m, rho, cs, P, omega, H);
@@ -533,6 +555,14 @@ __device__ __forceinline__ bool hInsideBounds(const Sym& H, double hmin, double 
 // packMode 1 / 2 also writes the node's pair record for the mid-point
 // evaluation / the end-of-step summed density (SPH members, see
 // packedByUpdate).
+// recordMid (the RK2 step, with packMode 1 in the mid-point update): for the
+// members whose mid-point records the update writes (SPH without grad-h) the
+// mid-point state lives in those records only.  The mid-point update leaves
+// S at the start of the step and writes to S0 only the start velocity (the
+// compatible energy's pair loop reads it while the full update overwrites
+// S) and the mid-point H and mass density (the mixed pair kernel's FP64
+// finish reads them, sph_eval_mixed_kernel's midInS0); the full update then
+// reads its source state from S.
 enum UpdateMode { UPDATE_IN_PLACE = 0, UPDATE_SAVE_START = 1, UPDATE_FROM_START = 2 };
 
 // COMPAT: the launch applies the compatible energy of its compatible members
@@ -541,7 +571,7 @@ enum UpdateMode { UPDATE_IN_PLACE = 0, UPDATE_SAVE_START = 1, UPDATE_FROM_START 
 // the other updates.
 template<bool COMPAT>
 __global__ void __launch_bounds__(128, 6) update_kernel(const Member* mem, BlockMap bm, double scale,
-                                                     int timeAdvanceOnly, int mode, int packMode) {
+                                                     int timeAdvanceOnly, int mode, int packMode, int recordMid) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = mem[mb.m];
   const int64_t n = MB.n;
@@ -554,9 +584,11 @@ __global__ void __launch_bounds__(128, 6) update_kernel(const Member* mem, Block
   const double compatDeps = compatible ? compatibleDepsDt(MB, i, 0.5*mult) : 0.0;
   double* S = MB.S;
   double* S0 = MB.S0;
-  const double* Src = mode == UPDATE_FROM_START ? S0 : S;
   const double* D = MB.D;
   const bool crk = P.hydro == SPHGPU_HYDRO_CRKSPH;
+  const bool recMid = recordMid && !crk && !P.gradh;
+  const bool midInRecords = recMid && mode == UPDATE_SAVE_START;   // S keeps the start state
+  const double* Src = mode == UPDATE_FROM_START && !recMid ? S0 : S;
   // the source state of the updated fields
   V3 x{Src[S_X*n + i], Src[S_Y*n + i], Src[S_Z*n + i]};
   V3 v{Src[S_VX*n + i], Src[S_VY*n + i], Src[S_VZ*n + i]};
@@ -565,7 +597,9 @@ __global__ void __launch_bounds__(128, 6) update_kernel(const Member* mem, Block
   const Sym H{Src[(S_H + 0)*n + i], Src[(S_H + 1)*n + i], Src[(S_H + 2)*n + i],
               Src[(S_H + 3)*n + i], Src[(S_H + 4)*n + i], Src[(S_H + 5)*n + i]};
   const double vol0 = crk ? Src[S_VOL*n + i] : 0.0;
-  if (mode == UPDATE_SAVE_START) {
+  if (midInRecords) {
+    S0[S_VX*n + i] = v.x; S0[S_VY*n + i] = v.y; S0[S_VZ*n + i] = v.z;
+  } else if (mode == UPDATE_SAVE_START) {
     S0[S_X*n + i] = x.x; S0[S_Y*n + i] = x.y; S0[S_Z*n + i] = x.z;
     S0[S_VX*n + i] = v.x; S0[S_VY*n + i] = v.y; S0[S_VZ*n + i] = v.z;
     S0[S_RHO*n + i] = rho0;
@@ -588,15 +622,16 @@ __global__ void __launch_bounds__(128, 6) update_kernel(const Member* mem, Block
              D[(D_HIDEAL + 3)*n + i], D[(D_HIDEAL + 4)*n + i], D[(D_HIDEAL + 5)*n + i]};
   }
   if (!hInsideBounds(Hn, P.hmin, P.hmax)) atomicOr(MB.err, DERR_H_CLAMP);
-  S[(S_H + 0)*n + i] = Hn.xx; S[(S_H + 1)*n + i] = Hn.xy; S[(S_H + 2)*n + i] = Hn.xz;
-  S[(S_H + 3)*n + i] = Hn.yy; S[(S_H + 4)*n + i] = Hn.yz; S[(S_H + 5)*n + i] = Hn.zz;
+  double* SH = midInRecords ? S0 : S;                // where the new H and mass density go
+  SH[(S_H + 0)*n + i] = Hn.xx; SH[(S_H + 1)*n + i] = Hn.xy; SH[(S_H + 2)*n + i] = Hn.xz;
+  SH[(S_H + 3)*n + i] = Hn.yy; SH[(S_H + 4)*n + i] = Hn.yz; SH[(S_H + 5)*n + i] = Hn.zz;
   // mass density: IncrementBoundedState
   const double drho = D[D_DRHODT*n + i];
   const double rho = dmin(P.rhoMax, dmax(P.rhoMin, rho0 + mult*(drho)));
-  S[S_RHO*n + i] = rho;
+  SH[S_RHO*n + i] = rho;
   // position: IncrementFieldList
   x = V3{x.x + D[(D_DXDT + 0)*n + i]*mult, x.y + D[(D_DXDT + 1)*n + i]*mult, x.z + D[(D_DXDT + 2)*n + i]*mult};
-  S[S_X*n + i] = x.x; S[S_Y*n + i] = x.y; S[S_Z*n + i] = x.z;
+  if (!midInRecords) { S[S_X*n + i] = x.x; S[S_Y*n + i] = x.y; S[S_Z*n + i] = x.z; }
   const double m = S[S_M*n + i];                     // constant within the step
   // CRKSPH node volume: ContinuityVolumePolicy (after mass density and H)
   if (crk) {
@@ -608,16 +643,18 @@ __global__ void __launch_bounds__(128, 6) update_kernel(const Member* mem, Block
   // specific thermal energy: IncrementFieldList, or the compatible policy
   // (from the start-of-step state: only in the full update)
   const double eps = compatible ? eps0 + compatDeps*mult : eps0 + mult*(D[D_DEPSDT*n + i]);
-  S[S_EPS*n + i] = eps;
   // pressure, sound speed (GammaLawGas, no active pressure limits)
   const double g1 = P.gamma - 1.0;
   const double Pn = g1*rho*eps;
   const double csn = sqrt(dmax(0.0, P.gamma*g1*eps));
-  S[S_P*n + i] = Pn;
-  S[S_CS*n + i] = csn;
   // velocity: IncrementFieldList (after the energy it depends on)
   v = V3{v.x + D[(D_DVDT + 0)*n + i]*mult, v.y + D[(D_DVDT + 1)*n + i]*mult, v.z + D[(D_DVDT + 2)*n + i]*mult};
-  S[S_VX*n + i] = v.x; S[S_VY*n + i] = v.y; S[S_VZ*n + i] = v.z;
+  if (!midInRecords) {
+    S[S_EPS*n + i] = eps;
+    S[S_P*n + i] = Pn;
+    S[S_CS*n + i] = csn;
+    S[S_VX*n + i] = v.x; S[S_VY*n + i] = v.y; S[S_VZ*n + i] = v.z;
+  }
   // the internal node's record for the next pair loop, from the new state
   const bool pack = packMode != 0 && !crk &&
                     (packMode == 1 ? !P.gradh : P.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM);
@@ -983,16 +1020,22 @@ int launch_sum_density_mixed(Batch& b, bool enforce) {
   return cuda_status(cudaGetLastError(), "sum density (mixed)");
 }
 
-int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode, int packMode) {
+int launch_update(Batch& b, double scale, bool timeAdvanceOnly, int mode, int packMode, bool recordMid) {
+  if (recordMid && mode == UPDATE_SAVE_START && packMode != PACK_FOR_EVAL) {
+    set_error("a record-only mid-point update packs the mid-point records");
+    return SPHGPU_ERR_ARG;
+  }
   BlockMap bm;
   unsigned grid = 0;
   SPH_TRY(map_nodes(b, 128, &bm, &grid));
   b.packedByUpdate = packMode;
+  b.midInS0 = recordMid && mode == UPDATE_SAVE_START;
+  const int rm = recordMid ? 1 : 0;
   if (grid) {
     bool compat = false;
     if (!timeAdvanceOnly && mode == UPDATE_FROM_START) for (const Problem* p : b.mem) compat = compat || p->prm.compatible;
-    if (compat) update_kernel<true><<<grid, 128, 0, b.stream>>>(b.d_mem, bm, scale, 0, mode, packMode);
-    else update_kernel<false><<<grid, 128, 0, b.stream>>>(b.d_mem, bm, scale, timeAdvanceOnly ? 1 : 0, mode, packMode);
+    if (compat) update_kernel<true><<<grid, 128, 0, b.stream>>>(b.d_mem, bm, scale, 0, mode, packMode, rm);
+    else update_kernel<false><<<grid, 128, 0, b.stream>>>(b.d_mem, bm, scale, timeAdvanceOnly ? 1 : 0, mode, packMode, rm);
     batch_count_launch(b);
   }
   return cuda_status(cudaGetLastError(), "update");

@@ -80,8 +80,12 @@ __device__ __forceinline__ void tableF(const float* coef, int n, float invStep, 
   }
 }
 
+// midInS0: the RK2 step's record-only mid point ran (update_kernel
+// recordMid): the FP64 mid-point H and mass density of a member without
+// grad-h are in S0, S holds the start of the step.
 template<bool XSPH, bool TENSILE, bool COMPAT, bool SOLO>
-__global__ void __launch_bounds__(128, 3) sph_eval_mixed_kernel(const Member* mem, BlockMap bm, const Member single) {
+__global__ void __launch_bounds__(128, 3) sph_eval_mixed_kernel(const Member* mem, BlockMap bm, const Member single,
+                                                                 int midInS0) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = SOLO ? single : mem[mb.m];   // one member: read from the kernel parameters
   const int64_t n = MB.n;
@@ -214,9 +218,10 @@ __global__ void __launch_bounds__(128, 3) sph_eval_mixed_kernel(const Member* me
 
   // ---- per-node finish in FP64 (src/SPH/SPHHydroBase.cc:834-902)
   // exact FP64 node values for the finish
-  const Sym Hi{S[(S_H + 0)*n + i], S[(S_H + 1)*n + i], S[(S_H + 2)*n + i],
-               S[(S_H + 3)*n + i], S[(S_H + 4)*n + i], S[(S_H + 5)*n + i]};
-  const double mi = S[S_M*n + i], rhoi = S[S_RHO*n + i], Hdeti = sdet(Hi);
+  const double* Sm = midInS0 && !P.gradh ? MB.S0 : S;
+  const Sym Hi{Sm[(S_H + 0)*n + i], Sm[(S_H + 1)*n + i], Sm[(S_H + 2)*n + i],
+               Sm[(S_H + 3)*n + i], Sm[(S_H + 4)*n + i], Sm[(S_H + 5)*n + i]};
+  const double mi = S[S_M*n + i], rhoi = Sm[S_RHO*n + i], Hdeti = sdet(Hi);
   const int numNeighbors = (int)(k1 - k0);
   double rhoS = rhoSum.value() + mi*P.W0*Hdeti;
   double nrm = norm.value() + mi/rhoi*P.W0*Hdeti;
@@ -331,6 +336,7 @@ int launch_eval_sph_mixed(Batch& b) {
   };
   const bool solo = b.mem.size() == 1;
   const Member one = solo ? describe_member(*b.mem[0]) : Member{};
+  const int mid = b.midInS0 ? 1 : 0;
   bool present[8] = {false, false, false, false, false, false, false, false};
   for (Problem* p : b.mem) if (mixed(*p)) present[key(*p)] = true;
   for (int v = 0; v < 8; ++v) {
@@ -339,8 +345,8 @@ int launch_eval_sph_mixed(Batch& b) {
                             &bm, &grid));
     if (!grid) continue;
 #define MIX_LAUNCH(X, T, C)                                                                             \
-    if (solo) sph_eval_mixed_kernel<X, T, C, true><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one);  \
-    else sph_eval_mixed_kernel<X, T, C, false><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one)
+    if (solo) sph_eval_mixed_kernel<X, T, C, true><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one, mid);  \
+    else sph_eval_mixed_kernel<X, T, C, false><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one, mid)
     switch (v) {
       case 0: MIX_LAUNCH(false, false, false); break;
       case 1: MIX_LAUNCH(false, false, true); break;
