@@ -852,10 +852,14 @@ int plan_capacities(Batch& b) {
     const int sub = p.grid.sub;
     // cells the grid wants at this subdivision (the last build's, rescaled), else the hint
     const int64_t cells = cells1 > 0.0 ? (int64_t)(cells1*sub*sub*sub) + 1 : p.hintCells;
-    // grow (with slack) only when the buffers hold less than the wanted cells
+    // grow (with slack) when the buffers hold less than the wanted cells, and
+    // once when the first measured count replaces the first build's guess (so
+    // that a later small drift of h does not reallocate mid-run)
     const int64_t cellsNeed = cells > 0 ? grow(cells) : p.candcap/2 + 64;
     const int64_t cellsMin = cells > 0 ? cells + cells/32 + 64 : cellsNeed;
-    if (cellsMin + 1 > p.cellcap) {
+    const bool firstMeasured = cells > 0 && !p.cellsMeasured;
+    if (cells > 0) p.cellsMeasured = true;
+    if (cellsMin + 1 > p.cellcap || (firstMeasured && cellsNeed + 1 > p.cellcap)) {
       cudaStreamSynchronize(b.stream);
       cudaFree(p.cellStart); cudaFree(p.cellFill);
       p.cellStart = nullptr; p.cellFill = nullptr;

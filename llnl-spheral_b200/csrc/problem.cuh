@@ -224,6 +224,7 @@ struct Problem {
   int64_t cellcap = 0;
   int64_t ncells = 0;
   int64_t cellsWanted = 0;      // cells of the last grid at its natural size
+  bool cellsMeasured = false;   // cellcap has been planned from a measured cell count
   int64_t ntot = 0;             // n + ghosts created so far (ghost passes)
   Grid grid{};
 
