@@ -79,7 +79,7 @@ def eval_alg_bytes(nodes, ghosts, entries):
 # DRAM traffic (read + write) of pack_mixed_kernel + sph_eval_mixed_kernel
 # measured by ncu on Kelvin-Helmholtz 96^3 (884,736 nodes, 56,456 ghosts,
 # 5,363,712 entries); scaled to other sizes by the algorithmic bytes.
-EVAL_TRAFFIC_96 = 157972224 + 74632448 + 204818688 + 463323136
+EVAL_TRAFFIC_96 = 150498816 + 67565056 + 190594816 + 386470912
 EVAL_UNITS_96 = (884736, 56456, 5363712)
 
 
