@@ -523,6 +523,9 @@ def measure_serving(pkg, duration, nsteps, rate=20.0, budget=150e9, rank=0, worl
     mine = [trace[k] for k in pkg.sharding.local_items(route, rank)]
     out = {}
     for name, prec in (("mixed", pkg.abi.PRECISION_MIXED), ("plain_fp64", pkg.abi.PRECISION_FP64)):
+        # untimed warm-up on the first requests (library, allocator pool)
+        if mine:
+            s.serve(mine[:4], prec, budget_bytes=budget)
         barrier(world)
         ttc, makespan, stats = s.serve(mine, prec, budget_bytes=budget) if mine else ([], 0.0, None)
         local = {"ttc": ttc, "makespan": makespan,

@@ -39,10 +39,10 @@ template<typename T>
 int dalloc(T*& ptr, int64_t count) {
   ptr = nullptr;
   if (count <= 0) count = 1;
-  const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&ptr), sizeof(T)*(size_t)count);
+  const cudaError_t e = dev_alloc(reinterpret_cast<void**>(&ptr), sizeof(T)*(size_t)count);
   if (e != cudaSuccess) {
     ptr = nullptr;
-    return cuda_status(e, "cudaMalloc");
+    return cuda_status(e, "device allocation");
   }
   return SPHGPU_OK;
 }
@@ -53,10 +53,10 @@ int grow_preserve(T*& ptr, int64_t oldCount, int64_t newCount, cudaStream_t st) 
   SPH_TRY(dalloc(np, newCount));
   if (ptr != nullptr && oldCount > 0) {
     const cudaError_t e = cudaMemcpyAsync(np, ptr, sizeof(T)*(size_t)oldCount, cudaMemcpyDeviceToDevice, st);
-    if (e != cudaSuccess) { cudaFree(np); return cuda_status(e, "grow copy"); }
+    if (e != cudaSuccess) { dev_free(np); return cuda_status(e, "grow copy"); }
   }
   cudaStreamSynchronize(st);
-  cudaFree(ptr);
+  dev_free(ptr);
   ptr = np;
   return SPHGPU_OK;
 }
@@ -188,7 +188,7 @@ void free_problem(Problem* p) {
                   p->cellStart, p->cellFill, p->counts, p->offsets, p->nbr, p->pacc, p->tableCoef, p->nperhTab,
                   p->wsumTab, p->blockSums, p->d_err, p->d_scal, p->d_red, p->staging, p->coefF, p->mrec, p->K, p->crec, p->hmaxi,
                   p->wsumBinsTab, p->qgrad};
-  for (void* q : ptrs) if (q) cudaFree(q);
+  dev_free_all(ptrs, (int)(sizeof(ptrs)/sizeof(ptrs[0])));
   if (p->pinned) cudaFreeHost(p->pinned);
   if (p->solo) { batch_free(*p->solo); delete p->solo; p->solo = nullptr; }
   if (p->ownStream && p->stream) cudaStreamDestroy(p->stream);
@@ -410,7 +410,7 @@ int enable_graph(Batch& b) {
   if (b.memGraphEvent == nullptr) SPH_CHECK(cudaEventCreateWithFlags(&b.memGraphEvent, cudaEventDisableTiming));
   if (b.d_mapArena == nullptr) {
     b.mapArenaCap = 1 << 18;
-    SPH_CHECK(cudaMalloc(&b.d_mapArena, sizeof(int32_t)*b.mapArenaCap));
+    SPH_CHECK(dev_alloc(reinterpret_cast<void**>(&b.d_mapArena), sizeof(int32_t)*b.mapArenaCap));
   }
   return SPHGPU_OK;
 }
@@ -420,10 +420,10 @@ int upload_graph_descriptors(Batch& b) {
   const int nm = (int)b.mem.size();
   if (nm > b.memGraphCap) {
     cudaStreamSynchronize(b.stream);
-    cudaFree(b.d_memGraph); cudaFreeHost(b.h_memGraph);
+    dev_free(b.d_memGraph); cudaFreeHost(b.h_memGraph);
     b.d_memGraph = nullptr; b.h_memGraph = nullptr;
     b.memGraphCap = nm + 16;
-    if (cudaMalloc(&b.d_memGraph, sizeof(Member)*b.memGraphCap) != cudaSuccess ||
+    if (dev_alloc(reinterpret_cast<void**>(&b.d_memGraph), sizeof(Member)*b.memGraphCap) != cudaSuccess ||
         cudaMallocHost(&b.h_memGraph, sizeof(Member)*b.memGraphCap) != cudaSuccess) {
       b.memGraphCap = 0;
       set_error("graph descriptor allocation failed");
@@ -652,7 +652,7 @@ int64_t problem_bytes(const Problem& p) {
 
 int ensure_block_sums(Problem& p, int64_t nblocks) {
   if (nblocks <= p.blockSumsCap) return SPHGPU_OK;
-  cudaFree(p.blockSums);
+  dev_free(p.blockSums);
   p.blockSums = nullptr;
   p.blockSumsCap = nblocks + 64;
   return dalloc(p.blockSums, p.blockSumsCap);
@@ -674,7 +674,7 @@ int ensure_capacity_ghosts(Problem& p, int64_t need) {
     for (int c = 0; c < 3; ++c)
       SPH_CHECK(cudaMemcpyAsync(np + c*ng, p.gpos + c*oldg, sizeof(double)*(size_t)oldg, cudaMemcpyDeviceToDevice, p.stream));
     SPH_CHECK(cudaStreamSynchronize(p.stream));
-    cudaFree(p.gpos);
+    dev_free(p.gpos);
   }
   p.gpos = np;
   p.gcap = ng;
@@ -683,9 +683,9 @@ int ensure_capacity_ghosts(Problem& p, int64_t need) {
   SPH_TRY(grow_preserve(p.offsets, oldc ? oldc + 1 : 0, nc + 1, p.stream));
   SPH_TRY(grow_preserve(p.cidx, 0, nc, p.stream));
   SPH_TRY(grow_preserve(p.sortedIdx, 0, nc, p.stream));
-  cudaFree(p.cand);
+  dev_free(p.cand);
   SPH_TRY(dalloc(p.cand, CAND_DOUBLES*nc));
-  cudaFree(p.rec);
+  dev_free(p.rec);
   SPH_TRY(dalloc(p.rec, RECW*nc));
   p.candcap = nc;
   p.reccap = nc;
@@ -695,8 +695,8 @@ int ensure_capacity_ghosts(Problem& p, int64_t need) {
 int ensure_capacity_entries(Problem& p, int64_t need) {
   if (need <= p.ecap) return SPHGPU_OK;
   const int64_t ne = need + need/8 + 1024;
-  cudaFree(p.nbr);
-  cudaFree(p.pacc);
+  void* old[] = {p.nbr, p.pacc};
+  dev_free_all(old, 2);
   p.nbr = nullptr;
   p.pacc = nullptr;
   SPH_TRY(dalloc(p.nbr, ne));
@@ -1061,7 +1061,7 @@ int sphgpu_checkpoint_load(sphgpu_problem* p, const void* buffer, int64_t bytes)
   SPH_CHECK(cudaMemcpy(p->S, d, sizeof(double)*NSTATE*(size_t)p->n, cudaMemcpyHostToDevice));
   SPH_CHECK(cudaMemcpy(p->D, d + NSTATE*p->n, sizeof(double)*NDERIV*(size_t)p->n, cudaMemcpyHostToDevice));
   if (ncrk) {
-    if (p->K == nullptr && cudaMalloc(&p->K, sizeof(double)*NCRK*(size_t)p->n) != cudaSuccess) {
+    if (p->K == nullptr && dev_alloc(reinterpret_cast<void**>(&p->K), sizeof(double)*NCRK*(size_t)p->n) != cudaSuccess) {
       p->K = nullptr;
       set_error("CRKSPH field allocation failed");
       return SPHGPU_ERR_NOMEM;

@@ -7,10 +7,64 @@
 // prefix table of per-member block counts).  Each member keeps its own
 // buffers, so a member's results do not depend on the other members.
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "problem.cuh"
 
 namespace sphgpu {
+
+namespace {
+
+cudaMemPool_t device_pool() {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = pools.find(dev);
+  if (it != pools.end()) return it->second;
+  cudaMemPoolProps props;
+  std::memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+  uint64_t keep = ~0ULL;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  pools[dev] = pool;
+  return pool;
+}
+
+}  // namespace
+
+cudaError_t dev_alloc(void** ptr, size_t bytes) {
+  *ptr = nullptr;
+  if (bytes == 0) bytes = 1;
+  cudaMemPool_t pool = device_pool();
+  if (pool == nullptr) return cudaErrorMemoryAllocation;
+  cudaError_t e = cudaMallocFromPoolAsync(ptr, bytes, pool, cudaStreamLegacy);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    cudaDeviceSynchronize();
+    cudaMemPoolTrimTo(pool, 0);
+    e = cudaMallocFromPoolAsync(ptr, bytes, pool, cudaStreamLegacy);
+  }
+  if (e != cudaSuccess) { *ptr = nullptr; return e; }
+  return cudaStreamSynchronize(cudaStreamLegacy);
+}
+
+void dev_free_all(void* const* ptrs, int count) {
+  bool any = false;
+  for (int k = 0; k < count; ++k) any = any || ptrs[k] != nullptr;
+  if (!any) return;
+  cudaDeviceSynchronize();
+  for (int k = 0; k < count; ++k) if (ptrs[k]) cudaFreeAsync(ptrs[k], cudaStreamLegacy);
+}
+
+void dev_free(void* ptr) { dev_free_all(&ptr, 1); }
+
 
 namespace {
 
@@ -194,7 +248,7 @@ int batch_init(Batch& b, cudaStream_t stream) {
   for (int k = 0; k < Batch::kMemSlots; ++k)
     if (cudaEventCreateWithFlags(&b.memEvents[k], cudaEventDisableTiming) != cudaSuccess)
       return cuda_status(cudaGetLastError(), "batch event");
-  if (cudaMalloc(&b.d_maps, sizeof(int32_t)*kMapRing) != cudaSuccess ||
+  if (dev_alloc(reinterpret_cast<void**>(&b.d_maps), sizeof(int32_t)*kMapRing) != cudaSuccess ||
       cudaMallocHost(&b.h_maps, sizeof(int32_t)*kMapRing) != cudaSuccess) {
     set_error("batch block-map ring allocation failed");
     return SPHGPU_ERR_NOMEM;
@@ -206,14 +260,15 @@ int batch_init(Batch& b, cudaStream_t stream) {
 
 void batch_free(Batch& b) {
   if (b.stream) cudaStreamSynchronize(b.stream);
-  cudaFree(b.d_memRing); cudaFreeHost(b.h_memRing);
-  cudaFree(b.d_maps); cudaFreeHost(b.h_maps);
-  cudaFree(b.d_gather); cudaFreeHost(b.h_gather);
+  void* dev[] = {b.d_memRing, b.d_maps, b.d_gather, b.d_mapArena, b.d_memGraph};
+  dev_free_all(dev, 5);
+  cudaFreeHost(b.h_memRing);
+  cudaFreeHost(b.h_maps);
+  cudaFreeHost(b.h_gather);
   for (int k = 0; k < Batch::kMemSlots; ++k) if (b.memEvents[k]) cudaEventDestroy(b.memEvents[k]);
   if (b.graphExec) cudaGraphExecDestroy(b.graphExec);
   if (b.sideStream) cudaStreamDestroy(b.sideStream);
-  cudaFree(b.d_mapArena);
-  cudaFree(b.d_memGraph); cudaFreeHost(b.h_memGraph);
+  cudaFreeHost(b.h_memGraph);
   if (b.memGraphEvent) cudaEventDestroy(b.memGraphEvent);
   if (b.ownStream && b.stream) cudaStreamDestroy(b.stream);
   b = Batch();
@@ -227,10 +282,10 @@ int batch_upload(Batch& b) {
   const int nm = (int)b.mem.size();
   if (nm > b.memcap) {
     cudaStreamSynchronize(b.stream);
-    cudaFree(b.d_memRing); cudaFreeHost(b.h_memRing);
+    dev_free(b.d_memRing); cudaFreeHost(b.h_memRing);
     b.d_memRing = nullptr; b.h_memRing = nullptr; b.d_mem = nullptr;
     const int cap = nm + 16;
-    if (cudaMalloc(&b.d_memRing, sizeof(Member)*cap*Batch::kMemSlots) != cudaSuccess ||
+    if (dev_alloc(reinterpret_cast<void**>(&b.d_memRing), sizeof(Member)*cap*Batch::kMemSlots) != cudaSuccess ||
         cudaMallocHost(&b.h_memRing, sizeof(Member)*cap*Batch::kMemSlots) != cudaSuccess) {
       set_error("batch descriptor allocation failed");
       b.memcap = 0;
@@ -319,10 +374,10 @@ int batch_gather(Batch& b, const int* slots, int nslots, std::vector<double>& ou
   const int64_t need = (int64_t)nm*nslots;
   if (need > b.gathercap) {
     cudaStreamSynchronize(b.stream);
-    cudaFree(b.d_gather); cudaFreeHost(b.h_gather);
+    dev_free(b.d_gather); cudaFreeHost(b.h_gather);
     b.d_gather = nullptr; b.h_gather = nullptr;
     const int64_t cap = need + 256;
-    if (cudaMalloc(&b.d_gather, sizeof(double)*cap) != cudaSuccess ||
+    if (dev_alloc(reinterpret_cast<void**>(&b.d_gather), sizeof(double)*cap) != cudaSuccess ||
         cudaMallocHost(&b.h_gather, sizeof(double)*cap) != cudaSuccess) {
       b.gathercap = 0;
       set_error("batch gather allocation failed");

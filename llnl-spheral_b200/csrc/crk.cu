@@ -510,7 +510,7 @@ int crk_prepare(Batch& b) {
     Problem& p = *pp;
     if (p.prm.hydro != SPHGPU_HYDRO_CRKSPH) continue;
     if (p.K == nullptr) {
-      if (cudaMalloc(&p.K, sizeof(double)*NCRK*(size_t)p.n) != cudaSuccess) {
+      if (dev_alloc(reinterpret_cast<void**>(&p.K), sizeof(double)*NCRK*(size_t)p.n) != cudaSuccess) {
         set_error("CRKSPH field allocation failed");
         return SPHGPU_ERR_NOMEM;
       }
@@ -518,7 +518,7 @@ int crk_prepare(Batch& b) {
       b.memDirty = true;
     }
     if (p.prm.qType == SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD && p.qgrad == nullptr) {
-      if (cudaMalloc(&p.qgrad, sizeof(double)*QGRADW*(size_t)p.n) != cudaSuccess) {
+      if (dev_alloc(reinterpret_cast<void**>(&p.qgrad), sizeof(double)*QGRADW*(size_t)p.n) != cudaSuccess) {
         p.qgrad = nullptr;
         set_error("CRKSPH Q gradient allocation failed");
         return SPHGPU_ERR_NOMEM;
@@ -528,9 +528,9 @@ int crk_prepare(Batch& b) {
     }
     if (p.candcap > p.creccap) {
       cudaStreamSynchronize(b.stream);
-      cudaFree(p.crec);
+      dev_free(p.crec);
       p.crec = nullptr;
-      if (cudaMalloc(&p.crec, sizeof(double)*CRECW*(size_t)p.candcap) != cudaSuccess) {
+      if (dev_alloc(reinterpret_cast<void**>(&p.crec), sizeof(double)*CRECW*(size_t)p.candcap) != cudaSuccess) {
         p.creccap = 0;
         set_error("CRKSPH record allocation failed");
         return SPHGPU_ERR_NOMEM;

@@ -861,11 +861,12 @@ int plan_capacities(Batch& b) {
     if (cells > 0) p.cellsMeasured = true;
     if (cellsMin + 1 > p.cellcap || (firstMeasured && cellsNeed + 1 > p.cellcap)) {
       cudaStreamSynchronize(b.stream);
-      cudaFree(p.cellStart); cudaFree(p.cellFill);
+      void* old[] = {p.cellStart, p.cellFill};
+      dev_free_all(old, 2);
       p.cellStart = nullptr; p.cellFill = nullptr;
       p.cellcap = cellsNeed + 1;
-      if (cudaMalloc(&p.cellStart, sizeof(int64_t)*(p.cellcap + 1)) != cudaSuccess ||
-          cudaMalloc(&p.cellFill, sizeof(int32_t)*p.cellcap) != cudaSuccess) {
+      if (dev_alloc(reinterpret_cast<void**>(&p.cellStart), sizeof(int64_t)*(p.cellcap + 1)) != cudaSuccess ||
+          dev_alloc(reinterpret_cast<void**>(&p.cellFill), sizeof(int32_t)*p.cellcap) != cudaSuccess) {
         p.cellcap = 0;
         set_error("cell list allocation failed");
         return SPHGPU_ERR_NOMEM;

@@ -419,6 +419,18 @@ struct Batch {
 
 // batch.cu
 int batch_init(Batch& b, cudaStream_t stream);
+
+// Device buffers of problems and batches come from one stream-ordered memory
+// pool per device that keeps freed blocks (release threshold unlimited), so
+// creating, growing and destroying problems maps no new memory once the pool
+// has grown.  dev_alloc orders the allocation on the legacy stream and
+// synchronises it: the block is ready for every stream on return.  dev_free
+// synchronises the device first, as cudaFree does, so no kernel still reads
+// the block when it returns to the pool; dev_free_all does that once for
+// several blocks.  An allocation that fails trims the pool and retries once.
+cudaError_t dev_alloc(void** ptr, size_t bytes);
+void dev_free(void* ptr);
+void dev_free_all(void* const* ptrs, int count);
 void batch_free(Batch& b);
 int batch_upload(Batch& b);                                  // member descriptors -> device (if dirty)
 Member describe_member(const Problem& p);                    // a problem's descriptor (host)

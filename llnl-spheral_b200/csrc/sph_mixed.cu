@@ -295,7 +295,7 @@ int prepare_mixed(Batch& b) {
     Problem& p = *pp;
     if (p.cfg.precision != SPHGPU_PRECISION_MIXED) continue;
     if (p.coefF == nullptr) {
-      if (cudaMalloc(&p.coefF, sizeof(float)*6*(size_t)p.prm.W.n) != cudaSuccess) {
+      if (dev_alloc(reinterpret_cast<void**>(&p.coefF), sizeof(float)*6*(size_t)p.prm.W.n) != cudaSuccess) {
         set_error("mixed table allocation failed");
         return SPHGPU_ERR_NOMEM;
       }
@@ -305,9 +305,9 @@ int prepare_mixed(Batch& b) {
     const int64_t need = p.candcap;
     if (need > p.mreccap) {
       cudaStreamSynchronize(b.stream);
-      cudaFree(p.mrec);
+      dev_free(p.mrec);
       p.mrec = nullptr;
-      if (cudaMalloc(&p.mrec, sizeof(double)*(p.prm.hydro == SPHGPU_HYDRO_CRKSPH ? CMRECW : MRECW)*(size_t)need) != cudaSuccess) {
+      if (dev_alloc(reinterpret_cast<void**>(&p.mrec), sizeof(double)*(p.prm.hydro == SPHGPU_HYDRO_CRKSPH ? CMRECW : MRECW)*(size_t)need) != cudaSuccess) {
         p.mreccap = 0;
         set_error("mixed record allocation failed");
         return SPHGPU_ERR_NOMEM;
