@@ -185,6 +185,36 @@ def test_batch_of_mixed_sph_and_mixed_crk_members(gpu_lib, pkg):
             assert np.array_equal(s.field(k), m.field(k)), k
 
 
+def test_batch_of_record_only_and_grad_h_members(gpu_lib, pkg):
+    """In the RK2 step the members without grad-h keep their mid-point state
+    in the records only (state0 holds the start velocity and the mid-point H
+    and density), while grad-h members take the full state0 copy.  Both kinds
+    in one batch, FP64 and mixed, compatible energy on and off: each member
+    equals its solo run bit for bit."""
+    abi = pkg.abi
+    specs = [_sod_member(pkg, 48, 1.4, 3.0, abi.PRECISION_MIXED, 31),
+             _sod_member(pkg, 40, 5.0 / 3.0, 2.0, abi.PRECISION_FP64, 32),
+             _sod_member(pkg, 40, 1.5, 4.0, abi.PRECISION_FP64, 33),
+             _sod_member(pkg, 48, 1.3, 2.5, abi.PRECISION_MIXED, 34),
+             _kh_member(pkg, abi.PRECISION_MIXED)]
+    specs[1][1].gradhCorrection = 1
+    specs[3][1].gradhCorrection = 1
+    specs[2][1].compatibleEnergyEvolution = 0
+    specs[2][1].densityUpdate = abi.DENSITY_INTEGRATE
+    solo = [pkg.SPHHydro(cfg, ns) for ns, cfg in specs]
+    mem = [pkg.SPHHydro(cfg, ns) for ns, cfg in specs]
+    for s in solo:
+        s.step(4)
+    batch = pkg.SPHBatch(mem)
+    batch.step(4)
+    for s, m in zip(solo, mem):
+        assert s.time == m.time
+        for k in STATE_KEYS:
+            assert np.array_equal(s.field(k), m.field(k)), k
+        for k in ("delta velocity hydro", "delta specific thermal energy", "new H"):
+            assert np.array_equal(s.field(k), m.field(k)), k
+
+
 def test_batch_rejects_duplicates(gpu_lib, pkg):
     ns, cfg = _sod_member(pkg, 32, 5.0 / 3.0, 4.0, pkg.abi.PRECISION_FP64, 5)
     a = pkg.SPHHydro(cfg, ns)
