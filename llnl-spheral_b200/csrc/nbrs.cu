@@ -568,7 +568,7 @@ __global__ void __launch_bounds__(kGhostThreads) cell_scatter_kernel(const Membe
 // at stash[c*stashStride + s]; nbr_compact_thread_kernel then moves them to
 // offsets[i], and the FILL pass does not run for it.
 template<bool FILL, int SUB>
-__global__ void __launch_bounds__(256, SUB == 1 ? 3 : 1) nbr_thread_kernel(const Member* mem, BlockMap bm, int cap, int maxNbr) {
+__global__ void __launch_bounds__(256, SUB == 1 ? 4 : 1) nbr_thread_kernel(const Member* mem, BlockMap bm, int cap, int maxNbr) {
   extern __shared__ int32_t lst[];
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
