@@ -88,8 +88,11 @@ enum DerivField {
 
 // Packed pair record: everything one side of a pair needs.
 enum RecField {
-  R_X = 0, R_Y, R_Z, R_VX, R_VY, R_VZ, R_M, R_RHO, R_CS, R_HDET,
-  R_H = 10,            // 6
+  // position, m, det H and H first: the summed density and the CRKSPH
+  // volumes read the first 96 bytes (three sectors) of a neighbor's record
+  R_X = 0, R_Y, R_Z, R_M, R_HDET,
+  R_H = 5,             // 6
+  R_VX = 11, R_VY, R_VZ, R_RHO, R_CS,
   R_PRHO = 16,         // safeOmega*P/(rho*rho)  (tensile-free P/rho^2 term)
   R_MRHO = 17,         // m/rho
   R_P = 18,
@@ -106,13 +109,13 @@ __device__ __forceinline__ void writeRecord(double* rec, int64_t k, const V3& x,
   const double somega = safeInv(omega, 1.0e-30);
   double2* q = reinterpret_cast<double2*>(rec + k*RECW);
   q[0] = make_double2(x.x, x.y);
-  q[1] = make_double2(x.z, v.x);
-  q[2] = make_double2(v.y, v.z);
-  q[3] = make_double2(m, rho);
-  q[4] = make_double2(cs, sdet(H));
-  q[5] = make_double2(H.xx, H.xy);
-  q[6] = make_double2(H.xz, H.yy);
-  q[7] = make_double2(H.yz, H.zz);
+  q[1] = make_double2(x.z, m);
+  q[2] = make_double2(sdet(H), H.xx);
+  q[3] = make_double2(H.xy, H.xz);
+  q[4] = make_double2(H.yy, H.yz);
+  q[5] = make_double2(H.zz, v.x);
+  q[6] = make_double2(v.y, v.z);
+  q[7] = make_double2(rho, cs);
   q[8] = make_double2(somega*P/(rho*rho), m/rho);
   q[9] = make_double2(P, somega);
 }

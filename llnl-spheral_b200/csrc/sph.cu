@@ -48,10 +48,12 @@ __device__ __forceinline__ Rec loadRec(const double* rec, int64_t k) {
   const double2 a0 = __ldg(q + 0), a1 = __ldg(q + 1), a2 = __ldg(q + 2), a3 = __ldg(q + 3), a4 = __ldg(q + 4);
   const double2 a5 = __ldg(q + 5), a6 = __ldg(q + 6), a7 = __ldg(q + 7), a8 = __ldg(q + 8), a9 = __ldg(q + 9);
   Rec R;
+  // the layout of writeRecord (problem.cuh)
   R.r = V3{a0.x, a0.y, a1.x};
-  R.v = V3{a1.y, a2.x, a2.y};
-  R.m = a3.x; R.rho = a3.y; R.cs = a4.x; R.Hdet = a4.y;
-  R.H = Sym{a5.x, a5.y, a6.x, a6.y, a7.x, a7.y};
+  R.m = a1.y; R.Hdet = a2.x;
+  R.H = Sym{a2.y, a3.x, a3.y, a4.x, a4.y, a5.x};
+  R.v = V3{a5.y, a6.x, a6.y};
+  R.rho = a7.x; R.cs = a7.y;
   R.Prho = a8.x; R.mrho = a8.y; R.P = a9.x; R.somega = a9.y;
   return R;
 }
