@@ -55,6 +55,9 @@ def parse():
                     help="RK2 steps of the mixed-vs-FP64 error and energy-drift line (0: skip)")
     ap.add_argument("--no-configs", dest="configs", action="store_false",
                     help="skip the Sod (plain FP64) and CRKSPH Kelvin-Helmholtz lines")
+    ap.add_argument("--kernel-survey", action="store_true",
+                    help="no timing: run every kernel of the SPH and CRKSPH steps once on small problems "
+                         "(the workload of the per-kernel profile) and exit")
     ap.add_argument("--batch", type=int, default=256, help="problems in the batched-ensemble line (0: skip)")
     ap.add_argument("--serving", type=float, default=2.0,
                     help="seconds of Poisson arrivals in the serving line (0: skip; 60 = the full trace)")
@@ -738,8 +741,37 @@ def run_ours(args):
     return 0
 
 
+def kernel_survey():
+    """Kelvin-Helmholtz 96^3 (SPH, mixed then FP64) and CRKSPH
+    Kelvin-Helmholtz 64x64x32 (mixed then FP64): build, initialize, one
+    derivative evaluation and two RK2 steps each, so that every kernel of
+    the path launches; nothing is timed."""
+    pkg = importlib.import_module("llnl-spheral_b200")
+    abi, gen = pkg.abi, pkg.generators
+    ns, cfg = kh_problem(pkg, 96)
+    ns2 = gen.kelvin_helmholtz(nx=64, ny=64, nz=32, box=((0, 0, 0), (1.0, 1.0, 1.0)))
+    cases = [(ns, cfg, prec) for prec in (abi.PRECISION_MIXED, abi.PRECISION_FP64)]
+    cases += [(ns2, gen.kh_config(abi, hydro=abi.HYDRO_CRKSPH, precision=prec), None)
+              for prec in (abi.PRECISION_MIXED, abi.PRECISION_FP64)]
+    for nodes, c, prec in cases:
+        if prec is not None:
+            c = c.copy()
+            c.precision = prec
+        h = pkg.SPHHydro(c, nodes)
+        h.build_neighbors()
+        h.initialize()
+        h.evaluateDerivatives()
+        h.step(2)
+        h.synchronize()
+        h.close()
+    print(json.dumps({"kernel_survey": "done", "problems": len(cases)}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.kernel_survey:
+        return kernel_survey()
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
