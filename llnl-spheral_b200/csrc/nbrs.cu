@@ -105,22 +105,25 @@ __global__ void build_init_kernel(const Member* mem, int nmem) {
 // box of the internal nodes and the largest 1/min(eig(H)) (SC_BOUNDS); the
 // largest max(eig(H)) of the problem (with the largest 1/min(eig(H)) it
 // bounds the FP32 pre-test error).
+// Fixed grid (member-local grid stride): each thread accumulates its nodes'
+// bounds, then one set of atomics per block.
 __global__ void __launch_bounds__(kGhostThreads) node_hmax_kernel(const Member* mem, BlockMap bm) {
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
-  const int64_t i = mb.block*blockDim.x + threadIdx.x;
   double lmax = 0.0, h = 0.0;
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  if (i < M.n) {
+  for (int64_t i = mb.block*(int64_t)blockDim.x + threadIdx.x; i < M.n; i += (int64_t)mb.blocks*blockDim.x) {
     const V3 ev = eigenValues(nodeH(M, i));
-    h = 1.0/vmin(ev);
-    M.hmaxi[i] = h;
-    lmax = vmax(ev);
-    M.hmaxi[M.n + i] = lmax;
-    if (!(lmax < 1.0e300)) lmax = 1.0e300;     // degenerate H: no FP32 pre-test
+    const double hi1 = 1.0/vmin(ev);
+    M.hmaxi[i] = hi1;
+    h = fmax(h, hi1);
+    double l = vmax(ev);
+    M.hmaxi[M.n + i] = l;
+    if (!(l < 1.0e300)) l = 1.0e300;           // degenerate H: no FP32 pre-test
+    lmax = dmax(lmax, l);
     const V3 r = nodePos(M, i);
-    lo[0] = r.x; lo[1] = r.y; lo[2] = r.z;
-    hi[0] = r.x; hi[1] = r.y; hi[2] = r.z;
+    lo[0] = fmin(lo[0], r.x); lo[1] = fmin(lo[1], r.y); lo[2] = fmin(lo[2], r.z);
+    hi[0] = fmax(hi[0], r.x); hi[1] = fmax(hi[1], r.y); hi[2] = fmax(hi[2], r.z);
   }
   for (int o = 16; o > 0; o >>= 1) {
     lmax = dmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
@@ -929,18 +932,15 @@ int launch_build(Batch& b) {
   cudaStream_t st = b.stream;
   const int nm = (int)b.mem.size();
   SPH_TRY(batch_upload(b));
-  BlockMap bm;
-  unsigned grid = 0;
   // ---- ghosts: six planar boundaries in order, sizes kept on the device
   build_init_kernel<<<(nm + 127)/128, 128, 0, st>>>(b.d_mem, nm); batch_count_launch(b);
-  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.n; }, kGhostThreads, &bm, &grid));
-  if (grid) { node_hmax_kernel<<<grid, kGhostThreads, 0, st>>>(b.d_mem, bm); batch_count_launch(b); }
   // fixed grids: at most kStreamBlocks blocks per member, member-local stride
   auto fixedItems = [](int64_t cap) { return cap < kStreamBlocks*kGhostThreads ? cap : kStreamBlocks*kGhostThreads; };
   BlockMap nmap, cap;
   unsigned ngrid = 0, capGrid = 0;
   SPH_TRY(batch_map_items(b, [&](const Problem& p) { return fixedItems(p.n); }, kGhostThreads, &nmap, &ngrid));
   SPH_TRY(batch_map_items(b, [&](const Problem& p) { return fixedItems(p.candcap); }, kGhostThreads, &cap, &capGrid));
+  if (ngrid) { node_hmax_kernel<<<ngrid, kGhostThreads, 0, st>>>(b.d_mem, nmap); batch_count_launch(b); }
   bool anyPeriodic = false;
   for (Problem* p : b.mem) for (int a = 0; a < 3; ++a) anyPeriodic = anyPeriodic || p->prm.bcs.periodic[a];
   if (anyPeriodic) {
