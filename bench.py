@@ -24,6 +24,7 @@ import json
 import multiprocessing as mp
 import os
 import platform
+import shutil
 import statistics
 import subprocess
 import sys
@@ -119,15 +120,27 @@ class Clocks:
     def start(self):
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+            # line-buffered output (stdbuf) so that no sample is lost when the
+            # sampler is stopped
+            pre = ["stdbuf", "-oL"] if shutil.which("stdbuf") else []
+            self.proc = subprocess.Popen(pre + ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                                "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.file, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # the sampler takes a moment to start: wait (at most 5 s) for its
+        # first sample, so that it covers the whole timed region
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            if os.path.getsize(self.file.name) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
             return None
+        time.sleep(0.12)          # a sample after the end of the timed region
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
