@@ -2,7 +2,9 @@
 
 FP64 parity translation units are compiled with -fmad=false so that no FMA is
 contracted: their per-pair arithmetic matches the x86-64 FP64 reference bit
-for bit.  The mixed-precision unit keeps FMA contraction on.
+for bit.  The mixed-precision units are too: otherwise the compiler may
+contract the one-problem and the batched instances of a kernel differently,
+and a batch member would differ from its solo run in the last bits.
 
     python llnl-spheral_b200/build.py [--force] [--verbose]
 """
@@ -25,9 +27,9 @@ UNITS = [
     ("batch.cu", []),
     ("nbrs.cu", ["-fmad=false"]),
     ("sph.cu", ["-fmad=false"]),
-    ("sph_mixed.cu", []),
+    ("sph_mixed.cu", ["-fmad=false"]),
     ("crk.cu", ["-fmad=false"]),
-    ("crk_mixed.cu", []),
+    ("crk_mixed.cu", ["-fmad=false"]),
     ("noalloc.cu", []),
     ("server.cu", []),
     ("table.cc", []),
