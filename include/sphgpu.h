@@ -145,6 +145,12 @@ int sphgpu_connectivity_size(sphgpu_problem* p, int64_t* num_ghosts, int64_t* nu
  * internal node it images (ghost_root[num_ghosts]).  Any pointer may be NULL. */
 int sphgpu_get_connectivity(sphgpu_problem* p, int64_t* offsets, int32_t* neighbors,
                             int32_t* ghost_root);
+/* Positions of the ghost nodes of the current connectivity (3 doubles per
+ * ghost, in ghost order): the NodeList's ghost "position" values, each its
+ * root's position mapped through the periodic planes as
+ * PlanarBoundary::setGhostNodes / updateGhostNodes do
+ * (src/Boundary/PlanarBoundary.cc:114-181,361-395). */
+int sphgpu_get_ghost_positions(sphgpu_problem* p, double* positions);
 
 /* Physics::initialize (SPHHydroBase::initialize, src/SPH/SPHHydroBase.cc:430-466;
  * CRKSPHHydroBase::initialize, src/CRKSPH/CRKSPHHydroBase.cc:583-641). */

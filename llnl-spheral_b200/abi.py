@@ -149,6 +149,7 @@ def load_library(path=None):
     lib.sphgpu_build_neighbors.argtypes = [P]
     lib.sphgpu_connectivity_size.argtypes = [P, ctypes.POINTER(I64), ctypes.POINTER(I64)]
     lib.sphgpu_get_connectivity.argtypes = [P, P, P, P]
+    lib.sphgpu_get_ghost_positions.argtypes = [P, P]
     for name in ("sphgpu_initialize", "sphgpu_evaluate_derivatives", "sphgpu_finalize_derivatives",
                  "sphgpu_finalize"):
         getattr(lib, name).argtypes = [P, ctypes.c_double, ctypes.c_double]

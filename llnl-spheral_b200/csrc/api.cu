@@ -901,6 +901,28 @@ int sphgpu_get_connectivity(sphgpu_problem* p, int64_t* offsets, int32_t* neighb
   return SPHGPU_OK;
 }
 
+int sphgpu_get_ghost_positions(sphgpu_problem* p, double* positions) {
+  if (p == nullptr || (positions == nullptr && p->G > 0)) return SPHGPU_ERR_ARG;
+  SPH_TRY(require_nbrs(solo(p)));
+  if (p->G == 0) return SPHGPU_OK;
+  const int64_t n = p->n, G = p->G;
+  std::vector<double> x(3*(size_t)n);
+  std::vector<int32_t> root((size_t)G);
+  std::vector<uint32_t> code((size_t)G);
+  for (int a = 0; a < 3; ++a)
+    SPH_CHECK(cudaMemcpyAsync(x.data() + a*n, p->S + (S_X + a)*n, sizeof(double)*(size_t)n, cudaMemcpyDeviceToHost,
+                              p->stream));
+  SPH_CHECK(cudaMemcpyAsync(root.data(), p->groot, sizeof(int32_t)*(size_t)G, cudaMemcpyDeviceToHost, p->stream));
+  SPH_CHECK(cudaMemcpyAsync(code.data(), p->gcode, sizeof(uint32_t)*(size_t)G, cudaMemcpyDeviceToHost, p->stream));
+  SPH_CHECK(cudaStreamSynchronize(p->stream));
+  for (int64_t g = 0; g < G; ++g) {
+    const int64_t r = root[g];
+    const V3 q = ghostPosition(p->prm.bcs, V3{x[r], x[n + r], x[2*n + r]}, code[g]);
+    positions[3*g] = q.x; positions[3*g + 1] = q.y; positions[3*g + 2] = q.z;
+  }
+  return SPHGPU_OK;
+}
+
 int sphgpu_initialize(sphgpu_problem* p, double time, double dt) {
   if (p == nullptr) return SPHGPU_ERR_ARG;
   (void)time; (void)dt;

@@ -141,7 +141,12 @@ __global__ void __launch_bounds__(256) crk_volume_from_density_kernel(const Memb
   const int64_t i = mb.block*blockDim.x + threadIdx.x;
   if (i >= n) return;
   double* S = MB.S;
-  S[S_VOL*n + i] = S[S_M*n + i]/S[S_RHO*n + i];
+  // mass/massDensity as the reference's FieldList quotient forms it: times
+  // safeInvVar(rho, 1e-60) (src/Field/FieldInline.hh:614-623,
+  // src/Utilities/safeInv.hh:24-27), not a division.
+  const double rho = S[S_RHO*n + i];
+  const double s = rho > 0.0 ? 1.0 : (rho < 0.0 ? -1.0 : 0.0);
+  S[S_VOL*n + i] = S[S_M*n + i]*(s/fmax(1.0e-60, fabs(rho)));
 }
 
 __global__ void __launch_bounds__(128) crk_sum_density_kernel(const Member* mem, BlockMap bm) {

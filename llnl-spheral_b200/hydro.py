@@ -105,6 +105,15 @@ class SPHHydro:
         abi.check(self.lib.sphgpu_get_connectivity(self.h, _p(off), _p(nb), _p(root)), self.lib)
         return off, nb[:e.value], root[:g.value]
 
+    def ghost_positions(self):
+        """Ghost node positions of the current connectivity, (G, 3)."""
+        g = ctypes.c_int64()
+        e = ctypes.c_int64()
+        abi.check(self.lib.sphgpu_connectivity_size(self.h, ctypes.byref(g), ctypes.byref(e)), self.lib)
+        out = np.empty((max(g.value, 1), 3))
+        abi.check(self.lib.sphgpu_get_ghost_positions(self.h, _p(out)), self.lib)
+        return out[:g.value]
+
     def num_pairs(self):
         v = ctypes.c_int64()
         abi.check(self.lib.sphgpu_num_pairs(self.h, ctypes.byref(v)), self.lib)

@@ -6,5 +6,10 @@ namespace boost {
 template<typename... T> using tuple = std::tuple<T...>;
 using std::make_tuple;
 using std::get;
+namespace tuples {
+template<typename... T> using tuple = std::tuple<T...>;
+using std::make_tuple;
+using std::get;
+}
 }
 #endif

@@ -1040,6 +1040,15 @@ void crkEvaluateDerivatives(Problem& p) {
 }
 
 // ContinuityVolumePolicy (fires after the mass density and H updates).
+// CRKMassOverDensity volume: the reference forms mass/massDensity as a
+// FieldList quotient, which multiplies by safeInvVar(rho, 1e-60)
+// (src/Field/FieldInline.hh:614-623, src/Utilities/safeInv.hh:24-27), not a
+// plain division.
+double massOverDensity(double m, double rho) {
+  const double s = rho > 0.0 ? 1.0 : (rho < 0.0 ? -1.0 : 0.0);
+  return m*(s/std::max(1.0e-60, std::fabs(rho)));
+}
+
 void crkVolumeUpdate(Problem& p, double multiplier) {
   for (int i = 0; i < p.nInt; ++i) {
     const double volMin = 0.5*p.m[i]*safeInvVar(p.rho[i]);
@@ -1088,7 +1097,10 @@ bool crkStepRK2(Problem& p, double& dtOut) {
   p.time = t + dt;
   applyGhostBoundaries(p);
   ghostCopy(p, p.vol);
-  crkSumVolume(p);
+  // CRKSPHHydroBase::finalize (src/CRKSPH/CRKSPHHydroBase.cc:1213-1216): the
+  // volume of the configured type, then the summed density.
+  if (p.cfg.crkVolumeType == SPHGPU_CRK_SUMVOLUME) crkSumVolume(p);
+  else for (int i = 0; i < numNodes(p); ++i) p.vol[i] = massOverDensity(p.m[i], p.rho[i]);
   if (p.cfg.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM) crkSumDensity(p);
   enforceBoundaries(p);
   p.cycle += 1;
@@ -1200,7 +1212,7 @@ int orc_build_neighbors(void* h) {
     crkResize(p);
     if (!p.crkVolumeReady) {
       if (p.cfg.crkVolumeType == SPHGPU_CRK_SUMVOLUME) crkSumVolume(p);
-      else for (int i = 0; i < numNodes(p); ++i) p.vol[i] = p.m[i]/p.rho[i];
+      else for (int i = 0; i < numNodes(p); ++i) p.vol[i] = massOverDensity(p.m[i], p.rho[i]);
       p.crkVolumeReady = true;
     }
     ghostCopy(p, p.vol);
@@ -1270,7 +1282,7 @@ int orc_finalize(void* h) {
   Problem& p = *static_cast<Problem*>(h);
   if (p.cfg.hydro == SPHGPU_HYDRO_CRKSPH) {
     if (p.cfg.crkVolumeType == SPHGPU_CRK_SUMVOLUME) crkSumVolume(p);
-    else for (int i = 0; i < numNodes(p); ++i) p.vol[i] = p.m[i]/p.rho[i];
+    else for (int i = 0; i < numNodes(p); ++i) p.vol[i] = massOverDensity(p.m[i], p.rho[i]);
     if (p.cfg.densityUpdate == SPHGPU_DENSITY_RIGOROUS_SUM) crkSumDensity(p);
   } else {
     finalizeStep(p);

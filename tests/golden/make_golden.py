@@ -1,36 +1,146 @@
-"""Regenerate tests/golden/reference_tables.npz from the reference's own code.
+"""Regenerate the fixtures in tests/golden/ from the reference's own code.
 
-Builds oracle/_ref/ref_tables with oracle/build_ref.sh (the reference's
-TableKernel, BSpline/Wendland C4 kernels, Dim<3> geometry and
-mapPositionThroughPlanes compiled unmodified from the reference source tree
-against the stand-in Eigen/boost headers in oracle/refshim), runs it and packs
-its raw outputs into one .npz.  Needs the reference tree, so it runs in the
-development container only; the committed .npz is what the tests read.
+Builds the checkers of oracle/build_ref.py (the reference's sources compiled
+unmodified from the reference tree against the stand-in Eigen/boost headers
+in oracle/refshim), runs them and packs their raw outputs:
 
-    python tests/golden/make_golden.py
+  reference_tables.npz      TableKernel, BSpline / Wendland C4, Dim<3>
+                            geometry, mapPositionThroughPlanes (ref_tables)
+  reference_sph_<case>.npz  one node set run through the reference's
+                            SPHHydroBase / CRKSPHHydroBase, ConnectivityMap,
+                            periodic boundaries and CheapSynchronousRK2
+                            (ref_sph): the inputs, the ghosts and the
+                            ConnectivityMap, every derivative field of one
+                            evaluateDerivatives at t = 0, and the state after a
+                            few RK2 steps
+
+Needs the reference tree, so it runs in the development container only; the
+committed .npz files are what the tests read.
+
+    python tests/golden/make_golden.py [case ...]
 """
+import hashlib
+import importlib
 import os
 import subprocess
+import sys
 import tempfile
 
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 
-def main():
-    exe = subprocess.check_output(["sh", os.path.join(ROOT, "oracle", "build_ref.sh")]).decode().strip().splitlines()[-1]
+def _sod(gen, abi, nx, ny, nz, **kw):
+    box = ((0.0, 0.0, 0.0), (1.0, ny / nx, nz / nx))
+    ns = gen.sod(nx=nx, ny=ny, nz=nz, box=box, jitter=0.05)
+    ns.vel[:, 0] = 0.05 * np.sin(2 * np.pi * ns.pos[:, 0])
+    return ns, gen.sod_config(abi, ns_box=box, **kw)
+
+
+def _kh(gen, abi, nx, ny, nz, **kw):
+    box = ((0.0, 0.0, 0.0), (1.0, ny / nx, nz / nx))
+    ns = gen.kelvin_helmholtz(nx=nx, ny=ny, nz=nz, box=box)
+    return ns, gen.kh_config(abi, xmax=box[1], **kw)
+
+
+def cases(pkg):
+    """name -> (node set, config, RK2 steps).  Together they switch every
+    option the device path implements at least once."""
+    gen, abi = pkg.generators, pkg.abi
+    c = {}
+    c["sod"] = _sod(gen, abi, 16, 4, 4) + (3,)
+    ns, cfg = _sod(gen, abi, 16, 4, 4, gradhCorrection=1, XSPH=1)
+    c["sod_gradh_xsph"] = (ns, cfg, 3)
+    ns, cfg = _sod(gen, abi, 16, 4, 4, densityUpdate=abi.DENSITY_INTEGRATE, HUpdate=abi.H_INTEGRATE,
+                   epsTensile=0.3, nTensile=4.0, linearInExpansion=1, quadraticInExpansion=1)
+    c["sod_integrate_tensile"] = (ns, cfg, 3)
+    c["kh"] = _kh(gen, abi, 12, 12, 6) + (5,)
+    ns, cfg = _kh(gen, abi, 12, 12, 6, compatibleEnergyEvolution=0, useVelocityMagnitudeForDt=1,
+                  correctVelocityGradient=0)
+    c["kh_noncompatible"] = (ns, cfg, 5)
+    c["crk_sod"] = _sod(gen, abi, 16, 4, 4, hydro=abi.HYDRO_CRKSPH) + (3,)
+    c["crk_kh"] = _kh(gen, abi, 12, 12, 6, hydro=abi.HYDRO_CRKSPH) + (5,)
+    ns, cfg = _sod(gen, abi, 16, 4, 4, hydro=abi.HYDRO_CRKSPH, XSPH=1, crkVolumeType=abi.CRK_MASSOVERDENSITY)
+    c["crk_sod_xsph_massoverdensity"] = (ns, cfg, 3)
+    ns, cfg = _sod(gen, abi, 16, 4, 4, hydro=abi.HYDRO_CRKSPH, qType=abi.Q_CRKSPH_MONAGHAN_GINGOLD)
+    c["crk_sod_crkq"] = (ns, cfg, 3)
+    ns, cfg = _kh(gen, abi, 12, 12, 6, hydro=abi.HYDRO_CRKSPH, densityUpdate=abi.DENSITY_INTEGRATE,
+                  crkVolumeType=abi.CRK_MASSOVERDENSITY)
+    c["crk_kh_integrate_massoverdensity"] = (ns, cfg, 5)
+    return c
+
+
+def write_input(path, cfg, ns, nsteps):
+    with open(path, "wb") as f:
+        f.write(np.int64(ns.n).tobytes())
+        f.write(np.int64(nsteps).tobytes())
+        f.write(bytes(cfg))
+        for a in (ns.pos, ns.vel, ns.mass, ns.rho, ns.eps, ns.H):
+            f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
+
+
+def run_reference(exe, cfg, ns, nsteps):
     with tempfile.TemporaryDirectory() as td:
-        subprocess.check_call([exe, td])
-        data = {}
-        for f in sorted(os.listdir(td)):
-            if f.endswith(".f64"):
-                data[f[:-4]] = np.fromfile(os.path.join(td, f), dtype="<f8")
-    out = os.path.join(HERE, "reference_tables.npz")
+        for sub in ("eval", "steps"):
+            os.makedirs(os.path.join(td, sub))
+        write_input(os.path.join(td, "in.bin"), cfg, ns, nsteps)
+        subprocess.check_call([exe, os.path.join(td, "in.bin"), td], stdout=subprocess.DEVNULL)
+        out = {}
+        for sub in ("", "eval", "steps"):
+            d = os.path.join(td, sub)
+            for f in sorted(os.listdir(d)):
+                key = (sub + "/" if sub else "") + f[:-4]
+                if f.endswith(".f64"):
+                    out[key] = np.fromfile(os.path.join(d, f), dtype="<f8")
+                elif f.endswith(".i64"):
+                    out[key] = np.fromfile(os.path.join(d, f), dtype="<i8")
+    return out
+
+
+def sph_fixture(exe, name, ns, cfg, nsteps):
+    r = run_reference(exe, cfg, ns, nsteps)
+    data = {"input/config": np.frombuffer(bytes(cfg), dtype=np.uint8), "input/nsteps": np.int64(nsteps),
+            "input/position": ns.pos, "input/velocity": ns.vel, "input/mass": ns.mass,
+            "input/mass density": ns.rho, "input/specific thermal energy": ns.eps, "input/H": ns.H}
+    for k, v in r.items():
+        if k == "eval/pair accelerations":
+            # Kept as a digest of the exact bytes (the array is 3 doubles per entry).
+            data["eval/pair accelerations sha256"] = np.frombuffer(hashlib.sha256(v.tobytes()).digest(),
+                                                                   dtype=np.uint8)
+            data["eval/pair accelerations size"] = np.int64(v.size)
+        elif k in ("conn_offsets", "conn_neighbors", "ghost_root"):
+            data[k] = v.astype(np.int32)
+        else:
+            data[k] = v
+    out = os.path.join(HERE, "reference_sph_%s.npz" % name)
     np.savez_compressed(out, **data)
-    print(out, sorted(data))
+    return out
+
+
+def main(argv):
+    build_ref = importlib.import_module("build_ref")
+    ref_sph, ref_tables = build_ref.build()
+    want = argv[1:]
+    if not want or "tables" in want:
+        with tempfile.TemporaryDirectory() as td:
+            subprocess.check_call([ref_tables, td], stdout=subprocess.DEVNULL)
+            data = {}
+            for f in sorted(os.listdir(td)):
+                if f.endswith(".f64"):
+                    data[f[:-4]] = np.fromfile(os.path.join(td, f), dtype="<f8")
+        out = os.path.join(HERE, "reference_tables.npz")
+        np.savez_compressed(out, **data)
+        print(out)
+    pkg = importlib.import_module("llnl-spheral_b200")
+    for name, (ns, cfg, nsteps) in cases(pkg).items():
+        if want and name not in want:
+            continue
+        print(sph_fixture(ref_sph, name, ns, cfg, nsteps))
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv)

@@ -3,7 +3,7 @@
 tests/golden/reference_tables.npz holds outputs of the reference's own
 TableKernel, BSpline/Wendland C4 kernels, Dim<3> geometry and
 mapPositionThroughPlanes, compiled unmodified from the reference tree
-(oracle/build_ref.sh, tests/golden/make_golden.py).  The oracle must
+(oracle/build_ref.py, tests/golden/make_golden.py).  The oracle must
 reproduce them bit for bit.
 """
 import ctypes
