@@ -203,10 +203,14 @@ int sphgpu_conservation(sphgpu_problem* p, double out[8]);
  * their own buffers under a fixed HBM budget).  Scratch is a fixed device
  * array inside the library, so n <= 16,777,216 (larger n returns
  * SPHGPU_ERR_CAPACITY).  The first call on each device looks up the scratch
- * address (set-up); make it before any stream capture.  Work is issued on
- * `stream` (cudaStream_t as void*, NULL = default stream); the call returns
- * after the results are in `out` (host memory).  Calls that overlap in time
- * on one device share the scratch and race. */
+ * address (set-up) and keeps it for the life of the process; make it before
+ * any stream capture, and do not call the entry point again on a device
+ * after a cudaDeviceReset of that device (the kept address is stale then).
+ * Work is issued on `stream` (cudaStream_t as void*, NULL = default stream).
+ * The call is synchronous: it waits for `stream` and returns with the results
+ * in `out` (host memory), so it must not be called while `stream` is being
+ * captured.  Calls that overlap in time on one device share the scratch and
+ * race. */
 int sphgpu_conservation_noalloc(const double* mass, const double* velocity,
                                 const double* specificThermalEnergy, int64_t n, void* stream,
                                 double out[8]);
@@ -295,6 +299,7 @@ typedef struct sphgpu_server sphgpu_server;
 #define SPHGPU_REQ_RUNNING 1
 #define SPHGPU_REQ_DONE    2
 #define SPHGPU_REQ_FAILED  3
+#define SPHGPU_REQ_CANCELLED 4
 /* Device bytes the server charges for a request before it runs (host only;
  * positions and H as for sphgpu_set_state). */
 int sphgpu_estimate_footprint(const sphgpu_config* cfg, int64_t n, const double* position, const double* H,
@@ -309,7 +314,13 @@ int sphgpu_server_submit(sphgpu_server* s, const sphgpu_config* cfg, int64_t n, 
 /* Admit what fits, advance every running simulation by one RK2 step, retire
  * the finished ones.  Returns the running and queued counts afterwards. */
 int sphgpu_server_tick(sphgpu_server* s, int32_t* running, int32_t* queued);
-/* Requests finished (done or failed) since the last call, up to `capacity`. */
+/* Withdraw a queued or running request (between ticks).  A running one
+ * gives its device memory back to the budget at once; the other running
+ * simulations are unaffected.  The request is reported as finished with
+ * state SPHGPU_REQ_CANCELLED; fetching it returns SPHGPU_ERR_STATE and
+ * releases it.  A finished request returns SPHGPU_ERR_STATE. */
+int sphgpu_server_cancel(sphgpu_server* s, int64_t id);
+/* Requests finished (done, failed or cancelled) since the last call, up to `capacity`. */
 int sphgpu_server_finished(sphgpu_server* s, int64_t* ids, int32_t capacity, int32_t* count);
 int sphgpu_server_status(sphgpu_server* s, int64_t id, int32_t* state, int64_t* steps_done, int64_t* pairs);
 /* Final state of a finished request (any pointer may be NULL); releases it. */

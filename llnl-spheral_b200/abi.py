@@ -184,6 +184,7 @@ def load_library(path=None):
     lib.sphgpu_server_submit.argtypes = [P, P, I64] + [P] * 6 + [I64, ctypes.POINTER(I64)]
     lib.sphgpu_server_tick.argtypes = [P, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
     lib.sphgpu_server_finished.argtypes = [P, P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+    lib.sphgpu_server_cancel.argtypes = [P, I64]
     lib.sphgpu_server_status.argtypes = [P, I64, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(I64),
                                          ctypes.POINTER(I64)]
     lib.sphgpu_server_fetch.argtypes = [P, I64] + [P] * 6 + [ctypes.POINTER(ctypes.c_double)]

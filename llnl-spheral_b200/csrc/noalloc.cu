@@ -18,6 +18,10 @@
 // reads is written by the partial pass earlier on the same stream.
 // Calls that overlap in time on one device (two host threads, or two
 // streams without ordering between them) share the scratch and race.
+// The scratch address of a device is looked up on the first call there and
+// kept for the life of the process; a cudaDeviceReset of that device reloads
+// the module and leaves the kept address stale, so the entry point is not to
+// be called on a device after it has been reset.
 #include <mutex>
 
 #include "problem.cuh"

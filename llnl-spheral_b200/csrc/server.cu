@@ -24,7 +24,7 @@
 namespace sphgpu {
 namespace {
 
-enum RequestState { REQ_QUEUED = 0, REQ_RUNNING = 1, REQ_DONE = 2, REQ_FAILED = 3 };
+enum RequestState { REQ_QUEUED = 0, REQ_RUNNING = 1, REQ_DONE = 2, REQ_FAILED = 3, REQ_CANCELLED = 4 };
 
 struct Request {
   sphgpu_config cfg{};
@@ -102,6 +102,7 @@ struct sphgpu_server {
   std::vector<int64_t> running;       // admission order
   std::vector<int64_t> finished;      // not yet reported by sphgpu_server_finished
   Batch batch;
+  bool deviceReady = false;           // stream and batch set up (first tick)
   int64_t inUse = 0, peak = 0;
   int64_t pairsTotal = 0, ticks = 0, completed = 0, steps = 0;
 };
@@ -115,6 +116,23 @@ void release(sphgpu_server& s, Request& r) {
   }
   s.inUse -= r.footprint;
   r.footprint = 0;
+}
+
+// The server's stream and batch descriptors, made on the first tick: queue
+// management (submit, cancel, status) needs no device.
+int server_device(sphgpu_server& s) {
+  if (s.deviceReady) return SPHGPU_OK;
+  cudaStream_t st = nullptr;
+  int rc = cuda_status(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "server stream");
+  if (rc != SPHGPU_OK) return rc;
+  rc = batch_init(s.batch, st);
+  s.batch.ownStream = true;
+  if (rc != SPHGPU_OK) {
+    batch_free(s.batch);
+    return rc;
+  }
+  s.deviceReady = true;
+  return SPHGPU_OK;
 }
 
 int admit(sphgpu_server& s, int64_t id, const Estimate& est) {
@@ -162,15 +180,6 @@ int sphgpu_server_create(double hbm_budget_bytes, int32_t max_members, sphgpu_se
   if (s == nullptr) { set_error("host allocation failed"); return SPHGPU_ERR_NOMEM; }
   s->budget = (int64_t)hbm_budget_bytes;
   s->maxMembers = max_members;
-  cudaStream_t st = nullptr;
-  int rc = cuda_status(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "server stream");
-  if (rc == SPHGPU_OK) rc = batch_init(s->batch, st);
-  s->batch.ownStream = true;
-  if (rc != SPHGPU_OK) {
-    batch_free(s->batch);
-    delete s;
-    return rc;
-  }
   *out = s;
   return SPHGPU_OK;
 }
@@ -178,7 +187,7 @@ int sphgpu_server_create(double hbm_budget_bytes, int32_t max_members, sphgpu_se
 void sphgpu_server_destroy(sphgpu_server* s) {
   if (s == nullptr) return;
   for (auto& kv : s->reqs) if (kv.second.prob) sphgpu_destroy(kv.second.prob);
-  batch_free(s->batch);
+  if (s->deviceReady) batch_free(s->batch);
   delete s;
 }
 
@@ -209,6 +218,7 @@ int sphgpu_server_submit(sphgpu_server* s, const sphgpu_config* cfg, int64_t n, 
 
 int sphgpu_server_tick(sphgpu_server* s, int32_t* running, int32_t* queued) {
   if (s == nullptr) return SPHGPU_ERR_ARG;
+  SPH_TRY(server_device(*s));
   // ---- admission, first come first served
   while (!s->queue.empty() && (int32_t)s->running.size() < s->maxMembers) {
     const int64_t id = s->queue.front();
@@ -282,6 +292,30 @@ int sphgpu_server_tick(sphgpu_server* s, int32_t* running, int32_t* queued) {
   return SPHGPU_OK;
 }
 
+int sphgpu_server_cancel(sphgpu_server* s, int64_t id) {
+  if (s == nullptr) return SPHGPU_ERR_ARG;
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) { set_error("sphgpu_server_cancel: unknown request"); return SPHGPU_ERR_ARG; }
+  Request& r = it->second;
+  if (r.state == REQ_QUEUED) {
+    s->queue.erase(std::find(s->queue.begin(), s->queue.end(), id));
+  } else if (r.state == REQ_RUNNING) {
+    // Between ticks no kernel of the request is in flight on the server's
+    // stream once it is drained; its buffers go back to the pool.
+    if (s->deviceReady) SPH_CHECK(cudaStreamSynchronize(s->batch.stream));
+    release(*s, r);
+    s->running.erase(std::find(s->running.begin(), s->running.end(), id));
+  } else {
+    set_error("sphgpu_server_cancel: request already finished");
+    return SPHGPU_ERR_STATE;
+  }
+  r.state = REQ_CANCELLED;
+  r.error = "request cancelled";
+  r.pos.clear(); r.vel.clear(); r.mass.clear(); r.rho.clear(); r.eps.clear(); r.H.clear();
+  s->finished.push_back(id);
+  return SPHGPU_OK;
+}
+
 int sphgpu_server_finished(sphgpu_server* s, int64_t* ids, int32_t capacity, int32_t* count) {
   if (s == nullptr || count == nullptr || (capacity > 0 && ids == nullptr)) return SPHGPU_ERR_ARG;
   const int32_t k = std::min<int32_t>(capacity, (int32_t)s->finished.size());
@@ -298,7 +332,7 @@ int sphgpu_server_status(sphgpu_server* s, int64_t id, int32_t* state, int64_t* 
   if (state) *state = it->second.state;
   if (steps_done) *steps_done = it->second.stepsDone;
   if (pairs) *pairs = it->second.pairs;
-  if (it->second.state == REQ_FAILED) set_error(it->second.error);
+  if (it->second.state == REQ_FAILED || it->second.state == REQ_CANCELLED) set_error(it->second.error);
   return SPHGPU_OK;
 }
 
@@ -308,7 +342,11 @@ int sphgpu_server_fetch(sphgpu_server* s, int64_t id, double* position, double* 
   auto it = s->reqs.find(id);
   if (it == s->reqs.end()) { set_error("sphgpu_server_fetch: unknown request"); return SPHGPU_ERR_ARG; }
   Request& r = it->second;
-  if (r.state == REQ_FAILED) { set_error(r.error); return SPHGPU_ERR_STATE; }
+  if (r.state == REQ_FAILED || r.state == REQ_CANCELLED) {
+    set_error(r.error);
+    s->reqs.erase(it);
+    return SPHGPU_ERR_STATE;
+  }
   if (r.state != REQ_DONE) { set_error("sphgpu_server_fetch: request not finished"); return SPHGPU_ERR_STATE; }
   const int64_t n = r.n;
   if (position) std::memcpy(position, r.pos.data(), sizeof(double)*3*n);

@@ -23,7 +23,7 @@ def _ptr(a):
 
 
 class Server:
-    QUEUED, RUNNING, DONE, FAILED = 0, 1, 2, 3
+    QUEUED, RUNNING, DONE, FAILED, CANCELLED = 0, 1, 2, 3, 4
 
     def __init__(self, budget_bytes, max_members=512):
         self.lib = abi.load_library()
@@ -57,6 +57,10 @@ class Server:
         q = ctypes.c_int32()
         abi.check(self.lib.sphgpu_server_tick(self.h, ctypes.byref(r), ctypes.byref(q)), self.lib)
         return r.value, q.value
+
+    def cancel(self, rid):
+        """Withdraw a queued or running request; it is reported finished as CANCELLED."""
+        abi.check(self.lib.sphgpu_server_cancel(self.h, int(rid)), self.lib)
 
     def finished(self):
         ids = np.zeros(4096, dtype=np.int64)

@@ -87,3 +87,34 @@ def test_oversized_request_fails_cleanly(gpu_lib, pkg):
     results, stats, _ = _run_server(pkg, reqs, 1.0e6, [0, 0])
     assert all(results[k][0] == 3 for k in range(2))
     assert stats["completed"] == 0
+
+
+def test_cancel_a_running_request(gpu_lib, pkg):
+    """A request cancelled while it runs gives its memory back at once; the
+    requests running beside it finish with the results they give alone."""
+    reqs = _requests(pkg, 1)[:3]
+    srv = pkg.serving.Server(40e9, max_members=64)
+    ids = [srv.submit(cfg, ns, nsteps) for ns, cfg, nsteps in reqs]
+    srv.tick()
+    before = srv.stats()["bytes_in_use"]
+    assert srv.status(ids[1])[0] == srv.RUNNING
+    srv.cancel(ids[1])
+    assert srv.stats()["bytes_in_use"] < before
+    done = {}
+    for _ in range(20):
+        srv.tick()
+        for rid in srv.finished():
+            done[rid] = srv.status(rid)[0]
+        if len(done) == 3:
+            break
+    assert done[ids[1]] == srv.CANCELLED
+    with pytest.raises(RuntimeError):
+        srv.fetch(ids[1])
+    for k in (0, 2):
+        assert done[ids[k]] == srv.DONE
+        out = srv.fetch(ids[k])
+        ns, cfg, nsteps = reqs[k]
+        ref, t = _solo(pkg, ns, cfg, nsteps)
+        for key, _ in KEYS:
+            assert np.array_equal(out[key], ref[key]), (k, key)
+    srv.close()

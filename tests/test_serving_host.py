@@ -32,3 +32,26 @@ def test_footprint_estimate_scales_with_nodes(pkg):
     ns, cfg = s.request_nodes("kh", 32768, 1, 1)
     kh = s.estimate_footprint(cfg, ns) / ns.n
     assert 800 < kh < est[1]                          # ~6 Wendland neighbors: fewer CSR bytes
+
+
+def test_cancel_queued_requests_on_the_host(pkg):
+    """Queue management needs no device: a queued request can be withdrawn,
+    is reported finished as cancelled, and its fetch fails and releases it."""
+    import pytest
+    s = pkg.serving
+    srv = s.Server(1e9, max_members=4)
+    reqs = [s.request_nodes("sod", 4096, seed, 1) for seed in (1, 2, 3)]
+    ids = [srv.submit(cfg, ns, 5) for ns, cfg in reqs]
+    srv.cancel(ids[1])
+    assert srv.status(ids[1])[0] == srv.CANCELLED
+    assert srv.status(ids[0])[0] == srv.QUEUED and srv.status(ids[2])[0] == srv.QUEUED
+    assert srv.finished() == [ids[1]]
+    with pytest.raises(RuntimeError):
+        srv.cancel(ids[1])                 # already finished
+    with pytest.raises(RuntimeError):
+        srv.fetch(ids[1])                  # cancelled: no result; the request is released
+    with pytest.raises(RuntimeError):
+        srv.status(ids[1])                 # unknown after release
+    srv.cancel(ids[2])
+    assert srv.finished() == [ids[2]]
+    srv.close()

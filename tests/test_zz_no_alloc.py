@@ -26,10 +26,11 @@ def _device_state(torch, g):
     return m, v, e
 
 
-def _noalloc(lib, m, v, e, n):
+def _noalloc(lib, m, v, e, n, stream=None):
     out = np.full(8, np.nan)
     rc = lib.sphgpu_conservation_noalloc(ctypes.c_void_p(m.data_ptr()), ctypes.c_void_p(v.data_ptr()),
-                                         ctypes.c_void_p(e.data_ptr()), n, None,
+                                         ctypes.c_void_p(e.data_ptr()), n,
+                                         None if stream is None else ctypes.c_void_p(stream.cuda_stream),
                                          out.ctypes.data_as(ctypes.c_void_p))
     return rc, out
 
@@ -62,6 +63,24 @@ def test_noalloc_matches_handle_conservation(gpu_lib, pkg, shape):
     for out in (out1, out2):
         assert np.all(np.abs(out - ref) <= 1e-12 * scale), (out, ref)
     assert np.array_equal(out1, out2)
+
+
+def test_noalloc_on_a_caller_stream(gpu_lib, pkg):
+    """A serving loop passes its own stream: the sums are the same bits as on
+    the default stream, call after call."""
+    import torch
+    gen, abi = pkg.generators, pkg.abi
+    ns = gen.kelvin_helmholtz(nx=32, ny=32, nz=16, box=((0, 0, 0), (1.0, 1.0, 0.5)))
+    g = pkg.SPHHydro(gen.kh_config(abi, xmax=(1.0, 1.0, 0.5)), ns)
+    m, v, e = _device_state(torch, g)
+    rc0, base = _noalloc(gpu_lib, m, v, e, ns.n)
+    assert rc0 == 0, gpu_lib.sphgpu_last_error()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    for _ in range(2):
+        rc, out = _noalloc(gpu_lib, m, v, e, ns.n, stream=s)
+        assert rc == 0, gpu_lib.sphgpu_last_error()
+        assert np.array_equal(out, base)
 
 
 def test_noalloc_rejects_sizes_beyond_scratch(gpu_lib):
