@@ -12,8 +12,13 @@ ConnectivityMap rebuilt, dt selected, mid-point derivatives, compatible-energy
 and state updates, sum density, boundary wrap.  The metric is
 pair-interactions/s (unordered neighbor pairs per derivative evaluation,
 the reference's ncalc, times steps, over time).  The headline `value` is the
-mixed FP32-pair form; the plain FP64 form and p50/p99 step latency are in
-the same line.
+plain FP64 form, the reference's own arithmetic; the mixed FP32-pair form,
+its ratio to FP64 and p50/p99 step latency of both are in the same line.
+
+--impl reference times the reference's own CPU path (SPHHydroBase +
+CheapSynchronousRK2 compiled from its sources into oracle/_ref/ref_sph; the
+oracle restatement where that binary is absent) on all host cores, one
+process per core on a z-slab of the same lattice.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -66,24 +71,28 @@ def parse():
     return ap.parse_args()
 
 
-# Algorithmic bytes of one mixed-form evaluateDerivatives (record pack + pair
+# Algorithmic bytes of one plain-FP64 evaluateDerivatives (record pack + pair
 # kernel): the pack reads 136 B of state per internal node (position,
-# velocity, m, rho, cs, P, omega, H) and writes a 112-byte record per node and
-# ghost; the pair kernel reads those records, writes 54 derivative doubles
-# per internal node (432 B; the reference's "internal velocity gradient" and
-# "local M" equal the velocity gradient and M for one NodeList and are not
-# stored twice), reads 4 B of CSR index and writes 24 B of pair acceleration
-# per directed entry.
-def eval_alg_bytes(nodes, ghosts, entries):
-    # pack (state in, records out), pair kernel (records in, 54 derivative
-    # doubles out, CSR index in, FP32 pair accelerations out)
+# velocity, m, rho, cs, P, omega, H) and writes a 160-byte pair record per
+# node and ghost; the pair kernel reads those records, writes 54 derivative
+# doubles per internal node (432 B; the reference's "internal velocity
+# gradient" and "local M" equal the velocity gradient and M for one NodeList
+# and are not stored twice), reads 4 B of CSR index and writes 24 B of FP64
+# pair acceleration per directed entry.
+def eval_alg_bytes_fp64(nodes, ghosts, entries):
+    return nodes * 136 + 2 * (nodes + ghosts) * 160 + nodes * 432 + 28 * entries
+
+
+# The same for the mixed form: 112-byte records, FP32 pair accelerations.
+def eval_alg_bytes_mixed(nodes, ghosts, entries):
     return nodes * 136 + 2 * (nodes + ghosts) * 112 + nodes * 432 + 16 * entries
 
 
-# DRAM traffic (read + write) of pack_mixed_kernel + sph_eval_mixed_kernel
-# measured by ncu on Kelvin-Helmholtz 96^3 (884,736 nodes, 56,456 ghosts,
-# 5,363,712 entries); scaled to other sizes by the algorithmic bytes.
-EVAL_TRAFFIC_96 = 150498816 + 67565056 + 190594816 + 386470912
+# DRAM traffic (read + write) measured by ncu on Kelvin-Helmholtz 96^3
+# (884,736 nodes, 56,456 ghosts, 5,363,712 entries) for the record pack and
+# the pair kernel of each form; scaled to other sizes by the algorithmic
+# bytes (all three units grow together).
+EVAL_TRAFFIC_96 = {"fp64": None, "mixed": 150498816 + 67565056 + 190594816 + 386470912}
 EVAL_UNITS_96 = (884736, 56456, 5363712)
 
 
@@ -326,14 +335,38 @@ def measure_e2e(pkg, ns, cfg, steps, warmup):
 
 ACCURACY_FIELDS = ["delta velocity hydro", "delta specific thermal energy", "delta mass density",
                    "velocity gradient", "new mass density", "new H", "M SPH gradient correction",
-                   "max viscous pressure", "weighted neighbor sum"]
+                   "max viscous pressure", "weighted neighbor sum", "delta H", "mass second moment",
+                   "effective viscous pressure", "viscous work rate", "normalization"]
+STATE_FIELDS = ["position", "velocity", "mass density", "specific thermal energy", "H"]
+
+
+def field_errors(a, b):
+    """Errors of `a` against the FP64 `b`: normwise max ||a - b||_inf /
+    ||b||_inf, normwise RMS, and a guarded pointwise max: |a_i - b_i| /
+    max(|b_i|, rms(b)) per component, which shows large relative errors at
+    nodes where the field is small without dividing by the exact zeros."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    d = np.abs(a - b)
+    bmax = max(float(np.abs(b).max()), 1e-300)
+    brms = max(float(np.sqrt(np.mean(b * b))), 1e-300)
+    return {"max_rel": float(d.max() / bmax), "rms_rel": float(np.sqrt(np.mean(d * d)) / brms),
+            "pointwise_max_rel": float((d / np.maximum(np.abs(b), brms)).max())}
+
+
+def energy(h):
+    c = h.conservation()
+    return float(c[6]), float(c[7])
 
 
 def measure_accuracy(pkg, ns, cfg, steps):
-    """Mixed form against plain FP64 on the same node set: max and RMS
-    relative error of every derivative field (normwise: ||d||/||fp64||) at
-    the start, and the relative total-energy drift of each form over
-    `steps` RK2 steps."""
+    """Mixed form against plain FP64 from the same start: every derivative
+    field's error at t = 0, and the state and the last mid-point derivatives
+    after `steps` RK2 steps (field_errors); the per-step latency of both forms
+    over those steps (CUDA events around each step call, host read-back of dt
+    included); the total energy at the start and the end as compensated sums
+    (hi + lo, two-sum on the device) and the relative drift they give."""
+    import torch
     abi = pkg.abi
     cf, cm = cfg.copy(), cfg.copy()
     cf.precision = abi.PRECISION_FP64
@@ -342,22 +375,39 @@ def measure_accuracy(pkg, ns, cfg, steps):
     for h in (hf, hm):
         h.build_neighbors()
         h.evaluateDerivatives()
-    errs = {}
-    for k in ACCURACY_FIELDS:
-        a, b = hm.field(k), hf.field(k)
-        d = np.abs(a - b)
-        errs[k] = {"max_rel": float(d.max() / max(np.abs(b).max(), 1e-300)),
-                   "rms_rel": float(np.sqrt(np.mean(d * d)) / max(np.sqrt(np.mean(b * b)), 1e-300))}
-    drift = {}
+    errs0 = {k: field_errors(hm.field(k), hf.field(k)) for k in ACCURACY_FIELDS}
+    out = {"field_error_vs_fp64_t0": errs0,
+           "max_field_error_t0": max(v["max_rel"] for v in errs0.values()),
+           "steps": steps}
+    lat, eng = {}, {}
     for name, h in (("plain_fp64", hf), ("mixed", hm)):
-        e0 = h.conservation()[6]
-        h.step(steps)
-        drift[name] = float(abs(h.conservation()[6] - e0) / abs(e0))
+        e0 = energy(h)
+        stream = torch.cuda.ExternalStream(h.stream())
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        ev[0].record(stream)
+        for k in range(steps):
+            h.step(1)
+            ev[k + 1].record(stream)
+        h.synchronize()
+        torch.cuda.synchronize()
+        per = sorted(ev[k].elapsed_time(ev[k + 1]) for k in range(steps))
+        lat[name] = {"p50_ms": per[len(per) // 2], "p99_ms": per[min(len(per) - 1, int(round(0.99 * (len(per) - 1))))],
+                     "max_ms": per[-1], "samples": steps}
+        e1 = energy(h)
+        drift = ((e1[0] - e0[0]) + (e1[1] - e0[1])) / abs(e0[0])
+        eng[name] = {"e0": e0[0], "e0_lo": e0[1], "e1": e1[0], "e1_lo": e1[1], "relative_drift": drift,
+                     "abs_relative_drift": abs(drift)}
+    errs1 = {k: field_errors(hm.field(k), hf.field(k)) for k in STATE_FIELDS + ACCURACY_FIELDS}
+    out["field_error_vs_fp64_after_steps"] = errs1
+    out["max_field_error_after_steps"] = max(v["max_rel"] for v in errs1.values())
+    out["step_latency"] = lat
+    out["energy"] = eng
+    out["energy_drift"] = {k: v["abs_relative_drift"] for k, v in eng.items()}
+    out["energy_sum"] = ("double-double (two-sum) total energy on the device: e = e0 + e0_lo; a drift is "
+                         "resolved to about 1e-30 relative")
     hf.close()
     hm.close()
-    return {"field_error_vs_fp64": errs,
-            "max_field_error": max(v["max_rel"] for v in errs.values()),
-            "energy_drift": drift, "drift_steps": steps}
+    return out
 
 
 def measure_rate(pkg, ns, cfg, steps, warmup, eval_reps=5):
@@ -425,9 +475,11 @@ def measure_config_crk(pkg, steps, warmup, drift_steps):
             h.build_neighbors()
             h.initialize()
             h.evaluateDerivatives()
-            e0 = h.conservation()[6]
+            e0 = energy(h)
             h.step(drift_steps)
-            out[name]["energy_drift"] = float(abs(h.conservation()[6] - e0) / abs(e0))
+            e1 = energy(h)
+            out[name]["energy_drift"] = abs(((e1[0] - e0[0]) + (e1[1] - e0[1])) / abs(e0[0]))
+            out[name]["energy"] = {"e0": e0[0], "e0_lo": e0[1], "e1": e1[0], "e1_lo": e1[1]}
             out[name]["drift_steps"] = drift_steps
             h.close()
     out["mixed_over_plain"] = out["mixed"]["value"] / out["plain_fp64"]["value"]
@@ -437,10 +489,10 @@ def measure_config_crk(pkg, steps, warmup, drift_steps):
     return out
 
 
-def batch_specs(pkg, count, seed=20261203, nmin=4096, nmax=262144):
+def batch_specs(pkg, count, precision, seed=20261203, nmin=4096, nmax=262144):
     """The batched-ensemble workload: `count` Sod-type tubes, n log-uniform in
     [nmin, nmax] as an 8k x k x k lattice, gamma ~ U[1.3, 1.67], left/right
-    density ratio ~ U[2, 8], cubic B-spline nPerh 1.51, mixed form."""
+    density ratio ~ U[2, 8], cubic B-spline nPerh 1.51."""
     gen, abi = pkg.generators, pkg.abi
     rng = np.random.default_rng(seed)
     out = []
@@ -452,29 +504,21 @@ def batch_specs(pkg, count, seed=20261203, nmin=4096, nmax=262144):
         box = ((0.0, 0.0, 0.0), (1.0, 0.125, 0.125))
         ns = gen.sod(nx=8 * kk, ny=kk, nz=kk, box=box, gamma=gamma, rho1=1.0, rho2=1.0 / ratio, P1=1.0,
                      P2=0.1795, seed=seed + 1 + k)
-        cfg = gen.sod_config(abi, ns_box=box, gamma=gamma, precision=abi.PRECISION_MIXED)
+        cfg = gen.sod_config(abi, ns_box=box, gamma=gamma, precision=precision)
         out.append((ns, cfg))
     return out
 
 
-def measure_batch(pkg, count, steps, warmup, rank=0, world=1):
-    """Batched ensemble: every stage one launch over all members (autotuned),
-    against the same problems stepped one at a time (one launch per problem
-    per stage).  With N GPUs the tubes are placed by size (longest first onto
-    the least-loaded rank; no exchange on the data path); each rank times
-    its batch with CUDA events on the batch stream, and the line takes the
-    max over ranks and the sum of the pairs."""
+def time_batch(pkg, probs, steps, warmup, world, graph):
+    """Batched steps of `probs` (autotuned schedules; the RK2 step after the
+    rebuild replayed as a CUDA graph when `graph`), timed with CUDA events on
+    the batch stream, max over ranks."""
     import torch
-    specs = batch_specs(pkg, count)
-    place = pkg.sharding.partition_by_cost([ns.n for ns, _ in specs], world)
-    mine = pkg.sharding.local_items(place, rank)
-    specs = [specs[k] for k in mine]
-    probs = [pkg.SPHHydro(cfg, ns) for ns, cfg in specs]
-    nodes = allsum(sum(ns.n for ns, _ in specs), world)
     batch = pkg.SPHBatch(probs)
     batch.build_neighbors()
     batch.evaluateDerivatives()
     tune = batch.autotune()
+    batch.set_schedule("step graph", 1 if graph else 0)
     stream = torch.cuda.ExternalStream(batch.stream())
     for _ in range(warmup):
         batch.step(1)
@@ -490,41 +534,68 @@ def measure_batch(pkg, count, steps, warmup, rank=0, world=1):
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
-    t_batch = allmax(e0.elapsed_time(e1) / 1e3, world)
+    t = allmax(e0.elapsed_time(e1) / 1e3, world)
     pairs = allsum(pairs, world)
     launches = batch.kernel_launches() - l0
-    # one launch sequence per problem, each on its own stream: host clock
-    # around device synchronisation
-    for _ in range(warmup):
-        for p in probs:
-            p.step(1)
-    torch.cuda.synchronize()
-    barrier(world)
-    t0 = time.perf_counter()
-    lpairs = 0
-    for _ in range(steps):
-        for p in probs:
-            p.step(1)
-            lpairs += p.num_pairs()
-    torch.cuda.synchronize()
-    t_loop = allmax(time.perf_counter() - t0, world)
-    lpairs = allsum(lpairs, world)
     batch.close()
-    for p in probs:
-        p.close()
-    return {"value": pairs / t_batch, "unit": METRIC, "ms_per_step": 1e3 * t_batch / steps,
-            "one_launch_per_problem": {"value": lpairs / t_loop, "unit": METRIC,
-                                       "ms_per_step": 1e3 * t_loop / steps},
-            "batched_over_loop": (pairs / t_batch) / (lpairs / t_loop),
-            "kernel_launches_per_step": launches / steps,
+    return {"value": pairs / t, "unit": METRIC, "ms_per_step": 1e3 * t / steps,
+            "kernel_launches_per_step": launches / steps, "step_graph": bool(graph),
             "autotuned": {"neighbor walk": ["auto", "thread per node", "warp per node"][tune["neighbor walk"]],
                           "neighbor cells per kernel reach": tune["neighbor cells"],
-                          "pair loop threads": tune["pair loop"]},
-            "config": {"workload": "%d Sod-type tubes, n log-uniform in [4096, 262144] (8k x k x k), "
-                                   "gamma ~ U[1.3, 1.67], density ratio ~ U[2, 8], cubic B-spline nPerh 1.51, "
-                                   "mixed form, fixed dt 1e-4" % count,
-                       "nodes": nodes, "steps": steps, "warmup": warmup,
-                       "placement": "tubes placed on %d GPU(s) by size, no data-path exchange" % world}}
+                          "pair loop threads": tune["pair loop"]}}
+
+
+def measure_batch(pkg, count, steps, warmup, rank=0, world=1):
+    """Batched ensemble, mixed form: every stage one launch over all members,
+    the RK2 step after the ghost/connectivity rebuild replayed as a CUDA graph;
+    against the same batch in plain FP64, and against the mixed problems
+    stepped one at a time (one launch sequence per problem).  With N GPUs the
+    tubes are placed by size (longest first onto the least-loaded rank; no
+    exchange on the data path); the lines take the max time over ranks and the
+    sum of the pairs."""
+    import torch
+    abi = pkg.abi
+    out = {}
+    nodes = None
+    for name, prec in (("mixed", abi.PRECISION_MIXED), ("plain_fp64", abi.PRECISION_FP64)):
+        specs = batch_specs(pkg, count, prec)
+        place = pkg.sharding.partition_by_cost([ns.n for ns, _ in specs], world)
+        mine = pkg.sharding.local_items(place, rank)
+        specs = [specs[k] for k in mine]
+        nodes = allsum(sum(ns.n for ns, _ in specs), world)
+        probs = [pkg.SPHHydro(cfg, ns) for ns, cfg in specs]
+        out[name] = time_batch(pkg, probs, steps, warmup, world, graph=True)
+        if name == "mixed":
+            out["mixed_eager"] = time_batch(pkg, probs, steps, warmup, world, graph=False)
+            # one launch sequence per problem: host clock around device synchronisation
+            for _ in range(warmup):
+                for p in probs:
+                    p.step(1)
+            torch.cuda.synchronize()
+            barrier(world)
+            t0 = time.perf_counter()
+            lpairs = 0
+            for _ in range(steps):
+                for p in probs:
+                    p.step(1)
+                    lpairs += p.num_pairs()
+            torch.cuda.synchronize()
+            t_loop = allmax(time.perf_counter() - t0, world)
+            lpairs = allsum(lpairs, world)
+            out["one_launch_per_problem"] = {"value": lpairs / t_loop, "unit": METRIC,
+                                             "ms_per_step": 1e3 * t_loop / steps}
+        for p in probs:
+            p.close()
+    out["value"] = out["mixed"]["value"]
+    out["unit"] = METRIC
+    out["mixed_over_plain"] = out["mixed"]["value"] / out["plain_fp64"]["value"]
+    out["batched_over_loop"] = out["mixed"]["value"] / out["one_launch_per_problem"]["value"]
+    out["config"] = {"workload": "%d Sod-type tubes, n log-uniform in [4096, 262144] (8k x k x k), "
+                                 "gamma ~ U[1.3, 1.67], density ratio ~ U[2, 8], cubic B-spline nPerh 1.51, "
+                                 "fixed dt 1e-4" % count,
+                     "nodes": nodes, "steps": steps, "warmup": warmup,
+                     "placement": "tubes placed on %d GPU(s) by size, no data-path exchange" % world}
+    return out
 
 
 def measure_serving(pkg, duration, nsteps, rate=20.0, budget=150e9, rank=0, world=1):
@@ -565,23 +636,65 @@ def measure_serving(pkg, duration, nsteps, rate=20.0, budget=150e9, rank=0, worl
                               "Kelvin-Helmholtz / Sod-type, n log-uniform in [8192, 1048576], %d RK2 steps each, "
                               "admission by device footprint under %.0f GB per GPU, routed to %d GPU(s)"
                               % (rate, duration, len(trace), nsteps, budget / 1e9, world)}
+    if duration < 60.0 or nsteps < 200:
+        out["config"]["shortened"] = (
+            "SHORTENED trace: %.1f s of arrivals and %d steps per request instead of the specified 60 s and 200 "
+            "steps; the specified trace holds about 8 minutes of GPU work per form, beyond the bench's time "
+            "limit (bench.py --serving 60 --serving-steps 200 runs it)" % (duration, nsteps))
     return out
 
 
-def cpu_baseline(pkg, ns, cfg):
-    """The oracle (a serial FP64 restatement of the reference path) on the
-    same workload: one RK2 step after the start-up evaluation, 1 core."""
-    import oracle
-    o = oracle.OracleProblem(cfg, ns)
-    o.build_neighbors()
-    o.evaluate_derivatives()
-    t0 = time.perf_counter()
-    o.step(1)
-    el = time.perf_counter() - t0
-    pairs = o.num_pairs()
-    return {"value": pairs / el, "unit": METRIC, "cores": 1, "kind": "port",
-            "sample": "1 CheapSynchronousRK2 step of the full %d-node workload (ghosts, neighbors, "
-                      "derivatives, updates), serial oracle, %.1f s" % (ns.n, el),
+REF_SPH = os.path.join(ROOT, "oracle", "_ref", "ref_sph")
+
+
+def write_reference_input(path, cfg, ns, nsteps):
+    """Input of oracle/_ref/ref_sph: int64 n, int64 steps, the raw
+    sphgpu_config, then the node arrays in the reference Field layouts."""
+    with open(path, "wb") as f:
+        f.write(np.int64(ns.n).tobytes())
+        f.write(np.int64(nsteps).tobytes())
+        f.write(bytes(cfg))
+        for a in (ns.pos, ns.vel, ns.mass, ns.rho, ns.eps, ns.H):
+            f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
+
+
+def time_reference(cfg, ns, steps, warmup):
+    """The reference's own SPHHydroBase + CheapSynchronousRK2 (compiled from
+    its sources into oracle/_ref/ref_sph): seconds and pair interactions of
+    `steps` timed RK2 steps after `warmup` untimed ones, one core."""
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "in.bin")
+        write_reference_input(path, cfg, ns, steps)
+        out = subprocess.check_output([REF_SPH, "--time", str(warmup), path]).decode()
+    r = json.loads(out.strip().splitlines()[-1])
+    return r["seconds"], r["pairs"]
+
+
+def cpu_baseline(pkg, nx):
+    """The reference's CPU path on the host, one core, on a bounded sample of
+    the workload: a z-slab of the same lattice (same spacing, stencil and
+    state), two timed RK2 steps after one untimed.  Falls back to the oracle
+    (the FP64 restatement of the reference path) where the reference could
+    not be compiled."""
+    nz = max(4, nx // 8)
+    ns, cfg = kh_problem(pkg, nx, nz)
+    if os.path.exists(REF_SPH):
+        el, pairs = time_reference(cfg, ns, 2, 1)
+        kind, what = "reference", "the reference's own SPHHydroBase + CheapSynchronousRK2 (oracle/_ref/ref_sph)"
+    else:
+        import oracle
+        o = oracle.OracleProblem(cfg, ns)
+        o.build_neighbors()
+        o.evaluate_derivatives()
+        o.step(1)
+        t0 = time.perf_counter()
+        o.step(2)
+        el = time.perf_counter() - t0
+        pairs = 2 * o.num_pairs()
+        kind, what = "port", "the oracle restatement of the reference path"
+    return {"value": pairs / el, "unit": METRIC, "cores": 1, "kind": kind,
+            "sample": "%s, serial, on a %dx%dx%d z-slab of the lattice (%d nodes, same spacing and stencil), "
+                      "2 timed RK2 steps, %.1f s" % (what, nx, nx, nz, ns.n, el),
             "cpu": platform.processor() or platform.machine()}
 
 
@@ -595,20 +708,24 @@ def _ref_worker(args):
     except Exception:
         pass
     pkg = importlib.import_module("llnl-spheral_b200")
-    import oracle
     ns, cfg = kh_problem(pkg, nx, nz, seed=20261203 + idx)
-    o = oracle.OracleProblem(cfg, ns)
-    o.build_neighbors()
-    o.evaluate_derivatives()
-    for _ in range(warmup):
-        o.step(1)
     barrier_obj.wait()
-    t0 = time.perf_counter()
-    pairs = 0
-    for _ in range(steps):
-        o.step(1)
-        pairs += o.num_pairs()
-    q.put((pairs, time.perf_counter() - t0))
+    if os.path.exists(REF_SPH):
+        el, pairs = time_reference(cfg, ns, steps, warmup)
+    else:
+        import oracle
+        o = oracle.OracleProblem(cfg, ns)
+        o.build_neighbors()
+        o.evaluate_derivatives()
+        for _ in range(warmup):
+            o.step(1)
+        t0 = time.perf_counter()
+        pairs = 0
+        for _ in range(steps):
+            o.step(1)
+            pairs += o.num_pairs()
+        el = time.perf_counter() - t0
+    q.put((pairs, el))
 
 
 def run_reference(args):
@@ -616,16 +733,17 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    import oracle
-    oracle.lib()
     cores = max(1, min(os.cpu_count() or 1, 32))
     try:
         import psutil
-        cores = max(1, min(cores, int(psutil.virtual_memory().available / 1.0e9)))
+        # each process holds about 0.8 GB for a 128x128x16 slab
+        cores = max(1, min(cores, int(psutil.virtual_memory().available / 2.0e9)))
     except Exception:
         pass
     nx = args.nx
-    nz = max(4, nx // 8)          # bounded sample: a z-slab of the same lattice (same dx, same stencil)
+    # bounded sample per process: a z-slab of the same lattice (same dx, same
+    # stencil); thinner when many steps are asked for
+    nz = max(4, nx // 8 if args.steps + args.warmup <= 16 else nx // 16)
     ctx = mp.get_context("spawn")
     bar = ctx.Barrier(cores)
     q = ctx.Queue()
@@ -639,18 +757,25 @@ def run_reference(args):
     pairs = sum(r[0] for r in res)
     el = max(r[1] for r in res)
     value = pairs / el
+    kind = "reference" if os.path.exists(REF_SPH) else "port"
+    what = ("the reference's own SPHHydroBase + CheapSynchronousRK2 compiled from its sources (oracle/_ref/ref_sph)"
+            if kind == "reference" else "the oracle restatement of the reference FP64 path")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample_nodes_per_process": nx * nx * nz,
-                       "sample": "%d concurrent processes, each a %dx%dx%d z-slab of the lattice "
-                                 "(same spacing and stencil), %d RK2 steps" % (cores, nx, nx, nz, args.steps)},
-            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port",
-                             "sample": "oracle restatement of the reference FP64 path, one serial process per core"},
+            "data": "synthetic", "config": bench_config(args.nx),
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind,
+                             "sample": "%s, one serial process per core, each a %dx%dx%d z-slab of the lattice "
+                                       "(same spacing, stencil and state), %d timed RK2 steps after %d untimed"
+                                       % (what, nx, nx, nz, args.steps, args.warmup)},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def bench_config(nx):
+    """The `config` both arms print (the same workload, the same precision)."""
+    return {"workload": WORKLOAD, "nodes": nx * nx * nx, "precision": "FP64 (the reference's arithmetic)"}
 
 
 # ------------------------------------------------------------------ our arm
@@ -664,68 +789,80 @@ def run_ours(args):
     ns, cfg = kh_problem(pkg, args.nx, seed=20261203 + rank)
     vis = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
     clocks = Clocks(vis[local] if local < len(vis) else local)
-    # headline: mixed form
-    hm, rm = measure_steps(pkg, ns, cfg, abi.PRECISION_MIXED, args.steps, args.warmup, world, clocks)
-    t_mixed = allmax(rm["total_ms"], world)
-    pairs_mixed = allsum(rm["pairs"], world)
-    # plain FP64 on the same workload
-    hp, rp = measure_steps(pkg, ns, cfg, abi.PRECISION_FP64, args.steps, args.warmup, world)
+    # headline: plain FP64, the reference's precision
+    hp, rp = measure_steps(pkg, ns, cfg, abi.PRECISION_FP64, args.steps, args.warmup, world, clocks)
     t_plain = allmax(rp["total_ms"], world)
     pairs_plain = allsum(rp["pairs"], world)
-    value = pairs_mixed / (t_mixed / 1e3)
-    plain_value = pairs_plain / (t_plain / 1e3)
-    # roofline of the dominant kernel (derivative evaluation)
+    # the mixed FP32-pair form on the same workload
+    hm, rm = measure_steps(pkg, ns, cfg, abi.PRECISION_MIXED, args.steps, args.warmup, world)
+    t_mixed = allmax(rm["total_ms"], world)
+    pairs_mixed = allsum(rm["pairs"], world)
+    value = pairs_plain / (t_plain / 1e3)
+    mixed_value = pairs_mixed / (t_mixed / 1e3)
+    # roofline of the dominant kernel pair of the step (evaluateDerivatives:
+    # record pack + pair kernel), each form
     peak, peak_kind = load_peaks()
     g = ctypes.c_int64()
     e = ctypes.c_int64()
-    hm.lib.sphgpu_connectivity_size(hm.h, ctypes.byref(g), ctypes.byref(e))
-    t_eval_mixed = measure_eval(hm)
-    t_eval_plain = measure_eval(hp)
-    t_build_mixed = measure_build(hm)
-    t_build_plain = measure_build(hp)
+    hp.lib.sphgpu_connectivity_size(hp.h, ctypes.byref(g), ctypes.byref(e))
     nodes, ghosts, entries = ns.n, g.value, e.value
-    alg_bytes = eval_alg_bytes(nodes, ghosts, entries)
-    achieved = alg_bytes / (t_eval_mixed / 1e3) / 1e9
-    traffic = EVAL_TRAFFIC_96 * alg_bytes / eval_alg_bytes(*EVAL_UNITS_96)
+    t_eval_plain = measure_eval(hp)
+    t_eval_mixed = measure_eval(hm)
+    t_build_plain = measure_build(hp)
+    t_build_mixed = measure_build(hm)
+
+    def roofline(form, alg, t_eval, kernel):
+        achieved = alg / (t_eval / 1e3) / 1e9
+        measured = EVAL_TRAFFIC_96[form]
+        units96 = eval_alg_bytes_fp64(*EVAL_UNITS_96) if form == "fp64" else eval_alg_bytes_mixed(*EVAL_UNITS_96)
+        return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
+                "peak_kind": peak_kind + " (MEASURED_PEAKS hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None if measured is None else measured * alg / units96,
+                "traffic_source": None if measured is None else
+                "ncu dram__bytes_read.sum + dram__bytes_write.sum of the two kernels on Kelvin-Helmholtz 96^3, "
+                "scaled by the algorithmic bytes",
+                "algorithmic_bytes": alg, "eval_ms": t_eval}
+
     result = None
     if rank == 0:
-        lat = sorted(rm["per_step_ms"])
-        latp = sorted(rp["per_step_ms"])
-
         def pct(v, q):
+            v = sorted(v)
             return v[min(len(v) - 1, int(round(q * (len(v) - 1))))]
         result = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_mixed / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair / f64 state", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "nodes_per_gpu": nodes, "ghosts": ghosts,
-                       "pairs_per_step": rm["pairs"] / args.steps, "precision": "mixed FP32-pair/FP64-critical",
-                       "parallelism": "one independent problem per GPU" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (state %.2f GB, pair records %.2f GB)" % (
-                           nodes * 18 * 8 / 1e9, (nodes + ghosts) * 160 / 1e9)},
-            "latency_ms": {"p50": pct(lat, 0.5), "p99": pct(lat, 0.99)},
-            "stage_ms": {"neighbor_build": t_build_mixed, "evaluate_derivatives": t_eval_mixed,
-                         "rk2_step": t_mixed / args.steps},
-            "plain_fp64": {"value": plain_value, "unit": METRIC, "ms_per_step": t_plain / args.steps,
-                           "latency_ms": {"p50": pct(latp, 0.5), "p99": pct(latp, 0.99)},
-                           "eval_ms": t_eval_plain, "build_ms": t_build_plain},
-            "mixed_over_plain": value / plain_value,
-            "roofline": {"bound": "hbm", "kernel": "evaluateDerivatives (record pack + sph_eval_mixed)",
-                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of pack_mixed_kernel + "
-                                           "sph_eval_mixed_kernel on Kelvin-Helmholtz 96^3, scaled by the "
-                                           "algorithmic bytes",
-                         "algorithmic_bytes": alg_bytes, "eval_ms": t_eval_mixed},
-            "gpu_launches": rm["launches"],
-            "clocks": rm["clocks"],
+            "warmup": args.warmup, "ms_per_step": t_plain / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": bench_config(args.nx),
+            "problem": {"nodes_per_gpu": nodes, "ghosts": ghosts, "pairs_per_step": rp["pairs"] / args.steps,
+                        "parallelism": "one independent problem per GPU" if world > 1 else "single GPU",
+                        "l2": "inputs larger than L2 (state %.2f GB, pair records %.2f GB)" % (
+                            nodes * 18 * 8 / 1e9, (nodes + ghosts) * 160 / 1e9)},
+            "latency_ms": {"p50": pct(rp["per_step_ms"], 0.5), "p99": pct(rp["per_step_ms"], 0.99)},
+            "stage_ms": {"neighbor_build": t_build_plain, "evaluate_derivatives": t_eval_plain,
+                         "rk2_step": t_plain / args.steps},
+            "mixed": {"value": mixed_value, "unit": METRIC, "ms_per_step": t_mixed / args.steps,
+                      "dtype": "f32 pair / f64 state",
+                      "latency_ms": {"p50": pct(rm["per_step_ms"], 0.5), "p99": pct(rm["per_step_ms"], 0.99)},
+                      "stage_ms": {"neighbor_build": t_build_mixed, "evaluate_derivatives": t_eval_mixed,
+                                   "rk2_step": t_mixed / args.steps},
+                      "roofline": roofline("mixed", eval_alg_bytes_mixed(nodes, ghosts, entries), t_eval_mixed,
+                                           "evaluateDerivatives (pack_mixed + sph_eval_mixed)"),
+                      "gpu_launches": rm["launches"]},
+            "mixed_over_plain": mixed_value / value,
+            "roofline": roofline("fp64", eval_alg_bytes_fp64(nodes, ghosts, entries), t_eval_plain,
+                                 "evaluateDerivatives (pack_records + sph_eval_fp64)"),
+            "gpu_launches": rp["launches"],
+            "clocks": rp["clocks"],
         }
         if not args.no_e2e:
+            esteps = max(3, args.steps // 2)
+            result["e2e"] = measure_e2e(pkg, ns, cfg, esteps, 1)
             cm = cfg.copy()
             cm.precision = abi.PRECISION_MIXED
-            result["e2e"] = measure_e2e(pkg, ns, cm, max(3, args.steps // 2), 1)
+            result["mixed"]["e2e"] = measure_e2e(pkg, ns, cm, esteps, 1)
         if world == 1 and not args.no_cpu_baseline:
-            result["cpu_baseline"] = cpu_baseline(pkg, ns, cfg)
+            result["cpu_baseline"] = cpu_baseline(pkg, args.nx)
     hm.close()
     hp.close()
     if args.accuracy_steps > 0:

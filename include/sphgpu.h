@@ -194,7 +194,11 @@ int sphgpu_checkpoint_size(sphgpu_problem* p, int64_t* bytes);
 int sphgpu_checkpoint_save(sphgpu_problem* p, void* buffer, int64_t bytes);
 int sphgpu_checkpoint_load(sphgpu_problem* p, const void* buffer, int64_t bytes);
 /* SpheralConservation (src/SimulationControl/SpheralConservation.py:27-63):
- * out = {mass, px, py, pz, kinetic E, thermal E, total E, 0}, FP64 on device. */
+ * out = {mass, px, py, pz, kinetic E, thermal E, total E, total E low part},
+ * FP64 on device.  The total energy is summed as a double-double (two-sum
+ * compensation): out[6] is its rounded value and out[6] + out[7] the total to
+ * about 2^-100 relative, so an energy drift below the rounding of a plain FP64
+ * sum is still resolved. */
 int sphgpu_conservation(sphgpu_problem* p, double out[8]);
 /* The same sums over caller-owned DEVICE arrays (reference Field layout:
  * mass[n], velocity[3n] AoS, specificThermalEnergy[n]) with no problem

@@ -837,29 +837,50 @@ __global__ void finish_step_kernel(const Member* mem, int nmem) {
 
 // ---------------------------------------------------------------- conservation
 // Fixed partition per member (grid-stride over its blocks), fixed-order
-// reduction: the sums are reproducible.
+// reduction: the sums are reproducible.  The total energy is also summed as
+// a double-double (Knuth's two-sum: each addition's rounding error is kept in
+// a second double), so that drifts far below the rounding of a plain FP64
+// sum over millions of nodes can be read: out[6] + out[7] is the total to
+// about 2^-100 relative, out[6] alone its rounded value.
+__device__ __forceinline__ void twoSumAdd(double& hi, double& lo, double x) {
+  const double s = hi + x;
+  const double bb = s - hi;
+  const double err = (hi - (s - bb)) + (x - bb);
+  hi = s;
+  lo += err;
+}
+
 __global__ void __launch_bounds__(256) conservation_partials_kernel(const Member* mem, BlockMap bm) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = mem[mb.m];
   const int64_t n = MB.n;
   const double* S = MB.S;
-  double acc[6] = {0, 0, 0, 0, 0, 0};
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int64_t i = mb.block*blockDim.x + threadIdx.x; i < n; i += (int64_t)mb.blocks*blockDim.x) {
     const double m = S[S_M*n + i];
     const V3 v{S[S_VX*n + i], S[S_VY*n + i], S[S_VZ*n + i]};
+    const double ke = 0.5*m*mag2(v), te = m*S[S_EPS*n + i];
     acc[0] += m;
     acc[1] += m*v.x; acc[2] += m*v.y; acc[3] += m*v.z;
-    acc[4] += 0.5*m*mag2(v);
-    acc[5] += m*S[S_EPS*n + i];
+    acc[4] += ke;
+    acc[5] += te;
+    twoSumAdd(acc[6], acc[7], ke);
+    twoSumAdd(acc[6], acc[7], te);
   }
-  __shared__ double sh[6][256];
-  for (int c = 0; c < 6; ++c) sh[c][threadIdx.x] = acc[c];
+  __shared__ double sh[8][256];
+  for (int c = 0; c < 8; ++c) sh[c][threadIdx.x] = acc[c];
   __syncthreads();
   for (int s = blockDim.x/2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) for (int c = 0; c < 6; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + s];
+    if (threadIdx.x < s) {
+      for (int c = 0; c < 6; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + s];
+      double hi = sh[6][threadIdx.x], lo = sh[7][threadIdx.x] + sh[7][threadIdx.x + s];
+      twoSumAdd(hi, lo, sh[6][threadIdx.x + s]);
+      sh[6][threadIdx.x] = hi;
+      sh[7][threadIdx.x] = lo;
+    }
     __syncthreads();
   }
-  if (threadIdx.x == 0) for (int c = 0; c < 6; ++c) MB.red[mb.block*6 + c] = sh[c][0];
+  if (threadIdx.x == 0) for (int c = 0; c < 8; ++c) MB.red[mb.block*8 + c] = sh[c][0];
 }
 
 __global__ void conservation_final_kernel(const Member* mem, int nmem, const int32_t* partialBlocks, int soloBlocks) {
@@ -868,11 +889,19 @@ __global__ void conservation_final_kernel(const Member* mem, int nmem, const int
   const Member& MB = mem[m];
   const int nb = partialBlocks ? partialBlocks[m + 1] - partialBlocks[m] : soloBlocks;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int b = 0; b < nb; ++b) for (int c = 0; c < 6; ++c) acc[c] += MB.red[b*6 + c];
+  double hi = 0.0, lo = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    for (int c = 0; c < 6; ++c) acc[c] += MB.red[b*8 + c];
+    lo += MB.red[b*8 + 7];
+    twoSumAdd(hi, lo, MB.red[b*8 + 6]);
+  }
+  // renormalise: hi the rounded total, lo what it leaves out
+  const double s = hi + lo;
+  const double e = lo - (s - hi);
   double* out = MB.scal + SC_CONS;
   for (int c = 0; c < 6; ++c) out[c] = acc[c];
-  out[6] = acc[4] + acc[5];
-  out[7] = 0.0;
+  out[6] = s;
+  out[7] = e;
 }
 
 __global__ void __launch_bounds__(256) zero_derivs_kernel(const Member* mem, BlockMap bm) {

@@ -13,10 +13,17 @@
 // finalizeDerivatives at the start time, then CheapSynchronousRK2 steps.
 //
 // usage: ref_sph input.bin outdir
+//        ref_sph --time WARMUP input.bin
+// The second form times the reference's CheapSynchronousRK2 steps instead of
+// writing fields: after the start-up and WARMUP untimed steps it runs the
+// input's step count, timing each step, and prints one JSON line with the
+// steps, the seconds they took and the pair interactions they evaluated (the
+// reference's ncalc: internal pairs j > i plus every ghost pair).
 // input.bin: int64 n, int64 nsteps, sphgpu_config (raw struct), then the
 // internal nodes' position[3n], velocity[3n], mass[n], mass density[n],
 // specific thermal energy[n], H[6n] (float64, the reference Field layouts).
 // Writes raw little-endian arrays (name.f64 / name.i64) into outdir.
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -58,9 +65,12 @@ typedef D::SymTensor SymTensor;
 namespace {
 
 std::string g_dir;
+bool g_timing = false;
+int g_warmup = 0;
 
 template<typename T>
 void dumpRaw(const std::string& name, const std::vector<T>& v, const char* ext) {
+  if (g_timing) return;
   const std::string path = g_dir + "/" + name + ext;
   FILE* f = std::fopen(path.c_str(), "wb");
   if (!f) { std::perror(path.c_str()); std::exit(1); }
@@ -84,6 +94,7 @@ void put(std::vector<double>& out, const SymTensor& x) {
 // Internal-node values of a one-NodeList FieldList.
 template<typename Value>
 void dumpField(const std::string& name, const FieldSpace::FieldList<D, Value>& fl, int n) {
+  if (g_timing) return;
   std::vector<double> out;
   const FieldSpace::Field<D, Value>& f = *fl[0];
   for (int i = 0; i < n; ++i) put(out, f(i));
@@ -91,6 +102,7 @@ void dumpField(const std::string& name, const FieldSpace::FieldList<D, Value>& f
 }
 template<typename Value>
 void dumpField(const std::string& name, const FieldSpace::Field<D, Value>& f, int n) {
+  if (g_timing) return;
   std::vector<double> out;
   for (int i = 0; i < n; ++i) put(out, f(i));
   dump(name, out);
@@ -220,6 +232,24 @@ int run(const Input& in, Hydro& hydro, NodeSpace::FluidNodeList<D>& nodes, DataB
   dumpForm(hydro, n);
   dump("eval/hydro dt", std::vector<double>(1, hydro.dt(db, state, derivs, 0.0).first));
 
+  if (g_timing) {
+    for (int s = 0; s < g_warmup; ++s) integ.step(1e30);
+    double seconds = 0.0;
+    int64_t pairs = 0;
+    for (int64_t s = 0; s < in.nsteps; ++s) {
+      const auto t0 = std::chrono::steady_clock::now();
+      integ.step(1e30);
+      seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      const NeighborSpace::ConnectivityMap<D>& cmap = db.connectivityMap();
+      for (int i = 0; i < n; ++i)
+        for (int j : cmap.connectivityForNode(&nodes, i)[0]) pairs += (j > i);
+    }
+    for (auto* bc : bcs) delete bc;
+    std::printf("{\"steps\": %lld, \"seconds\": %.6f, \"pairs\": %lld, \"nodes\": %d}\n",
+                (long long)in.nsteps, seconds, (long long)pairs, n);
+    return 0;
+  }
+
   // CheapSynchronousRK2 steps.
   std::vector<double> tdt;
   for (int64_t s = 0; s < in.nsteps; ++s) {
@@ -244,11 +274,21 @@ int run(const Input& in, Hydro& hydro, NodeSpace::FluidNodeList<D>& nodes, DataB
 }  // namespace
 
 int main(int argc, char** argv) {
-  if (argc < 3) { std::fprintf(stderr, "usage: %s input.bin outdir\n", argv[0]); return 2; }
-  g_dir = argv[2];
+  const char* inputPath = nullptr;
+  if (argc == 4 && std::string(argv[1]) == "--time") {
+    g_timing = true;
+    g_warmup = std::atoi(argv[2]);
+    inputPath = argv[3];
+  } else if (argc == 3) {
+    g_dir = argv[2];
+    inputPath = argv[1];
+  } else {
+    std::fprintf(stderr, "usage: %s input.bin outdir | %s --time WARMUP input.bin\n", argv[0], argv[0]);
+    return 2;
+  }
   Input in;
-  FILE* fin = std::fopen(argv[1], "rb");
-  if (!fin) { std::perror(argv[1]); return 1; }
+  FILE* fin = std::fopen(inputPath, "rb");
+  if (!fin) { std::perror(inputPath); return 1; }
   int64_t n64 = 0;
   if (std::fread(&n64, 8, 1, fin) != 1 || std::fread(&in.nsteps, 8, 1, fin) != 1 ||
       std::fread(&in.cfg, sizeof(in.cfg), 1, fin) != 1) { std::fprintf(stderr, "short input\n"); return 1; }

@@ -1,10 +1,14 @@
-"""The benchmark configurations at full size.
+"""The benchmark configurations at full size, against the oracle.
 
-Configuration 1 (Sod, 262,144 nodes, cubic B-spline, nPerh 1.51) is compared
-with the oracle directly; configuration 2 (Kelvin-Helmholtz, 2,097,152 nodes,
-Wendland C4, nPerh 1.35) through size-independent properties: neighbor count,
-exact momentum balance of the pair forces, compatible-energy conservation,
-and the mixed form's error against FP64.
+Configuration 1 (Sod, 262,144 nodes, cubic B-spline, nPerh 1.51),
+configuration 2 (Kelvin-Helmholtz, 2,097,152 nodes, Wendland C4, nPerh 1.35)
+and configuration 3 (CRKSPH Kelvin-Helmholtz, 1,048,576 nodes) are compared
+with the oracle directly: ghost roots and ConnectivityMap bit for bit, every
+derivative field within 1e-12 normwise and bit-equal outside the fields that
+go through the ideal-H cube root (CUDA pow vs glibc pow), the mixed form
+within 1e-5 of FP64.  Configuration 2 is also checked through
+size-independent properties: neighbor count, exact momentum balance of the
+pair forces and compatible-energy conservation over two steps.
 """
 import numpy as np
 import pytest
@@ -12,6 +16,68 @@ import pytest
 from conftest import normwise
 
 pytestmark = pytest.mark.gpu
+
+SPH_KEYS = ["delta velocity hydro", "delta specific thermal energy", "delta mass density", "delta position",
+            "new mass density", "normalization", "velocity gradient", "M SPH gradient correction", "delta H",
+            "new H", "weighted neighbor sum", "mass second moment", "max viscous pressure",
+            "effective viscous pressure", "viscous work rate"]
+CRK_KEYS = ["node volume", "A CRKSPH correction", "B CRKSPH correction", "grad A CRKSPH correction",
+            "grad B CRKSPH correction", "m0 CRKSPH moment", "m1 CRKSPH moment", "m2 CRKSPH moment",
+            "grad m0 CRKSPH moment", "grad m1 CRKSPH moment", "grad m2 CRKSPH moment",
+            "delta velocity hydro", "delta specific thermal energy", "delta mass density", "velocity gradient",
+            "delta H", "new H", "weighted neighbor sum", "mass second moment", "mass density gradient"]
+POW_KEYS = {"weighted neighbor sum", "new H"}
+MIXED_KEYS = ["delta velocity hydro", "delta specific thermal energy", "delta mass density"]
+
+
+def _full_parity(pkg, oracle_mod, ns, cfg, keys):
+    g = pkg.SPHHydro(cfg, ns)
+    o = oracle_mod.OracleProblem(cfg, ns)
+    g.build_neighbors()
+    o.build_neighbors()
+    go, gn, gr = g.connectivity()
+    oo, on, orr = o.connectivity()
+    assert len(gr) == len(orr) and np.array_equal(gr, orr)
+    assert np.array_equal(go, oo) and np.array_equal(gn, on)
+    g.initialize()
+    o.initialize()
+    g.evaluateDerivatives()
+    o.evaluate_derivatives()
+    for k in keys:
+        a, b = g.field(k), o.field(k)
+        assert normwise(a, b) <= 1e-12, k
+        if k not in POW_KEYS:
+            assert np.array_equal(a, b), k
+    ref = {k: o.field(k) for k in MIXED_KEYS}
+    del o
+    g.close()
+    cm = cfg.copy()
+    cm.precision = pkg.abi.PRECISION_MIXED
+    m = pkg.SPHHydro(cm, ns)
+    m.build_neighbors()
+    _, mn, _ = m.connectivity()
+    assert np.array_equal(mn, gn)
+    m.initialize()
+    m.evaluateDerivatives()
+    for k in MIXED_KEYS:
+        assert normwise(m.field(k), ref[k]) <= 1e-5, k
+    m.close()
+    return gn
+
+
+def test_config2_kh_full_parity(gpu_lib, pkg, oracle_mod):
+    gen, abi = pkg.generators, pkg.abi
+    ns = gen.kelvin_helmholtz()
+    assert ns.n == 2097152
+    gn = _full_parity(pkg, oracle_mod, ns, gen.kh_config(abi), SPH_KEYS)
+    assert 5.5 <= len(gn) / ns.n <= 6.5
+
+
+def test_config3_crk_kh_full_parity(gpu_lib, pkg, oracle_mod):
+    gen, abi = pkg.generators, pkg.abi
+    ns = gen.kelvin_helmholtz(nx=128, ny=128, nz=64, box=((0, 0, 0), (1.0, 1.0, 1.0)))
+    assert ns.n == 1048576
+    _full_parity(pkg, oracle_mod, ns, gen.kh_config(abi, hydro=abi.HYDRO_CRKSPH), CRK_KEYS)
 
 
 def test_config1_sod_full_parity(gpu_lib, pkg, oracle_mod):
