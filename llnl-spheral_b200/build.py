@@ -9,6 +9,7 @@ and a batch member would differ from its solo run in the last bits.
     python llnl-spheral_b200/build.py [--force] [--verbose]
 """
 import argparse
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -51,31 +52,40 @@ def needs_build():
     return any(_mtime(d) > t for d in deps)
 
 
-def build(force=False, verbose=False, ptxas_info=False):
-    if not force and not needs_build():
+def build(force=False, verbose=False, ptxas_info=False, lib_path=None, extra_flags=()):
+    """Compile every unit (in parallel) and link the library.  lib_path and
+    extra_flags (e.g. -D tuning constants) build a variant elsewhere."""
+    lib = lib_path or LIB
+    if lib_path is None and not force and not needs_build():
         return LIB
-    os.makedirs(BUILD, exist_ok=True)
-    objs = []
+    objdir = os.path.join(os.path.dirname(lib), "obj_" + os.path.basename(lib).replace(".", "_"))
+    os.makedirs(objdir, exist_ok=True)
+    cmds = []
     for src, extra in UNITS:
         path = os.path.join(CSRC, src)
         if not os.path.exists(path):
             continue
-        obj = os.path.join(BUILD, src + ".o")
-        cmd = [NVCC] + ARCH + COMMON + extra + ["-c", path, "-o", obj]
+        obj = os.path.join(objdir, src + ".o")
+        cmd = [NVCC] + ARCH + COMMON + extra + list(extra_flags) + ["-c", path, "-o", obj]
         if ptxas_info and src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"]
         if src.endswith(".cc"):
             cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off",
                    "-fno-fast-math", "-c", path, "-o", obj]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.check_call(cmd)
-        objs.append(obj)
-    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmds.append((cmd, obj))
+    with concurrent.futures.ThreadPoolExecutor(min(len(cmds), os.cpu_count() or 4)) as ex:
+        for cmd, r in zip(cmds, ex.map(lambda c: subprocess.run(c[0], capture_output=True, text=True), cmds)):
+            if verbose or ptxas_info:
+                print(" ".join(cmd[0]), flush=True)
+                sys.stdout.write(r.stdout + r.stderr)
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, cmd[0])
+    cmd = [NVCC] + ARCH + ["-shared", "-o", lib] + [o for _, o in cmds] + ["-lcudart"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

@@ -25,6 +25,15 @@
 #include "mixed.cuh"
 #include "../../include/sphgpu.h"
 
+// Blocks of 128 threads per SM the derivative pair kernels are compiled for
+// (the register budget follows: 65,536 / (128 x blocks)).
+#ifndef SPH_FP64_MIN_BLOCKS
+#define SPH_FP64_MIN_BLOCKS 1
+#endif
+#ifndef SPH_MIXED_MIN_BLOCKS
+#define SPH_MIXED_MIN_BLOCKS 3
+#endif
+
 namespace sphgpu {
 
 enum StateField {

@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(256) pack_mixed_kernel(const Member* mem, Bloc
 // One directed pair (i, j) of SPHHydroBase::evaluateDerivatives, formed in
 // owner orientation, accumulated into node i.
 template<bool XSPH, bool TENSILE, bool COMPAT, bool SOLO>
-__global__ void __launch_bounds__(128) sph_eval_fp64_kernel(const Member* mem, BlockMap bm, const Member single) {
+__global__ void __launch_bounds__(128, SPH_FP64_MIN_BLOCKS) sph_eval_fp64_kernel(const Member* mem, BlockMap bm, const Member single) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = SOLO ? single : mem[mb.m];   // one member: read from the kernel parameters
   const int64_t n = MB.n;

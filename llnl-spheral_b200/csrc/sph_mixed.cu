@@ -84,7 +84,7 @@ __device__ __forceinline__ void tableF(const float* coef, int n, float invStep, 
 // recordMid): the FP64 mid-point H and mass density of a member without
 // grad-h are in S0, S holds the start of the step.
 template<bool XSPH, bool TENSILE, bool COMPAT, bool SOLO>
-__global__ void __launch_bounds__(128, 3) sph_eval_mixed_kernel(const Member* mem, BlockMap bm, const Member single,
+__global__ void __launch_bounds__(128, SPH_MIXED_MIN_BLOCKS) sph_eval_mixed_kernel(const Member* mem, BlockMap bm, const Member single,
                                                                  int midInS0) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = SOLO ? single : mem[mb.m];   // one member: read from the kernel parameters

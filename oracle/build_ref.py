@@ -12,8 +12,8 @@ installed here), into oracle/_ref/:
               State and its update policies, SPHHydroBase, CRKSPHHydroBase, the
               CRKSPH moment / correction / volume / density functions,
               MonaghanGingoldViscosity, CRKSPHMonaghanGingoldViscosity,
-              SPHSmoothingScale, GammaLawGas, GenericHydro, Integrator and
-              CheapSynchronousRK2 (oracle/refshim/ref_sph.cc)
+              SPHSmoothingScale, GammaLawGas, GenericHydro, Integrator,
+              CheapSynchronousRK2 and iterateIdealH (oracle/refshim/ref_sph.cc)
 
 Every reference translation unit is compiled on its own, followed by one
 hand-written explicit instantiation for Dim<3> (the reference generates those
@@ -200,6 +200,10 @@ UNITS = [
         "template FieldList<Dim<3>, KeyTraits::Key> mortonOrderIndices<Dim<3> >(const DataBase<Dim<3> >&);\n"
         "template FieldList<Dim<3>, KeyTraits::Key> mortonOrderIndices<Dim<3> >(const DataBase<Dim<3> >&, "
         "const FieldList<Dim<3>, int>&);" % _fl("Vector"))),
+    ("Utilities/iterateIdealH.cc", USING % (
+        "template void iterateIdealH<Dim<3> >(DataBase<Dim<3> >&, const std::vector<BoundarySpace::Boundary<Dim<3> >*>&, "
+        "const TableKernel<Dim<3> >&, const SmoothingScaleBase<Dim<3> >&, const int, const double, const double, "
+        "const bool, const bool);")),
     ("DataOutput/RestartRegistrar.cc", ""),
     ("FileIO/FileIO.cc", ""),
 ]

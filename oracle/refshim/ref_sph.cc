@@ -14,11 +14,17 @@
 //
 // usage: ref_sph input.bin outdir
 //        ref_sph --time WARMUP input.bin
+//        ref_sph --ideal-h MAXITER TOLERANCE input.bin outdir
 // The second form times the reference's CheapSynchronousRK2 steps instead of
 // writing fields: after the start-up and WARMUP untimed steps it runs the
 // input's step count, timing each step, and prints one JSON line with the
 // steps, the seconds they took and the pair interactions they evaluated (the
-// reference's ncalc: internal pairs j > i plus every ghost pair).
+// reference's ncalc: internal pairs j > i plus every ghost pair).  The third
+// form runs the reference's iterateIdealH (src/Utilities/iterateIdealH.cc) the
+// way SpheralController.iterateIdealH calls it (SPHSmoothingScale, no nPerh
+// rescaling, no spherical start, no fixed determinant) after the start-up
+// ghosts, and writes the relaxed H and the iteration count and last change it
+// reports.
 // input.bin: int64 n, int64 nsteps, sphgpu_config (raw struct), then the
 // internal nodes' position[3n], velocity[3n], mass[n], mass density[n],
 // specific thermal energy[n], H[6n] (float64, the reference Field layouts).
@@ -28,7 +34,9 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <iostream>
 #include <memory>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -53,6 +61,7 @@
 #include "ArtificialViscosity/CRKSPHMonaghanGingoldViscosity.hh"
 #include "Geometry/GeomThirdRankTensor.hh"
 #include "Integrator/CheapSynchronousRK2.hh"
+#include "Utilities/iterateIdealH.hh"
 
 #include "sphgpu.h"
 
@@ -67,6 +76,8 @@ namespace {
 std::string g_dir;
 bool g_timing = false;
 int g_warmup = 0;
+int g_idealHMax = -1;          // >= 0: run iterateIdealH instead of the steps
+double g_idealHTol = 0.0;
 
 template<typename T>
 void dumpRaw(const std::string& name, const std::vector<T>& v, const char* ext) {
@@ -193,6 +204,27 @@ int run(const Input& in, Hydro& hydro, NodeSpace::FluidNodeList<D>& nodes, DataB
   integ.currentTime(0.0);
 
   integ.setGhostNodes();
+  if (g_idealHMax >= 0) {
+    // SpheralController.iterateIdealH (src/SimulationControl/SpheralController.py:718-731)
+    NodeSpace::SPHSmoothingScale<D> method;
+    std::stringstream log;
+    std::streambuf* old = std::cerr.rdbuf(log.rdbuf());
+    iterateIdealH(db, integ.uniqueBoundaryConditions(), hydro.kernel(), method, g_idealHMax, g_idealHTol,
+                  0.0, false, false);
+    std::cerr.rdbuf(old);
+    // its progress lines: "iterateIdealH: (iteration, deltaH) = (itr, maxDeltaH)"
+    double itr = -1.0, dh = -1.0;
+    std::string line;
+    while (std::getline(log, line)) {
+      const size_t k = line.find(") = (");
+      if (k != std::string::npos) std::sscanf(line.c_str() + k + 5, "%lf, %lf", &itr, &dh);
+    }
+    dumpField("idealh/H", nodes.Hfield(), n);
+    dump("idealh/iterations_delta", std::vector<double>{itr, dh});
+    for (auto* bc : bcs) delete bc;
+    std::printf("ok %d nodes, %g iterations\n", n, itr);
+    return 0;
+  }
   std::vector<PhysicsSpace::Physics<D>*> packages(1, &hydro);
   hydro.initializeProblemStartup(db);
   for (auto* bc : bcs) bc->initializeProblemStartup();
@@ -275,7 +307,12 @@ int run(const Input& in, Hydro& hydro, NodeSpace::FluidNodeList<D>& nodes, DataB
 
 int main(int argc, char** argv) {
   const char* inputPath = nullptr;
-  if (argc == 4 && std::string(argv[1]) == "--time") {
+  if (argc == 6 && std::string(argv[1]) == "--ideal-h") {
+    g_idealHMax = std::atoi(argv[2]);
+    g_idealHTol = std::atof(argv[3]);
+    inputPath = argv[4];
+    g_dir = argv[5];
+  } else if (argc == 4 && std::string(argv[1]) == "--time") {
     g_timing = true;
     g_warmup = std::atoi(argv[2]);
     inputPath = argv[3];

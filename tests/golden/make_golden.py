@@ -121,10 +121,53 @@ def sph_fixture(exe, name, ns, cfg, nsteps):
     return out
 
 
+def idealh_cases(pkg):
+    """name -> (node set, config): Sod tubes whose H are perturbed away from
+    the ideal (isotropic scale jitter; and with off-diagonal terms)."""
+    gen, abi = pkg.generators, pkg.abi
+    out = {}
+    for name, aniso in (("iso", False), ("aniso", True)):
+        box = ((0.0, 0.0, 0.0), (1.0, 0.25, 0.25))
+        ns = gen.sod(nx=32, ny=8, nz=8, box=box, jitter=0.1, seed=3)
+        rng = np.random.default_rng(1)
+        ns.H[:, [0, 3, 5]] *= rng.uniform(0.6, 1.5, (ns.n, 1))
+        if aniso:
+            ns.H[:, 1] = 0.05 * ns.H[:, 0] * rng.uniform(-1, 1, ns.n)
+            ns.H[:, 3] *= rng.uniform(0.8, 1.2, ns.n)
+        out[name] = (ns, gen.sod_config(abi, ns_box=box))
+    return out
+
+
+def idealh_fixture(exe, name, ns, cfg, max_iterations=50, tolerance=1.0e-4):
+    """The reference's iterateIdealH as its controller calls it: the relaxed
+    H, the iteration count and the last maximum change it reports (printed
+    to six significant digits by the reference)."""
+    with tempfile.TemporaryDirectory() as td:
+        os.makedirs(os.path.join(td, "idealh"))
+        write_input(os.path.join(td, "in.bin"), cfg, ns, 0)
+        subprocess.check_call([exe, "--ideal-h", str(max_iterations), repr(tolerance), os.path.join(td, "in.bin"), td],
+                              stdout=subprocess.DEVNULL)
+        H = np.fromfile(os.path.join(td, "idealh", "H.f64"), dtype="<f8")
+        itd = np.fromfile(os.path.join(td, "idealh", "iterations_delta.f64"), dtype="<f8")
+    data = {"input/config": np.frombuffer(bytes(cfg), dtype=np.uint8), "input/position": ns.pos,
+            "input/velocity": ns.vel, "input/mass": ns.mass, "input/mass density": ns.rho,
+            "input/specific thermal energy": ns.eps, "input/H": ns.H,
+            "input/max_iterations": np.int64(max_iterations), "input/tolerance": np.float64(tolerance),
+            "H": H, "iterations": np.int64(itd[0]), "max_delta_h_printed": np.float64(itd[1])}
+    out = os.path.join(HERE, "reference_idealh_%s.npz" % name)
+    np.savez_compressed(out, **data)
+    return out
+
+
 def main(argv):
     build_ref = importlib.import_module("build_ref")
     ref_sph, ref_tables = build_ref.build()
     want = argv[1:]
+    pkg = importlib.import_module("llnl-spheral_b200")
+    for name, (ns, cfg) in idealh_cases(pkg).items():
+        if want and "idealh_" + name not in want:
+            continue
+        print(idealh_fixture(ref_sph, name, ns, cfg))
     if not want or "tables" in want:
         with tempfile.TemporaryDirectory() as td:
             subprocess.check_call([ref_tables, td], stdout=subprocess.DEVNULL)

@@ -53,3 +53,19 @@ def test_gpu_matches_reference(gpu_lib, pkg, name):
         assert normwise(g.field(key).ravel(), fx["steps/" + key]) <= 1e-12, key
     if fx.cfg.hydro == pkg.abi.HYDRO_CRKSPH:
         assert normwise(g.field("node volume").ravel(), fx["steps/node volume"]) <= 1e-12
+
+
+from test_oracle_reference import IDEALH, idealh_fixture  # noqa: E402
+
+
+@pytest.mark.parametrize("path", IDEALH, ids=[p.split("/")[-1][:-4] for p in IDEALH])
+def test_gpu_iterate_ideal_h_matches_reference(gpu_lib, pkg, path):
+    """sphgpu_iterate_ideal_h against the reference's iterateIdealH: same
+    iteration count, the last change to the reference's printed digits, H
+    within 1e-12 (the cube root of the zeroth moment is CUDA's pow)."""
+    d, cfg, nodes = idealh_fixture(pkg, path)
+    g = pkg.SPHHydro(cfg, nodes)
+    itr, dh = g.iterateIdealH(int(d["input/max_iterations"]), float(d["input/tolerance"]))
+    assert itr == int(d["iterations"])
+    assert abs(dh - float(d["max_delta_h_printed"])) <= 1e-5 * dh
+    assert normwise(g.field("H").ravel(), d["H"]) <= 1e-12

@@ -123,3 +123,28 @@ def test_fixtures_match_a_fresh_reference_run(pkg):
                 assert np.array_equal(pair_acc_digest(v), fx["eval/pair accelerations sha256"])
             else:
                 assert np.array_equal(v, fx[k]), k
+
+
+IDEALH = sorted(glob.glob(os.path.join(HERE, "golden", "reference_idealh_*.npz")))
+
+
+def idealh_fixture(pkg, path):
+    d = np.load(path)
+    cfg = pkg.abi.SphConfig.from_buffer_copy(d["input/config"].tobytes())
+    nodes = pkg.generators.NodeSet(d["input/position"], d["input/velocity"], d["input/mass"], d["input/mass density"],
+                                   d["input/specific thermal energy"], d["input/H"], None)
+    return d, cfg, nodes
+
+
+@pytest.mark.parametrize("path", IDEALH, ids=[os.path.basename(p)[:-4] for p in IDEALH])
+def test_oracle_iterate_ideal_h_matches_reference(pkg, oracle_mod, path):
+    """The reference's iterateIdealH (src/Utilities/iterateIdealH.cc, run by
+    oracle/_ref/ref_sph as SpheralController.iterateIdealH calls it): the
+    oracle's relaxed H is bit-equal, its iteration count equal, and its last
+    change equal to the six digits the reference prints."""
+    d, cfg, nodes = idealh_fixture(pkg, path)
+    o = oracle_mod.OracleProblem(cfg, nodes)
+    itr, dh = o.iterate_ideal_h(int(d["input/max_iterations"]), float(d["input/tolerance"]))
+    assert itr == int(d["iterations"]) and 1 < itr < int(d["input/max_iterations"])
+    assert abs(dh - float(d["max_delta_h_printed"])) <= 1e-5 * dh
+    assert np.array_equal(o.field("H").ravel(), d["H"])
