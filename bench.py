@@ -92,7 +92,8 @@ def eval_alg_bytes_mixed(nodes, ghosts, entries):
 # (884,736 nodes, 56,456 ghosts, 5,363,712 entries) for the record pack and
 # the pair kernel of each form; scaled to other sizes by the algorithmic
 # bytes (all three units grow together).
-EVAL_TRAFFIC_96 = {"fp64": None, "mixed": 150498816 + 67565056 + 190594816 + 386470912}
+EVAL_TRAFFIC_96 = {"fp64": 155681536 + 107269376 + 180020480 + 449962752,
+                   "mixed": 150498816 + 67565056 + 190594816 + 386470912}
 EVAL_UNITS_96 = (884736, 56456, 5363712)
 
 
@@ -359,13 +360,34 @@ def energy(h):
     return float(c[6]), float(c[7])
 
 
+def position_errors(a, b, box):
+    """field_errors of positions with each difference taken to the nearest
+    periodic image (a node that crossed a periodic plane in one run and not
+    in the other is one box length away, not an error)."""
+    a = np.asarray(a, dtype=np.float64).reshape(-1, 3)
+    b = np.asarray(b, dtype=np.float64).reshape(-1, 3)
+    L = np.asarray(box, dtype=np.float64)
+    d = a - b
+    d -= L * np.round(d / L)
+    return field_errors(b + d, b)
+
+
+GROWTH_STEPS = (1, 2, 5, 10, 20, 50, 100, 200, 400)
+GROWTH_FIELDS = ("velocity", "specific thermal energy", "delta velocity hydro")
+
+
 def measure_accuracy(pkg, ns, cfg, steps):
-    """Mixed form against plain FP64 from the same start: every derivative
-    field's error at t = 0, and the state and the last mid-point derivatives
-    after `steps` RK2 steps (field_errors); the per-step latency of both forms
-    over those steps (CUDA events around each step call, host read-back of dt
-    included); the total energy at the start and the end as compensated sums
-    (hi + lo, two-sum on the device) and the relative drift they give."""
+    """Mixed form against plain FP64 from the same start.  At t = 0, every
+    derivative field's error (field_errors).  Then both forms step together
+    for `steps` RK2 steps: the state and the last mid-point derivatives are
+    compared at the end, and the errors of velocity, energy and acceleration
+    at checkpoints along the way (error_growth), which separates the
+    arithmetic error of the first steps from the divergence of two particle
+    systems that start a rounding apart (SPH particle noise is chaotic: any
+    perturbation grows until it saturates).  Per-step latency of both forms
+    (CUDA events recorded just before and after each step call); the total
+    energy at the start and the end as compensated sums (hi + lo, two-sum on
+    the device) and the relative drift they give."""
     import torch
     abi = pkg.abi
     cf, cm = cfg.copy(), cfg.copy()
@@ -379,27 +401,41 @@ def measure_accuracy(pkg, ns, cfg, steps):
     out = {"field_error_vs_fp64_t0": errs0,
            "max_field_error_t0": max(v["max_rel"] for v in errs0.values()),
            "steps": steps}
+    box = [cfg.xmax[a] - cfg.xmin[a] for a in range(3)]
+    e0 = {"plain_fp64": energy(hf), "mixed": energy(hm)}
+    per = {"plain_fp64": [], "mixed": []}
+    growth = []
+    ev = {name: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for name in per}
+    streams = {"plain_fp64": torch.cuda.ExternalStream(hf.stream()), "mixed": torch.cuda.ExternalStream(hm.stream())}
+    for k in range(1, steps + 1):
+        for name, h in (("plain_fp64", hf), ("mixed", hm)):
+            a, b = ev[name]
+            a.record(streams[name])
+            h.step(1)
+            b.record(streams[name])
+            b.synchronize()
+            per[name].append(a.elapsed_time(b))
+        if k in GROWTH_STEPS:
+            g = {"step": k, "time": hf.time}
+            for f in GROWTH_FIELDS:
+                g[f] = field_errors(hm.field(f), hf.field(f))["max_rel"]
+            g["position"] = position_errors(hm.field("position"), hf.field("position"), box)["max_rel"]
+            growth.append(g)
     lat, eng = {}, {}
     for name, h in (("plain_fp64", hf), ("mixed", hm)):
-        e0 = energy(h)
-        stream = torch.cuda.ExternalStream(h.stream())
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
-        ev[0].record(stream)
-        for k in range(steps):
-            h.step(1)
-            ev[k + 1].record(stream)
-        h.synchronize()
-        torch.cuda.synchronize()
-        per = sorted(ev[k].elapsed_time(ev[k + 1]) for k in range(steps))
-        lat[name] = {"p50_ms": per[len(per) // 2], "p99_ms": per[min(len(per) - 1, int(round(0.99 * (len(per) - 1))))],
-                     "max_ms": per[-1], "samples": steps}
+        s = sorted(per[name])
+        lat[name] = {"p50_ms": s[len(s) // 2], "p99_ms": s[min(len(s) - 1, int(round(0.99 * (len(s) - 1))))],
+                     "max_ms": s[-1], "samples": len(s)}
         e1 = energy(h)
-        drift = ((e1[0] - e0[0]) + (e1[1] - e0[1])) / abs(e0[0])
-        eng[name] = {"e0": e0[0], "e0_lo": e0[1], "e1": e1[0], "e1_lo": e1[1], "relative_drift": drift,
-                     "abs_relative_drift": abs(drift)}
-    errs1 = {k: field_errors(hm.field(k), hf.field(k)) for k in STATE_FIELDS + ACCURACY_FIELDS}
+        drift = ((e1[0] - e0[name][0]) + (e1[1] - e0[name][1])) / abs(e0[name][0])
+        eng[name] = {"e0": e0[name][0], "e0_lo": e0[name][1], "e1": e1[0], "e1_lo": e1[1],
+                     "relative_drift": drift, "abs_relative_drift": abs(drift)}
+    errs1 = {k: field_errors(hm.field(k), hf.field(k)) for k in STATE_FIELDS[1:] + ACCURACY_FIELDS}
+    errs1["position"] = position_errors(hm.field("position"), hf.field("position"), box)
     out["field_error_vs_fp64_after_steps"] = errs1
     out["max_field_error_after_steps"] = max(v["max_rel"] for v in errs1.values())
+    out["error_growth"] = growth
     out["step_latency"] = lat
     out["energy"] = eng
     out["energy_drift"] = {k: v["abs_relative_drift"] for k, v in eng.items()}
