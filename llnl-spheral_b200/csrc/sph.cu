@@ -141,13 +141,31 @@ __global__ void __launch_bounds__(128, SPH_FP64_MIN_BLOCKS) sph_eval_fp64_kernel
   double* D = MB.D;
   double* pacc = MB.pacc;
   const int64_t ecap = MB.ecap;
+#if SPH_FP64_SHARED_I
+  // node i's record lives in shared memory: the pair loop reads its fields
+  // from there instead of holding 19 doubles in registers across the loop
+  __shared__ Rec sI[128];
+  sI[threadIdx.x] = loadRec(rec, i);
+  const Rec& I = sI[threadIdx.x];
+#else
   const Rec I = loadRec(rec, i);
+#endif
   const bool isoI = isoSym(I.H);
   double rhoSum = 0.0, norm = 0.0, wns = 0.0, maxvp = 0.0, effvp = 0.0, viscW = 0.0, DepsDt = 0.0;
   double XSPHw = 0.0;
   V3 DvDt{0.0, 0.0, 0.0}, XSPHdv{0.0, 0.0, 0.0};
   Sym m2{0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#if SPH_FP64_SHARED_ACC
+  // the two tensor sums (velocity gradient, M) accumulate in shared memory,
+  // [component][thread]: 18 doubles per thread out of the register file
+  __shared__ double sAcc[18][128];
+  double* accDvDx = &sAcc[0][threadIdx.x];
+  double* accM = &sAcc[9][threadIdx.x];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) { accDvDx[128*c] = 0.0; accM[128*c] = 0.0; }
+#else
   T9 DvDx{0, 0, 0, 0, 0, 0, 0, 0, 0}, M{0, 0, 0, 0, 0, 0, 0, 0, 0};
+#endif
   const double Cl = P.Cl*(0.5*(1.0 + 1.0)*1.0);   // Cl *= 0.5*(fCli + fClj)*fshear, multipliers 1
   const double Cq = P.Cq*(0.5*(1.0 + 1.0)*1.0);
   const int64_t k0 = offsets[i], k1 = offsets[i + 1];
@@ -155,106 +173,116 @@ __global__ void __launch_bounds__(128, SPH_FP64_MIN_BLOCKS) sph_eval_fp64_kernel
     const int32_t j = __ldg(nbr + k);
     const Rec J = loadRec(rec, j);
     const bool own = j > (int32_t)i;       // calculatePairInteraction: i is the owner
-    // owner side A, other side B
-    const V3 rA = selv(own, I.r, J.r), rB = selv(own, J.r, I.r);
-    const V3 vA = selv(own, I.v, J.v), vB = selv(own, J.v, I.v);
-    const Sym HA = sels(own, I.H, J.H), HB = sels(own, J.H, I.H);
-    const double HdetA = own ? I.Hdet : J.Hdet, HdetB = own ? J.Hdet : I.Hdet;
-    const double mA = own ? I.m : J.m, mB = own ? J.m : I.m;
-    const double rhoA = own ? I.rho : J.rho, rhoB = own ? J.rho : I.rho;
-    const double csA = own ? I.cs : J.cs, csB = own ? J.cs : I.cs;
-    const double mrhoA = own ? I.mrho : J.mrho, mrhoB = own ? J.mrho : I.mrho;
-
-    const V3 rij = vsub(rA, rB);
+    // The reference forms every pair term from the owner A and the other
+    // node B.  Here each quantity is formed once for node i and once for
+    // node j, with the same operands in the same order: with the
+    // owner-oriented separation r_ij = r_A - r_B (= r_i - r_j or its exact
+    // negation), eta_i = H_i r_ij is eta_A when i owns the pair and eta_B
+    // otherwise, and likewise for j.  Sums of two pair terms are commutative
+    // and keep their bits; where three or more are added the owner's order
+    // is selected explicitly.
+    const V3 d = vsub(I.r, J.r);
+    const V3 rij = own ? d : V3{-d.x, -d.y, -d.z};
+    const V3 dv = vsub(I.v, J.v);
+    const V3 vij = own ? dv : V3{-dv.x, -dv.y, -dv.z};
     // H = h I (the common case): every H product reduces to a scaling with
     // the same bits (the off-diagonal terms add exact zeros)
     const bool iso = isoI && isoSym(J.H);
-    const V3 etaA = iso ? vmul(rij, HA.xx) : sdot(HA, rij);
-    const V3 etaB = iso ? vmul(rij, HB.xx) : sdot(HB, rij);
-    const double etaMagA = mag(etaA);
-    const double etaMagB = mag(etaB);
-    const V3 HetaA = iso ? vmul(unitVector(etaA), HA.xx) : sdot(HA, unitVector(etaA));
-    const V3 HetaB = iso ? vmul(unitVector(etaB), HB.xx) : sdot(HB, unitVector(etaB));
-    double WA, gWA, WB, gWB;
-    tableKernelAndGrad(P.W, etaMagA, HdetA, WA, gWA);
-    tableKernelAndGrad(P.W, etaMagB, HdetB, WB, gWB);
-    const V3 gradWA = vmul(HetaA, gWA);
-    const V3 gradWB = vmul(HetaB, gWB);
-    // node i's side of the symmetric quantities
-    const double Wi = own ? WA : WB;
-    const double gWi = own ? gWA : gWB;
-    const V3 gradWi = selv(own, gradWA, gradWB);
+    const V3 etaI = iso ? vmul(rij, I.H.xx) : sdot(I.H, rij);
+    const V3 etaJ = iso ? vmul(rij, J.H.xx) : sdot(J.H, rij);
+    const V3 uI = unitVector(etaI), uJ = unitVector(etaJ);
+    const V3 HetaI = iso ? vmul(uI, I.H.xx) : sdot(I.H, uI);
+    const V3 HetaJ = iso ? vmul(uJ, J.H.xx) : sdot(J.H, uJ);
+    double WI, gWI, WJ, gWJ;
+    tableKernelAndGrad(P.W, mag(etaI), I.Hdet, WI, gWI);
+    tableKernelAndGrad(P.W, mag(etaJ), J.Hdet, WJ, gWJ);
+    const V3 gradWI = vmul(HetaI, gWI);    // node i's side of the pair
+    const V3 gradWJ = vmul(HetaJ, gWJ);
 
     // moments for the ideal H
     const double rij2 = mag2(rij);
     const double thptS = safeInvVar(rij2*rij2*rij2);
-    wns += 1.0*fabs(gWi);
+    wns += 1.0*fabs(gWI);
     {
-      const double g2 = 1.0*mag2(gradWi);
+      const double g2 = 1.0*mag2(gradWI);
       const Sym thpt = smul(selfdyad(rij), thptS);
       m2 = sadd(m2, smul(thpt, g2));
     }
     // sum density / normalization (single NodeList)
-    rhoSum += (own ? mB : mA)*Wi;
-    norm += (own ? mrhoA : mrhoB)*Wi;
+    rhoSum += J.m*WI;
+    norm += I.mrho*WI;
 
     // Monaghan-Gingold Pi_ij
-    const V3 vij = vsub(vA, vB);
-    const double muA = dot(vij, etaA)/(mag2(etaA) + P.eps2);
-    const double muB = dot(vij, etaB)/(mag2(etaB) + P.eps2);
-    const double mA0 = dmin(0.0, muA), mB0 = dmin(0.0, muB);
-    const double eA = -Cl*csA*(P.linearInExp ? muA : mA0) + Cq*(P.quadInExp ? -sgn(muA)*muA*muA : mA0*mA0);
-    const double eB = -Cl*csB*(P.linearInExp ? muB : mB0) + Cq*(P.quadInExp ? -sgn(muB)*muB*muB : mB0*mB0);
-    const double qA = eA/rhoA, qB = eB/rhoB;   // (e/rho) * Tensor::one
+    const double muI = dot(vij, etaI)/(mag2(etaI) + P.eps2);
+    const double muJ = dot(vij, etaJ)/(mag2(etaJ) + P.eps2);
+    const double mI0 = dmin(0.0, muI), mJ0 = dmin(0.0, muJ);
+    const double eI = -Cl*I.cs*(P.linearInExp ? muI : mI0) + Cq*(P.quadInExp ? -sgn(muI)*muI*muI : mI0*mI0);
+    const double eJ = -Cl*J.cs*(P.linearInExp ? muJ : mJ0) + Cq*(P.quadInExp ? -sgn(muJ)*muJ*muJ : mJ0*mJ0);
+    const double qI = eI/I.rho, qJ = eJ/J.rho;   // (e/rho) * Tensor::one
     // 0.5*(Pi * gradWQ), with WQ = W (same table): the off-diagonal zeros of
     // Pi only add signed zeros.
-    const V3 QaccA = vmul(vmul(gradWA, qA), 0.5);
-    const V3 QaccB = vmul(vmul(gradWB, qB), 0.5);
-    const double workQA = dot(vij, QaccA);
-    const double workQB = dot(vij, QaccB);
-    const double QA = rhoA*rhoA*fabs(qA);
-    const double QB = rhoB*rhoB*fabs(qB);
-    const double Qi = own ? QA : QB;
-    maxvp = dmax(maxvp, Qi);
-    effvp += (own ? mrhoB : mrhoA)*Qi*Wi;
-    viscW += (own ? mB : mA)*(own ? workQA : workQB);
+    const V3 QaccI = vmul(vmul(gradWI, qI), 0.5);
+    const V3 QaccJ = vmul(vmul(gradWJ, qJ), 0.5);
+    const double workQI = dot(vij, QaccI);
+    const double QI = I.rho*I.rho*fabs(qI);
+    maxvp = dmax(maxvp, QI);
+    effvp += J.mrho*QI*WI;
+    viscW += J.m*workQI;
 
     // pressure terms (tensile correction uses the owner's W)
-    double PrhoA, PrhoB;
+    double PrhoI, PrhoJ;
     if (TENSILE) {
-      const double PA = own ? I.P : J.P, PB = own ? J.P : I.P;
-      const double sOA = own ? I.somega : J.somega, sOB = own ? J.somega : I.somega;
-      const double x = WA/(HdetA*P.WnPerh);
+      const double x = own ? WI/(I.Hdet*P.WnPerh) : WJ/(J.Hdet*P.WnPerh);
       const double fij = P.epsTensile*(x*x*x*x);
-      const double RA = fij*(PA < 0.0 ? -PA : 0.0);
-      const double RB = fij*(PB < 0.0 ? -PB : 0.0);
-      PrhoA = sOA*(PA + RA)/(rhoA*rhoA);
-      PrhoB = sOB*(PB + RB)/(rhoB*rhoB);
+      const double RI = fij*(I.P < 0.0 ? -I.P : 0.0);
+      const double RJ = fij*(J.P < 0.0 ? -J.P : 0.0);
+      PrhoI = I.somega*(I.P + RI)/(I.rho*I.rho);
+      PrhoJ = J.somega*(J.P + RJ)/(J.rho*J.rho);
     } else {
-      PrhoA = own ? I.Prho : J.Prho;
-      PrhoB = own ? J.Prho : I.Prho;
+      PrhoI = I.Prho;
+      PrhoJ = J.Prho;
     }
-    const V3 deltaDvDt = vadd(vadd(vadd(vmul(gradWA, PrhoA), vmul(gradWB, PrhoB)), QaccA), QaccB);
-    DvDt = vadd(DvDt, vmul(deltaDvDt, own ? -mB : mA));
-    const double Prhoi = own ? PrhoA : PrhoB;
-    const double workQi = own ? workQA : workQB;
-    DepsDt += (own ? mB : mA)*(Prhoi*dot(vij, gradWi) + workQi);
+    // ((gradW_A P_A + gradW_B P_B) + Qacc_A) + Qacc_B
+    const V3 pp = vadd(vmul(gradWI, PrhoI), vmul(gradWJ, PrhoJ));
+    const V3 deltaDvDt = vadd(vadd(pp, own ? QaccI : QaccJ), own ? QaccJ : QaccI);
+    DvDt = vadd(DvDt, vmul(deltaDvDt, own ? -J.m : J.m));
+    DepsDt += J.m*(PrhoI*dot(vij, gradWI) + workQI);
     if (COMPAT) {
       // the owner's pair acceleration, -m_other*deltaDvDt
-      const V3 pa = vmul(deltaDvDt, -mB);
+      const V3 pa = vmul(deltaDvDt, own ? -J.m : -I.m);
       pacc[k] = pa.x;
       pacc[ecap + k] = pa.y;
       pacc[2*ecap + k] = pa.z;
     }
-    const double mo = own ? mB : mA;      // the other node's mass
-    tsubfrom(DvDx, tmul(dyad(vij, gradWi), mo));
-    if (XSPH) {
-      const double w = 0.5*(mrhoA*WA + mrhoB*WB);
-      XSPHw += w;
-      const V3 dv = vmul(vij, w);
-      XSPHdv = own ? vsub(XSPHdv, dv) : vadd(XSPHdv, dv);
+#if SPH_FP64_SHARED_ACC
+    {
+      // DvDx -= (vij gradW_i) m_j, element by element as tsubfrom(tmul(dyad))
+      const double va[3] = {vij.x, vij.y, vij.z}, ga[3] = {gradWI.x, gradWI.y, gradWI.z};
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) accDvDx[128*(3*r + c)] = accDvDx[128*(3*r + c)] - (va[r]*ga[c])*J.m;
     }
-    tsubfrom(M, tmul(dyad(rij, gradWi), mo));
+#else
+    tsubfrom(DvDx, tmul(dyad(vij, gradWI), J.m));
+#endif
+    if (XSPH) {
+      const double w = 0.5*(I.mrho*WI + J.mrho*WJ);
+      XSPHw += w;
+      const V3 dvw = vmul(vij, w);
+      XSPHdv = own ? vsub(XSPHdv, dvw) : vadd(XSPHdv, dvw);
+    }
+#if SPH_FP64_SHARED_ACC
+    {
+      const double ra[3] = {rij.x, rij.y, rij.z}, ga[3] = {gradWI.x, gradWI.y, gradWI.z};
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) accM[128*(3*r + c)] = accM[128*(3*r + c)] - (ra[r]*ga[c])*J.m;
+    }
+#else
+    tsubfrom(M, tmul(dyad(rij, gradWI), J.m));
+#endif
   }
 
   // ---- per-node finish (src/SPH/SPHHydroBase.cc:834-902)
@@ -262,7 +290,17 @@ __global__ void __launch_bounds__(128, SPH_FP64_MIN_BLOCKS) sph_eval_fp64_kernel
   const int numNeighbors = (int)(k1 - k0);
   rhoSum += mi*P.W0*Hdeti;
   norm += mi/rhoi*P.W0*Hdeti;
+#if SPH_FP64_SHARED_ACC
+  T9 Mi, DvDxi;
+  {
+    double* mi9 = &Mi.xx;
+    double* dv9 = &DvDxi.xx;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) { mi9[c] = accM[128*c]; dv9[c] = accDvDx[128*c]; }
+  }
+#else
   T9 Mi = M, DvDxi = DvDx;
+#endif
   if (P.correctVelGrad && fabs(tdet(Mi)) > 1.0e-10 && numNeighbors > 8) {
     Mi = tinverse(Mi);
     DvDxi = tdot(DvDxi, Mi);
