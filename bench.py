@@ -45,13 +45,14 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 METRIC = "pair-interactions/s"
 WORKLOAD = ("Kelvin-Helmholtz 3-D periodic unit cube, 128^3 = 2,097,152 nodes, Wendland C4 "
             "TableKernel(1000), nPerh 1.35, MonaghanGingold Cl=Cq=1, compatible energy, "
-            "RigorousSumDensity, IdealH, Courant dt (cfl 0.25); one CheapSynchronousRK2 step per step")
+            "RigorousSumDensity, IdealH, Courant dt (cfl 0.25); H relaxed to the ideal smoothing scale at "
+            "start-up (iterateIdealH, untimed); one CheapSynchronousRK2 step per step")
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nx", type=int, default=128, help="lattice size per axis (default: the full workload)")
@@ -103,6 +104,22 @@ def kh_problem(pkg, nx, nz=None, seed=20261203):
     ns = gen.kelvin_helmholtz(nx=nx, ny=nx, nz=nz, box=((0, 0, 0), (1.0, 1.0, nz / nx)), seed=seed)
     cfg = gen.kh_config(abi, xmax=(1.0, 1.0, nz / nx))
     return ns, cfg
+
+
+# The controller's start-up relaxes H to the ideal smoothing scale before the
+# run (SpheralController's iterateInitialH, on by default): maximum
+# iterations and tolerance of that iterateIdealH.
+IDEAL_H = (50, 1.0e-4)
+
+
+def relax_h(pkg, ns, cfg):
+    """ns.H relaxed to the ideal smoothing scale on the device
+    (sphgpu_iterate_ideal_h), as the reference's start-up does; untimed set-up."""
+    h = pkg.SPHHydro(cfg, ns)
+    h.iterateIdealH(*IDEAL_H)
+    ns.H = np.ascontiguousarray(h.field("H"))
+    h.close()
+    return ns
 
 
 def load_peaks():
@@ -215,11 +232,15 @@ def barrier(world):
         dist.barrier()
 
 
-def measure_steps(pkg, ns, cfg, precision, steps, warmup, world, clocks=None):
+def measure_steps(pkg, ns, cfg, precision, steps, warmup, world, clocks=None, graph=True):
+    """K RK2 steps, one sphgpu_step_rk2 call per step, with CUDA events
+    around each step (per-step latency); `graph`: each call one replay of the
+    captured whole-step graph (the default schedule), else eager launches."""
     import torch
     c = cfg.copy()
     c.precision = precision
     h = pkg.SPHHydro(c, ns)
+    h.set_schedule("step graph", 1 if graph else 0)
     h.build_neighbors()
     h.evaluateDerivatives()          # derivatives at t = 0 feed the first predictor
     stream = torch.cuda.ExternalStream(h.stream())
@@ -246,6 +267,40 @@ def measure_steps(pkg, ns, cfg, precision, steps, warmup, world, clocks=None):
     per = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
     total_ms = ev[0].elapsed_time(ev[steps])
     return h, {"total_ms": total_ms, "per_step_ms": per, "pairs": pairs, "launches": launches, "clocks": clk}
+
+
+def measure_steps_graph(pkg, ns, cfg, precision, steps, warmup, world, clocks=None):
+    """K RK2 steps in ONE sphgpu_step_rk2 call with the "step graph" schedule:
+    the whole step (rebuild included) is a captured CUDA graph replayed K
+    times with no host round trip; pairs from the device-side pair counter."""
+    import torch
+    c = cfg.copy()
+    c.precision = precision
+    h = pkg.SPHHydro(c, ns)
+    h.set_schedule("step graph", 1)
+    h.build_neighbors()
+    h.evaluateDerivatives()
+    stream = torch.cuda.ExternalStream(h.stream())
+    for _ in range(max(warmup, 3)):      # eager step, capture + replay, replay
+        h.step(1)
+    h.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    p0 = h.pairs_evaluated()
+    l0 = h.kernel_launches()
+    if clocks:
+        clocks.start()
+    a.record(stream)
+    h.step(steps)
+    b.record(stream)
+    h.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop() if clocks else None
+    barrier(world)
+    return h, {"total_ms": a.elapsed_time(b), "pairs": h.pairs_evaluated() - p0,
+               "launches": h.kernel_launches() - l0, "clocks": clk}
 
 
 def measure_eval(h, reps=10):
@@ -502,6 +557,7 @@ def measure_config_crk(pkg, steps, warmup, drift_steps):
     mixed form, step rate and energy drift over `drift_steps` steps."""
     gen, abi = pkg.generators, pkg.abi
     ns = gen.kelvin_helmholtz(nx=128, ny=128, nz=64, box=((0, 0, 0), (1.0, 1.0, 1.0)))
+    relax_h(pkg, ns, gen.kh_config(abi))
     out = {}
     for name, prec in (("plain_fp64", abi.PRECISION_FP64), ("mixed", abi.PRECISION_MIXED)):
         cfg = gen.kh_config(abi, hydro=abi.HYDRO_CRKSPH, precision=prec)
@@ -546,9 +602,10 @@ def batch_specs(pkg, count, precision, seed=20261203, nmin=4096, nmax=262144):
 
 
 def time_batch(pkg, probs, steps, warmup, world, graph):
-    """Batched steps of `probs` (autotuned schedules; the RK2 step after the
-    rebuild replayed as a CUDA graph when `graph`), timed with CUDA events on
-    the batch stream, max over ranks."""
+    """K batched steps of `probs` in one call (autotuned schedules; the whole
+    RK2 step replayed as a captured CUDA graph when `graph`, eager launches
+    otherwise), timed with CUDA events on the batch stream, max over ranks;
+    pairs from the device-side pair counter."""
     import torch
     batch = pkg.SPHBatch(probs)
     batch.build_neighbors()
@@ -562,16 +619,14 @@ def time_batch(pkg, probs, steps, warmup, world, graph):
     barrier(world)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     l0 = batch.kernel_launches()
+    p0 = batch.pairs_evaluated()
     e0.record(stream)
-    pairs = 0
-    for _ in range(steps):
-        batch.step(1)
-        pairs += batch.num_pairs()
+    batch.step(steps)
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
     t = allmax(e0.elapsed_time(e1) / 1e3, world)
-    pairs = allsum(pairs, world)
+    pairs = allsum(batch.pairs_evaluated() - p0, world)
     launches = batch.kernel_launches() - l0
     batch.close()
     return {"value": pairs / t, "unit": METRIC, "ms_per_step": 1e3 * t / steps,
@@ -583,7 +638,7 @@ def time_batch(pkg, probs, steps, warmup, world, graph):
 
 def measure_batch(pkg, count, steps, warmup, rank=0, world=1):
     """Batched ensemble, mixed form: every stage one launch over all members,
-    the RK2 step after the ghost/connectivity rebuild replayed as a CUDA graph;
+    the whole RK2 step replayed as a captured CUDA graph;
     against the same batch in plain FP64, and against the mixed problems
     stepped one at a time (one launch sequence per problem).  With N GPUs the
     tubes are placed by size (longest first onto the least-loaded rank; no
@@ -697,11 +752,13 @@ def write_reference_input(path, cfg, ns, nsteps):
 def time_reference(cfg, ns, steps, warmup):
     """The reference's own SPHHydroBase + CheapSynchronousRK2 (compiled from
     its sources into oracle/_ref/ref_sph): seconds and pair interactions of
-    `steps` timed RK2 steps after `warmup` untimed ones, one core."""
+    `steps` timed RK2 steps after `warmup` untimed ones, one core; H relaxed
+    by the reference's own iterateIdealH first (untimed)."""
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "in.bin")
         write_reference_input(path, cfg, ns, steps)
-        out = subprocess.check_output([REF_SPH, "--time", str(warmup), path]).decode()
+        out = subprocess.check_output([REF_SPH, "--time", str(warmup), path,
+                                       str(IDEAL_H[0]), repr(IDEAL_H[1])]).decode()
     r = json.loads(out.strip().splitlines()[-1])
     return r["seconds"], r["pairs"]
 
@@ -720,6 +777,7 @@ def cpu_baseline(pkg, nx):
     else:
         import oracle
         o = oracle.OracleProblem(cfg, ns)
+        o.iterate_ideal_h(*IDEAL_H)
         o.build_neighbors()
         o.evaluate_derivatives()
         o.step(1)
@@ -751,6 +809,7 @@ def _ref_worker(args):
     else:
         import oracle
         o = oracle.OracleProblem(cfg, ns)
+        o.iterate_ideal_h(*IDEAL_H)
         o.build_neighbors()
         o.evaluate_derivatives()
         for _ in range(warmup):
@@ -779,7 +838,8 @@ def run_reference(args):
     nx = args.nx
     # bounded sample per process: a z-slab of the same lattice (same dx, same
     # stencil); thinner when many steps are asked for
-    nz = max(4, nx // 8 if args.steps + args.warmup <= 16 else nx // 16)
+    total = args.steps + args.warmup
+    nz = max(4, nx // 8 if total <= 16 else nx // 16 if total <= 64 else nx // 32)
     ctx = mp.get_context("spawn")
     bar = ctx.Barrier(cores)
     q = ctx.Queue()
@@ -823,18 +883,37 @@ def run_ours(args):
     importlib.import_module("llnl-spheral_b200.build").build()
     abi = pkg.abi
     ns, cfg = kh_problem(pkg, args.nx, seed=20261203 + rank)
+    relax_h(pkg, ns, cfg)
     vis = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
     clocks = Clocks(vis[local] if local < len(vis) else local)
-    # headline: plain FP64, the reference's precision
-    hp, rp = measure_steps(pkg, ns, cfg, abi.PRECISION_FP64, args.steps, args.warmup, world, clocks)
+    # headline: plain FP64, the reference's precision; K steps in one
+    # sphgpu_step_rk2 call (the captured whole-step graph replayed K times)
+    hg, rp = measure_steps_graph(pkg, ns, cfg, abi.PRECISION_FP64, args.steps, args.warmup, world, clocks)
+    hg.close()
     t_plain = allmax(rp["total_ms"], world)
     pairs_plain = allsum(rp["pairs"], world)
     # the mixed FP32-pair form on the same workload
-    hm, rm = measure_steps(pkg, ns, cfg, abi.PRECISION_MIXED, args.steps, args.warmup, world)
+    hg, rm = measure_steps_graph(pkg, ns, cfg, abi.PRECISION_MIXED, args.steps, args.warmup, world)
+    hg.close()
+    del hg
     t_mixed = allmax(rm["total_ms"], world)
     pairs_mixed = allsum(rm["pairs"], world)
     value = pairs_plain / (t_plain / 1e3)
     mixed_value = pairs_mixed / (t_mixed / 1e3)
+    # one call per step (per-step latency), graph replays and eager launches
+    hp, lp = measure_steps(pkg, ns, cfg, abi.PRECISION_FP64, args.steps, args.warmup, world)
+    hm, lm = measure_steps(pkg, ns, cfg, abi.PRECISION_MIXED, args.steps, args.warmup, world)
+    per_call = {}
+    for form, prec, r in (("fp64", abi.PRECISION_FP64, lp), ("mixed", abi.PRECISION_MIXED, lm)):
+        he, re_ = measure_steps(pkg, ns, cfg, prec, args.steps, args.warmup, world, graph=False)
+        he.close()
+        del he
+        tl = allmax(r["total_ms"], world)
+        te = allmax(re_["total_ms"], world)
+        per_call[form] = {"graph_replay": {"value": allsum(r["pairs"], world) / (tl / 1e3),
+                                           "ms_per_step": tl / args.steps},
+                          "eager": {"value": allsum(re_["pairs"], world) / (te / 1e3),
+                                    "ms_per_step": te / args.steps, "gpu_launches": re_["launches"]}}
     # roofline of the dominant kernel pair of the step (evaluateDerivatives:
     # record pack + pair kernel), each form
     peak, peak_kind = load_peaks()
@@ -870,22 +949,26 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": t_plain / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": bench_config(args.nx),
+            "timing": "K steps in one sphgpu_step_rk2 call (whole-step CUDA graph replayed K times, no "
+                      "host synchronisation between steps), CUDA events on the problem's stream",
             "problem": {"nodes_per_gpu": nodes, "ghosts": ghosts, "pairs_per_step": rp["pairs"] / args.steps,
                         "parallelism": "one independent problem per GPU" if world > 1 else "single GPU",
                         "l2": "inputs larger than L2 (state %.2f GB, pair records %.2f GB)" % (
                             nodes * 18 * 8 / 1e9, (nodes + ghosts) * 160 / 1e9)},
-            "latency_ms": {"p50": pct(rp["per_step_ms"], 0.5), "p99": pct(rp["per_step_ms"], 0.99)},
+            "latency_ms": {"p50": pct(lp["per_step_ms"], 0.5), "p99": pct(lp["per_step_ms"], 0.99),
+                           "of": "one sphgpu_step_rk2 call per step"},
             "stage_ms": {"neighbor_build": t_build_plain, "evaluate_derivatives": t_eval_plain,
                          "rk2_step": t_plain / args.steps},
             "mixed": {"value": mixed_value, "unit": METRIC, "ms_per_step": t_mixed / args.steps,
                       "dtype": "f32 pair / f64 state",
-                      "latency_ms": {"p50": pct(rm["per_step_ms"], 0.5), "p99": pct(rm["per_step_ms"], 0.99)},
+                      "latency_ms": {"p50": pct(lm["per_step_ms"], 0.5), "p99": pct(lm["per_step_ms"], 0.99)},
                       "stage_ms": {"neighbor_build": t_build_mixed, "evaluate_derivatives": t_eval_mixed,
                                    "rk2_step": t_mixed / args.steps},
                       "roofline": roofline("mixed", eval_alg_bytes_mixed(nodes, ghosts, entries), t_eval_mixed,
                                            "evaluateDerivatives (pack_mixed + sph_eval_mixed)"),
                       "gpu_launches": rm["launches"]},
             "mixed_over_plain": mixed_value / value,
+            "one_call_per_step": per_call,
             "roofline": roofline("fp64", eval_alg_bytes_fp64(nodes, ghosts, entries), t_eval_plain,
                                  "evaluateDerivatives (pack_records + sph_eval_fp64)"),
             "gpu_launches": rp["launches"],

@@ -222,6 +222,10 @@ int sphgpu_conservation_noalloc(const double* mass, const double* velocity,
 /* Pair interactions (the reference's ncalc summed over nodes,
  * src/SPH/SPHHydroBase.cc:674) of the current connectivity. */
 int sphgpu_num_pairs(sphgpu_problem* p, int64_t* pairs);
+/* sphgpu_num_pairs of each RK2 step's connectivity, summed over the steps
+ * taken so far (counted on the device, so it stays exact when many steps run
+ * in one call). */
+int sphgpu_pairs_evaluated(sphgpu_problem* p, int64_t* pairs);
 /* Number of CUDA kernels this problem has launched so far (diagnostics; the
  * reference's per-node "work" timing field, src/SPH/SPHHydroBase.cc:598,905-925,
  * has no device counterpart). */
@@ -235,11 +239,16 @@ int sphgpu_kernel_launches(sphgpu_problem* p, int64_t* launches);
  * clearly inside or outside the kernel support and the exact FP64 test the
  * rest (used only while every H has condition number <= 100, where the FP32
  * error is far inside the band, so the ConnectivityMap is unchanged); 0 = the
- * FP64 test for every candidate.  stage "step graph": 1 = the part of each
- * RK2 step after the ghost/connectivity rebuild (records, dt, updates,
- * derivatives, compatible energy, sum density, boundaries) is captured once
- * as a CUDA graph and replayed every step (re-captured when a buffer moves);
- * 0 = eager launches.  stage "neighbor passes": 1 (default) = the counting
+ * FP64 test for every candidate.  stage "step graph": 1 (default) = a whole RK2 step
+ * (ghost and connectivity rebuild, records, dt, updates, derivatives,
+ * compatible energy, sum density, boundaries) is captured once as a CUDA
+ * graph and sphgpu_step_rk2(p, n) replays it n times with no host round trip
+ * between steps; the rebuild's capacities are checked on the device and a
+ * conditional node skips the rest of the step when one overflows, after
+ * which the library grows the buffer, takes that step eagerly and captures
+ * again.  The graph is captured the second time a buffer layout recurs (a
+ * first step of a new layout runs eagerly).  Results are bit-identical to
+ * eager launches.  0 = eager launches.  stage "neighbor passes": 1 (default) = the counting
  * walk also builds each node's sorted list and parks it in the
  * pair-acceleration buffer (free until the next derivative evaluation), and
  * a compaction moves the lists into the ConnectivityMap, so the candidates
@@ -284,6 +293,8 @@ int sphgpu_batch_evaluate_derivatives(sphgpu_batch* b);
 int sphgpu_batch_step_rk2(sphgpu_batch* b, int64_t nsteps);
 /* Pair interactions of the members' current connectivity, summed. */
 int sphgpu_batch_pairs(sphgpu_batch* b, int64_t* pairs);
+/* sphgpu_pairs_evaluated summed over the members. */
+int sphgpu_batch_pairs_evaluated(sphgpu_batch* b, int64_t* pairs);
 int sphgpu_batch_kernel_launches(sphgpu_batch* b, int64_t* launches);
 /* Schedule for all members that have not set their own (see sphgpu_set_schedule). */
 int sphgpu_batch_set_schedule(sphgpu_batch* b, const char* stage, int32_t schedule);

@@ -162,6 +162,7 @@ def load_library(path=None):
     lib.sphgpu_checkpoint_save.argtypes = [P, P, I64]
     lib.sphgpu_checkpoint_load.argtypes = [P, P, I64]
     lib.sphgpu_num_pairs.argtypes = [P, ctypes.POINTER(I64)]
+    lib.sphgpu_pairs_evaluated.argtypes = [P, ctypes.POINTER(I64)]
     lib.sphgpu_kernel_launches.argtypes = [P, ctypes.POINTER(I64)]
     lib.sphgpu_time.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     lib.sphgpu_batch_create.argtypes = [P, ctypes.c_int32, ctypes.POINTER(P)]
@@ -172,6 +173,7 @@ def load_library(path=None):
     lib.sphgpu_batch_evaluate_derivatives.argtypes = [P]
     lib.sphgpu_batch_step_rk2.argtypes = [P, I64]
     lib.sphgpu_batch_pairs.argtypes = [P, ctypes.POINTER(I64)]
+    lib.sphgpu_batch_pairs_evaluated.argtypes = [P, ctypes.POINTER(I64)]
     lib.sphgpu_batch_kernel_launches.argtypes = [P, ctypes.POINTER(I64)]
     lib.sphgpu_batch_set_schedule.argtypes = [P, ctypes.c_char_p, ctypes.c_int32]
     lib.sphgpu_batch_get_stream.argtypes = [P, ctypes.POINTER(P)]

@@ -397,10 +397,16 @@ uint64_t graph_key(const Batch& b) {
   mix(b.mem.size());
   mix((uint64_t)b.evalThreads);
   for (const Problem* p : b.mem) {
-    const void* ptrs[] = {p->S, p->S0, p->D, p->K, p->rec, p->crec, p->mrec, p->groot, p->gcode, p->counts,
-                          p->offsets, p->nbr, p->pacc, p->d_scal, p->d_red, p->d_err, p->coefF, p};
+    const void* ptrs[] = {p->S, p->S0, p->D, p->K, p->qgrad, p->rec, p->crec, p->mrec, p->groot, p->gcode,
+                          p->gpos, p->cand, p->cidx, p->sortedIdx, p->cellStart, p->cellFill, p->counts,
+                          p->offsets, p->nbr, p->pacc, p->tableCoef, p->coefF, p->blockSums, p->d_scal,
+                          p->d_red, p->d_err, p->hmaxi, p};
     for (const void* q : ptrs) mix((uint64_t)(uintptr_t)q);
-    mix((uint64_t)p->n); mix((uint64_t)p->gcap); mix((uint64_t)p->ecap); mix((uint64_t)p->candcap);
+    // sizes and plans that set launch shapes, kernel variants and shared memory
+    const int64_t sizes[] = {p->n, p->gcap, p->ecap, p->candcap, p->cellcap, p->reccap, p->creccap,
+                             p->mreccap, p->blockSumsCap, p->redcap, p->maxNbr, p->fillCap, p->fillSchedule,
+                             p->grid.sub, p->grid.stashCap, p->grid.stashStride};
+    for (int64_t v : sizes) mix((uint64_t)v);
   }
   return h;
 }
@@ -439,50 +445,149 @@ int upload_graph_descriptors(Batch& b) {
   return SPHGPU_OK;
 }
 
-int capture_step(Batch& b) {
+// Capture of one whole RK2 step, rebuild included, as a CUDA graph:
+//   [open] -> IF(no error so far) { ghosts + ConnectivityMap launches }
+//   -> [gate] -> IF(no error) { dt vote, mid-point update, records,
+//   initialize, derivatives, full update with the compatible energy,
+//   finalize, boundaries, step bookkeeping }
+// The build is sized on the device and checks its capacities there; the gate
+// turns the rest of the step off (a conditional graph node) when a capacity
+// overflowed, so the state is left as it was, and the open kernel of every
+// later replay of the same call turns that replay off, rebuild included.  The
+// host redoes the overflowing step eagerly, with grown buffers, after the
+// call's one read-back.  Any other error bit (set by a build or by a step)
+// stops the replays the same way, and the call reports it.
+__global__ void step_gate_kernel(const Member* mem, int nmem, cudaGraphConditionalHandle handle) {
+  int bad = 0;
+  for (int m = threadIdx.x; m < nmem; m += blockDim.x) bad |= *mem[m].err != 0;
+  bad = __syncthreads_or(bad);
+  if (threadIdx.x == 0) cudaGraphSetConditional(handle, bad ? 0u : 1u);
+}
+
+// Per member: the device time from the host's, the step and pair counters zeroed.
+__global__ void step_counters_kernel(const Member* mem, int nmem, const double* times) {
+  const int m = blockIdx.x*blockDim.x + threadIdx.x;
+  if (m >= nmem) return;
+  double* s = mem[m].scal;
+  s[SC_TIME] = times[m];
+  reinterpret_cast<int64_t*>(s)[SC_STEPS] = 0;
+  reinterpret_cast<int64_t*>(s)[SC_PAIRSUM] = 0;
+}
+
+namespace {
+// Nodes of `g` with no dependents.
+int graph_leaves(cudaGraph_t g, std::vector<cudaGraphNode_t>& leaves) {
+  size_t nnodes = 0;
+  SPH_CHECK(cudaGraphGetNodes(g, nullptr, &nnodes));
+  std::vector<cudaGraphNode_t> nodes(nnodes);
+  SPH_CHECK(cudaGraphGetNodes(g, nodes.data(), &nnodes));
+  leaves.clear();
+  for (cudaGraphNode_t nd : nodes) {
+    size_t nout = 0;
+    SPH_CHECK(cudaGraphNodeGetDependentNodes(nd, nullptr, &nout));
+    if (nout == 0) leaves.push_back(nd);
+  }
+  return SPHGPU_OK;
+}
+
+// An IF node on `handle` after every leaf of `g`; its body graph in *body.
+int add_if_node(cudaGraph_t g, cudaGraphConditionalHandle handle, cudaGraphNode_t* node, cudaGraph_t* body) {
+  std::vector<cudaGraphNode_t> leaves;
+  SPH_TRY(graph_leaves(g, leaves));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  SPH_CHECK(cudaGraphAddNode(node, g, leaves.data(), leaves.size(), &cp));
+  *body = cp.conditional.phGraph_out[0];
+  return SPHGPU_OK;
+}
+
+// Launches of `fn` captured into `g` (after `dep` when given).
+template <class F>
+int capture_into(Batch& b, cudaGraph_t g, const cudaGraphNode_t* dep, F&& fn, const char* what) {
+  cudaError_t e = cudaStreamBeginCaptureToGraph(b.stream, g, dep, nullptr, dep ? 1 : 0,
+                                                cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) return cuda_status(e, what);
+  const int rc = fn();
+  cudaGraph_t captured = nullptr;
+  e = cudaStreamEndCapture(b.stream, &captured);
+  if (rc != SPHGPU_OK) return rc;
+  return e == cudaSuccess ? SPHGPU_OK : cuda_status(e, what);
+}
+}  // namespace
+
+int capture_full_step(Batch& b) {
   if (b.graphExec) { cudaGraphExecDestroy(b.graphExec); b.graphExec = nullptr; }
+  // everything the replay touches must exist before the capture
+  if (anyMember(b, isCrkP)) SPH_TRY(crk_prepare(b));
+  if (anyMember(b, isMixedSph) || anyMember(b, isMixedCrk)) SPH_TRY(prepare_mixed(b));
+  SPH_TRY(plan_build(b));
+  SPH_TRY(enable_graph(b));
+  SPH_TRY(upload_graph_descriptors(b));
   b.mapArenaPos = 0;
   const int64_t l0 = b.launches;
   std::vector<int64_t> m0;
   for (Problem* p : b.mem) m0.push_back(p->launches);
-  SPH_CHECK(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeRelaxed));
+  cudaGraph_t graph = nullptr;
+  SPH_CHECK(cudaGraphCreate(&graph, 0));
+  cudaGraphConditionalHandle hBuild, hStep;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&hBuild, graph, 0u, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hStep, graph, 0u, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) { cudaGraphDestroy(graph); return cuda_status(e, "graph conditional handle"); }
+  const int nm = (int)b.mem.size();
+  int rc = SPHGPU_OK;
   b.capturing = true;
   b.capacityGrids = true;
-  const int rc = step_after_connectivity(b);
+  do {
+    // the open kernel: no error left by an earlier replay of this call
+    rc = capture_into(b, graph, nullptr, [&]() {
+      step_gate_kernel<<<1, 128, 0, b.stream>>>(b.d_mem, nm, hBuild);
+      batch_count_launch(b);
+      return cuda_status(cudaGetLastError(), "step open");
+    }, "graph capture (open)");
+    if (rc != SPHGPU_OK) break;
+    cudaGraphNode_t ifBuild, ifStep;
+    cudaGraph_t buildBody, stepBody;
+    if ((rc = add_if_node(graph, hBuild, &ifBuild, &buildBody)) != SPHGPU_OK) break;
+    // the rebuild, in the first conditional's body
+    const int64_t lb = b.launches;
+    rc = capture_into(b, buildBody, nullptr, [&]() { return launch_build_captured(b); }, "graph capture (build)");
+    if (rc != SPHGPU_OK) break;
+    b.graphBuildLaunches = b.launches - lb;
+    // the gate, after the first conditional
+    rc = capture_into(b, graph, &ifBuild, [&]() {
+      step_gate_kernel<<<1, 128, 0, b.stream>>>(b.d_mem, nm, hStep);
+      batch_count_launch(b);
+      return cuda_status(cudaGetLastError(), "step gate");
+    }, "graph capture (gate)");
+    if (rc != SPHGPU_OK) break;
+    if ((rc = add_if_node(graph, hStep, &ifStep, &stepBody)) != SPHGPU_OK) break;
+    // the step after the rebuild, in the second conditional's body
+    rc = capture_into(b, stepBody, nullptr, [&]() { return step_after_connectivity(b); }, "graph capture (step)");
+  } while (false);
   b.capturing = false;
   b.capacityGrids = false;
-  cudaGraph_t graph = nullptr;
-  const cudaError_t e = cudaStreamEndCapture(b.stream, &graph);
   // launches are counted when the graph is replayed
   b.graphLaunches = b.launches - l0;
   b.launches = l0;
   for (size_t m = 0; m < b.mem.size(); ++m) b.mem[m]->launches = m0[m];
-  if (rc != SPHGPU_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
-  if (e != cudaSuccess) return cuda_status(e, "graph capture");
-  const cudaError_t ei = cudaGraphInstantiate(&b.graphExec, graph, 0);
+  if (rc == SPHGPU_OK) {
+    e = cudaGraphInstantiate(&b.graphExec, graph, 0);
+    if (e != cudaSuccess) { b.graphExec = nullptr; rc = cuda_status(e, "graph instantiate"); }
+  }
   cudaGraphDestroy(graph);
-  if (ei != cudaSuccess) { b.graphExec = nullptr; return cuda_status(ei, "graph instantiate"); }
-  b.graphKey = graph_key(b);
-  return SPHGPU_OK;
+  if (rc == SPHGPU_OK) b.graphKey = graph_key(b);
+  return rc;
 }
 
+// One eager CheapSynchronousRK2 step of every member (host read-backs after
+// the rebuild and after the step).
 int step_impl(Batch& b) {
   // preStepInitialize: ghosts + connectivity every cycle, then ghost state.
   SPH_TRY(build_neighbors_impl(b));
-  if (b.useGraph) {
-    // everything the replay touches must exist before the capture
-    if (anyMember(b, isCrkP)) SPH_TRY(crk_prepare(b));
-    if (anyMember(b, isMixedSph) || anyMember(b, isMixedCrk)) SPH_TRY(prepare_mixed(b));
-    SPH_TRY(enable_graph(b));
-    SPH_TRY(upload_graph_descriptors(b));
-    if (b.graphExec == nullptr || graph_key(b) != b.graphKey) SPH_TRY(capture_step(b));
-    SPH_CHECK(cudaGraphLaunch(b.graphExec, b.stream));
-    b.launches += b.graphLaunches;
-    for (Problem* p : b.mem) p->launches += b.graphLaunches;
-    b.memDirty = true;     // the next eager call uploads to the rotating slots again
-  } else {
-    SPH_TRY(step_after_connectivity(b));
-  }
+  SPH_TRY(step_after_connectivity(b));
   const int slots[2] = {SC_DT, -1};
   std::vector<double> res;
   SPH_TRY(batch_gather(b, slots, 2, res));
@@ -495,6 +600,109 @@ int step_impl(Batch& b) {
     p.lastDt = res[2*m];
     p.cycle += 1;
     p.haveDerivs = true;
+    p.pairsEvaluated += p.pairs;
+  }
+  return SPHGPU_OK;
+}
+
+// `count` steps as replays of the captured graph with no host synchronisation
+// in between, then one read-back.  *done: steps completed (fewer when a
+// rebuild outgrew its buffers; the state is then the one before that step).
+int run_graph_steps(Batch& b, int64_t count, int64_t* done) {
+  *done = 0;
+  const int nm = (int)b.mem.size();
+  SPH_TRY(upload_graph_descriptors(b));
+  {
+    // device time from the host's, counters zeroed (one small upload)
+    std::vector<double> t(nm);
+    for (int m = 0; m < nm; ++m) t[m] = b.mem[m]->time;
+    std::vector<double> unused;
+    if ((int64_t)nm > b.gathercap) {
+      const int s0 = SC_DT;
+      SPH_TRY(batch_gather(b, &s0, 1, unused));      // sizes the gather buffers
+    }
+    SPH_CHECK(cudaMemcpyAsync(b.d_gather, t.data(), sizeof(double)*nm, cudaMemcpyHostToDevice, b.stream));
+    step_counters_kernel<<<(nm + 127)/128, 128, 0, b.stream>>>(b.d_mem, nm, b.d_gather);
+    batch_count_launch(b);
+    SPH_CHECK(cudaGetLastError());
+  }
+  for (int64_t s = 0; s < count; ++s) SPH_CHECK(cudaGraphLaunch(b.graphExec, b.stream));
+  b.memDirty = true;     // the next eager call uploads to the rotating slots again
+  const int s1[8] = {SC_STEPS, -1, SC_TIME, SC_DT, SC_G, SC_TOTAL, SC_MAXCOUNT, SC_PAIRS};
+  const int s2[3] = {SC_NCELLS, SC_CELLSWANTED, SC_PAIRSUM};
+  std::vector<double> r1, r2;
+  SPH_TRY(batch_gather(b, s1, 8, r1));
+  SPH_TRY(batch_gather(b, s2, 3, r2));
+  int64_t ran = count;
+  for (int m = 0; m < nm; ++m) ran = asI64(r1[8*m]) < ran ? asI64(r1[8*m]) : ran;
+  // kernels run: every completed replay; the open kernel of each one that
+  // stopped, and the rebuild and gate of the one that overflowed
+  const int64_t launched = b.graphLaunches*ran + (ran < count ? (count - ran) + b.graphBuildLaunches + 1 : 0);
+  bool overflow = false;
+  for (int m = 0; m < nm; ++m) {
+    Problem& p = *b.mem[m];
+    const double* a = &r1[8*m];
+    const int64_t steps = asI64(a[0]);
+    const int herr = (int)a[1];
+    p.launches += launched;
+    p.time = a[2];
+    if (steps > 0) {
+      p.lastDt = a[3];
+      p.cycle += steps;
+      p.haveNbrs = true;
+      p.haveDerivs = true;
+    }
+    p.G = asI64(a[4]);
+    p.ntot = p.n + p.G;
+    p.E = asI64(a[5]);
+    p.maxCount = asI32(a[6]);
+    p.pairs = asI64(a[7]);
+    p.ncells = asI64(r2[3*m]);
+    p.cellsWanted = asI64(r2[3*m + 1]);
+    p.pairsEvaluated += asI64(r2[3*m + 2]);
+    if (herr & (DERR_GHOST_CAPACITY | DERR_ENTRY_CAPACITY | DERR_LIST_CAPACITY | DERR_NBR_CAPACITY)) overflow = true;
+    else if (herr) return batch_check_errors(b, "step_rk2");
+  }
+  b.launches += launched;
+  if (overflow) {
+    // the steps from the overflowing rebuild on did nothing; the next eager
+    // step replans the buffers (and reports a real neighbor-capacity error)
+    for (Problem* p : b.mem) SPH_CHECK(cudaMemsetAsync(p->d_err, 0, sizeof(int), b.stream));
+    b.graphCandidate = 0;
+  }
+  *done = ran;
+  return SPHGPU_OK;
+}
+
+// nsteps CheapSynchronousRK2 steps of every member.  Eager steps unless the
+// "step graph" schedule is on; then every step runs as one replay of the
+// captured whole-step graph, captured once the buffer layout of an eager step
+// recurs (so a batch whose membership keeps changing stays eager).
+int steps_impl(Batch& b, int64_t nsteps) {
+  int64_t done = 0;
+  while (done < nsteps) {
+    // (a CRKSPH start-up volume, after new state, is an eager step's work)
+    if (!b.useGraph || anyMember(b, needsStartupVolume)) { SPH_TRY(step_impl(b)); ++done; continue; }
+    const uint64_t key = graph_key(b);
+    if (b.graphExec == nullptr || key != b.graphKey) {
+      if (key != b.graphCandidate) {
+        SPH_TRY(step_impl(b));
+        b.graphCandidate = graph_key(b);
+        ++done;
+        continue;
+      }
+      SPH_TRY(capture_full_step(b));
+    }
+    const int64_t want = nsteps - done;
+    int64_t ran = 0;
+    SPH_TRY(run_graph_steps(b, want, &ran));
+    done += ran;
+    if (ran < want) {
+      // an overflow stopped the replays: one eager step regrows the buffers
+      SPH_TRY(step_impl(b));
+      b.graphCandidate = graph_key(b);
+      ++done;
+    }
   }
   return SPHGPU_OK;
 }
@@ -627,10 +835,12 @@ int autotune_impl(Batch& b, double* report) {
 
 }  // namespace
 
-int batch_step_rk2(Batch& b) {
+int batch_step_rk2(Batch& b) { return batch_steps_rk2(b, 1); }
+
+int batch_steps_rk2(Batch& b, int64_t nsteps) {
   b.memDirty = true;
   for (Problem* p : b.mem) SPH_CHECK(cudaStreamSynchronize(p->stream));
-  return step_impl(b);
+  return steps_impl(b, nsteps);
 }
 
 // Device bytes a problem holds, from its buffer capacities.
@@ -969,7 +1179,7 @@ int sphgpu_dt(sphgpu_problem* p, double* dt_out) {
 int sphgpu_step_rk2(sphgpu_problem* p, double* time, int64_t nsteps, double* last_dt) {
   if (p == nullptr || nsteps < 0) return SPHGPU_ERR_ARG;
   if (time) p->time = *time;
-  for (int64_t s = 0; s < nsteps; ++s) SPH_TRY(step_impl(solo(p)));
+  SPH_TRY(steps_impl(solo(p), nsteps));
   if (time) *time = p->time;
   if (last_dt) *last_dt = p->lastDt;
   return SPHGPU_OK;
@@ -1117,6 +1327,12 @@ int sphgpu_num_pairs(sphgpu_problem* p, int64_t* pairs) {
   if (p == nullptr || pairs == nullptr) return SPHGPU_ERR_ARG;
   SPH_TRY(require_nbrs(solo(p)));
   *pairs = p->pairs;
+  return SPHGPU_OK;
+}
+
+int sphgpu_pairs_evaluated(sphgpu_problem* p, int64_t* pairs) {
+  if (p == nullptr || pairs == nullptr) return SPHGPU_ERR_ARG;
+  *pairs = p->pairsEvaluated;
   return SPHGPU_OK;
 }
 
@@ -1270,7 +1486,7 @@ int sphgpu_batch_evaluate_derivatives(sphgpu_batch* b) {
 int sphgpu_batch_step_rk2(sphgpu_batch* b, int64_t nsteps) {
   if (b == nullptr || nsteps < 0) return SPHGPU_ERR_ARG;
   SPH_TRY(batch_begin(*b));
-  for (int64_t s = 0; s < nsteps; ++s) SPH_TRY(step_impl(*b));
+  SPH_TRY(steps_impl(*b, nsteps));
   return SPHGPU_OK;
 }
 
@@ -1279,6 +1495,14 @@ int sphgpu_batch_pairs(sphgpu_batch* b, int64_t* pairs) {
   SPH_TRY(require_nbrs(*b));
   int64_t t = 0;
   for (Problem* p : b->mem) t += p->pairs;
+  *pairs = t;
+  return SPHGPU_OK;
+}
+
+int sphgpu_batch_pairs_evaluated(sphgpu_batch* b, int64_t* pairs) {
+  if (b == nullptr || pairs == nullptr) return SPHGPU_ERR_ARG;
+  int64_t t = 0;
+  for (Problem* p : b->mem) t += p->pairsEvaluated;
   *pairs = t;
   return SPHGPU_OK;
 }

@@ -815,18 +815,6 @@ __global__ void __launch_bounds__(256, SUB == 1 ? 3 : 1) nbr_walk_kernel(const M
     atomicAdd(reinterpret_cast<unsigned long long*>(M.scal + SC_PAIRS), (unsigned long long)above);
 }
 
-int64_t asI64(double stored) {
-  int64_t v;
-  std::memcpy(&v, &stored, sizeof(v));
-  return v;
-}
-
-int asI32(double stored) {
-  int v;
-  std::memcpy(&v, &stored, sizeof(v));
-  return v;
-}
-
 int64_t grow(int64_t v) { return v + v/4 + 1024; }
 
 // Capacities for the next build, from the previous one (or first estimates).
@@ -931,7 +919,8 @@ namespace {
 int launch_build(Batch& b) {
   cudaStream_t st = b.stream;
   const int nm = (int)b.mem.size();
-  SPH_TRY(batch_upload(b));
+  // (a captured build reads the descriptor slot uploaded before the capture)
+  if (!b.capturing) SPH_TRY(batch_upload(b));
   // ---- ghosts: six planar boundaries in order, sizes kept on the device
   build_init_kernel<<<(nm + 127)/128, 128, 0, st>>>(b.d_mem, nm); batch_count_launch(b);
   // fixed grids: at most kStreamBlocks blocks per member, member-local stride
@@ -1064,6 +1053,12 @@ int launch_build(Batch& b) {
 }
 
 }  // namespace
+
+// The build's launches alone, for a CUDA-graph capture of the whole step:
+// capacities planned beforehand (plan_build), no read-back; a capacity
+// overflow sets the member's error flag on the device instead.
+int plan_build(Batch& b) { return plan_capacities(b); }
+int launch_build_captured(Batch& b) { return launch_build(b); }
 
 // Ghosts and ConnectivityMap of every member: all stages launched with the
 // sizes kept on the device, then one read-back of the sizes; a capacity

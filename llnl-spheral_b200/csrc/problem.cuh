@@ -16,6 +16,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -208,6 +209,7 @@ struct Problem {
   int64_t gcap = 0;
   int64_t E = 0, ecap = 0;  // CSR entries
   int64_t pairs = 0;        // unordered pairs (ncalc)
+  int64_t pairsEvaluated = 0;  // pair interactions of every evaluation in the RK2 steps so far
   int maxNbr = 1024;
   int maxCount = 0;         // largest neighbor count of the current connectivity
   int nbrSchedule = 0;      // NBR_SCHEDULE_* requested for the neighbor walk
@@ -344,10 +346,26 @@ enum ScalSlot {
   SC_REACH = 37,       // kernel reach in cells of the current grid
   SC_CELLSWANTED = 38, // cells of the grid at its natural cell size (i64)
   SC_DELTAH = 39,      // largest H change of an iterateIdealH iteration (double bits)
-  NSCAL = 40
+  // step bookkeeping kept on the device, so that steps replayed from a CUDA
+  // graph need no host read-back in between
+  SC_TIME = 40,        // current time (advanced by every completed step)
+  SC_STEPS = 41,       // completed steps since the host last reset it (i64)
+  SC_PAIRSUM = 42,     // pair interactions evaluated by all completed steps (i64)
+  NSCAL = 43
 };
 
 // Sizes and grid of the current connectivity (device side).
+// A gathered scalar slot that holds integer bits, on the host.
+inline int64_t asI64(double stored) {
+  int64_t v;
+  std::memcpy(&v, &stored, sizeof(v));
+  return v;
+}
+inline int asI32(double stored) {
+  int v;
+  std::memcpy(&v, &stored, sizeof(v));
+  return v;
+}
 __device__ __forceinline__ int64_t scalI(const double* scal, int slot) {
   return reinterpret_cast<const int64_t*>(scal)[slot];
 }
@@ -424,12 +442,15 @@ struct Batch {
   int packedByUpdate = 0;        // records the last update kernel wrote (PackNeed), 0: none
   bool midInS0 = false;          // a record-only mid-point update ran: its packed SPH
                                  // members' mid-point H and mass density are in S0
-  // CUDA-graph replay of the part of the RK2 step after the connectivity
-  // (api.cu): captured once per buffer layout, replayed every step.
-  bool useGraph = false;
+  // CUDA-graph replay of the whole RK2 step, rebuild included (api.cu):
+  // captured once per buffer layout, replayed for every step of a call
+  // (on unless the "step graph" schedule is set to 0).
+  bool useGraph = true;
+  uint64_t graphCandidate = 0;   // buffer layout of the last eager step (capture when it recurs)
   bool capturing = false;        // stream capture in progress: maps go to the arena
   bool capacityGrids = false;    // (n + ghosts)-sized kernels sized for the buffer capacity
   cudaGraphExec_t graphExec = nullptr;
+  int64_t graphBuildLaunches = 0;  // kernels of the captured rebuild
   uint64_t graphKey = 0;
   int64_t graphLaunches = 0;     // kernel nodes of the captured graph
   cudaStream_t sideStream = nullptr;
@@ -484,6 +505,8 @@ int batch_scan(Batch& b, int which);
 
 // ---- stages (ghosts/neighbors: nbrs.cu; SPH: sph.cu; mixed: sph_mixed.cu; CRKSPH: crk.cu)
 int build_connectivity(Batch& b);     // ghosts + ConnectivityMap, device-sized
+int plan_build(Batch& b);             // capacities and schedules of the next build
+int launch_build_captured(Batch& b);  // the build's launches, sized on the device, no read-back
 // FP64 pair records of the members that read them next (PACK_ALL: every member)
 enum PackNeed { PACK_ALL = 0, PACK_FOR_EVAL = 1, PACK_FOR_FINALIZE = 2 };
 int pack_records(Batch& b, int need = PACK_ALL);
@@ -528,6 +551,7 @@ int launch_crk_eval_mixed(Batch& b);                        // mixed-precision C
 
 // one CheapSynchronousRK2 step of every member (api.cu)
 int batch_step_rk2(Batch& b);
+int batch_steps_rk2(Batch& b, int64_t nsteps);   // graph replays where the schedule allows
 // TableKernel::equivalentNodesPerSmoothingScale (src/Kernel/TableKernel.cc:
 // 402-430): bisectSearch of the Wsum table, then linear interpolation of the
 // nPerh table.  The bisection starts from the bracket table's interval for w

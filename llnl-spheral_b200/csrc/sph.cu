@@ -868,9 +868,19 @@ __global__ void select_dt_kernel(const Member* mem, int nmem) {
   sc[SC_VOTE] = vote;
 }
 
+// End of a completed step: last dt, and the step bookkeeping a graph replay
+// reads back only at the end of a call (time += dt as the integrator does,
+// steps and pair interactions counted).
 __global__ void finish_step_kernel(const Member* mem, int nmem) {
   const int m = blockIdx.x*blockDim.x + threadIdx.x;
-  if (m < nmem) mem[m].scal[SC_LASTDT] = mem[m].scal[SC_DT];
+  if (m >= nmem) return;
+  double* s = mem[m].scal;
+  const double dt = s[SC_DT];
+  s[SC_LASTDT] = dt;
+  s[SC_TIME] = s[SC_TIME] + dt;
+  int64_t* si = reinterpret_cast<int64_t*>(s);
+  si[SC_STEPS] += 1;
+  si[SC_PAIRSUM] += si[SC_PAIRS];
 }
 
 // ---------------------------------------------------------------- conservation

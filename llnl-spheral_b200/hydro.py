@@ -119,6 +119,12 @@ class SPHHydro:
         abi.check(self.lib.sphgpu_num_pairs(self.h, ctypes.byref(v)), self.lib)
         return v.value
 
+    def pairs_evaluated(self):
+        """num_pairs() of every RK2 step taken so far, summed."""
+        v = ctypes.c_int64()
+        abi.check(self.lib.sphgpu_pairs_evaluated(self.h, ctypes.byref(v)), self.lib)
+        return v.value
+
     # ---- Physics<Dim> methods
     def initialize(self, time=0.0, dt=0.0):
         abi.check(self.lib.sphgpu_initialize(self.h, time, dt), self.lib)
@@ -271,6 +277,11 @@ class SPHBatch:
     def num_pairs(self):
         v = ctypes.c_int64()
         abi.check(self.lib.sphgpu_batch_pairs(self.h, ctypes.byref(v)), self.lib)
+        return v.value
+
+    def pairs_evaluated(self):
+        v = ctypes.c_int64()
+        abi.check(self.lib.sphgpu_batch_pairs_evaluated(self.h, ctypes.byref(v)), self.lib)
         return v.value
 
     def kernel_launches(self):

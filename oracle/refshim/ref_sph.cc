@@ -13,7 +13,7 @@
 // finalizeDerivatives at the start time, then CheapSynchronousRK2 steps.
 //
 // usage: ref_sph input.bin outdir
-//        ref_sph --time WARMUP input.bin
+//        ref_sph --time WARMUP input.bin [IDEALH_MAXITER IDEALH_TOLERANCE]
 //        ref_sph --ideal-h MAXITER TOLERANCE input.bin outdir
 // The second form times the reference's CheapSynchronousRK2 steps instead of
 // writing fields: after the start-up and WARMUP untimed steps it runs the
@@ -78,6 +78,8 @@ bool g_timing = false;
 int g_warmup = 0;
 int g_idealHMax = -1;          // >= 0: run iterateIdealH instead of the steps
 double g_idealHTol = 0.0;
+int g_timeIdealHMax = 0;        // --time: iterateIdealH before the run (0: none)
+double g_timeIdealHTol = 0.0;
 
 template<typename T>
 void dumpRaw(const std::string& name, const std::vector<T>& v, const char* ext) {
@@ -204,6 +206,18 @@ int run(const Input& in, Hydro& hydro, NodeSpace::FluidNodeList<D>& nodes, DataB
   integ.currentTime(0.0);
 
   integ.setGhostNodes();
+  if (g_timing && g_timeIdealHMax > 0) {
+    // the controller's start-up with iterateInitialH (its default): H
+    // relaxed to the ideal smoothing scale before the run, untimed
+    // (src/SimulationControl/SpheralController.py:186-187,718-731)
+    NodeSpace::SPHSmoothingScale<D> method;
+    std::stringstream log;
+    std::streambuf* old = std::cerr.rdbuf(log.rdbuf());
+    iterateIdealH(db, integ.uniqueBoundaryConditions(), hydro.kernel(), method, g_timeIdealHMax,
+                  g_timeIdealHTol, 0.0, false, false);
+    std::cerr.rdbuf(old);
+    integ.setGhostNodes();
+  }
   if (g_idealHMax >= 0) {
     // SpheralController.iterateIdealH (src/SimulationControl/SpheralController.py:718-731)
     NodeSpace::SPHSmoothingScale<D> method;
@@ -312,15 +326,20 @@ int main(int argc, char** argv) {
     g_idealHTol = std::atof(argv[3]);
     inputPath = argv[4];
     g_dir = argv[5];
-  } else if (argc == 4 && std::string(argv[1]) == "--time") {
+  } else if ((argc == 4 || argc == 6) && std::string(argv[1]) == "--time") {
     g_timing = true;
     g_warmup = std::atoi(argv[2]);
     inputPath = argv[3];
+    if (argc == 6) {
+      g_timeIdealHMax = std::atoi(argv[4]);
+      g_timeIdealHTol = std::atof(argv[5]);
+    }
   } else if (argc == 3) {
     g_dir = argv[2];
     inputPath = argv[1];
   } else {
-    std::fprintf(stderr, "usage: %s input.bin outdir | %s --time WARMUP input.bin\n", argv[0], argv[0]);
+    std::fprintf(stderr, "usage: %s input.bin outdir | %s --time WARMUP input.bin [IDEALH_MAXITER IDEALH_TOL] | "
+                         "%s --ideal-h MAXITER TOL input.bin outdir\n", argv[0], argv[0], argv[0]);
     return 2;
   }
   Input in;

@@ -141,13 +141,15 @@ def test_autotune_keeps_results(gpu_lib, pkg):
 
 
 def test_graph_replayed_steps_match_eager(gpu_lib, pkg):
-    """The post-connectivity part of the step as a captured CUDA graph (one
-    capture, then replays) gives exactly the eager results, for a batch
-    (SPH, mixed, CRKSPH members) and for a single problem."""
+    """The whole RK2 step, rebuild included, as a captured CUDA graph (one
+    capture, then replays with no host round trip) gives exactly the eager
+    results, for a batch (SPH, mixed, CRKSPH members) and for a single
+    problem."""
     specs = _specs(pkg)
     eager = [pkg.SPHHydro(cfg, ns) for ns, cfg in specs]
     mem = [pkg.SPHHydro(cfg, ns) for ns, cfg in specs]
     for e in eager:
+        e.set_schedule("step graph", 0)
         e.step(4)
     batch = pkg.SPHBatch(mem)
     batch.set_schedule("step graph", 1)
@@ -158,12 +160,74 @@ def test_graph_replayed_steps_match_eager(gpu_lib, pkg):
             assert np.array_equal(e.field(k), m.field(k)), k
     ns, cfg = specs[1]
     a, g = pkg.SPHHydro(cfg, ns), pkg.SPHHydro(cfg, ns)
-    g.set_schedule("step graph", 1)
+    a.set_schedule("step graph", 0)
+    assert a.schedule("step graph") == 0
     a.step(3)
     g.step(3)
     assert g.schedule("step graph") == 1
     for k in STATE_KEYS:
         assert np.array_equal(a.field(k), g.field(k)), k
+    assert g.pairs_evaluated() == a.pairs_evaluated()
+    assert batch.pairs_evaluated() == sum(e.pairs_evaluated() for e in eager)
+    # new state of the same layout: the next call replays the graph at once
+    for h in (a, g):
+        h.set_state(_State(h, 1.0))
+        h.step(2)
+    assert g.num_pairs() == a.num_pairs()
+    for k in STATE_KEYS:
+        assert np.array_equal(a.field(k), g.field(k)), k
+
+
+class _State:
+    """A node set read back from a problem, with H scaled."""
+
+    def __init__(self, h, hscale):
+        self.pos = h.field("position")
+        self.vel = h.field("velocity")
+        self.mass = h.field("mass")
+        self.rho = h.field("mass density")
+        self.eps = h.field("specific thermal energy")
+        self.H = h.field("H") * hscale
+
+
+@pytest.mark.parametrize("hydro", ["sph", "crksph"])
+def test_graph_steps_regrow_after_overflow(gpu_lib, pkg, hydro):
+    """Graph replays after new state that outgrows the buffers: the caller
+    shrinks every H by 2/3 between calls (about 3.4x the neighbors), so the
+    first replayed rebuild overflows its ghost, entry and list capacities; the
+    gate skips the rest of that step, the library grows the buffers, takes
+    the step eagerly (with the CRKSPH start-up volume new state needs) and
+    captures again.  States, times and the pair counter equal eager steps bit
+    for bit."""
+    abi = pkg.abi
+    ns, cfg = _kh_member(pkg, abi.PRECISION_FP64,
+                         hydro=abi.HYDRO_CRKSPH if hydro == "crksph" else None)
+    a, g = pkg.SPHHydro(cfg, ns), pkg.SPHHydro(cfg, ns)
+    a.set_schedule("step graph", 0)
+    pairs = 0
+    for _ in range(4):
+        a.step(1)
+        pairs += a.num_pairs()
+    g.step(4)
+    assert g.pairs_evaluated() == a.pairs_evaluated() == pairs
+    e0 = g.num_pairs()
+    for h in (a, g):
+        h.set_state(_State(h, 2.0 / 3.0))
+    p0 = g.pairs_evaluated()
+    per_step = []
+    for _ in range(5):
+        a.step(1)
+        per_step.append(a.num_pairs())
+    g.step(5)
+    assert per_step[0] > 2 * e0          # the first rebuild after the new state outgrew the buffers
+    assert g.time == a.time
+    for k in STATE_KEYS:
+        assert np.array_equal(a.field(k), g.field(k)), k
+    assert g.pairs_evaluated() - p0 == sum(per_step)
+    assert g.pairs_evaluated() == a.pairs_evaluated()
+    so, sn, sr = a.connectivity()
+    go, gn, gr = g.connectivity()
+    assert np.array_equal(so, go) and np.array_equal(sn, gn) and np.array_equal(sr, gr)
 
 
 def test_batch_of_mixed_sph_and_mixed_crk_members(gpu_lib, pkg):
