@@ -193,6 +193,33 @@ int sphgpu_iterate_ideal_h(sphgpu_problem* p, int32_t max_iterations, double tol
 int sphgpu_checkpoint_size(sphgpu_problem* p, int64_t* bytes);
 int sphgpu_checkpoint_save(sphgpu_problem* p, void* buffer, int64_t bytes);
 int sphgpu_checkpoint_load(sphgpu_problem* p, const void* buffer, int64_t bytes);
+/* Restart files in the reference's own layout: what RestartRegistrar::dumpState
+ * (src/DataOutput/RestartRegistrar.cc:155-171) writes through FlatFileIO in
+ * ascii form (src/FileIO/FlatFileIO.cc; "path value" lines at precision 20,
+ * Fields as "path n v0 v1 ...", FieldLists as path/NodeListNames + path/Field0)
+ * for the objects of a one-NodeList problem, in registration order under their
+ * unique labels: FluidNodeList (NodeList::dumpState + FluidNodeList::dumpState,
+ * src/NodeList/NodeList.cc:606-621, FluidNodeList.cc:180-189), the artificial
+ * viscosity (src/ArtificialViscosity/ArtificialViscosity.cc:173-179),
+ * SPHHydroBase (src/SPH/SPHHydroBase.cc:1286-1318) or CRKSPHHydroBase
+ * (src/CRKSPH/CRKSPHHydroBase.cc:1455-1485), PeriodicBoundary and its two
+ * PlanarBoundary planes per periodic axis (src/Boundary/PlanarBoundary.cc:
+ * 297-301), CheapSynchronousRK2 (src/Integrator/Integrator.cc:798-806).  The
+ * reference's FlatFileIO and RestartRegistrar::restoreState read the file into
+ * a reference problem of the same configuration; the NodeList's per-node
+ * "work" timing field is written as 0.
+ * sphgpu_restart_dump: node_list_name is the NodeList's name (NULL: "nodes").
+ * sphgpu_restart_restore: reads such a file (written by this library or by the
+ * reference) into a problem of the same configuration and node count: state,
+ * derivatives, CRKSPH corrections, time, last dt and cycle; the next step
+ * continues the run as SpheralController.loadRestartFile does
+ * (src/SimulationControl/SpheralController.py:514-550).  A missing key or
+ * another node count returns SPHGPU_ERR_ARG and leaves the problem unchanged.
+ * sphgpu_restart_labels: the labels a dump of `cfg` writes, one per line
+ * (host only, no device work). */
+int sphgpu_restart_dump(sphgpu_problem* p, const char* path, const char* node_list_name);
+int sphgpu_restart_restore(sphgpu_problem* p, const char* path);
+int sphgpu_restart_labels(const sphgpu_config* cfg, char* buffer, int64_t bytes);
 /* SpheralConservation (src/SimulationControl/SpheralConservation.py:27-63):
  * out = {mass, px, py, pz, kinetic E, thermal E, total E, total E low part},
  * FP64 on device.  The total energy is summed as a double-double (two-sum

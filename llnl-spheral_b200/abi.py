@@ -161,6 +161,9 @@ def load_library(path=None):
     lib.sphgpu_checkpoint_size.argtypes = [P, ctypes.POINTER(I64)]
     lib.sphgpu_checkpoint_save.argtypes = [P, P, I64]
     lib.sphgpu_checkpoint_load.argtypes = [P, P, I64]
+    lib.sphgpu_restart_dump.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p]
+    lib.sphgpu_restart_restore.argtypes = [P, ctypes.c_char_p]
+    lib.sphgpu_restart_labels.argtypes = [ctypes.POINTER(SphConfig), ctypes.c_char_p, I64]
     lib.sphgpu_num_pairs.argtypes = [P, ctypes.POINTER(I64)]
     lib.sphgpu_pairs_evaluated.argtypes = [P, ctypes.POINTER(I64)]
     lib.sphgpu_kernel_launches.argtypes = [P, ctypes.POINTER(I64)]
@@ -207,3 +210,12 @@ def check(rc, lib=None):
         msg = lib.sphgpu_last_error().decode() if lib is not None else ""
         raise RuntimeError("sphgpu error %d: %s" % (rc, msg))
     return rc
+
+
+def restart_labels(cfg):
+    """Unique labels, in order, of the objects a restart file of `cfg` holds
+    (sphgpu_restart_labels; host only)."""
+    lib = load_library()
+    buf = ctypes.create_string_buffer(4096)
+    check(lib.sphgpu_restart_labels(ctypes.byref(cfg), buf, len(buf)), lib)
+    return buf.value.decode().split()

@@ -33,6 +33,7 @@ UNITS = [
     ("crk_mixed.cu", ["-fmad=false"]),
     ("noalloc.cu", []),
     ("server.cu", []),
+    ("restart.cu", []),
     ("table.cc", []),
 ]
 HEADERS = ["devmath.cuh", "problem.cuh", "mixed.cuh"]

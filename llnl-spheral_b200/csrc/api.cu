@@ -81,6 +81,21 @@ __global__ void fill_kernel(double* dst, int64_t n, double v) {
   for (int64_t t = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x*blockDim.x) dst[t] = v;
 }
 
+// The restart-file values of the state the caller set (the reference's
+// start-up): the EOS entropy, GammaLawGas::setEntropy
+// (src/Material/GammaLawGas.cc:151-158, DataBase::fluidEntropy at the
+// hydro's construction), and specificThermalEnergy0 = the specific thermal
+// energy with the compatible energy, else 0
+// (src/SPH/SPHHydroBase.cc:262-272).
+__global__ void startup_restart_kernel(const double* S, double* S0, int64_t n, double gamma, int compatible) {
+  for (int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x*blockDim.x) {
+    const double rho = S[S_RHO*n + i], eps = S[S_EPS*n + i];
+    const double P = (gamma - 1.0)*rho*eps;
+    S0[S0_ENTROPY*n + i] = P*safeInvVar(pow(rho, gamma));
+    S0[S_EPS*n + i] = compatible ? eps : 0.0;
+  }
+}
+
 __global__ void check_state_kernel(const double* S, int64_t n, int* err) {
   for (int64_t i = blockIdx.x*(int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x*blockDim.x) {
     const double m = S[S_M*n + i], rho = S[S_RHO*n + i];
@@ -187,7 +202,7 @@ void free_problem(Problem* p) {
   void* ptrs[] = {p->S, p->S0, p->D, p->rec, p->groot, p->gcode, p->gpos, p->cand, p->cidx, p->sortedIdx,
                   p->cellStart, p->cellFill, p->counts, p->offsets, p->nbr, p->pacc, p->tableCoef, p->nperhTab,
                   p->wsumTab, p->blockSums, p->d_err, p->d_scal, p->d_red, p->staging, p->coefF, p->mrec, p->K, p->crec, p->hmaxi,
-                  p->wsumBinsTab, p->qgrad};
+                  p->wsumBinsTab, p->qgrad, p->Kheld};
   dev_free_all(ptrs, (int)(sizeof(ptrs)/sizeof(ptrs[0])));
   if (p->pinned) cudaFreeHost(p->pinned);
   if (p->solo) { batch_free(*p->solo); delete p->solo; p->solo = nullptr; }
@@ -268,10 +283,13 @@ int set_state_impl(Problem& p, const double* pos, const double* vel, const doubl
   fill_kernel<<<grid1(p.n), 256, 0, p.stream>>>(p.S + (int64_t)S_OMEGA*p.n, p.n, 1.0); ++p.launches;
   SPH_TRY(launch_eos(solo(&p)));
   check_state_kernel<<<grid1(p.n), 256, 0, p.stream>>>(p.S, p.n, p.d_err); ++p.launches;
+  startup_restart_kernel<<<grid1(p.n), 256, 0, p.stream>>>(p.S, p.S0, p.n, p.cfg.gamma,
+                                                           p.cfg.compatibleEnergyEvolution); ++p.launches;
   SPH_CHECK(cudaGetLastError());
   SPH_TRY(batch_check_errors(solo(&p), "set_state"));
   p.haveNbrs = false;
   p.crkVolumeReady = false;
+  p.omegaResetByStep = false;
   return SPHGPU_OK;
 }
 
@@ -321,6 +339,22 @@ int initialize_impl(Batch& b) {
     SPH_TRY(pack_records(b, PACK_FOR_EVAL));
   }
   return cuda_status(cudaGetLastError(), "initialize");
+}
+
+// After an initialize outside an RK2 step: the restart-file state the
+// reference's State then holds (Problem::Kheld, Problem::omegaResetByStep).
+int hold_restart_state(Batch& b) {
+  for (Problem* p : b.mem) {
+    p->omegaResetByStep = false;
+    if (!isCrkP(*p) || p->K == nullptr) continue;
+    const size_t bytes = sizeof(double)*K_M0*(size_t)p->n;
+    if (p->Kheld == nullptr && dev_alloc(reinterpret_cast<void**>(&p->Kheld), bytes) != cudaSuccess) {
+      set_error("CRKSPH correction copy allocation failed");
+      return SPHGPU_ERR_NOMEM;
+    }
+    SPH_CHECK(cudaMemcpyAsync(p->Kheld, p->K, bytes, cudaMemcpyDeviceToDevice, b.stream));
+  }
+  return SPHGPU_OK;
 }
 
 // Physics::finalize: CRK volumes then the summed density, or the SPH sum.
@@ -600,6 +634,7 @@ int step_impl(Batch& b) {
     p.lastDt = res[2*m];
     p.cycle += 1;
     p.haveDerivs = true;
+    p.omegaResetByStep = true;
     p.pairsEvaluated += p.pairs;
   }
   return SPHGPU_OK;
@@ -651,6 +686,7 @@ int run_graph_steps(Batch& b, int64_t count, int64_t* done) {
       p.cycle += steps;
       p.haveNbrs = true;
       p.haveDerivs = true;
+      p.omegaResetByStep = true;
     }
     p.G = asI64(a[4]);
     p.ntot = p.n + p.G;
@@ -813,6 +849,7 @@ int autotune_impl(Batch& b, double* report) {
     if ((rc = build_neighbors_impl(b)) != SPHGPU_OK) break;
     if ((rc = pack_records(b)) != SPHGPU_OK) break;
     if ((rc = initialize_impl(b)) != SPHGPU_OK) break;
+    if ((rc = hold_restart_state(b)) != SPHGPU_OK) break;
     // pair loop: threads per block
     const int widths[2] = {64, 128};
     best = 1e300;
@@ -855,7 +892,7 @@ int64_t problem_bytes(const Problem& p) {
   b += p.cellcap*(8 + 4) + 8 + 8*p.blockSumsCap;
   b += 8*(int64_t)(p.cfg.hydro == SPHGPU_HYDRO_CRKSPH ? CMRECW : MRECW)*p.mreccap +
        (p.coefF ? 4*6*(int64_t)p.prm.W.n : 0);
-  b += 8*(int64_t)CRECW*p.creccap + (p.K ? 8*(int64_t)NCRK*n : 0);
+  b += 8*(int64_t)CRECW*p.creccap + (p.K ? 8*(int64_t)NCRK*n : 0) + (p.Kheld ? 8*(int64_t)K_M0*n : 0);
   b += p.cfg.qType == SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD ? 8*(int64_t)QGRADW*n : 0;
   return b;
 }
@@ -1138,7 +1175,8 @@ int sphgpu_initialize(sphgpu_problem* p, double time, double dt) {
   (void)time; (void)dt;
   SPH_TRY(require_nbrs(solo(p)));
   SPH_TRY(pack_records(solo(p)));
-  return initialize_impl(solo(p));
+  SPH_TRY(initialize_impl(solo(p)));
+  return hold_restart_state(solo(p));
 }
 
 int sphgpu_evaluate_derivatives(sphgpu_problem* p, double time, double dt) {
@@ -1478,6 +1516,7 @@ int sphgpu_batch_evaluate_derivatives(sphgpu_batch* b) {
   SPH_TRY(require_nbrs(*b));
   SPH_TRY(pack_records(*b));
   SPH_TRY(initialize_impl(*b));
+  SPH_TRY(hold_restart_state(*b));
   SPH_TRY(launch_eval(*b));
   for (Problem* p : b->mem) p->haveDerivs = true;
   return batch_check_errors(*b, "batch evaluate_derivatives");

@@ -908,9 +908,9 @@ int64_t planned_bytes(const sphgpu_config& cfg, int64_t n, int64_t G, int64_t E,
   double marker = 0.0;                          // problem_bytes only tests these for null
   if (cfg.compatibleEnergyEvolution) p.pacc = &marker;
   if (cfg.precision == SPHGPU_PRECISION_MIXED) p.coefF = reinterpret_cast<float*>(&marker);
-  if (cfg.hydro == SPHGPU_HYDRO_CRKSPH) p.K = &marker;
+  if (cfg.hydro == SPHGPU_HYDRO_CRKSPH) { p.K = &marker; p.Kheld = &marker; }
   const int64_t b = problem_bytes(p);
-  p.pacc = nullptr; p.coefF = nullptr; p.K = nullptr;
+  p.pacc = nullptr; p.coefF = nullptr; p.K = nullptr; p.Kheld = nullptr;
   return b;
 }
 

@@ -55,6 +55,12 @@ enum StateField {
   S_VOL = 18,          // CRKSPH "node volume"
   NSTATE = 19
 };
+// Columns of the start-of-step copy S0 that no step reads, kept for the
+// restart files: the mass column (mass is constant within a step) holds the
+// entropy (the EOS's at the state the caller set; CRKSPH's EntropyPolicy
+// updates it every full update), and S_EPS holds the specific thermal energy
+// at the start of the last step (the reference's specificThermalEnergy0).
+constexpr int S0_ENTROPY = S_M;
 
 // CRKSPH corrections and moments of the internal nodes, SoA [NCRK][n].
 enum CrkField {
@@ -228,6 +234,14 @@ struct Problem {
   double* S0 = nullptr;
   double* D = nullptr;
   double* K = nullptr;          // [NCRK][n] CRKSPH fields (CRKSPH problems only)
+  double* Kheld = nullptr;      // [K_M0][n] the corrections A, B, grad A, grad B as the
+                                // reference's State holds them between RK2 steps: those of
+                                // the last initialize outside a step (each step's state0
+                                // copy restores them after its mid-point evaluation);
+                                // written to restart files only
+  bool omegaResetByStep = false; // the reference's omegaGradh is 1 after an RK2 step (each step's
+                                 // State construction resets it, its state0 copy restores that);
+                                 // a restart file written then holds 1
   double* qgrad = nullptr;      // [n][QGRADW] velocity gradient cached by the CRKSPH Q's initialize
   double* crec = nullptr;       // [n+G][CRECW] CRKSPH pair records
   int64_t creccap = 0;

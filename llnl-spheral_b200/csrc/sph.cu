@@ -689,6 +689,15 @@ __global__ void __launch_bounds__(128, 6) update_kernel(const Member* mem, Block
   const double csn = sqrt(dmax(0.0, P.gamma*g1*eps));
   // velocity: IncrementFieldList (after the energy it depends on)
   v = V3{v.x + D[(D_DVDT + 0)*n + i]*mult, v.y + D[(D_DVDT + 1)*n + i]*mult, v.z + D[(D_DVDT + 2)*n + i]*mult};
+  if (mode == UPDATE_FROM_START) {
+    // the start-of-step energy the reference's state0 leaves in its
+    // specificThermalEnergy0 (compatible energy; members that read their
+    // source from S0 have it there already)
+    if (P.compatible && Src == S) S0[S_EPS*n + i] = eps0;
+    // CRKSPH's EntropyPolicy (src/Hydro/EntropyPolicy.cc:52-82):
+    // GammaLawGas::setEntropy of the updated density and energy
+    if (crk) S0[S0_ENTROPY*n + i] = Pn*safeInvVar(pow(rho, P.gamma));
+  }
   if (!midInRecords) {
     S[S_EPS*n + i] = eps;
     S[S_P*n + i] = Pn;

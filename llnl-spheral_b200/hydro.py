@@ -12,6 +12,7 @@ Every call goes through libsphgpu.so; errors raise RuntimeError with the
 library's message (the reference throws VERIFYError).  There is no CPU path.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -182,13 +183,16 @@ class SPHHydro:
         abi.check(self.lib.sphgpu_checkpoint_load(self.h, _p(buf), buf.size), self.lib)
         self.sync_time()
 
-    def dumpState(self, path):
-        with open(path, "wb") as f:
-            f.write(self.checkpoint())
+    def dumpState(self, path, nodeListName="nodes"):
+        """The reference's restart file (RestartRegistrar::dumpState through
+        FlatFileIO, ascii) of this problem at `path`."""
+        abi.check(self.lib.sphgpu_restart_dump(self.h, os.fsencode(str(path)), nodeListName.encode()), self.lib)
 
     def restoreState(self, path):
-        with open(path, "rb") as f:
-            self.restore(f.read())
+        """Restore a restart file in the reference's layout (written by
+        dumpState or by the reference itself) and continue from it."""
+        abi.check(self.lib.sphgpu_restart_restore(self.h, os.fsencode(str(path))), self.lib)
+        self.sync_time()
 
     def kernel_launches(self):
         v = ctypes.c_int64()

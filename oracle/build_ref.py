@@ -206,6 +206,7 @@ UNITS = [
         "const bool, const bool);")),
     ("DataOutput/RestartRegistrar.cc", ""),
     ("FileIO/FileIO.cc", ""),
+    ("FileIO/FlatFileIO.cc", ""),
 ]
 
 TABLE_UNITS = ["Geometry/Dimension.cc", "Geometry/GeomVector.cc", "Geometry/GeomTensor.cc",

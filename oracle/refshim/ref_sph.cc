@@ -15,6 +15,8 @@
 // usage: ref_sph input.bin outdir
 //        ref_sph --time WARMUP input.bin [IDEALH_MAXITER IDEALH_TOLERANCE]
 //        ref_sph --ideal-h MAXITER TOLERANCE input.bin outdir
+//        ref_sph --restart-dump input.bin restart.txt
+//        ref_sph --restart-load input.bin restart.txt outdir
 // The second form times the reference's CheapSynchronousRK2 steps instead of
 // writing fields: after the start-up and WARMUP untimed steps it runs the
 // input's step count, timing each step, and prints one JSON line with the
@@ -24,7 +26,15 @@
 // way SpheralController.iterateIdealH calls it (SPHSmoothingScale, no nPerh
 // rescaling, no spherical start, no fixed determinant) after the start-up
 // ghosts, and writes the relaxed H and the iteration count and last change it
-// reports.
+// reports.  --restart-dump runs the start-up, the evaluation and the input's
+// steps, then writes the reference's restart file: RestartRegistrar::dumpState
+// (src/DataOutput/RestartRegistrar.cc) into a FlatFileIO ascii file
+// (src/FileIO/FlatFileIO.cc), every registered object under its unique label.
+// --restart-load runs the start-up, then restores every registered object
+// from such a file the way SpheralController.loadRestartFile does
+// (src/SimulationControl/SpheralController.py:514-550), runs the input's
+// steps and writes the steps/ fields; the input's node arrays only size the
+// problem.
 // input.bin: int64 n, int64 nsteps, sphgpu_config (raw struct), then the
 // internal nodes' position[3n], velocity[3n], mass[n], mass density[n],
 // specific thermal energy[n], H[6n] (float64, the reference Field layouts).
@@ -62,6 +72,8 @@
 #include "Geometry/GeomThirdRankTensor.hh"
 #include "Integrator/CheapSynchronousRK2.hh"
 #include "Utilities/iterateIdealH.hh"
+#include "FileIO/FlatFileIO.hh"
+#include "DataOutput/RestartRegistrar.hh"
 
 #include "sphgpu.h"
 
@@ -80,10 +92,13 @@ int g_idealHMax = -1;          // >= 0: run iterateIdealH instead of the steps
 double g_idealHTol = 0.0;
 int g_timeIdealHMax = 0;        // --time: iterateIdealH before the run (0: none)
 double g_timeIdealHTol = 0.0;
+std::string g_restartOut;       // --restart-dump: restart file written after the steps
+std::string g_restartIn;        // --restart-load: restart file restored before the steps
+bool g_quiet = false;           // no field dumps
 
 template<typename T>
 void dumpRaw(const std::string& name, const std::vector<T>& v, const char* ext) {
-  if (g_timing) return;
+  if (g_timing || g_quiet) return;
   const std::string path = g_dir + "/" + name + ext;
   FILE* f = std::fopen(path.c_str(), "wb");
   if (!f) { std::perror(path.c_str()); std::exit(1); }
@@ -247,6 +262,11 @@ int run(const Input& in, Hydro& hydro, NodeSpace::FluidNodeList<D>& nodes, DataB
   integ.preStepInitialize(state, derivs);
   integ.initializeDerivatives(0.0, 0.0, state, derivs);
 
+  if (!g_restartIn.empty()) {
+    FileIOSpace::FlatFileIO file(g_restartIn, FileIOSpace::AccessType::Read, FileIOSpace::FlatFileFormat::ascii);
+    DataOutput::RestartRegistrar::instance().restoreState(file);
+    file.close();
+  } else {
   // Ghosts: root internal node and position of every ghost.
   const int numNodes = nodes.numNodes();
   std::vector<int64_t> root(numNodes);
@@ -277,6 +297,7 @@ int run(const Input& in, Hydro& hydro, NodeSpace::FluidNodeList<D>& nodes, DataB
   integ.finalizeDerivatives(0.0, 0.0, db, state, derivs);
   dumpForm(hydro, n);
   dump("eval/hydro dt", std::vector<double>(1, hydro.dt(db, state, derivs, 0.0).first));
+  }
 
   if (g_timing) {
     for (int s = 0; s < g_warmup; ++s) integ.step(1e30);
@@ -303,6 +324,12 @@ int run(const Input& in, Hydro& hydro, NodeSpace::FluidNodeList<D>& nodes, DataB
     tdt.push_back(integ.currentTime());
     tdt.push_back(integ.lastDt());
   }
+  if (!g_restartOut.empty()) {
+    FileIOSpace::FlatFileIO file(g_restartOut, FileIOSpace::AccessType::Create, FileIOSpace::FlatFileFormat::ascii);
+    DataOutput::RestartRegistrar::instance().dumpState(file);
+    file.close();
+    for (const std::string& l : DataOutput::RestartRegistrar::instance().uniqueLabels()) std::printf("label %s\n", l.c_str());
+  }
   dump("steps/time_dt", tdt);
   dumpField("steps/position", nodes.positions(), n);
   dumpField("steps/velocity", nodes.velocity(), n);
@@ -313,7 +340,7 @@ int run(const Input& in, Hydro& hydro, NodeSpace::FluidNodeList<D>& nodes, DataB
   dumpField("steps/sound speed", hydro.soundSpeed(), n);
   dumpStepForm(hydro, n);
   for (auto* bc : bcs) delete bc;
-  std::printf("ok %d nodes, %d ghosts\n", n, numNodes - n);
+  std::printf("ok %d nodes, %d ghosts\n", n, nodes.numNodes() - n);
   return 0;
 }
 
@@ -334,12 +361,21 @@ int main(int argc, char** argv) {
       g_timeIdealHMax = std::atoi(argv[4]);
       g_timeIdealHTol = std::atof(argv[5]);
     }
+  } else if (argc == 4 && std::string(argv[1]) == "--restart-dump") {
+    inputPath = argv[2];
+    g_restartOut = argv[3];
+    g_quiet = true;
+  } else if (argc == 5 && std::string(argv[1]) == "--restart-load") {
+    inputPath = argv[2];
+    g_restartIn = argv[3];
+    g_dir = argv[4];
   } else if (argc == 3) {
     g_dir = argv[2];
     inputPath = argv[1];
   } else {
     std::fprintf(stderr, "usage: %s input.bin outdir | %s --time WARMUP input.bin [IDEALH_MAXITER IDEALH_TOL] | "
-                         "%s --ideal-h MAXITER TOL input.bin outdir\n", argv[0], argv[0], argv[0]);
+                         "%s --ideal-h MAXITER TOL input.bin outdir | %s --restart-dump input.bin restart.txt | "
+                         "%s --restart-load input.bin restart.txt outdir\n", argv[0], argv[0], argv[0], argv[0], argv[0]);
     return 2;
   }
   Input in;

@@ -6,6 +6,12 @@ in oracle/refshim), runs them and packs their raw outputs:
 
   reference_tables.npz      TableKernel, BSpline / Wendland C4, Dim<3>
                             geometry, mapPositionThroughPlanes (ref_tables)
+  reference_restart_<case>.npz  the reference's restart file (RestartRegistrar
+                            ::dumpState through FlatFileIO, ascii) after a few
+                            RK2 steps of one node set, and the state after
+                            the reference restored that file
+                            (RestartRegistrar::restoreState) and took more
+                            steps (ref_sph --restart-dump / --restart-load)
   reference_sph_<case>.npz  one node set run through the reference's
                             SPHHydroBase / CRKSPHHydroBase, ConnectivityMap,
                             periodic boundaries and CheapSynchronousRK2
@@ -159,6 +165,45 @@ def idealh_fixture(exe, name, ns, cfg, max_iterations=50, tolerance=1.0e-4):
     return out
 
 
+def restart_cases(pkg):
+    """name -> (node set, config, steps before the dump, steps after the
+    restore): SPH with compatible energy; SPH with grad-h, XSPH and no
+    compatible energy; CRKSPH with the CRKSPH Q; CRKSPH with the
+    Monaghan-Gingold Q."""
+    gen, abi = pkg.generators, pkg.abi
+    c = {}
+    c["sph_kh"] = _kh(gen, abi, 8, 8, 4) + (2, 2)
+    c["sph_sod_gradh_xsph_noncompatible"] = _sod(gen, abi, 16, 4, 4, gradhCorrection=1, XSPH=1,
+                                                 compatibleEnergyEvolution=0) + (2, 2)
+    c["crk_kh_crkq"] = _kh(gen, abi, 8, 8, 4, hydro=abi.HYDRO_CRKSPH, qType=abi.Q_CRKSPH_MONAGHAN_GINGOLD) + (2, 2)
+    c["crk_sod"] = _sod(gen, abi, 16, 4, 4, hydro=abi.HYDRO_CRKSPH) + (2, 2)
+    return c
+
+
+def restart_fixture(exe, name, ns, cfg, nsteps, nmore):
+    with tempfile.TemporaryDirectory() as td:
+        write_input(os.path.join(td, "a.bin"), cfg, ns, nsteps)
+        write_input(os.path.join(td, "b.bin"), cfg, ns, nmore)
+        rst = os.path.join(td, "restart.txt")
+        subprocess.check_call([exe, "--restart-dump", os.path.join(td, "a.bin"), rst], stdout=subprocess.DEVNULL)
+        os.makedirs(os.path.join(td, "cont", "steps"))
+        subprocess.check_call([exe, "--restart-load", os.path.join(td, "b.bin"), rst, os.path.join(td, "cont")],
+                              stdout=subprocess.DEVNULL)
+        with open(rst, "rb") as f:
+            text = f.read()
+        d = os.path.join(td, "cont", "steps")
+        cont = {"cont/" + f[:-4]: np.fromfile(os.path.join(d, f), dtype="<f8")
+                for f in sorted(os.listdir(d)) if f.endswith(".f64")}
+    data = {"input/config": np.frombuffer(bytes(cfg), dtype=np.uint8), "input/nsteps": np.int64(nsteps),
+            "input/nmore": np.int64(nmore), "input/position": ns.pos, "input/velocity": ns.vel,
+            "input/mass": ns.mass, "input/mass density": ns.rho, "input/specific thermal energy": ns.eps,
+            "input/H": ns.H, "restart": np.frombuffer(text, dtype=np.uint8)}
+    data.update(cont)
+    out = os.path.join(HERE, "reference_restart_%s.npz" % name)
+    np.savez_compressed(out, **data)
+    return out
+
+
 def main(argv):
     build_ref = importlib.import_module("build_ref")
     ref_sph, ref_tables = build_ref.build()
@@ -183,6 +228,10 @@ def main(argv):
         if want and name not in want:
             continue
         print(sph_fixture(ref_sph, name, ns, cfg, nsteps))
+    for name, (ns, cfg, nsteps, nmore) in restart_cases(pkg).items():
+        if want and "restart_" + name not in want:
+            continue
+        print(restart_fixture(ref_sph, name, ns, cfg, nsteps, nmore))
 
 
 if __name__ == "__main__":
