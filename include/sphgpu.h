@@ -134,6 +134,15 @@ int sphgpu_get_state(sphgpu_problem* p, double* position, double* velocity, doub
  * doubles in `out` and must equal n_internal * components. */
 int sphgpu_get_field(sphgpu_problem* p, const char* key, double* out, int64_t count);
 int sphgpu_field_components(const char* key, int32_t* components);
+/* Write a field by the same keys (host AoS, count = n_internal * components):
+ * the State or StateDerivatives value a caller carries in, e.g. a domain's
+ * derivatives from the last evaluation (FieldList assignment, as the
+ * reference's DistributedBoundary fills its ghost Fields).  A CRKSPH "node
+ * volume" written here stands for the start-up volume. */
+int sphgpu_set_field(sphgpu_problem* p, const char* key, const double* values, int64_t count);
+/* Integrator::dtMin / dtMax (src/Integrator/Integrator.hh) after creation,
+ * e.g. both set to a time step agreed between domains. */
+int sphgpu_set_dt_bounds(sphgpu_problem* p, double dt_min, double dt_max);
 
 /* Integrator::setGhostNodes (src/Integrator/Integrator.cc:445-597) without
  * ghost culling: periodic ghost images in boundary order x, y, z, then

@@ -17,3 +17,4 @@ from . import hydro  # noqa: F401
 from .hydro import SPHHydro, SPHBatch, CheapSynchronousRK2Integrator  # noqa: F401
 from . import serving  # noqa: F401
 from . import sharding  # noqa: F401
+from . import domains  # noqa: F401

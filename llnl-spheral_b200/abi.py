@@ -164,6 +164,8 @@ def load_library(path=None):
     lib.sphgpu_restart_dump.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p]
     lib.sphgpu_restart_restore.argtypes = [P, ctypes.c_char_p]
     lib.sphgpu_restart_labels.argtypes = [ctypes.POINTER(SphConfig), ctypes.c_char_p, I64]
+    lib.sphgpu_set_field.argtypes = [P, ctypes.c_char_p, P, I64]
+    lib.sphgpu_set_dt_bounds.argtypes = [P, ctypes.c_double, ctypes.c_double]
     lib.sphgpu_num_pairs.argtypes = [P, ctypes.POINTER(I64)]
     lib.sphgpu_pairs_evaluated.argtypes = [P, ctypes.POINTER(I64)]
     lib.sphgpu_kernel_launches.argtypes = [P, ctypes.POINTER(I64)]

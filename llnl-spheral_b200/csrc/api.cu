@@ -1123,6 +1123,47 @@ int sphgpu_get_field(sphgpu_problem* p, const char* key, double* out, int64_t co
   return download_aos(*p, f->array == 0 ? p->S : (f->array == 1 ? p->D : p->K), f->comps, f->field, out);
 }
 
+int sphgpu_set_field(sphgpu_problem* p, const char* key, const double* values, int64_t count) {
+  if (p == nullptr || values == nullptr) return SPHGPU_ERR_ARG;
+  const FieldSpec* f = findField(key);
+  if (f == nullptr) { set_error(std::string("unknown field key: ") + (key ? key : "(null)")); return SPHGPU_ERR_ARG; }
+  if (count != p->n*f->comps) { set_error("sphgpu_set_field: count mismatch"); return SPHGPU_ERR_ARG; }
+  const bool crk = p->cfg.hydro == SPHGPU_HYDRO_CRKSPH;
+  if (f->array == 2) {
+    if (!crk) { set_error("CRKSPH fields exist for CRKSPH problems only"); return SPHGPU_ERR_STATE; }
+    if (p->K == nullptr) {
+      if (dev_alloc(reinterpret_cast<void**>(&p->K), sizeof(double)*NCRK*(size_t)p->n) != cudaSuccess) {
+        set_error("CRKSPH field allocation failed");
+        return SPHGPU_ERR_NOMEM;
+      }
+      SPH_CHECK(cudaMemsetAsync(p->K, 0, sizeof(double)*NCRK*(size_t)p->n, p->stream));
+    }
+  }
+  double* base = f->array == 0 ? p->S : (f->array == 1 ? p->D : p->K);
+  const int64_t cnt = count;
+  SPH_CHECK(cudaMemcpyAsync(p->staging, values, sizeof(double)*(size_t)cnt, cudaMemcpyHostToDevice, p->stream));
+  aos_to_soa_kernel<<<grid1(cnt), 256, 0, p->stream>>>(p->staging, f->comps, p->n, base + (int64_t)f->field*p->n);
+  ++p->launches;
+  SPH_CHECK(cudaGetLastError());
+  SPH_CHECK(cudaStreamSynchronize(p->stream));
+  if (f->array == 1) p->haveDerivs = true;
+  // a CRKSPH node volume given by the caller replaces the start-up volume
+  if (f->array == 0 && f->field == S_VOL && crk) p->crkVolumeReady = true;
+  return SPHGPU_OK;
+}
+
+int sphgpu_set_dt_bounds(sphgpu_problem* p, double dt_min, double dt_max) {
+  if (p == nullptr || !(dt_min > 0.0) || !(dt_max >= dt_min)) {
+    set_error("sphgpu_set_dt_bounds: need 0 < dt_min <= dt_max");
+    return SPHGPU_ERR_ARG;
+  }
+  p->cfg.dtMin = dt_min;
+  p->cfg.dtMax = dt_max;
+  p->prm.dtMin = dt_min;
+  p->prm.dtMax = dt_max;
+  return SPHGPU_OK;
+}
+
 int sphgpu_build_neighbors(sphgpu_problem* p) {
   if (p == nullptr) return SPHGPU_ERR_ARG;
   SPH_TRY(build_neighbors_impl(solo(p)));

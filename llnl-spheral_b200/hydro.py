@@ -90,6 +90,14 @@ class SPHHydro:
         abi.check(self.lib.sphgpu_get_field(self.h, key.encode(), _p(out), out.size), self.lib)
         return out.reshape(self.n, c) if c > 1 else out
 
+    def set_field(self, key, values):
+        """Write a State / StateDerivatives field by its key (n x components)."""
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        abi.check(self.lib.sphgpu_set_field(self.h, key.encode(), _p(v), v.size), self.lib)
+
+    def set_dt_bounds(self, dt_min, dt_max):
+        abi.check(self.lib.sphgpu_set_dt_bounds(self.h, float(dt_min), float(dt_max)), self.lib)
+
     # ---- Integrator::setGhostNodes + ConnectivityMap
     def build_neighbors(self):
         abi.check(self.lib.sphgpu_build_neighbors(self.h), self.lib)
