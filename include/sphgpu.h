@@ -154,6 +154,18 @@ int sphgpu_connectivity_size(sphgpu_problem* p, int64_t* num_ghosts, int64_t* nu
  * internal node it images (ghost_root[num_ghosts]).  Any pointer may be NULL. */
 int sphgpu_get_connectivity(sphgpu_problem* p, int64_t* offsets, int32_t* neighbors,
                             int32_t* ghost_root);
+/* The pair-wise accelerations of the last derivative evaluation on the
+ * current ConnectivityMap (the reference's HydroFieldNames::pairAccelerations
+ * derivative, filled by SPHHydroBase::evaluateDerivatives,
+ * src/SPH/SPHHydroBase.cc:773-777): out[3k..3k+2] for ConnectivityMap entry k
+ * (node i's row in the order of sphgpu_get_connectivity).  Where node i owns
+ * the pair (neighbor j > i or a ghost) the value is the reference's
+ * -m_j deltaDvDt bit for bit; otherwise it is m_j deltaDvDt formed from the
+ * owner's value (the reference's SpecificThermalEnergyPolicy reads only the
+ * owner's entries).  count must be 3 x the entries.  Only problems that
+ * evolve energy compatibly keep them (SPHGPU_ERR_UNSUPPORTED otherwise);
+ * after a neighbor build without an evaluation, SPHGPU_ERR_STATE. */
+int sphgpu_get_pair_accelerations(sphgpu_problem* p, double* out, int64_t count);
 /* Positions of the ghost nodes of the current connectivity (3 doubles per
  * ghost, in ghost order): the NodeList's ghost "position" values, each its
  * root's position mapped through the periodic planes as

@@ -150,6 +150,7 @@ def load_library(path=None):
     lib.sphgpu_connectivity_size.argtypes = [P, ctypes.POINTER(I64), ctypes.POINTER(I64)]
     lib.sphgpu_get_connectivity.argtypes = [P, P, P, P]
     lib.sphgpu_get_ghost_positions.argtypes = [P, P]
+    lib.sphgpu_get_pair_accelerations.argtypes = [P, P, I64]
     for name in ("sphgpu_initialize", "sphgpu_evaluate_derivatives", "sphgpu_finalize_derivatives",
                  "sphgpu_finalize"):
         getattr(lib, name).argtypes = [P, ctypes.c_double, ctypes.c_double]

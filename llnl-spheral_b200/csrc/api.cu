@@ -377,6 +377,7 @@ int require_nbrs(Batch& b) {
 }
 
 int launch_eval(Batch& b) {
+  for (Problem* p : b.mem) p->paccReady = p->pacc != nullptr;
   if (anyMember(b, isCrkP)) {
     SPH_TRY(crk_prepare(b));
     SPH_TRY(launch_crk_eval(b));
@@ -1186,6 +1187,54 @@ int sphgpu_get_connectivity(sphgpu_problem* p, int64_t* offsets, int32_t* neighb
   if (neighbors && p->E) SPH_CHECK(cudaMemcpyAsync(neighbors, p->nbr, sizeof(int32_t)*(size_t)p->E, cudaMemcpyDeviceToHost, p->stream));
   if (ghost_root && p->G) SPH_CHECK(cudaMemcpyAsync(ghost_root, p->groot, sizeof(int32_t)*(size_t)p->G, cudaMemcpyDeviceToHost, p->stream));
   SPH_CHECK(cudaStreamSynchronize(p->stream));
+  return SPHGPU_OK;
+}
+
+int sphgpu_get_pair_accelerations(sphgpu_problem* p, double* out, int64_t count) {
+  if (p == nullptr || (out == nullptr && count > 0)) return SPHGPU_ERR_ARG;
+  SPH_TRY(require_nbrs(solo(p)));
+  if (p->pacc == nullptr) {
+    set_error("pair accelerations are kept only with compatible energy evolution");
+    return SPHGPU_ERR_UNSUPPORTED;
+  }
+  if (!p->paccReady) {
+    set_error("no derivative evaluation on the current connectivity");
+    return SPHGPU_ERR_STATE;
+  }
+  if (count != 3*p->E) {
+    set_error("pair accelerations: count must be 3 x the ConnectivityMap entries");
+    return SPHGPU_ERR_ARG;
+  }
+  const int64_t n = p->n, E = p->E;
+  std::vector<int64_t> off((size_t)n + 1);
+  std::vector<int32_t> nb((size_t)E);
+  std::vector<double> m((size_t)n), pa(3*(size_t)E);
+  std::vector<float> paF;
+  const bool mixed = p->cfg.precision == SPHGPU_PRECISION_MIXED;
+  SPH_CHECK(cudaMemcpyAsync(off.data(), p->offsets, sizeof(int64_t)*(size_t)(n + 1), cudaMemcpyDeviceToHost, p->stream));
+  if (E) SPH_CHECK(cudaMemcpyAsync(nb.data(), p->nbr, sizeof(int32_t)*(size_t)E, cudaMemcpyDeviceToHost, p->stream));
+  SPH_CHECK(cudaMemcpyAsync(m.data(), p->S + S_M*n, sizeof(double)*(size_t)n, cudaMemcpyDeviceToHost, p->stream));
+  if (mixed) paF.resize(3*(size_t)E);
+  for (int a = 0; a < 3 && E; ++a) {
+    if (mixed)
+      SPH_CHECK(cudaMemcpyAsync(paF.data() + a*E, reinterpret_cast<const float*>(p->pacc) + a*p->ecap,
+                                sizeof(float)*(size_t)E, cudaMemcpyDeviceToHost, p->stream));
+    else
+      SPH_CHECK(cudaMemcpyAsync(pa.data() + a*E, p->pacc + a*p->ecap, sizeof(double)*(size_t)E,
+                                cudaMemcpyDeviceToHost, p->stream));
+  }
+  SPH_CHECK(cudaStreamSynchronize(p->stream));
+  if (mixed) for (size_t t = 0; t < paF.size(); ++t) pa[t] = (double)paF[t];
+  // entry k of node i's row stores the owner's pair acceleration
+  // -m_other deltaDvDt; the reference's vector of node i holds that for the
+  // pairs i owns and m_owner deltaDvDt for the others
+  for (int64_t i = 0; i < n; ++i) {
+    for (int64_t k = off[i]; k < off[i + 1]; ++k) {
+      const int32_t j = nb[k];
+      const double s = j > (int32_t)i ? 1.0 : -(m[j]/m[i]);
+      for (int a = 0; a < 3; ++a) out[3*k + a] = s == 1.0 ? pa[a*E + k] : pa[a*E + k]*s;
+    }
+  }
   return SPHGPU_OK;
 }
 

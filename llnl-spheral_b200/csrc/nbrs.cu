@@ -44,6 +44,10 @@ constexpr float kFilterTol = 1.0e-3f;
 // shared memory for the per-thread lists of a 32-thread block (larger lists
 // take the warp schedule)
 constexpr size_t kMaxListSmem = 200*1024;
+// blocks of 256 threads per SM the thread walk is compiled for
+#ifndef NBR_THREAD_MIN_BLOCKS
+#define NBR_THREAD_MIN_BLOCKS 4
+#endif
 
 __device__ __forceinline__ unsigned long long orderedBits(double v) {
   const unsigned long long b = (unsigned long long)__double_as_longlong(v);
@@ -383,7 +387,10 @@ __global__ void __launch_bounds__(kGhostThreads) cell_index_kernel(const Member*
 
 // Cell-ordered candidate arrays (Problem::cand), one slot per node:
 //   pre     [candcap] float4:   FP32 offsets of the position from the lower
-//                               corner of the node's cell, FP32 min eig(H)
+//                               corner of the node's cell, and
+//                               k2hi/min eig(H)^2 (k2hi the upper edge of the
+//                               pre-test band): beyond that r^2 the node's own
+//                               eta^2 lies above the band
 //   lmax    [candcap] float:    FP32 max eig(H)
 // and sortedIdx[slot], the node of each slot.  The walks read only `pre` for
 // most candidates; `lmax` when the i-side test alone does not decide, and
@@ -414,7 +421,7 @@ __device__ __forceinline__ float symEta2F(const float* h, float x, float y, floa
 struct Walker {
   float hf[6];
   float lam2;          // isotropic H = lam I: lam^2 (then eta_i^2 = lam^2 |r|^2)
-  float lmin;          // min eig(H)
+  float T;             // k2hi/min eig(H)^2: beyond r^2 = T the node's own eta^2 exceeds the band
   bool iso;
   float ox, oy, oz;
   int cx, cy, cz;
@@ -436,7 +443,7 @@ __device__ __forceinline__ Walker makeWalker(const Member& M, const NbrArrays& a
   w.lam2 = w.hf[0]*w.hf[0];
   const float4 p = __ldg(a.pre + s);
   w.ox = p.x; w.oy = p.y; w.oz = p.z;
-  w.lmin = p.w;
+  w.T = p.w;
   w.cx = cellCoord(r.x, g.lo[0], g.cell, g.dim[0]);
   w.cy = cellCoord(r.y, g.lo[1], g.cell, g.dim[1]);
   w.cz = cellCoord(r.z, g.lo[2], g.cell, g.dim[2]);
@@ -515,7 +522,9 @@ __device__ __forceinline__ bool exactTest(const Member& M, int32_t i, int32_t j,
 // exact FP64 test in the reference's operation order.  eta^2 of either node
 // lies in [min eig(H)^2 r^2, max eig(H)^2 r^2]: a candidate beyond the band
 // for the smaller of the two minimum eigenvalues is rejected from r^2 alone
-// (most candidates of the window).
+// (most candidates of the window); each record carries that r^2 bound,
+// k2hi/min eig(H)^2, so the test is one comparison with the larger of the
+// two nodes' bounds.
 __device__ __forceinline__ bool candTest(const Member& M, const NbrArrays& a, const Walker& w, int32_t k,
                                          float dxc, float dyc, float dzc, double k2, float k2lo, float k2hi,
                                          bool pretest) {
@@ -523,13 +532,12 @@ __device__ __forceinline__ bool candTest(const Member& M, const NbrArrays& a, co
     const float4 c = __ldg(a.pre + k);
     const float fx = (w.ox - c.x) - dxc, fy = (w.oy - c.y) - dyc, fz = (w.oz - c.z) - dzc;
     const float r2 = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, fz*fz));
-    const float lo = fminf(w.lmin, c.w);
-    if (lo*lo*r2 > k2hi) return false;
+    if (r2 > fmaxf(w.T, c.w)) return false;
     float e2i;
     if (w.iso) e2i = w.lam2*r2;          // the common case: H = lam I
     else e2i = symEta2F(w.hf, fx, fy, fz);
     if (e2i <= k2lo) return true;
-    if (e2i > k2hi && c.w*c.w*r2 > k2hi) return false;
+    if (e2i > k2hi && r2 > c.w) return false;
     const float lm = __ldg(a.lmax + k);
     if (lm*lm*r2 <= k2lo) return true;
   }
@@ -543,6 +551,9 @@ __global__ void __launch_bounds__(kGhostThreads) cell_scatter_kernel(const Membe
   double* base = static_cast<double*>(M.cand);
   float4* pre = reinterpret_cast<float4*>(base);
   float* lmax = reinterpret_cast<float*>(base + 2*M.candcap);
+  // the pre-test's upper band edge, as the walks form it
+  const float k2f = (float)(M.prm.kernelExtent*M.prm.kernelExtent);
+  const double k2hi = (double)(k2f*(1.0f + g.filterTol));
   FOR_ITEMS(k, allNodes(M)) {
     const int c = M.cidx[k];
     const int64_t slot = M.cellStart[c] + atomicAdd(M.cellFill + c, 1);
@@ -552,8 +563,9 @@ __global__ void __launch_bounds__(kGhostThreads) cell_scatter_kernel(const Membe
     const int cy = cellCoord(r.y, g.lo[1], g.cell, g.dim[1]);
     const int cz = cellCoord(r.z, g.lo[2], g.cell, g.dim[2]);
     const int64_t root = k < M.n ? k : M.groot[k - M.n];
+    const double hm = M.hmaxi[root];
     pre[slot] = make_float4((float)(r.x - (g.lo[0] + cx*g.cell)), (float)(r.y - (g.lo[1] + cy*g.cell)),
-                            (float)(r.z - (g.lo[2] + cz*g.cell)), (float)(1.0/M.hmaxi[root]));
+                            (float)(r.z - (g.lo[2] + cz*g.cell)), (float)(k2hi*hm*hm));
     lmax[slot] = (float)M.hmaxi[M.n + root];
   }
 }
@@ -571,7 +583,7 @@ __global__ void __launch_bounds__(kGhostThreads) cell_scatter_kernel(const Membe
 // at stash[c*stashStride + s]; nbr_compact_thread_kernel then moves them to
 // offsets[i], and the FILL pass does not run for it.
 template<bool FILL, int SUB>
-__global__ void __launch_bounds__(256, SUB == 1 ? 4 : 1) nbr_thread_kernel(const Member* mem, BlockMap bm, int cap, int maxNbr) {
+__global__ void __launch_bounds__(256, SUB == 1 ? NBR_THREAD_MIN_BLOCKS : 1) nbr_thread_kernel(const Member* mem, BlockMap bm, int cap, int maxNbr) {
   extern __shared__ int32_t lst[];
   const MemberBlock mb = memberBlock(bm);
   const Member& M = mem[mb.m];
@@ -601,39 +613,41 @@ __global__ void __launch_bounds__(256, SUB == 1 ? 4 : 1) nbr_thread_kernel(const
     // window of +-SUB cells; with SUB > 1 the rows and cells farther than the
     // largest kernel reach (in cells, with a margin) are skipped
     const float rc2 = g.reach*g.reach*1.0001f;
-    const float fx = me.ox/cellf, fy = me.oy/cellf, fz = me.oz/cellf;
-    for (int dz = -SUB; dz <= SUB; ++dz) {
-      const int z = me.cz + dz;
-      if (z < 0 || z >= g.dim[2]) continue;
-      const float gz = axisGap(dz, fz);
-      const float dzc = (float)dz*cellf;
-      for (int dy = -SUB; dy <= SUB; ++dy) {
-        const int y = me.cy + dy;
-        if (y < 0 || y >= g.dim[1]) continue;
-        const float gy = axisGap(dy, fy);
-        const float gyz = gy*gy + gz*gz;
-        if (SUB > 1 && gyz > rc2) continue;
-        const float dyc = (float)dy*cellf;
-        const Row<SUB> row = loadRow<SUB>(M, g, me, y, z, fx, gyz, rc2);
-        {
-          for (int32_t k = row.start; k < row.end; ++k) {
-          if (k != s && candTest(M, a, me, k, rowDxc<SUB>(row, me, k, cellf), dyc, dzc, k2, k2lo, k2hi, pretest)) {
-            if (collect) {
-              const int32_t j = __ldg(M.sortedIdx + k);
-              if (count < lcap) {
-                int p = count;
-                while (p > 0) {
-                  const int32_t prev = lst[(p - 1)*bd + tid];
-                  if (prev < j) break;
-                  lst[p*bd + tid] = prev;
-                  --p;
-                }
-                lst[p*bd + tid] = j;
-              }
-              above += (j > i);
-            }
-            ++count;
+    auto accept = [&](int32_t k) {
+      if (collect) {
+        const int32_t j = __ldg(M.sortedIdx + k);
+        if (count < lcap) {
+          int p = count;
+          while (p > 0) {
+            const int32_t prev = lst[(p - 1)*bd + tid];
+            if (prev < j) break;
+            lst[p*bd + tid] = prev;
+            --p;
           }
+          lst[p*bd + tid] = j;
+        }
+        above += (j > i);
+      }
+      ++count;
+    };
+    {
+      const float fx = me.ox/cellf, fy = me.oy/cellf, fz = me.oz/cellf;
+      for (int dz = -SUB; dz <= SUB; ++dz) {
+        const int z = me.cz + dz;
+        if (z < 0 || z >= g.dim[2]) continue;
+        const float gz = axisGap(dz, fz);
+        const float dzc = (float)dz*cellf;
+        for (int dy = -SUB; dy <= SUB; ++dy) {
+          const int y = me.cy + dy;
+          if (y < 0 || y >= g.dim[1]) continue;
+          const float gy = axisGap(dy, fy);
+          const float gyz = gy*gy + gz*gz;
+          if (SUB > 1 && gyz > rc2) continue;
+          const float dyc = (float)dy*cellf;
+          const Row<SUB> row = loadRow<SUB>(M, g, me, y, z, fx, gyz, rc2);
+          for (int32_t k = row.start; k < row.end; ++k) {
+            if (k != s && candTest(M, a, me, k, rowDxc<SUB>(row, me, k, cellf), dyc, dzc, k2, k2lo, k2hi, pretest))
+              accept(k);
           }
         }
       }
@@ -919,6 +933,7 @@ namespace {
 int launch_build(Batch& b) {
   cudaStream_t st = b.stream;
   const int nm = (int)b.mem.size();
+  for (Problem* p : b.mem) p->paccReady = false;   // the walk parks its lists in pacc
   // (a captured build reads the descriptor slot uploaded before the capture)
   if (!b.capturing) SPH_TRY(batch_upload(b));
   // ---- ghosts: six planar boundaries in order, sizes kept on the device

@@ -298,6 +298,7 @@ struct Problem {
   int64_t launches = 0;         // kernels launched for this problem (diagnostics)
   bool haveNbrs = false;
   bool haveDerivs = false;
+  bool paccReady = false;       // pacc holds the pair accelerations of an evaluation on the current connectivity
   double time = 0.0;
   double lastDt = 1e-5;
   int64_t cycle = 0;

@@ -114,6 +114,17 @@ class SPHHydro:
         abi.check(self.lib.sphgpu_get_connectivity(self.h, _p(off), _p(nb), _p(root)), self.lib)
         return off, nb[:e.value], root[:g.value]
 
+    def pair_accelerations(self):
+        """The reference's pair-wise accelerations of the last evaluation, one
+        row per ConnectivityMap entry in row order, (E, 3)
+        (sphgpu_get_pair_accelerations)."""
+        g = ctypes.c_int64()
+        e = ctypes.c_int64()
+        abi.check(self.lib.sphgpu_connectivity_size(self.h, ctypes.byref(g), ctypes.byref(e)), self.lib)
+        out = np.empty((max(e.value, 1), 3))
+        abi.check(self.lib.sphgpu_get_pair_accelerations(self.h, _p(out), 3 * e.value), self.lib)
+        return out[:e.value]
+
     def ghost_positions(self):
         """Ghost node positions of the current connectivity, (G, 3)."""
         g = ctypes.c_int64()

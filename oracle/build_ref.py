@@ -7,6 +7,11 @@ installed here), into oracle/_ref/:
 
   ref_tables  TableKernel, BSpline / Wendland C4, Dim<3> geometry, GeomPlane
               and mapPositionThroughPlanes (oracle/refshim/ref_tables.cc)
+  ref_sph_gpu ref_sph with the drop-in adapter
+              llnl-spheral_b200/spheral/GpuSPHHydroBase.hh in place of
+              SPHHydroBase (its evaluateDerivatives on the GPU through
+              llnl-spheral_b200/_build/libsphgpu.so, found at run time by a
+              relative rpath); built when that library exists
   ref_sph     the whole SPH / CRKSPH fluid path: FluidNodeList,
               NestedGridNeighbor, ConnectivityMap, PeriodicBoundary, DataBase,
               State and its update policies, SPHHydroBase, CRKSPHHydroBase, the
@@ -37,6 +42,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 SHIM = os.path.join(HERE, "refshim")
 INCLUDE = os.path.join(HERE, "..", "include")
+PKG = os.path.join(HERE, "..", "llnl-spheral_b200")
 
 
 def reference_src():
@@ -273,6 +279,22 @@ def build(jobs=None, quiet=True):
         if os.path.exists(path) and all(os.path.getmtime(path) >= os.path.getmtime(o) for o in objs):
             continue
         subprocess.check_call([cxx, "-o", path] + objs)
+    # the same driver with the GPU adapter, linked against the CUDA library
+    lib = os.path.join(PKG, "_build", "libsphgpu.so")
+    if os.path.exists(lib):
+        tu = os.path.join(SHIM, "ref_sph.cc")
+        obj = os.path.join(objdir, "ref_sph_gpu.o")
+        adapter = os.path.join(PKG, "spheral", "GpuSPHHydroBase.hh")
+        _, rc, err = _compile((cxx, cflags + ["-DREF_SPH_GPU", "-I" + os.path.join(PKG, "spheral")], tu, obj,
+                               [tu, adapter] + shim))
+        if rc:
+            raise RuntimeError("ref_sph_gpu build failed:\n" + err[-4000:])
+        path = os.path.join(OUT, "ref_sph_gpu")
+        objs = unit_objs + [os.path.join(objdir, "ref_stubs.o"), obj]
+        if not (os.path.exists(path) and all(os.path.getmtime(path) >= os.path.getmtime(o) for o in objs + [lib])):
+            rpath = os.path.relpath(os.path.dirname(lib), OUT)
+            subprocess.check_call([cxx, "-o", path] + objs + ["-L" + os.path.dirname(lib), "-lsphgpu",
+                                                              "-Wl,-rpath,$ORIGIN/" + rpath])
     if not quiet:
         print(os.path.join(OUT, "ref_sph"))
     return os.path.join(OUT, "ref_sph"), os.path.join(OUT, "ref_tables")

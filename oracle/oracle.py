@@ -111,6 +111,13 @@ class OracleProblem:
         self.L.orc_get_connectivity(self.h, _p(off), _p(nb), _p(root))
         return off, nb[:e], root[:self.num_ghosts()]
 
+    def pair_accelerations(self):
+        """The reference's pair-wise accelerations, (E, 3) in row order."""
+        e = self.L.orc_num_entries(self.h)
+        out = np.zeros((max(e, 1), 3))
+        self.L.orc_get_pair_accelerations(self.h, _p(out))
+        return out[:e]
+
     def ghost_positions(self):
         g = np.zeros((max(self.num_ghosts(), 1), 3))
         self.L.orc_get_ghost_positions(self.h, _p(g))

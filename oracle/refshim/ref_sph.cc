@@ -39,6 +39,11 @@
 // internal nodes' position[3n], velocity[3n], mass[n], mass density[n],
 // specific thermal energy[n], H[6n] (float64, the reference Field layouts).
 // Writes raw little-endian arrays (name.f64 / name.i64) into outdir.
+// Built a second time with -DREF_SPH_GPU (oracle/_ref/ref_sph_gpu): the same
+// driver with GpuSPHHydroBase, the reference's SPHHydroBase whose
+// evaluateDerivatives runs on the GPU through libsphgpu.so, in place of
+// SPHHydroBase: the reference's integrator, policies and boundaries driving
+// the device derivatives.
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -76,6 +81,9 @@
 #include "DataOutput/RestartRegistrar.hh"
 
 #include "sphgpu.h"
+#ifdef REF_SPH_GPU
+#include "GpuSPHHydroBase.hh"
+#endif
 
 using namespace Spheral;
 typedef Dim<3> D;
@@ -433,12 +441,23 @@ int main(int argc, char** argv) {
     Q.epsilon2(cfg.epsilon2);
     // SPHHydroBase (src/SPH/SPHHydroBase.hh:53-71): filter 0, total energy off,
     // sumMassDensityOverAllNodeLists (one NodeList), unbounded box.
+#ifdef REF_SPH_GPU
+    // the same package with its evaluateDerivatives on the GPU (the drop-in
+    // adapter llnl-spheral_b200/spheral/GpuSPHHydroBase.hh); everything else
+    // stays the reference's
+    SPHSpace::GpuSPHHydroBase<D> hydro(cfg, smooth, Q, WT, WT, 0.0, cfg.cfl, cfg.useVelocityMagnitudeForDt != 0,
+#else
     SPHSpace::SPHHydroBase<D> hydro(smooth, Q, WT, WT, 0.0, cfg.cfl, cfg.useVelocityMagnitudeForDt != 0,
+#endif
                                     cfg.compatibleEnergyEvolution != 0, false, cfg.gradhCorrection != 0, cfg.XSPH != 0,
                                     cfg.correctVelocityGradient != 0, true, densityUpdate, HUpdate,
                                     cfg.epsTensile, cfg.nTensile, Vector(-1e100, -1e100, -1e100), Vector(1e100, 1e100, 1e100));
     return run(in, hydro, nodes, db);
   }
+#ifdef REF_SPH_GPU
+  std::fprintf(stderr, "the GPU adapter covers SPHHydroBase only\n");
+  return 2;
+#endif
   // CRKSPHHydroBase (src/CRKSPH/CRKSPHHydroBase.hh:59-78): filter 0, linear
   // order, no surface detection.
   std::unique_ptr<ArtificialViscositySpace::ArtificialViscosity<D> > Q;

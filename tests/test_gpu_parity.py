@@ -254,3 +254,38 @@ def test_connectivity_anisotropic_h(gpu_lib, pkg, oracle_mod, nfilter, cells):
     go, gn, gr = g.connectivity()
     oo, on, orr = o.connectivity()
     assert np.array_equal(go, oo) and np.array_equal(gn, on) and np.array_equal(gr, orr)
+
+
+@pytest.mark.parametrize("case", ["sod", "kh"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_pair_accelerations_reference_layout(gpu_lib, pkg, oracle_mod, case, precision):
+    """sphgpu_get_pair_accelerations against the oracle's pair-wise
+    accelerations (the reference's layout, bit-pinned to the reference): the
+    entries of the pairs a node owns (neighbor j > i or a ghost) are
+    bit-identical in FP64; the others (m_owner deltaDvDt formed from the
+    owner's value) agree to rounding.  Before an evaluation on the current
+    connectivity there are none to read."""
+    g, o, ns = _pair(pkg, oracle_mod, case)
+    g.build_neighbors()
+    with pytest.raises(RuntimeError):
+        g.pair_accelerations()
+    if precision == "mixed":
+        gen, abi = pkg.generators, pkg.abi
+        ns2, cfg2 = CASES[case](gen, abi)
+        cfg2.precision = abi.PRECISION_MIXED
+        g = pkg.SPHHydro(cfg2, ns2)
+        g.build_neighbors()
+    g.evaluateDerivatives()
+    o.build_neighbors()
+    o.evaluate_derivatives()
+    off, nb, _ = g.connectivity()
+    row = np.repeat(np.arange(ns.n), np.diff(off))
+    own = nb > row
+    a, b = g.pair_accelerations(), o.pair_accelerations()
+    assert a.shape == b.shape
+    scale = np.max(np.abs(b))
+    if precision == "fp64":
+        assert np.array_equal(a[own], b[own])
+        assert np.max(np.abs(a[~own] - b[~own])) <= 1e-14 * scale
+    else:
+        assert np.max(np.abs(a - b)) <= 1e-5 * scale
