@@ -755,32 +755,65 @@ __global__ void __launch_bounds__(256, SUB == 1 ? 3 : 1) nbr_walk_kernel(const M
   const float cellf = (float)g.cell;
   const float rc2 = g.reach*g.reach*1.0001f;
   const float fx = me.ox/cellf, fy = me.oy/cellf, fz = me.oz/cellf;
-  int count = 0;
-  for (int dz = -SUB; dz <= SUB; ++dz) {
-    const int z = me.cz + dz;
-    if (z < 0 || z >= g.dim[2]) continue;
-    const float gz = axisGap(dz, fz);
-    const float dzc = (float)dz*cellf;
-    for (int dy = -SUB; dy <= SUB; ++dy) {
-      const int y = me.cy + dy;
-      if (y < 0 || y >= g.dim[1]) continue;
-      const float gy = axisGap(dy, fy);
+  // The window's rows, one per lane (rows outside the grid or, with SUB > 1,
+  // beyond the kernel reach are empty), their candidates numbered in one
+  // sequence by a warp scan: the lanes then take 32 consecutive candidates at
+  // a time across row ends, so a warp iteration tests 32 candidates however
+  // short the rows are.
+  constexpr int NR = (2*SUB + 1)*(2*SUB + 1);
+  constexpr int RW = 3 + 2*SUB;                       // start, first candidate number, x0, cell ends
+  __shared__ int32_t rowTab[256/32][NR*RW];
+  int32_t* R = rowTab[wib];
+  int len = 0;
+  if (lane < NR) {
+    const int dy = lane % (2*SUB + 1) - SUB, dz = lane/(2*SUB + 1) - SUB;
+    const int y = me.cy + dy, z = me.cz + dz;
+    if (y >= 0 && y < g.dim[1] && z >= 0 && z < g.dim[2]) {
+      const float gy = axisGap(dy, fy), gz = axisGap(dz, fz);
       const float gyz = gy*gy + gz*gz;
-      if (SUB > 1 && gyz > rc2) continue;
-      const float dyc = (float)dy*cellf;
-      const Row<SUB> row = loadRow<SUB>(M, g, me, y, z, fx, gyz, rc2);
-      for (int32_t base = row.start; base < row.end; base += 32) {
-        const int32_t k = base + lane;
-        const bool pass = k < row.end && k != s &&
-                          candTest(M, a, me, k, rowDxc<SUB>(row, me, k, cellf), dyc, dzc, k2, k2lo, k2hi, pretest);
-        const unsigned ballot = __ballot_sync(0xffffffffu, pass);
-        if (collect && pass) {
-          const int pos = count + __popc(ballot & ((1u << lane) - 1u));
-          if (pos < cap) sbuf[pos] = __ldg(M.sortedIdx + k);
-        }
-        count += __popc(ballot);
+      if (SUB == 1 || gyz <= rc2) {
+        const Row<SUB> row = loadRow<SUB>(M, g, me, y, z, fx, gyz, rc2);
+        len = row.end > row.start ? row.end - row.start : 0;
+        R[lane*RW] = row.start;
+        R[lane*RW + 2] = row.x0;
+#pragma unroll
+        for (int c = 0; c < 2*SUB; ++c) R[lane*RW + 3 + c] = row.e[c];
       }
     }
+  }
+  int incl = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane < NR) R[lane*RW + 1] = incl - len;
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  __syncwarp();
+  int count = 0;
+  int r = 0;                                          // the lane's row (lanes only move forward)
+  for (int base = 0; base < total; base += 32) {
+    const int t = base + lane;
+    bool pass = false;
+    int32_t k = 0;
+    if (t < total) {
+      while (r + 1 < NR && R[(r + 1)*RW + 1] <= t) ++r;
+      const int32_t* row = R + r*RW;
+      k = row[0] + (t - row[1]);
+      if (k != s) {
+        int xc = row[2] - me.cx;
+#pragma unroll
+        for (int c = 0; c < 2*SUB; ++c) xc += (k >= row[3 + c]);
+        const float dyc = (float)(r % (2*SUB + 1) - SUB)*cellf, dzc = (float)(r/(2*SUB + 1) - SUB)*cellf;
+        pass = candTest(M, a, me, k, (float)xc*cellf, dyc, dzc, k2, k2lo, k2hi, pretest);
+      }
+    }
+    const unsigned ballot = __ballot_sync(0xffffffffu, pass);
+    if (collect && pass) {
+      const int pos = count + __popc(ballot & ((1u << lane) - 1u));
+      if (pos < cap) sbuf[pos] = __ldg(M.sortedIdx + k);
+    }
+    count += __popc(ballot);
   }
   if (!FILL) {
     if (lane == 0) {

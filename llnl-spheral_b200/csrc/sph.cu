@@ -125,8 +125,87 @@ __global__ void __launch_bounds__(256) pack_mixed_kernel(const Member* mem, Bloc
 }
 
 // ---------------------------------------------------------------- derivatives
-// One directed pair (i, j) of SPHHydroBase::evaluateDerivatives, formed in
-// owner orientation, accumulated into node i.
+// The terms of one directed pair (i, j) that node i's sums take, formed in
+// owner orientation (own: i owns the pair, j > i).  The reference forms every
+// pair term from the owner A and the other node B.  Here each quantity is
+// formed once for node i and once for node j, with the same operands in the
+// same order: with the owner-oriented separation r_ij = r_A - r_B (= r_i -
+// r_j or its exact negation), eta_i = H_i r_ij is eta_A when i owns the pair
+// and eta_B otherwise, and likewise for j.  Sums of two pair terms are
+// commutative and keep their bits; where three or more are added the owner's
+// order is selected explicitly.
+struct PairTerms {
+  V3 rij, vij, gradWI, dd;      // dd: deltaDvDt
+  double WI, WJ, gWI, thptS, QI, workQI, PrhoI, mj, mrhoj;
+  bool own;
+};
+
+template<bool TENSILE>
+__device__ __forceinline__ PairTerms pairTerms(const Rec& I, bool isoI, const Rec& J, bool own, const Params& P,
+                                               double Cl, double Cq) {
+  PairTerms t;
+  t.own = own;
+  t.mj = J.m;
+  t.mrhoj = J.mrho;
+  const V3 d = vsub(I.r, J.r);
+  const V3 rij = own ? d : V3{-d.x, -d.y, -d.z};
+  const V3 dv = vsub(I.v, J.v);
+  const V3 vij = own ? dv : V3{-dv.x, -dv.y, -dv.z};
+  t.rij = rij;
+  t.vij = vij;
+  // H = h I (the common case): every H product reduces to a scaling with
+  // the same bits (the off-diagonal terms add exact zeros)
+  const bool iso = isoI && isoSym(J.H);
+  const V3 etaI = iso ? vmul(rij, I.H.xx) : sdot(I.H, rij);
+  const V3 etaJ = iso ? vmul(rij, J.H.xx) : sdot(J.H, rij);
+  const V3 uI = unitVector(etaI), uJ = unitVector(etaJ);
+  const V3 HetaI = iso ? vmul(uI, I.H.xx) : sdot(I.H, uI);
+  const V3 HetaJ = iso ? vmul(uJ, J.H.xx) : sdot(J.H, uJ);
+  double WI, gWI, WJ, gWJ;
+  tableKernelAndGrad(P.W, mag(etaI), I.Hdet, WI, gWI);
+  tableKernelAndGrad(P.W, mag(etaJ), J.Hdet, WJ, gWJ);
+  const V3 gradWI = vmul(HetaI, gWI);    // node i's side of the pair
+  const V3 gradWJ = vmul(HetaJ, gWJ);
+  t.WI = WI; t.WJ = WJ; t.gWI = gWI; t.gradWI = gradWI;
+  // moments for the ideal H
+  const double rij2 = mag2(rij);
+  t.thptS = safeInvVar(rij2*rij2*rij2);
+  // Monaghan-Gingold Pi_ij
+  const double muI = dot(vij, etaI)/(mag2(etaI) + P.eps2);
+  const double muJ = dot(vij, etaJ)/(mag2(etaJ) + P.eps2);
+  const double mI0 = dmin(0.0, muI), mJ0 = dmin(0.0, muJ);
+  const double eI = -Cl*I.cs*(P.linearInExp ? muI : mI0) + Cq*(P.quadInExp ? -sgn(muI)*muI*muI : mI0*mI0);
+  const double eJ = -Cl*J.cs*(P.linearInExp ? muJ : mJ0) + Cq*(P.quadInExp ? -sgn(muJ)*muJ*muJ : mJ0*mJ0);
+  const double qI = eI/I.rho, qJ = eJ/J.rho;   // (e/rho) * Tensor::one
+  // 0.5*(Pi * gradWQ), with WQ = W (same table): the off-diagonal zeros of
+  // Pi only add signed zeros.
+  const V3 QaccI = vmul(vmul(gradWI, qI), 0.5);
+  const V3 QaccJ = vmul(vmul(gradWJ, qJ), 0.5);
+  t.workQI = dot(vij, QaccI);
+  t.QI = I.rho*I.rho*fabs(qI);
+  // pressure terms (tensile correction uses the owner's W)
+  double PrhoI, PrhoJ;
+  if (TENSILE) {
+    const double x = own ? WI/(I.Hdet*P.WnPerh) : WJ/(J.Hdet*P.WnPerh);
+    const double fij = P.epsTensile*(x*x*x*x);
+    const double RI = fij*(I.P < 0.0 ? -I.P : 0.0);
+    const double RJ = fij*(J.P < 0.0 ? -J.P : 0.0);
+    PrhoI = I.somega*(I.P + RI)/(I.rho*I.rho);
+    PrhoJ = J.somega*(J.P + RJ)/(J.rho*J.rho);
+  } else {
+    PrhoI = I.Prho;
+    PrhoJ = J.Prho;
+  }
+  t.PrhoI = PrhoI;
+  // ((gradW_A P_A + gradW_B P_B) + Qacc_A) + Qacc_B
+  const V3 pp = vadd(vmul(gradWI, PrhoI), vmul(gradWJ, PrhoJ));
+  t.dd = vadd(vadd(pp, own ? QaccI : QaccJ), own ? QaccJ : QaccI);
+  return t;
+}
+
+// SPHHydroBase::evaluateDerivatives: one thread per internal node i, its CSR
+// row in ascending order (the reference's accumulation order), node i's side
+// of every pair.
 template<bool XSPH, bool TENSILE, bool COMPAT, bool SOLO>
 __global__ void __launch_bounds__(128, SPH_FP64_MIN_BLOCKS) sph_eval_fp64_kernel(const Member* mem, BlockMap bm, const Member single) {
   const MemberBlock mb = memberBlock(bm);
@@ -169,87 +248,24 @@ __global__ void __launch_bounds__(128, SPH_FP64_MIN_BLOCKS) sph_eval_fp64_kernel
   const double Cl = P.Cl*(0.5*(1.0 + 1.0)*1.0);   // Cl *= 0.5*(fCli + fClj)*fshear, multipliers 1
   const double Cq = P.Cq*(0.5*(1.0 + 1.0)*1.0);
   const int64_t k0 = offsets[i], k1 = offsets[i + 1];
-  for (int64_t k = k0; k < k1; ++k) {
-    const int32_t j = __ldg(nbr + k);
-    const Rec J = loadRec(rec, j);
-    const bool own = j > (int32_t)i;       // calculatePairInteraction: i is the owner
-    // The reference forms every pair term from the owner A and the other
-    // node B.  Here each quantity is formed once for node i and once for
-    // node j, with the same operands in the same order: with the
-    // owner-oriented separation r_ij = r_A - r_B (= r_i - r_j or its exact
-    // negation), eta_i = H_i r_ij is eta_A when i owns the pair and eta_B
-    // otherwise, and likewise for j.  Sums of two pair terms are commutative
-    // and keep their bits; where three or more are added the owner's order
-    // is selected explicitly.
-    const V3 d = vsub(I.r, J.r);
-    const V3 rij = own ? d : V3{-d.x, -d.y, -d.z};
-    const V3 dv = vsub(I.v, J.v);
-    const V3 vij = own ? dv : V3{-dv.x, -dv.y, -dv.z};
-    // H = h I (the common case): every H product reduces to a scaling with
-    // the same bits (the off-diagonal terms add exact zeros)
-    const bool iso = isoI && isoSym(J.H);
-    const V3 etaI = iso ? vmul(rij, I.H.xx) : sdot(I.H, rij);
-    const V3 etaJ = iso ? vmul(rij, J.H.xx) : sdot(J.H, rij);
-    const V3 uI = unitVector(etaI), uJ = unitVector(etaJ);
-    const V3 HetaI = iso ? vmul(uI, I.H.xx) : sdot(I.H, uI);
-    const V3 HetaJ = iso ? vmul(uJ, J.H.xx) : sdot(J.H, uJ);
-    double WI, gWI, WJ, gWJ;
-    tableKernelAndGrad(P.W, mag(etaI), I.Hdet, WI, gWI);
-    tableKernelAndGrad(P.W, mag(etaJ), J.Hdet, WJ, gWJ);
-    const V3 gradWI = vmul(HetaI, gWI);    // node i's side of the pair
-    const V3 gradWJ = vmul(HetaJ, gWJ);
-
-    // moments for the ideal H
-    const double rij2 = mag2(rij);
-    const double thptS = safeInvVar(rij2*rij2*rij2);
-    wns += 1.0*fabs(gWI);
+  // node i's sums take the pair terms in row order
+  auto accumulate = [&](const PairTerms& t, int64_t k) {
+    wns += 1.0*fabs(t.gWI);
     {
-      const double g2 = 1.0*mag2(gradWI);
-      const Sym thpt = smul(selfdyad(rij), thptS);
+      const double g2 = 1.0*mag2(t.gradWI);
+      const Sym thpt = smul(selfdyad(t.rij), t.thptS);
       m2 = sadd(m2, smul(thpt, g2));
     }
-    // sum density / normalization (single NodeList)
-    rhoSum += J.m*WI;
-    norm += I.mrho*WI;
-
-    // Monaghan-Gingold Pi_ij
-    const double muI = dot(vij, etaI)/(mag2(etaI) + P.eps2);
-    const double muJ = dot(vij, etaJ)/(mag2(etaJ) + P.eps2);
-    const double mI0 = dmin(0.0, muI), mJ0 = dmin(0.0, muJ);
-    const double eI = -Cl*I.cs*(P.linearInExp ? muI : mI0) + Cq*(P.quadInExp ? -sgn(muI)*muI*muI : mI0*mI0);
-    const double eJ = -Cl*J.cs*(P.linearInExp ? muJ : mJ0) + Cq*(P.quadInExp ? -sgn(muJ)*muJ*muJ : mJ0*mJ0);
-    const double qI = eI/I.rho, qJ = eJ/J.rho;   // (e/rho) * Tensor::one
-    // 0.5*(Pi * gradWQ), with WQ = W (same table): the off-diagonal zeros of
-    // Pi only add signed zeros.
-    const V3 QaccI = vmul(vmul(gradWI, qI), 0.5);
-    const V3 QaccJ = vmul(vmul(gradWJ, qJ), 0.5);
-    const double workQI = dot(vij, QaccI);
-    const double QI = I.rho*I.rho*fabs(qI);
-    maxvp = dmax(maxvp, QI);
-    effvp += J.mrho*QI*WI;
-    viscW += J.m*workQI;
-
-    // pressure terms (tensile correction uses the owner's W)
-    double PrhoI, PrhoJ;
-    if (TENSILE) {
-      const double x = own ? WI/(I.Hdet*P.WnPerh) : WJ/(J.Hdet*P.WnPerh);
-      const double fij = P.epsTensile*(x*x*x*x);
-      const double RI = fij*(I.P < 0.0 ? -I.P : 0.0);
-      const double RJ = fij*(J.P < 0.0 ? -J.P : 0.0);
-      PrhoI = I.somega*(I.P + RI)/(I.rho*I.rho);
-      PrhoJ = J.somega*(J.P + RJ)/(J.rho*J.rho);
-    } else {
-      PrhoI = I.Prho;
-      PrhoJ = J.Prho;
-    }
-    // ((gradW_A P_A + gradW_B P_B) + Qacc_A) + Qacc_B
-    const V3 pp = vadd(vmul(gradWI, PrhoI), vmul(gradWJ, PrhoJ));
-    const V3 deltaDvDt = vadd(vadd(pp, own ? QaccI : QaccJ), own ? QaccJ : QaccI);
-    DvDt = vadd(DvDt, vmul(deltaDvDt, own ? -J.m : J.m));
-    DepsDt += J.m*(PrhoI*dot(vij, gradWI) + workQI);
+    rhoSum += t.mj*t.WI;
+    norm += I.mrho*t.WI;
+    maxvp = dmax(maxvp, t.QI);
+    effvp += t.mrhoj*t.QI*t.WI;
+    viscW += t.mj*t.workQI;
+    DvDt = vadd(DvDt, vmul(t.dd, t.own ? -t.mj : t.mj));
+    DepsDt += t.mj*(t.PrhoI*dot(t.vij, t.gradWI) + t.workQI);
     if (COMPAT) {
       // the owner's pair acceleration, -m_other*deltaDvDt
-      const V3 pa = vmul(deltaDvDt, own ? -J.m : -I.m);
+      const V3 pa = vmul(t.dd, t.own ? -t.mj : -I.m);
       pacc[k] = pa.x;
       pacc[ecap + k] = pa.y;
       pacc[2*ecap + k] = pa.z;
@@ -257,32 +273,36 @@ __global__ void __launch_bounds__(128, SPH_FP64_MIN_BLOCKS) sph_eval_fp64_kernel
 #if SPH_FP64_SHARED_ACC
     {
       // DvDx -= (vij gradW_i) m_j, element by element as tsubfrom(tmul(dyad))
-      const double va[3] = {vij.x, vij.y, vij.z}, ga[3] = {gradWI.x, gradWI.y, gradWI.z};
+      const double va[3] = {t.vij.x, t.vij.y, t.vij.z}, ga[3] = {t.gradWI.x, t.gradWI.y, t.gradWI.z};
 #pragma unroll
       for (int r = 0; r < 3; ++r)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) accDvDx[128*(3*r + c)] = accDvDx[128*(3*r + c)] - (va[r]*ga[c])*J.m;
+        for (int c = 0; c < 3; ++c) accDvDx[128*(3*r + c)] = accDvDx[128*(3*r + c)] - (va[r]*ga[c])*t.mj;
     }
 #else
-    tsubfrom(DvDx, tmul(dyad(vij, gradWI), J.m));
+    tsubfrom(DvDx, tmul(dyad(t.vij, t.gradWI), t.mj));
 #endif
     if (XSPH) {
-      const double w = 0.5*(I.mrho*WI + J.mrho*WJ);
+      const double w = 0.5*(I.mrho*t.WI + t.mrhoj*t.WJ);
       XSPHw += w;
-      const V3 dvw = vmul(vij, w);
-      XSPHdv = own ? vsub(XSPHdv, dvw) : vadd(XSPHdv, dvw);
+      const V3 dvw = vmul(t.vij, w);
+      XSPHdv = t.own ? vsub(XSPHdv, dvw) : vadd(XSPHdv, dvw);
     }
 #if SPH_FP64_SHARED_ACC
     {
-      const double ra[3] = {rij.x, rij.y, rij.z}, ga[3] = {gradWI.x, gradWI.y, gradWI.z};
+      const double ra[3] = {t.rij.x, t.rij.y, t.rij.z}, ga[3] = {t.gradWI.x, t.gradWI.y, t.gradWI.z};
 #pragma unroll
       for (int r = 0; r < 3; ++r)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) accM[128*(3*r + c)] = accM[128*(3*r + c)] - (ra[r]*ga[c])*J.m;
+        for (int c = 0; c < 3; ++c) accM[128*(3*r + c)] = accM[128*(3*r + c)] - (ra[r]*ga[c])*t.mj;
     }
 #else
-    tsubfrom(M, tmul(dyad(rij, gradWI), J.m));
+    tsubfrom(M, tmul(dyad(t.rij, t.gradWI), t.mj));
 #endif
+  };
+  for (int64_t k = k0; k < k1; ++k) {
+    const int32_t j = __ldg(nbr + k);
+    accumulate(pairTerms<TENSILE>(I, isoI, loadRec(rec, j), j > (int32_t)i, P, Cl, Cq), k);
   }
 
   // ---- per-node finish (src/SPH/SPHHydroBase.cc:834-902)
