@@ -260,7 +260,6 @@ int batch_check_errors(Batch& b, const char* where) {
     int r = SPHGPU_ERR_NUMERIC;
     if (herr & DERR_NBR_CAPACITY) { msg += " neighbor capacity exceeded;"; r = SPHGPU_ERR_CAPACITY; }
     if (herr & DERR_GHOST_CHAIN) { msg += " ghost imaged twice on one axis;"; r = SPHGPU_ERR_UNSUPPORTED; }
-    if (herr & DERR_H_CLAMP) { msg += " H eigenvalue clamp (hmin/hmax) would be active;"; r = SPHGPU_ERR_UNSUPPORTED; }
     if (herr & DERR_NONPOSITIVE) { msg += " non-positive mass/density/det(H) or non-finite state;"; r = SPHGPU_ERR_NUMERIC; }
     if (rc == SPHGPU_OK) rc = r;
   }

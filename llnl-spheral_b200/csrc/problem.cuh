@@ -308,7 +308,6 @@ struct Problem {
 enum DevError {
   DERR_NBR_CAPACITY = 1,
   DERR_GHOST_CHAIN = 2,
-  DERR_H_CLAMP = 4,
   DERR_NONPOSITIVE = 8,
   DERR_GHOST_CAPACITY = 16,   // more ghosts than the ghost buffers hold (build is redone)
   DERR_ENTRY_CAPACITY = 32,   // more CSR entries than the entry buffers hold (build is redone)

@@ -589,17 +589,17 @@ __device__ __forceinline__ double compatibleDepsDt(const Member& MB, int64_t i, 
 }
 
 // ---------------------------------------------------------------- policies
-// eig(H) strictly inside (1/hmax, 1/hmin), where the eigenvalue clamp of the
-// bounded H policies is inactive.  Gershgorin discs bound the eigenvalues;
-// when they lie inside with a relative margin far above the eigen solve's
-// rounding, the solve is skipped (the answer cannot differ).
-__device__ __forceinline__ bool hInsideBounds(const Sym& H, double hmin, double hmax) {
+// The bounded H policies: min(1/hmin, max(1/hmax, H)) with the eigenvalue
+// limiters (boundedSym).  When the Gershgorin discs of H lie inside
+// (1/hmax, 1/hmin) with a relative margin far above the eigen solve's
+// rounding, every eigenvalue does and the reference returns H unchanged;
+// only the other tensors take the eigen solve.
+__device__ __forceinline__ Sym boundH(const Sym& H, double hmin, double hmax) {
   const double rx = dabs(H.xy) + dabs(H.xz), ry = dabs(H.xy) + dabs(H.yz), rz = dabs(H.xz) + dabs(H.yz);
   const double glo = dmin(H.xx - rx, dmin(H.yy - ry, H.zz - rz));
   const double ghi = dmax(H.xx + rx, dmax(H.yy + ry, H.zz + rz));
-  if (glo > (1.0/hmax)*(1.0 + 1.0e-12) && ghi < (1.0/hmin)*(1.0 - 1.0e-12)) return true;
-  const V3 ev = eigenValues(H);
-  return vmin(ev) > 1.0/hmax && vmax(ev) < 1.0/hmin;
+  if (glo > (1.0/hmax)*(1.0 + 1.0e-12) && ghi < (1.0/hmin)*(1.0 - 1.0e-12)) return H;
+  return boundedSym(H, 1.0/hmax, 1.0/hmin);
 }
 
 // State::update of every policy, f = f_src + scale*dt*df, into S.
@@ -681,7 +681,7 @@ __global__ void __launch_bounds__(128, 6) update_kernel(const Member* mem, Block
     Hn = Sym{D[(D_HIDEAL + 0)*n + i], D[(D_HIDEAL + 1)*n + i], D[(D_HIDEAL + 2)*n + i],
              D[(D_HIDEAL + 3)*n + i], D[(D_HIDEAL + 4)*n + i], D[(D_HIDEAL + 5)*n + i]};
   }
-  if (!hInsideBounds(Hn, P.hmin, P.hmax)) atomicOr(MB.err, DERR_H_CLAMP);
+  Hn = boundH(Hn, P.hmin, P.hmax);
   double* SH = midInRecords ? S0 : S;                // where the new H and mass density go
   SH[(S_H + 0)*n + i] = Hn.xx; SH[(S_H + 1)*n + i] = Hn.xy; SH[(S_H + 2)*n + i] = Hn.xz;
   SH[(S_H + 3)*n + i] = Hn.yy; SH[(S_H + 4)*n + i] = Hn.yz; SH[(S_H + 5)*n + i] = Hn.zz;

@@ -119,6 +119,96 @@ inline V3 eigenValues(const Sym& s) {
 struct T9 {
   double xx, xy, xz, yx, yy, yz, zx, zy, zz;
 };
+// GeomSymmetricTensor<3>::eigenVectors (src/Geometry/GeomSymmetricTensor_default.cc:36-95):
+// scaled by the largest element, elements below 1e-20 zeroed, the 3x3
+// eigenproblem solved, eigenvalues scaled back, eigenvector columns
+// normalised.  The reference passes the solve to Eigen's
+// SelfAdjointEigenSolver, which is not installed here; the solve restated is
+// the cyclic Jacobi solver the reference checker links in its place
+// (oracle/refshim/Eigen/Dense): rotations (0,1), (0,2), (1,2) per sweep until
+// the off-diagonal mass is below 1e-32 of the diagonal, eigenvalues ascending.
+struct Eig3 {
+  V3 values;
+  T9 vectors;   // column c: the eigenvector of values[c]
+};
+inline Eig3 symEigenVectors(const Sym& s) {
+  const double fscale = std::max(10.0*2.220446049250313e-16, smaxAbsElement(s));
+  const double fscalei = 1.0/fscale;
+  const double e[6] = {s.xx*fscalei, s.xy*fscalei, s.xz*fscalei, s.yy*fscalei, s.yz*fscalei, s.zz*fscalei};
+  double d[6];
+  for (int k = 0; k < 6; ++k) d[k] = std::abs(e[k]) < 1.0e-20 ? 0.0 : e[k];
+  double A[3][3] = {{d[0], d[1], d[2]}, {d[1], d[3], d[4]}, {d[2], d[4], d[5]}};
+  double V[3][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}};
+  for (int sweep = 0; sweep < 64; ++sweep) {
+    const double off = A[0][1]*A[0][1] + A[0][2]*A[0][2] + A[1][2]*A[1][2];
+    const double diag = A[0][0]*A[0][0] + A[1][1]*A[1][1] + A[2][2]*A[2][2];
+    if (off <= 1e-32*diag || off == 0.0) break;
+    for (int p = 0; p < 2; ++p) for (int q = p + 1; q < 3; ++q) {
+      if (A[p][q] == 0.0) continue;
+      const double theta = (A[q][q] - A[p][p])/(2.0*A[p][q]);
+      const double t = (theta >= 0.0 ? 1.0 : -1.0)/(std::abs(theta) + std::sqrt(theta*theta + 1.0));
+      const double c = 1.0/std::sqrt(t*t + 1.0), sn = t*c;
+      for (int k = 0; k < 3; ++k) {
+        const double akp = A[k][p], akq = A[k][q];
+        A[k][p] = c*akp - sn*akq; A[k][q] = sn*akp + c*akq;
+      }
+      for (int k = 0; k < 3; ++k) {
+        const double apk = A[p][k], aqk = A[q][k];
+        A[p][k] = c*apk - sn*aqk; A[q][k] = sn*apk + c*aqk;
+      }
+      for (int k = 0; k < 3; ++k) {
+        const double vkp = V[k][p], vkq = V[k][q];
+        V[k][p] = c*vkp - sn*vkq; V[k][q] = sn*vkp + c*vkq;
+      }
+    }
+  }
+  int order[3] = {0, 1, 2};
+  for (int i = 0; i < 3; ++i) for (int j = i + 1; j < 3; ++j)
+    if (A[order[j]][order[j]] < A[order[i]][order[i]]) std::swap(order[i], order[j]);
+  double B[3][3];
+  for (int c = 0; c < 3; ++c) for (int r = 0; r < 3; ++r) B[r][c] = V[r][order[c]];
+  Eig3 out;
+  out.values = V3{A[order[0]][order[0]]*fscale, A[order[1]][order[1]]*fscale, A[order[2]][order[2]]*fscale};
+  const double x1 = 1.0/std::sqrt(B[0][0]*B[0][0] + B[1][0]*B[1][0] + B[2][0]*B[2][0]);
+  const double x2 = 1.0/std::sqrt(B[0][1]*B[0][1] + B[1][1]*B[1][1] + B[2][1]*B[2][1]);
+  const double x3 = 1.0/std::sqrt(B[0][2]*B[0][2] + B[1][2]*B[1][2] + B[2][2]*B[2][2]);
+  out.vectors = T9{B[0][0]*x1, B[0][1]*x2, B[0][2]*x3,
+                   B[1][0]*x1, B[1][1]*x2, B[1][2]*x3,
+                   B[2][0]*x1, B[2][1]*x2, B[2][2]*x3};
+  return out;
+}
+// GeomSymmetricTensor<3>::rotationalTransform (src/Geometry/GeomSymmetricTensorInline_default.hh:1981-2014)
+inline Sym rotationalTransform(const Sym& a, const T9& R) {
+  const double A0 = a.xx, A1 = a.xy, A2 = a.xz, A3 = a.yy, A4 = a.yz, A5 = a.zz;
+  const double R0 = R.xx, R1 = R.xy, R2 = R.xz, R3 = R.yx, R4 = R.yy, R5 = R.yz, R6 = R.zx, R7 = R.zy, R8 = R.zz;
+  const double T0 = A0*R0 + A1*R1 + A2*R2;
+  const double T1 = A0*R3 + A1*R4 + A2*R5;
+  const double T2 = A1*R0 + A3*R1 + A4*R2;
+  const double T3 = A1*R3 + A3*R4 + A4*R5;
+  const double T4 = A2*R0 + A4*R1 + A5*R2;
+  const double T5 = A2*R3 + A4*R4 + A5*R5;
+  return Sym{R0*T0 + R1*T2 + R2*T4, R3*T0 + R4*T2 + R5*T4, R6*T0 + R7*T2 + R8*T4,
+             R3*T1 + R4*T3 + R5*T5, R6*T1 + R7*T3 + R8*T5,
+             R6*(A0*R6 + A1*R7 + A2*R8) + R7*(A1*R6 + A3*R7 + A4*R8) + R8*(A2*R6 + A4*R7 + A5*R8)};
+}
+// max(double, SymTensor) and min(double, SymTensor)
+// (src/Geometry/GeomSymmetricTensorInline_default.hh:2286-2345): the
+// eigenvalues limited, the tensor rebuilt from its eigenvectors, unless no
+// eigenvalue crosses the bound.
+inline Sym symMax(double maxValue, const Sym& t) {
+  const Eig3 e = symEigenVectors(t);
+  if (minElement(e.values) > maxValue) return t;
+  const Sym d{std::max(maxValue, e.values.x), 0.0, 0.0, std::max(maxValue, e.values.y), 0.0,
+              std::max(maxValue, e.values.z)};
+  return rotationalTransform(d, e.vectors);
+}
+inline Sym symMin(double minValue, const Sym& t) {
+  const Eig3 e = symEigenVectors(t);
+  if (maxElement(e.values) < minValue) return t;
+  const Sym d{std::min(minValue, e.values.x), 0.0, 0.0, std::min(minValue, e.values.y), 0.0,
+              std::min(minValue, e.values.z)};
+  return rotationalTransform(d, e.vectors);
+}
 inline T9 tzero() { return T9{0, 0, 0, 0, 0, 0, 0, 0, 0}; }
 inline T9 dyad(const V3& a, const V3& b) {
   return T9{a.x*b.x, a.x*b.y, a.x*b.z,

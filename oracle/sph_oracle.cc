@@ -530,12 +530,13 @@ void computeSumMassDensity(Problem& p) {
   }
 }
 
-bool checkHBounds(const Problem& p, const Sym& H) {
-  // The eigenvalue clamp of Increment/ReplaceBoundedState<SymTensor> is a
-  // no-op when all eigenvalues lie inside [1/hmax, 1/hmin]; only that case is
-  // restated here.
-  const V3 ev = eigenValues(H);
-  return minElement(ev) > 1.0/p.cfg.hmax && maxElement(ev) < 1.0/p.cfg.hmin;
+// IncrementBoundedState / ReplaceBoundedState<SymTensor> for H
+// (src/DataBase/IncrementBoundedState.cc:131-133, ReplaceBoundedState.cc:134-136):
+// min(1/hmin, max(1/hmax, H)) with the eigenvalue limiters; SPHHydroBase
+// registers the policy with 1/hmax and 1/hmin (src/SPH/SPHHydroBase.cc:290-296).
+Sym boundH(const Problem& p, const Sym& H) {
+  const double hmaxInv = 1.0/p.cfg.hmax, hminInv = 1.0/p.cfg.hmin;
+  return symMin(hminInv, symMax(hmaxInv, H));
 }
 
 // State::update for the SPH policies.  timeAdvanceOnly selects updateAsIncrement.
@@ -549,8 +550,7 @@ bool stateUpdate(Problem& p, double multiplier, bool timeAdvanceOnly) {
     } else {
       Hn = p.Hideal[i];
     }
-    if (!checkHBounds(p, Hn)) { g_err = "H eigenvalue clamp would be active"; return false; }
-    p.H[i] = Hn;
+    p.H[i] = boundH(p, Hn);
   }
   if (p.cfg.densityUpdate == SPHGPU_DENSITY_INTEGRATE || true) {
     for (int i = 0; i < n; ++i)

@@ -64,6 +64,15 @@ def cases(pkg):
     ns, cfg = _sod(gen, abi, 16, 4, 4, densityUpdate=abi.DENSITY_INTEGRATE, HUpdate=abi.H_INTEGRATE,
                    epsTensile=0.3, nTensile=4.0, linearInExpansion=1, quadraticInExpansion=1)
     c["sod_integrate_tensile"] = (ns, cfg, 3)
+    # the eigenvalue clamp of the bounded H policy: anisotropic, integrated H
+    # with hmin and hmax inside the spread of its eigenvalues
+    ns, cfg = _sod(gen, abi, 16, 4, 4, HUpdate=abi.H_INTEGRATE, hmin=0.06, hmax=0.09)
+    rng = np.random.default_rng(7)
+    ns.H[:, 0] *= rng.uniform(0.8, 1.3, ns.n)
+    ns.H[:, 5] *= rng.uniform(1.0, 1.8, ns.n)
+    ns.H[:, 1] = 0.15 * ns.H[:, 0] * rng.uniform(-1, 1, ns.n)
+    ns.H[:, 4] = 0.15 * ns.H[:, 3] * rng.uniform(-1, 1, ns.n)
+    c["sod_hclamp"] = (ns, cfg, 3)
     c["kh"] = _kh(gen, abi, 12, 12, 6) + (5,)
     ns, cfg = _kh(gen, abi, 12, 12, 6, compatibleEnergyEvolution=0, useVelocityMagnitudeForDt=1,
                   correctVelocityGradient=0)
