@@ -96,7 +96,9 @@ typedef struct sphgpu_config {
   int32_t max_neighbors;         /* per-node neighbor capacity (0 = 1024) */
   double  dtMin, dtMax, dtGrowth, lastDt;  /* Integrator controls       */
   int32_t qType;                 /* SPHGPU_Q_*                           */
-  int32_t qPad;
+  int32_t balsaraShearCorrection; /* ArtificialViscosity::balsaraShearCorrection
+                                     (src/ArtificialViscosity/ArtificialViscosity.cc:123-148),
+                                     off by default; SPH problems only */
   double  etaCritFrac, etaFoldFrac;  /* CRKSPH Q: full Q below etaCritFrac/nPerh,
                                         fold width etaFoldFrac/nPerh (defaults 1, 0.2) */
 } sphgpu_config;

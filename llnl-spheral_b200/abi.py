@@ -63,7 +63,7 @@ class SphConfig(ctypes.Structure):
         ("dtGrowth", ctypes.c_double),
         ("lastDt", ctypes.c_double),
         ("qType", ctypes.c_int32),
-        ("qPad", ctypes.c_int32),
+        ("balsaraShearCorrection", ctypes.c_int32),
         ("etaCritFrac", ctypes.c_double),
         ("etaFoldFrac", ctypes.c_double),
     ]

@@ -188,6 +188,9 @@ int validate_config(const sphgpu_config& c) {
   if (c.qType != SPHGPU_Q_MONAGHAN_GINGOLD && c.qType != SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD) {
     set_error("unknown qType"); return SPHGPU_ERR_ARG;
   }
+  if (c.balsaraShearCorrection != 0 && c.hydro != SPHGPU_HYDRO_SPH) {
+    set_error("the Balsara shear correction is implemented for SPH problems"); return SPHGPU_ERR_UNSUPPORTED;
+  }
   if (c.qType == SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD && c.hydro != SPHGPU_HYDRO_CRKSPH) {
     set_error("the CRKSPH Monaghan-Gingold Q is implemented for CRKSPH problems"); return SPHGPU_ERR_UNSUPPORTED;
   }
@@ -202,7 +205,7 @@ void free_problem(Problem* p) {
   void* ptrs[] = {p->S, p->S0, p->D, p->rec, p->groot, p->gcode, p->gpos, p->cand, p->cidx, p->sortedIdx,
                   p->cellStart, p->cellFill, p->counts, p->offsets, p->nbr, p->pacc, p->tableCoef, p->nperhTab,
                   p->wsumTab, p->blockSums, p->d_err, p->d_scal, p->d_red, p->staging, p->coefF, p->mrec, p->K, p->crec, p->hmaxi,
-                  p->wsumBinsTab, p->qgrad, p->Kheld};
+                  p->wsumBinsTab, p->qgrad, p->Kheld, p->fshear};
   dev_free_all(ptrs, (int)(sizeof(ptrs)/sizeof(ptrs[0])));
   if (p->pinned) cudaFreeHost(p->pinned);
   if (p->solo) { batch_free(*p->solo); delete p->solo; p->solo = nullptr; }
@@ -329,6 +332,9 @@ int build_neighbors_impl(Batch& b) {
 
 // Physics::initialize: grad-h (SPH) or the CRKSPH moments and corrections.
 int initialize_impl(Batch& b) {
+  // ArtificialViscosity::initialize: the Balsara shear correction from the
+  // last evaluation's velocity gradient (before the derivatives are zeroed)
+  if (anyMember(b, [](const Problem& p) { return p.prm.balsara != 0; })) SPH_TRY(launch_balsara(b));
   if (anyMember(b, isCrkP)) {
     SPH_TRY(crk_prepare(b));
     SPH_TRY(launch_crk_initialize(b));
@@ -431,7 +437,7 @@ uint64_t graph_key(const Batch& b) {
   mix(b.mem.size());
   mix((uint64_t)b.evalThreads);
   for (const Problem* p : b.mem) {
-    const void* ptrs[] = {p->S, p->S0, p->D, p->K, p->qgrad, p->rec, p->crec, p->mrec, p->groot, p->gcode,
+    const void* ptrs[] = {p->S, p->S0, p->D, p->K, p->qgrad, p->fshear, p->rec, p->crec, p->mrec, p->groot, p->gcode,
                           p->gpos, p->cand, p->cidx, p->sortedIdx, p->cellStart, p->cellFill, p->counts,
                           p->offsets, p->nbr, p->pacc, p->tableCoef, p->coefF, p->blockSums, p->d_scal,
                           p->d_red, p->d_err, p->hmaxi, p};
@@ -894,6 +900,7 @@ int64_t problem_bytes(const Problem& p) {
        (p.coefF ? 4*6*(int64_t)p.prm.W.n : 0);
   b += 8*(int64_t)CRECW*p.creccap + (p.K ? 8*(int64_t)NCRK*n : 0) + (p.Kheld ? 8*(int64_t)K_M0*n : 0);
   b += p.cfg.qType == SPHGPU_Q_CRKSPH_MONAGHAN_GINGOLD ? 8*(int64_t)QGRADW*n : 0;
+  b += p.cfg.balsaraShearCorrection ? 8*n : 0;                        // fshear
   return b;
 }
 
@@ -1031,6 +1038,7 @@ int sphgpu_create(const sphgpu_config* cfg, int64_t n_internal, sphgpu_problem**
     P.gradh = cfg->gradhCorrection;
     P.hydro = cfg->hydro;
     P.qType = cfg->qType;
+    P.balsara = cfg->balsaraShearCorrection != 0;
     P.precision = cfg->precision;
     P.etaCrit = cfg->etaCritFrac/cfg->nPerh;
     P.etaFold = cfg->etaFoldFrac/cfg->nPerh;
@@ -1053,6 +1061,11 @@ int sphgpu_create(const sphgpu_config* cfg, int64_t n_internal, sphgpu_problem**
     if ((rc = dalloc(p->staging, (cfg->hydro == SPHGPU_HYDRO_CRKSPH ? 27 : 9)*n)) != SPHGPU_OK) break;
     if ((rc = dalloc(p->d_err, 4)) != SPHGPU_OK) break;
     if ((rc = dalloc(p->hmaxi, 2*n)) != SPHGPU_OK) break;
+    if (cfg->balsaraShearCorrection) {
+      // no correction (1) until the first initialize computes it
+      if ((rc = dalloc(p->fshear, n)) != SPHGPU_OK) break;
+      fill_kernel<<<grid1(n), 256>>>(p->fshear, n, 1.0); ++p->launches;
+    }
     if ((rc = dalloc(p->d_scal, NSCAL)) != SPHGPU_OK) break;
     p->redcap = 148*4*8;
     if ((rc = dalloc(p->d_red, p->redcap)) != SPHGPU_OK) break;

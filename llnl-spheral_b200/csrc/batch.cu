@@ -82,6 +82,7 @@ Member member_of(const Problem& p) {
   M.rec = p.rec; M.crec = p.crec; M.mrec = p.mrec;
   M.gpos = p.gpos; M.pacc = p.pacc; M.scal = p.d_scal; M.red = p.d_red; M.hmaxi = p.hmaxi;
   M.qgrad = p.qgrad;
+  M.fshear = p.fshear;
   M.groot = p.groot; M.cidx = p.cidx; M.sortedIdx = p.sortedIdx; M.counts = p.counts; M.nbr = p.nbr;
   M.cellFill = p.cellFill;
   M.gcode = p.gcode;

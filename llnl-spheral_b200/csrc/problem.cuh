@@ -182,6 +182,7 @@ struct Params {
   double kernelExtent;
   int compatible, XSPH, correctVelGrad, linearInExp, quadInExp, useVelMagDt;
   int HUpdate, densityUpdate, gradh;
+  int balsara;             // Balsara shear correction of the Q (SPH)
   int hydro;               // SPHGPU_HYDRO_*
   int qType;               // SPHGPU_Q_*
   int precision;           // SPHGPU_PRECISION_*
@@ -243,6 +244,7 @@ struct Problem {
                                  // State construction resets it, its state0 copy restores that);
                                  // a restart file written then holds 1
   double* qgrad = nullptr;      // [n][QGRADW] velocity gradient cached by the CRKSPH Q's initialize
+  double* fshear = nullptr;     // [n] Balsara shear correction of the Q's initialize
   double* crec = nullptr;       // [n+G][CRECW] CRKSPH pair records
   int64_t creccap = 0;
   bool crkVolumeReady = false;
@@ -391,7 +393,7 @@ struct Member {
   Params prm;
   double* S; double* S0; double* D; double* K;
   double* rec; double* crec; double* mrec;
-  double* gpos; double* pacc; double* scal; double* red; double* hmaxi; double* qgrad;
+  double* gpos; double* pacc; double* scal; double* red; double* hmaxi; double* qgrad; double* fshear;
   int32_t* groot; int32_t* cidx; int32_t* sortedIdx; int32_t* counts; int32_t* nbr; int32_t* cellFill;
   uint32_t* gcode;
   int64_t* offsets; int64_t* cellStart; int64_t* blockSums;
@@ -532,6 +534,7 @@ int pack_mixed(Batch& b, bool rigorousSumOnly);
 // cover the ghosts only
 bool packedByUpdate(const Problem& p, int packMode);
 int launch_gradh(Batch& b);
+int launch_balsara(Batch& b);
 int launch_eval_sph_fp64(Batch& b);
 int launch_eval_sph_mixed(Batch& b);
 // summed density of the plain FP64 / mixed-precision SPH members; enforce:

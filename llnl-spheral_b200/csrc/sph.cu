@@ -245,8 +245,10 @@ __global__ void __launch_bounds__(128, SPH_FP64_MIN_BLOCKS) sph_eval_fp64_kernel
 #else
   T9 DvDx{0, 0, 0, 0, 0, 0, 0, 0, 0}, M{0, 0, 0, 0, 0, 0, 0, 0, 0};
 #endif
-  const double Cl = P.Cl*(0.5*(1.0 + 1.0)*1.0);   // Cl *= 0.5*(fCli + fClj)*fshear, multipliers 1
-  const double Cq = P.Cq*(0.5*(1.0 + 1.0)*1.0);
+  // Cl *= 0.5*(fCli + fClj)*fshear (MonaghanGingoldViscosity::Piij), the Cl
+  // and Cq multipliers 1; fshear = max of the two nodes' Balsara corrections,
+  // else 1
+  const double fsi = P.balsara ? MB.fshear[i] : 1.0;
   const int64_t k0 = offsets[i], k1 = offsets[i + 1];
   // node i's sums take the pair terms in row order
   auto accumulate = [&](const PairTerms& t, int64_t k) {
@@ -302,7 +304,9 @@ __global__ void __launch_bounds__(128, SPH_FP64_MIN_BLOCKS) sph_eval_fp64_kernel
   };
   for (int64_t k = k0; k < k1; ++k) {
     const int32_t j = __ldg(nbr + k);
-    accumulate(pairTerms<TENSILE>(I, isoI, loadRec(rec, j), j > (int32_t)i, P, Cl, Cq), k);
+    const double fs = P.balsara ? dmax(fsi, MB.fshear[j < n ? (int64_t)j : (int64_t)MB.groot[j - n]]) : 1.0;
+    accumulate(pairTerms<TENSILE>(I, isoI, loadRec(rec, j), j > (int32_t)i, P, P.Cl*(0.5*(1.0 + 1.0)*fs),
+                                  P.Cq*(0.5*(1.0 + 1.0)*fs)), k);
   }
 
   // ---- per-node finish (src/SPH/SPHHydroBase.cc:834-902)
@@ -646,7 +650,9 @@ __global__ void __launch_bounds__(128, 6) update_kernel(const Member* mem, Block
   double* S0 = MB.S0;
   const double* D = MB.D;
   const bool crk = P.hydro == SPHGPU_HYDRO_CRKSPH;
-  const bool recMid = recordMid && !crk && !P.gradh;
+  // (grad-h changes omega and the Balsara correction reads the mid-point H
+  // and sound speed after this update: those members keep the state in S)
+  const bool recMid = recordMid && !crk && !P.gradh && !P.balsara;
   const bool midInRecords = recMid && mode == UPDATE_SAVE_START;   // S keeps the start state
   const double* Src = mode == UPDATE_FROM_START && !recMid ? S0 : S;
   // the source state of the updated fields
@@ -1061,6 +1067,40 @@ int pack_mixed(Batch& b, bool rigorousSumOnly) {
   };
   auto ghosts = [&](const Problem& p) { return b.packedByUpdate == need && packedByUpdate(p, need); };
   return launch_pack(b, wants, ghosts, true);
+}
+
+// ArtificialViscosity::initialize with the Balsara shear correction
+// (src/ArtificialViscosity/ArtificialViscosity.cc:123-148): per internal node
+// fshear = |div v| / (|div v| + |curl v| + eps^2 max(1e-10, c_s) (det H)^(1/3))
+// from the velocity gradient of the last evaluation; ghosts read their root's.
+__global__ void __launch_bounds__(256) balsara_kernel(const Member* mem, BlockMap bm) {
+  const MemberBlock mb = memberBlock(bm);
+  const Member& M = mem[mb.m];
+  const int64_t n = M.n;
+  const int64_t i = mb.block*blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* D = M.D;
+  const double* S = M.S;
+  double g[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) g[c] = D[(D_DVDX + c)*n + i];
+  const double div = fabs(g[0] + g[4] + g[8]);                      // Tensor::Trace
+  const double a = g[7] - g[5], b = g[2] - g[6], c = g[3] - g[1];  // zy - yz, xz - zx, yx - xy
+  const double curl = sqrt(a*a + b*b + c*c);                        // curlVelocityMagnitude
+  const Sym H{S[(S_H + 0)*n + i], S[(S_H + 1)*n + i], S[(S_H + 2)*n + i],
+              S[(S_H + 3)*n + i], S[(S_H + 4)*n + i], S[(S_H + 5)*n + i]};
+  const double detH = sdet(H);
+  const double hmaxinverse = sgn(detH)*pow(fabs(detH), 0.3333333333333333);   // Dim<3>::rootnu
+  const double cs = dmax(1.0e-10, S[S_CS*n + i]);                   // negligibleSoundSpeed
+  M.fshear[i] = div/(div + curl + M.prm.eps2*cs*hmaxinverse);
+}
+
+int launch_balsara(Batch& b) {
+  BlockMap bm;
+  unsigned grid = 0;
+  SPH_TRY(batch_map_items(b, [](const Problem& p) { return p.prm.balsara ? p.n : (int64_t)0; }, 256, &bm, &grid));
+  if (grid) { balsara_kernel<<<grid, 256, 0, b.stream>>>(b.d_mem, bm); batch_count_launch(b); }
+  return cuda_status(cudaGetLastError(), "balsara");
 }
 
 int launch_gradh(Batch& b) {

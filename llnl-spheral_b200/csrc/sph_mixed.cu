@@ -114,10 +114,14 @@ __global__ void __launch_bounds__(128, SPH_MIXED_MIN_BLOCKS) sph_eval_mixed_kern
 #pragma unroll
   for (int c = 0; c < 9; ++c) { DvDx[c].init(); M[c].init(); }
   float maxvp = 0.0f;
+  const float fsi = P.balsara ? (float)MB.fshear[i] : 1.0f;
   const int64_t k0 = offsets[i], k1 = offsets[i + 1];
   for (int64_t k = k0; k < k1; ++k) {
     const int32_t j = __ldg(nbr + k);
     const MRec J = loadMRec(mrec, j);
+    // the Balsara shear correction of the pair (max of the two nodes'), else 1
+    const float fs = P.balsara ? fmaxf(fsi, (float)MB.fshear[j < n ? (int64_t)j : (int64_t)MB.groot[j - n]]) : 1.0f;
+    const float ClP = Cl*fs, CqP = Cq*fs;
     // FP64 differences, rounded once
     const F3 rij{(float)(I.x - J.x), (float)(I.y - J.y), (float)(I.z - J.z)};
     const F3 vij{(float)(I.vx - J.vx), (float)(I.vy - J.vy), (float)(I.vz - J.vz)};
@@ -166,8 +170,8 @@ __global__ void __launch_bounds__(128, SPH_MIXED_MIN_BLOCKS) sph_eval_mixed_kern
     const float mui = __fdividef(vij.x*etai.x + vij.y*etai.y + vij.z*etai.z, e2i + eps2);
     const float muj = __fdividef(vij.x*etaj.x + vij.y*etaj.y + vij.z*etaj.z, e2j + eps2);
     const float mi0 = fminf(0.0f, mui), mj0 = fminf(0.0f, muj);
-    const float ei = -Cl*I.cs*(P.linearInExp ? mui : mi0) + Cq*(P.quadInExp ? -copysignf(1.0f, mui)*mui*mui : mi0*mi0);
-    const float ej = -Cl*J.cs*(P.linearInExp ? muj : mj0) + Cq*(P.quadInExp ? -copysignf(1.0f, muj)*muj*muj : mj0*mj0);
+    const float ei = -ClP*I.cs*(P.linearInExp ? mui : mi0) + CqP*(P.quadInExp ? -copysignf(1.0f, mui)*mui*mui : mi0*mi0);
+    const float ej = -ClP*J.cs*(P.linearInExp ? muj : mj0) + CqP*(P.quadInExp ? -copysignf(1.0f, muj)*muj*muj : mj0*mj0);
     const float qi = __fdividef(ei, I.rho), qj = __fdividef(ej, J.rho);
     const F3 Qacci{0.5f*qi*gradWi.x, 0.5f*qi*gradWi.y, 0.5f*qi*gradWi.z};
     const F3 Qaccj{0.5f*qj*gradWj.x, 0.5f*qj*gradWj.y, 0.5f*qj*gradWj.z};
@@ -218,7 +222,7 @@ __global__ void __launch_bounds__(128, SPH_MIXED_MIN_BLOCKS) sph_eval_mixed_kern
 
   // ---- per-node finish in FP64 (src/SPH/SPHHydroBase.cc:834-902)
   // exact FP64 node values for the finish
-  const double* Sm = midInS0 && !P.gradh ? MB.S0 : S;
+  const double* Sm = midInS0 && !P.gradh && !P.balsara ? MB.S0 : S;
   const Sym Hi{Sm[(S_H + 0)*n + i], Sm[(S_H + 1)*n + i], Sm[(S_H + 2)*n + i],
                Sm[(S_H + 3)*n + i], Sm[(S_H + 4)*n + i], Sm[(S_H + 5)*n + i]};
   const double mi = S[S_M*n + i], rhoi = Sm[S_RHO*n + i], Hdeti = sdet(Hi);

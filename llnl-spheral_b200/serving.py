@@ -144,36 +144,90 @@ def poisson_trace(rate=20.0, duration=60.0, nmin=8192, nmax=1048576, nsteps=200,
         out.append(dict(arrival=t, kind=kind, n=n, nsteps=nsteps, seed=int(rng.integers(1 << 30))))
 
 
-def serve(trace, precision, budget_bytes=150e9, max_members=512, prepare=None, sleep=time.sleep):
+def serve(trace, precision, budget_bytes=150e9, max_members=512, prepare=None, sleep=time.sleep, max_queued=64,
+          prebuilt_nodes=48_000_000, lookahead=128):
     """Replay `trace` in real time on a fresh server.  Returns per-request
-    times to completion (s), the makespan and the server statistics."""
-    reqs = prepare(trace, precision) if prepare else [request_nodes(r["kind"], r["n"], r["seed"], precision)
-                                                      for r in trace]
-    srv = Server(budget_bytes, max_members)
+    times to completion (s), the makespan and the server statistics.
+
+    Node sets are built before the replay starts (untimed) in arrival order
+    while they hold at most `prebuilt_nodes` nodes (every request of a short
+    trace); a background thread builds the rest in order, at most `lookahead`
+    ahead of the submissions.  A request that has arrived and is built goes to
+    the server while fewer than `max_queued` wait in the server's queue: the
+    server admits its queue first come first served, head of line, so the
+    admissions are those of an unbounded queue while host memory holds a
+    bounded number of waiting node sets, however far a long trace outruns the
+    device.  Times to completion run from each request's arrival."""
+    import threading
+
+    def make(k):
+        r = trace[k]
+        return prepare([r], precision)[0] if prepare else request_nodes(r["kind"], r["n"], r["seed"], precision)
+
     order = sorted(range(len(trace)), key=lambda k: trace[k]["arrival"])
+    built = {}
+    cv = threading.Condition()
+    state = {"submitted": 0, "stop": False}
+    nodes_built, nbuilt = 0, 0
+    while nbuilt < len(order) and nodes_built < prebuilt_nodes:
+        built[order[nbuilt]] = make(order[nbuilt])
+        nodes_built += trace[order[nbuilt]]["n"]
+        nbuilt += 1
+
+    def producer(start):
+        for idx in range(start, len(order)):
+            with cv:
+                while idx - state["submitted"] >= lookahead and not state["stop"]:
+                    cv.wait(0.1)
+                if state["stop"]:
+                    return
+            item = make(order[idx])
+            with cv:
+                built[order[idx]] = item
+                cv.notify_all()
+
+    worker = threading.Thread(target=producer, args=(nbuilt,), daemon=True)
+    worker.start()
+    srv = Server(budget_bytes, max_members)
     ids, ttc = {}, {}
-    nxt = 0
-    t0 = time.perf_counter()
-    while len(ttc) < len(trace):
-        now = time.perf_counter() - t0
-        while nxt < len(order) and trace[order[nxt]]["arrival"] <= now:
-            k = order[nxt]
-            ns, cfg = reqs[k]
-            ids[srv.submit(cfg, ns, trace[k]["nsteps"])] = k
-            nxt += 1
-        running, queued = srv.tick()
-        done_at = time.perf_counter() - t0
-        for rid in srv.finished():
-            k = ids[rid]
-            st, _, _ = srv.status(rid)
-            ttc[k] = done_at - trace[k]["arrival"] if st == Server.DONE else float("nan")
-            if st == Server.DONE:
-                srv.fetch(rid)
-        if running == 0 and queued == 0 and nxt < len(order):
-            wait = trace[order[nxt]]["arrival"] - (time.perf_counter() - t0)
-            if wait > 0:
-                sleep(wait)
-    makespan = time.perf_counter() - t0
-    stats = srv.stats()
-    srv.close()
+    nxt, queued = 0, 0
+    try:
+        t0 = time.perf_counter()
+        while len(ttc) < len(trace):
+            now = time.perf_counter() - t0
+            while nxt < len(order) and trace[order[nxt]]["arrival"] <= now and queued < max_queued:
+                k = order[nxt]
+                with cv:
+                    item = built.pop(k, None)
+                if item is None:
+                    break                     # not built yet: keep the device busy meanwhile
+                ns, cfg = item
+                ids[srv.submit(cfg, ns, trace[k]["nsteps"])] = k
+                nxt += 1
+                queued += 1
+                with cv:
+                    state["submitted"] = nxt
+                    cv.notify_all()
+            running, queued = srv.tick()
+            done_at = time.perf_counter() - t0
+            for rid in srv.finished():
+                k = ids[rid]
+                st, _, _ = srv.status(rid)
+                ttc[k] = done_at - trace[k]["arrival"] if st == Server.DONE else float("nan")
+                if st == Server.DONE:
+                    srv.fetch(rid)
+            if running == 0 and queued == 0 and nxt < len(order):
+                wait = trace[order[nxt]]["arrival"] - (time.perf_counter() - t0)
+                if wait > 0:
+                    sleep(wait)
+                elif order[nxt] not in built:
+                    sleep(0.001)              # the next request is still being built
+        makespan = time.perf_counter() - t0
+        stats = srv.stats()
+    finally:
+        with cv:
+            state["stop"] = True
+            cv.notify_all()
+        worker.join()
+        srv.close()
     return [ttc[k] for k in range(len(trace))], makespan, stats

@@ -439,6 +439,7 @@ int main(int argc, char** argv) {
     ArtificialViscositySpace::MonaghanGingoldViscosity<D> Q(cfg.Cl, cfg.Cq, cfg.linearInExpansion != 0,
                                                             cfg.quadraticInExpansion != 0);
     Q.epsilon2(cfg.epsilon2);
+    Q.balsaraShearCorrection(cfg.balsaraShearCorrection != 0);
     // SPHHydroBase (src/SPH/SPHHydroBase.hh:53-71): filter 0, total energy off,
     // sumMassDensityOverAllNodeLists (one NodeList), unbounded box.
 #ifdef REF_SPH_GPU

@@ -61,6 +61,7 @@ struct Problem {
   // Full node arrays: internal [0, nInt) then ghosts.
   std::vector<V3> pos, vel;
   std::vector<double> m, rho, eps, P, cs, omega, eps0;
+  std::vector<double> fshear;   // ArtificialViscosity's Balsara shear correction (internal + ghosts)
   std::vector<Sym> H;
   // Ghost bookkeeping, in creation order.
   std::vector<PlanarBC> bcs;                 // 2 per periodic axis, x then y then z
@@ -95,6 +96,7 @@ int numNodes(const Problem& p) { return int(p.pos.size()); }
 void resizeAll(Problem& p, int n) {
   p.pos.resize(n); p.vel.resize(n); p.m.resize(n); p.rho.resize(n); p.eps.resize(n);
   p.P.resize(n); p.cs.resize(n); p.omega.resize(n, 1.0); p.eps0.resize(n); p.H.resize(n);
+  p.fshear.resize(n, 1.0);
 }
 
 // ---------------------------------------------------------------- EOS
@@ -309,12 +311,14 @@ void gradhCorrection(Problem& p) {
 }
 
 // MonaghanGingoldViscosity::Piij, returning the diagonal value e/rho of each side.
+// fsi, fsj: the two nodes' shear corrections (ArtificialViscosity.cc:123-148; 1 without it).
 inline void Piij(const Problem& p, const V3& etai, const V3& vi, double rhoi, double csi,
-                 const V3& etaj, const V3& vj, double rhoj, double csj, T9& QPi, T9& QPj) {
+                 const V3& etaj, const V3& vj, double rhoj, double csj, T9& QPi, T9& QPj,
+                 double fsi = 1.0, double fsj = 1.0) {
   double Cl = p.cfg.Cl, Cq = p.cfg.Cq;
   const double eps2 = p.cfg.epsilon2;
   const double fCli = 1.0, fCqi = 1.0, fClj = 1.0, fCqj = 1.0;
-  const double fshear = std::max(1.0, 1.0);
+  const double fshear = std::max(fsi, fsj);
   Cl *= 0.5*(fCli + fClj)*fshear;
   Cq *= 0.5*(fCqi + fCqj)*fshear;
   const V3 vij = vsub(vi, vj);
@@ -387,7 +391,7 @@ void evaluateDerivatives(Problem& p) {
 
       const V3 vij = vsub(vi, vj);
       T9 QPi, QPj;
-      Piij(p, etai, vi, rhoi, ci, etaj, vj, rhoj, cj, QPi, QPj);
+      Piij(p, etai, vi, rhoi, ci, etaj, vj, rhoj, cj, QPi, QPj, p.fshear[i], p.fshear[j]);
       const V3 Qacci = vmul(tvdot(QPi, gradWQi), 0.5);
       const V3 Qaccj = vmul(tvdot(QPj, gradWQj), 0.5);
       const double workQi = dot(vij, Qacci);
@@ -635,7 +639,26 @@ double selectDt(Problem& p) {
   return dt;
 }
 
+// ArtificialViscosity::initialize with the Balsara shear correction
+// (src/ArtificialViscosity/ArtificialViscosity.cc:123-148): from the velocity
+// gradient of the last evaluation, the derivatives not yet zeroed; ghosts
+// take their control node's value (applyFieldListGhostBoundary).
+void balsaraShearCorrection(Problem& p) {
+  for (int i = 0; i < p.nInt; ++i) {
+    const T9 g = i < int(p.DvDx.size()) ? p.DvDx[i] : tzero();   // none before the first evaluation
+    const double div = std::abs(g.xx + g.yy + g.zz);
+    const double a = g.zy - g.yz, b = g.xz - g.zx, c = g.yx - g.xy;
+    const double curl = std::sqrt(a*a + b*b + c*c);
+    const double hmaxinverse = CubeRootHalley2(sdet(p.H[i]));
+    const double cs = std::max(1.0e-10, p.cs[i]);
+    p.fshear[i] = div/(div + curl + p.cfg.epsilon2*cs*hmaxinverse);
+  }
+  for (size_t b = 0; b < p.bcs.size(); ++b)
+    for (size_t k = 0; k < p.control[b].size(); ++k) p.fshear[p.ghosts[b][k]] = p.fshear[p.control[b][k]];
+}
+
 void initializeDerivatives(Problem& p) {
+  if (p.cfg.balsaraShearCorrection) balsaraShearCorrection(p);
   if (p.cfg.gradhCorrection) {
     gradhCorrection(p);
     for (size_t b = 0; b < p.bcs.size(); ++b)

@@ -74,6 +74,9 @@ def cases(pkg):
     ns.H[:, 4] = 0.15 * ns.H[:, 3] * rng.uniform(-1, 1, ns.n)
     c["sod_hclamp"] = (ns, cfg, 3)
     c["kh"] = _kh(gen, abi, 12, 12, 6) + (5,)
+    # the Balsara shear correction of the Q (sheared flow: curl and div both nonzero)
+    ns, cfg = _kh(gen, abi, 12, 12, 6, balsaraShearCorrection=1)
+    c["kh_balsara"] = (ns, cfg, 5)
     ns, cfg = _kh(gen, abi, 12, 12, 6, compatibleEnergyEvolution=0, useVelocityMagnitudeForDt=1,
                   correctVelocityGradient=0)
     c["kh_noncompatible"] = (ns, cfg, 5)
