@@ -303,6 +303,20 @@ def measure_steps_graph(pkg, ns, cfg, precision, steps, warmup, world, clocks=No
                "launches": h.kernel_launches() - l0, "clocks": clk}
 
 
+def measure_shuffled(pkg, ns, cfg, steps, warmup, world):
+    """Plain FP64 RK2 steps (whole-step graph) on the node set permuted by a
+    seeded random order: the same physics, every per-node and per-pair
+    access in the caller's numbering scattered."""
+    perm = np.random.default_rng(7).permutation(ns.n)
+    sh = pkg.generators.NodeSet(ns.pos[perm], ns.vel[perm], ns.mass[perm], ns.rho[perm], ns.eps[perm],
+                                ns.H[perm], ns.dx)
+    h, r = measure_steps_graph(pkg, sh, cfg, pkg.abi.PRECISION_FP64, steps, warmup, world)
+    h.close()
+    t = allmax(r["total_ms"], world)
+    return {"value": allsum(r["pairs"], world) / (t / 1e3), "unit": METRIC, "ms_per_step": t / steps,
+            "steps": steps, "workload": "the headline node set in a seeded random order (plain FP64)"}
+
+
 def measure_eval(h, reps=10):
     """Duration of one evaluateDerivatives (record pack + pair kernel) on the stream."""
     import torch
@@ -984,6 +998,11 @@ def run_ours(args):
             result["cpu_baseline"] = cpu_baseline(pkg, args.nx)
     hm.close()
     hp.close()
+    # the same node set in a seeded random order: nothing reorders the
+    # caller's nodes, so the pair kernels' gathers follow the caller's order
+    shuffled = measure_shuffled(pkg, ns, cfg, max(3, args.steps // 5), args.warmup, world)
+    if rank == 0:
+        result["shuffled_input"] = shuffled
     if args.accuracy_steps > 0:
         acc = measure_accuracy(pkg, ns, cfg, args.accuracy_steps)
         if rank == 0:
