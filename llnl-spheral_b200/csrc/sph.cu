@@ -206,7 +206,7 @@ __device__ __forceinline__ PairTerms pairTerms(const Rec& I, bool isoI, const Re
 // SPHHydroBase::evaluateDerivatives: one thread per internal node i, its CSR
 // row in ascending order (the reference's accumulation order), node i's side
 // of every pair.
-template<bool XSPH, bool TENSILE, bool COMPAT, bool SOLO>
+template<bool XSPH, bool TENSILE, bool COMPAT, bool SOLO, bool BALSARA>
 __global__ void __launch_bounds__(128, SPH_FP64_MIN_BLOCKS) sph_eval_fp64_kernel(const Member* mem, BlockMap bm, const Member single) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = SOLO ? single : mem[mb.m];   // one member: read from the kernel parameters
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(128, SPH_FP64_MIN_BLOCKS) sph_eval_fp64_kernel
   // Cl *= 0.5*(fCli + fClj)*fshear (MonaghanGingoldViscosity::Piij), the Cl
   // and Cq multipliers 1; fshear = max of the two nodes' Balsara corrections,
   // else 1
-  const double fsi = P.balsara ? MB.fshear[i] : 1.0;
+  const double fsi = BALSARA ? MB.fshear[i] : 1.0;
   const int64_t k0 = offsets[i], k1 = offsets[i + 1];
   // node i's sums take the pair terms in row order
   auto accumulate = [&](const PairTerms& t, int64_t k) {
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(128, SPH_FP64_MIN_BLOCKS) sph_eval_fp64_kernel
   };
   for (int64_t k = k0; k < k1; ++k) {
     const int32_t j = __ldg(nbr + k);
-    const double fs = P.balsara ? dmax(fsi, MB.fshear[j < n ? (int64_t)j : (int64_t)MB.groot[j - n]]) : 1.0;
+    const double fs = BALSARA ? dmax(fsi, MB.fshear[j < n ? (int64_t)j : (int64_t)MB.groot[j - n]]) : 1.0;
     accumulate(pairTerms<TENSILE>(I, isoI, loadRec(rec, j), j > (int32_t)i, P, P.Cl*(0.5*(1.0 + 1.0)*fs),
                                   P.Cq*(0.5*(1.0 + 1.0)*fs)), k);
   }
@@ -1112,35 +1112,41 @@ int launch_gradh(Batch& b) {
   return cuda_status(cudaGetLastError(), "gradh");
 }
 
+// One launch of the FP64 pair kernel variant <XSPH, TENSILE, COMPAT, BALSARA>.
+template<bool X, bool T, bool C, bool B>
+void launch_fp64_variant(Batch& b, unsigned grid, BlockMap bm, const Member& one, bool solo) {
+  if (solo) sph_eval_fp64_kernel<X, T, C, true, B><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one);
+  else sph_eval_fp64_kernel<X, T, C, false, B><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one);
+}
+using Fp64Launch = void (*)(Batch&, unsigned, BlockMap, const Member&, bool);
+// indexed by BALSARA << 3 | XSPH << 2 | TENSILE << 1 | COMPAT
+const Fp64Launch kFp64Launch[16] = {
+    &launch_fp64_variant<false, false, false, false>, &launch_fp64_variant<false, false, true, false>,
+    &launch_fp64_variant<false, true, false, false>, &launch_fp64_variant<false, true, true, false>,
+    &launch_fp64_variant<true, false, false, false>, &launch_fp64_variant<true, false, true, false>,
+    &launch_fp64_variant<true, true, false, false>, &launch_fp64_variant<true, true, true, false>,
+    &launch_fp64_variant<false, false, false, true>, &launch_fp64_variant<false, false, true, true>,
+    &launch_fp64_variant<false, true, false, true>, &launch_fp64_variant<false, true, true, true>,
+    &launch_fp64_variant<true, false, false, true>, &launch_fp64_variant<true, false, true, true>,
+    &launch_fp64_variant<true, true, false, true>, &launch_fp64_variant<true, true, true, true>};
+
 int launch_eval_sph_fp64(Batch& b) {
   auto key = [](const Problem& p) {
-    return (p.prm.XSPH ? 4 : 0) | (p.prm.epsTensile != 0.0 ? 2 : 0) | (p.prm.compatible ? 1 : 0);
+    return (p.prm.balsara ? 8 : 0) | (p.prm.XSPH ? 4 : 0) | (p.prm.epsTensile != 0.0 ? 2 : 0) |
+           (p.prm.compatible ? 1 : 0);
   };
   const bool solo = b.mem.size() == 1;
   const Member one = solo ? describe_member(*b.mem[0]) : Member{};
-  bool present[8] = {false, false, false, false, false, false, false, false};
+  bool present[16] = {};
   for (Problem* p : b.mem) if (isFp64Sph(*p)) present[key(*p)] = true;
-  for (int v = 0; v < 8; ++v) {
+  for (int v = 0; v < 16; ++v) {
     if (!present[v]) continue;
     BlockMap bm;
     unsigned grid = 0;
     SPH_TRY(batch_map_items(b, [&](const Problem& p) { return isFp64Sph(p) && key(p) == v ? p.n : (int64_t)0; },
                             b.evalThreads, &bm, &grid));
     if (!grid) continue;
-#define SPH_LAUNCH(X, T, C)                                                                            \
-    if (solo) sph_eval_fp64_kernel<X, T, C, true><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one);  \
-    else sph_eval_fp64_kernel<X, T, C, false><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one)
-    switch (v) {
-      case 0: SPH_LAUNCH(false, false, false); break;
-      case 1: SPH_LAUNCH(false, false, true); break;
-      case 2: SPH_LAUNCH(false, true, false); break;
-      case 3: SPH_LAUNCH(false, true, true); break;
-      case 4: SPH_LAUNCH(true, false, false); break;
-      case 5: SPH_LAUNCH(true, false, true); break;
-      case 6: SPH_LAUNCH(true, true, false); break;
-      default: SPH_LAUNCH(true, true, true); break;
-    }
-#undef SPH_LAUNCH
+    kFp64Launch[v](b, grid, bm, one, solo);
     batch_count_launch(b);
   }
   return cuda_status(cudaGetLastError(), "evaluate (FP64)");

@@ -83,7 +83,7 @@ __device__ __forceinline__ void tableF(const float* coef, int n, float invStep, 
 // midInS0: the RK2 step's record-only mid point ran (update_kernel
 // recordMid): the FP64 mid-point H and mass density of a member without
 // grad-h are in S0, S holds the start of the step.
-template<bool XSPH, bool TENSILE, bool COMPAT, bool SOLO>
+template<bool XSPH, bool TENSILE, bool COMPAT, bool SOLO, bool BALSARA>
 __global__ void __launch_bounds__(128, SPH_MIXED_MIN_BLOCKS) sph_eval_mixed_kernel(const Member* mem, BlockMap bm, const Member single,
                                                                  int midInS0) {
   const MemberBlock mb = memberBlock(bm);
@@ -114,13 +114,13 @@ __global__ void __launch_bounds__(128, SPH_MIXED_MIN_BLOCKS) sph_eval_mixed_kern
 #pragma unroll
   for (int c = 0; c < 9; ++c) { DvDx[c].init(); M[c].init(); }
   float maxvp = 0.0f;
-  const float fsi = P.balsara ? (float)MB.fshear[i] : 1.0f;
+  const float fsi = BALSARA ? (float)MB.fshear[i] : 1.0f;
   const int64_t k0 = offsets[i], k1 = offsets[i + 1];
   for (int64_t k = k0; k < k1; ++k) {
     const int32_t j = __ldg(nbr + k);
     const MRec J = loadMRec(mrec, j);
     // the Balsara shear correction of the pair (max of the two nodes'), else 1
-    const float fs = P.balsara ? fmaxf(fsi, (float)MB.fshear[j < n ? (int64_t)j : (int64_t)MB.groot[j - n]]) : 1.0f;
+    const float fs = BALSARA ? fmaxf(fsi, (float)MB.fshear[j < n ? (int64_t)j : (int64_t)MB.groot[j - n]]) : 1.0f;
     const float ClP = Cl*fs, CqP = Cq*fs;
     // FP64 differences, rounded once
     const F3 rij{(float)(I.x - J.x), (float)(I.y - J.y), (float)(I.z - J.z)};
@@ -330,38 +330,44 @@ bool mixedSph(const Problem& p) {
   return p.cfg.precision == SPHGPU_PRECISION_MIXED && p.prm.hydro == SPHGPU_HYDRO_SPH;
 }
 
+// One launch of the mixed pair kernel variant <XSPH, TENSILE, COMPAT, BALSARA>.
+template<bool X, bool T, bool C, bool B>
+void launch_mixed_variant(Batch& b, unsigned grid, BlockMap bm, const Member& one, bool solo, int mid) {
+  if (solo) sph_eval_mixed_kernel<X, T, C, true, B><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one, mid);
+  else sph_eval_mixed_kernel<X, T, C, false, B><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one, mid);
+}
+using MixedLaunch = void (*)(Batch&, unsigned, BlockMap, const Member&, bool, int);
+// indexed by BALSARA << 3 | XSPH << 2 | TENSILE << 1 | COMPAT
+const MixedLaunch kMixedLaunch[16] = {
+    &launch_mixed_variant<false, false, false, false>, &launch_mixed_variant<false, false, true, false>,
+    &launch_mixed_variant<false, true, false, false>, &launch_mixed_variant<false, true, true, false>,
+    &launch_mixed_variant<true, false, false, false>, &launch_mixed_variant<true, false, true, false>,
+    &launch_mixed_variant<true, true, false, false>, &launch_mixed_variant<true, true, true, false>,
+    &launch_mixed_variant<false, false, false, true>, &launch_mixed_variant<false, false, true, true>,
+    &launch_mixed_variant<false, true, false, true>, &launch_mixed_variant<false, true, true, true>,
+    &launch_mixed_variant<true, false, false, true>, &launch_mixed_variant<true, false, true, true>,
+    &launch_mixed_variant<true, true, false, true>, &launch_mixed_variant<true, true, true, true>};
+
 int launch_eval_sph_mixed(Batch& b) {
   auto mixed = mixedSph;
-  BlockMap bm;
-  unsigned grid = 0;
   SPH_TRY(pack_mixed(b, false));
   auto key = [](const Problem& p) {
-    return (p.prm.XSPH ? 4 : 0) | (p.prm.epsTensile != 0.0 ? 2 : 0) | (p.prm.compatible ? 1 : 0);
+    return (p.prm.balsara ? 8 : 0) | (p.prm.XSPH ? 4 : 0) | (p.prm.epsTensile != 0.0 ? 2 : 0) |
+           (p.prm.compatible ? 1 : 0);
   };
   const bool solo = b.mem.size() == 1;
   const Member one = solo ? describe_member(*b.mem[0]) : Member{};
   const int mid = b.midInS0 ? 1 : 0;
-  bool present[8] = {false, false, false, false, false, false, false, false};
+  bool present[16] = {};
   for (Problem* p : b.mem) if (mixed(*p)) present[key(*p)] = true;
-  for (int v = 0; v < 8; ++v) {
+  for (int v = 0; v < 16; ++v) {
     if (!present[v]) continue;
+    BlockMap bm;
+    unsigned grid = 0;
     SPH_TRY(batch_map_items(b, [&](const Problem& p) { return mixed(p) && key(p) == v ? p.n : (int64_t)0; }, b.evalThreads,
                             &bm, &grid));
     if (!grid) continue;
-#define MIX_LAUNCH(X, T, C)                                                                             \
-    if (solo) sph_eval_mixed_kernel<X, T, C, true><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one, mid);  \
-    else sph_eval_mixed_kernel<X, T, C, false><<<grid, b.evalThreads, 0, b.stream>>>(b.d_mem, bm, one, mid)
-    switch (v) {
-      case 0: MIX_LAUNCH(false, false, false); break;
-      case 1: MIX_LAUNCH(false, false, true); break;
-      case 2: MIX_LAUNCH(false, true, false); break;
-      case 3: MIX_LAUNCH(false, true, true); break;
-      case 4: MIX_LAUNCH(true, false, false); break;
-      case 5: MIX_LAUNCH(true, false, true); break;
-      case 6: MIX_LAUNCH(true, true, false); break;
-      default: MIX_LAUNCH(true, true, true); break;
-    }
-#undef MIX_LAUNCH
+    kMixedLaunch[v](b, grid, bm, one, solo, mid);
     batch_count_launch(b);
   }
   return cuda_status(cudaGetLastError(), "evaluate (mixed)");
