@@ -308,7 +308,11 @@ int sphgpu_kernel_launches(sphgpu_problem* p, int64_t* launches);
  * cells": cells per kernel reach of the walk's grid, 0 = automatic (1),
  * 1 = cells of one reach (27-cell window), 2 = cells of half a reach
  * (125-cell window, rows and cells beyond the reach skipped).  Same
- * ConnectivityMap either way.
+ * ConnectivityMap either way.  stage "ghost passes": the six periodic
+ * boundary passes of the ghost build, 0 = automatic (2 for a problem or a
+ * batch of at most 4 members, else 1), 1 = four launches and a prefix sum
+ * per pass, 2 = all six passes in one cooperative launch with grid
+ * barriers.  Same ghosts in the same order either way.
  * sphgpu_get_schedule reports what the last call used. */
 int sphgpu_set_schedule(sphgpu_problem* p, const char* stage, int32_t schedule);
 int sphgpu_get_schedule(sphgpu_problem* p, const char* stage, int32_t* schedule);

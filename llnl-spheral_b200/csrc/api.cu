@@ -264,6 +264,7 @@ int batch_check_errors(Batch& b, const char* where) {
     if (herr & DERR_NBR_CAPACITY) { msg += " neighbor capacity exceeded;"; r = SPHGPU_ERR_CAPACITY; }
     if (herr & DERR_GHOST_CHAIN) { msg += " ghost imaged twice on one axis;"; r = SPHGPU_ERR_UNSUPPORTED; }
     if (herr & DERR_NONPOSITIVE) { msg += " non-positive mass/density/det(H) or non-finite state;"; r = SPHGPU_ERR_NUMERIC; }
+    if (herr & DERR_BARRIER) { msg += " a grid barrier of the fused ghost passes timed out;"; r = SPHGPU_ERR_CUDA; }
     if (rc == SPHGPU_OK) rc = r;
   }
   if (rc != SPHGPU_OK) {
@@ -788,6 +789,14 @@ int set_schedule_impl(Batch& b, int* nbrSchedule, int* nbrCells, const char* sta
       return SPHGPU_ERR_ARG;
     }
     for (Problem* p : b.mem) p->nbrStash = schedule == 1;
+    return SPHGPU_OK;
+  }
+  if (std::strcmp(stage, "ghost passes") == 0) {
+    if (schedule < 0 || schedule > 2) {
+      set_error("ghost passes is 0 (auto), 1 (launches per pass) or 2 (one cooperative launch)");
+      return SPHGPU_ERR_ARG;
+    }
+    b.ghostPasses = schedule;
     return SPHGPU_OK;
   }
   if (std::strcmp(stage, "step graph") == 0) {
@@ -1499,6 +1508,10 @@ int sphgpu_get_schedule(sphgpu_problem* p, const char* stage, int32_t* schedule)
   }
   if (std::strcmp(stage, "step graph") == 0) {
     *schedule = p->solo->useGraph ? 1 : 0;
+    return SPHGPU_OK;
+  }
+  if (std::strcmp(stage, "ghost passes") == 0) {
+    *schedule = p->solo->lastGhostPasses;
     return SPHGPU_OK;
   }
   if (std::strcmp(stage, "neighbor passes") == 0) {

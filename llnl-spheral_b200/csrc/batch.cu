@@ -261,8 +261,8 @@ int batch_init(Batch& b, cudaStream_t stream) {
 
 void batch_free(Batch& b) {
   if (b.stream) cudaStreamSynchronize(b.stream);
-  void* dev[] = {b.d_memRing, b.d_maps, b.d_gather, b.d_mapArena, b.d_memGraph};
-  dev_free_all(dev, 5);
+  void* dev[] = {b.d_memRing, b.d_maps, b.d_gather, b.d_mapArena, b.d_memGraph, b.d_fuse};
+  dev_free_all(dev, 6);
   cudaFreeHost(b.h_memRing);
   cudaFreeHost(b.h_maps);
   cudaFreeHost(b.h_gather);

@@ -97,6 +97,7 @@ __global__ void build_init_kernel(const Member* mem, int nmem) {
   setScalI(s, SC_NTOT, mem[m].n);
   setScalI(s, SC_G, 0);
   s[SC_HMAX] = 0.0;
+  for (int b = 0; b < 6; ++b) s[SC_PHMAX + b] = 0.0;
   s[SC_LMAXALL] = 0.0;
   unsigned long long* bb = reinterpret_cast<unsigned long long*>(s + SC_BOUNDS);
   for (int a = 0; a < 3; ++a) { bb[a] = ~0ULL; bb[3 + a] = 0ULL; }
@@ -294,6 +295,239 @@ __global__ void ghost_advance_kernel(const Member* mem, int nmem) {
   setScalI(M.scal, SC_NTOT, M.n + g);
   setScalI(M.scal, SC_G, g);
   M.scal[SC_HMAX] = 0.0;
+}
+
+// ---------------------------------------------------------------- fused ghost passes
+// The six boundary passes in one cooperative launch, for a batch of a few
+// members: the per-pass hmax, the flags, their prefix sum and the scatter
+// of the new images, separated by grid barriers.  An item's share of a
+// pass's hmax depends on the item alone, so the near-plane nodes give their
+// shares to every pass before the first one, and each new image to the
+// passes after its own as it is made; a pass then needs two barriers (after
+// its block counts, after its scatter).  Block k takes the k-th contiguous
+// chunk of a pass's items and numbers its images in item order, so the
+// images, their order and the error bits are those of the per-pass launches.
+__device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
+constexpr int kFusedGhostMembers = 4;
+constexpr int kFusedGhostBlocks = 148*2;
+constexpr int kBarrierPolls = 1 << 21;
+
+// Grid barrier of a cooperative launch (every block resident).  bar[0]
+// counts arrivals, bar[1] is the generation.  A block that polls more than
+// kBarrierPolls times records DERR_BARRIER in every member and returns
+// false; its launch then ends without finishing the passes.
+__device__ bool grid_barrier(unsigned int* bar, const Member* mem, int nm) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    volatile unsigned int* gen = bar + 1;
+    const unsigned int g0 = *gen;
+    __threadfence();
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      int polls = 0;
+      while (*gen == g0) {
+        if (++polls > kBarrierPolls) {
+          for (int m = 0; m < nm; ++m) atomicOr(mem[m].err, DERR_BARRIER);
+          ok = 0;
+          break;
+        }
+        __nanosleep(100);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// position of item node k (ghost positions are written during the launch:
+// read through L2)
+__device__ __forceinline__ V3 fusedPos(const Member& M, int64_t k) {
+  const int64_t n = M.n;
+  if (k < n) return V3{M.S[S_X*n + k], M.S[S_Y*n + k], M.S[S_Z*n + k]};
+  const int64_t g = k - n;
+  return V3{__ldcg(M.gpos + g), __ldcg(M.gpos + M.gcap + g), __ldcg(M.gpos + 2*M.gcap + g)};
+}
+__device__ __forceinline__ int32_t fusedRoot(const Member& M, int64_t k) {
+  return k < M.n ? (int32_t)k : __ldcg(M.groot + (k - M.n));
+}
+
+// an item's shares of the hmax of passes [from, 6) (ghost_hmax_kernel's test)
+__device__ __forceinline__ void hmaxShares(const Member& M, const V3& r, double hmaxi, int from, double* loc) {
+#pragma unroll
+  for (int b = 0; b < 6; ++b) {
+    if (b < from || !M.prm.bcs.periodic[b >> 1]) continue;
+    const PlanarBC& bc = M.prm.bcs.bc[b];
+    if (dmin(minimumDistance(bc.exit, r), minimumDistance(bc.enter, r)) < M.prm.kernelExtent*hmaxi)
+      loc[b] = dmax(loc[b], hmaxi);
+  }
+}
+
+// block maxima of the shares into the member's pass hmax words
+__device__ void hmaxFlush(const Member& M, double* loc, int from) {
+  __shared__ double red[6][kGhostThreads/32];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int b = 0; b < 6; ++b) {
+    double v = loc[b];
+    for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (lane == 0) red[b][w] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6 && (int)threadIdx.x >= from) {
+    double v = 0.0;
+    for (int k = 0; k < kGhostThreads/32; ++k) v = dmax(v, red[threadIdx.x][k]);
+    if (v > 0.0)
+      atomicMax(reinterpret_cast<unsigned long long*>(M.scal + SC_PHMAX + threadIdx.x),
+                (unsigned long long)__double_as_longlong(v));
+  }
+  __syncthreads();
+}
+
+// ghost_flag_kernel's test of item t for pass b
+__device__ __forceinline__ bool ghostFlag(const Member& M, int b, double hmax, int64_t t, int64_t nnear) {
+  if (!M.prm.bcs.periodic[b >> 1] || !(hmax > 0.0)) return false;
+  const V3 r = fusedPos(M, passNode(M, t, nnear));
+  const double disti = signedDistance(M.prm.bcs.bc[b].exit, r)/hmax;
+  return disti >= 0.0 && disti <= M.prm.kernelExtent;
+}
+
+__global__ void __launch_bounds__(kGhostThreads) ghost_passes_fused_kernel(const Member* mem, int nm, unsigned int* fuse) {
+  unsigned int* bar = fuse;
+  int64_t* blk = reinterpret_cast<int64_t*>(fuse + 2);      // [member][block] counts of a pass
+  const int nb = gridDim.x, kb = blockIdx.x;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ int64_t wsum[kGhostThreads/32];
+  __shared__ int64_t sG[kFusedGhostMembers];
+  __shared__ int64_t sPre, sTot;
+  if (threadIdx.x < kFusedGhostMembers) sG[threadIdx.x] = 0;
+  // the near-plane nodes' shares of every pass's hmax
+  for (int m = 0; m < nm; ++m) {
+    const Member& M = mem[m];
+    const int64_t nnear = scalI(M.scal, SC_NNEAR);
+    double loc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int64_t t = kb*(int64_t)blockDim.x + threadIdx.x; t < nnear; t += (int64_t)nb*blockDim.x) {
+      const int64_t k = M.cidx[t];
+      hmaxShares(M, nodePos(M, k), M.hmaxi[k], 0, loc);
+    }
+    hmaxFlush(M, loc, 0);
+  }
+  if (!grid_barrier(bar, mem, nm)) return;
+  for (int b = 0; b < 6; ++b) {
+    bool any = false;
+    for (int m = 0; m < nm; ++m) any = any || mem[m].prm.bcs.periodic[b >> 1];
+    if (!any) continue;
+    // flags of this block's chunk: the block's count
+    for (int m = 0; m < nm; ++m) {
+      const Member& M = mem[m];
+      const int64_t nnear = scalI(M.scal, SC_NNEAR);
+      const int64_t items = nnear + sG[m];
+      const int64_t chunk = (items + nb - 1)/nb;
+      const int64_t c0 = imin64(items, kb*chunk), c1 = imin64(items, c0 + chunk);
+      const double hmax = __longlong_as_double((long long)__ldcg(reinterpret_cast<const unsigned long long*>(M.scal + SC_PHMAX + b)));
+      int64_t cnt = 0;
+      for (int64_t t = c0 + threadIdx.x; t < c1; t += blockDim.x) cnt += ghostFlag(M, b, hmax, t, nnear) ? 1 : 0;
+      for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+      if (lane == 0) wsum[w] = cnt;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int64_t s = 0;
+        for (int k = 0; k < kGhostThreads/32; ++k) s += wsum[k];
+        blk[m*nb + kb] = s;
+      }
+      __syncthreads();
+    }
+    if (!grid_barrier(bar, mem, nm)) return;
+    // the block's offset among the chunks, the pass total, the scatter
+    for (int m = 0; m < nm; ++m) {
+      const Member& M = mem[m];
+      const int64_t n = M.n;
+      const int64_t nnear = scalI(M.scal, SC_NNEAR);
+      const int64_t G = sG[m];
+      const int64_t items = nnear + G;
+      const int64_t chunk = (items + nb - 1)/nb;
+      const int64_t c0 = imin64(items, kb*chunk), c1 = imin64(items, c0 + chunk);
+      const double hmax = __longlong_as_double((long long)__ldcg(reinterpret_cast<const unsigned long long*>(M.scal + SC_PHMAX + b)));
+      int64_t pre = 0, tot = 0;
+      for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        const int64_t c = __ldcg(blk + m*nb + k);
+        tot += c;
+        if (k < kb) pre += c;
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        pre += __shfl_xor_sync(0xffffffffu, pre, o);
+        tot += __shfl_xor_sync(0xffffffffu, tot, o);
+      }
+      __shared__ int64_t wpre[kGhostThreads/32];
+      if (lane == 0) { wsum[w] = tot; wpre[w] = pre; }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int64_t a = 0, c = 0;
+        for (int k = 0; k < kGhostThreads/32; ++k) { a += wpre[k]; c += wsum[k]; }
+        sPre = a;
+        sTot = c;
+      }
+      __syncthreads();
+      int64_t next = G + sPre;                         // ghost index of this block's first image
+      const PlanarBC& bc = M.prm.bcs.bc[b];
+      const int axis = b >> 1;
+      double loc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      for (int64_t base = c0; base < c1; base += blockDim.x) {
+        const int64_t t = base + threadIdx.x;
+        const bool f = t < c1 && ghostFlag(M, b, hmax, t, nnear);
+        const unsigned bal = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) wsum[w] = __popc(bal);
+        __syncthreads();
+        int64_t off = 0, tileTot = 0;
+        for (int k = 0; k < kGhostThreads/32; ++k) {
+          if (k < w) off += wsum[k];
+          tileTot += wsum[k];
+        }
+        off += __popc(bal & ((1u << lane) - 1u));
+        if (f) {
+          const int64_t k = passNode(M, t, nnear);
+          const int64_t g = next + off;
+          if (g >= M.gcap) {
+            atomicOr(M.err, DERR_GHOST_CAPACITY);
+          } else {
+            const V3 gp = mapPositionThroughPlanes(fusedPos(M, k), bc.exit, bc.enter);
+            const int32_t root = fusedRoot(M, k);
+            uint32_t code = k < n ? 0u : __ldcg(M.gcode + (k - n));
+            if ((code >> (2*axis)) & 3u) atomicOr(M.err, DERR_GHOST_CHAIN);
+            code |= (uint32_t)((b & 1) + 1) << (2*axis);
+            M.groot[g] = root;
+            M.gcode[g] = code;
+            M.gpos[g] = gp.x; M.gpos[M.gcap + g] = gp.y; M.gpos[2*M.gcap + g] = gp.z;
+            hmaxShares(M, gp, M.hmaxi[root], b + 1, loc);
+          }
+        }
+        next += tileTot;
+        __syncthreads();
+      }
+      hmaxFlush(M, loc, b + 1);
+      if (threadIdx.x == 0) {
+        int64_t g = G + sTot;
+        if (g > M.gcap) {
+          if (kb == 0) atomicOr(M.err, DERR_GHOST_CAPACITY);
+          g = M.gcap;
+        }
+        sG[m] = g;
+      }
+      __syncthreads();
+    }
+    if (!grid_barrier(bar, mem, nm)) return;
+  }
+  if (kb == 0 && threadIdx.x < nm) {
+    const Member& M = mem[threadIdx.x];
+    setScalI(M.scal, SC_NTOT, M.n + sG[threadIdx.x]);
+    setScalI(M.scal, SC_G, sG[threadIdx.x]);
+    M.scal[SC_HMAX] = 0.0;
+  }
 }
 
 // ---------------------------------------------------------------- cells
@@ -963,6 +1197,54 @@ int64_t planned_bytes(const sphgpu_config& cfg, int64_t n, int64_t G, int64_t E,
 
 namespace {
 
+// Grid of the fused ghost passes: every block must be resident at once.
+int fused_ghost_grid() {
+  static int grid = -1;
+  if (grid < 0) {
+    int dev = 0, sms = 0, occ = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ghost_passes_fused_kernel, kGhostThreads, 0) != cudaSuccess) {
+      cudaGetLastError();
+      grid = 0;
+    } else {
+      grid = sms*occ < kFusedGhostBlocks ? sms*occ : kFusedGhostBlocks;
+    }
+  }
+  return grid;
+}
+
+// The fused passes for this build: by the schedule, or (automatic) for a
+// batch of at most kFusedGhostMembers members.  Their scratch is allocated
+// outside a capture; a captured build without it takes the per-pass launches.
+bool use_fused_ghost_passes(Batch& b) {
+  const int nm = (int)b.mem.size();
+  if (b.ghostPasses == 1 || nm > kFusedGhostMembers || fused_ghost_grid() <= 0) return false;
+  if (b.d_fuse == nullptr) {
+    if (b.capturing) return false;
+    const size_t bytes = 2*sizeof(unsigned int) + sizeof(int64_t)*(size_t)kFusedGhostMembers*kFusedGhostBlocks + 8;
+    if (dev_alloc(reinterpret_cast<void**>(&b.d_fuse), bytes) != cudaSuccess) { cudaGetLastError(); return false; }
+    if (cudaMemset(b.d_fuse, 0, bytes) != cudaSuccess) { cudaGetLastError(); return false; }
+  }
+  return true;
+}
+
+int launch_fused_ghost_passes(Batch& b) {
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3((unsigned)fused_ghost_grid());
+  lc.blockDim = dim3(kGhostThreads);
+  lc.dynamicSmemBytes = 0;
+  lc.stream = b.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  const int nm = (int)b.mem.size();
+  return cuda_status(cudaLaunchKernelEx(&lc, ghost_passes_fused_kernel, (const Member*)b.d_mem, nm, b.d_fuse),
+                     "fused ghost passes");
+}
+
 int launch_build(Batch& b) {
   cudaStream_t st = b.stream;
   const int nm = (int)b.mem.size();
@@ -986,7 +1268,14 @@ int launch_build(Batch& b) {
     SPH_TRY(batch_scan(b, SCAN_COUNTS));
     near_list_kernel<<<ngrid, kGhostThreads, 0, st>>>(b.d_mem, nmap); batch_count_launch(b);
   }
-  for (int bnd = 0; bnd < 6; ++bnd) {
+  const bool fused = anyPeriodic && use_fused_ghost_passes(b);
+  if (anyPeriodic) b.lastGhostPasses = fused ? 2 : 1;
+  if (fused) {
+    SPH_CHECK(cudaMemsetAsync(b.d_fuse, 0, 2*sizeof(unsigned int), st));
+    SPH_TRY(launch_fused_ghost_passes(b));
+    batch_count_launch(b);
+  }
+  for (int bnd = 0; bnd < 6 && !fused; ++bnd) {
     bool any = false;
     for (Problem* p : b.mem) any = any || p->prm.bcs.periodic[bnd >> 1];
     if (!any) continue;
@@ -1146,6 +1435,10 @@ int build_connectivity(Batch& b) {
       if (herr & DERR_NONPOSITIVE) {
         set_error("non-positive or non-finite smoothing scale");
         return SPHGPU_ERR_NUMERIC;
+      }
+      if (herr & DERR_BARRIER) {
+        set_error("neighbor build: a grid barrier of the fused ghost passes timed out");
+        return SPHGPU_ERR_CUDA;
       }
       if (herr & DERR_GHOST_CAPACITY) { p.G = 2*p.gcap; redo = true; }        // ghost count unknown: double
       if (herr & DERR_ENTRY_CAPACITY) redo = true;                           // p.E is the true entry count

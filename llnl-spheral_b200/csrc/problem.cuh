@@ -314,6 +314,7 @@ enum DevError {
   DERR_GHOST_CAPACITY = 16,   // more ghosts than the ghost buffers hold (build is redone)
   DERR_ENTRY_CAPACITY = 32,   // more CSR entries than the entry buffers hold (build is redone)
   DERR_LIST_CAPACITY = 64,    // a neighbor list longer than the fill pass's list (build is redone)
+  DERR_BARRIER = 128,         // a grid barrier of the fused ghost passes waited past its limit
 };
 
 // Neighbor-walk schedules (values of sphgpu_set_schedule's "neighbor walk").
@@ -367,7 +368,8 @@ enum ScalSlot {
   SC_TIME = 40,        // current time (advanced by every completed step)
   SC_STEPS = 41,       // completed steps since the host last reset it (i64)
   SC_PAIRSUM = 42,     // pair interactions evaluated by all completed steps (i64)
-  NSCAL = 43
+  SC_PHMAX = 43,       // 6 ghost hmax words, one per boundary pass (fused ghost passes, double bits)
+  NSCAL = 49
 };
 
 // Sizes and grid of the current connectivity (device side).
@@ -462,6 +464,12 @@ struct Batch {
   // captured once per buffer layout, replayed for every step of a call
   // (on unless the "step graph" schedule is set to 0).
   bool useGraph = true;
+  // boundary passes of the ghost build: 0 = automatic (one cooperative
+  // launch for batches of at most kFusedGhostMembers members), 1 = four
+  // launches and a prefix sum per pass, 2 = one cooperative launch
+  int ghostPasses = 0;
+  int lastGhostPasses = 0;        // what the last build used (1 or 2; 0 before any periodic build)
+  unsigned int* d_fuse = nullptr; // fused ghost passes: grid barrier (2 words), then per-block counts
   uint64_t graphCandidate = 0;   // buffer layout of the last eager step (capture when it recurs)
   bool capturing = false;        // stream capture in progress: maps go to the arena
   bool capacityGrids = false;    // (n + ghosts)-sized kernels sized for the buffer capacity

@@ -633,8 +633,11 @@ enum UpdateMode { UPDATE_IN_PLACE = 0, UPDATE_SAVE_START = 1, UPDATE_FROM_START 
 // (only from the start-of-step state: mode UPDATE_FROM_START, the full update
 // of the RK2 step); a separate instance keeps the pair loop's registers out of
 // the other updates.
+#ifndef SPH_UPDATE_MIN_BLOCKS
+#define SPH_UPDATE_MIN_BLOCKS 6
+#endif
 template<bool COMPAT>
-__global__ void __launch_bounds__(128, 6) update_kernel(const Member* mem, BlockMap bm, double scale,
+__global__ void __launch_bounds__(128, SPH_UPDATE_MIN_BLOCKS) update_kernel(const Member* mem, BlockMap bm, double scale,
                                                      int timeAdvanceOnly, int mode, int packMode, int recordMid) {
   const MemberBlock mb = memberBlock(bm);
   const Member& MB = mem[mb.m];

@@ -88,7 +88,9 @@ def test_batch_evaluate_derivatives_matches_solo(gpu_lib, pkg):
 
 def test_batch_launch_count_independent_of_members(gpu_lib, pkg):
     """One launch per stage: a step of 2 members and of 5 members of the same
-    kind issue the same number of kernels."""
+    kind issue the same number of kernels (with the ghost passes as launches
+    per pass; the automatic schedule runs them as one cooperative launch for
+    batches of at most 4 members)."""
     abi = pkg.abi
     counts = []
     for nm in (2, 5):
@@ -97,6 +99,7 @@ def test_batch_launch_count_independent_of_members(gpu_lib, pkg):
             ns, cfg = _sod_member(pkg, 32 + 8 * k, 5.0 / 3.0, 4.0, abi.PRECISION_MIXED, 10 + k)
             mem.append(pkg.SPHHydro(cfg, ns))
         batch = pkg.SPHBatch(mem)
+        batch.set_schedule("ghost passes", 1)
         batch.step(1)
         before = batch.kernel_launches()
         batch.step(1)

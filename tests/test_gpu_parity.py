@@ -95,6 +95,30 @@ def test_connectivity_every_schedule(gpu_lib, pkg, oracle_mod, case, schedule, n
     assert g.num_pairs() == o.num_pairs()
 
 
+@pytest.mark.parametrize("case", ["sod", "kh", "sod_x_periodic_only"])
+@pytest.mark.parametrize("passes", [1, 2])
+def test_ghost_passes_every_schedule(gpu_lib, pkg, oracle_mod, case, passes):
+    """The six boundary passes as four launches and a prefix sum each, or all
+    in one cooperative launch with grid barriers, make the reference's ghosts
+    (roots, positions, order) and the same CSR."""
+    g, o, ns = _pair(pkg, oracle_mod, case)
+    g.set_schedule("ghost passes", passes)
+    g.build_neighbors()
+    assert g.schedule("ghost passes") == passes
+    o.build_neighbors()
+    go, gn, gr = g.connectivity()
+    oo, on, orr = o.connectivity()
+    assert np.array_equal(gr, orr)
+    assert np.array_equal(g.ghost_positions(), o.ghost_positions())
+    assert np.array_equal(go, oo)
+    assert np.array_equal(gn, on)
+    # and again after steps (the graph-replayed rebuild)
+    g.step(3)
+    o.step(3)
+    assert np.array_equal(g.connectivity()[2], o.connectivity()[2])
+    assert np.array_equal(g.connectivity()[1], o.connectivity()[1])
+
+
 @pytest.mark.parametrize("case", list(CASES))
 def test_evaluate_derivatives_parity(gpu_lib, pkg, oracle_mod, case):
     g, o, ns = _pair(pkg, oracle_mod, case)
