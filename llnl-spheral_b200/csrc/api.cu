@@ -222,27 +222,70 @@ Batch& solo(Problem* p) {
   return *p->solo;
 }
 
-// AoS host array -> SoA fields of S (via the device staging buffer).
-int upload_aos(Problem& p, const double* host, int comps, int field, bool device) {
-  if (host == nullptr) return SPHGPU_OK;
-  const int64_t cnt = p.n*comps;
-  const double* src = host;
-  if (!device) {
-    SPH_CHECK(cudaMemcpyAsync(p.staging, host, sizeof(double)*(size_t)cnt, cudaMemcpyHostToDevice, p.stream));
-    src = p.staging;
+// AoS host arrays -> SoA fields of S (via the device staging buffer).  The
+// host-to-device copies go back to back into the staging buffer (9 n
+// doubles: position, velocity, mass, density and energy at once, then H), a
+// transpose kernel follows each group, and the call synchronises once, at
+// its end (the caller's arrays are free again then).
+struct AosField { const double* host; int comps; int field; };
+
+int upload_group(Problem& p, const AosField* f, int nf, bool device) {
+  int64_t off = 0;
+  const double* src[6];
+  for (int k = 0; k < nf; ++k) {
+    src[k] = f[k].host;
+    if (f[k].host == nullptr || device) continue;
+    const int64_t cnt = p.n*f[k].comps;
+    SPH_CHECK(cudaMemcpyAsync(p.staging + off, f[k].host, sizeof(double)*(size_t)cnt, cudaMemcpyHostToDevice,
+                              p.stream));
+    src[k] = p.staging + off;
+    off += cnt;
   }
-  aos_to_soa_kernel<<<grid1(cnt), 256, 0, p.stream>>>(src, comps, p.n, p.S + (int64_t)field*p.n); ++p.launches;
+  for (int k = 0; k < nf; ++k) {
+    if (f[k].host == nullptr) continue;
+    const int64_t cnt = p.n*f[k].comps;
+    aos_to_soa_kernel<<<grid1(cnt), 256, 0, p.stream>>>(src[k], f[k].comps, p.n, p.S + (int64_t)f[k].field*p.n);
+    ++p.launches;
+  }
+  return cuda_status(cudaGetLastError(), "set_state (transpose)");
+}
+
+int upload_state(Problem& p, const double* pos, const double* vel, const double* mass, const double* rho,
+                 const double* eps, const double* H, bool device) {
+  const AosField g1[5] = {{pos, 3, S_X}, {vel, 3, S_VX}, {mass, 1, S_M}, {rho, 1, S_RHO}, {eps, 1, S_EPS}};
+  const AosField g2[1] = {{H, 6, S_H}};
+  SPH_TRY(upload_group(p, g1, 5, device));
+  SPH_TRY(upload_group(p, g2, 1, device));      // reuses the staging buffer after the first transposes
+  return SPHGPU_OK;
+}
+
+// SoA fields -> AoS host arrays: transpose into the staging buffer, then the
+// device-to-host copies back to back; one synchronisation at the end.
+int download_group(Problem& p, const double* base, const AosField* f, int nf) {
+  int64_t off = 0;
+  int64_t at[6];
+  for (int k = 0; k < nf; ++k) {
+    at[k] = off;
+    if (f[k].host == nullptr) continue;
+    const int64_t cnt = p.n*f[k].comps;
+    soa_to_aos_kernel<<<grid1(cnt), 256, 0, p.stream>>>(base + (int64_t)f[k].field*p.n, f[k].comps, p.n,
+                                                        p.staging + off);
+    ++p.launches;
+    off += cnt;
+  }
   SPH_CHECK(cudaGetLastError());
-  if (!device) SPH_CHECK(cudaStreamSynchronize(p.stream));
+  for (int k = 0; k < nf; ++k) {
+    if (f[k].host == nullptr) continue;
+    SPH_CHECK(cudaMemcpyAsync(const_cast<double*>(f[k].host), p.staging + at[k],
+                              sizeof(double)*(size_t)(p.n*f[k].comps), cudaMemcpyDeviceToHost, p.stream));
+  }
   return SPHGPU_OK;
 }
 
 int download_aos(Problem& p, const double* base, int comps, int field, double* host) {
   if (host == nullptr) return SPHGPU_OK;
-  const int64_t cnt = p.n*comps;
-  soa_to_aos_kernel<<<grid1(cnt), 256, 0, p.stream>>>(base + (int64_t)field*p.n, comps, p.n, p.staging); ++p.launches;
-  SPH_CHECK(cudaGetLastError());
-  SPH_CHECK(cudaMemcpyAsync(host, p.staging, sizeof(double)*(size_t)cnt, cudaMemcpyDeviceToHost, p.stream));
+  const AosField f[1] = {{host, comps, field}};
+  SPH_TRY(download_group(p, base, f, 1));
   SPH_CHECK(cudaStreamSynchronize(p.stream));
   return SPHGPU_OK;
 }
@@ -276,12 +319,7 @@ int batch_check_errors(Batch& b, const char* where) {
 
 int set_state_impl(Problem& p, const double* pos, const double* vel, const double* mass, const double* rho,
                    const double* eps, const double* H, bool device) {
-  SPH_TRY(upload_aos(p, pos, 3, S_X, device));
-  SPH_TRY(upload_aos(p, vel, 3, S_VX, device));
-  SPH_TRY(upload_aos(p, mass, 1, S_M, device));
-  SPH_TRY(upload_aos(p, rho, 1, S_RHO, device));
-  SPH_TRY(upload_aos(p, eps, 1, S_EPS, device));
-  SPH_TRY(upload_aos(p, H, 6, S_H, device));
+  SPH_TRY(upload_state(p, pos, vel, mass, rho, eps, H, device));
   // initializeProblemStartup: omega = 1, P and cs from the EOS.
   fill_kernel<<<grid1(p.n), 256, 0, p.stream>>>(p.S + (int64_t)S_OMEGA*p.n, p.n, 1.0); ++p.launches;
   SPH_TRY(launch_eos(solo(&p)));
@@ -1120,12 +1158,12 @@ int sphgpu_set_state_device(sphgpu_problem* p, const double* position, const dou
 int sphgpu_get_state(sphgpu_problem* p, double* position, double* velocity, double* mass, double* massDensity,
                      double* specificThermalEnergy, double* H) {
   if (p == nullptr) return SPHGPU_ERR_ARG;
-  SPH_TRY(download_aos(*p, p->S, 3, S_X, position));
-  SPH_TRY(download_aos(*p, p->S, 3, S_VX, velocity));
-  SPH_TRY(download_aos(*p, p->S, 1, S_M, mass));
-  SPH_TRY(download_aos(*p, p->S, 1, S_RHO, massDensity));
-  SPH_TRY(download_aos(*p, p->S, 1, S_EPS, specificThermalEnergy));
-  SPH_TRY(download_aos(*p, p->S, 6, S_H, H));
+  const AosField g1[5] = {{position, 3, S_X}, {velocity, 3, S_VX}, {mass, 1, S_M}, {massDensity, 1, S_RHO},
+                          {specificThermalEnergy, 1, S_EPS}};
+  const AosField g2[1] = {{H, 6, S_H}};
+  SPH_TRY(download_group(*p, p->S, g1, 5));
+  SPH_TRY(download_group(*p, p->S, g2, 1));     // stream order: after the first group's copies
+  SPH_CHECK(cudaStreamSynchronize(p->stream));
   return SPHGPU_OK;
 }
 

@@ -309,7 +309,10 @@ __global__ void ghost_advance_kernel(const Member* mem, int nmem) {
 // images, their order and the error bits are those of the per-pass launches.
 __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
 constexpr int kFusedGhostMembers = 4;
-constexpr int kFusedGhostBlocks = 148*2;
+#ifndef FUSED_GHOST_MIN_BLOCKS
+#define FUSED_GHOST_MIN_BLOCKS 2
+#endif
+constexpr int kFusedGhostBlocks = 148*FUSED_GHOST_MIN_BLOCKS;
 constexpr int kBarrierPolls = 1 << 21;
 
 // Grid barrier of a cooperative launch (every block resident).  bar[0]
@@ -397,7 +400,7 @@ __device__ __forceinline__ bool ghostFlag(const Member& M, int b, double hmax, i
   return disti >= 0.0 && disti <= M.prm.kernelExtent;
 }
 
-__global__ void __launch_bounds__(kGhostThreads) ghost_passes_fused_kernel(const Member* mem, int nm, unsigned int* fuse) {
+__global__ void __launch_bounds__(kGhostThreads, FUSED_GHOST_MIN_BLOCKS) ghost_passes_fused_kernel(const Member* mem, int nm, unsigned int* fuse) {
   unsigned int* bar = fuse;
   int64_t* blk = reinterpret_cast<int64_t*>(fuse + 2);      // [member][block] counts of a pass
   const int nb = gridDim.x, kb = blockIdx.x;
