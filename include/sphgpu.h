@@ -191,6 +191,18 @@ int sphgpu_dt(sphgpu_problem* p, double* dt_out);
 /* CheapSynchronousRK2::step (src/Integrator/CheapSynchronousRK2.cc:81-143),
  * nsteps times; *time advances, *last_dt receives the last step size. */
 int sphgpu_step_rk2(sphgpu_problem* p, double* time, int64_t nsteps, double* last_dt);
+/* One CheapSynchronousRK2::step (src/Integrator/CheapSynchronousRK2.cc:81-143)
+ * of a state that lives in host arrays, as the reference's integrator holds
+ * it in its Fields: the state in (as sphgpu_set_state; all six inputs
+ * required), one step, the new state out (as sphgpu_get_state; a NULL
+ * output is skipped; outputs may alias the inputs).  Same results as those
+ * three calls.  The position and H copies go first; for SPH problems the
+ * ghost and connectivity rebuild, which reads only those, is queued before
+ * the rest of the state is copied on a second stream.  Synchronous. */
+int sphgpu_step_rk2_host(sphgpu_problem* p, const double* position, const double* velocity, const double* mass,
+                         const double* massDensity, const double* specificThermalEnergy, const double* H,
+                         double* position_out, double* velocity_out, double* mass_out, double* massDensity_out,
+                         double* specificThermalEnergy_out, double* H_out, double* time, double* last_dt);
 /* Integrator::currentTime and lastDt (src/Integrator/Integrator.hh) of the problem. */
 int sphgpu_time(sphgpu_problem* p, double* time, double* last_dt);
 /* iterateIdealH (src/Utilities/iterateIdealH.cc:26-349) as the reference's

@@ -156,6 +156,7 @@ def load_library(path=None):
         getattr(lib, name).argtypes = [P, ctypes.c_double, ctypes.c_double]
     lib.sphgpu_dt.argtypes = [P, D]
     lib.sphgpu_step_rk2.argtypes = [P, D, I64, D]
+    lib.sphgpu_step_rk2_host.argtypes = [P] + [P] * 12 + [D, D]
     lib.sphgpu_conservation.argtypes = [P, P]
     lib.sphgpu_iterate_ideal_h.argtypes = [P, ctypes.c_int32, ctypes.c_double, ctypes.POINTER(ctypes.c_int32),
                                            ctypes.POINTER(ctypes.c_double)]

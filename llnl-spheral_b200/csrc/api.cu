@@ -208,6 +208,10 @@ void free_problem(Problem* p) {
                   p->wsumBinsTab, p->qgrad, p->Kheld, p->fshear};
   dev_free_all(ptrs, (int)(sizeof(ptrs)/sizeof(ptrs[0])));
   if (p->pinned) cudaFreeHost(p->pinned);
+  if (p->stagingB) { void* sb[] = {p->stagingB}; dev_free_all(sb, 1); }
+  if (p->evCopyStart) cudaEventDestroy(p->evCopyStart);
+  if (p->evCopyDone) cudaEventDestroy(p->evCopyDone);
+  if (p->copyStream) cudaStreamDestroy(p->copyStream);
   if (p->solo) { batch_free(*p->solo); delete p->solo; p->solo = nullptr; }
   if (p->ownStream && p->stream) cudaStreamDestroy(p->stream);
   delete p;
@@ -229,22 +233,23 @@ Batch& solo(Problem* p) {
 // its end (the caller's arrays are free again then).
 struct AosField { const double* host; int comps; int field; };
 
-int upload_group(Problem& p, const AosField* f, int nf, bool device) {
+int upload_group(Problem& p, const AosField* f, int nf, bool device, double* staging, cudaStream_t st,
+                 cudaEvent_t copied = nullptr) {
   int64_t off = 0;
   const double* src[6];
   for (int k = 0; k < nf; ++k) {
     src[k] = f[k].host;
     if (f[k].host == nullptr || device) continue;
     const int64_t cnt = p.n*f[k].comps;
-    SPH_CHECK(cudaMemcpyAsync(p.staging + off, f[k].host, sizeof(double)*(size_t)cnt, cudaMemcpyHostToDevice,
-                              p.stream));
-    src[k] = p.staging + off;
+    SPH_CHECK(cudaMemcpyAsync(staging + off, f[k].host, sizeof(double)*(size_t)cnt, cudaMemcpyHostToDevice, st));
+    src[k] = staging + off;
     off += cnt;
   }
+  if (copied) SPH_CHECK(cudaEventRecord(copied, st));
   for (int k = 0; k < nf; ++k) {
     if (f[k].host == nullptr) continue;
     const int64_t cnt = p.n*f[k].comps;
-    aos_to_soa_kernel<<<grid1(cnt), 256, 0, p.stream>>>(src[k], f[k].comps, p.n, p.S + (int64_t)f[k].field*p.n);
+    aos_to_soa_kernel<<<grid1(cnt), 256, 0, st>>>(src[k], f[k].comps, p.n, p.S + (int64_t)f[k].field*p.n);
     ++p.launches;
   }
   return cuda_status(cudaGetLastError(), "set_state (transpose)");
@@ -254,8 +259,8 @@ int upload_state(Problem& p, const double* pos, const double* vel, const double*
                  const double* eps, const double* H, bool device) {
   const AosField g1[5] = {{pos, 3, S_X}, {vel, 3, S_VX}, {mass, 1, S_M}, {rho, 1, S_RHO}, {eps, 1, S_EPS}};
   const AosField g2[1] = {{H, 6, S_H}};
-  SPH_TRY(upload_group(p, g1, 5, device));
-  SPH_TRY(upload_group(p, g2, 1, device));      // reuses the staging buffer after the first transposes
+  SPH_TRY(upload_group(p, g1, 5, device, p.staging, p.stream));
+  SPH_TRY(upload_group(p, g2, 1, device, p.staging, p.stream));   // reuses the staging buffer after the first transposes
   return SPHGPU_OK;
 }
 
@@ -307,7 +312,11 @@ int batch_check_errors(Batch& b, const char* where) {
     if (herr & DERR_NBR_CAPACITY) { msg += " neighbor capacity exceeded;"; r = SPHGPU_ERR_CAPACITY; }
     if (herr & DERR_GHOST_CHAIN) { msg += " ghost imaged twice on one axis;"; r = SPHGPU_ERR_UNSUPPORTED; }
     if (herr & DERR_NONPOSITIVE) { msg += " non-positive mass/density/det(H) or non-finite state;"; r = SPHGPU_ERR_NUMERIC; }
-    if (herr & DERR_BARRIER) { msg += " a grid barrier of the fused ghost passes timed out;"; r = SPHGPU_ERR_CUDA; }
+    if (herr & DERR_BARRIER) {
+      msg += " a grid barrier of the fused ghost passes timed out;";
+      r = SPHGPU_ERR_CUDA;
+      if (b.d_fuse) cudaMemsetAsync(b.d_fuse, 0, 2*sizeof(unsigned int), b.stream);
+    }
     if (rc == SPHGPU_OK) rc = r;
   }
   if (rc != SPHGPU_OK) {
@@ -317,17 +326,22 @@ int batch_check_errors(Batch& b, const char* where) {
   return rc;
 }
 
-int set_state_impl(Problem& p, const double* pos, const double* vel, const double* mass, const double* rho,
-                   const double* eps, const double* H, bool device) {
-  SPH_TRY(upload_state(p, pos, vel, mass, rho, eps, H, device));
-  // initializeProblemStartup: omega = 1, P and cs from the EOS.
+// initializeProblemStartup after new state: omega = 1, P and cs from the
+// EOS, the state checked, the restart copies of the compatible energy.
+int startup_after_upload(Problem& p, const char* where) {
   fill_kernel<<<grid1(p.n), 256, 0, p.stream>>>(p.S + (int64_t)S_OMEGA*p.n, p.n, 1.0); ++p.launches;
   SPH_TRY(launch_eos(solo(&p)));
   check_state_kernel<<<grid1(p.n), 256, 0, p.stream>>>(p.S, p.n, p.d_err); ++p.launches;
   startup_restart_kernel<<<grid1(p.n), 256, 0, p.stream>>>(p.S, p.S0, p.n, p.cfg.gamma,
                                                            p.cfg.compatibleEnergyEvolution); ++p.launches;
   SPH_CHECK(cudaGetLastError());
-  SPH_TRY(batch_check_errors(solo(&p), "set_state"));
+  return batch_check_errors(solo(&p), where);
+}
+
+int set_state_impl(Problem& p, const double* pos, const double* vel, const double* mass, const double* rho,
+                   const double* eps, const double* H, bool device) {
+  SPH_TRY(upload_state(p, pos, vel, mass, rho, eps, H, device));
+  SPH_TRY(startup_after_upload(p, "set_state"));
   p.haveNbrs = false;
   p.crkVolumeReady = false;
   p.omegaResetByStep = false;
@@ -663,9 +677,16 @@ int capture_full_step(Batch& b) {
 
 // One eager CheapSynchronousRK2 step of every member (host read-backs after
 // the rebuild and after the step).
+int step_finish(Batch& b);
+
 int step_impl(Batch& b) {
   // preStepInitialize: ghosts + connectivity every cycle, then ghost state.
   SPH_TRY(build_neighbors_impl(b));
+  return step_finish(b);
+}
+
+// The step after the connectivity, then the host's step bookkeeping.
+int step_finish(Batch& b) {
   SPH_TRY(step_after_connectivity(b));
   const int slots[2] = {SC_DT, -1};
   std::vector<double> res;
@@ -785,6 +806,76 @@ int steps_impl(Batch& b, int64_t nsteps) {
       ++done;
     }
   }
+  return SPHGPU_OK;
+}
+
+// One RK2 step with the state in and out of host arrays: what
+// set_state + step_rk2(1) + get_state do, with the position and H copies
+// first and, for SPH problems, the ghost/connectivity rebuild (which reads
+// only those) launched while velocity, mass, density and energy still cross
+// the host link on the copy stream.  Same results as the three calls.
+int step_host_impl(Problem& p, const double* const in[6], double* const out[6]) {
+  for (int k = 0; k < 6; ++k) {
+    if (in[k] == nullptr) { set_error("sphgpu_step_rk2_host: every input array is required"); return SPHGPU_ERR_ARG; }
+  }
+  if (p.copyStream == nullptr) {
+    SPH_CHECK(cudaStreamCreateWithFlags(&p.copyStream, cudaStreamNonBlocking));
+    SPH_CHECK(cudaEventCreateWithFlags(&p.evCopyStart, cudaEventDisableTiming));
+    SPH_CHECK(cudaEventCreateWithFlags(&p.evCopyDone, cudaEventDisableTiming));
+  }
+  if (p.stagingB == nullptr && dev_alloc(reinterpret_cast<void**>(&p.stagingB), sizeof(double)*6*(size_t)p.n) != cudaSuccess) {
+    p.stagingB = nullptr;
+    set_error("sphgpu_step_rk2_host: staging allocation failed");
+    return SPHGPU_ERR_NOMEM;
+  }
+  const bool overlap = p.cfg.hydro != SPHGPU_HYDRO_CRKSPH;
+  // the copy stream starts after the position and H copies (and everything
+  // queued before them on the problem's stream): on a shared host link the
+  // two groups would otherwise split the bandwidth and the first would
+  // finish no earlier than the whole state
+  const AosField ga[2] = {{in[0], 3, S_X}, {in[5], 6, S_H}};
+  const AosField gb[4] = {{in[1], 3, S_VX}, {in[2], 1, S_M}, {in[3], 1, S_RHO}, {in[4], 1, S_EPS}};
+  SPH_TRY(upload_group(p, ga, 2, false, p.staging, p.stream, p.evCopyStart));
+  SPH_CHECK(cudaStreamWaitEvent(p.copyStream, p.evCopyStart, 0));
+  Batch& b = solo(&p);
+  bool second = false;
+  auto copySecond = [&]() {
+    second = true;
+    SPH_TRY(upload_group(p, gb, 4, false, p.stagingB, p.copyStream));
+    return cuda_status(cudaEventRecord(p.evCopyDone, p.copyStream), "step_rk2_host (copy event)");
+  };
+  if (overlap) {
+    // the rebuild's host-to-device traffic (its descriptors) goes first, and
+    // its kernels are queued before the second copy group is issued
+    SPH_TRY(plan_build(b));
+    SPH_TRY(batch_upload(b));
+    b.buildPlanned = true;
+    b.afterBuildLaunch = copySecond;
+    p.haveNbrs = false;
+    const int rc = build_neighbors_impl(b);
+    b.buildPlanned = false;
+    b.afterBuildLaunch = nullptr;
+    if (!second) SPH_TRY(copySecond());
+    SPH_TRY(rc);
+    SPH_CHECK(cudaStreamWaitEvent(p.stream, p.evCopyDone, 0));
+    SPH_TRY(startup_after_upload(p, "step_rk2_host"));
+  } else {
+    // CRKSPH: the start-up volume of the build reads the whole state
+    SPH_TRY(copySecond());
+    SPH_CHECK(cudaStreamWaitEvent(p.stream, p.evCopyDone, 0));
+    SPH_TRY(startup_after_upload(p, "step_rk2_host"));
+    p.haveNbrs = false;
+    p.crkVolumeReady = false;
+    SPH_TRY(build_neighbors_impl(solo(&p)));
+  }
+  p.omegaResetByStep = false;
+  SPH_TRY(step_finish(solo(&p)));
+  const AosField o1[5] = {{out[0], 3, S_X}, {out[1], 3, S_VX}, {out[2], 1, S_M}, {out[3], 1, S_RHO},
+                          {out[4], 1, S_EPS}};
+  const AosField o2[1] = {{out[5], 6, S_H}};
+  SPH_TRY(download_group(p, p.S, o1, 5));
+  SPH_TRY(download_group(p, p.S, o2, 1));
+  SPH_CHECK(cudaStreamSynchronize(p.stream));
   return SPHGPU_OK;
 }
 
@@ -1367,6 +1458,20 @@ int sphgpu_step_rk2(sphgpu_problem* p, double* time, int64_t nsteps, double* las
   if (p == nullptr || nsteps < 0) return SPHGPU_ERR_ARG;
   if (time) p->time = *time;
   SPH_TRY(steps_impl(solo(p), nsteps));
+  if (time) *time = p->time;
+  if (last_dt) *last_dt = p->lastDt;
+  return SPHGPU_OK;
+}
+
+int sphgpu_step_rk2_host(sphgpu_problem* p, const double* position, const double* velocity, const double* mass,
+                         const double* massDensity, const double* specificThermalEnergy, const double* H,
+                         double* position_out, double* velocity_out, double* mass_out, double* massDensity_out,
+                         double* specificThermalEnergy_out, double* H_out, double* time, double* last_dt) {
+  if (p == nullptr) return SPHGPU_ERR_ARG;
+  const double* const in[6] = {position, velocity, mass, massDensity, specificThermalEnergy, H};
+  double* const out[6] = {position_out, velocity_out, mass_out, massDensity_out, specificThermalEnergy_out, H_out};
+  if (time) p->time = *time;
+  SPH_TRY(step_host_impl(*p, in, out));
   if (time) *time = p->time;
   if (last_dt) *last_dt = p->lastDt;
   return SPHGPU_OK;

@@ -1253,7 +1253,8 @@ int launch_build(Batch& b) {
   const int nm = (int)b.mem.size();
   for (Problem* p : b.mem) p->paccReady = false;   // the walk parks its lists in pacc
   // (a captured build reads the descriptor slot uploaded before the capture)
-  if (!b.capturing) SPH_TRY(batch_upload(b));
+  if (!b.capturing && !b.buildPlanned) SPH_TRY(batch_upload(b));
+  b.buildPlanned = false;
   // ---- ghosts: six planar boundaries in order, sizes kept on the device
   build_init_kernel<<<(nm + 127)/128, 128, 0, st>>>(b.d_mem, nm); batch_count_launch(b);
   // fixed grids: at most kStreamBlocks blocks per member, member-local stride
@@ -1274,7 +1275,8 @@ int launch_build(Batch& b) {
   const bool fused = anyPeriodic && use_fused_ghost_passes(b);
   if (anyPeriodic) b.lastGhostPasses = fused ? 2 : 1;
   if (fused) {
-    SPH_CHECK(cudaMemsetAsync(b.d_fuse, 0, 2*sizeof(unsigned int), st));
+    // (the barrier's arrival counter is back at zero after every completed
+    // barrier; a build that reported a timed-out barrier clears it)
     SPH_TRY(launch_fused_ghost_passes(b));
     batch_count_launch(b);
   }
@@ -1409,8 +1411,13 @@ int build_connectivity(Batch& b) {
     if (p->n + p->gcap > INT_MAX) { set_error("too many nodes for 32-bit neighbor indices"); return SPHGPU_ERR_CAPACITY; }
   }
   for (int attempt = 0; attempt < 6; ++attempt) {
-    SPH_TRY(plan_capacities(b));
+    if (!(attempt == 0 && b.buildPlanned)) SPH_TRY(plan_capacities(b));
     SPH_TRY(launch_build(b));
+    if (b.afterBuildLaunch) {
+      const std::function<int()> f = std::move(b.afterBuildLaunch);
+      b.afterBuildLaunch = nullptr;
+      SPH_TRY(f());
+    }
     const int slots[7] = {SC_G, SC_TOTAL, SC_MAXCOUNT, SC_PAIRS, SC_NCELLS, SC_CELLSWANTED, -1};
     std::vector<double> r;
     SPH_TRY(batch_gather(b, slots, 7, r));
@@ -1440,6 +1447,7 @@ int build_connectivity(Batch& b) {
         return SPHGPU_ERR_NUMERIC;
       }
       if (herr & DERR_BARRIER) {
+        if (b.d_fuse) cudaMemsetAsync(b.d_fuse, 0, 2*sizeof(unsigned int), b.stream);
         set_error("neighbor build: a grid barrier of the fused ghost passes timed out");
         return SPHGPU_ERR_CUDA;
       }

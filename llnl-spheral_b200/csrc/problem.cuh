@@ -18,6 +18,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <functional>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -295,6 +296,12 @@ struct Problem {
   double* hmaxi = nullptr;      // [2][n] 1/min(eig(H)), max(eig(H)) of each internal node, per build
   double* pinned = nullptr;     // pinned host staging for get/set
   int64_t pinnedcap = 0;
+  // sphgpu_step_rk2_host (made on its first call): a copy stream, its
+  // events and a second staging buffer (6 n doubles) for the state that
+  // crosses the host link while the connectivity is rebuilt
+  cudaStream_t copyStream = nullptr;
+  cudaEvent_t evCopyStart = nullptr, evCopyDone = nullptr;
+  double* stagingB = nullptr;
 
   Batch* solo = nullptr;        // this problem as a batch of one
   int64_t launches = 0;         // kernels launched for this problem (diagnostics)
@@ -470,6 +477,12 @@ struct Batch {
   int ghostPasses = 0;
   int lastGhostPasses = 0;        // what the last build used (1 or 2; 0 before any periodic build)
   unsigned int* d_fuse = nullptr; // fused ghost passes: grid barrier (2 words), then per-block counts
+  // the next build's capacities are planned and its descriptors uploaded
+  // already (sphgpu_step_rk2_host does both before its copy stream starts)
+  bool buildPlanned = false;
+  // called once right after the next build's launches are enqueued, before
+  // its read-back (sphgpu_step_rk2_host enqueues its second copy group there)
+  std::function<int()> afterBuildLaunch;
   uint64_t graphCandidate = 0;   // buffer layout of the last eager step (capture when it recurs)
   bool capturing = false;        // stream capture in progress: maps go to the arena
   bool capacityGrids = false;    // (n + ghosts)-sized kernels sized for the buffer capacity

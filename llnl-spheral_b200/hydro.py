@@ -171,6 +171,21 @@ class SPHHydro:
         self.time = t.value
         return t.value, dt.value
 
+    def step_host(self, state_in, state_out=None):
+        """One RK2 step of a host-resident state (sphgpu_step_rk2_host):
+        state_in holds the six arrays of set_state (float64, C order),
+        state_out six arrays that receive the new state (None: state_in)."""
+        state_out = state_in if state_out is None else state_out
+        for a in list(state_in) + list(state_out):
+            if a is not None and (a.dtype != np.float64 or not a.flags.c_contiguous):
+                raise ValueError("step_host arrays must be C-contiguous float64")
+        t = ctypes.c_double(self.time)
+        dt = ctypes.c_double()
+        ptrs = [_p(a) for a in state_in] + [None if a is None else _p(a) for a in state_out]
+        abi.check(self.lib.sphgpu_step_rk2_host(self.h, *ptrs, ctypes.byref(t), ctypes.byref(dt)), self.lib)
+        self.time = t.value
+        return t.value, dt.value
+
     def conservation(self):
         out = np.empty(8)
         abi.check(self.lib.sphgpu_conservation(self.h, _p(out)), self.lib)
