@@ -355,8 +355,7 @@ def measure_build(h, reps=10):
 def measure_e2e(pkg, ns, cfg, steps, warmup):
     """Public API with host buffers: per step one sphgpu_step_rk2_host call
     takes the state host->device from pinned memory, runs one RK2 step and
-    brings the new state back device->host into the same arrays (the
-    rebuild overlaps the copy of the velocity, mass, density and energy)."""
+    brings the new state back device->host into the same arrays."""
     import torch
     n = ns.n
 
